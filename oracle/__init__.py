@@ -1,0 +1,207 @@
+"""CPU checkers for the LELA hot path -- TEST INFRASTRUCTURE ONLY.
+
+Two libraries sit behind this module:
+
+* ``oracle/liboracle.so`` -- the plain-C restatement in ``lela_oracle.c``
+  (every function cites the LELA routine it restates);
+* ``oracle/_ref/liblela_ref.so`` -- LELA's own CPU code, compiled from the
+  unmodified reference sources by ``oracle/Makefile`` (present only where the
+  reference tree was available at build time, or where the prebuilt file was
+  carried along).
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
+``bench.py`` may import this package, and only as the checker.  The product
+(``lela_b200``) never imports it.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_P = ctypes.c_void_p
+_S = ctypes.c_size_t
+_U = ctypes.c_uint32
+_I = ctypes.c_int
+
+_lib = None
+_ref = None
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def lib():
+    """The C restatement (liboracle.so); built on first use if missing."""
+    global _lib
+    if _lib is None:
+        path = os.path.join(_HERE, "liboracle.so")
+        if not os.path.exists(path):
+            import subprocess
+            subprocess.run(["make", "-C", _HERE, "liboracle.so"], check=True,
+                           stdout=subprocess.DEVNULL)
+        L = ctypes.CDLL(path)
+        L.oracle_gemm_zp_u32.argtypes = [_U, _S, _S, _S, _U, _P, _S, _P, _S, _U, _P, _S]
+        L.oracle_gemm_zp_u32_threads.argtypes = [_I, _U, _S, _S, _S, _U, _P, _S, _P, _S, _U, _P, _S]
+        L.oracle_trsm_zp_u32.argtypes = [_U, _I, _I, _S, _S, _U, _P, _S, _P, _S, ctypes.POINTER(_S)]
+        L.oracle_echelon_zp_u32.argtypes = [_U, _S, _S, _P, _S, ctypes.POINTER(_S), ctypes.POINTER(_U)]
+        L.oracle_fl_echelonize_zp_u32.argtypes = [_U, _S, _S, _P, _P, _P, _I, _I, _P, _S,
+                                                  ctypes.POINTER(_S), ctypes.POINTER(_U),
+                                                  ctypes.POINTER(_S), ctypes.POINTER(_S)]
+        L.oracle_gemm_gf2.argtypes = [_S, _S, _S, _I, _P, _S, _P, _S, _I, _P, _S]
+        L.oracle_echelon_gf2.argtypes = [_S, _S, _P, _S, ctypes.POINTER(_S)]
+        L.oracle_inv_zp.argtypes = [_U, _U]
+        L.oracle_inv_zp.restype = _U
+        _lib = L
+    return _lib
+
+
+def ref_path():
+    return os.path.join(_HERE, "_ref", "liblela_ref.so")
+
+
+def have_ref():
+    return os.path.exists(ref_path())
+
+
+def ref():
+    """LELA's own CPU code (oracle/_ref/liblela_ref.so), or None."""
+    global _ref
+    if _ref is None and have_ref():
+        L = ctypes.CDLL(ref_path())
+        L.lela_ref_gemm_zp_u32.argtypes = [_I, _U, _S, _S, _S, _U, _P, _S, _P, _S, _U, _P, _S]
+        L.lela_ref_gemm_zp_u32_threads.argtypes = [_I, _U, _S, _S, _S, _U, _P, _S, _P, _S, _U, _P, _S]
+        L.lela_ref_trsm_zp_u32.argtypes = [_U, _I, _I, _S, _S, _U, _P, _S, _P, _S, ctypes.POINTER(_S)]
+        L.lela_ref_trsm_zp_u32_threads.argtypes = [_I, _U, _I, _I, _S, _S, _U, _P, _S, _P, _S]
+        L.lela_ref_echelon_zp_u32.argtypes = [_U, _S, _S, _P, _S, ctypes.POINTER(_S), ctypes.POINTER(_U)]
+        L.lela_ref_elim_echelon_zp_u32.argtypes = [_U, _S, _S, _P, _S, ctypes.POINTER(_S), ctypes.POINTER(_U)]
+        L.lela_ref_fl_echelonize_zp_u32.argtypes = [_U, _S, _S, _P, _P, _P, _I, _I, _P, _S,
+                                                    ctypes.POINTER(_S), ctypes.POINTER(_U), ctypes.POINTER(_S)]
+        L.lela_ref_gemm_gf2.argtypes = [_S, _S, _S, _I, _P, _S, _P, _S, _I, _P, _S]
+        L.lela_ref_echelon_gf2.argtypes = [_S, _S, _P, _S, ctypes.POINTER(_S)]
+        _ref = L
+    return _ref
+
+
+def _c(a, dt):
+    return np.ascontiguousarray(a, dtype=dt)
+
+
+# ------------------------------------------------------------- restatement --
+
+def gemm_zp(p, A, B, C, a=1, b=1, threads=1):
+    A = _c(A, np.uint32); B = _c(B, np.uint32); C = _c(C, np.uint32).copy()
+    m, k = A.shape; n = B.shape[1]
+    if threads > 1:
+        lib().oracle_gemm_zp_u32_threads(threads, p, m, n, k, a, _ptr(A), k, _ptr(B), n, b, _ptr(C), n)
+    else:
+        lib().oracle_gemm_zp_u32(p, m, n, k, a, _ptr(A), k, _ptr(B), n, b, _ptr(C), n)
+    return C
+
+
+def trsm_zp(p, A, B, upper, diag_is_one, a=1):
+    """Returns (B', bad_idx or None)."""
+    A = _c(A, np.uint32); B = _c(B, np.uint32).copy()
+    m = A.shape[0]; n = B.shape[1]
+    bad = _S(0)
+    rc = lib().oracle_trsm_zp_u32(p, int(upper), int(diag_is_one), m, n, a, _ptr(A), m, _ptr(B), n, ctypes.byref(bad))
+    return B, (bad.value if rc else None)
+
+
+def echelon_zp(p, A):
+    A = _c(A, np.uint32).copy()
+    m, n = A.shape
+    r = _S(0); d = _U(0)
+    rc = lib().oracle_echelon_zp_u32(p, m, n, _ptr(A), n, ctypes.byref(r), ctypes.byref(d))
+    if rc:
+        raise ArithmeticError("pivot not invertible")
+    return A, r.value, d.value
+
+
+def fl_echelonize_zp(p, m, n, rowptr, colidx, vals, reduced=True, only_D=False):
+    """Returns dict(status, R (rows x n), rank, det, bad_row)."""
+    rowptr = _c(rowptr, np.uint64); colidx = _c(colidx, np.uint32); vals = _c(vals, np.uint32)
+    R = np.zeros((max(m, 1), n), dtype=np.uint32)
+    rk = _S(0); det = _U(0); rows = _S(0); bad = _S(0)
+    st = lib().oracle_fl_echelonize_zp_u32(p, m, n, _ptr(rowptr), _ptr(colidx), _ptr(vals),
+                                           int(reduced), int(only_D), _ptr(R), n,
+                                           ctypes.byref(rk), ctypes.byref(det), ctypes.byref(rows),
+                                           ctypes.byref(bad))
+    return dict(status=st, R=R[:rows.value] if st == 0 else None, rank=rk.value, det=det.value,
+                bad_row=bad.value)
+
+
+def gemm_gf2(A, B, C, k, n, a=1, b=1):
+    A = _c(A, np.uint64); B = _c(B, np.uint64); C = _c(C, np.uint64).copy()
+    m = A.shape[0]
+    lib().oracle_gemm_gf2(m, n, k, a, _ptr(A), A.shape[1], _ptr(B), B.shape[1], b, _ptr(C), C.shape[1])
+    return C
+
+
+def echelon_gf2(A, n):
+    A = _c(A, np.uint64).copy()
+    r = _S(0)
+    lib().oracle_echelon_gf2(A.shape[0], n, _ptr(A), A.shape[1], ctypes.byref(r))
+    return A, r.value
+
+
+def inv_zp(p, x):
+    return lib().oracle_inv_zp(p, x)
+
+
+# ------------------------------------------------------- LELA's own code --
+
+def ref_gemm_zp(p, A, B, C, a=1, b=1, module=0, threads=1):
+    A = _c(A, np.uint32); B = _c(B, np.uint32); C = _c(C, np.uint32).copy()
+    m, k = A.shape; n = B.shape[1]
+    if threads > 1:
+        ref().lela_ref_gemm_zp_u32_threads(threads, p, m, n, k, a, _ptr(A), k, _ptr(B), n, b, _ptr(C), n)
+    else:
+        ref().lela_ref_gemm_zp_u32(module, p, m, n, k, a, _ptr(A), k, _ptr(B), n, b, _ptr(C), n)
+    return C
+
+
+def ref_trsm_zp(p, A, B, upper, diag_is_one, a=1, threads=1):
+    A = _c(A, np.uint32); B = _c(B, np.uint32).copy()
+    m = A.shape[0]; n = B.shape[1]
+    if threads > 1:
+        ref().lela_ref_trsm_zp_u32_threads(threads, p, int(upper), int(diag_is_one), m, n, a,
+                                           _ptr(A), m, _ptr(B), n)
+        return B, None
+    bad = _S(0)
+    rc = ref().lela_ref_trsm_zp_u32(p, int(upper), int(diag_is_one), m, n, a, _ptr(A), m, _ptr(B), n, ctypes.byref(bad))
+    return B, (bad.value if rc else None)
+
+
+def ref_echelon_zp(p, A, classical=False):
+    A = _c(A, np.uint32).copy()
+    m, n = A.shape
+    r = _S(0); d = _U(0)
+    fn = ref().lela_ref_elim_echelon_zp_u32 if classical else ref().lela_ref_echelon_zp_u32
+    fn(p, m, n, _ptr(A), n, ctypes.byref(r), ctypes.byref(d))
+    return A, r.value, d.value
+
+
+def ref_fl_echelonize_zp(p, m, n, rowptr, colidx, vals, reduced=True, only_D=False):
+    rowptr = _c(rowptr, np.uint64); colidx = _c(colidx, np.uint32); vals = _c(vals, np.uint32)
+    R = np.zeros((max(m, 1), n), dtype=np.uint32)
+    rk = _S(0); det = _U(0); rows = _S(0)
+    st = ref().lela_ref_fl_echelonize_zp_u32(p, m, n, _ptr(rowptr), _ptr(colidx), _ptr(vals),
+                                             int(reduced), int(only_D), _ptr(R), n,
+                                             ctypes.byref(rk), ctypes.byref(det), ctypes.byref(rows))
+    return dict(status=st, R=R[:rows.value] if st == 0 else None, rank=rk.value, det=det.value)
+
+
+def ref_gemm_gf2(A, B, C, k, n, a=1, b=1):
+    A = _c(A, np.uint64); B = _c(B, np.uint64); C = _c(C, np.uint64).copy()
+    m = A.shape[0]
+    ref().lela_ref_gemm_gf2(m, n, k, a, _ptr(A), A.shape[1], _ptr(B), B.shape[1], b, _ptr(C), C.shape[1])
+    return C
+
+
+def ref_echelon_gf2(A, n):
+    A = _c(A, np.uint64).copy()
+    r = _S(0)
+    ref().lela_ref_echelon_gf2(A.shape[0], n, _ptr(A), A.shape[1], ctypes.byref(r))
+    return A, r.value

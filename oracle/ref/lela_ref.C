@@ -1,0 +1,353 @@
+/* oracle/ref/lela_ref.C -- C entry points onto LELA's own CPU implementation.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is compiled (by oracle/Makefile)
+ * together with the unmodified LELA headers and sources of the reference
+ * tree into oracle/_ref/liblela_ref.so.  The library is the checker for the
+ * CUDA path and the "reference" CPU baseline of bench.py; nothing in the
+ * product (lela_b200/, include/) links or loads it.
+ *
+ * Every entry point copies plain row-major arrays into LELA's own matrix
+ * types, runs the reference routine named in its comment through LELA's
+ * public BLAS3 / algorithm interfaces, and copies the result back.
+ */
+
+#include <cstring>
+#include <vector>
+#include <pthread.h>
+#include <algorithm>
+#include <stdint.h>
+
+#include "lela/ring/modular.h"
+#include "lela/ring/gf2.h"
+#include "lela/blas/context.h"
+#include "lela/blas/level3.h"
+#include "lela/matrix/dense.h"
+#include "lela/matrix/sparse.h"
+#include "lela/algorithms/faugere-lachartre.h"
+#include "lela/algorithms/gauss-jordan.h"
+#include "lela/algorithms/elimination.h"
+#include "lela/util/error.h"
+
+using namespace LELA;
+
+typedef Modular<uint32> Zp;
+
+namespace {
+
+void load_dense (DenseMatrix<uint32> &M, const uint32_t *src, size_t ld)
+{
+	for (size_t i = 0; i < M.rowdim (); ++i)
+		std::memcpy (&M[i][0], src + i * ld, M.coldim () * sizeof (uint32_t));
+}
+
+void store_dense (const DenseMatrix<uint32> &M, uint32_t *dst, size_t ld)
+{
+	for (size_t i = 0; i < M.rowdim (); ++i)
+		std::memcpy (dst + i * ld, &M[i][0], M.coldim () * sizeof (uint32_t));
+}
+
+template <class Modules>
+void gemm_with (uint32_t p, size_t m, size_t n, size_t k, uint32_t a,
+		const uint32_t *A, size_t lda, const uint32_t *B, size_t ldb,
+		uint32_t b, uint32_t *C, size_t ldc)
+{
+	Zp F (p);
+	Context<Zp, Modules> ctx (F);
+	DenseMatrix<uint32> MA (m, k), MB (k, n), MC (m, n);
+	if (m && k) load_dense (MA, A, lda);
+	if (k && n) load_dense (MB, B, ldb);
+	if (m && n) load_dense (MC, C, ldc);
+	BLAS3::gemm (ctx, a, MA, MB, b, MC);
+	if (m && n) store_dense (MC, C, ldc);
+}
+
+// GF(2) dense matrices: LELA's DenseMatrix<bool> rows are BitVector words,
+// LittleEndian bit order (bit j of word w is column 64w+j).
+void load_gf2 (DenseMatrix<bool> &M, const uint64_t *src, size_t ldw)
+{
+	size_t words = (M.coldim () + 63) / 64;
+	size_t i = 0;
+	for (DenseMatrix<bool>::RowIterator r = M.rowBegin (); r != M.rowEnd (); ++r, ++i) {
+		DenseMatrix<bool>::Row::word_iterator w = r->word_begin ();
+		for (size_t j = 0; j < words; ++j, ++w) {
+			uint64_t v = src[i * ldw + j];
+			if (j == words - 1 && (M.coldim () & 63))
+				v &= (~0ULL) >> (64 - (M.coldim () & 63));
+			*w = v;
+		}
+	}
+}
+
+void store_gf2 (const DenseMatrix<bool> &M, uint64_t *dst, size_t ldw)
+{
+	size_t words = (M.coldim () + 63) / 64;
+	size_t i = 0;
+	for (DenseMatrix<bool>::ConstRowIterator r = M.rowBegin (); r != M.rowEnd (); ++r, ++i) {
+		DenseMatrix<bool>::ConstRow::const_word_iterator w = r->word_begin ();
+		for (size_t j = 0; j < words; ++j, ++w)
+			dst[i * ldw + j] = *w;
+	}
+}
+
+// One slice of a process-parallel CPU run: kind 0 = gemm on a block of rows
+// of A and C, kind 1 = trsm on a block of right-hand-side columns of B (C).
+struct SliceJob {
+	int kind; uint32_t p; size_t m, n, k; uint32_t a;
+	const uint32_t *A; size_t lda; const uint32_t *B; size_t ldb;
+	uint32_t b; uint32_t *C; size_t ldc; int upper, diag_is_one;
+};
+
+void *run_slice (void *arg)
+{
+	SliceJob *j = (SliceJob *) arg;
+	if (j->kind == 0) {
+		gemm_with<ZpModule<uint32> > (j->p, j->m, j->n, j->k, j->a, j->A, j->lda, j->B, j->ldb, j->b, j->C, j->ldc);
+	} else {
+		Zp F (j->p);
+		Context<Zp, ZpModule<uint32> > ctx (F);
+		DenseMatrix<uint32> MA (j->m, j->m), MB (j->m, j->n);
+		load_dense (MA, j->A, j->lda);
+		load_dense (MB, j->C, j->ldc);
+		BLAS3::trsm (ctx, j->a, MA, MB, j->upper ? UpperTriangular : LowerTriangular, j->diag_is_one != 0);
+		store_dense (MB, j->C, j->ldc);
+	}
+	return 0;
+}
+
+void run_jobs (std::vector<SliceJob> &jobs)
+{
+	std::vector<pthread_t> th (jobs.size ());
+	for (size_t t = 0; t < jobs.size (); ++t) pthread_create (&th[t], 0, run_slice, &jobs[t]);
+	for (size_t t = 0; t < jobs.size (); ++t) pthread_join (th[t], 0);
+}
+
+} // namespace
+
+extern "C" {
+
+/* BLAS3::gemm (lela/blas/level3.h:82) over Modular<uint32>.
+ * module: 0 = ZpModule<uint32>, 1 = GenericModule, 2 = AllModules (the
+ * default stack, Strassen-Winograd over ZpModule). */
+int lela_ref_gemm_zp_u32 (int module, uint32_t p, size_t m, size_t n, size_t k, uint32_t a,
+			  const uint32_t *A, size_t lda, const uint32_t *B, size_t ldb,
+			  uint32_t b, uint32_t *C, size_t ldc)
+{
+	try {
+		if (module == 0)
+			gemm_with<ZpModule<uint32> > (p, m, n, k, a, A, lda, B, ldb, b, C, ldc);
+		else if (module == 1)
+			gemm_with<GenericModule<Zp> > (p, m, n, k, a, A, lda, B, ldb, b, C, ldc);
+		else
+			gemm_with<AllModules<Zp> > (p, m, n, k, a, A, lda, B, ldb, b, C, ldc);
+	} catch (...) {
+		return -1;
+	}
+	return 0;
+}
+
+/* Row-sliced, multi-threaded use of the same LELA routine: each thread runs
+ * ZpModule gemm on its own block of rows of A and C with its own Context.
+ * Z/p arithmetic is exact, so the result equals the single call. */
+int lela_ref_gemm_zp_u32_threads (int nthreads, uint32_t p, size_t m, size_t n, size_t k, uint32_t a,
+				  const uint32_t *A, size_t lda, const uint32_t *B, size_t ldb,
+				  uint32_t b, uint32_t *C, size_t ldc)
+{
+	if (nthreads < 1) nthreads = 1;
+	std::vector<SliceJob> jobs;
+	size_t chunk = (m + nthreads - 1) / nthreads;
+	for (int t = 0; t < nthreads; ++t) {
+		size_t r0 = t * chunk, r1 = std::min (m, r0 + chunk);
+		if (r0 >= r1) break;
+		SliceJob j = { 0, p, r1 - r0, n, k, a, A + r0 * lda, lda, B, ldb, b, C + r0 * ldc, ldc, 0, 0 };
+		jobs.push_back (j);
+	}
+	run_jobs (jobs);
+	return 0;
+}
+
+/* BLAS3::trsm (lela/blas/level3.h:121) -> _trsm<.., GenericModule::Tag>
+ * (lela/blas/level3-generic.tcc:421-498).  B <- a A^-1 B.
+ * upper: 1 = UpperTriangular, 0 = LowerTriangular.
+ * Returns 0, or 1 with *bad_idx set when LELA throws
+ * DiagonalEntryNotInvertible(idx). */
+int lela_ref_trsm_zp_u32 (uint32_t p, int upper, int diag_is_one, size_t m, size_t n, uint32_t a,
+			  const uint32_t *A, size_t lda, uint32_t *B, size_t ldb, size_t *bad_idx)
+{
+	Zp F (p);
+	Context<Zp, ZpModule<uint32> > ctx (F);
+	DenseMatrix<uint32> MA (m, m), MB (m, n);
+	if (m) load_dense (MA, A, lda);
+	if (m && n) load_dense (MB, B, ldb);
+	try {
+		BLAS3::trsm (ctx, a, MA, MB, upper ? UpperTriangular : LowerTriangular, diag_is_one != 0);
+	} catch (DiagonalEntryNotInvertible &e) {
+		if (bad_idx) *bad_idx = e.idx ();
+		if (m && n) store_dense (MB, B, ldb);
+		return 1;
+	}
+	if (m && n) store_dense (MB, B, ldb);
+	return 0;
+}
+
+/* Column-sliced, multi-threaded trsm: each thread solves its own block of
+ * right-hand-side columns with the same LELA routine. */
+int lela_ref_trsm_zp_u32_threads (int nthreads, uint32_t p, int upper, int diag_is_one, size_t m, size_t n,
+				  uint32_t a, const uint32_t *A, size_t lda, uint32_t *B, size_t ldb)
+{
+	if (nthreads < 1) nthreads = 1;
+	std::vector<SliceJob> jobs;
+	size_t chunk = (n + nthreads - 1) / nthreads;
+	for (int t = 0; t < nthreads; ++t) {
+		size_t c0 = t * chunk, c1 = std::min (n, c0 + chunk);
+		if (c0 >= c1) break;
+		SliceJob j = { 1, p, m, c1 - c0, m, a, A, lda, 0, 0, 0, B + c0, ldb, upper, diag_is_one };
+		jobs.push_back (j);
+	}
+	run_jobs (jobs);
+	return 0;
+}
+
+/* Dense non-reduced row-echelon form as EchelonForm::echelonize does it for
+ * a DenseMatrix (lela/solutions/echelon-form.h:103-134): GaussJordan::
+ * echelonize (lela/algorithms/gauss-jordan.tcc:413-432) followed by
+ * Elimination::move_L (lela/algorithms/elimination.tcc:372-391).
+ * Also returns rank and det (product of the pivots). */
+int lela_ref_echelon_zp_u32 (uint32_t p, size_t m, size_t n, uint32_t *A, size_t lda, size_t *rank, uint32_t *det)
+{
+	Zp F (p);
+	Context<Zp> ctx (F);
+	DenseMatrix<uint32> MA (m, n);
+	if (m && n) load_dense (MA, A, lda);
+	GaussJordan<Zp> GJ (ctx);
+	Elimination<Zp> elim (ctx);
+	GaussJordan<Zp>::Permutation P;
+	size_t r = 0;
+	Zp::Element d;
+	try {
+		GJ.echelonize (MA, P, r, d);
+		elim.move_L (MA, MA);
+	} catch (...) {
+		return -1;
+	}
+	if (m && n) store_dense (MA, A, lda);
+	*rank = r;
+	/* GaussJordan's own det output is not the product of the pivots when
+	 * the recursion meets zero column blocks; FaugereLachartre instead takes
+	 * det from the leading entries of the echelon form (setup_splicer,
+	 * lela/algorithms/faugere-lachartre.tcc:119), which is what is returned
+	 * here. */
+	Zp::Element pd = 1;
+	for (size_t i = 0; i < r; ++i) {
+		size_t c = 0;
+		while (c < n && MA[i][c] == 0) ++c;
+		if (c < n) F.mulin (pd, MA[i][c]);
+	}
+	*det = pd;
+	(void) d;
+	return 0;
+}
+
+/* Classical elimination Elimination::echelonize (lela/algorithms/
+ * elimination.tcc:47-139), the reference's own cross-check for the
+ * recursive GaussJordan result. */
+int lela_ref_elim_echelon_zp_u32 (uint32_t p, size_t m, size_t n, uint32_t *A, size_t lda, size_t *rank, uint32_t *det)
+{
+	Zp F (p);
+	Context<Zp> ctx (F);
+	DenseMatrix<uint32> MA (m, n);
+	if (m && n) load_dense (MA, A, lda);
+	Elimination<Zp> elim (ctx);
+	Elimination<Zp>::Permutation P;
+	size_t r = 0;
+	Zp::Element d;
+	elim.echelonize (MA, P, r, d, DensePivotStrategy<Zp, AllModules<Zp> > (ctx), false);
+	if (m && n) store_dense (MA, A, lda);
+	*rank = r;
+	*det = d;
+	return 0;
+}
+
+/* FaugereLachartre::echelonize (lela/algorithms/faugere-lachartre.tcc:
+ * 735-917) on a SparseMatrix<uint32> given in CSR form (rows sorted by
+ * column).  R is returned dense row-major m x n (ldr), so callers can
+ * compare it entry by entry.
+ * Returns 0 = ok, 1 = WrongMatrixForm (the reference throws it from
+ * setup_splicer, lela/algorithms/faugere-lachartre.tcc:80-81). */
+int lela_ref_fl_echelonize_zp_u32 (uint32_t p, size_t m, size_t n,
+				   const uint64_t *rowptr, const uint32_t *colidx, const uint32_t *vals,
+				   int reduced, int only_D,
+				   uint32_t *R, size_t ldr, size_t *rank, uint32_t *det, size_t *out_rows)
+{
+	Zp F (p);
+	Context<Zp> ctx (F);
+	typedef SparseMatrix<uint32> SM;
+	SM X (m, n), Rm (m, n);
+	size_t i = 0;
+	for (SM::RowIterator r = X.rowBegin (); r != X.rowEnd (); ++r, ++i) {
+		for (uint64_t e = rowptr[i]; e < rowptr[i + 1]; ++e)
+			r->push_back (SM::Row::value_type (colidx[e], vals[e]));
+	}
+	FaugereLachartre<Zp> FL (ctx);
+	size_t rk = 0;
+	Zp::Element d;
+	try {
+		FL.echelonize (Rm, X, rk, d, reduced != 0, only_D != 0);
+	} catch (WrongMatrixForm &e) {
+		return 1;
+	}
+	size_t rows = Rm.rowdim ();
+	for (size_t a = 0; a < rows; ++a)
+		std::memset (R + a * ldr, 0, n * sizeof (uint32_t));
+	i = 0;
+	for (SM::ConstRowIterator r = Rm.rowBegin (); r != Rm.rowEnd (); ++r, ++i)
+		for (SM::ConstRow::const_iterator e = r->begin (); e != r->end (); ++e)
+			R[i * ldr + (size_t) (uint32_t) e->first] = (uint32_t) e->second;
+	*rank = rk;
+	*det = d;
+	*out_rows = rows;
+	return 0;
+}
+
+/* BLAS3::gemm over GF2 with DenseMatrix<bool> operands: AllModules<GF2>
+ * without M4RI = StrassenModule over GenericModule (lela/ring/gf2.h:337-345),
+ * i.e. the generic Row*Row*Row gemm (lela/blas/level3-generic.tcc:243-263). */
+int lela_ref_gemm_gf2 (size_t m, size_t n, size_t k, int a,
+		       const uint64_t *A, size_t lda, const uint64_t *B, size_t ldb,
+		       int b, uint64_t *C, size_t ldc)
+{
+	GF2 F;
+	Context<GF2> ctx (F);
+	DenseMatrix<bool> MA (m, k), MB (k, n), MC (m, n);
+	load_gf2 (MA, A, lda);
+	load_gf2 (MB, B, ldb);
+	load_gf2 (MC, C, ldc);
+	BLAS3::gemm (ctx, a != 0, MA, MB, b != 0, MC);
+	store_gf2 (MC, C, ldc);
+	return 0;
+}
+
+/* GF(2) dense non-reduced echelon form: the EchelonForm dense path without
+ * M4RI (GaussJordan + move_L), as for Modular<uint32>. */
+int lela_ref_echelon_gf2 (size_t m, size_t n, uint64_t *A, size_t lda, size_t *rank)
+{
+	GF2 F;
+	Context<GF2> ctx (F);
+	DenseMatrix<bool> MA (m, n);
+	load_gf2 (MA, A, lda);
+	GaussJordan<GF2> GJ (ctx);
+	Elimination<GF2> elim (ctx);
+	GaussJordan<GF2>::Permutation P;
+	size_t r = 0;
+	bool d;
+	try {
+		GJ.echelonize (MA, P, r, d);
+		elim.move_L (MA, MA);
+	} catch (...) {
+		return -1;
+	}
+	store_gf2 (MA, A, lda);
+	*rank = r;
+	return 0;
+}
+
+} // extern "C"
