@@ -1,0 +1,350 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 exact linear-algebra path (one JSON line on stdout).
+
+Workload (one "step"): dense gemm over Z/65521 (Modular<uint32>) at
+8192 x 8192 x 8192, C <- A*B + C, entries uniform in [0, p), seeded
+synthetic inputs already resident in HBM (3 x 256 MiB, larger than L2, so no
+flush is needed between steps).  Metric: Z/p operations per second
+(2*M*N*K per step), reported in Gop/s; results are bit-exact (the GPU tests
+check them against the CPU oracle).
+
+Also reported on the same line:
+  e2e           the same metric through the host-pointer C ABI
+                (lela_cuda_gemm_zp_u32) with pinned host buffers: every step
+                copies A, B, C to the device and C back;
+  plain_gpu     the CUDA-core delayed-reduction gemm on the same GPU;
+  roofline      the tensor-core kernel's int8 tensor throughput against the
+                int8 peak measured in this run (cuBLASLt int8 gemm);
+  cpu_baseline  LELA's own CPU gemm (oracle/_ref) on a bounded row slice,
+                all host threads.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With N > 1 (torchrun, one process per GPU) every rank runs an independent
+replica of the workload ("replicas only": a single gemm is not sharded) and
+value = total operations of all ranks / the slowest rank's time.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Z/p gemm Gop/s at 8192^3 (Modular<uint32>, p=65521), bit-exact"
+P = 65521
+N = 8192
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=N)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
+            int(os.environ.get("LOCAL_RANK", 0)))
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "--query-gpu=" + self.FIELDS,
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is not None:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        rows = []
+        for line in self.f.read().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9 or parts[0] != str(self.device):
+                continue
+            try:
+                rows.append(dict(sm=float(parts[1]), smax=float(parts[2]), power=float(parts[3]),
+                                 hw=parts[5], hwt=parts[6], swt=parts[7], pcap=parts[8]))
+            except ValueError:
+                continue
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        reasons = set()
+        for r in rows:
+            for key, name in (("hw", "hw_slowdown"), ("hwt", "hw_thermal_slowdown"),
+                              ("swt", "sw_thermal_slowdown"), ("pcap", "sw_power_cap")):
+                if r[key].lower() == "active":
+                    reasons.add(name)
+        load = [r for r in rows if r["power"] > 300] or rows
+        return {"sm_mhz": statistics.median(r["sm"] for r in load),
+                "sm_max_mhz": max(r["smax"] for r in rows), "reasons": sorted(reasons),
+                "samples": len(rows), "samples_under_load": len(load)}
+
+
+# --------------------------------------------------------------- helpers
+def int8_peak_tops(torch, dev):
+    """Dense int8 tensor-core peak measured here: cuBLASLt int8 gemm
+    (torch._int_mm) at 8192^3, best of 5, CUDA events."""
+    try:
+        a = torch.randint(-128, 127, (8192, 8192), dtype=torch.int8, device=dev)
+        b = torch.randint(-128, 127, (8192, 8192), dtype=torch.int8, device=dev).t()
+        for _ in range(3):
+            torch._int_mm(a, b)
+        best = None
+        for _ in range(5):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            torch._int_mm(a, b)
+            e1.record()
+            torch.cuda.synchronize()
+            t = e0.elapsed_time(e1) / 1e3
+            best = t if best is None else min(best, t)
+        del a, b
+        return 2 * 8192 ** 3 / best / 1e12, "cuBLASLt int8 gemm 8192^3 (torch._int_mm), best of 5"
+    except Exception as ex:  # fall back to twice the measured dense bf16 peak
+        try:
+            peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+            return 2 * peaks["bf16_tflops"], "2 x measured bf16 dense (int8 gemm unavailable: %s)" % ex
+        except Exception:
+            return 2 * 1590.0, "2 x fallback bf16 1.59 PFLOP/s"
+
+
+def cpu_baseline(n, threads):
+    """LELA's own CPU gemm on a bounded sample: rows 0..r-1 of the n^3
+    workload, ZpModule gemm row-sliced over all host threads."""
+    import oracle
+    from lela_b200 import gen
+    rows = max(threads, 16)
+    A = gen.dense_zp(101, rows, n, P)
+    B = gen.dense_zp(102, n, n, P)
+    C = gen.dense_zp(103, rows, n, P)
+    if oracle.have_ref():
+        fn, kind = (lambda: oracle.ref_gemm_zp(P, A, B, C, 1, 1, threads=threads)), "reference"
+    else:
+        fn, kind = (lambda: oracle.gemm_zp(P, A, B, C, 1, 1, threads=threads)), "port"
+    t0 = time.perf_counter()
+    fn()
+    t = time.perf_counter() - t0
+    return {"value": round(2 * rows * n * n / t / 1e9, 4), "unit": "Gop/s", "cores": threads,
+            "kind": kind,
+            "sample": "rows 0-%d of the %d^3 gemm (%dx%dx%d), LELA ZpModule gemm row-sliced over %d threads, %.1f s"
+                      % (rows - 1, n, rows, n, n, threads, t)}
+
+
+# ------------------------------------------------------------ reference
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    import oracle
+    from lela_b200 import gen
+    threads = os.cpu_count() or 1
+    n = args.n
+    rows = max(threads, 16)
+    A = gen.dense_zp(101, rows, n, P)
+    B = gen.dense_zp(102, n, n, P)
+    C = gen.dense_zp(103, rows, n, P)
+    if oracle.have_ref():
+        fn, kind = (lambda: oracle.ref_gemm_zp(P, A, B, C, 1, 1, threads=threads)), "reference"
+    else:
+        fn, kind = (lambda: oracle.gemm_zp(P, A, B, C, 1, 1, threads=threads)), "port"
+    for _ in range(args.warmup):
+        fn()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        fn()
+    t = (time.perf_counter() - t0) / args.steps
+    v = 2 * rows * n * n / t / 1e9
+    line = {"metric": METRIC, "value": round(v, 4), "unit": "Gop/s", "impl": "reference",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(t * 1e3, 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32 (u64 accumulate)", "data": "synthetic",
+            "config": {"workload": "gemm Z/65521 %d^3 (sample: %d rows per step)" % (n, rows),
+                       "p": P, "m": n, "n": n, "k": n, "parallelism": "host threads"},
+            "cpu_baseline": {"value": round(v, 4), "unit": "Gop/s", "cores": threads, "kind": kind,
+                             "sample": "rows 0-%d of the %d^3 gemm per step" % (rows - 1, n)},
+            "e2e": {"value": round(v, 4), "unit": "Gop/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ ours
+def run_ours(args):
+    import torch
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=dev)
+    from lela_b200 import gen, CudaModule
+
+    n = args.n
+    cm = CudaModule(local)
+    stream = torch.cuda.Stream(device=dev)
+    cm.set_stream(stream)
+
+    A = gen.dense_zp(11 + rank, n, n, P)
+    B = gen.dense_zp(12 + rank, n, n, P)
+    C = gen.dense_zp(13 + rank, n, n, P)
+    dA = torch.from_numpy(A.view(np.int32)).to(dev)
+    dB = torch.from_numpy(B.view(np.int32)).to(dev)
+    dC = torch.from_numpy(C.view(np.int32)).to(dev)
+    torch.cuda.synchronize()
+
+    peak, peak_src = int8_peak_tops(torch, dev)
+
+    def step():
+        cm.gemm(P, 1, dA, dB, 1, dC)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    cm.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+
+    clocks = ClockSampler(local)
+    cm.profile_reset()
+    cm.profile(True)
+    launches0 = cm.launch_count
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    cm.synchronize()
+    torch.cuda.synchronize()
+    launches = cm.launch_count - launches0
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    tc_ms, tc_n = cm.profile_read("zp_gemm_tc")
+    sp_ms, sp_n = cm.profile_read("zp_split")
+    cm.profile(False)
+
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    ms_max = float(t.item())
+    ops_step = 2.0 * n ** 3
+    value = world * ops_step * args.steps / (ms_max / 1e3) / 1e9
+
+    # dominant kernel roofline: int8 tensor ops actually required
+    L = 2
+    tc_avg = tc_ms / max(tc_n, 1)
+    achieved = L * L * 2.0 * n ** 3 / (tc_avg / 1e3) / 1e12
+    roofline = {"bound": "tensor", "kernel": "zp_gemm_tc_kernel<2>", "achieved": round(achieved, 1),
+                "peak": round(peak, 1), "unit": "TFLOP/s", "frac": round(achieved / peak, 4),
+                "traffic": None,
+                "ops_per_launch": "4 limb products x 2*8192^3 int8 multiply-adds = %.3e" % (L * L * 2.0 * n ** 3),
+                "kernel_ms_avg": round(tc_avg, 4), "split_ms_avg": round(sp_ms / max(sp_n, 1), 4),
+                "peak_source": peak_src + " (measured in this run)"}
+
+    out = {"metric": METRIC, "value": round(value, 2), "unit": "Gop/s", "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4),
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "u32 (u8 limbs, s32 tensor accumulate)", "data": "synthetic",
+           "config": {"workload": "gemm Z/65521 %d^3 C<-A*B+C" % n, "p": P, "m": n, "n": n, "k": n,
+                      "limbs": L, "parallelism": "replicas" if world > 1 else "single GPU",
+                      "l2": "inputs 3 x %d MiB > L2 (no flush)" % (n * n * 4 >> 20)},
+           "roofline": roofline, "clocks": clk, "gpu_launches": int(launches)}
+
+    # plain CUDA-core gemm on the same GPU (the "plain GPU form")
+    if not args.no_plain:
+        cm.set_gemm_kernel(1)
+        cm.gemm(P, 1, dA, dB, 1, dC)
+        cm.synchronize()
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        reps = 2
+        for _ in range(reps):
+            cm.gemm(P, 1, dA, dB, 1, dC)
+        f1.record(stream)
+        cm.synchronize()
+        pms = f0.elapsed_time(f1) / reps
+        cm.set_gemm_kernel(0)
+        out["plain_gpu"] = {"value": round(ops_step / (pms / 1e3) / 1e9, 2), "unit": "Gop/s",
+                            "ms_per_step": round(pms, 3), "kernel": "zp_gemm_plain_kernel"}
+        out["speedup_vs_plain"] = round(out["value"] / world / out["plain_gpu"]["value"], 2)
+
+    del dA, dB, dC
+    torch.cuda.empty_cache()
+
+    # end to end through the host-pointer C ABI, pinned host buffers
+    if not args.no_e2e:
+        pin = lambda x: torch.from_numpy(x.view(np.int32)).pin_memory().numpy().view(np.uint32)
+        hA, hB, hC = pin(A), pin(B), pin(C)
+        cm.gemm(P, 1, hA, hB, 1, hC)
+        steps = max(1, min(args.steps, 5))
+        if world > 1:
+            torch.distributed.barrier()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            cm.gemm(P, 1, hA, hB, 1, hC)
+        te = (time.perf_counter() - t0) / steps
+        tt = torch.tensor([te], dtype=torch.float64, device=dev)
+        if world > 1:
+            torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        te = float(tt.item())
+        out["e2e"] = {"value": round(world * ops_step / te / 1e9, 2), "unit": "Gop/s",
+                      "h2d_bytes_per_step": 3 * n * n * 4, "d2h_bytes_per_step": n * n * 4,
+                      "ms_per_step": round(te * 1e3, 3),
+                      "api": "lela_cuda_gemm_zp_u32 (host pointers, pinned)"}
+
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(n, os.cpu_count() or 1)
+
+    cm.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

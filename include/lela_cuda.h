@@ -1,0 +1,114 @@
+/* include/lela_cuda.h -- C ABI of the B200 (sm_100a) implementation of
+ * LELA's exact linear-algebra hot path.
+ *
+ * Plain C: pointers, sizes and an int status.  No CUDA or C++ types appear
+ * in the signatures, so the functions can be bound from C, C++ (the
+ * CUDAModule in include/lela_cuda/cuda-module.h), ctypes or any FFI.
+ *
+ * Conventions
+ *  - Matrices are row-major with an explicit leading dimension (row stride)
+ *    counted in elements (uint32 for Z/p, 64-bit words for GF(2)); this is
+ *    the `&A[0][0]` + `A.disp ()` view of a LELA DenseMatrix
+ *    (lela/matrix/dense.h:319, 434) and of its submatrices (:425-429).
+ *  - Z/p entries are canonical representatives in [0, p), p in [2, 2^32):
+ *    the element convention of Modular<uint32> (lela/ring/modular.h:203-245).
+ *  - GF(2) rows are packed LittleEndian: bit j of word w is column 64w + j,
+ *    as LELA's BitVector<LittleEndian<uint64>> stores a DenseMatrix<bool>
+ *    row (lela/vector/bit-iterator.h:249-296).
+ *  - Functions without the _dev suffix take HOST pointers: the library
+ *    copies inputs to the device, computes, copies results back and
+ *    synchronises before returning.  The caller keeps ownership.
+ *  - _dev functions take DEVICE pointers (on the handle's device) and are
+ *    asynchronous on the handle's stream; device-side errors of an _dev call
+ *    are reported by the next lela_cuda_synchronize().
+ *  - A handle is not re-entrant (like a LELA Context, lela/blas/context.h:
+ *    61-63): use one handle per host thread.
+ *
+ * Status codes map onto LELA's exceptions in the C++ layer:
+ *  LELA_CUDA_DIAG_NOT_INVERTIBLE  -> DiagonalEntryNotInvertible(idx)
+ *                                    (lela/util/error.h; thrown at
+ *                                    lela/blas/level3-generic.tcc:441-442)
+ *  LELA_CUDA_WRONG_MATRIX_FORM    -> WrongMatrixForm(row)
+ *                                    (lela/algorithms/faugere-lachartre.tcc:32-41)
+ *  LELA_CUDA_PIVOT_NOT_INVERTIBLE -> LELAError("Could not invert pivot-element
+ *                                    in the ring") (lela/algorithms/elimination.tcc:102)
+ *  LELA_CUDA_ERR_ARG              -> PreconditionFailed (lela_check, lela/util/debug.h)
+ */
+#ifndef LELA_CUDA_H
+#define LELA_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct lela_cuda_ctx lela_cuda_ctx;
+
+enum {
+	LELA_CUDA_OK = 0,
+	LELA_CUDA_ERR_ARG = 1,
+	LELA_CUDA_ERR_CUDA = 2,
+	LELA_CUDA_ERR_NOMEM = 3,
+	LELA_CUDA_DIAG_NOT_INVERTIBLE = 4,
+	LELA_CUDA_WRONG_MATRIX_FORM = 5,
+	LELA_CUDA_PIVOT_NOT_INVERTIBLE = 6,
+	LELA_CUDA_ERR_TIMEOUT = 7,
+	LELA_CUDA_ERR_UNSUPPORTED = 8
+};
+
+/* Kernel choice for the Z/p gemm (lela_cuda_set_gemm_kernel). */
+enum {
+	LELA_CUDA_GEMM_AUTO = 0,   /* tensor-core kernel */
+	LELA_CUDA_GEMM_PLAIN = 1,  /* CUDA-core delayed-reduction kernel */
+	LELA_CUDA_GEMM_TC = 2      /* limb-split INT8 tcgen05 kernel */
+};
+
+/* ---------------------------------------------------------------- handle
+ * Replaces the state a LELA Modules object owns (ZpModule's _tmp scratch,
+ * lela/ring/modular.h:576; StrassenModule's sw, lela/algorithms/
+ * strassen-winograd.h:148): stream, device workspace, kernel choice. */
+int lela_cuda_create (lela_cuda_ctx **ctx, int device);
+int lela_cuda_destroy (lela_cuda_ctx *ctx);
+/* Use the caller's cudaStream_t (passed as void*); NULL restores the
+ * handle's own stream. */
+int lela_cuda_set_stream (lela_cuda_ctx *ctx, void *stream);
+void *lela_cuda_get_stream (lela_cuda_ctx *ctx);
+/* Wait for all work queued on the handle's stream and report any error a
+ * kernel recorded (e.g. LELA_CUDA_ERR_TIMEOUT). */
+int lela_cuda_synchronize (lela_cuda_ctx *ctx);
+int lela_cuda_set_gemm_kernel (lela_cuda_ctx *ctx, int kernel);
+const char *lela_cuda_status_string (int status);
+const char *lela_cuda_last_error (lela_cuda_ctx *ctx);
+/* Number of SMs of the handle's device. */
+int lela_cuda_num_sms (lela_cuda_ctx *ctx);
+/* Kernel launches issued through the handle so far (all kernels). */
+uint64_t lela_cuda_launch_count (lela_cuda_ctx *ctx);
+/* Per-kernel device timing: when enabled, each launch of a main kernel
+ * ("zp_gemm_tc", "zp_gemm_plain", ...) is bracketed by CUDA events on the
+ * handle's stream; profile_read synchronises, returns the summed
+ * milliseconds and launch count of one kernel name and forgets them. */
+int lela_cuda_profile_enable (lela_cuda_ctx *ctx, int on);
+int lela_cuda_profile_read (lela_cuda_ctx *ctx, const char *kernel, double *total_ms,
+			    uint64_t *launches);
+int lela_cuda_profile_reset (lela_cuda_ctx *ctx);
+
+/* ------------------------------------------------------------- Z/p gemm
+ * C <- a*A*B + b*C mod p, A m x k, B k x n, C m x n.
+ * Replaces BLAS3::gemm (lela/blas/level3.h:82) for Modular<uint32> and dense
+ * operands: _gemm<Modular<uint32>, Tag> reached through StrassenModule ->
+ * ZpModule -> GenericModule (lela/blas/level3-sw.h:25-62,
+ * lela/blas/level3-generic.tcc:285-322). */
+int lela_cuda_gemm_zp_u32 (lela_cuda_ctx *ctx, size_t m, size_t n, size_t k, uint32_t p,
+			   uint32_t a, const uint32_t *A, size_t lda, const uint32_t *B, size_t ldb,
+			   uint32_t b, uint32_t *C, size_t ldc);
+int lela_cuda_gemm_zp_u32_dev (lela_cuda_ctx *ctx, size_t m, size_t n, size_t k, uint32_t p,
+			       uint32_t a, const uint32_t *A, size_t lda, const uint32_t *B,
+			       size_t ldb, uint32_t b, uint32_t *C, size_t ldc);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LELA_CUDA_H */

@@ -1,0 +1,244 @@
+"""Host-side mirror of LELA's BLAS3 / algorithm interface for the CUDA module.
+
+``CudaModule`` plays the role of a LELA ``Context<Ring, CUDAModule>``
+(lela/blas/context.h:72-84): it owns one handle of the C ABI
+(include/lela_cuda.h) -- a CUDA stream, device workspace and kernel choice.
+Operation names and argument order follow LELA:
+
+    gemm(p, a, A, B, b, C)          BLAS3::gemm     (lela/blas/level3.h:82)
+    trsm(p, a, A, B, upper, unit)   BLAS3::trsm     (lela/blas/level3.h:121)
+
+NumPy arrays are host matrices (uint32 for Z/p, uint64 words for GF(2));
+torch CUDA tensors are device matrices and take the ``*_dev`` entry points.
+Status codes become LELA's exceptions.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+
+_P = ctypes.c_void_p
+_S = ctypes.c_size_t
+_U = ctypes.c_uint32
+_I = ctypes.c_int
+
+OK, ERR_ARG, ERR_CUDA, ERR_NOMEM, DIAG, WRONG_FORM, PIVOT, TIMEOUT, UNSUPPORTED = range(9)
+GEMM_AUTO, GEMM_PLAIN, GEMM_TC = 0, 1, 2
+
+
+class LELAError(Exception):
+    """LELAError (lela/util/error.h)."""
+
+
+class PreconditionFailed(LELAError):
+    """lela_check failure (lela/util/debug.h): bad dimensions or arguments."""
+
+
+class DiagonalEntryNotInvertible(LELAError):
+    """Thrown by trsm for a singular diagonal entry
+    (lela/blas/level3-generic.tcc:441-442); ``idx`` is its row index."""
+
+    def __init__(self, idx):
+        super().__init__("Diagonal entry %d not invertible" % idx)
+        self.idx = idx
+
+
+class WrongMatrixForm(LELAError):
+    """Bad Faugere-Lachartre input at ``row``
+    (lela/algorithms/faugere-lachartre.tcc:32-41)."""
+
+    def __init__(self, row):
+        super().__init__("Bad input-matrix for Faugere-Lachartre at row-index %d" % row)
+        self.row = row
+
+
+class CudaError(LELAError):
+    """CUDA runtime failure, device-side timeout or missing device."""
+
+
+def library_path():
+    return os.path.join(_HERE, "liblela_cuda.so")
+
+
+_lib = None
+
+
+def load_library():
+    """Load liblela_cuda.so; raises (no fallback) when it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = library_path()
+    if not os.path.exists(path):
+        raise CudaError("CUDA library %s is not built (run python -m lela_b200.build)" % path)
+    L = ctypes.CDLL(path)
+    L.lela_cuda_create.argtypes = [ctypes.POINTER(_P), _I]
+    L.lela_cuda_destroy.argtypes = [_P]
+    L.lela_cuda_set_stream.argtypes = [_P, _P]
+    L.lela_cuda_get_stream.argtypes = [_P]
+    L.lela_cuda_get_stream.restype = _P
+    L.lela_cuda_synchronize.argtypes = [_P]
+    L.lela_cuda_set_gemm_kernel.argtypes = [_P, _I]
+    L.lela_cuda_status_string.argtypes = [_I]
+    L.lela_cuda_status_string.restype = ctypes.c_char_p
+    L.lela_cuda_last_error.argtypes = [_P]
+    L.lela_cuda_last_error.restype = ctypes.c_char_p
+    L.lela_cuda_num_sms.argtypes = [_P]
+    L.lela_cuda_launch_count.argtypes = [_P]
+    L.lela_cuda_launch_count.restype = ctypes.c_uint64
+    L.lela_cuda_profile_enable.argtypes = [_P, _I]
+    L.lela_cuda_profile_read.argtypes = [_P, ctypes.c_char_p, ctypes.POINTER(ctypes.c_double),
+                                         ctypes.POINTER(ctypes.c_uint64)]
+    L.lela_cuda_profile_reset.argtypes = [_P]
+    gemm_args = [_P, _S, _S, _S, _U, _U, _P, _S, _P, _S, _U, _P, _S]
+    L.lela_cuda_gemm_zp_u32.argtypes = gemm_args
+    L.lela_cuda_gemm_zp_u32_dev.argtypes = gemm_args
+    _bind_optional(L)
+    _lib = L
+    return L
+
+
+def _bind_optional(L):
+    """Argument types of the entry points added alongside gemm."""
+    sigs = {
+        "lela_cuda_trsm_zp_u32": [_P, _I, _I, _S, _S, _U, _U, _P, _S, _P, _S, ctypes.POINTER(_S)],
+        "lela_cuda_trsm_zp_u32_dev": [_P, _I, _I, _S, _S, _U, _U, _P, _S, _P, _S, ctypes.POINTER(_S)],
+        "lela_cuda_echelon_zp_u32": [_P, _S, _S, _U, _P, _S, ctypes.POINTER(_S), ctypes.POINTER(_U)],
+        "lela_cuda_echelon_zp_u32_dev": [_P, _S, _S, _U, _P, _S, ctypes.POINTER(_S), ctypes.POINTER(_U)],
+        "lela_cuda_fl_echelonize_zp_u32": [_P, _S, _S, _U, _P, _P, _P, _I, _I, _P, _S,
+                                           ctypes.POINTER(_S), ctypes.POINTER(_U),
+                                           ctypes.POINTER(_S), ctypes.POINTER(_S)],
+        "lela_cuda_gemm_gf2": [_P, _S, _S, _S, _I, _P, _S, _P, _S, _I, _P, _S],
+        "lela_cuda_gemm_gf2_dev": [_P, _S, _S, _S, _I, _P, _S, _P, _S, _I, _P, _S],
+        "lela_cuda_echelon_gf2": [_P, _S, _S, _P, _S, ctypes.POINTER(_S)],
+        "lela_cuda_echelon_gf2_dev": [_P, _S, _S, _P, _S, ctypes.POINTER(_S)],
+        "lela_cuda_set_gf2_kernel": [_P, _I],
+    }
+    for name, args in sigs.items():
+        if hasattr(L, name):
+            getattr(L, name).argtypes = args
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _dptr(t):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+class CudaModule:
+    """One handle of the CUDA module on ``device`` (default 0)."""
+
+    def __init__(self, device=0):
+        self.L = load_library()
+        h = _P()
+        st = self.L.lela_cuda_create(ctypes.byref(h), int(device))
+        if st != OK:
+            raise CudaError("lela_cuda_create(device=%d) failed: %s" %
+                            (device, self.L.lela_cuda_status_string(st).decode()))
+        self.h = h
+        self.device = device
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.lela_cuda_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ---------------------------------------------------------------- misc
+    def _raise(self, st, aux=0):
+        if st == OK:
+            return
+        msg = self.L.lela_cuda_last_error(self.h).decode()
+        if st == DIAG:
+            raise DiagonalEntryNotInvertible(aux)
+        if st == WRONG_FORM:
+            raise WrongMatrixForm(aux)
+        if st == PIVOT:
+            raise LELAError("Could not invert pivot-element in the ring")
+        if st == ERR_ARG:
+            raise PreconditionFailed(msg)
+        raise CudaError("%s: %s" % (self.L.lela_cuda_status_string(st).decode(), msg))
+
+    def set_stream(self, stream):
+        """Run on a caller stream (cudaStream_t as int / torch.cuda.Stream)."""
+        handle = getattr(stream, "cuda_stream", stream)
+        self._raise(self.L.lela_cuda_set_stream(self.h, _P(handle)))
+
+    def stream(self):
+        return self.L.lela_cuda_get_stream(self.h)
+
+    def synchronize(self):
+        self._raise(self.L.lela_cuda_synchronize(self.h))
+
+    def set_gemm_kernel(self, kernel):
+        self._raise(self.L.lela_cuda_set_gemm_kernel(self.h, int(kernel)))
+
+    @property
+    def num_sms(self):
+        return self.L.lela_cuda_num_sms(self.h)
+
+    @property
+    def launch_count(self):
+        """Kernel launches issued through this handle so far."""
+        return int(self.L.lela_cuda_launch_count(self.h))
+
+    def profile(self, on=True):
+        self._raise(self.L.lela_cuda_profile_enable(self.h, int(on)))
+
+    def profile_read(self, kernel):
+        """(total device ms, launches) of one kernel since the last read."""
+        ms = ctypes.c_double(0)
+        n = ctypes.c_uint64(0)
+        self._raise(self.L.lela_cuda_profile_read(self.h, kernel.encode(), ctypes.byref(ms),
+                                                  ctypes.byref(n)))
+        return ms.value, int(n.value)
+
+    def profile_reset(self):
+        self._raise(self.L.lela_cuda_profile_reset(self.h))
+
+    # ---------------------------------------------------------- Z/p gemm
+    def gemm(self, p, a, A, B, b, C):
+        """C <- a*A*B + b*C mod p in place (BLAS3::gemm); returns C.
+        Host numpy uint32 matrices or torch CUDA tensors (int32/uint32)."""
+        if _is_torch(C):
+            m, n = C.shape
+            k = A.shape[1]
+            _check(A.shape[0] == m and B.shape == (k, n), "gemm: dimension mismatch")
+            st = self.L.lela_cuda_gemm_zp_u32_dev(self.h, m, n, k, p, a % p, _dptr(A), A.stride(0),
+                                                  _dptr(B), B.stride(0), b % p, _dptr(C), C.stride(0))
+            self._raise(st)
+            return C
+        _check(C.dtype == np.uint32 and A.dtype == np.uint32 and B.dtype == np.uint32,
+               "gemm: uint32 matrices expected")
+        m, n = C.shape
+        k = A.shape[1]
+        _check(A.shape[0] == m and B.shape == (k, n), "gemm: dimension mismatch")
+        _check(C.flags.c_contiguous or C.strides[1] == 4, "gemm: rows of C must be contiguous")
+        st = self.L.lela_cuda_gemm_zp_u32(self.h, m, n, k, p, a % p, _ptr(A), A.strides[0] // 4,
+                                          _ptr(B), B.strides[0] // 4, b % p, _ptr(C), C.strides[0] // 4)
+        self._raise(st)
+        return C
+
+
+def _is_torch(x):
+    return type(x).__module__.startswith("torch")
+
+
+def _check(cond, msg):
+    if not cond:
+        raise PreconditionFailed(msg)

@@ -1,0 +1,343 @@
+// lela_b200/csrc/api.cu -- the C ABI (include/lela_cuda.h): handle
+// management and the host-pointer / device-pointer entry points.
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <new>
+
+#include "../../include/lela_cuda.h"
+#include "common.cuh"
+#include "context.h"
+#include "zp_gemm.h"
+
+struct lela_cuda_ctx {
+  lela::Ctx c;
+};
+
+namespace lela {
+
+int ctx_fail(Ctx *c, int code, const char *msg) {
+  c->last_error = msg ? msg : "";
+  return code;
+}
+
+int ctx_cuda(Ctx *c, cudaError_t e, const char *what) {
+  char buf[256];
+  snprintf(buf, sizeof buf, "%s: %s", what, cudaGetErrorString(e));
+  c->last_error = buf;
+  if (e == cudaErrorMemoryAllocation) return ST_NOMEM;
+  return ST_CUDA;
+}
+
+static int grow(Ctx *c, void **buf, size_t *have, size_t bytes, const char *what) {
+  if (bytes <= *have && *buf) return ST_OK;
+  if (*buf) {
+    // The old buffer may still be in use by queued work.
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return ctx_cuda(c, e, "cudaStreamSynchronize");
+    cudaFree(*buf);
+    *buf = nullptr;
+    *have = 0;
+  }
+  size_t want = std::max(bytes, (size_t)1 << 20);
+  cudaError_t e = cudaMalloc(buf, want);
+  if (e != cudaSuccess) {
+    *buf = nullptr;
+    return ctx_cuda(c, e, what);
+  }
+  *have = want;
+  return ST_OK;
+}
+
+int ctx_workspace(Ctx *c, size_t bytes, void **out) {
+  int st = grow(c, &c->ws, &c->ws_bytes, bytes, "cudaMalloc(workspace)");
+  *out = c->ws;
+  return st;
+}
+
+int ctx_workspace2(Ctx *c, size_t bytes, void **out) {
+  int st = grow(c, &c->ws2, &c->ws2_bytes, bytes, "cudaMalloc(workspace2)");
+  *out = c->ws2;
+  return st;
+}
+
+int ctx_stage(Ctx *c, int slot, size_t bytes, void **out) {
+  int st = grow(c, &c->stage[slot], &c->stage_bytes[slot], bytes, "cudaMalloc(staging)");
+  *out = c->stage[slot];
+  return st;
+}
+
+int ctx_clear_status(Ctx *c) {
+  cudaError_t e = cudaMemsetAsync(c->dstatus, 0, 16 * sizeof(uint32_t), c->stream);
+  return e == cudaSuccess ? ST_OK : ctx_cuda(c, e, "cudaMemsetAsync(status)");
+}
+
+int ctx_check_status(Ctx *c, const char *what) {
+  cudaError_t e = cudaMemcpyAsync(c->hstatus, c->dstatus, 16 * sizeof(uint32_t),
+                                  cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return ctx_cuda(c, e, what);
+  if (c->hstatus[0] & DEVERR_TIMEOUT) {
+    char buf[160];
+    snprintf(buf, sizeof buf, "%s: a device-side wait exceeded its limit", what);
+    return ctx_fail(c, ST_TIMEOUT, buf);
+  }
+  return ST_OK;
+}
+
+static cudaEvent_t pool_event(Ctx *c) {
+  if (!c->event_pool.empty()) {
+    cudaEvent_t e = c->event_pool.back();
+    c->event_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+int prof_begin(Ctx *c, const char *name) {
+  if (!c->profile) return -1;
+  Ctx::ProfRec r;
+  r.name = name;
+  r.a = pool_event(c);
+  r.b = pool_event(c);
+  cudaEventRecord(r.a, c->stream);
+  c->prof.push_back(r);
+  return (int)c->prof.size() - 1;
+}
+
+void prof_end(Ctx *c, int idx) {
+  if (idx < 0 || idx >= (int)c->prof.size()) return;
+  cudaEventRecord(c->prof[idx].b, c->stream);
+}
+
+}  // namespace lela
+
+using namespace lela;
+
+extern "C" {
+
+int lela_cuda_create(lela_cuda_ctx **out, int device) {
+  if (!out) return ST_ARG;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) return ST_CUDA;
+  lela_cuda_ctx *h = new (std::nothrow) lela_cuda_ctx;
+  if (!h) return ST_NOMEM;
+  Ctx *c = &h->c;
+  c->device = device;
+  cudaError_t e = cudaSetDevice(device);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
+  int major = 0;
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device);
+  if (e == cudaSuccess && major != 10) {
+    delete h;
+    return ST_UNSUPPORTED;
+  }
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) c->own_stream = true;
+  if (e == cudaSuccess) e = cudaMalloc(&c->dstatus, 16 * sizeof(uint32_t));
+  if (e == cudaSuccess) e = cudaMemset(c->dstatus, 0, 16 * sizeof(uint32_t));
+  if (e == cudaSuccess) e = cudaMallocHost(&c->hstatus, 16 * sizeof(uint32_t));
+  if (e == cudaSuccess) {
+    cudaDriverEntryPointQueryResult q;
+    e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &c->encode_tiled, cudaEnableDefault, &q);
+    if (e == cudaSuccess && q != cudaDriverEntryPointSuccess) c->encode_tiled = nullptr;
+  }
+  if (e != cudaSuccess) {
+    lela_cuda_destroy(h);
+    return e == cudaErrorMemoryAllocation ? ST_NOMEM : ST_CUDA;
+  }
+  *out = h;
+  return ST_OK;
+}
+
+int lela_cuda_destroy(lela_cuda_ctx *h) {
+  if (!h) return ST_OK;
+  Ctx *c = &h->c;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->ws) cudaFree(c->ws);
+  if (c->ws2) cudaFree(c->ws2);
+  for (int i = 0; i < 4; ++i)
+    if (c->stage[i]) cudaFree(c->stage[i]);
+  if (c->dstatus) cudaFree(c->dstatus);
+  if (c->hstatus) cudaFreeHost(c->hstatus);
+  for (auto &r : c->prof) {
+    cudaEventDestroy(r.a);
+    cudaEventDestroy(r.b);
+  }
+  for (auto e : c->event_pool) cudaEventDestroy(e);
+  if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+  delete h;
+  return ST_OK;
+}
+
+int lela_cuda_set_stream(lela_cuda_ctx *h, void *stream) {
+  if (!h) return ST_ARG;
+  Ctx *c = &h->c;
+  cudaStreamSynchronize(c->stream);
+  if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+  c->own_stream = false;
+  c->stream = static_cast<cudaStream_t>(stream);
+  if (!stream) {
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
+      return ST_CUDA;
+    c->own_stream = true;
+  }
+  return ST_OK;
+}
+
+void *lela_cuda_get_stream(lela_cuda_ctx *h) { return h ? (void *)h->c.stream : nullptr; }
+
+int lela_cuda_synchronize(lela_cuda_ctx *h) {
+  if (!h) return ST_ARG;
+  Ctx *c = &h->c;
+  int st = ctx_check_status(c, "synchronize");
+  if (st == ST_OK) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return ctx_cuda(c, e, "synchronize");
+  }
+  if (st != ST_OK) ctx_clear_status(c);
+  return st;
+}
+
+int lela_cuda_set_gemm_kernel(lela_cuda_ctx *h, int kernel) {
+  if (!h || kernel < GEMM_AUTO || kernel > GEMM_TC) return ST_ARG;
+  h->c.gemm_kernel = kernel;
+  return ST_OK;
+}
+
+const char *lela_cuda_status_string(int s) {
+  switch (s) {
+    case ST_OK: return "ok";
+    case ST_ARG: return "invalid argument";
+    case ST_CUDA: return "CUDA error";
+    case ST_NOMEM: return "out of device memory";
+    case ST_DIAG: return "diagonal entry not invertible";
+    case ST_WRONG_FORM: return "wrong matrix form";
+    case ST_PIVOT: return "pivot not invertible in the ring";
+    case ST_TIMEOUT: return "device-side wait timed out";
+    case ST_UNSUPPORTED: return "unsupported";
+    default: return "unknown status";
+  }
+}
+
+const char *lela_cuda_last_error(lela_cuda_ctx *h) { return h ? h->c.last_error.c_str() : ""; }
+
+int lela_cuda_num_sms(lela_cuda_ctx *h) { return h ? h->c.num_sms : 0; }
+
+uint64_t lela_cuda_launch_count(lela_cuda_ctx *h) { return h ? h->c.launches : 0; }
+
+int lela_cuda_profile_enable(lela_cuda_ctx *h, int on) {
+  if (!h) return ST_ARG;
+  h->c.profile = on != 0;
+  return ST_OK;
+}
+
+int lela_cuda_profile_read(lela_cuda_ctx *h, const char *kernel, double *total_ms,
+                           uint64_t *launches) {
+  if (!h || !kernel || !total_ms || !launches) return ST_ARG;
+  Ctx *c = &h->c;
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return ctx_cuda(c, e, "profile_read");
+  double ms = 0;
+  uint64_t n = 0;
+  std::vector<Ctx::ProfRec> keep;
+  for (auto &r : c->prof) {
+    if (strcmp(r.name, kernel) == 0) {
+      float t = 0;
+      if (cudaEventElapsedTime(&t, r.a, r.b) == cudaSuccess) {
+        ms += t;
+        ++n;
+      }
+      c->event_pool.push_back(r.a);
+      c->event_pool.push_back(r.b);
+    } else {
+      keep.push_back(r);
+    }
+  }
+  c->prof.swap(keep);
+  *total_ms = ms;
+  *launches = n;
+  return ST_OK;
+}
+
+int lela_cuda_profile_reset(lela_cuda_ctx *h) {
+  if (!h) return ST_ARG;
+  Ctx *c = &h->c;
+  cudaStreamSynchronize(c->stream);
+  for (auto &r : c->prof) {
+    c->event_pool.push_back(r.a);
+    c->event_pool.push_back(r.b);
+  }
+  c->prof.clear();
+  return ST_OK;
+}
+
+int lela_cuda_gemm_zp_u32_dev(lela_cuda_ctx *h, size_t m, size_t n, size_t k, uint32_t p,
+                              uint32_t a, const uint32_t *A, size_t lda, const uint32_t *B,
+                              size_t ldb, uint32_t b, uint32_t *C, size_t ldc) {
+  if (!h) return ST_ARG;
+  Ctx *c = &h->c;
+  if (m > (size_t)INT32_MAX || n > (size_t)INT32_MAX || k > (size_t)INT32_MAX)
+    return ctx_fail(c, ST_ARG, "dimension too large");
+  if ((m && n && !C) || (m && k && n && (!A || !B))) return ctx_fail(c, ST_ARG, "null pointer");
+  return zp_gemm_dev(c, GEMM_AUTO, (int)m, (int)n, (int)k, p, a, A, lda, B, ldb, b, C, ldc,
+                     nullptr);
+}
+
+// Copy a host matrix with row stride ld into a dense device buffer
+// (row stride = cols) and back.
+static int h2d_matrix(Ctx *c, void *dst, const void *src, size_t rows, size_t cols, size_t ld,
+                      size_t esz) {
+  if (!rows || !cols) return ST_OK;
+  cudaError_t e = cudaMemcpy2DAsync(dst, cols * esz, src, ld * esz, cols * esz, rows,
+                                    cudaMemcpyHostToDevice, c->stream);
+  return e == cudaSuccess ? ST_OK : ctx_cuda(c, e, "host->device copy");
+}
+
+static int d2h_matrix(Ctx *c, void *dst, const void *src, size_t rows, size_t cols, size_t ld,
+                      size_t esz) {
+  if (!rows || !cols) return ST_OK;
+  cudaError_t e = cudaMemcpy2DAsync(dst, ld * esz, src, cols * esz, cols * esz, rows,
+                                    cudaMemcpyDeviceToHost, c->stream);
+  return e == cudaSuccess ? ST_OK : ctx_cuda(c, e, "device->host copy");
+}
+
+int lela_cuda_gemm_zp_u32(lela_cuda_ctx *h, size_t m, size_t n, size_t k, uint32_t p, uint32_t a,
+                          const uint32_t *A, size_t lda, const uint32_t *B, size_t ldb, uint32_t b,
+                          uint32_t *C, size_t ldc) {
+  if (!h) return ST_ARG;
+  Ctx *c = &h->c;
+  if (m > (size_t)INT32_MAX || n > (size_t)INT32_MAX || k > (size_t)INT32_MAX)
+    return ctx_fail(c, ST_ARG, "dimension too large");
+  if (p < 2) return ctx_fail(c, ST_ARG, "modulus must be at least 2");
+  if (m == 0 || n == 0) return ST_OK;
+  if (!C || (k && (!A || !B))) return ctx_fail(c, ST_ARG, "null pointer");
+  if (ldc < n || (k && (lda < k || ldb < n)))
+    return ctx_fail(c, ST_ARG, "leading dimension smaller than the row length");
+  cudaSetDevice(c->device);
+  void *dA = nullptr, *dB = nullptr, *dC = nullptr;
+  int st = ST_OK;
+  if (!st && k) st = ctx_stage(c, 0, m * k * 4, &dA);
+  if (!st && k) st = ctx_stage(c, 1, k * n * 4, &dB);
+  if (!st) st = ctx_stage(c, 2, m * n * 4, &dC);
+  if (!st) st = ctx_clear_status(c);
+  if (!st && k) st = h2d_matrix(c, dA, A, m, k, lda, 4);
+  if (!st && k) st = h2d_matrix(c, dB, B, k, n, ldb, 4);
+  // With b = 0 mod p the kernels never read C.
+  if (!st && (b % p) != 0) st = h2d_matrix(c, dC, C, m, n, ldc, 4);
+  if (!st)
+    st = zp_gemm_dev(c, GEMM_AUTO, (int)m, (int)n, (int)k, p, a, (const uint32_t *)dA, k,
+                     (const uint32_t *)dB, n, b, (uint32_t *)dC, n, nullptr);
+  if (!st) st = d2h_matrix(c, C, dC, m, n, ldc, 4);
+  if (!st) st = ctx_check_status(c, "gemm_zp_u32");
+  return st;
+}
+
+}  // extern "C"

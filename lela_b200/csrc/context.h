@@ -1,0 +1,86 @@
+// lela_b200/csrc/context.h -- per-handle host state of the CUDA module.
+//
+// A handle owns one CUDA stream (or borrows the caller's), a growable device
+// workspace, a small device status block that kernels report errors into,
+// and the pinned host staging used by the host-pointer entry points.  Like
+// a LELA Context (lela/blas/context.h:61-63) a handle is not re-entrant:
+// use one handle per host thread.
+#pragma once
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace lela {
+
+// Kernel families a caller (or the selector) can force.
+enum GemmKernel : int {
+  GEMM_AUTO = 0,   // tensor-core path when the shape allows it
+  GEMM_PLAIN = 1,  // CUDA-core 64-bit delayed-reduction gemm
+  GEMM_TC = 2,     // limb-split INT8 tcgen05 gemm
+};
+
+struct Ctx {
+  int device = 0;
+  int num_sms = 148;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+
+  // Device workspace (grown on demand, never shrunk until destroy).
+  void *ws = nullptr;
+  size_t ws_bytes = 0;
+  // Second workspace for callers that need two live scratch regions.
+  void *ws2 = nullptr;
+  size_t ws2_bytes = 0;
+
+  // Device status words: [0] = error bits, [1..] = auxiliary outputs.
+  uint32_t *dstatus = nullptr;
+  // Pinned host mirror of the status block.
+  uint32_t *hstatus = nullptr;
+
+  // Device staging buffers for the host-pointer entry points.
+  void *stage[4] = {nullptr, nullptr, nullptr, nullptr};
+  size_t stage_bytes[4] = {0, 0, 0, 0};
+
+  int gemm_kernel = GEMM_AUTO;
+  std::string last_error;
+
+  // Kernel launches issued through this handle (all kernels of the library).
+  uint64_t launches = 0;
+  // Optional per-kernel device timing: an event pair around each launch of
+  // the named kernels, summed by lela_cuda_profile_read.
+  bool profile = false;
+  struct ProfRec {
+    const char *name;
+    cudaEvent_t a, b;
+  };
+  std::vector<ProfRec> prof;
+  std::vector<cudaEvent_t> event_pool;
+
+  // cuTensorMapEncodeTiled, resolved through the runtime at handle creation.
+  void *encode_tiled = nullptr;
+};
+
+// Grow-only allocation helpers; return ST_OK or ST_NOMEM.
+int ctx_workspace(Ctx *c, size_t bytes, void **out);
+int ctx_workspace2(Ctx *c, size_t bytes, void **out);
+int ctx_stage(Ctx *c, int slot, size_t bytes, void **out);
+// Record a CUDA error (returns ST_CUDA) or a message (returns code).
+int ctx_fail(Ctx *c, int code, const char *msg);
+int ctx_cuda(Ctx *c, cudaError_t e, const char *what);
+// Reset the device error word (async on the handle's stream).
+int ctx_clear_status(Ctx *c);
+// Read back the device error word (synchronises the stream) and map it to
+// a status code.
+int ctx_check_status(Ctx *c, const char *what);
+
+// Profiling: prof_begin records the start event of a named kernel launch
+// (returns an index, or -1 when profiling is off); prof_end its end event.
+int prof_begin(Ctx *c, const char *name);
+void prof_end(Ctx *c, int idx);
+inline void ctx_launched(Ctx *c, int n = 1) { c->launches += (uint64_t)n; }
+
+}  // namespace lela

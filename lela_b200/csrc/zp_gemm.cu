@@ -1,0 +1,609 @@
+// lela_b200/csrc/zp_gemm.cu -- dense gemm over Z/p (Modular<uint32>):
+//   C <- alpha * A * B + beta * C  (mod p),  p in [2, 2^32).
+//
+// Replaces the per-entry delayed-reduction dot products of LELA's generic
+// gemm (lela/blas/level3-generic.tcc:285-322 with _dot<Modular<uint32>,
+// ZpModule> of lela/blas/level1-modular.tcc:135-158).  Two kernels:
+//
+// 1. zp_gemm_tc_kernel<L> -- limb-split INT8 tensor-core gemm.  Every entry
+//    x in [0, p) is split into L unsigned 8-bit limbs, x = sum_i x_i 2^(8i),
+//    with L = 1 (p <= 2^8), 2 (p <= 2^16) or 4 (p <= 2^32).  For each pair of
+//    limbs (i, j) the tensor cores form P_ij = A_i * B_j with exact signed
+//    32-bit accumulation (tcgen05.mma .kind::i8, accumulators in TMEM).
+//    Overflow bound: a limb product is at most 255^2 = 65025, so a K-chunk
+//    of at most 33025 terms cannot exceed 2^31 - 1; the host splits K into
+//    chunks of KCHUNK = 32768 (the first chunk applies beta, the others add
+//    with beta = 1).  The epilogue recombines
+//        A*B = sum_s 2^(8s) D_s,   D_s = sum_{i+j=s} P_ij   (D_s < 4 * 2^31)
+//    reduces mod p with Barrett reduction and applies alpha and beta; the
+//    result is exact, i.e. bit-identical to LELA's.
+//
+//    Data layout.  A is split into L planes of M x Kp bytes (K-major, i.e.
+//    row-major A), B into L planes of N x Kp bytes (K-major, i.e. B^T); Kp =
+//    K rounded up to 16 bytes (the TMA row-pitch rule).  One CTA owns a
+//    128 x BN tile of C and stacks the limbs: the A operand of the i-th MMA
+//    is A_i (128 rows), the B operand is [B_0; ..; B_{L-1}] (L*BN rows), so
+//    one 128 x (L*BN) accumulator per A-limb holds P_i0 .. P_i(L-1) side by
+//    side; L accumulators use all 512 TMEM columns for L = 2 and 4.
+//
+//    Pipeline (persistent, warp-specialised, 192 threads): warp 0 issues TMA
+//    loads of 128-byte-swizzled K-blocks (128 bytes of K) into a ring of
+//    shared-memory stages; warp 1 issues 4*L MMAs of K = 32 per stage and
+//    releases stages with tcgen05.commit; warps 2-5 drain the accumulators
+//    (one TMEM lane = one row of C per thread).  Every wait is bounded.
+//
+// 2. zp_gemm_plain_kernel -- the "plain GPU form": a CUDA-core tiled gemm
+//    whose inner loop is exactly the reference's delayed-reduction dot
+//    (64-bit sum of 32x32-bit products, + 2^64 mod p on wrap-around, one
+//    final reduction).
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <cstdio>
+
+#include "common.cuh"
+#include "context.h"
+#include "zp_gemm.h"
+
+namespace lela {
+
+// ------------------------------------------------------------ tile configs
+template <int L>
+struct TcCfg;
+template <>
+struct TcCfg<1> {
+  static constexpr int BN = 256, NMMA = 256, STAGES = 4, ACC = 2;
+};
+template <>
+struct TcCfg<2> {
+  static constexpr int BN = 128, NMMA = 256, STAGES = 3, ACC = 1;
+};
+template <>
+struct TcCfg<4> {
+  static constexpr int BN = 32, NMMA = 128, STAGES = 2, ACC = 1;
+};
+
+constexpr int BM = 128;         // rows of C per tile (UMMA M)
+constexpr int BK = 128;         // bytes (= limb elements) of K per stage
+constexpr int GROUP_M = 16;     // tile raster: 16 row-blocks per group
+constexpr int TMEM_COLS = 512;
+
+template <int L>
+struct TcLayout {
+  using Cfg = TcCfg<L>;
+  static constexpr int A_BYTES = L * BM * BK;
+  static constexpr int B_BYTES = Cfg::NMMA * BK;
+  static constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
+  static constexpr int BAR_OFF = Cfg::STAGES * STAGE_BYTES;
+  // full[S], empty[S], tfull[ACC], tempty[ACC], done, tmem base
+  static constexpr int BAR_BYTES = 8 * (2 * Cfg::STAGES + 2 * Cfg::ACC + 1) + 8;
+  static constexpr int SMEM = BAR_OFF + BAR_BYTES + 1024;
+};
+
+__device__ __forceinline__ void tile_coords(int t, int tiles_m, int tiles_n, int &mb, int &nb) {
+  int per_group = GROUP_M * tiles_n;
+  int g = t / per_group;
+  int first_m = g * GROUP_M;
+  int gsize = min(GROUP_M, tiles_m - first_m);
+  int w = t - g * per_group;
+  mb = first_m + w % gsize;
+  nb = w / gsize;
+}
+
+// Bounded wait that ignores the error word (used only to drain in-flight
+// asynchronous operations before the block exits).
+__device__ __forceinline__ void mbar_drain(uint64_t *bar, uint32_t parity, uint32_t *err) {
+  uint64_t t0 = globaltimer_ns();
+  while (!mbar_try_wait(bar, parity)) {
+    if (globaltimer_ns() - t0 > WAIT_LIMIT_NS) {
+      atomicOr(err, DEVERR_TIMEOUT);
+      return;
+    }
+  }
+}
+
+template <int L>
+__device__ __forceinline__ void epilogue_chunk(uint32_t tcol, int gm, int gn0, int M, int N,
+                                               uint32_t *C, size_t ldc, const Modulus &mod,
+                                               uint32_t alpha, uint32_t beta);
+
+// L = 1: one product, P_00 < 2^31.
+template <>
+__device__ __forceinline__ void epilogue_chunk<1>(uint32_t tcol, int gm, int gn0, int M, int N,
+                                                  uint32_t *C, size_t ldc, const Modulus &mod,
+                                                  uint32_t alpha, uint32_t beta) {
+  uint32_t r[16];
+  tmem_ld16(tcol, r);
+  tmem_ld_wait();
+  if (gm < M) {
+    uint32_t *crow = C + (size_t)gm * ldc;
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+      int gn = gn0 + i;
+      if (gn < N) {
+        uint32_t v = mod_reduce((uint64_t)r[i], mod);
+        uint32_t c = beta ? crow[gn] : 0u;
+        crow[gn] = mod_axpby(alpha, v, beta, c, mod);
+      }
+    }
+  }
+}
+
+// L = 2: A*B = 2^16 P_11 + 2^8 (P_01 + P_10) + P_00 < 2^48.
+template <>
+__device__ __forceinline__ void epilogue_chunk<2>(uint32_t tcol, int gm, int gn0, int M, int N,
+                                                  uint32_t *C, size_t ldc, const Modulus &mod,
+                                                  uint32_t alpha, uint32_t beta) {
+  constexpr int BN = TcCfg<2>::BN, NMMA = TcCfg<2>::NMMA;
+  uint32_t p00[16], p01[16], p10[16], p11[16];
+  tmem_ld16(tcol, p00);
+  tmem_ld16(tcol + BN, p01);
+  tmem_ld16(tcol + NMMA, p10);
+  tmem_ld16(tcol + NMMA + BN, p11);
+  tmem_ld_wait();
+  if (gm < M) {
+    uint32_t *crow = C + (size_t)gm * ldc;
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+      int gn = gn0 + i;
+      if (gn < N) {
+        uint64_t v = ((uint64_t)p11[i] << 16) + (((uint64_t)p01[i] + p10[i]) << 8) + p00[i];
+        uint32_t vr = mod_reduce(v, mod);
+        uint32_t c = beta ? crow[gn] : 0u;
+        crow[gn] = mod_axpby(alpha, vr, beta, c, mod);
+      }
+    }
+  }
+}
+
+// L = 4: D_s = sum_{i+j=s} P_ij < 2^33, Horner in s with a reduction per
+// step ((r < 2^32) * 2^8 + D_s < 2^41).  Eight columns at a time to keep the
+// seven 64-bit partial sums in registers.
+template <>
+__device__ __forceinline__ void epilogue_chunk<4>(uint32_t tcol, int gm, int gn0, int M, int N,
+                                                  uint32_t *C, size_t ldc, const Modulus &mod,
+                                                  uint32_t alpha, uint32_t beta) {
+  constexpr int BN = TcCfg<4>::BN, NMMA = TcCfg<4>::NMMA;
+#pragma unroll 1
+  for (int h = 0; h < 16; h += 8) {
+    uint64_t D[7][8];
+#pragma unroll
+    for (int s = 0; s < 7; ++s)
+#pragma unroll
+      for (int i = 0; i < 8; ++i) D[s][i] = 0;
+#pragma unroll
+    for (int li = 0; li < 4; ++li) {
+#pragma unroll
+      for (int lj = 0; lj < 4; ++lj) {
+        uint32_t r[8];
+        tmem_ld8(tcol + h + li * NMMA + lj * BN, r);
+        tmem_ld_wait();
+#pragma unroll
+        for (int i = 0; i < 8; ++i) D[li + lj][i] += r[i];
+      }
+    }
+    if (gm < M) {
+      uint32_t *crow = C + (size_t)gm * ldc;
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        int gn = gn0 + h + i;
+        if (gn < N) {
+          uint32_t acc = mod_reduce(D[6][i], mod);
+#pragma unroll
+          for (int s = 5; s >= 0; --s) acc = mod_reduce(((uint64_t)acc << 8) + D[s][i], mod);
+          uint32_t c = beta ? crow[gn] : 0u;
+          crow[gn] = mod_axpby(alpha, acc, beta, c, mod);
+        }
+      }
+    }
+  }
+}
+
+template <int L>
+__global__ void __launch_bounds__(192, 1)
+    zp_gemm_tc_kernel(const __grid_constant__ CUtensorMap tmA,
+                      const __grid_constant__ CUtensorMap tmB, uint32_t *__restrict__ C,
+                      size_t ldc, int M, int N, int K, Modulus mod, uint32_t alpha, uint32_t beta,
+                      uint32_t *err) {
+  using Cfg = TcCfg<L>;
+  using Lay = TcLayout<L>;
+  constexpr int S = Cfg::STAGES, ACC = Cfg::ACC, BN = Cfg::BN, NMMA = Cfg::NMMA;
+  constexpr uint32_t IDESC = idesc_u8_s32(BM, NMMA);
+
+  extern __shared__ uint8_t smem_raw[];
+  uint32_t base_off = smem_u32(smem_raw);
+  uint8_t *smem = smem_raw + ((1024 - (base_off & 1023)) & 1023);
+  uint64_t *full = reinterpret_cast<uint64_t *>(smem + Lay::BAR_OFF);
+  uint64_t *empty = full + S;
+  uint64_t *tfull = empty + S;
+  uint64_t *tempty = tfull + ACC;
+  uint64_t *done = tempty + ACC;
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(done + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int num_kb = (K + BK - 1) / BK;
+  const int tiles_m = (M + BM - 1) / BM, tiles_n = (N + BN - 1) / BN;
+  const int num_tiles = tiles_m * tiles_n;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < S; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    for (int a = 0; a < ACC; ++a) {
+      mbar_init(&tfull[a], 1);
+      mbar_init(&tempty[a], 128);
+    }
+    mbar_init(done, 1);
+    fence_barrier_init();
+    prefetch_tmap(&tmA);
+    prefetch_tmap(&tmB);
+  }
+  if (warp == 1) tmem_alloc(tmem_slot, TMEM_COLS);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      // ---------------------------------------------------------- producer
+      uint32_t s = 0, ph = 0;
+      uint32_t issued = 0, last_ph[S];
+      for (int i = 0; i < S; ++i) last_ph[i] = 0;
+      bool ok = true;
+      for (int t = blockIdx.x; t < num_tiles && ok; t += gridDim.x) {
+        int mb, nb;
+        tile_coords(t, tiles_m, tiles_n, mb, nb);
+        for (int kb = 0; kb < num_kb; ++kb) {
+          if (!mbar_wait(&empty[s], ph ^ 1, err)) { ok = false; break; }
+          uint8_t *sa = smem + s * Lay::STAGE_BYTES;
+          uint8_t *sb = sa + Lay::A_BYTES;
+          mbar_arrive_expect_tx(&full[s], Lay::STAGE_BYTES);
+          tma_load_3d(sa, &tmA, &full[s], kb * BK, mb * BM, 0);
+          tma_load_3d(sb, &tmB, &full[s], kb * BK, nb * BN, 0);
+          issued |= 1u << s;
+          last_ph[s] = ph;
+          if (++s == S) { s = 0; ph ^= 1; }
+        }
+      }
+      if (!ok) {
+        // Wait for the loads already in flight before the block may exit.
+        for (int i = 0; i < S; ++i)
+          if (issued & (1u << i)) mbar_drain(&full[i], last_ph[i], err);
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      // --------------------------------------------------------- MMA issue
+      uint32_t s = 0, ph = 0;
+      int it = 0;
+      bool ok = true;
+      for (int t = blockIdx.x; t < num_tiles && ok; t += gridDim.x, ++it) {
+        const int a = it % ACC;
+        const uint32_t aph = (uint32_t)(it / ACC) & 1u;
+        if (!mbar_wait(&tempty[a], aph ^ 1, err)) { ok = false; break; }
+        tc_fence_after();
+        const uint32_t dbase = tmem + (uint32_t)(a * L * NMMA);
+        for (int kb = 0; kb < num_kb; ++kb) {
+          if (!mbar_wait(&full[s], ph, err)) { ok = false; break; }
+          tc_fence_after();
+          uint8_t *sa = smem + s * Lay::STAGE_BYTES;
+          uint8_t *sb = sa + Lay::A_BYTES;
+          const uint64_t bd = smem_desc_sw128(sb);
+#pragma unroll
+          for (int l = 0; l < L; ++l) {
+            const uint64_t ad = smem_desc_sw128(sa + l * BM * BK);
+#pragma unroll
+            for (int kk = 0; kk < BK / 32; ++kk) {
+              // +32 bytes of K inside the 128-byte swizzled row = +2 in the
+              // descriptor's (address >> 4) field.
+              mma_u8(dbase + (uint32_t)(l * NMMA), ad + 2 * kk, bd + 2 * kk, IDESC,
+                     (kb | kk) != 0);
+            }
+          }
+          mma_commit(&empty[s]);
+          if (++s == S) { s = 0; ph ^= 1; }
+        }
+        if (!ok) break;
+        mma_commit(&tfull[a]);
+      }
+      // All MMAs of this thread must finish before TMEM is released.
+      mma_commit(done);
+      mbar_drain(done, 0, err);
+    }
+  } else {
+    // ------------------------------------------------------------ epilogue
+    const int q = warp & 3;  // TMEM lane quadrant this warp may access
+    const int row = q * 32 + lane;
+    int it = 0;
+    for (int t = blockIdx.x; t < num_tiles; t += gridDim.x, ++it) {
+      int mb, nb;
+      tile_coords(t, tiles_m, tiles_n, mb, nb);
+      const int a = it % ACC;
+      const uint32_t aph = (uint32_t)(it / ACC) & 1u;
+      if (!mbar_wait(&tfull[a], aph, err)) break;
+      tc_fence_after();
+      const uint32_t tbase = tmem + (uint32_t)(a * L * NMMA) + ((uint32_t)(q * 32) << 16);
+      const int gm = mb * BM + row;
+#pragma unroll 1
+      for (int c0 = 0; c0 < BN; c0 += 16)
+        epilogue_chunk<L>(tbase + c0, gm, nb * BN + c0, M, N, C, ldc, mod, alpha, beta);
+      tc_fence_before();
+      mbar_arrive(&tempty[a]);
+    }
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    tmem_dealloc(tmem, TMEM_COLS);
+  }
+}
+
+// ------------------------------------------------------------ limb splits
+// A (M x kc, row stride lda, u32) -> L planes of M x Kp bytes.
+template <int L>
+__global__ void split_rows_kernel(const uint32_t *__restrict__ A, size_t lda, int M, int kc,
+                                  uint8_t *__restrict__ out, int Kp) {
+  const int kq = (kc + 3) >> 2;
+  const size_t total = (size_t)M * kq;
+  const size_t plane = (size_t)M * Kp;
+  for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (size_t)gridDim.x * blockDim.x) {
+    const int r = (int)(idx / kq), k = (int)(idx % kq) * 4;
+    const uint32_t *src = A + (size_t)r * lda + k;
+    uint32_t v[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) v[i] = (k + i < kc) ? __ldg(src + i) : 0u;
+#pragma unroll
+    for (int l = 0; l < L; ++l) {
+      uint32_t w = 0;
+#pragma unroll
+      for (int i = 0; i < 4; ++i) w |= ((v[i] >> (8 * l)) & 0xFFu) << (8 * i);
+      *reinterpret_cast<uint32_t *>(out + l * plane + (size_t)r * Kp + k) = w;
+    }
+  }
+}
+
+// B (kc x N, row stride ldb, u32) -> L planes of N x Kp bytes (transposed),
+// through a 64 (k) x 32 (n) shared-memory tile.
+template <int L>
+__global__ void split_cols_kernel(const uint32_t *__restrict__ B, size_t ldb, int kc, int N,
+                                  uint8_t *__restrict__ out, int Kp) {
+  __shared__ uint32_t tile[64][33];
+  const int n0 = blockIdx.x * 32, k0 = blockIdx.y * 64;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  const size_t plane = (size_t)N * Kp;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    int k = k0 + ty + 8 * i, n = n0 + tx;
+    tile[ty + 8 * i][tx] = (k < kc && n < N) ? __ldg(B + (size_t)k * ldb + n) : 0u;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < 2; ++j) {
+    int w = threadIdx.x + 256 * j;
+    int n = w >> 4, kw = (w & 15) * 4;
+    int gn = n0 + n, gk = k0 + kw;
+    if (gn < N && gk < Kp) {
+#pragma unroll
+      for (int l = 0; l < L; ++l) {
+        uint32_t word = 0;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) word |= ((tile[kw + i][n] >> (8 * l)) & 0xFFu) << (8 * i);
+        *reinterpret_cast<uint32_t *>(out + l * plane + (size_t)gn * Kp + gk) = word;
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------ plain gemm
+constexpr int PT = 64, PK = 32;
+
+__global__ void __launch_bounds__(256)
+    zp_gemm_plain_kernel(const uint32_t *__restrict__ A, size_t lda,
+                         const uint32_t *__restrict__ B, size_t ldb, uint32_t *__restrict__ C,
+                         size_t ldc, int M, int N, int K, Modulus mod, uint32_t two64,
+                         uint32_t alpha, uint32_t beta) {
+  __shared__ uint32_t As[PK][PT + 1];
+  __shared__ uint32_t Bs[PK][PT + 1];
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const int m0 = blockIdx.y * PT, n0 = blockIdx.x * PT;
+  uint64_t acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = 0;
+
+  for (int k0 = 0; k0 < K; k0 += PK) {
+#pragma unroll
+    for (int e = 0; e < (PT * PK) / 256; ++e) {
+      int idx = threadIdx.x + 256 * e;
+      int r = idx / PK, kk = idx % PK;  // A tile: 64 rows x 32 k
+      int gm = m0 + r, gk = k0 + kk;
+      As[kk][r] = (gm < M && gk < K) ? __ldg(A + (size_t)gm * lda + gk) : 0u;
+      int kr = idx / PT, c = idx % PT;  // B tile: 32 k x 64 cols
+      int gk2 = k0 + kr, gn = n0 + c;
+      Bs[kr][c] = (gk2 < K && gn < N) ? __ldg(B + (size_t)gk2 * ldb + gn) : 0u;
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int kk = 0; kk < PK; ++kk) {
+      uint32_t a[4], b[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i] = As[kk][ty + 16 * i];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) b[j] = Bs[kk][tx + 16 * j];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          uint64_t t = (uint64_t)a[i] * b[j];
+          uint64_t s = acc[i][j] + t;
+          acc[i][j] = (s < t) ? s + two64 : s;
+        }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    int gm = m0 + ty + 16 * i;
+    if (gm >= M) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      int gn = n0 + tx + 16 * j;
+      if (gn >= N) continue;
+      uint32_t d = mod_reduce(acc[i][j], mod);
+      uint32_t c = beta ? C[(size_t)gm * ldc + gn] : 0u;
+      C[(size_t)gm * ldc + gn] = mod_axpby(alpha, d, beta, c, mod);
+    }
+  }
+}
+
+// Scale C <- beta * C (mod p), used when K = 0 or alpha = 0.
+__global__ void zp_scale_kernel(uint32_t *C, size_t ldc, int M, int N, Modulus mod,
+                                uint32_t beta) {
+  const size_t total = (size_t)M * N;
+  for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (size_t)gridDim.x * blockDim.x) {
+    size_t r = idx / N, c = idx % N;
+    uint32_t *x = C + r * ldc + c;
+    *x = beta ? mod_mul(*x, beta, mod) : 0u;
+  }
+}
+
+// ------------------------------------------------------------------ host
+static uint32_t host_two64(uint32_t p) {
+  uint64_t t = 2;
+  for (int i = 0; i < 6; ++i) t = (t * t) % p;
+  return (uint32_t)t;
+}
+
+int zp_limbs_for(uint32_t p) { return p <= 256u ? 1 : (p <= 65536u ? 2 : 4); }
+
+static int encode_3d(Ctx *c, CUtensorMap *tm, void *base, uint64_t d0, uint64_t d1, uint64_t d2,
+                     uint64_t stride1, uint64_t stride2, uint32_t b0, uint32_t b1, uint32_t b2) {
+  auto fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(c->encode_tiled);
+  if (!fn) return ctx_fail(c, ST_CUDA, "cuTensorMapEncodeTiled unavailable");
+  cuuint64_t dims[3] = {d0, d1, d2};
+  cuuint64_t strides[2] = {stride1, stride2};
+  cuuint32_t box[3] = {b0, b1, b2};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = fn(tm, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, base, dims, strides, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    char msg[160];
+    snprintf(msg, sizeof msg, "cuTensorMapEncodeTiled failed (%d) dims %llu %llu %llu", (int)r,
+             (unsigned long long)d0, (unsigned long long)d1, (unsigned long long)d2);
+    return ctx_fail(c, ST_CUDA, msg);
+  }
+  return ST_OK;
+}
+
+template <int L>
+static int launch_tc(Ctx *c, int M, int N, int K, const Modulus &mod, uint32_t alpha,
+                     const uint32_t *A, size_t lda, const uint32_t *B, size_t ldb, uint32_t beta,
+                     uint32_t *C, size_t ldc, uint8_t *ws) {
+  using Cfg = TcCfg<L>;
+  using Lay = TcLayout<L>;
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaError_t e = cudaFuncSetAttribute(zp_gemm_tc_kernel<L>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, Lay::SMEM);
+    if (e != cudaSuccess) return ctx_cuda(c, e, "cudaFuncSetAttribute(zp_gemm_tc)");
+    attr_set = true;
+  }
+  const int tiles = ((M + BM - 1) / BM) * ((N + Cfg::BN - 1) / Cfg::BN);
+  uint32_t b = beta;
+  for (int k0 = 0; k0 < K; k0 += ZP_KCHUNK) {
+    const int kc = std::min(ZP_KCHUNK, K - k0);
+    const int Kp = (kc + 15) & ~15;
+    uint8_t *Al = ws;
+    uint8_t *Bl = ws + (size_t)L * M * Kp;
+    {
+      const size_t total = (size_t)M * ((kc + 3) / 4);
+      int grid = (int)std::min<size_t>((total + 255) / 256, (size_t)c->num_sms * 16);
+      int pi = prof_begin(c, "zp_split");
+      split_rows_kernel<L><<<grid, 256, 0, c->stream>>>(A + k0, lda, M, kc, Al, Kp);
+      dim3 grid2((N + 31) / 32, (Kp + 63) / 64);
+      split_cols_kernel<L><<<grid2, 256, 0, c->stream>>>(B + (size_t)k0 * ldb, ldb, kc, N, Bl, Kp);
+      prof_end(c, pi);
+      ctx_launched(c, 2);
+    }
+    CUtensorMap tmA, tmB;
+    int st = encode_3d(c, &tmA, Al, (uint64_t)kc, (uint64_t)M, L, (uint64_t)Kp,
+                       (uint64_t)M * Kp, BK, BM, L);
+    if (st) return st;
+    st = encode_3d(c, &tmB, Bl, (uint64_t)kc, (uint64_t)N, L, (uint64_t)Kp, (uint64_t)N * Kp, BK,
+                   Cfg::BN, L);
+    if (st) return st;
+    const int grid = std::min(tiles, c->num_sms);
+    int pi = prof_begin(c, "zp_gemm_tc");
+    zp_gemm_tc_kernel<L><<<grid, 192, Lay::SMEM, c->stream>>>(tmA, tmB, C, ldc, M, N, kc, mod,
+                                                              alpha, b, c->dstatus);
+    prof_end(c, pi);
+    ctx_launched(c);
+    b = 1;
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return ctx_cuda(c, e, "zp_gemm_tc launch");
+  return ST_OK;
+}
+
+size_t zp_gemm_workspace_bytes(uint32_t p, int M, int N, int K) {
+  const int L = zp_limbs_for(p);
+  const int kc = std::min(ZP_KCHUNK, K);
+  const size_t Kp = (size_t)((kc + 15) & ~15);
+  return (size_t)L * ((size_t)M + N) * Kp + 256;
+}
+
+int zp_gemm_dev(Ctx *c, int kernel, int M, int N, int K, uint32_t p, uint32_t alpha,
+                const uint32_t *A, size_t lda, const uint32_t *B, size_t ldb, uint32_t beta,
+                uint32_t *C, size_t ldc, uint8_t *ws_override) {
+  if (p < 2) return ctx_fail(c, ST_ARG, "modulus must be at least 2");
+  if (M < 0 || N < 0 || K < 0) return ctx_fail(c, ST_ARG, "negative dimension");
+  if (M == 0 || N == 0) return ST_OK;
+  if (ldc < (size_t)N || (K > 0 && (lda < (size_t)K || ldb < (size_t)N)))
+    return ctx_fail(c, ST_ARG, "leading dimension smaller than the row length");
+  const Modulus mod = make_modulus(p);
+  alpha %= p;
+  beta %= p;
+  if (K == 0 || alpha == 0) {
+    if (beta == 1) return ST_OK;
+    const size_t total = (size_t)M * N;
+    int grid = (int)std::min<size_t>((total + 255) / 256, (size_t)c->num_sms * 8);
+    zp_scale_kernel<<<grid, 256, 0, c->stream>>>(C, ldc, M, N, mod, beta);
+    ctx_launched(c);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? ST_OK : ctx_cuda(c, e, "zp_scale launch");
+  }
+  if (kernel == GEMM_AUTO) kernel = c->gemm_kernel == GEMM_AUTO ? GEMM_TC : c->gemm_kernel;
+  if (kernel == GEMM_PLAIN) {
+    dim3 grid((N + PT - 1) / PT, (M + PT - 1) / PT);
+    int pi = prof_begin(c, "zp_gemm_plain");
+    zp_gemm_plain_kernel<<<grid, 256, 0, c->stream>>>(A, lda, B, ldb, C, ldc, M, N, K, mod,
+                                                      host_two64(p), alpha, beta);
+    prof_end(c, pi);
+    ctx_launched(c);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? ST_OK : ctx_cuda(c, e, "zp_gemm_plain launch");
+  }
+  uint8_t *ws = ws_override;
+  if (!ws) {
+    void *w = nullptr;
+    int st = ctx_workspace(c, zp_gemm_workspace_bytes(p, M, N, K), &w);
+    if (st) return st;
+    ws = static_cast<uint8_t *>(w);
+  }
+  switch (zp_limbs_for(p)) {
+    case 1: return launch_tc<1>(c, M, N, K, mod, alpha, A, lda, B, ldb, beta, C, ldc, ws);
+    case 2: return launch_tc<2>(c, M, N, K, mod, alpha, A, lda, B, ldb, beta, C, ldc, ws);
+    default: return launch_tc<4>(c, M, N, K, mod, alpha, A, lda, B, ldb, beta, C, ldc, ws);
+  }
+}
+
+}  // namespace lela

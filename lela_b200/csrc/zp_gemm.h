@@ -1,0 +1,24 @@
+// lela_b200/csrc/zp_gemm.h -- dense Z/p gemm entry points (device pointers).
+#pragma once
+#include <cstddef>
+#include <cstdint>
+
+#include "context.h"
+
+namespace lela {
+
+// Largest K handled by one tensor-core launch: 32768 * 255^2 < 2^31.
+constexpr int ZP_KCHUNK = 32768;
+
+int zp_limbs_for(uint32_t p);
+size_t zp_gemm_workspace_bytes(uint32_t p, int M, int N, int K);
+
+// C <- alpha*A*B + beta*C mod p on the handle's stream (asynchronous).
+// kernel: GEMM_AUTO, GEMM_PLAIN or GEMM_TC.  ws_override, when non-null,
+// is used instead of the handle workspace for the limb planes and must hold
+// zp_gemm_workspace_bytes(p, M, N, K) bytes.
+int zp_gemm_dev(Ctx *c, int kernel, int M, int N, int K, uint32_t p, uint32_t alpha,
+                const uint32_t *A, size_t lda, const uint32_t *B, size_t ldb, uint32_t beta,
+                uint32_t *C, size_t ldc, uint8_t *ws_override);
+
+}  // namespace lela

@@ -1,0 +1,51 @@
+"""The C ABI library loads and exports every function include/*.h declares
+(no GPU needed: nothing is called that touches the device)."""
+import ctypes
+import glob
+import os
+import re
+
+import pytest
+
+from lela_b200 import api
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    names = set()
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        src = open(h).read()
+        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        for m in re.finditer(r"\b(lela_cuda_[a-z0-9_]+)\s*\(", src):
+            names.add(m.group(1))
+    return sorted(names)
+
+
+def test_header_declares_entry_points():
+    names = declared_functions()
+    assert "lela_cuda_gemm_zp_u32" in names
+    assert "lela_cuda_create" in names
+
+
+def test_library_exports_every_declared_symbol():
+    lib = api.load_library()
+    missing = [n for n in declared_functions() if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_status_strings():
+    lib = api.load_library()
+    lib.lela_cuda_status_string.restype = ctypes.c_char_p
+    assert lib.lela_cuda_status_string(0) == b"ok"
+    assert lib.lela_cuda_status_string(4) == b"diagonal entry not invertible"
+
+
+def test_create_without_device_fails_cleanly():
+    """No GPU in this container: creation must fail with a status, not
+    crash, and the Python layer must raise (no CPU fallback)."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(api.CudaError):
+        api.CudaModule(0)
