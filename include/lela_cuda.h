@@ -107,6 +107,29 @@ int lela_cuda_gemm_zp_u32_dev (lela_cuda_ctx *ctx, size_t m, size_t n, size_t k,
 			       uint32_t a, const uint32_t *A, size_t lda, const uint32_t *B,
 			       size_t ldb, uint32_t b, uint32_t *C, size_t ldc);
 
+/* The same tensor-core gemm for callers that cannot allocate device memory:
+ * code whose device memory is owned by someone else (a host framework's
+ * caching allocator, a fixed per-process budget) or that must not call
+ * cudaMalloc/cudaFree because they may synchronise the device.  No
+ * counterpart in the reference: LELA has no device code.
+ *
+ * A, B and C are DEVICE pointers on the current device; `stream` is a
+ * cudaStream_t (NULL = legacy default stream).  No handle is needed and
+ * nothing is allocated: the kernel's scratch (the 8-bit limb planes of A and
+ * B) lives in a fixed 64 MiB __device__ array inside the library, which
+ * every GPU that loads the library keeps until the process exits.
+ *  - Limit: L*(m+n)*round16(min(k,32768)) <= 64 MiB, with L = 1, 2 or 4
+ *    limbs for p <= 2^8, 2^16, 2^32 (m = n = k = 4096 fits at p = 65521);
+ *    larger problems return LELA_CUDA_ERR_ARG before any GPU work.
+ *  - The first call on a device sets up that device (looks up the array's
+ *    device address); make it before any stream capture.
+ *  - All calls share the array and it keeps the last call's contents; calls
+ *    whose GPU work overlaps (other streams or threads without ordering)
+ *    race on it.  The call synchronises `stream` before returning. */
+int lela_cuda_gemm_zp_u32_noalloc (size_t m, size_t n, size_t k, uint32_t p, uint32_t a,
+				   const uint32_t *A, size_t lda, const uint32_t *B, size_t ldb,
+				   uint32_t b, uint32_t *C, size_t ldc, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

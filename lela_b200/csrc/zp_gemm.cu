@@ -41,6 +41,7 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <mutex>
 
 #include "common.cuh"
 #include "context.h"
@@ -607,3 +608,183 @@ int zp_gemm_dev(Ctx *c, int kernel, int M, int N, int K, uint32_t p, uint32_t al
 }
 
 }  // namespace lela
+
+// ====================================================== no-allocation gemm
+//
+// lela_cuda_gemm_zp_u32_noalloc: the tensor-core Z/p gemm for callers that
+// cannot allocate device memory -- code running under a memory manager that
+// owns every device allocation (a host framework's caching allocator or a
+// fixed per-process memory budget), or latency-critical paths where
+// cudaMalloc/cudaFree, which may synchronise the device, are not allowed.
+// Such a caller passes device pointers for A, B and C; the limb planes the
+// kernel needs as scratch live in the fixed array below instead of a
+// handle's workspace, so this entry point calls no cudaMalloc, cudaFree or
+// other allocating routine and needs no handle.
+//
+// Limits and sharing:
+//  - the scratch is NOALLOC_PLANE_BYTES = 64 MiB of limb planes, enough for
+//    L * (m + n) * round16(min(k, 32768)) bytes, L = 1, 2 or 4 limbs for
+//    p <= 2^8, 2^16, 2^32 (e.g. m = n = k = 4096 at p = 65521); larger
+//    problems are rejected with LELA_CUDA_ERR_ARG before any GPU work;
+//  - the array is a file-scope __device__ variable: every GPU that loads
+//    this library holds it (plus 256 bytes of status) until the process
+//    exits;
+//  - all calls on a device share it and it keeps the last call's contents.
+//    Each call writes every scratch byte its kernel reads (the K tail of a
+//    row is never read: the TMA descriptors stop at k) and clears its
+//    status word first, so nothing else must start at zero.  Calls whose
+//    GPU work overlaps (different streams or host threads without
+//    ordering) race on the scratch and give wrong results.
+//  - The first call on a device does its set-up there, with that device
+//    current: it looks up the array's device address with
+//    cudaGetSymbolAddress and sets the kernels' shared-memory attribute.
+//    Make that first call before any stream capture.
+namespace lela {
+
+constexpr size_t NOALLOC_STATUS_BYTES = 256;
+constexpr size_t NOALLOC_PLANE_BYTES = (size_t)64 << 20;
+static __device__ __align__(256) uint8_t g_noalloc_scratch[NOALLOC_STATUS_BYTES + NOALLOC_PLANE_BYTES];
+
+namespace {
+
+constexpr int NOALLOC_MAX_DEVICES = 64;
+struct NoallocDevice {
+  bool ready;
+  uint8_t *base;  // device address of g_noalloc_scratch on this device
+  int num_sms;
+};
+NoallocDevice g_noalloc_dev[NOALLOC_MAX_DEVICES];
+std::mutex g_noalloc_mu;
+PFN_cuTensorMapEncodeTiled_v12000 g_noalloc_encode = nullptr;
+
+// Once per device, with that device current.
+int noalloc_setup(int dev, NoallocDevice *out) {
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return ST_ARG;
+  NoallocDevice &d = g_noalloc_dev[dev];
+  if (!d.ready) {
+    void *ptr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+    if (e != cudaSuccess || ptr == nullptr) return ST_CUDA;
+    int sms = 0;
+    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return ST_CUDA;
+    e = cudaFuncSetAttribute(zp_gemm_tc_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             TcLayout<1>::SMEM);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(zp_gemm_tc_kernel<2>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, TcLayout<2>::SMEM);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(zp_gemm_tc_kernel<4>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, TcLayout<4>::SMEM);
+    if (e != cudaSuccess) return ST_CUDA;
+    if (!g_noalloc_encode) {
+      void *fn = nullptr;
+      cudaDriverEntryPointQueryResult q;
+      e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q);
+      if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !fn) return ST_CUDA;
+      g_noalloc_encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }
+    d.base = static_cast<uint8_t *>(ptr);
+    d.num_sms = sms;
+    d.ready = true;
+  }
+  *out = d;
+  return ST_OK;
+}
+
+bool noalloc_map(CUtensorMap *tm, void *base, uint64_t d0, uint64_t d1, uint64_t d2,
+                 uint64_t stride1, uint64_t stride2, uint32_t b0, uint32_t b1, uint32_t b2) {
+  cuuint64_t dims[3] = {d0, d1, d2};
+  cuuint64_t strides[2] = {stride1, stride2};
+  cuuint32_t box[3] = {b0, b1, b2};
+  cuuint32_t estr[3] = {1, 1, 1};
+  return g_noalloc_encode(tm, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, base, dims, strides, box, estr,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <int L>
+int noalloc_launch(cudaStream_t s, const NoallocDevice &d, int M, int N, int K,
+                   const Modulus &mod, uint32_t alpha, const uint32_t *A, size_t lda,
+                   const uint32_t *B, size_t ldb, uint32_t beta, uint32_t *C, size_t ldc) {
+  using Cfg = TcCfg<L>;
+  using Lay = TcLayout<L>;
+  uint32_t *err = reinterpret_cast<uint32_t *>(d.base);
+  uint8_t *planes = d.base + NOALLOC_STATUS_BYTES;
+  const int tiles = ((M + BM - 1) / BM) * ((N + Cfg::BN - 1) / Cfg::BN);
+  uint32_t b = beta;
+  for (int k0 = 0; k0 < K; k0 += ZP_KCHUNK) {
+    const int kc = std::min(ZP_KCHUNK, K - k0);
+    const int Kp = (kc + 15) & ~15;
+    uint8_t *Al = planes;
+    uint8_t *Bl = planes + (size_t)L * M * Kp;
+    const size_t total = (size_t)M * ((kc + 3) / 4);
+    int grid = (int)std::min<size_t>((total + 255) / 256, (size_t)d.num_sms * 16);
+    split_rows_kernel<L><<<grid, 256, 0, s>>>(A + k0, lda, M, kc, Al, Kp);
+    dim3 grid2((N + 31) / 32, (Kp + 63) / 64);
+    split_cols_kernel<L><<<grid2, 256, 0, s>>>(B + (size_t)k0 * ldb, ldb, kc, N, Bl, Kp);
+    CUtensorMap tmA, tmB;
+    if (!noalloc_map(&tmA, Al, (uint64_t)kc, (uint64_t)M, L, (uint64_t)Kp, (uint64_t)M * Kp,
+                     BK, BM, L) ||
+        !noalloc_map(&tmB, Bl, (uint64_t)kc, (uint64_t)N, L, (uint64_t)Kp, (uint64_t)N * Kp,
+                     BK, Cfg::BN, L))
+      return ST_CUDA;
+    zp_gemm_tc_kernel<L><<<std::min(tiles, d.num_sms), 192, Lay::SMEM, s>>>(
+        tmA, tmB, C, ldc, M, N, kc, mod, alpha, b, err);
+    b = 1;
+  }
+  return cudaGetLastError() == cudaSuccess ? ST_OK : ST_CUDA;
+}
+
+}  // namespace
+
+}  // namespace lela
+
+extern "C" int lela_cuda_gemm_zp_u32_noalloc(size_t m, size_t n, size_t k, uint32_t p,
+                                             uint32_t a, const uint32_t *A, size_t lda,
+                                             const uint32_t *B, size_t ldb, uint32_t b,
+                                             uint32_t *C, size_t ldc, void *stream) {
+  using namespace lela;
+  if (p < 2) return ST_ARG;
+  if (m > (size_t)INT32_MAX || n > (size_t)INT32_MAX || k > (size_t)INT32_MAX) return ST_ARG;
+  if (m == 0 || n == 0) return ST_OK;
+  if (!C || (k && (!A || !B))) return ST_ARG;
+  if (ldc < n || (k && (lda < k || ldb < n))) return ST_ARG;
+  const int L = zp_limbs_for(p);
+  const size_t kc = std::min<size_t>(k, (size_t)ZP_KCHUNK);
+  const size_t need = (size_t)L * (m + n) * ((kc + 15) & ~(size_t)15);
+  if (need > NOALLOC_PLANE_BYTES) return ST_ARG;  // beyond the fixed scratch
+
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return ST_CUDA;
+  NoallocDevice d;
+  int st = noalloc_setup(dev, &d);
+  if (st) return st;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const Modulus mod = make_modulus(p);
+  a %= p;
+  b %= p;
+  if (cudaMemsetAsync(d.base, 0, sizeof(uint32_t), s) != cudaSuccess) return ST_CUDA;
+  if (k == 0 || a == 0) {
+    if (b != 1) {
+      const size_t total = m * n;
+      int grid = (int)std::min<size_t>((total + 255) / 256, (size_t)d.num_sms * 8);
+      zp_scale_kernel<<<grid, 256, 0, s>>>(C, ldc, (int)m, (int)n, mod, b);
+      if (cudaGetLastError() != cudaSuccess) return ST_CUDA;
+    }
+  } else {
+    switch (L) {
+      case 1: st = noalloc_launch<1>(s, d, (int)m, (int)n, (int)k, mod, a, A, lda, B, ldb, b, C, ldc); break;
+      case 2: st = noalloc_launch<2>(s, d, (int)m, (int)n, (int)k, mod, a, A, lda, B, ldb, b, C, ldc); break;
+      default: st = noalloc_launch<4>(s, d, (int)m, (int)n, (int)k, mod, a, A, lda, B, ldb, b, C, ldc); break;
+    }
+    if (st) return st;
+  }
+  uint32_t word = 0;
+  if (cudaMemcpyAsync(&word, d.base, sizeof word, cudaMemcpyDeviceToHost, s) != cudaSuccess)
+    return ST_CUDA;
+  if (cudaStreamSynchronize(s) != cudaSuccess) return ST_CUDA;
+  return (word & DEVERR_TIMEOUT) ? ST_TIMEOUT : ST_OK;
+}
