@@ -179,7 +179,8 @@ def ref_echelon_zp(p, A, classical=False):
     m, n = A.shape
     r = _S(0); d = _U(0)
     fn = ref().lela_ref_elim_echelon_zp_u32 if classical else ref().lela_ref_echelon_zp_u32
-    fn(p, m, n, _ptr(A), n, ctypes.byref(r), ctypes.byref(d))
+    if fn(p, m, n, _ptr(A), n, ctypes.byref(r), ctypes.byref(d)):
+        raise ArithmeticError("pivot not invertible")
     return A, r.value, d.value
 
 

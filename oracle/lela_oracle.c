@@ -49,21 +49,41 @@ static uint32_t axpy_mod (uint32_t p, uint32_t r, uint32_t a, uint32_t x)
 	return (uint32_t) (((uint64_t) a * x + r) % p);
 }
 
-/* Modular::inv by the extended Euclidean algorithm (lela/ring/modular.h:
- * 460-474, 540-557).  Returns 0 when gcd(x, p) != 1. */
+/* Modular<uint32>::eea (lela/ring/modular.h:540-557) in its EEAElement
+ * type, which is a 32-bit int for uint32 elements (modular.h:210): every
+ * intermediate wraps modulo 2^32 exactly as the reference's arithmetic does.
+ * For p < 2^31 this is the textbook extended Euclidean algorithm; for
+ * p >= 2^31 the modulus itself wraps negative and the reference's inverse
+ * fails (or returns what the wrapped arithmetic yields), and so does this. */
+static void eea32 (int32_t *gcd, int32_t *a, int32_t x, int32_t *b, int32_t y)
+{
+	if (y == 0) {
+		*gcd = x; *a = 1; *b = 0;
+	} else {
+		int32_t q, r;
+		if (y == -1) { q = (int32_t) (0u - (uint32_t) x); r = 0; }
+		else { q = x / y; r = x % y; }
+		eea32 (gcd, b, y, a, r);
+		*b = (int32_t) ((uint32_t) *b - (uint32_t) q * (uint32_t) *a);
+	}
+}
+
+/* Modular<uint32>::inv (lela/ring/modular.h:460-474): eea on (y, p) as
+ * 32-bit ints; on gcd == 1 the coefficient is shifted up by p if negative
+ * (shift_up, :228-229), converted to uint32 and shifted down once if >= p
+ * (shift_down, :230-232).  Returns 0 when the reference reports failure. */
 uint32_t oracle_inv_zp (uint32_t p, uint32_t x)
 {
-	int64_t r0 = p, r1 = x % p, s0 = 0, s1 = 1;
-	while (r1 != 0) {
-		int64_t q = r0 / r1, t;
-		t = r0 - q * r1; r0 = r1; r1 = t;
-		t = s0 - q * s1; s0 = s1; s1 = t;
-	}
-	if (r0 != 1)
+	int32_t gcd, ty, tm;
+	eea32 (&gcd, &ty, (int32_t) x, &tm, (int32_t) p);
+	if (gcd != 1)
 		return 0;
-	s0 %= (int64_t) p;
-	if (s0 < 0) s0 += p;
-	return (uint32_t) s0;
+	if (ty < 0)
+		ty = (int32_t) ((uint32_t) ty + p);
+	uint32_t r = (uint32_t) ty;
+	if ((uint64_t) r >= (uint64_t) p)
+		r -= p;
+	return r;
 }
 
 /* Generic gemm, Row x Col case (lela/blas/level3-generic.tcc:285-322): one

@@ -260,7 +260,11 @@ int lela_ref_elim_echelon_zp_u32 (uint32_t p, size_t m, size_t n, uint32_t *A, s
 	Elimination<Zp>::Permutation P;
 	size_t r = 0;
 	Zp::Element d;
-	elim.echelonize (MA, P, r, d, DensePivotStrategy<Zp, AllModules<Zp> > (ctx), false);
+	try {
+		elim.echelonize (MA, P, r, d, DensePivotStrategy<Zp, AllModules<Zp> > (ctx), false);
+	} catch (...) {
+		return -1;
+	}
 	if (m && n) store_dense (MA, A, lda);
 	*rank = r;
 	*det = d;

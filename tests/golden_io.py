@@ -1,0 +1,69 @@
+"""Access to the committed golden fixtures (tests/golden/lela_golden.*),
+computed by LELA's own CPU code (tests/golden/make_golden.py)."""
+import hashlib
+import json
+import os
+
+import numpy as np
+
+HERE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+_cache = {}
+
+
+def data():
+    if "npz" not in _cache:
+        _cache["npz"] = dict(np.load(os.path.join(HERE, "lela_golden.npz")))
+        _cache["json"] = json.load(open(os.path.join(HERE, "lela_golden.json")))
+    return _cache["npz"], _cache["json"]
+
+
+def sha(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def gemm_cases():
+    z, man = data()
+    for pre in man["gemm_small"]:
+        p, a, b = (int(x) for x in z[pre + "meta"])
+        yield pre, p, a, b, z[pre + "A"], z[pre + "B"], z[pre + "C"], z[pre + "R"]
+
+
+def trsm_cases():
+    z, man = data()
+    for pre in man["trsm"]:
+        p, upper, unit, a, bad = (int(x) for x in z[pre + "meta"])
+        yield pre, p, upper, unit, a, (None if bad < 0 else bad), z[pre + "A"], z[pre + "B"], z[pre + "R"]
+
+
+def echelon_cases():
+    z, man = data()
+    for pre in man["echelon"]:
+        p, st, r, d = (int(x) for x in z[pre + "meta"])
+        yield pre, p, st, r, d, z[pre + "A"], z[pre + "E"]
+
+
+def fl_cases(with_inputs_only=True):
+    """Faugere-Lachartre cases whose inputs are stored (the reference test's
+    matrix family)."""
+    z, man = data()
+    for pre in man["fl"]:
+        meta = [int(x) for x in z[pre + "meta"]]
+        if pre + "rowptr" not in z:
+            continue
+        p, m, n, red, od, st, rank, det = meta
+        yield (pre, p, m, n, red, od, st, rank, det, z[pre + "rowptr"], z[pre + "colidx"],
+               z[pre + "vals"], z[pre + "R"])
+
+
+def gf2_gemm_cases():
+    z, man = data()
+    for pre in man["gf2_gemm"]:
+        m, n, k = (int(x) for x in z[pre + "meta"])
+        yield pre, m, n, k, z[pre + "A"], z[pre + "B"], z[pre + "C"], z[pre + "R"]
+
+
+def gf2_echelon_cases():
+    z, man = data()
+    for pre in man["gf2_echelon"]:
+        m, n, r = (int(x) for x in z[pre + "meta"])
+        yield pre, m, n, r, z[pre + "A"], z[pre + "E"]

@@ -1,0 +1,218 @@
+"""Pinning the CPU oracle (the C restatement in oracle/lela_oracle.c):
+(1) against the golden fixtures computed by LELA's own code, committed under
+tests/golden/; (2) against LELA's own code live, where oracle/_ref was built
+(randomised cases, including the error paths).  No GPU needed."""
+import numpy as np
+import pytest
+
+import golden_io
+import oracle
+import props
+from lela_b200 import gen
+
+need_ref = pytest.mark.skipif(not oracle.have_ref(), reason="oracle/_ref (LELA's CPU code) not built")
+
+
+def test_golden_gemm_small():
+    for pre, p, a, b, A, B, C, R in golden_io.gemm_cases():
+        assert np.array_equal(oracle.gemm_zp(p, A, B, C, a, b), R), pre
+
+
+def test_golden_gemm_512():
+    g = golden_io.data()[1]["gemm512"]
+    p, n = g["p"], g["n"]
+    A = gen.dense_zp(g["seeds"][0], n, n, p)
+    B = gen.dense_zp(g["seeds"][1], n, n, p)
+    C = gen.dense_zp(g["seeds"][2], n, n, p)
+    assert golden_io.sha(A) == g["A"] and golden_io.sha(B) == g["B"] and golden_io.sha(C) == g["C"], \
+        "input generator drifted"
+    R = oracle.gemm_zp(p, A, B, C, 1, 1, threads=8)
+    assert golden_io.sha(R) == g["R"]
+
+
+def test_golden_trsm():
+    for pre, p, upper, unit, a, bad, A, B, R in golden_io.trsm_cases():
+        got, gbad = oracle.trsm_zp(p, A, B, upper, unit, a)
+        assert gbad == bad, pre
+        if bad is None:
+            assert np.array_equal(got, R), pre
+
+
+def test_golden_echelon():
+    for pre, p, st, r, d, A, E in golden_io.echelon_cases():
+        if st:
+            with pytest.raises(ArithmeticError):
+                oracle.echelon_zp(p, A)
+            continue
+        got, gr, gd = oracle.echelon_zp(p, A)
+        assert (gr, gd) == (r, d), pre
+        assert np.array_equal(got, E), pre
+
+
+def test_golden_fl():
+    for (pre, p, m, n, red, od, st, rank, det, rowptr, colidx, vals, R) in golden_io.fl_cases():
+        got = oracle.fl_echelonize_zp(p, m, n, rowptr, colidx, vals, red, od)
+        assert got["status"] == st, pre
+        assert (got["rank"], got["det"]) == (rank, det), pre
+        assert np.array_equal(got["R"], R), pre
+
+
+def test_golden_fl_f4_digest():
+    z, man = golden_io.data()
+    X = gen.f4_matrix(7, 300, 65521, density=0.03)
+    for pre in man["fl"]:
+        if pre + "R_sha" not in man:
+            continue
+        assert golden_io.sha(np.concatenate([X.rowptr.view(np.uint32), X.colidx, X.vals])) == man[pre + "X_sha"]
+        _, _, _, red, od, st, rank, det = (int(x) for x in z[pre + "meta"])
+        got = oracle.fl_echelonize_zp(65521, X.m, X.n, X.rowptr, X.colidx, X.vals, red, od)
+        assert (got["status"], got["rank"], got["det"]) == (st, rank, det), pre
+        assert golden_io.sha(got["R"]) == man[pre + "R_sha"], pre
+
+
+def test_golden_gf2():
+    for pre, m, n, k, A, B, C, R in golden_io.gf2_gemm_cases():
+        assert np.array_equal(oracle.gemm_gf2(A, B, C, k, n, 1, 1), R), pre
+    for pre, m, n, r, A, E in golden_io.gf2_echelon_cases():
+        got, gr = oracle.echelon_gf2(A, n)
+        assert gr == r and np.array_equal(got, E), pre
+
+
+def test_freivalds_catches_planted_error():
+    """The property check used at full size rejects a result with one wrong
+    entry (the mistake is planted in the oracle's own output, on the CPU)."""
+    p = 65521
+    A = gen.dense_zp(1, 64, 80, p); B = gen.dense_zp(2, 80, 50, p); C0 = gen.dense_zp(3, 64, 50, p)
+    C = oracle.gemm_zp(p, A, B, C0, 1, 1)
+    assert props.freivalds_gemm(p, A, B, C0, C, 1, 1)
+    C[5, 7] = (C[5, 7] + 1) % p
+    assert not props.freivalds_gemm(p, A, B, C0, C, 1, 1)
+
+
+# ------------------------------------------------- live against LELA's code
+
+@need_ref
+@pytest.mark.parametrize("seed", range(4))
+def test_live_gemm(seed):
+    rng = np.random.default_rng(seed)
+    for p in (251, 65521, 2147483647, 4294967291):
+        m, n, k = (int(x) for x in rng.integers(1, 60, size=3))
+        a, b = int(rng.integers(0, p)), int(rng.integers(0, p))
+        A = gen.dense_zp(seed, m, k, p); B = gen.dense_zp(seed + 1, k, n, p); C = gen.dense_zp(seed + 2, m, n, p)
+        assert np.array_equal(oracle.gemm_zp(p, A, B, C, a, b), oracle.ref_gemm_zp(p, A, B, C, a, b))
+
+
+@need_ref
+@pytest.mark.parametrize("seed", range(4))
+def test_live_trsm(seed):
+    rng = np.random.default_rng(100 + seed)
+    for upper in (0, 1):
+        for unit in (0, 1):
+            p = int(rng.choice([251, 65521, 2147483647]))
+            m, n = int(rng.integers(1, 70)), int(rng.integers(1, 20))
+            U = gen.upper_zp(seed, m, p, unit=bool(unit))
+            if not unit and m > 3 and seed % 2:
+                U[m // 3, m // 3] = 0
+            A = U if upper else np.ascontiguousarray(U.T)
+            B = gen.dense_zp(seed + 5, m, n, p)
+            a = int(rng.integers(0, p))
+            r1, b1 = oracle.trsm_zp(p, A, B, upper, unit, a)
+            r2, b2 = oracle.ref_trsm_zp(p, A, B, upper, unit, a)
+            assert b1 == b2
+            if b1 is None:
+                assert np.array_equal(r1, r2)
+
+
+def test_inverse_matches_lela_int_arithmetic():
+    """Modular<uint32>::inv runs its Euclid in 32-bit ints: exact inverses
+    below 2^31, and for p >= 2^31 the reference's wrapped result (here:
+    failure for every tested unit)."""
+    for p in (3, 251, 65521, 2147483647):
+        for x in (1, 2, p - 1, 12345 % p or 1):
+            y = oracle.inv_zp(p, x)
+            assert y and (x * y) % p == 1
+        assert oracle.inv_zp(p, 0) == 0
+    assert oracle.inv_zp(65536, 2) == 0
+
+
+@need_ref
+def test_live_inverse_large_modulus():
+    """p >= 2^31: whether LELA can invert a pivot decides whether the
+    echelon form succeeds; the restatement must agree case by case."""
+    for p in (2147483659, 4294967291):
+        for seed in range(3):
+            A = gen.dense_zp(seed, 6, 5, p)
+            try:
+                e2 = oracle.ref_echelon_zp(p, A, classical=True)
+            except ArithmeticError:
+                e2 = None
+            try:
+                e1 = oracle.echelon_zp(p, A)
+            except ArithmeticError:
+                e1 = None
+            assert (e1 is None) == (e2 is None)
+            if e1 is not None:
+                assert np.array_equal(e1[0], e2[0]) and e1[1:] == e2[1:]
+
+
+@need_ref
+@pytest.mark.parametrize("seed", range(4))
+def test_live_echelon(seed):
+    p = [65521, 251, 2147483647, 3][seed]
+    A = gen.dense_zp(seed, 45, 38, p)
+    A[:, 5] = 0
+    A[30:] = (A[:15] * 7) % p
+    e1, r1, d1 = oracle.echelon_zp(p, A)
+    e2, r2, d2 = oracle.ref_echelon_zp(p, A)
+    e3, r3, d3 = oracle.ref_echelon_zp(p, A, classical=True)
+    assert np.array_equal(e1, e2) and np.array_equal(e1, e3)
+    assert (r1, d1) == (r2, d2) == (r3, d3)
+
+
+@need_ref
+@pytest.mark.parametrize("seed", range(6))
+def test_live_fl(seed):
+    p = 65521
+    X = gen.f4_matrix_small(50 + seed, 50 + 10 * seed, 60 + 13 * seed, p, 0.08 + 0.02 * seed)
+    for red, od in ((1, 0), (0, 0), (1, 1), (0, 1)):
+        a = oracle.fl_echelonize_zp(p, X.m, X.n, X.rowptr, X.colidx, X.vals, red, od)
+        b = oracle.ref_fl_echelonize_zp(p, X.m, X.n, X.rowptr, X.colidx, X.vals, red, od)
+        assert (a["status"], a["rank"], a["det"]) == (b["status"], b["rank"], b["det"])
+        assert np.array_equal(a["R"], b["R"])
+
+
+@need_ref
+def test_live_fl_wrong_form():
+    """A row whose head lies left of the previous pivot: WrongMatrixForm."""
+    p = 65521
+    D = np.zeros((4, 6), dtype=np.uint32)
+    D[0, 1] = 1; D[1, 3] = 1; D[2, 2] = 5; D[3, 4] = 1
+    X = gen.CSR.from_dense(D)
+    a = oracle.fl_echelonize_zp(p, X.m, X.n, X.rowptr, X.colidx, X.vals, 1, 0)
+    b = oracle.ref_fl_echelonize_zp(p, X.m, X.n, X.rowptr, X.colidx, X.vals, 1, 0)
+    assert a["status"] == b["status"] == 1
+    assert a["bad_row"] == 2
+
+
+@need_ref
+def test_live_fl_f4_shaped():
+    p = 65521
+    X = gen.f4_matrix(3, 400, p, density=0.02)
+    a = oracle.fl_echelonize_zp(p, X.m, X.n, X.rowptr, X.colidx, X.vals, 1, 0)
+    b = oracle.ref_fl_echelonize_zp(p, X.m, X.n, X.rowptr, X.colidx, X.vals, 1, 0)
+    assert (a["rank"], a["det"]) == (b["rank"], b["det"])
+    assert np.array_equal(a["R"], b["R"])
+    assert a["rank"] < X.m     # the planted dependencies lower the rank
+
+
+@need_ref
+@pytest.mark.parametrize("seed", range(3))
+def test_live_gf2(seed):
+    m, n, k = 40 + seed * 30, 70 + seed * 40, 65 + seed * 20
+    A = gen.dense_gf2(seed, m, k); B = gen.dense_gf2(seed + 1, k, n); C = gen.dense_gf2(seed + 2, m, n)
+    for a, b in ((1, 1), (1, 0), (0, 1)):
+        assert np.array_equal(oracle.gemm_gf2(A, B, C, k, n, a, b), oracle.ref_gemm_gf2(A, B, C, k, n, a, b))
+    E = gen.planted_rank_gf2(seed, m, n, min(m, n) // 2)
+    e1, r1 = oracle.echelon_gf2(E, n)
+    e2, r2 = oracle.ref_echelon_gf2(E, n)
+    assert r1 == r2 and np.array_equal(e1, e2)
