@@ -107,6 +107,23 @@ int lela_cuda_gemm_zp_u32_dev (lela_cuda_ctx *ctx, size_t m, size_t n, size_t k,
 			       uint32_t a, const uint32_t *A, size_t lda, const uint32_t *B,
 			       size_t ldb, uint32_t b, uint32_t *C, size_t ldc);
 
+/* ------------------------------------------------------------- Z/p trsm
+ * B <- a * A^-1 * B, A m x m upper (upper != 0) or lower triangular, unit
+ * diagonal when diag_is_one != 0, B m x n.
+ * Replaces BLAS3::trsm (lela/blas/level3.h:121) ->
+ * _trsm<Ring, GenericModule::Tag>::trsm_impl (lela/blas/level3-generic.tcc:
+ * 421-498) for dense operands.  Returns LELA_CUDA_DIAG_NOT_INVERTIBLE with
+ * *bad_idx = the index LELA's DiagonalEntryNotInvertible carries (smallest
+ * singular index for lower, largest for upper); B is then unchanged.
+ * With a = 0 the result is B = 0 and A is not inspected, as in LELA.
+ * The _dev form synchronises the stream once (diagonal check). */
+int lela_cuda_trsm_zp_u32 (lela_cuda_ctx *ctx, int upper, int diag_is_one, size_t m, size_t n,
+			   uint32_t p, uint32_t a, const uint32_t *A, size_t lda, uint32_t *B,
+			   size_t ldb, size_t *bad_idx);
+int lela_cuda_trsm_zp_u32_dev (lela_cuda_ctx *ctx, int upper, int diag_is_one, size_t m,
+			       size_t n, uint32_t p, uint32_t a, const uint32_t *A, size_t lda,
+			       uint32_t *B, size_t ldb, size_t *bad_idx);
+
 /* The same tensor-core gemm for callers that cannot allocate device memory:
  * code whose device memory is owned by someone else (a host framework's
  * caching allocator, a fixed per-process budget) or that must not call

@@ -235,6 +235,27 @@ class CudaModule:
         return C
 
 
+    # ---------------------------------------------------------- Z/p trsm
+    def trsm(self, p, a, A, B, upper, diag_is_one=False):
+        """B <- a*A^-1*B mod p in place (BLAS3::trsm with UpperTriangular /
+        LowerTriangular); raises DiagonalEntryNotInvertible(idx)."""
+        m = A.shape[0]
+        _check(A.shape == (m, m) and B.shape[0] == m, "trsm: dimension mismatch")
+        n = B.shape[1]
+        bad = _S(0)
+        if _is_torch(B):
+            st = self.L.lela_cuda_trsm_zp_u32_dev(self.h, int(upper), int(diag_is_one), m, n, p,
+                                                  a % p, _dptr(A), A.stride(0), _dptr(B), B.stride(0),
+                                                  ctypes.byref(bad))
+        else:
+            _check(A.dtype == np.uint32 and B.dtype == np.uint32, "trsm: uint32 matrices expected")
+            st = self.L.lela_cuda_trsm_zp_u32(self.h, int(upper), int(diag_is_one), m, n, p, a % p,
+                                              _ptr(A), A.strides[0] // 4, _ptr(B), B.strides[0] // 4,
+                                              ctypes.byref(bad))
+        self._raise(st, bad.value)
+        return B
+
+
 def _is_torch(x):
     return type(x).__module__.startswith("torch")
 

@@ -11,6 +11,7 @@
 #include "../../include/lela_cuda.h"
 #include "common.cuh"
 #include "context.h"
+#include "tri.h"
 #include "zp_gemm.h"
 
 struct lela_cuda_ctx {
@@ -61,6 +62,12 @@ int ctx_workspace(Ctx *c, size_t bytes, void **out) {
 int ctx_workspace2(Ctx *c, size_t bytes, void **out) {
   int st = grow(c, &c->ws2, &c->ws2_bytes, bytes, "cudaMalloc(workspace2)");
   *out = c->ws2;
+  return st;
+}
+
+int ctx_buffer(Ctx *c, int slot, size_t bytes, void **out) {
+  int st = grow(c, &c->buf[slot], &c->buf_bytes[slot], bytes, "cudaMalloc(buffer)");
+  *out = c->buf[slot];
   return st;
 }
 
@@ -165,6 +172,8 @@ int lela_cuda_destroy(lela_cuda_ctx *h) {
   if (c->ws2) cudaFree(c->ws2);
   for (int i = 0; i < 4; ++i)
     if (c->stage[i]) cudaFree(c->stage[i]);
+  for (int i = 0; i < 16; ++i)
+    if (c->buf[i]) cudaFree(c->buf[i]);
   if (c->dstatus) cudaFree(c->dstatus);
   if (c->hstatus) cudaFreeHost(c->hstatus);
   for (auto &r : c->prof) {
@@ -337,6 +346,42 @@ int lela_cuda_gemm_zp_u32(lela_cuda_ctx *h, size_t m, size_t n, size_t k, uint32
                      (const uint32_t *)dB, n, b, (uint32_t *)dC, n, nullptr);
   if (!st) st = d2h_matrix(c, C, dC, m, n, ldc, 4);
   if (!st) st = ctx_check_status(c, "gemm_zp_u32");
+  return st;
+}
+
+int lela_cuda_trsm_zp_u32_dev(lela_cuda_ctx *h, int upper, int diag_is_one, size_t m, size_t n,
+                              uint32_t p, uint32_t a, const uint32_t *A, size_t lda, uint32_t *B,
+                              size_t ldb, size_t *bad_idx) {
+  if (!h) return ST_ARG;
+  Ctx *c = &h->c;
+  if (m > (size_t)INT32_MAX || n > (size_t)INT32_MAX) return ctx_fail(c, ST_ARG, "dimension too large");
+  if (m && (!A || (n && !B))) return ctx_fail(c, ST_ARG, "null pointer");
+  return zp_trsm_dev(c, upper != 0, diag_is_one != 0, (int)m, (int)n, p, a, A, lda, B, ldb,
+                     bad_idx);
+}
+
+int lela_cuda_trsm_zp_u32(lela_cuda_ctx *h, int upper, int diag_is_one, size_t m, size_t n,
+                          uint32_t p, uint32_t a, const uint32_t *A, size_t lda, uint32_t *B,
+                          size_t ldb, size_t *bad_idx) {
+  if (!h) return ST_ARG;
+  Ctx *c = &h->c;
+  if (m > (size_t)INT32_MAX || n > (size_t)INT32_MAX) return ctx_fail(c, ST_ARG, "dimension too large");
+  if (p < 2) return ctx_fail(c, ST_ARG, "modulus must be at least 2");
+  if (m == 0) return ST_OK;
+  if (!A || (n && !B)) return ctx_fail(c, ST_ARG, "null pointer");
+  if (lda < m || (n && ldb < n)) return ctx_fail(c, ST_ARG, "leading dimension smaller than the row length");
+  cudaSetDevice(c->device);
+  void *dA = nullptr, *dB = nullptr;
+  int st = ctx_stage(c, 0, m * m * 4, &dA);
+  if (!st && n) st = ctx_stage(c, 1, m * n * 4, &dB);
+  if (!st) st = ctx_clear_status(c);
+  if (!st) st = h2d_matrix(c, dA, A, m, m, lda, 4);
+  if (!st && n) st = h2d_matrix(c, dB, B, m, n, ldb, 4);
+  if (!st)
+    st = zp_trsm_dev(c, upper != 0, diag_is_one != 0, (int)m, (int)n, p, a, (const uint32_t *)dA,
+                     m, (uint32_t *)dB, n, bad_idx);
+  if (!st && n) st = d2h_matrix(c, B, dB, m, n, ldb, 4);
+  if (!st) st = ctx_check_status(c, "trsm_zp_u32");
   return st;
 }
 

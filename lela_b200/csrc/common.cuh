@@ -64,6 +64,49 @@ __device__ __forceinline__ uint32_t mod_axpby(uint32_t a, uint32_t x, uint32_t b
   return (uint32_t)(u >= m.p ? u - m.p : u);
 }
 
+// Modular inverse with the semantics of Modular<uint32>::inv
+// (lela/ring/modular.h:460-474, eea at :540-557): the extended Euclidean
+// algorithm runs in 32-bit signed ints (ModularTraits<uint32>::EEAElement,
+// modular.h:210), so all coefficient arithmetic wraps modulo 2^32.  The
+// iterative form below yields the same Bezout coefficient modulo 2^32 as the
+// reference's recursion (both are ring operations on the same quotient
+// sequence).  Exact for p < 2^31; for p >= 2^31 it reproduces the reference's
+// wrapped result, normally a failure.  Returns 0 when the reference reports
+// "not invertible".
+__host__ __device__ inline uint32_t lela_inv_u32(uint32_t p, uint32_t x) {
+  int32_t r0 = (int32_t)x, r1 = (int32_t)p;
+  int32_t s0 = 1, s1 = 0;
+  while (r1 != 0) {
+    int32_t q, r;
+    if (r1 == -1) {
+      q = (int32_t)(0u - (uint32_t)r0);
+      r = 0;
+    } else {
+      q = r0 / r1;
+      r = r0 % r1;
+    }
+    r0 = r1;
+    r1 = r;
+    int32_t s = (int32_t)((uint32_t)s0 - (uint32_t)q * (uint32_t)s1);
+    s0 = s1;
+    s1 = s;
+  }
+  if (r0 != 1) return 0;
+  int32_t ty = s0;
+  if (ty < 0) ty = (int32_t)((uint32_t)ty + p);
+  uint32_t out = (uint32_t)ty;
+  if ((uint64_t)out >= (uint64_t)p) out -= p;
+  return out;
+}
+
+// 2^64 mod p (the delayed-reduction correction of ZpModule<uint32>,
+// lela/ring/modular.h:604-626).
+__host__ __device__ inline uint32_t two64_mod(uint32_t p) {
+  uint64_t t = 2;
+  for (int i = 0; i < 6; ++i) t = (t * t) % p;
+  return (uint32_t)t;
+}
+
 // ------------------------------------------------------ bounded waiting
 //
 // Every spin-wait in these kernels is bounded: after WAIT_LIMIT_NS of

@@ -45,6 +45,10 @@ struct Ctx {
   void *stage[4] = {nullptr, nullptr, nullptr, nullptr};
   size_t stage_bytes[4] = {0, 0, 0, 0};
 
+  // Named grow-only device buffers of the algorithms (see BufSlot).
+  void *buf[16] = {};
+  size_t buf_bytes[16] = {};
+
   int gemm_kernel = GEMM_AUTO;
   std::string last_error;
 
@@ -64,7 +68,26 @@ struct Ctx {
   void *encode_tiled = nullptr;
 };
 
+// Buffer slots owned by the algorithms.
+enum BufSlot : int {
+  BUF_DINV = 0,     // inverted diagonals (trsm)
+  BUF_ECH_0 = 1,    // echelon form: pivot bookkeeping
+  BUF_ECH_1 = 2,
+  BUF_FL_A = 3,     // Faugere-Lachartre blocks A, B, C, D
+  BUF_FL_B = 4,
+  BUF_FL_C = 5,
+  BUF_FL_D = 6,
+  BUF_FL_X = 7,     // device copy of the CSR input
+  BUF_FL_IDX = 8,   // row / column classification
+  BUF_FL_R = 9,     // output
+  BUF_FL_T = 10,    // temporaries
+  BUF_GF2_0 = 11,
+  BUF_GF2_1 = 12,
+  BUF_MISC = 13,
+};
+
 // Grow-only allocation helpers; return ST_OK or ST_NOMEM.
+int ctx_buffer(Ctx *c, int slot, size_t bytes, void **out);
 int ctx_workspace(Ctx *c, size_t bytes, void **out);
 int ctx_workspace2(Ctx *c, size_t bytes, void **out);
 int ctx_stage(Ctx *c, int slot, size_t bytes, void **out);

@@ -1,0 +1,221 @@
+// lela_b200/csrc/tri.cu -- triangular solves over Z/p (Modular<uint32>).
+//
+//   B <- alpha * A^-1 * B,  A m x m upper or lower triangular, unit or
+//   non-unit diagonal, B m x n.
+//
+// Replaces _trsm<Ring, GenericModule::Tag>::trsm_impl (lela/blas/
+// level3-generic.tcc:421-498) for dense operands.  The recursion is the
+// reference's (split at l ~ m/2; lower: solve A11, B2 <- alpha*B2 - A21*B1,
+// solve A22 with coefficient 1; upper: A22 first, then B1 <- alpha*B1 -
+// A12*B2, then A11), with the off-diagonal updates on the limb-split
+// tensor-core gemm and 64-row diagonal leaves solved on CUDA cores.
+//
+// Error behaviour.  With alpha = 0 the reference returns alpha*B = 0
+// without looking at A (:433-434); otherwise a diagonal entry that
+// Modular<uint32>::inv cannot invert throws DiagonalEntryNotInvertible(idx)
+// where idx is the first such entry in the recursion's visiting order: the
+// smallest index for lower, the largest for upper.  Here all diagonal
+// inverses are computed first (one kernel); on failure the same idx is
+// reported and B is left unchanged (the reference leaves it partially
+// solved, which callers such as Faugere-Lachartre discard).
+#include <algorithm>
+
+#include "common.cuh"
+#include "context.h"
+#include "tri.h"
+#include "zp_gemm.h"
+
+namespace lela {
+
+constexpr int TRI_NB = 64;
+
+// dinv[i] = inverse of A(i,i) (1 for a unit diagonal).  Failures record the
+// smallest (status[1]) and largest + 1 (status[2]) failing index.
+__global__ void diag_inverse_kernel(const uint32_t *__restrict__ A, size_t lda, int m, uint32_t p,
+                                    uint32_t *__restrict__ dinv, uint32_t *status) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+    uint32_t v = lela_inv_u32(p, A[(size_t)i * lda + i]);
+    dinv[i] = v;
+    if (v == 0) {
+      atomicMin(&status[1], (uint32_t)i);
+      atomicMax(&status[2], (uint32_t)i + 1);
+    }
+  }
+}
+
+// Left solve of one diagonal block: for every column of B (one thread per
+// column) x <- alpha * T^-1 x, T = nb x nb (nb <= 64) lower or upper
+// triangular with inverted diagonal dinv (nullptr: unit diagonal).  The
+// column lives in registers; products accumulate in 64 bits with the
+// reference's wrap-around correction (+2^64 mod p) and one reduction per
+// entry.
+template <bool UPPER>
+__global__ void __launch_bounds__(128)
+    tri_left_kernel(const uint32_t *__restrict__ T, size_t ldt, int nb,
+                    const uint32_t *__restrict__ dinv, uint32_t *__restrict__ B, size_t ldb,
+                    int ncols, Modulus mod, uint32_t two64, uint32_t alpha) {
+  __shared__ uint32_t sT[TRI_NB][TRI_NB + 1];
+  __shared__ uint32_t sD[TRI_NB];
+  for (int e = threadIdx.x; e < TRI_NB * TRI_NB; e += blockDim.x) {
+    int r = e / TRI_NB, cc = e % TRI_NB;
+    sT[r][cc] = (r < nb && cc < nb) ? T[(size_t)r * ldt + cc] : 0u;
+  }
+  for (int e = threadIdx.x; e < TRI_NB; e += blockDim.x) sD[e] = (e < nb && dinv) ? dinv[e] : 1u;
+  __syncthreads();
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= ncols) return;
+  const uint32_t p = (uint32_t)mod.p;
+  uint32_t x[TRI_NB];
+#pragma unroll
+  for (int k = 0; k < TRI_NB; ++k) {
+    uint32_t v = (k < nb) ? B[(size_t)k * ldb + col] : 0u;
+    x[k] = (alpha == 1u) ? v : mod_mul(v, alpha, mod);
+  }
+  if (!UPPER) {
+#pragma unroll
+    for (int k = 0; k < TRI_NB; ++k) {
+      uint64_t s = 0;
+#pragma unroll
+      for (int j = 0; j < k; ++j) {
+        uint64_t t = (uint64_t)sT[k][j] * x[j];
+        s += t;
+        if (s < t) s += two64;
+      }
+      uint32_t r = mod_reduce(s, mod);
+      uint32_t v = x[k] >= r ? x[k] - r : x[k] + (p - r);
+      x[k] = (k < nb) ? mod_mul(v, sD[k], mod) : 0u;
+    }
+  } else {
+#pragma unroll
+    for (int k = TRI_NB - 1; k >= 0; --k) {
+      uint64_t s = 0;
+#pragma unroll
+      for (int j = k + 1; j < TRI_NB; ++j) {
+        uint64_t t = (uint64_t)sT[k][j] * x[j];
+        s += t;
+        if (s < t) s += two64;
+      }
+      uint32_t r = mod_reduce(s, mod);
+      uint32_t v = x[k] >= r ? x[k] - r : x[k] + (p - r);
+      x[k] = (k < nb) ? mod_mul(v, sD[k], mod) : 0u;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < TRI_NB; ++k)
+    if (k < nb) B[(size_t)k * ldb + col] = x[k];
+}
+
+// C <- beta * C for an m x n block (beta in [0, p)).
+__global__ void zp_scale2_kernel(uint32_t *C, size_t ldc, int M, int N, Modulus mod,
+                                 uint32_t beta) {
+  const size_t total = (size_t)M * N;
+  for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (size_t)gridDim.x * blockDim.x) {
+    size_t r = idx / N, cc = idx % N;
+    uint32_t *x = C + r * ldc + cc;
+    *x = beta ? mod_mul(*x, beta, mod) : 0u;
+  }
+}
+
+int tri_left_block(Ctx *c, bool upper, int nb, const uint32_t *T, size_t ldt,
+                   const uint32_t *dinv, uint32_t *B, size_t ldb, int ncols, uint32_t p,
+                   uint32_t alpha) {
+  if (nb <= 0 || ncols <= 0) return ST_OK;
+  const Modulus mod = make_modulus(p);
+  const uint32_t t64 = two64_mod(p);
+  const int threads = 128;
+  const int grid = (ncols + threads - 1) / threads;
+  int pi = prof_begin(c, "tri_left");
+  if (upper)
+    tri_left_kernel<true><<<grid, threads, 0, c->stream>>>(T, ldt, nb, dinv, B, ldb, ncols, mod,
+                                                           t64, alpha);
+  else
+    tri_left_kernel<false><<<grid, threads, 0, c->stream>>>(T, ldt, nb, dinv, B, ldb, ncols, mod,
+                                                            t64, alpha);
+  prof_end(c, pi);
+  ctx_launched(c);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? ST_OK : ctx_cuda(c, e, "tri_left launch");
+}
+
+// Recursive solve on diagonal offset `off` of the full system (dinv is the
+// inverted diagonal of the whole matrix).
+static int trsm_rec(Ctx *c, bool upper, int m, int n, uint32_t p, uint32_t alpha,
+                    const uint32_t *A, size_t lda, const uint32_t *dinv, uint32_t *B, size_t ldb,
+                    uint8_t *gemm_ws) {
+  if (m <= 0) return ST_OK;
+  if (m <= TRI_NB) return tri_left_block(c, upper, m, A, lda, dinv, B, ldb, n, p, alpha);
+  // split at a multiple of the leaf size, near the middle
+  int l = ((m / 2 + TRI_NB - 1) / TRI_NB) * TRI_NB;
+  if (l >= m) l = m - TRI_NB;
+  const uint32_t *A11 = A, *A12 = A + l, *A21 = A + (size_t)l * lda, *A22 = A21 + l;
+  uint32_t *B1 = B, *B2 = B + (size_t)l * ldb;
+  int st;
+  if (!upper) {
+    if ((st = trsm_rec(c, upper, l, n, p, alpha, A11, lda, dinv, B1, ldb, gemm_ws))) return st;
+    if ((st = zp_gemm_dev(c, GEMM_AUTO, m - l, n, l, p, p - 1, A21, lda, B1, ldb, alpha, B2, ldb,
+                          gemm_ws)))
+      return st;
+    return trsm_rec(c, upper, m - l, n, p, 1, A22, lda, dinv ? dinv + l : nullptr, B2, ldb,
+                    gemm_ws);
+  } else {
+    if ((st = trsm_rec(c, upper, m - l, n, p, alpha, A22, lda, dinv ? dinv + l : nullptr, B2,
+                        ldb, gemm_ws)))
+      return st;
+    if ((st = zp_gemm_dev(c, GEMM_AUTO, l, n, m - l, p, p - 1, A12, lda, B2, ldb, alpha, B1, ldb,
+                          gemm_ws)))
+      return st;
+    return trsm_rec(c, upper, l, n, p, 1, A11, lda, dinv, B1, ldb, gemm_ws);
+  }
+}
+
+int zp_trsm_dev(Ctx *c, bool upper, bool unit, int m, int n, uint32_t p, uint32_t alpha,
+                const uint32_t *A, size_t lda, uint32_t *B, size_t ldb, size_t *bad_idx) {
+  if (p < 2) return ctx_fail(c, ST_ARG, "modulus must be at least 2");
+  if (m < 0 || n < 0) return ctx_fail(c, ST_ARG, "negative dimension");
+  if (m == 0) return ST_OK;
+  if (lda < (size_t)m || (n > 0 && ldb < (size_t)n))
+    return ctx_fail(c, ST_ARG, "leading dimension smaller than the row length");
+  alpha %= p;
+  const Modulus mod = make_modulus(p);
+  if (alpha == 0) {
+    if (n == 0) return ST_OK;
+    const size_t total = (size_t)m * n;
+    int grid = (int)std::min<size_t>((total + 255) / 256, (size_t)c->num_sms * 8);
+    zp_scale2_kernel<<<grid, 256, 0, c->stream>>>(B, ldb, m, n, mod, 0);
+    ctx_launched(c);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? ST_OK : ctx_cuda(c, e, "scale launch");
+  }
+  void *buf = nullptr;
+  int st = ctx_buffer(c, BUF_DINV, (size_t)m * sizeof(uint32_t), &buf);
+  if (st) return st;
+  uint32_t *dinv = static_cast<uint32_t *>(buf);
+  if (!unit) {
+    // status[1] = min failing index (init all ones), status[2] = max + 1
+    cudaError_t e = cudaMemsetAsync(c->dstatus + 1, 0xFF, sizeof(uint32_t), c->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(c->dstatus + 2, 0, sizeof(uint32_t), c->stream);
+    if (e != cudaSuccess) return ctx_cuda(c, e, "cudaMemsetAsync");
+    int grid = std::min((m + 255) / 256, c->num_sms * 4);
+    diag_inverse_kernel<<<grid, 256, 0, c->stream>>>(A, lda, m, p, dinv, c->dstatus);
+    ctx_launched(c);
+    e = cudaMemcpyAsync(c->hstatus, c->dstatus, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                        c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return ctx_cuda(c, e, "diagonal inverses");
+    if (c->hstatus[2] != 0) {
+      size_t idx = upper ? (size_t)c->hstatus[2] - 1 : (size_t)c->hstatus[1];
+      if (bad_idx) *bad_idx = idx;
+      return ctx_fail(c, ST_DIAG, "diagonal entry not invertible");
+    }
+  }
+  if (n == 0) return ST_OK;
+  void *w = nullptr;
+  // the largest update is about (m/2) x n x (m/2)
+  st = ctx_workspace(c, zp_gemm_workspace_bytes(p, m, n, (m + 1) / 2 + TRI_NB), &w);
+  if (st) return st;
+  return trsm_rec(c, upper, m, n, p, alpha, A, lda, unit ? nullptr : dinv, B, ldb,
+                  static_cast<uint8_t *>(w));
+}
+
+}  // namespace lela

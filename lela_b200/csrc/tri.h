@@ -1,0 +1,21 @@
+// lela_b200/csrc/tri.h -- triangular solves over Z/p (device pointers).
+#pragma once
+#include <cstddef>
+#include <cstdint>
+
+#include "context.h"
+
+namespace lela {
+
+// B <- alpha * A^-1 * B (see tri.cu).  Synchronises once to read the
+// diagonal check; returns ST_DIAG with *bad_idx on a singular diagonal.
+int zp_trsm_dev(Ctx *c, bool upper, bool unit, int m, int n, uint32_t p, uint32_t alpha,
+                const uint32_t *A, size_t lda, uint32_t *B, size_t ldb, size_t *bad_idx);
+
+// One diagonal block (nb <= 64) solved on CUDA cores: B <- alpha*T^-1*B;
+// dinv = inverted diagonal (nullptr for a unit diagonal).
+int tri_left_block(Ctx *c, bool upper, int nb, const uint32_t *T, size_t ldt,
+                   const uint32_t *dinv, uint32_t *B, size_t ldb, int ncols, uint32_t p,
+                   uint32_t alpha);
+
+}  // namespace lela
