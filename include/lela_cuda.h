@@ -124,6 +124,21 @@ int lela_cuda_trsm_zp_u32_dev (lela_cuda_ctx *ctx, int upper, int diag_is_one, s
 			       size_t n, uint32_t p, uint32_t a, const uint32_t *A, size_t lda,
 			       uint32_t *B, size_t ldb, size_t *bad_idx);
 
+/* ------------------------------------------------------- Z/p echelon form
+ * A (m x n) <- its non-reduced row-echelon form, in place; *rank, *det =
+ * product of the pivots.  Replaces EchelonForm::echelonize on a DenseMatrix
+ * (lela/solutions/echelon-form.h:103-134: GaussJordan::echelonize +
+ * Elimination::move_L), whose result equals Elimination::echelonize
+ * (lela/algorithms/elimination.tcc:47-139) with DensePivotStrategy
+ * (lela/algorithms/pivot-strategy.tcc:19-42): first nonzero in the column
+ * at or below the current row, row transpositions, pivots not normalised.
+ * LELA_CUDA_PIVOT_NOT_INVERTIBLE when Modular<uint32> cannot invert a pivot
+ * (p >= 2^31). */
+int lela_cuda_echelon_zp_u32 (lela_cuda_ctx *ctx, size_t m, size_t n, uint32_t p, uint32_t *A,
+			      size_t lda, size_t *rank, uint32_t *det);
+int lela_cuda_echelon_zp_u32_dev (lela_cuda_ctx *ctx, size_t m, size_t n, uint32_t p,
+				  uint32_t *A, size_t lda, size_t *rank, uint32_t *det);
+
 /* The same tensor-core gemm for callers that cannot allocate device memory:
  * code whose device memory is owned by someone else (a host framework's
  * caching allocator, a fixed per-process budget) or that must not call

@@ -256,6 +256,24 @@ class CudaModule:
         return B
 
 
+    # ------------------------------------------------------- echelon form
+    def echelonize(self, p, A):
+        """A <- non-reduced row-echelon form in place (EchelonForm::echelonize
+        on a DenseMatrix, LELA's pivot rule); returns (A, rank, det)."""
+        m, n = A.shape
+        r = _S(0)
+        d = _U(0)
+        if _is_torch(A):
+            st = self.L.lela_cuda_echelon_zp_u32_dev(self.h, m, n, p, _dptr(A), A.stride(0),
+                                                     ctypes.byref(r), ctypes.byref(d))
+        else:
+            _check(A.dtype == np.uint32, "echelonize: uint32 matrix expected")
+            st = self.L.lela_cuda_echelon_zp_u32(self.h, m, n, p, _ptr(A), A.strides[0] // 4,
+                                                 ctypes.byref(r), ctypes.byref(d))
+        self._raise(st)
+        return A, r.value, d.value
+
+
 def _is_torch(x):
     return type(x).__module__.startswith("torch")
 

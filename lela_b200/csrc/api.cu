@@ -11,6 +11,7 @@
 #include "../../include/lela_cuda.h"
 #include "common.cuh"
 #include "context.h"
+#include "echelon.h"
 #include "tri.h"
 #include "zp_gemm.h"
 
@@ -346,6 +347,41 @@ int lela_cuda_gemm_zp_u32(lela_cuda_ctx *h, size_t m, size_t n, size_t k, uint32
                      (const uint32_t *)dB, n, b, (uint32_t *)dC, n, nullptr);
   if (!st) st = d2h_matrix(c, C, dC, m, n, ldc, 4);
   if (!st) st = ctx_check_status(c, "gemm_zp_u32");
+  return st;
+}
+
+int lela_cuda_echelon_zp_u32_dev(lela_cuda_ctx *h, size_t m, size_t n, uint32_t p, uint32_t *A,
+                                 size_t lda, size_t *rank, uint32_t *det) {
+  if (!h || !rank || !det) return ST_ARG;
+  Ctx *c = &h->c;
+  if (m > (size_t)INT32_MAX || n > (size_t)INT32_MAX) return ctx_fail(c, ST_ARG, "dimension too large");
+  if (m && n && !A) return ctx_fail(c, ST_ARG, "null pointer");
+  int st = zp_echelon_dev(c, (int)m, (int)n, p, A, lda, rank, det, nullptr);
+  if (!st) st = ctx_check_status(c, "echelon_zp_u32");
+  return st;
+}
+
+int lela_cuda_echelon_zp_u32(lela_cuda_ctx *h, size_t m, size_t n, uint32_t p, uint32_t *A,
+                             size_t lda, size_t *rank, uint32_t *det) {
+  if (!h || !rank || !det) return ST_ARG;
+  Ctx *c = &h->c;
+  if (m > (size_t)INT32_MAX || n > (size_t)INT32_MAX) return ctx_fail(c, ST_ARG, "dimension too large");
+  if (p < 2) return ctx_fail(c, ST_ARG, "modulus must be at least 2");
+  if (m == 0 || n == 0) {
+    *rank = 0;
+    *det = 1 % p;
+    return ST_OK;
+  }
+  if (!A) return ctx_fail(c, ST_ARG, "null pointer");
+  if (lda < n) return ctx_fail(c, ST_ARG, "leading dimension smaller than the row length");
+  cudaSetDevice(c->device);
+  void *dA = nullptr;
+  int st = ctx_stage(c, 0, m * n * 4, &dA);
+  if (!st) st = ctx_clear_status(c);
+  if (!st) st = h2d_matrix(c, dA, A, m, n, lda, 4);
+  if (!st) st = zp_echelon_dev(c, (int)m, (int)n, p, (uint32_t *)dA, n, rank, det, nullptr);
+  if (!st) st = d2h_matrix(c, A, dA, m, n, lda, 4);
+  if (!st) st = ctx_check_status(c, "echelon_zp_u32");
   return st;
 }
 
