@@ -139,6 +139,31 @@ int lela_cuda_echelon_zp_u32 (lela_cuda_ctx *ctx, size_t m, size_t n, uint32_t p
 int lela_cuda_echelon_zp_u32_dev (lela_cuda_ctx *ctx, size_t m, size_t n, uint32_t p,
 				  uint32_t *A, size_t lda, size_t *rank, uint32_t *det);
 
+/* ------------------------------------------- Faugere-Lachartre echelon form
+ * Echelon form of the F4 matrix X (m x n, CSR: rowptr[m+1], colidx, vals;
+ * column indices strictly increasing within a row, stored values in [0,p)).
+ * Replaces FaugereLachartre<Modular<uint32>>::echelonize (lela/algorithms/
+ * faugere-lachartre.h:80-81, .tcc:735-917) with R returned dense (row stride
+ * ldr >= n): reduced != 0 gives the reduced row-echelon form (m rows, zero
+ * rows last); only_D as in the reference (*out_rows = rank of D rows).
+ * *rank and *det are the reference's outputs (det = product of the leading
+ * entries of the X pivot rows and of the echelon form of D).
+ * Status: LELA_CUDA_WRONG_MATRIX_FORM with *bad_row (rows not sorted by
+ * leading column: WrongMatrixForm, faugere-lachartre.tcc:80-81);
+ * LELA_CUDA_DIAG_NOT_INVERTIBLE when A's diagonal cannot be inverted (the
+ * reference returns early from echelonize, :792-799; R is then untouched).
+ * The _dev form takes the CSR arrays and R on the device. */
+int lela_cuda_fl_echelonize_zp_u32 (lela_cuda_ctx *ctx, size_t m, size_t n, uint32_t p,
+				    const uint64_t *rowptr, const uint32_t *colidx,
+				    const uint32_t *vals, int reduced, int only_D, uint32_t *R,
+				    size_t ldr, size_t *rank, uint32_t *det, size_t *out_rows,
+				    size_t *bad_row);
+int lela_cuda_fl_echelonize_zp_u32_dev (lela_cuda_ctx *ctx, size_t m, size_t n, uint32_t p,
+					const uint64_t *rowptr, const uint32_t *colidx,
+					const uint32_t *vals, int reduced, int only_D, uint32_t *R,
+					size_t ldr, size_t *rank, uint32_t *det, size_t *out_rows,
+					size_t *bad_row);
+
 /* The same tensor-core gemm for callers that cannot allocate device memory:
  * code whose device memory is owned by someone else (a host framework's
  * caching allocator, a fixed per-process budget) or that must not call

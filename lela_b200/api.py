@@ -110,6 +110,9 @@ def _bind_optional(L):
         "lela_cuda_fl_echelonize_zp_u32": [_P, _S, _S, _U, _P, _P, _P, _I, _I, _P, _S,
                                            ctypes.POINTER(_S), ctypes.POINTER(_U),
                                            ctypes.POINTER(_S), ctypes.POINTER(_S)],
+        "lela_cuda_fl_echelonize_zp_u32_dev": [_P, _S, _S, _U, _P, _P, _P, _I, _I, _P, _S,
+                                               ctypes.POINTER(_S), ctypes.POINTER(_U),
+                                               ctypes.POINTER(_S), ctypes.POINTER(_S)],
         "lela_cuda_gemm_gf2": [_P, _S, _S, _S, _I, _P, _S, _P, _S, _I, _P, _S],
         "lela_cuda_gemm_gf2_dev": [_P, _S, _S, _S, _I, _P, _S, _P, _S, _I, _P, _S],
         "lela_cuda_echelon_gf2": [_P, _S, _S, _P, _S, ctypes.POINTER(_S)],
@@ -272,6 +275,38 @@ class CudaModule:
                                                  ctypes.byref(r), ctypes.byref(d))
         self._raise(st)
         return A, r.value, d.value
+
+
+    # ------------------------------------------------- Faugere-Lachartre
+    def fl_echelonize(self, p, X, reduced=True, only_D=False, R=None):
+        """FaugereLachartre::echelonize of the CSR matrix X (an object with
+        m, n, rowptr, colidx, vals -- numpy arrays for the host path, torch
+        CUDA tensors for the device path).  Returns (R, rank, det); R is the
+        dense output (out_rows x n).  Raises WrongMatrixForm(row); a singular
+        pivot block raises DiagonalEntryNotInvertible (the reference returns
+        early there)."""
+        m, n = X.m, X.n
+        rk, det, rows, bad = _S(0), _U(0), _S(0), _S(0)
+        if _is_torch(X.rowptr):
+            import torch
+            if R is None:
+                R = torch.empty((max(m, 1), n), dtype=torch.int32, device=X.rowptr.device)
+            st = self.L.lela_cuda_fl_echelonize_zp_u32_dev(
+                self.h, m, n, p, _dptr(X.rowptr), _dptr(X.colidx), _dptr(X.vals), int(reduced),
+                int(only_D), _dptr(R), R.stride(0), ctypes.byref(rk), ctypes.byref(det),
+                ctypes.byref(rows), ctypes.byref(bad))
+        else:
+            if R is None:
+                R = np.zeros((max(m, 1), n), dtype=np.uint32)
+            rowptr = np.ascontiguousarray(X.rowptr, dtype=np.uint64)
+            colidx = np.ascontiguousarray(X.colidx, dtype=np.uint32)
+            vals = np.ascontiguousarray(X.vals, dtype=np.uint32)
+            st = self.L.lela_cuda_fl_echelonize_zp_u32(
+                self.h, m, n, p, _ptr(rowptr), _ptr(colidx), _ptr(vals), int(reduced), int(only_D),
+                _ptr(R), R.strides[0] // 4, ctypes.byref(rk), ctypes.byref(det), ctypes.byref(rows),
+                ctypes.byref(bad))
+        self._raise(st, bad.value)
+        return R[:rows.value], rk.value, det.value
 
 
 def _is_torch(x):

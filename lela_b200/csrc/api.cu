@@ -12,6 +12,7 @@
 #include "common.cuh"
 #include "context.h"
 #include "echelon.h"
+#include "fl.h"
 #include "tri.h"
 #include "zp_gemm.h"
 
@@ -348,6 +349,91 @@ int lela_cuda_gemm_zp_u32(lela_cuda_ctx *h, size_t m, size_t n, size_t k, uint32
   if (!st) st = d2h_matrix(c, C, dC, m, n, ldc, 4);
   if (!st) st = ctx_check_status(c, "gemm_zp_u32");
   return st;
+}
+
+static int fl_finish(Ctx *c, int st, const FlResult &r, size_t *rank, uint32_t *det,
+                     size_t *out_rows, size_t *bad_row) {
+  if (rank) *rank = r.rank;
+  if (det) *det = r.det;
+  if (out_rows) *out_rows = (st == ST_OK) ? r.out_rows : 0;
+  if (bad_row) *bad_row = r.bad_row;
+  if (st == ST_OK) st = ctx_check_status(c, "fl_echelonize_zp_u32");
+  return st;
+}
+
+int lela_cuda_fl_echelonize_zp_u32(lela_cuda_ctx *h, size_t m, size_t n, uint32_t p,
+                                   const uint64_t *rowptr, const uint32_t *colidx,
+                                   const uint32_t *vals, int reduced, int only_D, uint32_t *R,
+                                   size_t ldr, size_t *rank, uint32_t *det, size_t *out_rows,
+                                   size_t *bad_row) {
+  if (!h) return ST_ARG;
+  Ctx *c = &h->c;
+  if (m > (size_t)INT32_MAX || n > (size_t)INT32_MAX) return ctx_fail(c, ST_ARG, "dimension too large");
+  if (p < 2) return ctx_fail(c, ST_ARG, "modulus must be at least 2");
+  if (!rowptr || (m && (!R || ldr < n))) return ctx_fail(c, ST_ARG, "bad output or row pointers");
+  const uint64_t nnz = rowptr[m];
+  if (nnz && (!colidx || !vals)) return ctx_fail(c, ST_ARG, "null pointer");
+  for (size_t r = 0; r < m; ++r)
+    if (rowptr[r + 1] < rowptr[r]) return ctx_fail(c, ST_ARG, "row pointers decrease");
+  for (uint64_t e = 0; e < nnz; ++e)
+    if (colidx[e] >= n) return ctx_fail(c, ST_ARG, "column index out of range");
+  cudaSetDevice(c->device);
+  std::vector<uint32_t> heads(m), hv(m);
+  for (size_t r = 0; r < m; ++r) {
+    const bool empty = rowptr[r + 1] == rowptr[r];
+    heads[r] = empty ? 0 : colidx[rowptr[r]];
+    hv[r] = empty ? 0 : vals[rowptr[r]];
+  }
+  void *dX = nullptr, *dR = nullptr;
+  const size_t xbytes = (m + 1) * 8 + nnz * 8 + 64;
+  int st = ctx_buffer(c, BUF_FL_X, xbytes, &dX);
+  if (!st) st = ctx_buffer(c, BUF_FL_R, std::max<size_t>(m * n * 4, 16), &dR);
+  if (st) return st;
+  uint64_t *d_rowptr = (uint64_t *)dX;
+  uint32_t *d_col = (uint32_t *)(d_rowptr + m + 1);
+  uint32_t *d_val = d_col + nnz;
+  cudaError_t e = cudaMemcpyAsync(d_rowptr, rowptr, (m + 1) * 8, cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess && nnz)
+    e = cudaMemcpyAsync(d_col, colidx, nnz * 4, cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess && nnz)
+    e = cudaMemcpyAsync(d_val, vals, nnz * 4, cudaMemcpyHostToDevice, c->stream);
+  if (e != cudaSuccess) return ctx_cuda(c, e, "fl: input copy");
+  if ((st = ctx_clear_status(c))) return st;
+  FlResult res{};
+  st = zp_fl_echelonize_dev(c, (int)m, (int)n, p, d_rowptr, d_col, d_val, rowptr, heads.data(),
+                            hv.data(), reduced != 0, only_D != 0, (uint32_t *)dR, n, &res);
+  if (st == ST_OK && res.out_rows)
+    st = d2h_matrix(c, R, dR, res.out_rows, n, ldr, 4);
+  return fl_finish(c, st, res, rank, det, out_rows, bad_row);
+}
+
+int lela_cuda_fl_echelonize_zp_u32_dev(lela_cuda_ctx *h, size_t m, size_t n, uint32_t p,
+                                       const uint64_t *rowptr, const uint32_t *colidx,
+                                       const uint32_t *vals, int reduced, int only_D, uint32_t *R,
+                                       size_t ldr, size_t *rank, uint32_t *det, size_t *out_rows,
+                                       size_t *bad_row) {
+  if (!h) return ST_ARG;
+  Ctx *c = &h->c;
+  if (m > (size_t)INT32_MAX || n > (size_t)INT32_MAX) return ctx_fail(c, ST_ARG, "dimension too large");
+  if (p < 2) return ctx_fail(c, ST_ARG, "modulus must be at least 2");
+  if (!rowptr || (m && (!R || ldr < n))) return ctx_fail(c, ST_ARG, "bad output or row pointers");
+  std::vector<uint64_t> hrow(m + 1);
+  std::vector<uint32_t> heads(m), hv(m);
+  void *dH = nullptr;
+  int st = ctx_buffer(c, BUF_FL_HEADS, 2 * (m + 1) * 4 + 64, &dH);
+  if (st) return st;
+  uint32_t *d_heads = (uint32_t *)dH, *d_hv = d_heads + m + 1;
+  if ((st = fl_row_heads_dev(c, (int)m, rowptr, colidx, vals, d_heads, d_hv))) return st;
+  cudaError_t e = cudaMemcpyAsync(hrow.data(), rowptr, (m + 1) * 8, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess && m)
+    e = cudaMemcpyAsync(heads.data(), d_heads, m * 4, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess && m) e = cudaMemcpyAsync(hv.data(), d_hv, m * 4, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return ctx_cuda(c, e, "fl: row heads");
+  FlResult res{};
+  st = zp_fl_echelonize_dev(c, (int)m, (int)n, p, rowptr, colidx, vals, hrow.data(), heads.data(),
+                            hv.data(), reduced != 0, only_D != 0, R, ldr, &res);
+  return fl_finish(c, st, res, rank, det, out_rows, bad_row);
 }
 
 int lela_cuda_echelon_zp_u32_dev(lela_cuda_ctx *h, size_t m, size_t n, uint32_t p, uint32_t *A,

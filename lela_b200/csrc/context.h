@@ -84,6 +84,7 @@ enum BufSlot : int {
   BUF_GF2_0 = 11,
   BUF_GF2_1 = 12,
   BUF_MISC = 13,
+  BUF_FL_HEADS = 14,  // device row heads of a device CSR input
 };
 
 // Grow-only allocation helpers; return ST_OK or ST_NOMEM.

@@ -1,0 +1,368 @@
+// lela_b200/csrc/fl.cu -- Faugere-Lachartre echelon form of an F4 matrix
+// over Z/p on the GPU.
+//
+// Reference: FaugereLachartre::echelonize (lela/algorithms/
+// faugere-lachartre.tcc:735-917).  Steps and their GPU form:
+//
+//  setup_splicer (:47-146)  The head of a sparse row is its first stored
+//      entry (BLAS1::head on a sparse vector, lela/blas/level1-generic.tcc:
+//      452-460).  Walking the rows: a head larger than the last pivot column
+//      makes a pivot row (det *= head value), an equal head a non-pivot row,
+//      a smaller head throws WrongMatrixForm(row), and the first empty row
+//      ends the walk (every later row is a non-pivot row).  This O(m) walk
+//      runs on the host over the row heads.
+//  split (MatrixGrid1, :766)  One scatter kernel places every stored entry
+//      into dense A (pivot rows x pivot columns, upper triangular), B, C, D.
+//  B <- A^-1 B (:791)  Dense trsm (tri.cu): tensor-core updates, CUDA-core
+//      leaves.  A singular diagonal makes the reference return early
+//      (:792-799); reported here as LELA_CUDA_DIAG_NOT_INVERTIBLE with rank
+//      and det as the reference leaves them.
+//  D <- D - C B (:805)  Limb-split INT8 tensor-core gemm (zp_gemm.cu).
+//  echelon(D) (:822, then setup_splicer on it, :833)  echelon.cu; its pivots
+//      multiply det and add to the rank.
+//  reduced (:851-902)  D1 | D2 split by D's pivot columns, D2 <- D1^-1 D2
+//      (trsm), B2 <- B2 - B1 D2 (gemm), then the rows are assembled in
+//      pivot-column order (the reduced row-echelon form is unique).
+//  non-reduced / only_D (:867-874, :906-911)  as the reference's
+//      MatrixGrid4/5 write them (see oracle/lela_oracle.c for the exact rows).
+#include <algorithm>
+#include <vector>
+
+#include "common.cuh"
+#include "context.h"
+#include "echelon.h"
+#include "fl.h"
+#include "tri.h"
+#include "zp_gemm.h"
+
+namespace lela {
+
+// Row r of X: pos[r] = index of r among pivot rows (>= 0) or -(1 + index
+// among non-pivot rows); column c: cpos likewise.
+__global__ void fl_split_kernel(const uint64_t *__restrict__ rowptr,
+                                const uint32_t *__restrict__ colidx,
+                                const uint32_t *__restrict__ vals, int m,
+                                const int *__restrict__ rpos, const int *__restrict__ cpos,
+                                uint32_t *A, size_t npiv, uint32_t *B, size_t nres, uint32_t *C,
+                                uint32_t *D) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int r = warp; r < m; r += nwarps) {
+    const int rp = rpos[r];
+    for (uint64_t e = rowptr[r] + lane; e < rowptr[r + 1]; e += 32) {
+      const int cp = cpos[colidx[e]];
+      const uint32_t v = vals[e];
+      if (rp >= 0) {
+        if (cp >= 0) A[(size_t)rp * npiv + cp] = v;
+        else B[(size_t)rp * nres + (-1 - cp)] = v;
+      } else {
+        if (cp >= 0) C[(size_t)(-1 - rp) * npiv + cp] = v;
+        else D[(size_t)(-1 - rp) * nres + (-1 - cp)] = v;
+      }
+    }
+  }
+}
+
+// Gather columns: out[r][j] = in[r][cols[j]] for r < rows, j < ncols.
+__global__ void gather_cols_kernel(const uint32_t *__restrict__ in, size_t ldi, int rows,
+                                   const int *__restrict__ cols, int ncols,
+                                   uint32_t *__restrict__ out, size_t ldo) {
+  const size_t total = (size_t)rows * ncols;
+  for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (size_t)gridDim.x * blockDim.x) {
+    size_t r = idx / ncols, j = idx % ncols;
+    out[r * ldo + j] = in[r * ldi + cols[j]];
+  }
+}
+
+// Assemble output rows, one block per row.  For output row o: kind[o] =
+// 0 (zero row), 1 (values from M1 row src_row[o]), 2 (values from M2 row
+// src_row[o]), 4 (no values); unit_col[o] = column that gets a 1 (or -1).
+// Values of a row are scattered to columns vcols[0..nv).
+__global__ void fl_assemble_kernel(uint32_t *__restrict__ R, size_t ldr, int rows, int n,
+                                   const int *__restrict__ kind, const int *__restrict__ src_row,
+                                   const int *__restrict__ unit_col,
+                                   const uint32_t *__restrict__ M1, size_t ld1,
+                                   const uint32_t *__restrict__ M2, size_t ld2,
+                                   const int *__restrict__ vcols, int nv) {
+  for (int o = blockIdx.x; o < rows; o += gridDim.x) {
+    uint32_t *out = R + (size_t)o * ldr;
+    const int k = kind[o];
+    for (int j = threadIdx.x; j < n; j += blockDim.x) out[j] = 0u;
+    __syncthreads();
+    if (k == 1 || k == 2) {
+      const uint32_t *src = (k == 1 ? M1 + (size_t)src_row[o] * ld1 : M2 + (size_t)src_row[o] * ld2);
+      for (int j = threadIdx.x; j < nv; j += blockDim.x) out[vcols[j]] = src[j];
+    }
+    if (k != 0 && threadIdx.x == 0 && unit_col[o] >= 0) out[unit_col[o]] = 1u;
+    __syncthreads();
+  }
+}
+
+__global__ void fl_heads_kernel(int m, const uint64_t *__restrict__ rowptr,
+                                const uint32_t *__restrict__ colidx,
+                                const uint32_t *__restrict__ vals, uint32_t *heads,
+                                uint32_t *headvals) {
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < m; r += gridDim.x * blockDim.x) {
+    const uint64_t e = rowptr[r];
+    const bool empty = rowptr[r + 1] == e;
+    heads[r] = empty ? 0u : colidx[e];
+    headvals[r] = empty ? 0u : vals[e];
+  }
+}
+
+int fl_row_heads_dev(Ctx *c, int m, const uint64_t *d_rowptr, const uint32_t *d_colidx,
+                     const uint32_t *d_vals, uint32_t *d_heads, uint32_t *d_headvals) {
+  if (m <= 0) return ST_OK;
+  int grid = std::min((m + 255) / 256, c->num_sms * 8);
+  fl_heads_kernel<<<grid, 256, 0, c->stream>>>(m, d_rowptr, d_colidx, d_vals, d_heads, d_headvals);
+  ctx_launched(c);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? ST_OK : ctx_cuda(c, e, "fl heads launch");
+}
+
+static int upload(Ctx *c, void *dst, const void *src, size_t bytes, const char *what) {
+  if (!bytes) return ST_OK;
+  cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->stream);
+  return e == cudaSuccess ? ST_OK : ctx_cuda(c, e, what);
+}
+
+int zp_fl_echelonize_dev(Ctx *c, int m, int n, uint32_t p, const uint64_t *d_rowptr,
+                         const uint32_t *d_colidx, const uint32_t *d_vals,
+                         const uint64_t *h_rowptr, const uint32_t *h_heads,
+                         const uint32_t *h_headvals, bool reduced, bool only_D, uint32_t *R,
+                         size_t ldr, FlResult *res) {
+  res->rank = 0;
+  res->det = 1 % p;
+  res->out_rows = 0;
+  res->bad_row = 0;
+  if (p < 2) return ctx_fail(c, ST_ARG, "modulus must be at least 2");
+  int st;
+  uint64_t det = 1 % p;
+
+  // ---- setup_splicer on the row heads
+  std::vector<int> rpos(m), cpos(n, 0);
+  std::vector<char> is_piv_col(n, 0);
+  std::vector<int> piv_rows, res_rows, piv_cols, res_cols;
+  long last_col = -1;
+  bool walking = true;
+  for (int r = 0; r < m; ++r) {
+    bool piv = false;
+    if (walking && h_rowptr[r] == h_rowptr[r + 1]) walking = false;  // first empty row
+    if (walking) {
+      long col = h_heads[r];
+      if (col < last_col) {
+        res->bad_row = (size_t)r;
+        return ctx_fail(c, ST_WRONG_FORM, "Bad input-matrix for Faugere-Lachartre");
+      }
+      if (col > last_col) {
+        piv = true;
+        is_piv_col[col] = 1;
+        last_col = col;
+      }
+      det = (det * h_headvals[r]) % p;
+    }
+    if (piv) {
+      rpos[r] = (int)piv_rows.size();
+      piv_rows.push_back(r);
+    } else {
+      rpos[r] = -1 - (int)res_rows.size();
+      res_rows.push_back(r);
+    }
+  }
+  const int npiv = (int)piv_rows.size();
+  for (int col = 0; col < n; ++col) {
+    if (is_piv_col[col]) {
+      cpos[col] = (int)piv_cols.size();
+      piv_cols.push_back(col);
+    } else {
+      cpos[col] = -1 - (int)res_cols.size();
+      res_cols.push_back(col);
+    }
+  }
+  const int mres = (int)res_rows.size(), nres = (int)res_cols.size();
+  res->rank = (size_t)npiv;
+  res->det = (uint32_t)det;
+
+  // ---- device blocks
+  void *vA, *vB, *vC, *vD, *vI;
+  const size_t szA = (size_t)npiv * npiv, szB = (size_t)npiv * nres, szC = (size_t)mres * npiv,
+               szD = (size_t)mres * nres;
+  if ((st = ctx_buffer(c, BUF_FL_A, szA * 4 + 16, &vA))) return st;
+  if ((st = ctx_buffer(c, BUF_FL_B, szB * 4 + 16, &vB))) return st;
+  if ((st = ctx_buffer(c, BUF_FL_C, szC * 4 + 16, &vC))) return st;
+  if ((st = ctx_buffer(c, BUF_FL_D, szD * 4 + 16, &vD))) return st;
+  const size_t idx_words = (size_t)m + n + 4 * ((size_t)m + n) + 64;
+  if ((st = ctx_buffer(c, BUF_FL_IDX, idx_words * sizeof(int), &vI))) return st;
+  uint32_t *A = (uint32_t *)vA, *B = (uint32_t *)vB, *C = (uint32_t *)vC, *D = (uint32_t *)vD;
+  int *d_rpos = (int *)vI, *d_cpos = d_rpos + m, *d_aux = d_cpos + n;
+  cudaMemsetAsync(A, 0, szA * 4, c->stream);
+  cudaMemsetAsync(B, 0, szB * 4, c->stream);
+  cudaMemsetAsync(C, 0, szC * 4, c->stream);
+  cudaMemsetAsync(D, 0, szD * 4, c->stream);
+  if ((st = upload(c, d_rpos, rpos.data(), (size_t)m * sizeof(int), "fl: rows"))) return st;
+  if ((st = upload(c, d_cpos, cpos.data(), (size_t)n * sizeof(int), "fl: cols"))) return st;
+  if (m > 0) {
+    int grid = std::min((m * 32 + 255) / 256, c->num_sms * 16);
+    int pi = prof_begin(c, "fl_split");
+    fl_split_kernel<<<grid, 256, 0, c->stream>>>(d_rowptr, d_colidx, d_vals, m, d_rpos, d_cpos, A,
+                                                 npiv, B, nres, C, D);
+    prof_end(c, pi);
+    ctx_launched(c);
+  }
+
+  // ---- B <- A^-1 B
+  size_t bad = 0;
+  if (npiv > 0) {
+    st = zp_trsm_dev(c, true, false, npiv, nres, p, 1, A, npiv, B, nres, &bad);
+    if (st == ST_DIAG) {
+      res->bad_row = bad;
+      return st;  // the reference returns early (rank, det as set so far)
+    }
+    if (st) return st;
+  }
+  // ---- D <- D - C B
+  if (mres > 0 && nres > 0 && npiv > 0)
+    if ((st = zp_gemm_dev(c, GEMM_AUTO, mres, nres, npiv, p, p - 1, C, npiv, B, nres, 1, D, nres,
+                          nullptr)))
+      return st;
+  // ---- echelon form of D
+  size_t rd = 0;
+  uint32_t detD = 1 % p;
+  std::vector<int> dpiv;
+  if ((st = zp_echelon_dev(c, mres, nres, p, D, nres, &rd, &detD, &dpiv))) return st;
+  det = (det * detD) % p;
+  res->rank = (size_t)npiv + rd;
+  res->det = (uint32_t)det;
+
+  // ---- output assembly plans (host), then one assembly kernel
+  std::vector<char> is_dpiv(nres, 0);
+  for (int k : dpiv) is_dpiv[k] = 1;
+  std::vector<int> rem;  // non-pivot columns of D (indices into res cols)
+  for (int j = 0; j < nres; ++j)
+    if (!is_dpiv[j]) rem.push_back(j);
+  const int nrem = (int)rem.size();
+  const int rdi = (int)rd;
+
+  int out_rows = only_D ? rdi : m;
+  std::vector<int> kind(std::max(out_rows, 1), 0), srow(std::max(out_rows, 1), 0),
+      ucol(std::max(out_rows, 1), -1), vcols;
+  const uint32_t *M1 = nullptr, *M2 = nullptr;
+  size_t ld1 = 1, ld2 = 1;
+
+  void *vT = nullptr;
+  if (reduced) {
+    // D1 | D2 split, D2 <- D1^-1 D2
+    const size_t szD1 = (size_t)rdi * rdi, szD2 = (size_t)rdi * nrem;
+    const size_t szB1 = only_D ? 0 : (size_t)npiv * rdi, szB2 = only_D ? 0 : (size_t)npiv * nrem;
+    if ((st = ctx_buffer(c, BUF_FL_T, (szD1 + szD2 + szB1 + szB2) * 4 + 64, &vT))) return st;
+    uint32_t *D1 = (uint32_t *)vT, *D2 = D1 + szD1, *B1 = D2 + szD2, *B2 = B1 + szB1;
+    std::vector<int> cols_all(dpiv);
+    cols_all.insert(cols_all.end(), rem.begin(), rem.end());
+    int *d_cols = d_aux;
+    if ((st = upload(c, d_cols, cols_all.data(), cols_all.size() * sizeof(int), "fl: columns")))
+      return st;
+    auto gather = [&](const uint32_t *in, size_t ldi, int rows, const int *cols, int ncols,
+                      uint32_t *out, size_t ldo) {
+      if (!rows || !ncols) return;
+      const size_t total = (size_t)rows * ncols;
+      int grid = (int)std::min<size_t>((total + 255) / 256, (size_t)c->num_sms * 16);
+      gather_cols_kernel<<<grid, 256, 0, c->stream>>>(in, ldi, rows, cols, ncols, out, ldo);
+      ctx_launched(c);
+    };
+    gather(D, nres, rdi, d_cols, rdi, D1, (size_t)std::max(rdi, 1));
+    gather(D, nres, rdi, d_cols + rdi, nrem, D2, (size_t)std::max(nrem, 1));
+    if (rdi > 0 && nrem > 0) {
+      st = zp_trsm_dev(c, true, false, rdi, nrem, p, 1, D1, rdi, D2, nrem, &bad);
+      if (st) return st;
+    }
+    if (!only_D) {
+      gather(B, nres, npiv, d_cols, rdi, B1, (size_t)std::max(rdi, 1));
+      gather(B, nres, npiv, d_cols + rdi, nrem, B2, (size_t)std::max(nrem, 1));
+      if (npiv > 0 && nrem > 0 && rdi > 0)
+        if ((st = zp_gemm_dev(c, GEMM_AUTO, npiv, nrem, rdi, p, p - 1, B1, rdi, D2, nrem, 1, B2,
+                              nrem, nullptr)))
+          return st;
+    }
+    // value columns: the non-pivot columns of D, in original numbering
+    for (int j = 0; j < nrem; ++j) vcols.push_back(res_cols[rem[j]]);
+    M1 = B2;
+    ld1 = (size_t)std::max(nrem, 1);
+    M2 = D2;
+    ld2 = (size_t)std::max(nrem, 1);
+    if (only_D) {
+      for (int k = 0; k < rdi; ++k) {
+        kind[k] = 2;
+        srow[k] = k;
+        ucol[k] = res_cols[dpiv[k]];
+      }
+    } else {
+      int xi = 0, di = 0, o = 0;
+      while (xi < npiv || di < rdi) {
+        long xc = xi < npiv ? piv_cols[xi] : (long)1 << 40;
+        long dc = di < rdi ? res_cols[dpiv[di]] : (long)1 << 40;
+        if (xc < dc) {
+          kind[o] = 1; srow[o] = xi; ucol[o] = (int)xc; ++xi;
+        } else {
+          kind[o] = 2; srow[o] = di; ucol[o] = (int)dc; ++di;
+        }
+        ++o;
+      }
+    }
+  } else {
+    // non-reduced: X pivot rows = e_piv + (A^-1 B) on the non-pivot
+    // columns; D rows = echelon(D) on the non-pivot columns
+    for (int j = 0; j < nres; ++j) vcols.push_back(res_cols[j]);
+    M1 = B;
+    ld1 = (size_t)std::max(nres, 1);
+    M2 = D;
+    ld2 = (size_t)std::max(nres, 1);
+    if (only_D) {
+      // The reference's MatrixGrid4 is handed D in its D2 slot while the
+      // splicer carries only source-0/1 column blocks: no entry of D is
+      // written and row k is the unit vector at the k-th non-pivot column.
+      for (int k = 0; k < rdi; ++k) {
+        kind[k] = 3;
+        ucol[k] = res_cols[k];
+      }
+    } else {
+      int xi = 0, di = 0, o = 0;
+      while (xi < npiv || di < rdi) {
+        long xc = xi < npiv ? piv_cols[xi] : (long)1 << 40;
+        long dc = di < rdi ? res_cols[dpiv[di]] : (long)1 << 40;
+        if (xc < dc) {
+          kind[o] = 1; srow[o] = xi; ucol[o] = (int)xc; ++xi;
+        } else {
+          kind[o] = 2; srow[o] = di; ucol[o] = -1; ++di;
+        }
+        ++o;
+      }
+    }
+  }
+  res->out_rows = (size_t)out_rows;
+  if (out_rows > 0) {
+    // kind 3 (unit row only) is encoded as a value-less row
+    const int nv = (int)vcols.size();
+    std::vector<int> plan;
+    plan.reserve(3 * out_rows + nv);
+    for (int o = 0; o < out_rows; ++o) plan.push_back(kind[o] == 3 ? 4 : kind[o]);
+    plan.insert(plan.end(), srow.begin(), srow.begin() + out_rows);
+    plan.insert(plan.end(), ucol.begin(), ucol.begin() + out_rows);
+    plan.insert(plan.end(), vcols.begin(), vcols.end());
+    void *vP = nullptr;
+    if ((st = ctx_buffer(c, BUF_MISC, plan.size() * sizeof(int) + 64, &vP))) return st;
+    int *d_plan = (int *)vP;
+    if ((st = upload(c, d_plan, plan.data(), plan.size() * sizeof(int), "fl: plan"))) return st;
+    const int grid = std::min(out_rows, c->num_sms * 16);
+    int pi = prof_begin(c, "fl_assemble");
+    fl_assemble_kernel<<<grid, 256, 0, c->stream>>>(R, ldr, out_rows, n, d_plan, d_plan + out_rows,
+                                                    d_plan + 2 * out_rows, M1, ld1, M2, ld2,
+                                                    d_plan + 3 * out_rows, nv);
+    prof_end(c, pi);
+    ctx_launched(c);
+  }
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? ST_OK : ctx_cuda(c, e, "fl launch");
+}
+
+}  // namespace lela
