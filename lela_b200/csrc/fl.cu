@@ -213,6 +213,7 @@ int zp_fl_echelonize_dev(Ctx *c, int m, int n, uint32_t p, const uint64_t *d_row
 
   // ---- B <- A^-1 B
   size_t bad = 0;
+  int ph = prof_begin(c, "fl_phase_trsm");
   if (npiv > 0) {
     st = zp_trsm_dev(c, true, false, npiv, nres, p, 1, A, npiv, B, nres, &bad);
     if (st == ST_DIAG) {
@@ -221,16 +222,22 @@ int zp_fl_echelonize_dev(Ctx *c, int m, int n, uint32_t p, const uint64_t *d_row
     }
     if (st) return st;
   }
+  prof_end(c, ph);
   // ---- D <- D - C B
+  ph = prof_begin(c, "fl_phase_schur");
   if (mres > 0 && nres > 0 && npiv > 0)
     if ((st = zp_gemm_dev(c, GEMM_AUTO, mres, nres, npiv, p, p - 1, C, npiv, B, nres, 1, D, nres,
                           nullptr)))
       return st;
+  prof_end(c, ph);
   // ---- echelon form of D
   size_t rd = 0;
   uint32_t detD = 1 % p;
   std::vector<int> dpiv;
+  ph = prof_begin(c, "fl_phase_echelon");
   if ((st = zp_echelon_dev(c, mres, nres, p, D, nres, &rd, &detD, &dpiv))) return st;
+  prof_end(c, ph);
+  ph = prof_begin(c, "fl_phase_reduce");
   det = (det * detD) % p;
   res->rank = (size_t)npiv + rd;
   res->det = (uint32_t)det;
@@ -339,6 +346,7 @@ int zp_fl_echelonize_dev(Ctx *c, int m, int n, uint32_t p, const uint64_t *d_row
       }
     }
   }
+  prof_end(c, ph);
   res->out_rows = (size_t)out_rows;
   if (out_rows > 0) {
     // kind 3 (unit row only) is encoded as a value-less row
