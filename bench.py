@@ -46,13 +46,16 @@ N = 8192
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=N)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-fl", action="store_true")
+    ap.add_argument("--fl-m", type=int, default=20000)
+    ap.add_argument("--fl-count", type=int, default=3)
     return ap.parse_args()
 
 
@@ -74,7 +77,7 @@ class ClockSampler:
         self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
         try:
             self.p = subprocess.Popen(["nvidia-smi", "--query-gpu=" + self.FIELDS,
-                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                       "--format=csv,noheader,nounits", "-lms", "100"],
                                       stdout=self.f, stderr=subprocess.DEVNULL)
         except OSError:
             self.p = None
@@ -147,7 +150,7 @@ def cpu_baseline(n, threads):
     workload, ZpModule gemm row-sliced over all host threads."""
     import oracle
     from lela_b200 import gen
-    rows = max(threads, 16)
+    rows = max(64, 8 * threads)
     A = gen.dense_zp(101, rows, n, P)
     B = gen.dense_zp(102, n, n, P)
     C = gen.dense_zp(103, rows, n, P)
@@ -164,8 +167,93 @@ def cpu_baseline(n, threads):
                       % (rows - 1, n, rows, n, n, threads, t)}
 
 
+# ----------------------------------------------------- Faugere-Lachartre
+FL_DENSITY = 0.025
+
+
+def run_fl(args, cm, stream, torch, dev, rank):
+    """FaugereLachartre::echelonize (reduced) on F4-shaped matrices over
+    Z/65521: m rows, n = 1.2 m columns, 75% pivot rows, row density 2.5%,
+    5% of the non-pivot rows dependent.  The CSR input and the dense output
+    stay on the device; each matrix is timed with CUDA events on the
+    module's stream (host orchestration between kernels included).  Also
+    timed: the plain per-matrix pipeline (same algorithm with every gemm on
+    the CUDA-core kernel)."""
+    import types
+    from lela_b200 import gen
+    m = args.fl_m
+    res = {"workload": "FL reduced echelon form, F4-shaped, p=65521, m=%d, n=%d, density %.3f, %d matrices"
+                       % (m, int(1.2 * m), FL_DENSITY, args.fl_count),
+           "unit": "ms/matrix"}
+    mats = []
+    for s in range(args.fl_count):
+        X = gen.f4_matrix(1000 + 17 * rank + s, m, P, density=FL_DENSITY)
+        T = types.SimpleNamespace(
+            m=X.m, n=X.n, nnz=X.nnz,
+            rowptr=torch.from_numpy(X.rowptr.view(np.int64)).to(dev),
+            colidx=torch.from_numpy(X.colidx.view(np.int32)).to(dev),
+            vals=torch.from_numpy(X.vals.view(np.int32)).to(dev))
+        mats.append(T)
+    R = torch.empty((m, int(1.2 * m)), dtype=torch.int32, device=dev)
+
+    def timed(T):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        _, rk, det = cm.fl_echelonize(P, T, True, False, R=R)
+        e1.record(stream)
+        cm.synchronize()
+        return e0.elapsed_time(e1), rk, det
+
+    cm.fl_echelonize(P, mats[0], True, False, R=R)  # warm-up
+    cm.synchronize()
+    cm.profile_reset()
+    cm.profile(True)
+    times, ranks = [], []
+    for T in mats:
+        t, rk, _ = timed(T)
+        times.append(t)
+        ranks.append(rk)
+    phases = {k.replace("fl_phase_", ""): round(cm.profile_read(k)[0] / len(mats), 2)
+              for k in ("fl_phase_trsm", "fl_phase_schur", "fl_phase_echelon", "fl_phase_reduce")}
+    cm.profile(False)
+    res.update({"ms_per_matrix": round(sum(times) / len(times), 2), "ms_each": [round(t, 2) for t in times],
+                "ranks": ranks, "phase_ms": phases, "nnz": [T.nnz for T in mats]})
+    if not args.no_plain:
+        cm.set_gemm_kernel(1)
+        t, rk, _ = timed(mats[0])
+        cm.set_gemm_kernel(0)
+        res["plain_ms_per_matrix"] = round(t, 2)
+        res["speedup_vs_plain"] = round(t / times[0], 2)
+    del R
+    return res
+
+
+def fl_cpu_baseline(m_target):
+    """LELA's own FaugereLachartre (oracle/_ref) on the same matrix family at
+    m = 1000 and 2000, single-threaded (LELA has no threading), fitted as
+    c*m^3 and extrapolated; labelled as such."""
+    import oracle
+    from lela_b200 import gen
+    if not oracle.have_ref():
+        return {"unavailable": "oracle/_ref not built"}
+    pts = []
+    for m in (1000, 2000):
+        X = gen.f4_matrix(500 + m, m, P, density=FL_DENSITY)
+        t0 = time.perf_counter()
+        oracle.ref_fl_echelonize_zp(P, X.m, X.n, X.rowptr, X.colidx, X.vals, 1, 0)
+        pts.append((m, time.perf_counter() - t0))
+    c = pts[-1][1] / pts[-1][0] ** 3
+    return {"kind": "reference", "cores": 1, "measured_s": {str(m): round(t, 3) for m, t in pts},
+            "extrapolated_ms_per_matrix": round(c * m_target ** 3 * 1e3, 1),
+            "extrapolation": "c*m^3 with c from the m=2000 run, at m=%d" % m_target}
+
+
 # ------------------------------------------------------------ reference
 def run_reference(args):
+    """LELA's own CPU gemm (oracle/_ref; the C restatement if LELA was not
+    built) on the bench's workload, all host threads, each step a row slice
+    of the 8192^3 gemm sized so that warm-up + steps take about two minutes."""
     rank, world, _ = dist_env()
     if rank != 0:
         return
@@ -173,29 +261,38 @@ def run_reference(args):
     from lela_b200 import gen
     threads = os.cpu_count() or 1
     n = args.n
-    rows = max(threads, 16)
-    A = gen.dense_zp(101, rows, n, P)
     B = gen.dense_zp(102, n, n, P)
-    C = gen.dense_zp(103, rows, n, P)
-    if oracle.have_ref():
-        fn, kind = (lambda: oracle.ref_gemm_zp(P, A, B, C, 1, 1, threads=threads)), "reference"
-    else:
-        fn, kind = (lambda: oracle.gemm_zp(P, A, B, C, 1, 1, threads=threads)), "port"
+    kind = "reference" if oracle.have_ref() else "port"
+
+    def run(rows):
+        A = gen.dense_zp(101, rows, n, P)
+        C = gen.dense_zp(103, rows, n, P)
+        t0 = time.perf_counter()
+        if kind == "reference":
+            oracle.ref_gemm_zp(P, A, B, C, 1, 1, threads=threads)
+        else:
+            oracle.gemm_zp(P, A, B, C, 1, 1, threads=threads)
+        return time.perf_counter() - t0
+
+    t1 = run(threads)  # calibration: one row per thread
+    budget = 120.0 / max(1, args.steps + args.warmup)
+    rows = threads * max(1, int(budget / max(t1, 1e-3)))
     for _ in range(args.warmup):
-        fn()
-    t0 = time.perf_counter()
+        run(rows)
+    tot = 0.0
     for _ in range(args.steps):
-        fn()
-    t = (time.perf_counter() - t0) / args.steps
+        tot += run(rows)
+    t = tot / args.steps
     v = 2 * rows * n * n / t / 1e9
     line = {"metric": METRIC, "value": round(v, 4), "unit": "Gop/s", "impl": "reference",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(t * 1e3, 3), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u32 (u64 accumulate)", "data": "synthetic",
-            "config": {"workload": "gemm Z/65521 %d^3 (sample: %d rows per step)" % (n, rows),
-                       "p": P, "m": n, "n": n, "k": n, "parallelism": "host threads"},
+            "config": {"workload": "gemm Z/65521 %d^3 C<-A*B+C" % n, "p": P, "m": n, "n": n, "k": n,
+                       "parallelism": "host threads (row slices)"},
             "cpu_baseline": {"value": round(v, 4), "unit": "Gop/s", "cores": threads, "kind": kind,
-                             "sample": "rows 0-%d of the %d^3 gemm per step" % (rows - 1, n)},
+                             "sample": "rows 0-%d of the %d^3 gemm per step (LELA ZpModule gemm, row-sliced)"
+                                       % (rows - 1, n)},
             "e2e": {"value": round(v, 4), "unit": "Gop/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -328,8 +425,13 @@ def run_ours(args):
                       "ms_per_step": round(te * 1e3, 3),
                       "api": "lela_cuda_gemm_zp_u32 (host pointers, pinned)"}
 
+    if not args.no_fl:
+        out["fl"] = run_fl(args, cm, stream, torch, dev, rank)
+
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(n, os.cpu_count() or 1)
+        if not args.no_fl:
+            out["fl"]["cpu_lela"] = fl_cpu_baseline(args.fl_m)
 
     cm.close()
     if world > 1:

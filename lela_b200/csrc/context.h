@@ -85,6 +85,7 @@ enum BufSlot : int {
   BUF_GF2_1 = 12,
   BUF_MISC = 13,
   BUF_FL_HEADS = 14,  // device row heads of a device CSR input
+  BUF_TINV = 15,      // inverted 64 x 64 diagonal blocks (trsm)
 };
 
 // Grow-only allocation helpers; return ST_OK or ST_NOMEM.

@@ -105,6 +105,97 @@ __global__ void __launch_bounds__(128)
     if (k < nb) B[(size_t)k * ldb + col] = x[k];
 }
 
+// Inverses of all diagonal blocks at once: block b (rows/cols 64b ..
+// 64b+nb) of the triangular A; one CTA of 64 threads per block, thread j
+// solves T x = e_j with x in registers.  Out: Tinv[b] (64 x 64, zero padded).
+template <bool UPPER>
+__global__ void __launch_bounds__(64)
+    tri_inv_blocks_kernel(const uint32_t *__restrict__ A, size_t lda, int m,
+                          const uint32_t *__restrict__ dinv, uint32_t *__restrict__ Tinv,
+                          Modulus mod, uint32_t two64) {
+  __shared__ uint32_t sT[TRI_NB][TRI_NB + 1];
+  __shared__ uint32_t sD[TRI_NB];
+  const int b = blockIdx.x;
+  const int r0 = b * TRI_NB;
+  const int nb = min(TRI_NB, m - r0);
+  const uint32_t *T = A + (size_t)r0 * lda + r0;
+  for (int e = threadIdx.x; e < TRI_NB * TRI_NB; e += blockDim.x) {
+    int r = e / TRI_NB, cc = e % TRI_NB;
+    sT[r][cc] = (r < nb && cc < nb) ? T[(size_t)r * lda + cc] : 0u;
+  }
+  for (int e = threadIdx.x; e < TRI_NB; e += blockDim.x) sD[e] = (e < nb && dinv) ? dinv[r0 + e] : 1u;
+  __syncthreads();
+  const int j = threadIdx.x;
+  const uint32_t p = (uint32_t)mod.p;
+  uint32_t x[TRI_NB];
+#pragma unroll
+  for (int k = 0; k < TRI_NB; ++k) x[k] = (k == j) ? 1u : 0u;
+  if (!UPPER) {
+#pragma unroll
+    for (int k = 0; k < TRI_NB; ++k) {
+      uint64_t s = 0;
+#pragma unroll
+      for (int q = 0; q < k; ++q) {
+        uint64_t t = (uint64_t)sT[k][q] * x[q];
+        s += t;
+        if (s < t) s += two64;
+      }
+      uint32_t r = mod_reduce(s, mod);
+      uint32_t v = x[k] >= r ? x[k] - r : x[k] + (p - r);
+      x[k] = (k < nb) ? mod_mul(v, sD[k], mod) : 0u;
+    }
+  } else {
+#pragma unroll
+    for (int k = TRI_NB - 1; k >= 0; --k) {
+      uint64_t s = 0;
+#pragma unroll
+      for (int q = k + 1; q < TRI_NB; ++q) {
+        uint64_t t = (uint64_t)sT[k][q] * x[q];
+        s += t;
+        if (s < t) s += two64;
+      }
+      uint32_t r = mod_reduce(s, mod);
+      uint32_t v = x[k] >= r ? x[k] - r : x[k] + (p - r);
+      x[k] = (k < nb) ? mod_mul(v, sD[k], mod) : 0u;
+    }
+  }
+  uint32_t *out = Tinv + (size_t)b * TRI_NB * TRI_NB;
+#pragma unroll
+  for (int k = 0; k < TRI_NB; ++k) out[k * TRI_NB + j] = (j < nb) ? x[k] : 0u;
+}
+
+// B (nb x ncols) <- alpha * Tinv * B in place: one CTA per 64-column tile
+// (the tile is read completely before it is overwritten).
+__global__ void __launch_bounds__(256)
+    tri_apply_kernel(const uint32_t *__restrict__ Tinv, int nb, uint32_t *__restrict__ B,
+                     size_t ldb, int ncols, Modulus mod, uint32_t two64, uint32_t alpha) {
+  __shared__ uint32_t sT[TRI_NB][TRI_NB + 1];
+  __shared__ uint32_t sB[TRI_NB][TRI_NB + 1];
+  const int c0 = blockIdx.x * TRI_NB;
+  for (int e = threadIdx.x; e < TRI_NB * TRI_NB; e += blockDim.x) {
+    int r = e / TRI_NB, cc = e % TRI_NB;
+    sT[r][cc] = Tinv[r * TRI_NB + cc];
+    sB[r][cc] = (r < nb && c0 + cc < ncols) ? B[(size_t)r * ldb + c0 + cc] : 0u;
+  }
+  __syncthreads();
+  const int cc = threadIdx.x & 63, r4 = threadIdx.x >> 6;  // 4 row groups of 16 rows
+  if (c0 + cc >= ncols) return;
+#pragma unroll 1
+  for (int rr = 0; rr < 16; ++rr) {
+    const int r = r4 * 16 + rr;
+    if (r >= nb) break;
+    uint64_t s = 0;
+#pragma unroll 16
+    for (int k = 0; k < TRI_NB; ++k) {
+      uint64_t t = (uint64_t)sT[r][k] * sB[k][cc];
+      s += t;
+      if (s < t) s += two64;
+    }
+    uint32_t v = mod_reduce(s, mod);
+    B[(size_t)r * ldb + c0 + cc] = (alpha == 1u) ? v : mod_mul(v, alpha, mod);
+  }
+}
+
 // C <- beta * C for an m x n block (beta in [0, p)).
 __global__ void zp_scale2_kernel(uint32_t *C, size_t ldc, int M, int N, Modulus mod,
                                  uint32_t beta) {
@@ -138,13 +229,34 @@ int tri_left_block(Ctx *c, bool upper, int nb, const uint32_t *T, size_t ldt,
   return e == cudaSuccess ? ST_OK : ctx_cuda(c, e, "tri_left launch");
 }
 
-// Recursive solve on diagonal offset `off` of the full system (dinv is the
-// inverted diagonal of the whole matrix).
-static int trsm_rec(Ctx *c, bool upper, int m, int n, uint32_t p, uint32_t alpha,
-                    const uint32_t *A, size_t lda, const uint32_t *dinv, uint32_t *B, size_t ldb,
-                    uint8_t *gemm_ws) {
+// Inverted diagonal blocks of the whole system: the leaf whose top-left
+// entry is A_base[off*(lda+1)] uses tinv + (off/64) * 64*64 (leaves start
+// at multiples of 64 because every split point is one).
+struct TriLeaves {
+  const uint32_t *A_base;
+  const uint32_t *tinv;
+};
+
+static int tri_apply_leaf(Ctx *c, const TriLeaves &L, int m, const uint32_t *A, size_t lda,
+                          uint32_t *B, size_t ldb, int n, uint32_t p, uint32_t alpha) {
+  if (n <= 0) return ST_OK;
+  const size_t off = (size_t)(A - L.A_base) / (lda + 1);
+  const uint32_t *T = L.tinv + (off / TRI_NB) * TRI_NB * TRI_NB;
+  int pi = prof_begin(c, "tri_apply");
+  tri_apply_kernel<<<(n + TRI_NB - 1) / TRI_NB, 256, 0, c->stream>>>(
+      T, m, B, ldb, n, make_modulus(p), two64_mod(p), alpha);
+  prof_end(c, pi);
+  ctx_launched(c);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? ST_OK : ctx_cuda(c, e, "tri_apply launch");
+}
+
+// Recursive solve (dinv is the inverted diagonal of the current sub-system).
+static int trsm_rec(Ctx *c, const TriLeaves &TL, bool upper, int m, int n, uint32_t p,
+                    uint32_t alpha, const uint32_t *A, size_t lda, const uint32_t *dinv,
+                    uint32_t *B, size_t ldb, uint8_t *gemm_ws) {
   if (m <= 0) return ST_OK;
-  if (m <= TRI_NB) return tri_left_block(c, upper, m, A, lda, dinv, B, ldb, n, p, alpha);
+  if (m <= TRI_NB) return tri_apply_leaf(c, TL, m, A, lda, B, ldb, n, p, alpha);
   // split at a multiple of the leaf size, near the middle
   int l = ((m / 2 + TRI_NB - 1) / TRI_NB) * TRI_NB;
   if (l >= m) l = m - TRI_NB;
@@ -152,20 +264,20 @@ static int trsm_rec(Ctx *c, bool upper, int m, int n, uint32_t p, uint32_t alpha
   uint32_t *B1 = B, *B2 = B + (size_t)l * ldb;
   int st;
   if (!upper) {
-    if ((st = trsm_rec(c, upper, l, n, p, alpha, A11, lda, dinv, B1, ldb, gemm_ws))) return st;
+    if ((st = trsm_rec(c, TL, upper, l, n, p, alpha, A11, lda, dinv, B1, ldb, gemm_ws))) return st;
     if ((st = zp_gemm_dev(c, GEMM_AUTO, m - l, n, l, p, p - 1, A21, lda, B1, ldb, alpha, B2, ldb,
                           gemm_ws)))
       return st;
-    return trsm_rec(c, upper, m - l, n, p, 1, A22, lda, dinv ? dinv + l : nullptr, B2, ldb,
+    return trsm_rec(c, TL, upper, m - l, n, p, 1, A22, lda, dinv ? dinv + l : nullptr, B2, ldb,
                     gemm_ws);
   } else {
-    if ((st = trsm_rec(c, upper, m - l, n, p, alpha, A22, lda, dinv ? dinv + l : nullptr, B2,
-                        ldb, gemm_ws)))
+    if ((st = trsm_rec(c, TL, upper, m - l, n, p, alpha, A22, lda, dinv ? dinv + l : nullptr, B2,
+                       ldb, gemm_ws)))
       return st;
     if ((st = zp_gemm_dev(c, GEMM_AUTO, l, n, m - l, p, p - 1, A12, lda, B2, ldb, alpha, B1, ldb,
                           gemm_ws)))
       return st;
-    return trsm_rec(c, upper, l, n, p, 1, A11, lda, dinv, B1, ldb, gemm_ws);
+    return trsm_rec(c, TL, upper, l, n, p, 1, A11, lda, dinv, B1, ldb, gemm_ws);
   }
 }
 
@@ -210,11 +322,27 @@ int zp_trsm_dev(Ctx *c, bool upper, bool unit, int m, int n, uint32_t p, uint32_
     }
   }
   if (n == 0) return ST_OK;
+  // inverses of all 64 x 64 diagonal blocks, in one launch
+  const int nblk = (m + TRI_NB - 1) / TRI_NB;
+  void *tb = nullptr;
+  if ((st = ctx_buffer(c, BUF_TINV, (size_t)nblk * TRI_NB * TRI_NB * 4, &tb))) return st;
+  uint32_t *tinv = static_cast<uint32_t *>(tb);
+  {
+    const uint32_t *dv = unit ? nullptr : dinv;
+    if (upper)
+      tri_inv_blocks_kernel<true><<<nblk, 64, 0, c->stream>>>(A, lda, m, dv, tinv, mod,
+                                                              two64_mod(p));
+    else
+      tri_inv_blocks_kernel<false><<<nblk, 64, 0, c->stream>>>(A, lda, m, dv, tinv, mod,
+                                                               two64_mod(p));
+    ctx_launched(c);
+  }
   void *w = nullptr;
   // the largest update is about (m/2) x n x (m/2)
   st = ctx_workspace(c, zp_gemm_workspace_bytes(p, m, n, (m + 1) / 2 + TRI_NB), &w);
   if (st) return st;
-  return trsm_rec(c, upper, m, n, p, alpha, A, lda, unit ? nullptr : dinv, B, ldb,
+  TriLeaves TL{A, tinv};
+  return trsm_rec(c, TL, upper, m, n, p, alpha, A, lda, unit ? nullptr : dinv, B, ldb,
                   static_cast<uint8_t *>(w));
 }
 
