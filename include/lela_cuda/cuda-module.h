@@ -1,0 +1,248 @@
+/* include/lela_cuda/cuda-module.h -- the CUDA module for LELA's compile-time
+ * Context/Module dispatch.
+ *
+ * With
+ *
+ *     Modular<uint32> F (65521);
+ *     Context<Modular<uint32>, CUDAModule<uint32> > ctx (F);
+ *
+ * BLAS3::gemm (ctx, a, A, B, b, C) and BLAS3::trsm (ctx, a, A, B, type,
+ * diagIsOne) on DenseMatrix<uint32> operands run on the GPU through the C
+ * ABI of include/lela_cuda.h, and FaugereLachartre<Modular<uint32>,
+ * CUDAModule<uint32> >::echelonize runs the whole Faugere-Lachartre pipeline
+ * there.  Operand combinations the GPU path does not take (sparse or
+ * transposed operands) fall through to the parent module, exactly as an
+ * unimplemented operation falls through LELA's module stack
+ * (lela/blas/context.h:109-146).
+ *
+ * Mechanism (the reference's own): a Modules class with a Tag whose Parent
+ * is the next module (ZpModule<uint32>, lela/ring/modular.h:604-626), and
+ * partial specialisations _gemm<Modular<uint32>, CUDAModule<uint32>::Tag>
+ * and _trsm<...> of the class templates in lela/blas/level3-ll.h:52-75,
+ * dispatched on MatrixStorageTypes as lela/blas/level3-modular.h:28-47 does.
+ * Errors become LELA's exceptions: DiagonalEntryNotInvertible(idx)
+ * (lela/util/error.h:83-91), WrongMatrixForm(row), LELAError.
+ *
+ * Header-only; include it after the LELA headers it names and link
+ * liblela_cuda.so.  Written to compile as C++98 like LELA itself.
+ */
+#ifndef LELA_CUDA_CUDA_MODULE_H
+#define LELA_CUDA_CUDA_MODULE_H
+
+#include <cstdlib>
+#include <vector>
+
+#include "lela/blas/context.h"
+#include "lela/blas/level3-ll.h"
+#include "lela/matrix/dense.h"
+#include "lela/matrix/sparse.h"
+#include "lela/ring/modular.h"
+#include "lela/util/error.h"
+#include "lela/algorithms/faugere-lachartre.h"
+
+#include "../lela_cuda.h"
+
+namespace LELA
+{
+
+/** Shared, reference-counted handle of the C ABI (one CUDA stream and
+ * device workspace).  The device is taken from LELA_CUDA_DEVICE (default
+ * 0).  A Context is not re-entrant (lela/blas/context.h:61-63), and neither
+ * is its handle. */
+class CUDAHandle
+{
+	struct Rep { lela_cuda_ctx *ctx; int refs; };
+	Rep *_rep;
+
+public:
+	CUDAHandle () : _rep (new Rep)
+	{
+		_rep->refs = 1;
+		_rep->ctx = 0;
+		const char *d = std::getenv ("LELA_CUDA_DEVICE");
+		int st = lela_cuda_create (&_rep->ctx, d ? std::atoi (d) : 0);
+		if (st != LELA_CUDA_OK) {
+			delete _rep;
+			_rep = 0;
+			throw LELAError ("CUDAModule: no usable B200 device (lela_cuda_create failed)");
+		}
+	}
+	CUDAHandle (const CUDAHandle &h) : _rep (h._rep) { ++_rep->refs; }
+	CUDAHandle &operator = (const CUDAHandle &h)
+	{
+		++h._rep->refs;
+		release ();
+		_rep = h._rep;
+		return *this;
+	}
+	~CUDAHandle () { release (); }
+	lela_cuda_ctx *get () const { return _rep->ctx; }
+
+private:
+	void release ()
+	{
+		if (_rep && --_rep->refs == 0) {
+			lela_cuda_destroy (_rep->ctx);
+			delete _rep;
+		}
+		_rep = 0;
+	}
+};
+
+/** Throw the LELA exception that corresponds to a C ABI status. */
+inline void lela_cuda_check (lela_cuda_ctx *ctx, int st, size_t aux = 0)
+{
+	switch (st) {
+	case LELA_CUDA_OK: return;
+	case LELA_CUDA_DIAG_NOT_INVERTIBLE: throw DiagonalEntryNotInvertible (aux);
+	case LELA_CUDA_PIVOT_NOT_INVERTIBLE: throw LELAError ("Could not invert pivot-element in the ring");
+	default: throw LELAError (lela_cuda_last_error (ctx));
+	}
+}
+
+template <class Element>
+struct CUDAModule;
+
+/** The CUDA module over Modular<uint32>: GPU gemm, trsm and
+ * Faugere-Lachartre; everything else is ZpModule<uint32>'s. */
+template <>
+struct CUDAModule<uint32> : public ZpModule<uint32>
+{
+	struct Tag { typedef ZpModule<uint32>::Tag Parent; };
+
+	CUDAHandle cuda;
+
+	CUDAModule (const Modular<uint32> &R) : ZpModule<uint32> (R) {}
+};
+
+namespace BLAS3
+{
+
+template <>
+class _gemm<Modular<uint32>, CUDAModule<uint32>::Tag>
+{
+	template <class Modules, class Matrix1, class Matrix2, class Matrix3>
+	static Matrix3 &gemm_impl (const Modular<uint32> &F, Modules &M, uint32 a, const Matrix1 &A, const Matrix2 &B, uint32 b, Matrix3 &C,
+				   MatrixStorageTypes::Generic, MatrixStorageTypes::Generic, MatrixStorageTypes::Generic)
+		{ return _gemm<Modular<uint32>, CUDAModule<uint32>::Tag::Parent>::op (F, M, a, A, B, b, C); }
+
+	template <class Modules, class Matrix1, class Matrix2, class Matrix3>
+	static Matrix3 &gemm_impl (const Modular<uint32> &F, Modules &M, uint32 a, const Matrix1 &A, const Matrix2 &B, uint32 b, Matrix3 &C,
+				   MatrixStorageTypes::Dense, MatrixStorageTypes::Dense, MatrixStorageTypes::Dense)
+	{
+		lela_check (A.coldim () == B.rowdim ());
+		lela_check (A.rowdim () == C.rowdim ());
+		lela_check (B.coldim () == C.coldim ());
+		size_t m = C.rowdim (), n = C.coldim (), k = A.coldim ();
+		if (m == 0 || n == 0)
+			return C;
+		const uint32 *pa = k ? &A[0][0] : 0, *pb = k ? &B[0][0] : 0;
+		int st = lela_cuda_gemm_zp_u32 (M.cuda.get (), m, n, k, F._modulus, a, pa, k ? A.disp () : 1,
+						pb, k ? B.disp () : 1, b, &C[0][0], C.disp ());
+		lela_cuda_check (M.cuda.get (), st);
+		return C;
+	}
+
+public:
+	template <class Modules, class Matrix1, class Matrix2, class Matrix3>
+	static Matrix3 &op (const Modular<uint32> &F, Modules &M, uint32 a, const Matrix1 &A, const Matrix2 &B, uint32 b, Matrix3 &C)
+		{ return gemm_impl (F, M, a, A, B, b, C,
+				    typename Matrix1::StorageType (),
+				    typename Matrix2::StorageType (),
+				    typename Matrix3::StorageType ()); }
+};
+
+template <>
+class _trsm<Modular<uint32>, CUDAModule<uint32>::Tag>
+{
+	template <class Modules, class Matrix1, class Matrix2>
+	static Matrix2 &trsm_impl (const Modular<uint32> &F, Modules &M, uint32 a, const Matrix1 &A, Matrix2 &B,
+				   TriangularMatrixType type, bool diagIsOne,
+				   MatrixStorageTypes::Generic, MatrixStorageTypes::Generic)
+		{ return _trsm<Modular<uint32>, CUDAModule<uint32>::Tag::Parent>::op (F, M, a, A, B, type, diagIsOne); }
+
+	template <class Modules, class Matrix1, class Matrix2>
+	static Matrix2 &trsm_impl (const Modular<uint32> &F, Modules &M, uint32 a, const Matrix1 &A, Matrix2 &B,
+				   TriangularMatrixType type, bool diagIsOne,
+				   MatrixStorageTypes::Dense, MatrixStorageTypes::Dense)
+	{
+		lela_check (A.coldim () == B.rowdim ());
+		lela_check (A.rowdim () == B.rowdim ());
+		size_t m = A.rowdim (), n = B.coldim ();
+		if (m == 0)
+			return B;
+		size_t bad = 0;
+		int st = lela_cuda_trsm_zp_u32 (M.cuda.get (), type == UpperTriangular, diagIsOne, m, n, F._modulus, a,
+						&A[0][0], A.disp (), n ? &B[0][0] : 0, n ? B.disp () : 1, &bad);
+		lela_cuda_check (M.cuda.get (), st, bad);
+		return B;
+	}
+
+public:
+	template <class Modules, class Matrix1, class Matrix2>
+	static Matrix2 &op (const Modular<uint32> &F, Modules &M, uint32 a, const Matrix1 &A, Matrix2 &B,
+			    TriangularMatrixType type, bool diagIsOne)
+		{ return trsm_impl (F, M, a, A, B, type, diagIsOne,
+				    typename Matrix1::StorageType (),
+				    typename Matrix2::StorageType ()); }
+};
+
+} // namespace BLAS3
+
+/** FaugereLachartre over Modular<uint32> with the CUDA module: the same
+ * interface as lela/algorithms/faugere-lachartre.h:40-82, the whole
+ * pipeline on the GPU.  X is read row by row (any matrix type with sparse
+ * rows: SparseMatrix<uint32>); R receives the result (resized to the
+ * reference's shape when only_D is set). */
+template <>
+class FaugereLachartre<Modular<uint32>, CUDAModule<uint32> >
+{
+	Context<Modular<uint32>, CUDAModule<uint32> > &ctx;
+
+public:
+	FaugereLachartre (Context<Modular<uint32>, CUDAModule<uint32> > &_ctx) : ctx (_ctx) {}
+
+	template <class Matrix>
+	void echelonize (Matrix &R, const Matrix &X, size_t &rank, uint32 &det, bool reduced = true, bool only_D = false)
+	{
+		const size_t m = X.rowdim (), n = X.coldim ();
+		std::vector<uint64_t> rowptr (m + 1, 0);
+		std::vector<uint32_t> colidx, vals;
+		size_t i = 0;
+		for (typename Matrix::ConstRowIterator r = X.rowBegin (); r != X.rowEnd (); ++r, ++i) {
+			for (typename Matrix::ConstRow::const_iterator e = r->begin (); e != r->end (); ++e) {
+				colidx.push_back ((uint32_t) (uint32) e->first);
+				vals.push_back ((uint32_t) e->second);
+			}
+			rowptr[i + 1] = colidx.size ();
+		}
+		std::vector<uint32_t> dense (m * n + 1);
+		size_t rk = 0, rows = 0, bad = 0;
+		uint32_t d = 1;
+		int st = lela_cuda_fl_echelonize_zp_u32 (ctx.M.cuda.get (), m, n, ctx.F._modulus, &rowptr[0],
+							 colidx.empty () ? 0 : &colidx[0], vals.empty () ? 0 : &vals[0],
+							 reduced, only_D, &dense[0], n, &rk, &d, &rows, &bad);
+		rank = rk;
+		det = d;
+		if (st == LELA_CUDA_WRONG_MATRIX_FORM)
+			throw WrongMatrixForm (bad);
+		if (st == LELA_CUDA_DIAG_NOT_INVERTIBLE)
+			return;  // the reference catches this and returns early (faugere-lachartre.tcc:790-799)
+		lela_cuda_check (ctx.M.cuda.get (), st);
+		if (only_D)
+			R.resize (rows, n);
+		i = 0;
+		for (typename Matrix::RowIterator r = R.rowBegin (); r != R.rowEnd (); ++r, ++i) {
+			r->clear ();
+			if (i >= rows)
+				continue;
+			for (size_t j = 0; j < n; ++j)
+				if (dense[i * n + j])
+					r->push_back (typename Matrix::Row::value_type (j, dense[i * n + j]));
+		}
+	}
+};
+
+} // namespace LELA
+
+#endif /* LELA_CUDA_CUDA_MODULE_H */

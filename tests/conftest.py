@@ -8,6 +8,15 @@ if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
 
+def pytest_sessionstart(session):
+    """Build the CUDA library in-tree if it is missing (nvcc cross-compiles
+    without a GPU); a GPU machine uses the prebuilt file."""
+    lib = os.path.join(ROOT, "lela_b200", "liblela_cuda.so")
+    if not os.path.exists(lib):
+        from lela_b200 import build
+        build.build()
+
+
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a B200 GPU (runs the CUDA path)")
     config.addinivalue_line("markers", "slow: long-running test")
