@@ -164,6 +164,31 @@ int lela_cuda_fl_echelonize_zp_u32_dev (lela_cuda_ctx *ctx, size_t m, size_t n, 
 					size_t ldr, size_t *rank, uint32_t *det, size_t *out_rows,
 					size_t *bad_row);
 
+/* ----------------------------------------------------------------- GF(2)
+ * Packed rows (bit j of 64-bit word w = column 64w + j), strides in words.
+ * C <- a*A*B + b*C with a, b in {0, 1}.  Replaces BLAS3::gemm over GF2 on
+ * DenseMatrix<bool>: without M4RI the generic Row*Row*Row gemm
+ * (lela/blas/level3-generic.tcc:243-263 -> lela/blas/level2-gf2.tcc:132-155),
+ * with M4RI mzd_mul/mzd_addmul (lela/blas/level3-m4ri.tcc:78-80).
+ * Kernels (lela_cuda_set_gf2_kernel): 0 = auto (tensor cores), 1 =
+ * int8-expanded tcgen05, 2 = bit-packed four-Russians on CUDA cores. */
+int lela_cuda_set_gf2_kernel (lela_cuda_ctx *ctx, int kernel);
+int lela_cuda_gemm_gf2 (lela_cuda_ctx *ctx, size_t m, size_t n, size_t k, int a,
+			const uint64_t *A, size_t lda, const uint64_t *B, size_t ldb, int b,
+			uint64_t *C, size_t ldc);
+int lela_cuda_gemm_gf2_dev (lela_cuda_ctx *ctx, size_t m, size_t n, size_t k, int a,
+			    const uint64_t *A, size_t lda, const uint64_t *B, size_t ldb, int b,
+			    uint64_t *C, size_t ldc);
+/* A (m x n) <- its non-reduced row-echelon form over GF(2), in place; *rank.
+ * Replaces EchelonForm<GF2>::echelonize on a DenseMatrix<bool> without M4RI
+ * (GaussJordan + move_L, lela/solutions/echelon-form.h:103-134), equal to
+ * Elimination::echelonize with the dense pivot rule (first row with a 1,
+ * transpositions; lela/algorithms/pivot-strategy.tcc:44-66). */
+int lela_cuda_echelon_gf2 (lela_cuda_ctx *ctx, size_t m, size_t n, uint64_t *A, size_t lda,
+			   size_t *rank);
+int lela_cuda_echelon_gf2_dev (lela_cuda_ctx *ctx, size_t m, size_t n, uint64_t *A, size_t lda,
+			       size_t *rank);
+
 /* The same tensor-core gemm for callers that cannot allocate device memory:
  * code whose device memory is owned by someone else (a host framework's
  * caching allocator, a fixed per-process budget) or that must not call

@@ -309,6 +309,41 @@ class CudaModule:
         return R[:rows.value], rk.value, det.value
 
 
+    # ------------------------------------------------------------- GF(2)
+    def set_gf2_kernel(self, kernel):
+        """0 = auto (tensor cores), 1 = int8-expanded tcgen05, 2 = M4RM."""
+        self._raise(self.L.lela_cuda_set_gf2_kernel(self.h, int(kernel)))
+
+    def gemm_gf2(self, A, B, C, n, k, a=1, b=1):
+        """C <- a*A*B + b*C over GF(2) in place; packed uint64 rows (bit j of
+        word w = column 64w + j); n, k = bit widths of C/B and A."""
+        m = C.shape[0]
+        if _is_torch(C):
+            st = self.L.lela_cuda_gemm_gf2_dev(self.h, m, n, k, int(a), _dptr(A), A.stride(0),
+                                               _dptr(B), B.stride(0), int(b), _dptr(C), C.stride(0))
+        else:
+            _check(C.dtype == np.uint64 and A.dtype == np.uint64 and B.dtype == np.uint64,
+                   "gemm_gf2: uint64 words expected")
+            st = self.L.lela_cuda_gemm_gf2(self.h, m, n, k, int(a), _ptr(A), A.strides[0] // 8,
+                                           _ptr(B), B.strides[0] // 8, int(b), _ptr(C),
+                                           C.strides[0] // 8)
+        self._raise(st)
+        return C
+
+    def echelonize_gf2(self, A, n):
+        """A <- non-reduced row-echelon form over GF(2) in place; returns
+        (A, rank)."""
+        m = A.shape[0]
+        r = _S(0)
+        if _is_torch(A):
+            st = self.L.lela_cuda_echelon_gf2_dev(self.h, m, n, _dptr(A), A.stride(0), ctypes.byref(r))
+        else:
+            _check(A.dtype == np.uint64, "echelonize_gf2: uint64 words expected")
+            st = self.L.lela_cuda_echelon_gf2(self.h, m, n, _ptr(A), A.strides[0] // 8, ctypes.byref(r))
+        self._raise(st)
+        return A, r.value
+
+
 def _is_torch(x):
     return type(x).__module__.startswith("torch")
 

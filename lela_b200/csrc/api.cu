@@ -13,6 +13,7 @@
 #include "context.h"
 #include "echelon.h"
 #include "fl.h"
+#include "gf2.h"
 #include "tri.h"
 #include "zp_gemm.h"
 
@@ -348,6 +349,86 @@ int lela_cuda_gemm_zp_u32(lela_cuda_ctx *h, size_t m, size_t n, size_t k, uint32
                      (const uint32_t *)dB, n, b, (uint32_t *)dC, n, nullptr);
   if (!st) st = d2h_matrix(c, C, dC, m, n, ldc, 4);
   if (!st) st = ctx_check_status(c, "gemm_zp_u32");
+  return st;
+}
+
+int lela_cuda_set_gf2_kernel(lela_cuda_ctx *h, int kernel) {
+  if (!h || kernel < GF2_AUTO || kernel > GF2_M4RM) return ST_ARG;
+  h->c.gf2_kernel = kernel;
+  return ST_OK;
+}
+
+int lela_cuda_gemm_gf2_dev(lela_cuda_ctx *h, size_t m, size_t n, size_t k, int a,
+                           const uint64_t *A, size_t lda, const uint64_t *B, size_t ldb, int b,
+                           uint64_t *C, size_t ldc) {
+  if (!h) return ST_ARG;
+  Ctx *c = &h->c;
+  if (m > (size_t)INT32_MAX || n > (size_t)INT32_MAX || k > (size_t)INT32_MAX)
+    return ctx_fail(c, ST_ARG, "dimension too large");
+  if ((m && n && !C) || (m && n && k && (!A || !B))) return ctx_fail(c, ST_ARG, "null pointer");
+  return gf2_gemm_dev(c, GF2_AUTO, (int)m, (int)n, (int)k, a, A, lda, B, ldb, b, C, ldc);
+}
+
+int lela_cuda_gemm_gf2(lela_cuda_ctx *h, size_t m, size_t n, size_t k, int a, const uint64_t *A,
+                       size_t lda, const uint64_t *B, size_t ldb, int b, uint64_t *C, size_t ldc) {
+  if (!h) return ST_ARG;
+  Ctx *c = &h->c;
+  if (m > (size_t)INT32_MAX || n > (size_t)INT32_MAX || k > (size_t)INT32_MAX)
+    return ctx_fail(c, ST_ARG, "dimension too large");
+  if (m == 0 || n == 0) return ST_OK;
+  const size_t nw = (n + 63) / 64, kw = (k + 63) / 64;
+  if (!C || (k && (!A || !B))) return ctx_fail(c, ST_ARG, "null pointer");
+  if (ldc < nw || (k && (lda < kw || ldb < nw)))
+    return ctx_fail(c, ST_ARG, "leading dimension smaller than the row length");
+  cudaSetDevice(c->device);
+  void *dA = nullptr, *dB = nullptr, *dC = nullptr;
+  int st = ST_OK;
+  if (k) st = ctx_stage(c, 0, m * kw * 8, &dA);
+  if (!st && k) st = ctx_stage(c, 1, k * nw * 8, &dB);
+  if (!st) st = ctx_stage(c, 2, m * nw * 8, &dC);
+  if (!st) st = ctx_clear_status(c);
+  if (!st && k) st = h2d_matrix(c, dA, A, m, kw, lda, 8);
+  if (!st && k) st = h2d_matrix(c, dB, B, k, nw, ldb, 8);
+  if (!st && (b & 1)) st = h2d_matrix(c, dC, C, m, nw, ldc, 8);
+  if (!st)
+    st = gf2_gemm_dev(c, GF2_AUTO, (int)m, (int)n, (int)k, a, (const uint64_t *)dA, kw,
+                      (const uint64_t *)dB, nw, b, (uint64_t *)dC, nw);
+  if (!st) st = d2h_matrix(c, C, dC, m, nw, ldc, 8);
+  if (!st) st = ctx_check_status(c, "gemm_gf2");
+  return st;
+}
+
+int lela_cuda_echelon_gf2_dev(lela_cuda_ctx *h, size_t m, size_t n, uint64_t *A, size_t lda,
+                              size_t *rank) {
+  if (!h || !rank) return ST_ARG;
+  Ctx *c = &h->c;
+  if (m > (size_t)INT32_MAX || n > (size_t)INT32_MAX) return ctx_fail(c, ST_ARG, "dimension too large");
+  if (m && n && !A) return ctx_fail(c, ST_ARG, "null pointer");
+  int st = gf2_echelon_dev(c, (int)m, (int)n, A, lda, rank);
+  if (!st) st = ctx_check_status(c, "echelon_gf2");
+  return st;
+}
+
+int lela_cuda_echelon_gf2(lela_cuda_ctx *h, size_t m, size_t n, uint64_t *A, size_t lda,
+                          size_t *rank) {
+  if (!h || !rank) return ST_ARG;
+  Ctx *c = &h->c;
+  if (m > (size_t)INT32_MAX || n > (size_t)INT32_MAX) return ctx_fail(c, ST_ARG, "dimension too large");
+  if (m == 0 || n == 0) {
+    *rank = 0;
+    return ST_OK;
+  }
+  const size_t nw = (n + 63) / 64;
+  if (!A) return ctx_fail(c, ST_ARG, "null pointer");
+  if (lda < nw) return ctx_fail(c, ST_ARG, "leading dimension smaller than the row length");
+  cudaSetDevice(c->device);
+  void *dA = nullptr;
+  int st = ctx_stage(c, 0, m * nw * 8, &dA);
+  if (!st) st = ctx_clear_status(c);
+  if (!st) st = h2d_matrix(c, dA, A, m, nw, lda, 8);
+  if (!st) st = gf2_echelon_dev(c, (int)m, (int)n, (uint64_t *)dA, nw, rank);
+  if (!st) st = d2h_matrix(c, A, dA, m, nw, lda, 8);
+  if (!st) st = ctx_check_status(c, "echelon_gf2");
   return st;
 }
 

@@ -23,6 +23,13 @@ enum GemmKernel : int {
   GEMM_TC = 2,     // limb-split INT8 tcgen05 gemm
 };
 
+// GF(2) gemm kernels.
+enum Gf2Kernel : int {
+  GF2_AUTO = 0,  // tensor cores
+  GF2_TC = 1,    // int8-expanded tcgen05 gemm
+  GF2_M4RM = 2,  // bit-packed four-Russians on CUDA cores
+};
+
 struct Ctx {
   int device = 0;
   int num_sms = 148;
@@ -50,6 +57,7 @@ struct Ctx {
   size_t buf_bytes[16] = {};
 
   int gemm_kernel = GEMM_AUTO;
+  int gf2_kernel = GF2_AUTO;
   std::string last_error;
 
   // Kernel launches issued through this handle (all kernels of the library).

@@ -201,12 +201,47 @@ __device__ __forceinline__ void epilogue_chunk<4>(uint32_t tcol, int gm, int gn0
   }
 }
 
-template <int L>
+// GF(2) output (OUT = 1, one limb of 0/1 bytes): the accumulator holds the
+// integer count of the row/column bit products; its parity is the GF(2)
+// product.  The 256 columns of a tile are packed into four 64-bit
+// LittleEndian words (bit j of word w = column 64w + j) and combined as
+// C <- (beta ? C : 0) XOR (alpha ? A*B : 0); bits at columns >= N are
+// cleared.
+__device__ __forceinline__ void epilogue_gf2(uint32_t tcol, int gm, int gn0, int M, int N,
+                                             uint64_t *C, size_t ldc_words, uint32_t alpha,
+                                             uint32_t beta) {
+  uint64_t word = 0;
+#pragma unroll 1
+  for (int c0 = 0; c0 < 256; c0 += 16) {
+    uint32_t r[16];
+    tmem_ld16(tcol + c0, r);
+    tmem_ld_wait();
+    uint64_t bits = 0;
+#pragma unroll
+    for (int i = 0; i < 16; ++i) bits |= (uint64_t)(r[i] & 1u) << i;
+    word |= bits << (c0 & 63);
+    if ((c0 & 63) == 48) {
+      const int wcol = gn0 + (c0 & ~63);
+      if (gm < M && wcol < N) {
+        const int valid = min(64, N - wcol);
+        const uint64_t mask = valid == 64 ? ~0ull : ((1ull << valid) - 1ull);
+        uint64_t *dst = C + (size_t)gm * ldc_words + (wcol >> 6);
+        const uint64_t old = beta ? *dst : 0ull;
+        *dst = (old ^ (alpha ? word : 0ull)) & mask;
+      }
+      word = 0;
+    }
+  }
+}
+
+template <int L, int OUT>
 __global__ void __launch_bounds__(192, 1)
     zp_gemm_tc_kernel(const __grid_constant__ CUtensorMap tmA,
-                      const __grid_constant__ CUtensorMap tmB, uint32_t *__restrict__ C,
+                      const __grid_constant__ CUtensorMap tmB, void *__restrict__ Cv,
                       size_t ldc, int M, int N, int K, Modulus mod, uint32_t alpha, uint32_t beta,
                       uint32_t *err) {
+  static_assert(OUT == 0 || L == 1, "GF(2) output uses one limb");
+  uint32_t *C = static_cast<uint32_t *>(Cv);
   using Cfg = TcCfg<L>;
   using Lay = TcLayout<L>;
   constexpr int S = Cfg::STAGES, ACC = Cfg::ACC, BN = Cfg::BN, NMMA = Cfg::NMMA;
@@ -328,9 +363,13 @@ __global__ void __launch_bounds__(192, 1)
       tc_fence_after();
       const uint32_t tbase = tmem + (uint32_t)(a * L * NMMA) + ((uint32_t)(q * 32) << 16);
       const int gm = mb * BM + row;
+      if constexpr (OUT == 0) {
 #pragma unroll 1
-      for (int c0 = 0; c0 < BN; c0 += 16)
-        epilogue_chunk<L>(tbase + c0, gm, nb * BN + c0, M, N, C, ldc, mod, alpha, beta);
+        for (int c0 = 0; c0 < BN; c0 += 16)
+          epilogue_chunk<L>(tbase + c0, gm, nb * BN + c0, M, N, C, ldc, mod, alpha, beta);
+      } else {
+        epilogue_gf2(tbase, gm, nb * BN, M, N, static_cast<uint64_t *>(Cv), ldc, alpha, beta);
+      }
       tc_fence_before();
       mbar_arrive(&tempty[a]);
     }
@@ -513,7 +552,7 @@ static int launch_tc(Ctx *c, int M, int N, int K, const Modulus &mod, uint32_t a
   using Lay = TcLayout<L>;
   static bool attr_set = false;
   if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(zp_gemm_tc_kernel<L>,
+    cudaError_t e = cudaFuncSetAttribute(zp_gemm_tc_kernel<L, 0>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, Lay::SMEM);
     if (e != cudaSuccess) return ctx_cuda(c, e, "cudaFuncSetAttribute(zp_gemm_tc)");
     attr_set = true;
@@ -544,7 +583,7 @@ static int launch_tc(Ctx *c, int M, int N, int K, const Modulus &mod, uint32_t a
     if (st) return st;
     const int grid = std::min(tiles, c->num_sms);
     int pi = prof_begin(c, "zp_gemm_tc");
-    zp_gemm_tc_kernel<L><<<grid, 192, Lay::SMEM, c->stream>>>(tmA, tmB, C, ldc, M, N, kc, mod,
+    zp_gemm_tc_kernel<L, 0><<<grid, 192, Lay::SMEM, c->stream>>>(tmA, tmB, C, ldc, M, N, kc, mod,
                                                               alpha, b, c->dstatus);
     prof_end(c, pi);
     ctx_launched(c);
@@ -669,13 +708,13 @@ int noalloc_setup(int dev, NoallocDevice *out) {
     int sms = 0;
     e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) return ST_CUDA;
-    e = cudaFuncSetAttribute(zp_gemm_tc_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = cudaFuncSetAttribute(zp_gemm_tc_kernel<1, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              TcLayout<1>::SMEM);
     if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(zp_gemm_tc_kernel<2>,
+      e = cudaFuncSetAttribute(zp_gemm_tc_kernel<2, 0>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize, TcLayout<2>::SMEM);
     if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(zp_gemm_tc_kernel<4>,
+      e = cudaFuncSetAttribute(zp_gemm_tc_kernel<4, 0>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize, TcLayout<4>::SMEM);
     if (e != cudaSuccess) return ST_CUDA;
     if (!g_noalloc_encode) {
@@ -731,7 +770,7 @@ int noalloc_launch(cudaStream_t s, const NoallocDevice &d, int M, int N, int K,
         !noalloc_map(&tmB, Bl, (uint64_t)kc, (uint64_t)N, L, (uint64_t)Kp, (uint64_t)N * Kp,
                      BK, Cfg::BN, L))
       return ST_CUDA;
-    zp_gemm_tc_kernel<L><<<std::min(tiles, d.num_sms), 192, Lay::SMEM, s>>>(
+    zp_gemm_tc_kernel<L, 0><<<std::min(tiles, d.num_sms), 192, Lay::SMEM, s>>>(
         tmA, tmB, C, ldc, M, N, kc, mod, alpha, b, err);
     b = 1;
   }
@@ -788,3 +827,39 @@ extern "C" int lela_cuda_gemm_zp_u32_noalloc(size_t m, size_t n, size_t k, uint3
   if (cudaStreamSynchronize(s) != cudaSuccess) return ST_CUDA;
   return (word & DEVERR_TIMEOUT) ? ST_TIMEOUT : ST_OK;
 }
+
+// ======================================================= GF(2) on tensor cores
+namespace lela {
+
+// C (packed GF(2) words) <- (beta ? C : 0) XOR (alpha ? A*B : 0) from 0/1
+// byte planes Ab (M x Kp, K-major) and Bb (N x Kp, K-major) of K columns:
+// the one-limb tensor-core kernel with the bit-packing epilogue.
+int gf2_gemm_tc_planes(Ctx *c, int M, int N, int K, const uint8_t *Ab, const uint8_t *Bb, int Kp,
+                       uint32_t alpha, uint32_t beta, uint64_t *C, size_t ldc_words) {
+  using Cfg = TcCfg<1>;
+  using Lay = TcLayout<1>;
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaError_t e = cudaFuncSetAttribute(zp_gemm_tc_kernel<1, 1>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, Lay::SMEM);
+    if (e != cudaSuccess) return ctx_cuda(c, e, "cudaFuncSetAttribute(gf2 tc)");
+    attr_set = true;
+  }
+  CUtensorMap tmA, tmB;
+  int st = encode_3d(c, &tmA, const_cast<uint8_t *>(Ab), (uint64_t)K, (uint64_t)M, 1,
+                     (uint64_t)Kp, (uint64_t)M * Kp, BK, BM, 1);
+  if (st) return st;
+  st = encode_3d(c, &tmB, const_cast<uint8_t *>(Bb), (uint64_t)K, (uint64_t)N, 1, (uint64_t)Kp,
+                 (uint64_t)N * Kp, BK, Cfg::BN, 1);
+  if (st) return st;
+  const int tiles = ((M + BM - 1) / BM) * ((N + Cfg::BN - 1) / Cfg::BN);
+  int pi = prof_begin(c, "gf2_gemm_tc");
+  zp_gemm_tc_kernel<1, 1><<<std::min(tiles, c->num_sms), 192, Lay::SMEM, c->stream>>>(
+      tmA, tmB, C, ldc_words, M, N, K, make_modulus(2), alpha, beta, c->dstatus);
+  prof_end(c, pi);
+  ctx_launched(c);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? ST_OK : ctx_cuda(c, e, "gf2 tc launch");
+}
+
+}  // namespace lela

@@ -22,3 +22,9 @@ int zp_gemm_dev(Ctx *c, int kernel, int M, int N, int K, uint32_t p, uint32_t al
                 uint32_t *C, size_t ldc, uint8_t *ws_override);
 
 }  // namespace lela
+
+namespace lela {
+// GF(2) product on the tensor cores from 0/1 byte planes (see zp_gemm.cu).
+int gf2_gemm_tc_planes(Ctx *c, int M, int N, int K, const uint8_t *Ab, const uint8_t *Bb, int Kp,
+                       uint32_t alpha, uint32_t beta, uint64_t *C, size_t ldc_words);
+}  // namespace lela

@@ -1,0 +1,89 @@
+"""GF(2) gemm and echelon form on the GPU against LELA's generic GF(2) path
+(the golden fixtures) and the oracle: the counterpart of
+tests/test-blas-generic-module-gf2.C and the GF(2) half of
+tests/test-gauss-jordan.C / test-elimination.C.  Bit-exact."""
+import numpy as np
+import pytest
+
+import golden_io
+import oracle
+from lela_b200 import gen
+
+KERNELS = (1, 2)  # int8-expanded tensor cores, four-Russians
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kernel", KERNELS)
+def test_gf2_gemm_golden(cuda, kernel):
+    cuda.set_gf2_kernel(kernel)
+    try:
+        for pre, m, n, k, A, B, C, R in golden_io.gf2_gemm_cases():
+            got = cuda.gemm_gf2(A, B, C.copy(), n, k, 1, 1)
+            assert np.array_equal(got, R), (kernel, pre)
+    finally:
+        cuda.set_gf2_kernel(0)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kernel", KERNELS)
+def test_gf2_gemm_against_oracle(cuda, kernel):
+    cuda.set_gf2_kernel(kernel)
+    try:
+        for seed, (m, n, k) in enumerate([(1, 1, 1), (7, 65, 63), (130, 257, 300), (300, 64, 1000),
+                                          (512, 600, 2100), (129, 1000, 64)]):
+            A = gen.dense_gf2(seed, m, k)
+            B = gen.dense_gf2(seed + 100, k, n)
+            C = gen.dense_gf2(seed + 200, m, n)
+            for a, b in ((1, 1), (1, 0), (0, 1)):
+                want = oracle.gemm_gf2(A, B, C, k, n, a, b)
+                got = cuda.gemm_gf2(A, B, C.copy(), n, k, a, b)
+                assert np.array_equal(got, want), (kernel, m, n, k, a, b)
+    finally:
+        cuda.set_gf2_kernel(0)
+
+
+@pytest.mark.gpu
+def test_gf2_gemm_kernels_agree_large(cuda):
+    """4096^3: the two kernels give the same product (and so LELA's, by the
+    tests above); Freivalds-style check on random vectors as well."""
+    n = 4096
+    A = gen.dense_gf2(1, n, n)
+    B = gen.dense_gf2(2, n, n)
+    C0 = np.zeros((n, n // 64), dtype=np.uint64)
+    outs = []
+    for kernel in KERNELS:
+        cuda.set_gf2_kernel(kernel)
+        outs.append(cuda.gemm_gf2(A, B, C0.copy(), n, n, 1, 0))
+    cuda.set_gf2_kernel(0)
+    assert np.array_equal(outs[0], outs[1])
+    a = gen.unpack_gf2(A, n).astype(np.int64)
+    b = gen.unpack_gf2(B, n).astype(np.int64)
+    c = gen.unpack_gf2(outs[0], n).astype(np.int64)
+    x = np.random.default_rng(0).integers(0, 2, size=n)
+    assert np.array_equal((c @ x) % 2, (a @ ((b @ x) % 2)) % 2)
+
+
+@pytest.mark.gpu
+def test_gf2_echelon_golden(cuda):
+    for pre, m, n, r, A, E in golden_io.gf2_echelon_cases():
+        got, gr = cuda.echelonize_gf2(A.copy(), n)
+        assert gr == r, pre
+        assert np.array_equal(got, E), pre
+
+
+@pytest.mark.gpu
+def test_gf2_echelon_against_oracle(cuda):
+    for seed, (m, n, r) in enumerate([(1, 1, 1), (5, 70, 5), (64, 64, 64), (100, 90, 40),
+                                      (300, 200, 150), (257, 513, 200), (700, 700, 650)]):
+        A = gen.planted_rank_gf2(seed, m, n, r)
+        if seed % 2:
+            A[:, 0] = 0  # a zero first word column
+        want, wr = oracle.echelon_gf2(A, n)
+        got, gr = cuda.echelonize_gf2(A.copy(), n)
+        assert gr == wr, (m, n, r)
+        assert np.array_equal(got, want), (m, n, r)
+    for seed, (m, n) in enumerate([(200, 300), (333, 129)]):
+        A = gen.dense_gf2(50 + seed, m, n)
+        want, wr = oracle.echelon_gf2(A, n)
+        got, gr = cuda.echelonize_gf2(A.copy(), n)
+        assert gr == wr and np.array_equal(got, want), (m, n)
