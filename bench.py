@@ -56,6 +56,10 @@ def parse():
     ap.add_argument("--no-fl", action="store_true")
     ap.add_argument("--fl-m", type=int, default=20000)
     ap.add_argument("--fl-count", type=int, default=3)
+    ap.add_argument("--no-gf2", action="store_true")
+    ap.add_argument("--gf2-n", type=int, default=16384)
+    ap.add_argument("--gf2-ech-n", type=int, default=32768)
+    ap.add_argument("--gf2-ech-rank", type=int, default=30000)
     return ap.parse_args()
 
 
@@ -226,6 +230,63 @@ def run_fl(args, cm, stream, torch, dev, rank):
         res["plain_ms_per_matrix"] = round(t, 2)
         res["speedup_vs_plain"] = round(t / times[0], 2)
     del R
+    return res
+
+
+def run_gf2(args, cm, stream, torch, dev):
+    """GF(2) workloads: packed gemm 16384^3 with Bernoulli(1/2) bits on both
+    kernels (int8-expanded tensor cores, bit-packed four-Russians), and the
+    echelon form of a 32768 x 32768 matrix of planted rank 30000 (product of
+    random 32768 x 30000 and 30000 x 32768 factors, formed on the device with
+    the GF(2) gemm).  Inputs resident in HBM."""
+    n = args.gf2_n
+    w = n // 64
+    res = {"gemm_workload": "GF(2) gemm %d^3, Bernoulli(1/2), packed words" % n, "unit": "ms"}
+    g = torch.Generator(device=dev)
+    g.manual_seed(7)
+
+    def rnd(rows, cols_words):
+        return torch.randint(-2 ** 63, 2 ** 63 - 1, (rows, cols_words), dtype=torch.int64,
+                             device=dev, generator=g)
+
+    A, B, C = rnd(n, w), rnd(n, w), torch.zeros((n, w), dtype=torch.int64, device=dev)
+    for kernel, name in ((1, "tc"), (2, "m4rm")):
+        cm.set_gf2_kernel(kernel)
+        cm.gemm_gf2(A, B, C, n, n, 1, 0)
+        cm.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        reps = 5
+        e0.record(stream)
+        for _ in range(reps):
+            cm.gemm_gf2(A, B, C, n, n, 1, 0)
+        e1.record(stream)
+        cm.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        res["gemm_%s_ms" % name] = round(ms, 3)
+        res["gemm_%s_Tbitop_s" % name] = round(2.0 * n ** 3 / (ms / 1e3) / 1e12, 1)
+    cm.set_gf2_kernel(0)
+    del A, B, C
+    # planted-rank echelon
+    m, r = args.gf2_ech_n, args.gf2_ech_rank
+    mw, rw = m // 64, (r + 63) // 64
+    F1 = rnd(m, rw)
+    if r % 64:
+        F1[:, -1] &= (1 << (r % 64)) - 1
+    F2 = rnd(r, mw)
+    D = torch.zeros((m, mw), dtype=torch.int64, device=dev)
+    cm.gemm_gf2(F1, F2, D, m, r, 1, 0)
+    del F1, F2
+    cm.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    _, rank = cm.echelonize_gf2(D, m)
+    e1.record(stream)
+    cm.synchronize()
+    res.update({"echelon_workload": "GF(2) echelon %d x %d, planted rank %d" % (m, m, r),
+                "echelon_ms": round(e0.elapsed_time(e1), 2), "echelon_rank": rank})
+    del D
     return res
 
 
@@ -427,6 +488,8 @@ def run_ours(args):
 
     if not args.no_fl:
         out["fl"] = run_fl(args, cm, stream, torch, dev, rank)
+    if not args.no_gf2:
+        out["gf2"] = run_gf2(args, cm, stream, torch, dev)
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(n, os.cpu_count() or 1)
