@@ -31,7 +31,7 @@
  *  LELA_CUDA_WRONG_MATRIX_FORM    -> WrongMatrixForm(row)
  *                                    (lela/algorithms/faugere-lachartre.tcc:32-41)
  *  LELA_CUDA_PIVOT_NOT_INVERTIBLE -> LELAError("Could not invert pivot-element
- *                                    in the ring") (lela/algorithms/elimination.tcc:102)
+ *                                    in the ring") (lela/algorithms/elimination.tcc:106)
  *  LELA_CUDA_ERR_ARG              -> PreconditionFailed (lela_check, lela/util/debug.h)
  */
 #ifndef LELA_CUDA_H
