@@ -189,6 +189,50 @@ int lela_cuda_echelon_gf2 (lela_cuda_ctx *ctx, size_t m, size_t n, uint64_t *A, 
 int lela_cuda_echelon_gf2_dev (lela_cuda_ctx *ctx, size_t m, size_t n, uint64_t *A, size_t lda,
 			       size_t *rank);
 
+/* --------------------------------------------------------------- batches
+ * No single LELA counterpart: these run many independent instances of the
+ * routines above (EchelonForm::echelonize on dense blocks, FaugereLachartre
+ * ::echelonize) per call, with the same results per instance.
+ *
+ * Dense Z/p echelon blocks, all matrices on the DEVICE, descriptors on the
+ * host.  kernel[i] (or NULL = all 0): 0 = automatic (blocks that fit one
+ * CTA's shared memory go to the batched kernel, the rest to the panel
+ * pipeline with tensor-core updates), 1 = batched shared-memory kernel,
+ * 2 = panel pipeline with tensor-core updates, 3 = panel pipeline with
+ * CUDA-core updates.  The shared-memory blocks are processed by one
+ * persistent launch captured in a CUDA graph.  status[i] = 0 or
+ * LELA_CUDA_PIVOT_NOT_INVERTIBLE. */
+int lela_cuda_echelon_zp_u32_batch (lela_cuda_ctx *ctx, size_t count, uint32_t *const *A,
+				    const size_t *lda, const size_t *m, const size_t *n,
+				    const uint32_t *p, const int *kernel, size_t *rank,
+				    uint32_t *det, int *status);
+/* Faugere-Lachartre on `count` CSR matrices (arrays on the DEVICE; R[i] is a
+ * device output of m[i] rows, stride ldr[i]), spread over nworkers threads
+ * with their own streams.  status[i] as for the single call. */
+int lela_cuda_fl_echelonize_zp_u32_batch (lela_cuda_ctx *ctx, size_t count, const size_t *m,
+					  const size_t *n, const uint32_t *p,
+					  const uint64_t *const *rowptr, const uint32_t *const *colidx,
+					  const uint32_t *const *vals, uint32_t *const *R,
+					  const size_t *ldr, int reduced, int nworkers, size_t *rank,
+					  uint32_t *det, int *status);
+
+/* ------------------------------------------------------------ cost model
+ * No reference counterpart (LELA chooses implementations at compile time).
+ * A fully connected FP32 network nfeat -> 64 -> 64 -> 1 with ReLU that
+ * predicts the log time of a kernel choice from block features; its choice
+ * never changes a result.  All pointers are DEVICE pointers; parameters are
+ * one float array laid out W1[nfeat][64], b1[64], W2[64][64], b2[64],
+ * W3[64], b3 (lela_cuda_mlp_param_count floats), nfeat <= 16.
+ * mlp_grad zeroes grad and loss, then writes d(MSE)/d(params) and the MSE;
+ * mlp_adam applies one Adam step (step counts from 1). */
+size_t lela_cuda_mlp_param_count (int nfeat);
+int lela_cuda_mlp_forward (lela_cuda_ctx *ctx, const float *params, int nfeat, const float *X,
+			   size_t n, float *out);
+int lela_cuda_mlp_grad (lela_cuda_ctx *ctx, const float *params, int nfeat, const float *X,
+			const float *target, size_t n, float *grad, float *loss);
+int lela_cuda_mlp_adam (lela_cuda_ctx *ctx, float *params, const float *grad, float *m, float *v,
+			size_t count, int step, float lr);
+
 /* The same tensor-core gemm for callers that cannot allocate device memory:
  * code whose device memory is owned by someone else (a host framework's
  * caching allocator, a fixed per-process budget) or that must not call

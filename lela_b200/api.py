@@ -344,6 +344,50 @@ class CudaModule:
         return A, r.value
 
 
+    # ------------------------------------------------------------- batches
+    def echelonize_batch(self, mats, ps, kernels=None):
+        """Echelon forms of many dense device blocks (torch CUDA tensors,
+        int32 storage) in place; ps = moduli; kernels per block as for
+        lela_cuda_echelon_zp_u32_batch (0 auto, 1 shared-memory batch kernel,
+        2 panels + tensor-core updates, 3 panels + CUDA-core updates).
+        Returns (ranks, dets, statuses)."""
+        n = len(mats)
+        P = (ctypes.c_void_p * n)(*[t.data_ptr() for t in mats])
+        lda = (_S * n)(*[t.stride(0) for t in mats])
+        ms = (_S * n)(*[t.shape[0] for t in mats])
+        ns = (_S * n)(*[t.shape[1] for t in mats])
+        pp = (_U * n)(*ps)
+        kk = (ctypes.c_int * n)(*(kernels or [0] * n))
+        rk = (_S * n)()
+        dt = (_U * n)()
+        stt = (ctypes.c_int * n)()
+        fn = self.L.lela_cuda_echelon_zp_u32_batch
+        fn.argtypes = [_P, _S, _P, _P, _P, _P, _P, _P, _P, _P, _P]
+        st = fn(self.h, n, ctypes.cast(P, _P), ctypes.cast(lda, _P), ctypes.cast(ms, _P),
+                ctypes.cast(ns, _P), ctypes.cast(pp, _P), ctypes.cast(kk, _P), ctypes.cast(rk, _P),
+                ctypes.cast(dt, _P), ctypes.cast(stt, _P))
+        self._raise(st)
+        return list(rk), list(dt), list(stt)
+
+    def fl_echelonize_batch(self, Xs, ps, Rs, reduced=True, nworkers=4):
+        """Faugere-Lachartre on many device CSR matrices (objects with m, n,
+        rowptr, colidx, vals as torch CUDA tensors) into device outputs Rs;
+        returns (ranks, dets, statuses)."""
+        n = len(Xs)
+        arr = lambda vals, T: (T * n)(*vals)
+        ptrs = lambda ts: (ctypes.c_void_p * n)(*[t.data_ptr() for t in ts])
+        rk, dt, stt = (_S * n)(), (_U * n)(), (ctypes.c_int * n)()
+        fn = self.L.lela_cuda_fl_echelonize_zp_u32_batch
+        fn.argtypes = [_P, _S, _P, _P, _P, _P, _P, _P, _P, _P, _I, _I, _P, _P, _P]
+        c = lambda x: ctypes.cast(x, _P)
+        st = fn(self.h, n, c(arr([X.m for X in Xs], _S)), c(arr([X.n for X in Xs], _S)),
+                c(arr(ps, _U)), c(ptrs([X.rowptr for X in Xs])), c(ptrs([X.colidx for X in Xs])),
+                c(ptrs([X.vals for X in Xs])), c(ptrs(Rs)), c(arr([R.stride(0) for R in Rs], _S)),
+                int(reduced), int(nworkers), c(rk), c(dt), c(stt))
+        self._raise(st)
+        return list(rk), list(dt), list(stt)
+
+
 def _is_torch(x):
     return type(x).__module__.startswith("torch")
 

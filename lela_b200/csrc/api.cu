@@ -4,21 +4,29 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 #include <new>
+#include <thread>
+#include <vector>
 
 #include "../../include/lela_cuda.h"
+#include "batch.h"
 #include "common.cuh"
 #include "context.h"
 #include "echelon.h"
 #include "fl.h"
 #include "gf2.h"
+#include "mlp.h"
 #include "tri.h"
 #include "zp_gemm.h"
 
 struct lela_cuda_ctx {
   lela::Ctx c;
+  // Worker handles of the batched Faugere-Lachartre entry point (each with
+  // its own stream and buffers), created on first use.
+  std::vector<lela_cuda_ctx *> workers;
 };
 
 namespace lela {
@@ -168,6 +176,8 @@ int lela_cuda_create(lela_cuda_ctx **out, int device) {
 
 int lela_cuda_destroy(lela_cuda_ctx *h) {
   if (!h) return ST_OK;
+  for (lela_cuda_ctx *w : h->workers) lela_cuda_destroy(w);
+  h->workers.clear();
   Ctx *c = &h->c;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
@@ -175,7 +185,7 @@ int lela_cuda_destroy(lela_cuda_ctx *h) {
   if (c->ws2) cudaFree(c->ws2);
   for (int i = 0; i < 4; ++i)
     if (c->stage[i]) cudaFree(c->stage[i]);
-  for (int i = 0; i < 16; ++i)
+  for (int i = 0; i < 32; ++i)
     if (c->buf[i]) cudaFree(c->buf[i]);
   if (c->dstatus) cudaFree(c->dstatus);
   if (c->hstatus) cudaFreeHost(c->hstatus);
@@ -432,6 +442,123 @@ int lela_cuda_echelon_gf2(lela_cuda_ctx *h, size_t m, size_t n, uint64_t *A, siz
   return st;
 }
 
+int lela_cuda_echelon_zp_u32_batch(lela_cuda_ctx *h, size_t count, uint32_t *const *A,
+                                   const size_t *lda, const size_t *m, const size_t *n,
+                                   const uint32_t *p, const int *kernel, size_t *rank,
+                                   uint32_t *det, int *status) {
+  if (!h) return ST_ARG;
+  Ctx *c = &h->c;
+  if (count == 0) return ST_OK;
+  if (!A || !lda || !m || !n || !p || !rank || !det || !status)
+    return ctx_fail(c, ST_ARG, "null pointer");
+  cudaSetDevice(c->device);
+  std::vector<SmallItem> small;
+  std::vector<size_t> small_idx, big_idx;
+  for (size_t i = 0; i < count; ++i) {
+    if (m[i] > (size_t)INT32_MAX || n[i] > (size_t)INT32_MAX || p[i] < 2 || (m[i] && n[i] && (!A[i] || lda[i] < n[i])))
+      return ctx_fail(c, ST_ARG, "bad batch item");
+    const int k = kernel ? kernel[i] : 0;
+    const bool fits = small_echelon_fits((int)m[i], (int)n[i]);
+    if (k == 1 && !fits) return ctx_fail(c, ST_ARG, "batch item too large for the small kernel");
+    if ((k == 0 || k == 1) && fits && m[i] && n[i]) {
+      SmallItem it{A[i], (uint64_t)lda[i], (int)m[i], (int)n[i], p[i], 0};
+      small.push_back(it);
+      small_idx.push_back(i);
+    } else {
+      big_idx.push_back(i);
+    }
+  }
+  int st = ctx_clear_status(c);
+  if (st) return st;
+  if (!small.empty()) {
+    const size_t ns = small.size();
+    void *buf = nullptr;
+    const size_t bytes = ns * (sizeof(SmallItem) + 8 + 4 + 4) + 256;
+    if ((st = ctx_buffer(c, BUF_BATCH, bytes, &buf))) return st;
+    SmallItem *d_items = (SmallItem *)buf;
+    uint64_t *d_rank = (uint64_t *)(d_items + ns);
+    uint32_t *d_det = (uint32_t *)(d_rank + ns);
+    uint32_t *d_status = d_det + ns;
+    unsigned *d_next = (unsigned *)(d_status + ns);
+    cudaError_t e = cudaMemcpyAsync(d_items, small.data(), ns * sizeof(SmallItem),
+                                    cudaMemcpyHostToDevice, c->stream);
+    if (e != cudaSuccess) return ctx_cuda(c, e, "batch: items");
+    // one persistent launch, captured in a CUDA graph and replayed once
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    if ((st = echelon_small_batch_prepare(c))) return st;
+    const bool was_profiling = c->profile;
+    c->profile = false;  // no event records inside the capture
+    e = cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal);
+    c->profile = was_profiling;
+    if (e == cudaSuccess) c->profile = false;
+    if (e != cudaSuccess) return ctx_cuda(c, e, "batch: begin capture");
+    st = echelon_small_batch_dev(c, (int)ns, d_items, d_next, d_rank, d_det, d_status);
+    e = cudaStreamEndCapture(c->stream, &graph);
+    c->profile = was_profiling;
+    if (st) {
+      if (graph) cudaGraphDestroy(graph);
+      return st;
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+    if (e == cudaSuccess) e = cudaGraphLaunch(exec, c->stream);
+    std::vector<uint64_t> hr(ns);
+    std::vector<uint32_t> hd(ns), hs(ns);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(hr.data(), d_rank, ns * 8, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(hd.data(), d_det, ns * 4, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(hs.data(), d_status, ns * 4, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return ctx_cuda(c, e, "batch: small blocks");
+    for (size_t j = 0; j < ns; ++j) {
+      const size_t i = small_idx[j];
+      rank[i] = (size_t)hr[j];
+      det[i] = hd[j];
+      status[i] = (int)hs[j];
+    }
+  }
+  const int saved = c->gemm_kernel;
+  for (size_t i : big_idx) {
+    const int k = kernel ? kernel[i] : 0;
+    c->gemm_kernel = (k == 3) ? GEMM_PLAIN : GEMM_TC;
+    size_t r = 0;
+    uint32_t d = 1;
+    int s = zp_echelon_dev(c, (int)m[i], (int)n[i], p[i], A[i], lda[i], &r, &d, nullptr);
+    if (s != ST_OK && s != ST_PIVOT) {
+      c->gemm_kernel = saved;
+      return s;
+    }
+    rank[i] = r;
+    det[i] = d;
+    status[i] = s;
+  }
+  c->gemm_kernel = saved;
+  return ctx_check_status(c, "echelon_zp_u32_batch");
+}
+
+size_t lela_cuda_mlp_param_count(int nfeat) { return mlp_param_count(nfeat); }
+
+int lela_cuda_mlp_forward(lela_cuda_ctx *h, const float *params, int nfeat, const float *X,
+                          size_t n, float *out) {
+  if (!h) return ST_ARG;
+  if (n > (size_t)INT32_MAX) return ctx_fail(&h->c, ST_ARG, "mlp: too many samples");
+  return mlp_forward_dev(&h->c, params, nfeat, X, (int)n, out);
+}
+
+int lela_cuda_mlp_grad(lela_cuda_ctx *h, const float *params, int nfeat, const float *X,
+                       const float *target, size_t n, float *grad, float *loss) {
+  if (!h) return ST_ARG;
+  if (n > (size_t)INT32_MAX) return ctx_fail(&h->c, ST_ARG, "mlp: too many samples");
+  return mlp_grad_dev(&h->c, params, nfeat, X, target, (int)n, grad, loss);
+}
+
+int lela_cuda_mlp_adam(lela_cuda_ctx *h, float *params, const float *grad, float *m, float *v,
+                       size_t count, int step, float lr) {
+  if (!h || step < 1) return ST_ARG;
+  return mlp_adam_dev(&h->c, params, grad, m, v, (int)count, step, lr);
+}
+
 static int fl_finish(Ctx *c, int st, const FlResult &r, size_t *rank, uint32_t *det,
                      size_t *out_rows, size_t *bad_row) {
   if (rank) *rank = r.rank;
@@ -515,6 +642,57 @@ int lela_cuda_fl_echelonize_zp_u32_dev(lela_cuda_ctx *h, size_t m, size_t n, uin
   st = zp_fl_echelonize_dev(c, (int)m, (int)n, p, rowptr, colidx, vals, hrow.data(), heads.data(),
                             hv.data(), reduced != 0, only_D != 0, R, ldr, &res);
   return fl_finish(c, st, res, rank, det, out_rows, bad_row);
+}
+
+int lela_cuda_fl_echelonize_zp_u32_batch(lela_cuda_ctx *h, size_t count, const size_t *m,
+                                         const size_t *n, const uint32_t *p,
+                                         const uint64_t *const *rowptr,
+                                         const uint32_t *const *colidx,
+                                         const uint32_t *const *vals, uint32_t *const *R,
+                                         const size_t *ldr, int reduced, int nworkers,
+                                         size_t *rank, uint32_t *det, int *status) {
+  if (!h) return ST_ARG;
+  Ctx *c = &h->c;
+  if (count == 0) return ST_OK;
+  if (!m || !n || !p || !rowptr || !colidx || !vals || !R || !ldr || !rank || !det || !status)
+    return ctx_fail(c, ST_ARG, "null pointer");
+  if (nworkers < 1) nworkers = 1;
+  if (nworkers > 16) nworkers = 16;
+  if ((size_t)nworkers > count) nworkers = (int)count;
+  while ((int)h->workers.size() < nworkers) {
+    lela_cuda_ctx *w = nullptr;
+    int st = lela_cuda_create(&w, c->device);
+    if (st) return ctx_fail(c, st, "batch: worker handle");
+    w->c.gemm_kernel = c->gemm_kernel;
+    h->workers.push_back(w);
+  }
+  // the caller's queued work must be done before the workers read inputs
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return ctx_cuda(c, e, "batch: synchronize");
+  // largest matrices first
+  std::vector<size_t> order(count);
+  for (size_t i = 0; i < count; ++i) order[i] = i;
+  std::sort(order.begin(), order.end(), [&](size_t a, size_t b) { return m[a] * n[a] > m[b] * n[b]; });
+  std::atomic<size_t> next(0);
+  std::atomic<int> fatal(0);
+  auto work = [&](lela_cuda_ctx *w) {
+    cudaSetDevice(w->c.device);
+    w->c.gemm_kernel = c->gemm_kernel;
+    for (size_t j = next++; j < count && !fatal.load(); j = next++) {
+      const size_t i = order[j];
+      size_t rows = 0, bad = 0;
+      int st = lela_cuda_fl_echelonize_zp_u32_dev(w, m[i], n[i], p[i], rowptr[i], colidx[i],
+                                                  vals[i], reduced, 0, R[i], ldr[i], &rank[i],
+                                                  &det[i], &rows, &bad);
+      status[i] = st;
+      if (st != ST_OK && st != ST_WRONG_FORM && st != ST_DIAG && st != ST_PIVOT) fatal = st;
+    }
+  };
+  std::vector<std::thread> th;
+  for (int t = 0; t < nworkers; ++t) th.emplace_back(work, h->workers[t]);
+  for (auto &x : th) x.join();
+  if (fatal.load()) return ctx_fail(c, fatal.load(), "batch: a worker failed");
+  return ST_OK;
 }
 
 int lela_cuda_echelon_zp_u32_dev(lela_cuda_ctx *h, size_t m, size_t n, uint32_t p, uint32_t *A,

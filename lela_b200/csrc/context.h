@@ -53,8 +53,8 @@ struct Ctx {
   size_t stage_bytes[4] = {0, 0, 0, 0};
 
   // Named grow-only device buffers of the algorithms (see BufSlot).
-  void *buf[16] = {};
-  size_t buf_bytes[16] = {};
+  void *buf[32] = {};
+  size_t buf_bytes[32] = {};
 
   int gemm_kernel = GEMM_AUTO;
   int gf2_kernel = GF2_AUTO;
@@ -94,6 +94,9 @@ enum BufSlot : int {
   BUF_MISC = 13,
   BUF_FL_HEADS = 14,  // device row heads of a device CSR input
   BUF_TINV = 15,      // inverted 64 x 64 diagonal blocks (trsm)
+  BUF_BATCH = 16,     // batch item descriptors and results
+  BUF_MLP = 17,       // cost-model scratch
+  BUF_COUNT = 18,
 };
 
 // Grow-only allocation helpers; return ST_OK or ST_NOMEM.

@@ -27,6 +27,7 @@
 // scheme as the Z/p version (echelon.cu) with 64-column panels = one word
 // per row; the trailing update is an M4RM product.
 #include <algorithm>
+#include <mutex>
 #include <vector>
 
 #include "common.cuh"
@@ -115,13 +116,13 @@ int gf2_m4rm_dev(Ctx *c, int M, int N, int K, int alpha, const uint64_t *A, size
   const uint64_t tail = (N & 63) ? ((1ull << (N & 63)) - 1ull) : ~0ull;
   dim3 grid((Nw + M4_BW - 1) / M4_BW, (M + M4_THREADS * M4_ROWS - 1) / (M4_THREADS * M4_ROWS));
   constexpr int smem = (4 * M4_BW * 256 + M4_KC * M4_BW) * 8;
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(gf2_m4rm_kernel,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    if (e != cudaSuccess) return ctx_cuda(c, e, "cudaFuncSetAttribute(gf2_m4rm)");
-    attr_set = true;
-  }
+  static std::once_flag once;
+  static cudaError_t attr_err = cudaSuccess;
+  std::call_once(once, [] {
+    attr_err = cudaFuncSetAttribute(gf2_m4rm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)((4 * M4_BW * 256 + M4_KC * M4_BW) * 8));
+  });
+  if (attr_err != cudaSuccess) return ctx_cuda(c, attr_err, "cudaFuncSetAttribute(gf2_m4rm)");
   int pi = prof_begin(c, "gf2_m4rm");
   gf2_m4rm_kernel<<<grid, M4_THREADS, smem, c->stream>>>(A, lda, B, ldb, C, ldc, M, Nw, K, tail,
                                                          alpha, beta);

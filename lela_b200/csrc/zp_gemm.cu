@@ -550,13 +550,13 @@ static int launch_tc(Ctx *c, int M, int N, int K, const Modulus &mod, uint32_t a
                      uint32_t *C, size_t ldc, uint8_t *ws) {
   using Cfg = TcCfg<L>;
   using Lay = TcLayout<L>;
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(zp_gemm_tc_kernel<L, 0>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, Lay::SMEM);
-    if (e != cudaSuccess) return ctx_cuda(c, e, "cudaFuncSetAttribute(zp_gemm_tc)");
-    attr_set = true;
-  }
+  static std::once_flag once;
+  static cudaError_t attr_err = cudaSuccess;
+  std::call_once(once, [] {
+    attr_err = cudaFuncSetAttribute(zp_gemm_tc_kernel<L, 0>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, Lay::SMEM);
+  });
+  if (attr_err != cudaSuccess) return ctx_cuda(c, attr_err, "cudaFuncSetAttribute(zp_gemm_tc)");
   const int tiles = ((M + BM - 1) / BM) * ((N + Cfg::BN - 1) / Cfg::BN);
   uint32_t b = beta;
   for (int k0 = 0; k0 < K; k0 += ZP_KCHUNK) {
@@ -838,13 +838,13 @@ int gf2_gemm_tc_planes(Ctx *c, int M, int N, int K, const uint8_t *Ab, const uin
                        uint32_t alpha, uint32_t beta, uint64_t *C, size_t ldc_words) {
   using Cfg = TcCfg<1>;
   using Lay = TcLayout<1>;
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(zp_gemm_tc_kernel<1, 1>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, Lay::SMEM);
-    if (e != cudaSuccess) return ctx_cuda(c, e, "cudaFuncSetAttribute(gf2 tc)");
-    attr_set = true;
-  }
+  static std::once_flag once;
+  static cudaError_t attr_err = cudaSuccess;
+  std::call_once(once, [] {
+    attr_err = cudaFuncSetAttribute(zp_gemm_tc_kernel<1, 1>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, Lay::SMEM);
+  });
+  if (attr_err != cudaSuccess) return ctx_cuda(c, attr_err, "cudaFuncSetAttribute(gf2 tc)");
   CUtensorMap tmA, tmB;
   int st = encode_3d(c, &tmA, const_cast<uint8_t *>(Ab), (uint64_t)K, (uint64_t)M, 1,
                      (uint64_t)Kp, (uint64_t)M * Kp, BK, BM, 1);
