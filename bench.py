@@ -26,6 +26,7 @@ value = total operations of all ranks / the slowest rank's time.
 """
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -57,6 +58,9 @@ def parse():
     ap.add_argument("--fl-m", type=int, default=20000)
     ap.add_argument("--fl-count", type=int, default=3)
     ap.add_argument("--no-gf2", action="store_true")
+    ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--batch-fl", type=int, default=12)
+    ap.add_argument("--batch-dense", type=int, default=48)
     ap.add_argument("--gf2-n", type=int, default=16384)
     ap.add_argument("--gf2-ech-n", type=int, default=32768)
     ap.add_argument("--gf2-ech-rank", type=int, default=30000)
@@ -290,6 +294,92 @@ def run_gf2(args, cm, stream, torch, dev):
     return res
 
 
+def run_batch(args, cm, stream, torch, dev):
+    """Batched workload (scaled to minutes): F4-shaped FL matrices with m
+    log-uniform in [2000, 8000] plus dense Z/p echelon blocks of sizes
+    log-uniform in [64, 4096], p in {251, 65521, 2^31-1}.
+    * ours: the FL matrices through the batched entry point (4 worker
+      streams, tensor-core gemms) and the dense blocks through one batched
+      call whose kernel per block is chosen by the MLP cost model, trained
+      first on autotuner timings of a separate set of blocks;
+    * plain: the per-matrix pipeline -- one matrix at a time on one stream
+      with every gemm on the CUDA-core kernel and every dense block through
+      the panel pipeline."""
+    import types
+    from lela_b200 import gen
+    from lela_b200 import selector as sel
+    rng = np.random.default_rng(11)
+    primes = [251, 65521, 2147483647]
+    fl_items = []
+    for i in range(args.batch_fl):
+        m = int(2 ** rng.uniform(math.log2(2000), math.log2(8000)))
+        X = gen.f4_matrix(3000 + i, m, P, density=FL_DENSITY)
+        fl_items.append(types.SimpleNamespace(
+            m=X.m, n=X.n, rowptr=torch.from_numpy(X.rowptr.view(np.int64)).to(dev),
+            colidx=torch.from_numpy(X.colidx.view(np.int32)).to(dev),
+            vals=torch.from_numpy(X.vals.view(np.int32)).to(dev)))
+    dense = []
+    for i in range(args.batch_dense):
+        s = int(2 ** rng.uniform(6, 12))
+        p = int(rng.choice(primes))
+        dense.append((torch.from_numpy(gen.dense_zp(4000 + i, s, s, p).view(np.int32)).to(dev), p))
+    Rs = [torch.empty((X.m, X.n), dtype=torch.int32, device=dev) for X in fl_items]
+    work = [torch.empty_like(A) for A, _ in dense]
+
+    # cost model from autotuner timings on separate blocks
+    t0 = time.perf_counter()
+    tuner = sel.Autotuner(cm, reps=2)
+    for i in range(24):
+        s = int(2 ** rng.uniform(6, 11.5))
+        tuner.tune_echelon(s, s, int(rng.choice(primes)), seed=9000 + i)
+    X, y = sel.records_to_xy(tuner.records)
+    model = sel.CostModel(cm, seed=1)
+    model.fit(X, y, epochs=600)
+    choose = sel.Selector(model)
+    kernels = [choose.choose("echelon", A.shape[0], A.shape[1], 0, 1.0, p.bit_length(), A.shape[0])
+               for A, p in dense]
+    tune_s = time.perf_counter() - t0
+
+    def ours():
+        for w, (A, _) in zip(work, dense):
+            w.copy_(A)
+        cm.fl_echelonize_batch(fl_items, [P] * len(fl_items), Rs, True, nworkers=4)
+        cm.echelonize_batch(work, [p for _, p in dense], kernels)
+
+    def plain():
+        for w, (A, _) in zip(work, dense):
+            w.copy_(A)
+        cm.set_gemm_kernel(1)
+        try:
+            for X, R in zip(fl_items, Rs):
+                cm.fl_echelonize(P, X, True, False, R=R)
+            cm.echelonize_batch(work, [p for _, p in dense], [3] * len(dense))
+        finally:
+            cm.set_gemm_kernel(0)
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        cm.synchronize()
+        t = time.perf_counter()
+        fn()
+        cm.synchronize()
+        torch.cuda.synchronize()
+        return (time.perf_counter() - t) * 1e3
+
+    ours()
+    t_ours = min(timed(ours) for _ in range(2))
+    plain()
+    t_plain = timed(plain)
+    return {"workload": "%d F4 matrices (m log-uniform 2000-8000, p=65521) + %d dense echelon blocks "
+                        "(64-4096, p in {251, 65521, 2^31-1})" % (len(fl_items), len(dense)),
+            "unit": "ms/batch", "ms": round(t_ours, 1), "plain_ms": round(t_plain, 1),
+            "speedup_vs_plain": round(t_plain / t_ours, 2),
+            "selector": {"kernels": {str(k): kernels.count(k) for k in sorted(set(kernels))},
+                         "tuning_and_training_s": round(tune_s, 1),
+                         "names": {str(k): sel.KERNEL_NAMES[("echelon", k)] for k in (1, 2, 3)}},
+            "timing": "host wall clock around the synchronised batch (includes host orchestration)"}
+
+
 def fl_cpu_baseline(m_target):
     """LELA's own FaugereLachartre (oracle/_ref) on the same matrix family at
     m = 1000 and 2000, single-threaded (LELA has no threading), fitted as
@@ -490,6 +580,8 @@ def run_ours(args):
         out["fl"] = run_fl(args, cm, stream, torch, dev, rank)
     if not args.no_gf2:
         out["gf2"] = run_gf2(args, cm, stream, torch, dev)
+    if not args.no_batch:
+        out["batch"] = run_batch(args, cm, stream, torch, dev)
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(n, os.cpu_count() or 1)

@@ -249,6 +249,112 @@ __global__ void panel_writeback_kernel(uint32_t *__restrict__ D, size_t ld, int 
   }
 }
 
+// Speculative fast path for dense panels.  LU without pivoting of the
+// w x w block D[i0 .. i0+w, c0 .. c0+w) (one CTA, shared memory).  When all
+// w pivots are nonzero and invertible the reference's rule picks exactly
+// these rows, in order, with no transposition: at step k row i0+k has a
+// nonzero entry in column c0+k and is the first row at or below i0+k.
+// out[0] = number of leading nonzero invertible pivots; blk = L\U (row
+// stride EW); pinv = inverted pivots; out[1] = product of the pivots.
+__global__ void __launch_bounds__(1024)
+    spec_lu_kernel(const uint32_t *__restrict__ D, size_t ld, int i0, int c0, int w, Modulus mod,
+                   uint32_t *__restrict__ blk, uint32_t *__restrict__ pinv, uint32_t *out) {
+  __shared__ uint32_t S[EW][EW + 1];
+  __shared__ uint32_t s_inv;
+  __shared__ int s_stop;
+  const uint32_t p = (uint32_t)mod.p;
+  for (int e = threadIdx.x; e < EW * EW; e += blockDim.x) {
+    int r = e / EW, j = e % EW;
+    S[r][j] = (r < w && j < w) ? D[(size_t)(i0 + r) * ld + c0 + j] : 0u;
+  }
+  if (threadIdx.x == 0) s_stop = 0;
+  __syncthreads();
+  int t = w;
+  uint32_t det = 1u % p;
+  for (int k = 0; k < w; ++k) {
+    if (threadIdx.x == 0) {
+      const uint32_t piv = S[k][k];
+      const uint32_t inv = piv ? lela_inv_u32(p, piv) : 0u;
+      if (inv == 0u) s_stop = 1;
+      s_inv = inv;
+      pinv[k] = inv;
+      det = mod_mul(det, piv, mod);
+    }
+    __syncthreads();
+    if (s_stop) {
+      t = k;
+      break;
+    }
+    const uint32_t inv = s_inv;
+    const int rem = w - k - 1;
+    for (int e = threadIdx.x; e < rem; e += blockDim.x) S[k + 1 + e][k] = mod_mul(S[k + 1 + e][k], inv, mod);
+    __syncthreads();
+    for (int e = threadIdx.x; e < rem * rem; e += blockDim.x) {
+      const int j = k + 1 + e / rem, q = k + 1 + e % rem;
+      const uint32_t l = S[j][k];
+      if (l) S[j][q] = sub_mod(S[j][q], mod_mul(l, S[k][q], mod), p);
+    }
+    __syncthreads();
+  }
+  for (int e = threadIdx.x; e < EW * EW; e += blockDim.x) blk[e] = S[e / EW][e % EW];
+  if (threadIdx.x == 0) {
+    out[0] = (uint32_t)t;
+    out[1] = det;
+  }
+}
+
+// Rows r0..m-1: L[r - r0][k] = (D[r][c..c+t) * U11^-1)_k, and the eliminated
+// block D[r][c..c+t) becomes zero.  One thread per row.
+__global__ void __launch_bounds__(128)
+    spec_right_solve_kernel(uint32_t *__restrict__ D, size_t ld, int r0, int m, int c, int t,
+                            const uint32_t *__restrict__ blk, const uint32_t *__restrict__ pinv,
+                            uint32_t *__restrict__ L, Modulus mod, uint32_t two64) {
+  __shared__ uint32_t U[EW][EW + 1];
+  __shared__ uint32_t sI[EW];
+  for (int e = threadIdx.x; e < EW * EW; e += blockDim.x) {
+    const int r = e / EW, j = e % EW;
+    U[r][j] = (r < t && j < t && j >= r) ? blk[r * EW + j] : 0u;
+  }
+  for (int e = threadIdx.x; e < EW; e += blockDim.x) sI[e] = e < t ? pinv[e] : 0u;
+  __syncthreads();
+  const int r = r0 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= m) return;
+  const uint32_t p = (uint32_t)mod.p;
+  uint32_t *row = D + (size_t)r * ld + c;
+  uint32_t x[EW];
+#pragma unroll
+  for (int k = 0; k < EW; ++k) x[k] = k < t ? row[k] : 0u;
+#pragma unroll
+  for (int k = 0; k < EW; ++k) {
+    uint64_t s = 0;
+#pragma unroll
+    for (int j = 0; j < k; ++j) {
+      const uint64_t q = (uint64_t)x[j] * U[j][k];
+      s += q;
+      if (s < q) s += two64;
+    }
+    x[k] = mod_mul(sub_mod(x[k], mod_reduce(s, mod), p), sI[k], mod);
+  }
+  uint32_t *lrow = L + (size_t)(r - r0) * t;
+#pragma unroll
+  for (int k = 0; k < EW; ++k)
+    if (k < t) {
+      lrow[k] = x[k];
+      row[k] = 0u;
+    }
+}
+
+// Pivot rows i..i+t-1, panel columns c..c+t-1 <- U11 (zeros below the
+// diagonal); L11 (unit lower, row stride EW) for the U12 solve.
+__global__ void spec_write_kernel(uint32_t *__restrict__ D, size_t ld, int i, int c, int t,
+                                  const uint32_t *__restrict__ blk, uint32_t *__restrict__ L11) {
+  for (int e = threadIdx.x; e < t * EW; e += blockDim.x) {
+    const int r = e / EW, j = e % EW;
+    if (j < t) D[(size_t)(i + r) * ld + c + j] = (j >= r) ? blk[r * EW + j] : 0u;
+    L11[r * EW + j] = (j < r) ? blk[r * EW + j] : (j == r ? 1u : 0u);
+  }
+}
+
 __global__ void zero_kernel(uint32_t *x, size_t n) {
   for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n;
        k += (size_t)gridDim.x * blockDim.x)
@@ -283,8 +389,10 @@ int zp_echelon_dev(Ctx *c, int m, int n, uint32_t p, uint32_t *D, size_t ld, siz
   const size_t l11_bytes = EW * EW * 4;
   const size_t tmp_bytes = (size_t)2 * EW * n * 4;
   void *base = nullptr;
+  const size_t spec_bytes = (size_t)(EW * EW + EW + 4) * 4;
   int st = ctx_buffer(c, BUF_ECH_0,
-                      out_bytes + i_bytes + 3 * v_bytes + l11_bytes + tmp_bytes + 1024, &base);
+                      out_bytes + i_bytes + 3 * v_bytes + l11_bytes + tmp_bytes + spec_bytes + 1024,
+                      &base);
   if (st) return st;
   uint8_t *b8 = static_cast<uint8_t *>(base);
   PanelOut *d_out = reinterpret_cast<PanelOut *>(b8);
@@ -296,15 +404,64 @@ int zp_echelon_dev(Ctx *c, int m, int n, uint32_t p, uint32_t *D, size_t ld, siz
   uint32_t *d_L21 = d_mult + (size_t)m * EW;
   uint32_t *d_L11 = d_L21 + (size_t)m * EW;
   uint32_t *d_tmp = d_L11 + EW * EW;
+  uint32_t *d_blk = d_tmp + (size_t)2 * EW * n;
+  uint32_t *d_pinv = d_blk + EW * EW;
+  uint32_t *d_spec = d_pinv + EW;
   void *gws = nullptr;
   st = ctx_workspace(c, zp_gemm_workspace_bytes(p, m, n, EW), &gws);
   if (st) return st;
+  const uint32_t t64 = two64_mod(p);
 
   PanelOut h;
   std::vector<int> at, src, dst;
   int i = 0;
+  int backoff = 1, skip = 0;  // speculation is retried less often after failures
   for (int c0 = 0; c0 < n && i < m; c0 += EW) {
     const int w = std::min(EW, n - c0);
+    if (skip > 0) {
+      --skip;
+    } else if (m - i >= w) {
+      // speculative dense panel: rows i .. i+w-1 are the pivots, in order
+      int ps = prof_begin(c, "ech_spec_lu");
+      spec_lu_kernel<<<1, 1024, 0, c->stream>>>(D, ld, i, c0, w, mod, d_blk, d_pinv, d_spec);
+      prof_end(c, ps);
+      ctx_launched(c);
+      uint32_t hs[2];
+      if ((st = sync_read(c, d_spec, hs, sizeof hs, "echelon: speculation"))) return st;
+      if ((int)hs[0] == w) {
+        backoff = 1;
+        spec_write_kernel<<<1, 1024, 0, c->stream>>>(D, ld, i, c0, w, d_blk, d_L11);
+        ctx_launched(c);
+        const int r0 = i + w, below = m - r0, rest = n - (c0 + w);
+        if (below > 0) {
+          ps = prof_begin(c, "ech_spec_solve");
+          spec_right_solve_kernel<<<(below + 127) / 128, 128, 0, c->stream>>>(
+              D, ld, r0, m, c0, w, d_blk, d_pinv, d_L21, mod, t64);
+          prof_end(c, ps);
+          ctx_launched(c);
+        }
+        if (rest > 0) {
+          uint32_t *U12 = D + (size_t)i * ld + c0 + w;
+          if ((st = tri_left_block(c, false, w, d_L11, EW, nullptr, U12, ld, rest, p, 1)))
+            return st;
+          if (below > 0) {
+            ps = prof_begin(c, "ech_update");
+            st = zp_gemm_dev(c, GEMM_AUTO, below, rest, w, p, p - 1, d_L21, (size_t)w, U12, ld, 1,
+                             D + (size_t)r0 * ld + c0 + w, ld, static_cast<uint8_t *>(gws));
+            prof_end(c, ps);
+            if (st) return st;
+          }
+        }
+        det = (det * hs[1]) % p;
+        if (pivot_cols)
+          for (int k = 0; k < w; ++k) pivot_cols->push_back(c0 + k);
+        rank += w;
+        i += w;
+        continue;
+      }
+      backoff = std::min(backoff * 2, 32);
+      skip = backoff - 1;
+    }
     int pi = prof_begin(c, "ech_panel");
     panel_kernel<<<1, 1024, 0, c->stream>>>(D, ld, i, m, c0, w, mod, d_act_row, d_act_pos, d_vals,
                                             d_mult, d_out);

@@ -26,11 +26,12 @@
 //    one 128 x (L*BN) accumulator per A-limb holds P_i0 .. P_i(L-1) side by
 //    side; L accumulators use all 512 TMEM columns for L = 2 and 4.
 //
-//    Pipeline (persistent, warp-specialised, 192 threads): warp 0 issues TMA
+//    Pipeline (persistent, warp-specialised, 320 threads): warp 0 issues TMA
 //    loads of 128-byte-swizzled K-blocks (128 bytes of K) into a ring of
 //    shared-memory stages; warp 1 issues 4*L MMAs of K = 32 per stage and
-//    releases stages with tcgen05.commit; warps 2-5 drain the accumulators
-//    (one TMEM lane = one row of C per thread).  Every wait is bounded.
+//    releases stages with tcgen05.commit; warps 2-9 drain the accumulators
+//    (one TMEM lane = one row of C per thread, two warps per lane quadrant
+//    on the two halves of the tile's columns).  Every wait is bounded.
 //
 // 2. zp_gemm_plain_kernel -- the "plain GPU form": a CUDA-core tiled gemm
 //    whose inner loop is exactly the reference's delayed-reduction dot
@@ -69,6 +70,9 @@ constexpr int BM = 128;         // rows of C per tile (UMMA M)
 constexpr int BK = 128;         // bytes (= limb elements) of K per stage
 constexpr int GROUP_M = 16;     // tile raster: 16 row-blocks per group
 constexpr int TMEM_COLS = 512;
+// warp 0: TMA, warp 1: MMA, warps 2-9: epilogue (two per TMEM lane quadrant)
+constexpr int TC_EPI_THREADS = 256;
+constexpr int TC_THREADS = 64 + TC_EPI_THREADS;
 
 template <int L>
 struct TcLayout {
@@ -209,10 +213,10 @@ __device__ __forceinline__ void epilogue_chunk<4>(uint32_t tcol, int gm, int gn0
 // cleared.
 __device__ __forceinline__ void epilogue_gf2(uint32_t tcol, int gm, int gn0, int M, int N,
                                              uint64_t *C, size_t ldc_words, uint32_t alpha,
-                                             uint32_t beta) {
+                                             uint32_t beta, int cbeg, int cend) {
   uint64_t word = 0;
 #pragma unroll 1
-  for (int c0 = 0; c0 < 256; c0 += 16) {
+  for (int c0 = cbeg; c0 < cend; c0 += 16) {
     uint32_t r[16];
     tmem_ld16(tcol + c0, r);
     tmem_ld_wait();
@@ -235,7 +239,7 @@ __device__ __forceinline__ void epilogue_gf2(uint32_t tcol, int gm, int gn0, int
 }
 
 template <int L, int OUT>
-__global__ void __launch_bounds__(192, 1)
+__global__ void __launch_bounds__(TC_THREADS, 1)
     zp_gemm_tc_kernel(const __grid_constant__ CUtensorMap tmA,
                       const __grid_constant__ CUtensorMap tmB, void *__restrict__ Cv,
                       size_t ldc, int M, int N, int K, Modulus mod, uint32_t alpha, uint32_t beta,
@@ -269,7 +273,7 @@ __global__ void __launch_bounds__(192, 1)
     }
     for (int a = 0; a < ACC; ++a) {
       mbar_init(&tfull[a], 1);
-      mbar_init(&tempty[a], 128);
+      mbar_init(&tempty[a], TC_EPI_THREADS);
     }
     mbar_init(done, 1);
     fence_barrier_init();
@@ -351,8 +355,11 @@ __global__ void __launch_bounds__(192, 1)
     }
   } else {
     // ------------------------------------------------------------ epilogue
+    // warps 2..9: two warps per TMEM lane quadrant, each on half the columns
     const int q = warp & 3;  // TMEM lane quadrant this warp may access
     const int row = q * 32 + lane;
+    const int half = (warp - 2) >> 2;
+    const int cbeg = half * (BN / 2), cend = cbeg + BN / 2;
     int it = 0;
     for (int t = blockIdx.x; t < num_tiles; t += gridDim.x, ++it) {
       int mb, nb;
@@ -365,10 +372,11 @@ __global__ void __launch_bounds__(192, 1)
       const int gm = mb * BM + row;
       if constexpr (OUT == 0) {
 #pragma unroll 1
-        for (int c0 = 0; c0 < BN; c0 += 16)
+        for (int c0 = cbeg; c0 < cend; c0 += 16)
           epilogue_chunk<L>(tbase + c0, gm, nb * BN + c0, M, N, C, ldc, mod, alpha, beta);
       } else {
-        epilogue_gf2(tbase, gm, nb * BN, M, N, static_cast<uint64_t *>(Cv), ldc, alpha, beta);
+        epilogue_gf2(tbase, gm, nb * BN, M, N, static_cast<uint64_t *>(Cv), ldc, alpha, beta,
+                     cbeg, cend);
       }
       tc_fence_before();
       mbar_arrive(&tempty[a]);
@@ -583,7 +591,7 @@ static int launch_tc(Ctx *c, int M, int N, int K, const Modulus &mod, uint32_t a
     if (st) return st;
     const int grid = std::min(tiles, c->num_sms);
     int pi = prof_begin(c, "zp_gemm_tc");
-    zp_gemm_tc_kernel<L, 0><<<grid, 192, Lay::SMEM, c->stream>>>(tmA, tmB, C, ldc, M, N, kc, mod,
+    zp_gemm_tc_kernel<L, 0><<<grid, TC_THREADS, Lay::SMEM, c->stream>>>(tmA, tmB, C, ldc, M, N, kc, mod,
                                                               alpha, b, c->dstatus);
     prof_end(c, pi);
     ctx_launched(c);
@@ -770,7 +778,7 @@ int noalloc_launch(cudaStream_t s, const NoallocDevice &d, int M, int N, int K,
         !noalloc_map(&tmB, Bl, (uint64_t)kc, (uint64_t)N, L, (uint64_t)Kp, (uint64_t)N * Kp,
                      BK, Cfg::BN, L))
       return ST_CUDA;
-    zp_gemm_tc_kernel<L, 0><<<std::min(tiles, d.num_sms), 192, Lay::SMEM, s>>>(
+    zp_gemm_tc_kernel<L, 0><<<std::min(tiles, d.num_sms), TC_THREADS, Lay::SMEM, s>>>(
         tmA, tmB, C, ldc, M, N, kc, mod, alpha, b, err);
     b = 1;
   }
@@ -854,7 +862,7 @@ int gf2_gemm_tc_planes(Ctx *c, int M, int N, int K, const uint8_t *Ab, const uin
   if (st) return st;
   const int tiles = ((M + BM - 1) / BM) * ((N + Cfg::BN - 1) / Cfg::BN);
   int pi = prof_begin(c, "gf2_gemm_tc");
-  zp_gemm_tc_kernel<1, 1><<<std::min(tiles, c->num_sms), 192, Lay::SMEM, c->stream>>>(
+  zp_gemm_tc_kernel<1, 1><<<std::min(tiles, c->num_sms), TC_THREADS, Lay::SMEM, c->stream>>>(
       tmA, tmB, C, ldc_words, M, N, K, make_modulus(2), alpha, beta, c->dstatus);
   prof_end(c, pi);
   ctx_launched(c);
