@@ -125,6 +125,22 @@ class ClockSampler:
 
 
 # --------------------------------------------------------------- helpers
+def max_over_ranks(torch, value, dev, world):
+    """The slowest rank's time: MAX all-reduce over the process group (NCCL
+    on GPUs; gloo in the CPU tests), identity on one rank."""
+    if world <= 1:
+        return float(value)
+    t = torch.tensor([float(value)], dtype=torch.float64, device=dev)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_gops(world, ops_per_step, steps, ms_max):
+    """Whole-job throughput: every rank runs `steps` replicas of the step;
+    total operations over the slowest rank's time."""
+    return world * ops_per_step * steps / (ms_max / 1e3) / 1e9
+
+
 def int8_peak_tops(torch, dev):
     """Dense int8 tensor-core peak measured here: cuBLASLt int8 gemm
     (torch._int_mm) at 8192^3, best of 5, CUDA events."""
@@ -506,12 +522,9 @@ def run_ours(args):
     sp_ms, sp_n = cm.profile_read("zp_split")
     cm.profile(False)
 
-    t = torch.tensor([ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    ms_max = float(t.item())
+    ms_max = max_over_ranks(torch, ms, dev, world)
     ops_step = 2.0 * n ** 3
-    value = world * ops_step * args.steps / (ms_max / 1e3) / 1e9
+    value = whole_job_gops(world, ops_step, args.steps, ms_max)
 
     # dominant kernel roofline: int8 tensor ops actually required
     L = 2
@@ -566,11 +579,7 @@ def run_ours(args):
         t0 = time.perf_counter()
         for _ in range(steps):
             cm.gemm(P, 1, hA, hB, 1, hC)
-        te = (time.perf_counter() - t0) / steps
-        tt = torch.tensor([te], dtype=torch.float64, device=dev)
-        if world > 1:
-            torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        te = float(tt.item())
+        te = max_over_ranks(torch, (time.perf_counter() - t0) / steps, dev, world)
         out["e2e"] = {"value": round(world * ops_step / te / 1e9, 2), "unit": "Gop/s",
                       "h2d_bytes_per_step": 3 * n * n * 4, "d2h_bytes_per_step": n * n * 4,
                       "ms_per_step": round(te * 1e3, 3),
