@@ -12,24 +12,42 @@
 // row_i * (-a/x) added.  Pivots are not normalised.
 //
 // Blocked right-looking form, exact.  The columns are taken in panels of
-// W = 64.  For a panel [c0, c0+W):
-//  1. panel_kernel (one CTA) collects the "active" rows -- rows at or below
-//     the current row with a nonzero in the panel; no other row can be a
-//     pivot of these columns or be changed by their elimination steps, so
-//     the reference's steps restricted to the panel run on the active rows
-//     alone: per column, the active row with the smallest current position
-//     and a nonzero entry is the pivot, the transposition (i, q) is recorded
-//     (tracking where active rows move), and the active rows below are
-//     eliminated inside the panel, keeping their multipliers;
-//  2. the host replays the recorded transpositions on the row positions and
-//     moves the affected rows (at most two per pivot) with one gather;
-//  3. the panel values are written back, U12 = L11^-1 A12 is solved on CUDA
-//     cores, and A22 -= L21 U12 runs on the limb-split tensor-core gemm over
-//     the rows from the first row below the pivots to the last active one.
+// W = 64.  Facts the design rests on, for one panel:
+//  * the value of a row after elimination by the panel's pivot rows
+//    U_0..U_{t-1} is the unique vector of v + span(U) that is zero in the
+//    pivot columns, whatever order the eliminations take, and so are the
+//    multipliers l (v = l U + reduced);
+//  * after the whole panel every row below the pivots is zero in all W
+//    columns (a skipped column was zero in every row at or below the
+//    current row, and every later pivot row is zero there as well);
+//  * the pivot of column c is the first row at or below the current row
+//    whose reduced entry in c is nonzero, and that entry only involves the
+//    row's entries in the pivot columns found so far and in c.
+// So per panel:
+//  1. panel_heads_kernel: each row at or below the current row records the
+//     first nonzero column of its panel part (64: none), with a histogram;
+//  2. panel_search_kernel (one CTA) replays the reference's pivot choice on
+//     a window of the first rows, held in shared memory and eliminated
+//     eagerly without division (a row W becomes y W - W[c] P for pivot row
+//     P with pivot value y), so no inverse is on this sequential path; rows
+//     below the window are reduced only when the head histogram says one of
+//     them may hold a pivot the window lacks.  The pivot inverses and the
+//     pivot rows U_k come out of parallel inversions at the end;
+//  3. the host replays the recorded transpositions and moves the affected
+//     rows (at most two per pivot) with one gather;
+//  4. panel_solve_kernel (all SMs, one warp per row): for every row from the
+//     first pivot to the last possibly nonzero row, the reference's
+//     elimination steps on its panel part give its multipliers (the L11 row
+//     of a pivot row, the L21 row otherwise); the panel becomes U_k in pivot
+//     row k and zero below;
+//  5. U12 = L11^-1 A12 on CUDA cores and A22 -= L21 U12 on the limb-split
+//     tensor-core gemm over the rows down to the last possibly nonzero row.
 // F4 Schur complements are staircase-shaped (rows sorted by head), so few
-// rows are active per panel; dense matrices make every row active and the
+// rows are touched per panel; dense matrices make every row active and the
 // scheme becomes ordinary blocked LU with LELA's pivot choice.
 #include <algorithm>
+#include <cstddef>
+#include <mutex>
 #include <vector>
 
 #include "common.cuh"
@@ -40,164 +58,409 @@
 
 namespace lela {
 
-constexpr int EW = 64;  // panel width
+constexpr int EW = 64;                     // panel width
+constexpr int PS_THREADS = 512;            // panel search CTA
+constexpr int PS_FAST = PS_THREADS / 32;   // positions tested per column by whole warps
+constexpr int PS_PARTS = PS_THREADS / EW;  // k-slices of a row-wide sum
+constexpr uint8_t HEAD_NONE = 64;
 
 struct PanelOut {
   uint32_t t;         // pivots found in the panel
   uint32_t err;       // 1: a pivot is not invertible in Modular<uint32>
-  uint32_t nact;      // active rows
-  uint32_t last_pos;  // largest final position of an active non-pivot row (or 0)
+  uint32_t pad0;
+  uint32_t last_pos;  // largest final position of a non-pivot row with a nonzero panel (or 0)
   uint32_t det;       // product of the panel's pivots
   uint32_t pad[3];
   uint32_t pcol[EW];  // pivot columns (relative to c0)
   uint32_t ti[EW];    // transposition k: (ti[k], tq[k])
   uint32_t tq[EW];
-  uint32_t prow[EW];  // active index of pivot k
 };
 
 __device__ __forceinline__ uint32_t sub_mod(uint32_t a, uint32_t b, uint32_t p) {
   return a >= b ? a - b : a + (p - b);
 }
 
-// Block-wide ordered compaction helper: returns this thread's exclusive
-// prefix of `flag` within the block and writes the block total to *total.
-__device__ __forceinline__ int block_scan_flag(int flag, int *warp_sums, int *total) {
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
-  unsigned b = __ballot_sync(0xffffffffu, flag);
-  int in_warp = __popc(b & ((1u << lane) - 1u));
-  if (lane == 0) warp_sums[wid] = __popc(b);
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    int s = 0;
-    for (int w = 0; w < nw; ++w) {
-      int v = warp_sums[w];
-      warp_sums[w] = s;
-      s += v;
-    }
-    *total = s;
+// Exact inverse of a unit x modulo p (any p < 2^32): extended Euclid on
+// unsigned remainders with 64-bit signed coefficients.  0 when gcd != 1.
+__device__ __forceinline__ uint32_t inv_exact_u32(uint32_t p, uint32_t x) {
+  uint32_t r0 = p, r1 = x;
+  int64_t s0 = 0, s1 = 1;
+  while (r1 != 0) {
+    const uint32_t q = r0 / r1;
+    const uint32_t r = r0 - q * r1;
+    r0 = r1;
+    r1 = r;
+    const int64_t s = s0 - (int64_t)q * s1;
+    s0 = s1;
+    s1 = s;
   }
-  __syncthreads();
-  int r = warp_sums[wid] + in_warp;
-  __syncthreads();
-  return r;
+  if (r0 != 1) return 0;
+  int64_t v = s0 % (int64_t)p;
+  if (v < 0) v += p;
+  return (uint32_t)v;
 }
 
-__global__ void __launch_bounds__(1024)
-    panel_kernel(const uint32_t *__restrict__ D, size_t ld, int i0, int m, int c0, int w,
-                 Modulus mod, int *__restrict__ act_row, int *__restrict__ act_pos,
-                 uint32_t *__restrict__ vals, uint32_t *__restrict__ mult, PanelOut *out) {
-  __shared__ int warp_sums[32];
-  __shared__ int s_total, s_nact;
-  __shared__ unsigned long long s_key;
-  __shared__ int s_at_i;
-  __shared__ uint32_t prow_vals[EW];
-  __shared__ uint32_t s_xinv;
-  __shared__ int s_stop;
-  const uint32_t p = (uint32_t)mod.p;
+// Row index currently at position pos: positions touched by this panel's
+// transpositions carry the panel's epoch stamp.
+__device__ __forceinline__ int row_at(int pos, const int *p2r, const int *stamp, int epoch) {
+  return stamp[pos] == epoch ? p2r[pos] : pos;
+}
 
-  // 1. active rows, in position order
-  if (threadIdx.x == 0) s_nact = 0;
-  __syncthreads();
-  for (int base = i0; base < m; base += blockDim.x) {
-    const int r = base + threadIdx.x;
-    int flag = 0;
-    if (r < m) {
-      const uint32_t *row = D + (size_t)r * ld + c0;
-      uint32_t any = 0;
-      for (int j = 0; j < w; ++j) any |= row[j];
-      flag = any != 0;
-    }
-    int off = block_scan_flag(flag, warp_sums, &s_total);
-    if (flag) act_row[s_nact + off] = r;
-    __syncthreads();
-    if (threadIdx.x == 0) s_nact += s_total;
-    __syncthreads();
+// sum of two products a*b + c*d modulo p (a, b, c, d < p < 2^32)
+__device__ __forceinline__ uint32_t mod_dot2(uint32_t a, uint32_t b, uint32_t c, uint32_t d,
+                                             const Modulus &mod, uint32_t two64) {
+  const uint64_t x = (uint64_t)a * b, y = (uint64_t)c * d;
+  uint64_t s = x + y;
+  if (s < y) s += two64;
+  return mod_reduce(s, mod);
+}
+
+// Field arithmetic for the panel kernels, in two forms chosen by the host:
+// ArithSmall for p < 2^16 (every product fits in 32 bits; Barrett reduction
+// with a 32-bit reciprocal, one correction) and ArithWide for any p < 2^32
+// (64-bit products and Barrett reduction).  Both return canonical residues.
+struct ArithSmall {
+  uint32_t p, mu;  // mu = floor(2^32 / p)
+  __host__ static ArithSmall make(uint32_t p) {
+    ArithSmall a;
+    a.p = p;
+    a.mu = (uint32_t)((1ull << 32) / p);
+    return a;
   }
-  const int nact = s_nact;
-  for (int a = threadIdx.x; a < nact; a += blockDim.x) {
-    const int r = act_row[a];
-    act_pos[a] = r;
+  __device__ __forceinline__ uint32_t red(uint32_t x) const {
+    const uint32_t r = x - __umulhi(x, mu) * p;
+    return r >= p ? r - p : r;
+  }
+  __device__ __forceinline__ uint32_t mul(uint32_t a, uint32_t b) const { return red(a * b); }
+  // a*b + c*d
+  __device__ __forceinline__ uint32_t dot2(uint32_t a, uint32_t b, uint32_t c, uint32_t d) const {
+    const uint32_t r = red(a * b) + red(c * d);
+    return r >= p ? r - p : r;
+  }
+};
+struct ArithWide {
+  Modulus mod;
+  uint32_t p, two64;
+  __host__ static ArithWide make(uint32_t p) {
+    ArithWide a;
+    a.mod = make_modulus(p);
+    a.p = p;
+    a.two64 = two64_mod(p);
+    return a;
+  }
+  __device__ __forceinline__ uint32_t mul(uint32_t a, uint32_t b) const {
+    return mod_mul(a, b, mod);
+  }
+  __device__ __forceinline__ uint32_t dot2(uint32_t a, uint32_t b, uint32_t c, uint32_t d) const {
+    return mod_dot2(a, b, c, d, mod, two64);
+  }
+};
+
+// Delayed-reduction accumulator: 64-bit sum of u32 products, 2^64 mod p
+// added back whenever the sum wraps (the reference's ZpModule dot,
+// lela/blas/level1-modular.tcc:135-181).
+__device__ __forceinline__ void acc_add(uint64_t &s, uint64_t prod, uint32_t two64) {
+  s += prod;
+  if (s < prod) s += two64;
+}
+
+// 1. First nonzero column of each row's panel part, rows i0..m-1 (one warp
+// per row); the histogram of these heads (hist[0..64], which the caller
+// has zeroed) and the largest row index with a nonzero panel (*last, which
+// the caller has set to -1).
+constexpr int HEADS_THREADS = 256;
+__global__ void __launch_bounds__(HEADS_THREADS)
+    panel_heads_kernel(const uint32_t *__restrict__ D, size_t ld, int i0, int m, int c0, int w,
+                       uint8_t *__restrict__ head, uint8_t *__restrict__ act, int *hist,
+                       int *last) {
+  __shared__ int s_last;
+  __shared__ int s_hist[EW + 1];
+  if (threadIdx.x == 0) s_last = -1;
+  if (threadIdx.x <= EW) s_hist[threadIdx.x] = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  int my_last = -1;
+  for (int r = i0 + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); r < m; r += warps) {
     const uint32_t *row = D + (size_t)r * ld + c0;
-    uint32_t *v = vals + (size_t)a * EW;
-    uint32_t *mu = mult + (size_t)a * EW;
-    for (int j = 0; j < EW; ++j) {
-      v[j] = j < w ? row[j] : 0u;
-      mu[j] = 0u;
+    const uint32_t a = lane < w ? row[lane] : 0u;
+    const uint32_t b = lane + 32 < w ? row[lane + 32] : 0u;
+    const unsigned ba = __ballot_sync(0xffffffffu, a != 0u);
+    const unsigned bb = __ballot_sync(0xffffffffu, b != 0u);
+    const int h = ba ? __ffs(ba) - 1 : (bb ? 32 + __ffs(bb) - 1 : HEAD_NONE);
+    if (lane == 0) {
+      head[r] = (uint8_t)h;
+      act[r] = h < HEAD_NONE;
+      atomicAdd(&s_hist[h], 1);
     }
+    if (h < HEAD_NONE) my_last = r;
   }
-  if (threadIdx.x == 0) s_stop = 0;
+  if (lane == 0 && my_last >= 0) atomicMax(&s_last, my_last);
+  __syncthreads();
+  if (threadIdx.x == 0 && s_last >= 0) atomicMax(last, s_last);
+  if (threadIdx.x <= EW && s_hist[threadIdx.x]) atomicAdd(&hist[threadIdx.x], s_hist[threadIdx.x]);
+}
+
+// 2. The reference's pivot choice on the panel (see the file comment).
+// The rows at positions i0 .. i0+PW_R-1 form a window kept in shared memory
+// and eliminated eagerly, without division: when the pivot row P (pivot
+// value y) is chosen, every other window row W below it becomes
+// y W - W[col] P.  So a non-pivot window row holds S_t times its row
+// reduced by the t pivots so far (S_t = y_0 ... y_{t-1}) and pivot row k
+// holds S_k U_k; the pivot of a column is the first window row, by
+// position, with a nonzero there.  Rows below the window are touched only
+// when no window row has one and the head histogram says that one of them
+// may: they are then reduced by the same recurrence, in position order.
+// At the end the S_k and the pivots x_k = y_k / S_k are inverted in
+// parallel.  Outputs: PanelOut; U (t x EW, row stride EW: the pivot rows'
+// final panel values) and the pivot inverses.  Resets *last_act to -1 and
+// hist[] to zero for the next panel.
+//
+// Window bookkeeping: perm[s] is the shared-memory slot of the row at
+// position i0 + s (double-buffered, rewritten each column), wrow[slot] its
+// row index in D.  Rows below the window are found through p2r / stamp and
+// carry in head[] a lower bound of the first nonzero column of their
+// reduced panel part; cnt[h] counts them by that bound.
+constexpr int PW_R = 80;                     // window rows
+constexpr int PW_FIND = (PW_R + 31) / 32;    // warps that test window rows
+
+template <class A>
+__global__ void __launch_bounds__(PS_THREADS)
+    panel_search_kernel(const uint32_t *__restrict__ D, size_t ld, int i0, int m, int c0, int w,
+                        A ar, uint8_t *__restrict__ head,
+                        const uint8_t *__restrict__ act, int *__restrict__ hist,
+                        int *__restrict__ last_act, int *__restrict__ p2r, int *__restrict__ stamp,
+                        int epoch, uint32_t *__restrict__ Uout, uint32_t *__restrict__ xinv_out,
+                        PanelOut *out) {
+  __shared__ uint32_t Wv[PW_R][EW];
+  __shared__ int perm[2][PW_R];
+  __shared__ int wrow[PW_R];
+  __shared__ uint32_t s_red[PS_FAST][EW];  // rows below the window, reduced (one per warp)
+  __shared__ int s_pcol[EW];
+  __shared__ uint32_t s_y[EW], s_S[EW], s_x[EW], s_sinv[EW];
+  __shared__ int s_cnt[EW + 1];
+  __shared__ int s_first[PS_FAST], s_wcnt[PS_FAST];
+  __shared__ int s_list[PS_THREADS], s_lrow[PS_THREADS], s_lhead[PS_THREADS];
+  __shared__ int s_err, s_last, s_hi;
+  const uint32_t p = ar.p;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int nw = min(PW_R, m - i0);
+  const int wend = i0 + nw;  // first position below the window
+
+  for (int e = tid; e < nw * EW; e += PS_THREADS) {
+    const int k = e / EW, c = e % EW;
+    const uint32_t *src = D + (size_t)(i0 + k) * ld + c0;
+    cp_async4(&Wv[k][c], src + (c < w ? c : 0), c < w);
+  }
+  for (int k = tid; k < nw; k += PS_THREADS) {
+    perm[0][k] = k;
+    wrow[k] = i0 + k;
+  }
+  if (tid <= EW) {
+    s_cnt[tid] = hist[tid];
+    hist[tid] = 0;
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  for (int k = tid; k < nw; k += PS_THREADS) atomicSub(&s_cnt[head[i0 + k]], 1);
   __syncthreads();
 
-  // 2. the reference's steps on the panel
-  int i = i0, t = 0;
-  uint32_t det = 1u % p;
+  int cur = 0, i = i0, t = 0;
+  uint32_t S = 1u % p;
   for (int col = 0; col < w && i < m; ++col) {
-    if (threadIdx.x == 0) {
-      s_key = ~0ull;
-      s_at_i = -1;
+    const int *pm = perm[cur];
+    // A. first window row at or below position i with a nonzero in col
+    if (wid < PW_FIND) {
+      const int s = t + tid;
+      const bool nz = s < nw && Wv[pm[s]][col] != 0u;
+      const unsigned b = __ballot_sync(0xffffffffu, nz);
+      if (lane == 0) s_first[wid] = b ? s + __ffs(b) - 1 - lane : 0x7fffffff;
     }
     __syncthreads();
-    for (int a = threadIdx.x; a < nact; a += blockDim.x) {
-      const int pos = act_pos[a];
-      if (pos >= i && vals[(size_t)a * EW + col] != 0u)
-        atomicMin(&s_key, ((unsigned long long)(unsigned)pos << 32) | (unsigned)a);
-      if (pos == i) s_at_i = a;
+    int qs = 0x7fffffff;
+    for (int k = 0; k < PW_FIND; ++k) qs = min(qs, s_first[k]);
+    if (qs == 0x7fffffff) {
+      // none in the window: rows below it whose bound allows a pivot here
+      int cand = 0;
+      if (wend < m)
+        for (int h = 0; h <= col; ++h) cand += s_cnt[h];
+      __syncthreads();  // every thread has its count before s_cnt changes
+      if (cand == 0) continue;
+      // scan them in position order: per pass the CTA lists the candidates
+      // among PS_THREADS positions (ordered compaction), then each warp
+      // reduces one of them by the t pivots, W <- y_k W - W[pcol_k] (S_k U_k),
+      // and records its exact head
+      int found = -1, fw = 0;
+      for (int base = wend; base < m && cand > 0 && found < 0; base += PS_THREADS) {
+        const int pos = base + tid;
+        int r = -1, hr = HEAD_NONE;
+        if (pos < m) {
+          r = row_at(pos, p2r, stamp, epoch);
+          hr = head[r];
+        }
+        const bool isc = hr <= col;
+        const unsigned bal = __ballot_sync(0xffffffffu, isc);
+        if (lane == 0) s_wcnt[wid] = __popc(bal);
+        __syncthreads();
+        int off = 0, ncand = 0;
+        for (int k = 0; k < PS_FAST; ++k) {
+          const int v = s_wcnt[k];
+          off += k < wid ? v : 0;
+          ncand += v;
+        }
+        if (isc) {
+          const int o = off + __popc(bal & ((1u << lane) - 1u));
+          s_list[o] = pos;
+          s_lrow[o] = r;
+          s_lhead[o] = hr;
+        }
+        __syncthreads();
+        for (int j0 = 0; j0 < ncand && found < 0; j0 += PS_FAST) {
+          const int j = j0 + wid;
+          int hit_pos = 0x7fffffff;
+          if (j < ncand) {
+            const int rj = s_lrow[j], hrj = s_lhead[j];
+            const uint32_t *v = D + (size_t)rj * ld + c0;
+            uint32_t a0 = lane < w ? v[lane] : 0u, a1 = lane + 32 < w ? v[lane + 32] : 0u;
+            for (int k = 0; k < t; ++k) {
+              const int pc = s_pcol[k];
+              const uint32_t f = __shfl_sync(0xffffffffu, pc < 32 ? a0 : a1, pc & 31);
+              const uint32_t nf = f ? p - f : 0u;
+              const uint32_t *P = Wv[pm[k]];
+              a0 = ar.dot2(s_y[k], a0, nf, P[lane]);
+              a1 = ar.dot2(s_y[k], a1, nf, P[lane + 32]);
+            }
+            s_red[wid][lane] = a0;
+            s_red[wid][lane + 32] = a1;
+            const unsigned b0 = __ballot_sync(0xffffffffu, a0 != 0u && lane >= col);
+            const unsigned b1 = __ballot_sync(0xffffffffu, a1 != 0u && lane + 32 >= col);
+            const int hn = b0 ? __ffs(b0) - 1 : (b1 ? 32 + __ffs(b1) - 1 : HEAD_NONE);
+            if (hn == col) hit_pos = s_list[j];
+            if (lane == 0 && hn != hrj) {
+              head[rj] = (uint8_t)hn;
+              atomicSub(&s_cnt[hrj], 1);
+              atomicAdd(&s_cnt[hn], 1);
+            }
+          }
+          if (lane == 0) s_first[wid] = hit_pos;
+          __syncthreads();
+          for (int k = 0; k < PS_FAST; ++k)
+            if (s_first[k] < (found < 0 ? 0x7fffffff : found)) {
+              found = s_first[k];
+              fw = k;
+            }
+          __syncthreads();  // s_first and s_red are rewritten by the next round
+        }
+        cand -= ncand;
+      }
+      if (found < 0) {
+        __syncthreads();
+        continue;
+      }
+      // the pivot comes from below the window: it takes the slot of position
+      // i, whose row goes to position `found` with the bound of its values
+      const int slot = pm[t];
+      if (wid == 0) {
+        const uint32_t b0v = Wv[slot][lane], b1v = Wv[slot][lane + 32];
+        const unsigned b0 = __ballot_sync(0xffffffffu, b0v != 0u && lane > col);
+        const unsigned b1 = __ballot_sync(0xffffffffu, b1v != 0u && lane + 32 > col);
+        const int hd = b0 ? __ffs(b0) - 1 : (b1 ? 32 + __ffs(b1) - 1 : HEAD_NONE);
+        if (lane == 0) {
+          const int ri = wrow[slot], rq = row_at(found, p2r, stamp, epoch);
+          head[ri] = (uint8_t)hd;
+          atomicAdd(&s_cnt[hd], 1);
+          atomicSub(&s_cnt[head[rq]], 1);
+          p2r[found] = ri;
+          stamp[found] = epoch;
+          wrow[slot] = rq;
+        }
+      }
+      __syncthreads();
+      if (tid < EW) Wv[slot][tid] = s_red[fw][tid];
+      if (tid == 0) s_first[0] = found;
+      __syncthreads();
+      qs = -1;  // marks "pivot now in slot pm[t]", transposition (i, found)
     }
-    __syncthreads();
-    const unsigned long long key = s_key;
-    const int ai = s_at_i;
-    __syncthreads();  // every thread has read s_key / s_at_i before they change
-    if (key == ~0ull) continue;  // no pivot in this column
-    const int ap = (int)(key & 0xffffffffu), q = (int)(key >> 32);
-    if (threadIdx.x == 0) {
-      const uint32_t x = vals[(size_t)ap * EW + col];
-      const uint32_t xinv = lela_inv_u32(p, x);
-      if (xinv == 0) s_stop = 1;
-      s_xinv = xinv;
-      det = mod_mul(det, x, mod);
-      out->pcol[t] = (uint32_t)col;
-      out->ti[t] = (uint32_t)i;
-      out->tq[t] = (uint32_t)q;
-      out->prow[t] = (uint32_t)ap;
-      if (ai >= 0 && ai != ap) act_pos[ai] = q;
-      act_pos[ap] = i;
-    }
-    for (int j = threadIdx.x; j < EW; j += blockDim.x) prow_vals[j] = vals[(size_t)ap * EW + j];
-    __syncthreads();
-    if (s_stop) break;
-    const uint32_t xinv = s_xinv;
-    // eliminate the active rows below
-    for (int a = threadIdx.x; a < nact; a += blockDim.x) {
-      if (act_pos[a] <= i) continue;
-      uint32_t *v = vals + (size_t)a * EW;
-      const uint32_t av = v[col];
-      if (av == 0u) continue;
-      const uint32_t f = mod_mul(av, xinv, mod);
-      mult[(size_t)a * EW + t] = f;
-      v[col] = 0u;
-      for (int j = col + 1; j < w; ++j) {
-        const uint32_t pj = prow_vals[j];
-        if (pj) v[j] = sub_mod(v[j], mod_mul(f, pj, mod), p);
+    // B. pivot at position slot qp; eliminate the other window rows below
+    const int qp = qs < 0 ? t : qs;
+    const int tq = qs < 0 ? s_first[0] : i0 + qs;
+    const int ps = pm[qp];
+    const uint32_t y = Wv[ps][col];
+    {
+      const int c = tid & (EW - 1);
+      if (c > col && c < w) {
+        const uint32_t pc = Wv[ps][c];
+        for (int s = t + (tid >> 6); s < nw; s += PS_PARTS) {
+          if (s == qp) continue;
+          const int pr = pm[s];
+          const uint32_t a = Wv[pr][col];
+          Wv[pr][c] = ar.dot2(y, Wv[pr][c], a ? p - a : 0u, pc);
+        }
       }
     }
+    int *pn = perm[cur ^ 1];
+    for (int s = tid; s < nw; s += PS_THREADS) pn[s] = s == t ? pm[qp] : (s == qp ? pm[t] : pm[s]);
+    if (tid == 0) {
+      s_pcol[t] = col;
+      s_y[t] = y;
+      s_S[t] = S;
+      out->pcol[t] = (uint32_t)col;
+      out->ti[t] = (uint32_t)i;
+      out->tq[t] = (uint32_t)tq;
+    }
     __syncthreads();
+    cur ^= 1;
+    S = ar.mul(S, y);
     ++i;
     ++t;
   }
-  // 3. results
-  if (threadIdx.x == 0) {
-    s_key = 0;
+
+  // inverses in parallel: S_k^-1 (exact), the pivots x_k = y_k / S_k, and
+  // the reference's inverse of each pivot (its failure is the reference's
+  // error)
+  if (tid == 0) {
+    s_err = 0;
+    s_last = -1;
+    s_hi = i - 1;
   }
   __syncthreads();
-  for (int a = threadIdx.x; a < nact; a += blockDim.x)
-    if (act_pos[a] >= i) atomicMax(&s_key, (unsigned long long)(unsigned)act_pos[a]);
+  if (tid < t) {
+    const uint32_t si = inv_exact_u32(p, s_S[tid]);
+    const uint32_t x = ar.mul(s_y[tid], si);
+    const uint32_t xi = lela_inv_u32(p, x);
+    s_sinv[tid] = si;
+    s_x[tid] = x;
+    xinv_out[tid] = xi;
+    if (si == 0u || xi == 0u) atomicOr(&s_err, 1);
+    atomicMax(&s_hi, (int)out->tq[tid]);
+  }
   __syncthreads();
-  if (threadIdx.x == 0) {
+  // U_k = (S_k U_k) / S_k; the window keeps only the columns right of the
+  // latest pivot up to date, and U_k is zero left of its pivot column
+  for (int e = tid; e < t * EW; e += PS_THREADS) {
+    const int k = e / EW, c = e % EW;
+    Uout[e] = c < s_pcol[k] ? 0u : ar.mul(Wv[perm[cur][k]][c], s_sinv[k]);
+  }
+  // last final position of a non-pivot row with a nonzero panel: window
+  // positions through their slots, positions below it up to the largest
+  // transposition target through p2r, beyond that rows have not moved
+  const int hi = s_hi;
+  for (int s = t + tid; s < nw; s += PS_THREADS)
+    if (act[wrow[perm[cur][s]]]) atomicMax(&s_last, i0 + s);
+  for (int pos = max(wend, i) + tid; pos <= hi && pos < m; pos += PS_THREADS)
+    if (act[row_at(pos, p2r, stamp, epoch)]) atomicMax(&s_last, pos);
+  __syncthreads();
+  if (tid == 0) {
+    const int la = *last_act;
+    int last = s_last;
+    if (la > hi) last = max(last, la);
+    uint32_t det = 1u % p;
+    for (int k = 0; k < t; ++k) det = ar.mul(det, s_x[k]);
     out->t = (uint32_t)t;
-    out->err = (uint32_t)s_stop;
-    out->nact = (uint32_t)nact;
-    out->last_pos = (uint32_t)s_key;
+    out->err = (uint32_t)s_err;
+    out->last_pos = (uint32_t)(last >= 0 ? last : 0);
     out->det = det;
+    *last_act = -1;
   }
 }
 
@@ -223,142 +486,60 @@ __global__ void scatter_rows_kernel(uint32_t *__restrict__ D, size_t ld, int n,
   }
 }
 
-// After the permutation: panel values of the active rows go back to D at
-// their final positions; L11 (t x t, unit lower, row stride EW) and L21
-// (rows r0..r1 by position, t columns, zero for rows without multipliers)
-// are laid out for the solve and the gemm.
-__global__ void panel_writeback_kernel(uint32_t *__restrict__ D, size_t ld, int c0, int w,
-                                       int nact, const int *__restrict__ act_pos,
-                                       const uint32_t *__restrict__ vals,
-                                       const uint32_t *__restrict__ mult, int i0, int t,
-                                       uint32_t *__restrict__ L11, uint32_t *__restrict__ L21,
-                                       int r0) {
-  for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nact; a += gridDim.x * blockDim.x) {
-    const int pos = act_pos[a];
+// 4. Rows i0..r1 at their final positions, one warp per row: the
+// reference's elimination steps on the panel part, pivot k applied with
+// multiplier l_k = v[pcol_k] / x_k (v: the row's current value) and
+// v -= l_k U_k.  Pivot row k takes the pivots before it (its L11 row, unit
+// lower, row stride EW; its panel becomes U_k); rows below take all t (their
+// L21 row of t entries; their panel becomes zero).
+constexpr int SOLVE_THREADS = 256;
+template <class A>
+__global__ void __launch_bounds__(SOLVE_THREADS)
+    panel_solve_kernel(uint32_t *__restrict__ D, size_t ld, int i0, int r1, int c0, int w, int t,
+                       const uint32_t *__restrict__ pcol, const uint32_t *__restrict__ Uin,
+                       const uint32_t *__restrict__ xinv, A ar,
+                       uint32_t *__restrict__ L11, uint32_t *__restrict__ L21) {
+  __shared__ uint32_t sU[EW][EW];
+  __shared__ uint32_t sX[EW];
+  __shared__ int sP[EW];
+  const int tid = threadIdx.x, lane = tid & 31;
+  for (int e = tid; e < t * EW; e += SOLVE_THREADS) sU[e / EW][e % EW] = Uin[e];
+  if (tid < EW) {
+    sX[tid] = tid < t ? xinv[tid] : 0u;
+    sP[tid] = tid < t ? (int)pcol[tid] : 0;
+  }
+  __syncthreads();
+  const uint32_t p = ar.p;
+  const int r0 = i0 + t;
+  const int warps = (gridDim.x * SOLVE_THREADS) >> 5;
+  for (int pos = i0 + ((blockIdx.x * SOLVE_THREADS + tid) >> 5); pos <= r1; pos += warps) {
     uint32_t *row = D + (size_t)pos * ld + c0;
-    const uint32_t *v = vals + (size_t)a * EW;
-    for (int j = 0; j < w; ++j) row[j] = v[j];
-    const uint32_t *mu = mult + (size_t)a * EW;
-    if (pos < i0 + t) {
-      const int k = pos - i0;  // pivot index
-      for (int j = 0; j < EW; ++j) L11[k * EW + j] = (j < k) ? mu[j] : (j == k ? 1u : 0u);
-    } else if (pos >= r0) {
-      uint32_t *l = L21 + (size_t)(pos - r0) * t;
-      for (int j = 0; j < t; ++j) l[j] = mu[j];
+    uint32_t a0 = lane < w ? row[lane] : 0u, a1 = lane + 32 < w ? row[lane + 32] : 0u;
+    const int kk = pos - i0, lim = kk < t ? kk : t;
+    uint32_t l0 = 0u, l1 = 0u;  // multipliers k = lane, lane + 32
+    if (__any_sync(0xffffffffu, (a0 | a1) != 0u)) {
+      for (int k = 0; k < lim; ++k) {
+        const int pc = sP[k];
+        const uint32_t f = __shfl_sync(0xffffffffu, pc < 32 ? a0 : a1, pc & 31);
+        const uint32_t l = ar.mul(f, sX[k]);
+        if (k == lane) l0 = l;
+        if (k == lane + 32) l1 = l;
+        const uint32_t nl = l ? p - l : 0u;
+        a0 = ar.dot2(1u, a0, nl, sU[k][lane]);
+        a1 = ar.dot2(1u, a1, nl, sU[k][lane + 32]);
+      }
+    }
+    if (lane < w) row[lane] = a0;
+    if (lane + 32 < w) row[lane + 32] = a1;
+    if (kk < t) {
+      L11[kk * EW + lane] = lane < kk ? l0 : (lane == kk ? 1u : 0u);
+      L11[kk * EW + lane + 32] = lane + 32 < kk ? l1 : (lane + 32 == kk ? 1u : 0u);
+    } else {
+      uint32_t *lr = L21 + (size_t)(pos - r0) * t;
+      if (lane < t) lr[lane] = l0;
+      if (lane + 32 < t) lr[lane + 32] = l1;
     }
   }
-}
-
-// Speculative fast path for dense panels.  LU without pivoting of the
-// w x w block D[i0 .. i0+w, c0 .. c0+w) (one CTA, shared memory).  When all
-// w pivots are nonzero and invertible the reference's rule picks exactly
-// these rows, in order, with no transposition: at step k row i0+k has a
-// nonzero entry in column c0+k and is the first row at or below i0+k.
-// out[0] = number of leading nonzero invertible pivots; blk = L\U (row
-// stride EW); pinv = inverted pivots; out[1] = product of the pivots.
-__global__ void __launch_bounds__(1024)
-    spec_lu_kernel(const uint32_t *__restrict__ D, size_t ld, int i0, int c0, int w, Modulus mod,
-                   uint32_t *__restrict__ blk, uint32_t *__restrict__ pinv, uint32_t *out) {
-  __shared__ uint32_t S[EW][EW + 1];
-  __shared__ uint32_t s_inv;
-  __shared__ int s_stop;
-  const uint32_t p = (uint32_t)mod.p;
-  for (int e = threadIdx.x; e < EW * EW; e += blockDim.x) {
-    int r = e / EW, j = e % EW;
-    S[r][j] = (r < w && j < w) ? D[(size_t)(i0 + r) * ld + c0 + j] : 0u;
-  }
-  if (threadIdx.x == 0) s_stop = 0;
-  __syncthreads();
-  int t = w;
-  uint32_t det = 1u % p;
-  for (int k = 0; k < w; ++k) {
-    if (threadIdx.x == 0) {
-      const uint32_t piv = S[k][k];
-      const uint32_t inv = piv ? lela_inv_u32(p, piv) : 0u;
-      if (inv == 0u) s_stop = 1;
-      s_inv = inv;
-      pinv[k] = inv;
-      det = mod_mul(det, piv, mod);
-    }
-    __syncthreads();
-    if (s_stop) {
-      t = k;
-      break;
-    }
-    const uint32_t inv = s_inv;
-    const int rem = w - k - 1;
-    for (int e = threadIdx.x; e < rem; e += blockDim.x) S[k + 1 + e][k] = mod_mul(S[k + 1 + e][k], inv, mod);
-    __syncthreads();
-    for (int e = threadIdx.x; e < rem * rem; e += blockDim.x) {
-      const int j = k + 1 + e / rem, q = k + 1 + e % rem;
-      const uint32_t l = S[j][k];
-      if (l) S[j][q] = sub_mod(S[j][q], mod_mul(l, S[k][q], mod), p);
-    }
-    __syncthreads();
-  }
-  for (int e = threadIdx.x; e < EW * EW; e += blockDim.x) blk[e] = S[e / EW][e % EW];
-  if (threadIdx.x == 0) {
-    out[0] = (uint32_t)t;
-    out[1] = det;
-  }
-}
-
-// Rows r0..m-1: L[r - r0][k] = (D[r][c..c+t) * U11^-1)_k, and the eliminated
-// block D[r][c..c+t) becomes zero.  One thread per row.
-__global__ void __launch_bounds__(128)
-    spec_right_solve_kernel(uint32_t *__restrict__ D, size_t ld, int r0, int m, int c, int t,
-                            const uint32_t *__restrict__ blk, const uint32_t *__restrict__ pinv,
-                            uint32_t *__restrict__ L, Modulus mod, uint32_t two64) {
-  __shared__ uint32_t U[EW][EW + 1];
-  __shared__ uint32_t sI[EW];
-  for (int e = threadIdx.x; e < EW * EW; e += blockDim.x) {
-    const int r = e / EW, j = e % EW;
-    U[r][j] = (r < t && j < t && j >= r) ? blk[r * EW + j] : 0u;
-  }
-  for (int e = threadIdx.x; e < EW; e += blockDim.x) sI[e] = e < t ? pinv[e] : 0u;
-  __syncthreads();
-  const int r = r0 + blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= m) return;
-  const uint32_t p = (uint32_t)mod.p;
-  uint32_t *row = D + (size_t)r * ld + c;
-  uint32_t x[EW];
-#pragma unroll
-  for (int k = 0; k < EW; ++k) x[k] = k < t ? row[k] : 0u;
-#pragma unroll
-  for (int k = 0; k < EW; ++k) {
-    uint64_t s = 0;
-#pragma unroll
-    for (int j = 0; j < k; ++j) {
-      const uint64_t q = (uint64_t)x[j] * U[j][k];
-      s += q;
-      if (s < q) s += two64;
-    }
-    x[k] = mod_mul(sub_mod(x[k], mod_reduce(s, mod), p), sI[k], mod);
-  }
-  uint32_t *lrow = L + (size_t)(r - r0) * t;
-#pragma unroll
-  for (int k = 0; k < EW; ++k)
-    if (k < t) {
-      lrow[k] = x[k];
-      row[k] = 0u;
-    }
-}
-
-// Pivot rows i..i+t-1, panel columns c..c+t-1 <- U11 (zeros below the
-// diagonal); L11 (unit lower, row stride EW) for the U12 solve.
-__global__ void spec_write_kernel(uint32_t *__restrict__ D, size_t ld, int i, int c, int t,
-                                  const uint32_t *__restrict__ blk, uint32_t *__restrict__ L11) {
-  for (int e = threadIdx.x; e < t * EW; e += blockDim.x) {
-    const int r = e / EW, j = e % EW;
-    if (j < t) D[(size_t)(i + r) * ld + c + j] = (j >= r) ? blk[r * EW + j] : 0u;
-    L11[r * EW + j] = (j < r) ? blk[r * EW + j] : (j == r ? 1u : 0u);
-  }
-}
-
-__global__ void zero_kernel(uint32_t *x, size_t n) {
-  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n;
-       k += (size_t)gridDim.x * blockDim.x)
-    x[k] = 0u;
 }
 
 static int sync_read(Ctx *c, const void *dev, void *host, size_t bytes, const char *what) {
@@ -380,93 +561,69 @@ int zp_echelon_dev(Ctx *c, int m, int n, uint32_t p, uint32_t *D, size_t ld, siz
     *det_out = (uint32_t)det;
     return ST_OK;
   }
-  const Modulus mod = make_modulus(p);
 
   // device scratch
   const size_t out_bytes = (sizeof(PanelOut) + 255) & ~(size_t)255;
-  const size_t i_bytes = (((size_t)2 * m + 4 * EW) * sizeof(int) + 255) & ~(size_t)255;
-  const size_t v_bytes = (size_t)m * EW * 4;
-  const size_t l11_bytes = EW * EW * 4;
+  // p2r, stamp (m each); permutation lists (4 EW); last row (1); histogram (EW + 1)
+  const size_t i_bytes =
+      (((size_t)2 * m + 4 * EW + 1 + EW + 1) * sizeof(int) + 255) & ~(size_t)255;
+  const size_t h_bytes = ((size_t)2 * m + 255) & ~(size_t)255;
+  const size_t sq_bytes = (size_t)EW * EW * 4;
+  const size_t l21_bytes = (size_t)m * EW * 4;
   const size_t tmp_bytes = (size_t)2 * EW * n * 4;
   void *base = nullptr;
-  const size_t spec_bytes = (size_t)(EW * EW + EW + 4) * 4;
   int st = ctx_buffer(c, BUF_ECH_0,
-                      out_bytes + i_bytes + 3 * v_bytes + l11_bytes + tmp_bytes + spec_bytes + 1024,
+                      out_bytes + i_bytes + h_bytes + 3 * sq_bytes + l21_bytes + tmp_bytes + 1024,
                       &base);
   if (st) return st;
   uint8_t *b8 = static_cast<uint8_t *>(base);
   PanelOut *d_out = reinterpret_cast<PanelOut *>(b8);
-  int *d_act_row = reinterpret_cast<int *>(b8 + out_bytes);
-  int *d_act_pos = d_act_row + m;
-  int *d_perm = d_act_pos + m;  // 4*EW ints: src list, dst list
-  uint32_t *d_vals = reinterpret_cast<uint32_t *>(b8 + out_bytes + i_bytes);
-  uint32_t *d_mult = d_vals + (size_t)m * EW;
-  uint32_t *d_L21 = d_mult + (size_t)m * EW;
-  uint32_t *d_L11 = d_L21 + (size_t)m * EW;
-  uint32_t *d_tmp = d_L11 + EW * EW;
-  uint32_t *d_blk = d_tmp + (size_t)2 * EW * n;
-  uint32_t *d_pinv = d_blk + EW * EW;
-  uint32_t *d_spec = d_pinv + EW;
+  int *d_p2r = reinterpret_cast<int *>(b8 + out_bytes);
+  int *d_stamp = d_p2r + m;
+  int *d_perm = d_stamp + m;      // 4*EW ints: src list, dst list
+  int *d_last = d_perm + 4 * EW;  // largest row with a nonzero panel
+  int *d_hist = d_last + 1;       // EW + 1 head counts
+  uint8_t *d_head = b8 + out_bytes + i_bytes;
+  uint8_t *d_act = d_head + m;
+  uint32_t *d_U = reinterpret_cast<uint32_t *>(b8 + out_bytes + i_bytes + h_bytes);
+  uint32_t *d_xinv = d_U + EW * EW;  // pivot inverses (EW)
+  uint32_t *d_L11 = d_xinv + EW * EW;
+  uint32_t *d_L21 = d_L11 + EW * EW;
+  uint32_t *d_tmp = d_L21 + (size_t)m * EW;
+  const uint32_t *d_pcol = reinterpret_cast<const uint32_t *>(b8 + offsetof(PanelOut, pcol));
   void *gws = nullptr;
   st = ctx_workspace(c, zp_gemm_workspace_bytes(p, m, n, EW), &gws);
   if (st) return st;
-  const uint32_t t64 = two64_mod(p);
+  const bool small = p < (1u << 16);
+  const ArithSmall ars = ArithSmall::make(p);
+  const ArithWide arw = ArithWide::make(p);
+  cudaError_t e = cudaMemsetAsync(d_stamp, 0xff, (size_t)m * sizeof(int), c->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(d_last, 0xff, sizeof(int), c->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(d_hist, 0, (EW + 1) * sizeof(int), c->stream);
+  if (e != cudaSuccess) return ctx_cuda(c, e, "echelon: scratch");
 
   PanelOut h;
   std::vector<int> at, src, dst;
-  int i = 0;
-  int backoff = 1, skip = 0;  // speculation is retried less often after failures
+  int i = 0, epoch = 0;
+  const int head_grid = std::max(1, std::min((m + 7) / 8, c->num_sms * 2));
   for (int c0 = 0; c0 < n && i < m; c0 += EW) {
     const int w = std::min(EW, n - c0);
-    if (skip > 0) {
-      --skip;
-    } else if (m - i >= w) {
-      // speculative dense panel: rows i .. i+w-1 are the pivots, in order
-      int ps = prof_begin(c, "ech_spec_lu");
-      spec_lu_kernel<<<1, 1024, 0, c->stream>>>(D, ld, i, c0, w, mod, d_blk, d_pinv, d_spec);
-      prof_end(c, ps);
-      ctx_launched(c);
-      uint32_t hs[2];
-      if ((st = sync_read(c, d_spec, hs, sizeof hs, "echelon: speculation"))) return st;
-      if ((int)hs[0] == w) {
-        backoff = 1;
-        spec_write_kernel<<<1, 1024, 0, c->stream>>>(D, ld, i, c0, w, d_blk, d_L11);
-        ctx_launched(c);
-        const int r0 = i + w, below = m - r0, rest = n - (c0 + w);
-        if (below > 0) {
-          ps = prof_begin(c, "ech_spec_solve");
-          spec_right_solve_kernel<<<(below + 127) / 128, 128, 0, c->stream>>>(
-              D, ld, r0, m, c0, w, d_blk, d_pinv, d_L21, mod, t64);
-          prof_end(c, ps);
-          ctx_launched(c);
-        }
-        if (rest > 0) {
-          uint32_t *U12 = D + (size_t)i * ld + c0 + w;
-          if ((st = tri_left_block(c, false, w, d_L11, EW, nullptr, U12, ld, rest, p, 1)))
-            return st;
-          if (below > 0) {
-            ps = prof_begin(c, "ech_update");
-            st = zp_gemm_dev(c, GEMM_AUTO, below, rest, w, p, p - 1, d_L21, (size_t)w, U12, ld, 1,
-                             D + (size_t)r0 * ld + c0 + w, ld, static_cast<uint8_t *>(gws));
-            prof_end(c, ps);
-            if (st) return st;
-          }
-        }
-        det = (det * hs[1]) % p;
-        if (pivot_cols)
-          for (int k = 0; k < w; ++k) pivot_cols->push_back(c0 + k);
-        rank += w;
-        i += w;
-        continue;
-      }
-      backoff = std::min(backoff * 2, 32);
-      skip = backoff - 1;
-    }
-    int pi = prof_begin(c, "ech_panel");
-    panel_kernel<<<1, 1024, 0, c->stream>>>(D, ld, i, m, c0, w, mod, d_act_row, d_act_pos, d_vals,
-                                            d_mult, d_out);
+    int pi = prof_begin(c, "ech_heads");
+    panel_heads_kernel<<<head_grid, HEADS_THREADS, 0, c->stream>>>(D, ld, i, m, c0, w, d_head,
+                                                                    d_act, d_hist, d_last);
     prof_end(c, pi);
-    ctx_launched(c);
+    pi = prof_begin(c, "ech_search");
+    if (small)
+      panel_search_kernel<<<1, PS_THREADS, 0, c->stream>>>(
+          D, ld, i, m, c0, w, ars, d_head, d_act, d_hist, d_last, d_p2r, d_stamp, epoch, d_U,
+          d_xinv, d_out);
+    else
+      panel_search_kernel<<<1, PS_THREADS, 0, c->stream>>>(
+          D, ld, i, m, c0, w, arw, d_head, d_act, d_hist, d_last, d_p2r, d_stamp, epoch, d_U,
+          d_xinv, d_out);
+    ++epoch;
+    prof_end(c, pi);
+    ctx_launched(c, 2);
     if ((st = sync_read(c, d_out, &h, sizeof h, "echelon: panel"))) return st;
     if (h.err) return ctx_fail(c, ST_PIVOT, "Could not invert pivot-element in the ring");
     const int t = (int)h.t;
@@ -489,29 +646,31 @@ int zp_echelon_dev(Ctx *c, int m, int n, uint32_t p, uint32_t *D, size_t ld, siz
     if (cnt > 0) {
       std::vector<int> both(src);
       both.insert(both.end(), dst.begin(), dst.end());
-      cudaError_t e = cudaMemcpyAsync(d_perm, both.data(), both.size() * sizeof(int),
-                                      cudaMemcpyHostToDevice, c->stream);
+      e = cudaMemcpyAsync(d_perm, both.data(), both.size() * sizeof(int), cudaMemcpyHostToDevice,
+                          c->stream);
       if (e != cudaSuccess) return ctx_cuda(c, e, "echelon: permutation");
       dim3 grid((n + 255) / 256, cnt);
       gather_rows_kernel<<<grid, 256, 0, c->stream>>>(D, ld, n, d_perm, cnt, d_tmp);
       scatter_rows_kernel<<<grid, 256, 0, c->stream>>>(D, ld, n, d_perm + cnt, cnt, d_tmp);
       ctx_launched(c, 2);
     }
-    // write back, L11 / L21
+    // L11 / L21 and the panel's final values
     const int r0 = i + t;
     const int r1 = (h.last_pos >= (uint32_t)r0) ? (int)h.last_pos : r0 - 1;
     const int below = r1 - r0 + 1;
-    if (below > 0) {
-      const size_t words = (size_t)below * t;
-      zero_kernel<<<(int)std::min<size_t>((words + 255) / 256, (size_t)c->num_sms * 8), 256, 0,
-                    c->stream>>>(d_L21, words);
+    {
+      const int groups = (r1 - i + 1 + SOLVE_THREADS / 32 - 1) / (SOLVE_THREADS / 32);
+      pi = prof_begin(c, "ech_solve");
+      const int sgrid = std::max(1, std::min(groups, c->num_sms * 8));
+      if (small)
+        panel_solve_kernel<<<sgrid, SOLVE_THREADS, 0, c->stream>>>(D, ld, i, r1, c0, w, t, d_pcol,
+                                                                   d_U, d_xinv, ars, d_L11, d_L21);
+      else
+        panel_solve_kernel<<<sgrid, SOLVE_THREADS, 0, c->stream>>>(D, ld, i, r1, c0, w, t, d_pcol,
+                                                                   d_U, d_xinv, arw, d_L11, d_L21);
+      prof_end(c, pi);
       ctx_launched(c);
     }
-    const int nact = (int)h.nact;
-    panel_writeback_kernel<<<std::max(1, std::min((nact + 127) / 128, c->num_sms * 4)), 128, 0,
-                             c->stream>>>(D, ld, c0, w, nact, d_act_pos, d_vals, d_mult, i, t,
-                                          d_L11, d_L21, r0);
-    ctx_launched(c);
     const int rest = n - (c0 + w);
     if (rest > 0) {
       uint32_t *U12 = D + (size_t)i * ld + c0 + w;

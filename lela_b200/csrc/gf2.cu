@@ -27,6 +27,7 @@
 // scheme as the Z/p version (echelon.cu) with 64-column panels = one word
 // per row; the trailing update is an M4RM product.
 #include <algorithm>
+#include <cstddef>
 #include <mutex>
 #include <vector>
 
@@ -210,111 +211,277 @@ int gf2_gemm_dev(Ctx *c, int kernel, int M, int N, int K, int alpha, const uint6
 }
 
 // --------------------------------------------------------------- echelon
+//
+// Per 64-column panel (one word per row), the Z/p panel scheme of
+// echelon.cu with GF(2) arithmetic:
+//  * gf2_heads_kernel: first set bit of each row's panel word, the head
+//    histogram and the last row with a nonzero word;
+//  * gf2_search_kernel: the reference's pivot choice, lazily.  The pivot
+//    rows are kept as a reduced basis g_k (bit pcol_j of g_k is delta_kj)
+//    and, per column c, the mask M[c] = (1 << c) | sum_k g_k[c] << pcol_k,
+//    so bit c of a row reduced by all pivots so far is parity(v & M[c]):
+//    32 positions are tested per ballot;
+//  * the host replays the transpositions and moves the rows;
+//  * gf2_solve_kernel: per row from the first pivot down to the last
+//    possibly nonzero row, the reference's elimination steps on the word
+//    (pivot k XOR-ed in when bit pcol_k is set) give the multipliers; pivot
+//    rows become U_k, rows below become zero;
+//  * U12 = L11^-1 A12 and the M4RM trailing update C ^= L21 U12.
 constexpr int GW = 64;
+constexpr uint8_t GF2_HEAD_NONE = 64;
+constexpr int GF2_WIN = 4096;  // positions staged in shared memory by the search
+constexpr int GF2_SEARCH_THREADS = 256;
+constexpr size_t GF2_SEARCH_SMEM = (size_t)GF2_WIN * 13;
 
 struct Gf2PanelOut {
-  uint32_t t, nact, last_pos, pad;
+  uint32_t t, pad0, last_pos, pad;
   uint32_t ti[GW], tq[GW], pcol[GW];
 };
 
-__device__ __forceinline__ int gf2_block_scan(int flag, int *warp_sums, int *total) {
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
-  unsigned b = __ballot_sync(0xffffffffu, flag);
-  int in_warp = __popc(b & ((1u << lane) - 1u));
-  if (lane == 0) warp_sums[wid] = __popc(b);
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    int s = 0;
-    for (int w = 0; w < nw; ++w) {
-      int v = warp_sums[w];
-      warp_sums[w] = s;
-      s += v;
-    }
-    *total = s;
-  }
-  __syncthreads();
-  int r = warp_sums[wid] + in_warp;
-  __syncthreads();
-  return r;
+__device__ __forceinline__ int gf2_row_at(int pos, const int *p2r, const int *stamp, int epoch) {
+  return stamp[pos] == epoch ? p2r[pos] : pos;
 }
 
-// The reference's steps restricted to panel word `wc` (w valid bits) on the
-// rows at or below i0 that have a bit set there (see echelon.cu).
-__global__ void __launch_bounds__(1024)
-    gf2_panel_kernel(const uint64_t *__restrict__ D, size_t ld, int i0, int m, int wc, int w,
-                     int *__restrict__ act_row, int *__restrict__ act_pos,
-                     uint64_t *__restrict__ vals, uint64_t *__restrict__ mult, Gf2PanelOut *out) {
-  __shared__ int warp_sums[32];
-  __shared__ int s_total, s_nact;
-  __shared__ unsigned long long s_key;
-  __shared__ int s_at_i;
-  const uint64_t mask = (w == 64) ? ~0ull : ((1ull << w) - 1ull);
-  if (threadIdx.x == 0) s_nact = 0;
+constexpr int GF2_HEADS_THREADS = 256;
+__global__ void __launch_bounds__(GF2_HEADS_THREADS)
+    gf2_heads_kernel(const uint64_t *__restrict__ D, size_t ld, int i0, int m, int wc,
+                     uint64_t pmask, uint8_t *__restrict__ head, uint8_t *__restrict__ act,
+                     int *hist, int *last) {
+  __shared__ int s_last;
+  __shared__ int s_hist[GW + 1];
+  if (threadIdx.x == 0) s_last = -1;
+  if (threadIdx.x <= GW) s_hist[threadIdx.x] = 0;
   __syncthreads();
-  for (int base = i0; base < m; base += blockDim.x) {
-    const int r = base + threadIdx.x;
-    const int flag = (r < m) && (D[(size_t)r * ld + wc] & mask) != 0ull;
-    int off = gf2_block_scan(flag, warp_sums, &s_total);
-    if (flag) act_row[s_nact + off] = r;
-    __syncthreads();
-    if (threadIdx.x == 0) s_nact += s_total;
-    __syncthreads();
+  int my_last = -1;
+  for (int r = i0 + blockIdx.x * blockDim.x + threadIdx.x; r < m; r += gridDim.x * blockDim.x) {
+    const uint64_t v = D[(size_t)r * ld + wc] & pmask;
+    const int h = v ? __ffsll((long long)v) - 1 : GF2_HEAD_NONE;
+    head[r] = (uint8_t)h;
+    act[r] = v != 0ull;
+    atomicAdd(&s_hist[h], 1);
+    if (v) my_last = r;
   }
-  const int nact = s_nact;
-  for (int a = threadIdx.x; a < nact; a += blockDim.x) {
-    act_pos[a] = act_row[a];
-    vals[a] = D[(size_t)act_row[a] * ld + wc] & mask;
-    mult[a] = 0ull;
-  }
+  if (my_last >= 0) atomicMax(&s_last, my_last);
   __syncthreads();
+  if (threadIdx.x == 0 && s_last >= 0) atomicMax(last, s_last);
+  if (threadIdx.x <= GW && s_hist[threadIdx.x]) atomicAdd(&hist[threadIdx.x], s_hist[threadIdx.x]);
+}
+
+// The CTA stages the words of positions i0 .. i0+GF2_WIN-1 in shared
+// memory; then one warp searches.  The head of a row is a lower bound of the
+// first set bit of its reduced word (exact when set by a bulk scan); cnt[h]
+// counts the non-pivot rows at or below the current row whose bound is h.
+// Outputs: Gf2PanelOut, U (the pivot rows' final words).  Resets *last_act
+// and hist[] for the next panel.
+__global__ void __launch_bounds__(GF2_SEARCH_THREADS)
+    gf2_search_kernel(const uint64_t *__restrict__ D, size_t ld, int i0, int m, int wc, int w,
+                      uint64_t pmask, uint8_t *__restrict__ head, const uint8_t *__restrict__ act,
+                      int *__restrict__ hist, int *__restrict__ last_act, int *__restrict__ p2r,
+                      int *__restrict__ stamp, int epoch, uint64_t *__restrict__ Uout,
+                      Gf2PanelOut *out) {
+  extern __shared__ __align__(16) uint8_t gdyn[];
+  __shared__ uint64_t G[GW], M[GW];
+  __shared__ int s_pcol[GW];
+  __shared__ int s_cnt[GW + 1];
+  uint64_t *sword = reinterpret_cast<uint64_t *>(gdyn);
+  int *srow = reinterpret_cast<int *>(gdyn + (size_t)GF2_WIN * 8);
+  uint8_t *shead = gdyn + (size_t)GF2_WIN * 12;
+  const int nwin = min(GF2_WIN, m - i0);
+  for (int k = threadIdx.x; k < nwin; k += blockDim.x) {
+    cp_async8(&sword[k], D + (size_t)(i0 + k) * ld + wc, true);
+    srow[k] = i0 + k;
+    shead[k] = head[i0 + k];
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  for (int k = threadIdx.x; k < nwin; k += blockDim.x) sword[k] &= pmask;
+  __syncthreads();
+  if (threadIdx.x >= 32) return;
+  const int lane = threadIdx.x;
+  auto in_win = [&](int pos) { return pos - i0 < nwin; };
+  auto word_at = [&](int pos) -> uint64_t {
+    return in_win(pos) ? sword[pos - i0]
+                       : D[(size_t)gf2_row_at(pos, p2r, stamp, epoch) * ld + wc] & pmask;
+  };
+  auto head_at = [&](int pos) -> int {
+    return in_win(pos) ? shead[pos - i0] : head[gf2_row_at(pos, p2r, stamp, epoch)];
+  };
+  auto set_head = [&](int pos, int h) {
+    if (in_win(pos))
+      shead[pos - i0] = (uint8_t)h;
+    else
+      head[gf2_row_at(pos, p2r, stamp, epoch)] = (uint8_t)h;
+  };
+  for (int h = lane; h <= GW; h += 32) {
+    s_cnt[h] = hist[h];
+    hist[h] = 0;
+  }
+  M[lane] = 1ull << lane;
+  M[lane + 32] = 1ull << (lane + 32);
+  __syncwarp();
   int i = i0, t = 0;
   for (int col = 0; col < w && i < m; ++col) {
-    if (threadIdx.x == 0) {
-      s_key = ~0ull;
-      s_at_i = -1;
+    const uint64_t mc = M[col];
+    int q = -1;
+    {
+      const int pos = i + lane;
+      int nz = 0;
+      if (pos < m) {
+        const int hr = head_at(pos);
+        if (hr <= col) {
+          nz = __popcll(word_at(pos) & mc) & 1;
+          if (!nz) {
+            set_head(pos, col + 1);
+            atomicSub(&s_cnt[hr], 1);
+            atomicAdd(&s_cnt[col + 1], 1);
+          }
+        }
+      }
+      const unsigned b = __ballot_sync(0xffffffffu, nz);
+      if (b) q = i + __ffs(b) - 1;
     }
-    __syncthreads();
-    for (int a = threadIdx.x; a < nact; a += blockDim.x) {
-      const int pos = act_pos[a];
-      if (pos >= i && ((vals[a] >> col) & 1ull))
-        atomicMin(&s_key, ((unsigned long long)(unsigned)pos << 32) | (unsigned)a);
-      if (pos == i) s_at_i = a;
+    __syncwarp();
+    if (q < 0) {
+      int cand = 0;
+      for (int h = lane; h <= col; h += 32) cand += s_cnt[h];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) cand += __shfl_xor_sync(0xffffffffu, cand, o);
+      __syncwarp();
+      for (int base = i + 32; base < m && cand > 0; base += 32) {
+        const int pos = base + lane;
+        int is_cand = 0, hit = 0;
+        if (pos < m) {
+          const int hr = head_at(pos);
+          if (hr <= col) {
+            is_cand = 1;
+            const uint64_t v = word_at(pos);
+            int c = col;
+            while (c < w && !(__popcll(v & M[c]) & 1)) ++c;
+            const int hn = c < w ? c : GF2_HEAD_NONE;
+            set_head(pos, hn);
+            if (hn != hr) {
+              atomicSub(&s_cnt[hr], 1);
+              atomicAdd(&s_cnt[hn], 1);
+            }
+            hit = c == col;
+          }
+        }
+        cand -= __popc(__ballot_sync(0xffffffffu, is_cand));
+        const unsigned hb = __ballot_sync(0xffffffffu, hit);
+        if (hb) {
+          q = base + __ffs(hb) - 1;
+          break;
+        }
+      }
+      __syncwarp();
+      if (q < 0) continue;  // no pivot in this column
     }
-    __syncthreads();
-    const unsigned long long key = s_key;
-    const int ai = s_at_i;
-    __syncthreads();
-    if (key == ~0ull) continue;
-    const int ap = (int)(key & 0xffffffffu), q = (int)(key >> 32);
-    const uint64_t pw = vals[ap];
-    if (threadIdx.x == 0) {
+    // the pivot row reduced by the pivots so far: U = v ^ sum_{k: v bit pcol_k} g_k
+    const uint64_t v = word_at(q);
+    uint64_t x = 0;
+    if (lane < t && ((v >> s_pcol[lane]) & 1ull)) x ^= G[lane];
+    if (lane + 32 < t && ((v >> s_pcol[lane + 32]) & 1ull)) x ^= G[lane + 32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x ^= __shfl_xor_sync(0xffffffffu, x, o);
+    const uint64_t U = v ^ x;
+    // basis and masks: g_k ^= U where g_k has bit col; M[c] ^= M[col] (which
+    // holds bit col and the pivot columns whose g has bit col) for the
+    // columns c > col where U has a bit
+    __syncwarp();
+    if (lane < t && ((G[lane] >> col) & 1ull)) G[lane] ^= U;
+    if (lane + 32 < t && ((G[lane + 32] >> col) & 1ull)) G[lane + 32] ^= U;
+    for (int c = lane; c < w; c += 32)
+      if (c > col && ((U >> c) & 1ull)) M[c] ^= mc;
+    if (lane == 0) {
+      G[t] = U;
+      s_pcol[t] = col;
+      Uout[t] = U;
+      out->pcol[t] = (uint32_t)col;
       out->ti[t] = (uint32_t)i;
       out->tq[t] = (uint32_t)q;
-      out->pcol[t] = (uint32_t)col;
-      if (ai >= 0 && ai != ap) act_pos[ai] = q;
-      act_pos[ap] = i;
-    }
-    __syncthreads();
-    for (int a = threadIdx.x; a < nact; a += blockDim.x) {
-      if (act_pos[a] <= i) continue;
-      if ((vals[a] >> col) & 1ull) {
-        vals[a] ^= pw;
-        mult[a] |= 1ull << t;
+      atomicSub(&s_cnt[head_at(q)], 1);
+      // transposition (i, q): inside the window the entries swap; a pivot
+      // from beyond it takes slot i and the row it displaces goes to
+      // position q in the global maps (with its head bound)
+      const int ki = i - i0;
+      if (q != i) {
+        if (in_win(q)) {
+          const int kq = q - i0;
+          const uint64_t tw = sword[ki];
+          const int tr = srow[ki];
+          const uint8_t th = shead[ki];
+          sword[ki] = sword[kq];
+          srow[ki] = srow[kq];
+          shead[ki] = shead[kq];
+          sword[kq] = tw;
+          srow[kq] = tr;
+          shead[kq] = th;
+        } else {
+          const int ap = gf2_row_at(q, p2r, stamp, epoch);
+          const int ri = srow[ki];
+          head[ri] = shead[ki];
+          p2r[q] = ri;
+          stamp[q] = epoch;
+          sword[ki] = v;
+          srow[ki] = ap;
+        }
       }
     }
-    __syncthreads();
+    __syncwarp();
     ++i;
     ++t;
   }
-  if (threadIdx.x == 0) s_key = 0;
-  __syncthreads();
-  for (int a = threadIdx.x; a < nact; a += blockDim.x)
-    if (act_pos[a] >= i) atomicMax(&s_key, (unsigned long long)(unsigned)act_pos[a]);
-  __syncthreads();
-  if (threadIdx.x == 0) {
+  // last final position of a non-pivot row with a nonzero word
+  int hi = i - 1;
+  for (int k = lane; k < t; k += 32) hi = max(hi, (int)out->tq[k]);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+  int last = -1;
+  for (int pos = i + lane; pos <= hi && pos < m; pos += 32)
+    if (act[in_win(pos) ? srow[pos - i0] : gf2_row_at(pos, p2r, stamp, epoch)]) last = pos;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) last = max(last, __shfl_xor_sync(0xffffffffu, last, o));
+  if (lane == 0) {
+    const int la = *last_act;
+    if (la > hi) last = la;
     out->t = (uint32_t)t;
-    out->nact = (uint32_t)nact;
-    out->last_pos = (uint32_t)s_key;
+    out->last_pos = (uint32_t)(last >= 0 ? last : 0);
+    *last_act = -1;
+  }
+}
+
+// Rows i0..r1 at their final positions: the reference's elimination steps
+// on the panel word give the multipliers (L11 row of pivot row k over the
+// pivots before it; L21 row of the rows below over all t) and the final
+// word (U_k; zero below).  One thread per row.
+__global__ void gf2_solve_kernel(uint64_t *__restrict__ D, size_t ld, int i0, int r1, int wc,
+                                 uint64_t pmask, int t, const uint32_t *__restrict__ pcol,
+                                 const uint64_t *__restrict__ Uin, uint64_t *__restrict__ L11,
+                                 uint64_t *__restrict__ L21) {
+  __shared__ uint64_t sU[GW];
+  __shared__ int sP[GW];
+  if (threadIdx.x < GW) {
+    sU[threadIdx.x] = threadIdx.x < t ? Uin[threadIdx.x] : 0ull;
+    sP[threadIdx.x] = threadIdx.x < t ? (int)pcol[threadIdx.x] : 0;
+  }
+  __syncthreads();
+  const int r0 = i0 + t;
+  for (int pos = i0 + blockIdx.x * blockDim.x + threadIdx.x; pos <= r1;
+       pos += gridDim.x * blockDim.x) {
+    uint64_t *x = D + (size_t)pos * ld + wc;
+    uint64_t v = *x & pmask;
+    const int kk = pos - i0, lim = kk < t ? kk : t;
+    uint64_t l = 0;
+    for (int k = 0; k < lim; ++k)
+      if ((v >> sP[k]) & 1ull) {
+        v ^= sU[k];
+        l |= 1ull << k;
+      }
+    *x = (*x & ~pmask) | v;
+    if (kk < t)
+      L11[kk] = l;
+    else
+      L21[pos - r0] = l;
   }
 }
 
@@ -331,26 +498,6 @@ __global__ void gf2_scatter_rows_kernel(uint64_t *__restrict__ D, size_t ld, int
   for (int k = blockIdx.y; k < cnt; k += gridDim.y)
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nw; j += gridDim.x * blockDim.x)
       D[(size_t)dst[k] * ld + j] = tmp[(size_t)k * nw + j];
-}
-
-// Panel words back into D; L11 rows (pivot k: its multiplier bits) and the
-// L21 word of every row in r0..r1 (zero when the row was not eliminated).
-__global__ void gf2_panel_writeback_kernel(uint64_t *__restrict__ D, size_t ld, int wc,
-                                           uint64_t keep_mask, int nact,
-                                           const int *__restrict__ act_pos,
-                                           const uint64_t *__restrict__ vals,
-                                           const uint64_t *__restrict__ mult, int i0, int t,
-                                           uint64_t *__restrict__ L11, uint64_t *__restrict__ L21,
-                                           int r0) {
-  for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nact; a += gridDim.x * blockDim.x) {
-    const int pos = act_pos[a];
-    uint64_t *x = D + (size_t)pos * ld + wc;
-    *x = (*x & keep_mask) | vals[a];
-    if (pos < i0 + t)
-      L11[pos - i0] = mult[a];
-    else if (pos >= r0)
-      L21[pos - r0] = mult[a];
-  }
 }
 
 // U12 = L11^-1 A12 over GF(2): pivot rows i0..i0+t-1, words from w1; row k
@@ -378,12 +525,6 @@ __global__ void gf2_l11_solve_kernel(uint64_t *__restrict__ D, size_t ld, int i0
     if (k < t) D[(size_t)(i0 + k) * ld + w] = x[k];
 }
 
-__global__ void gf2_zero_kernel(uint64_t *x, size_t n) {
-  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n;
-       k += (size_t)gridDim.x * blockDim.x)
-    x[k] = 0ull;
-}
-
 int gf2_echelon_dev(Ctx *c, int m, int n, uint64_t *D, size_t ld, size_t *rank_out) {
   if (m < 0 || n < 0) return ctx_fail(c, ST_ARG, "negative dimension");
   const int nw = (n + 63) / 64;
@@ -394,35 +535,61 @@ int gf2_echelon_dev(Ctx *c, int m, int n, uint64_t *D, size_t ld, size_t *rank_o
     return ST_OK;
   }
   const size_t out_bytes = (sizeof(Gf2PanelOut) + 255) & ~(size_t)255;
-  const size_t i_bytes = (((size_t)2 * m + 4 * GW) * sizeof(int) + 255) & ~(size_t)255;
-  const size_t v_bytes = (size_t)m * 8;
+  // p2r, stamp (m each); permutation lists (4 GW); last row (1); histogram (GW + 1)
+  const size_t i_bytes =
+      (((size_t)2 * m + 4 * GW + 1 + GW + 1) * sizeof(int) + 255) & ~(size_t)255;
+  const size_t h_bytes = ((size_t)2 * m + 255) & ~(size_t)255;
   void *base = nullptr;
   int st = ctx_buffer(c, BUF_GF2_0,
-                      out_bytes + i_bytes + 3 * v_bytes + GW * 8 + (size_t)2 * GW * nw * 8 + 1024,
+                      out_bytes + i_bytes + h_bytes + (size_t)m * 8 + 2 * GW * 8 +
+                          (size_t)2 * GW * nw * 8 + 1024,
                       &base);
   if (st) return st;
   uint8_t *b8 = static_cast<uint8_t *>(base);
   Gf2PanelOut *d_out = reinterpret_cast<Gf2PanelOut *>(b8);
-  int *d_act_row = reinterpret_cast<int *>(b8 + out_bytes);
-  int *d_act_pos = d_act_row + m;
-  int *d_perm = d_act_pos + m;
-  uint64_t *d_vals = reinterpret_cast<uint64_t *>(b8 + out_bytes + i_bytes);
-  uint64_t *d_mult = d_vals + m;
-  uint64_t *d_L21 = d_mult + m;
+  int *d_p2r = reinterpret_cast<int *>(b8 + out_bytes);
+  int *d_stamp = d_p2r + m;
+  int *d_perm = d_stamp + m;      // 4*GW ints
+  int *d_last = d_perm + 4 * GW;  // largest row with a nonzero word
+  int *d_hist = d_last + 1;       // GW + 1 head counts
+  uint8_t *d_head = b8 + out_bytes + i_bytes;
+  uint8_t *d_act = d_head + m;
+  uint64_t *d_L21 = reinterpret_cast<uint64_t *>(b8 + out_bytes + i_bytes + h_bytes);
   uint64_t *d_L11 = d_L21 + m;
-  uint64_t *d_tmp = d_L11 + GW;
+  uint64_t *d_U = d_L11 + GW;
+  uint64_t *d_tmp = d_U + GW;
+  const uint32_t *d_pcol = reinterpret_cast<const uint32_t *>(b8 + offsetof(Gf2PanelOut, pcol));
+  static std::once_flag once;
+  static cudaError_t attr_err = cudaSuccess;
+  std::call_once(once, [] {
+    attr_err = cudaFuncSetAttribute(gf2_search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)GF2_SEARCH_SMEM);
+  });
+  if (attr_err != cudaSuccess) return ctx_cuda(c, attr_err, "gf2 echelon: search attributes");
+  cudaError_t e = cudaMemsetAsync(d_stamp, 0xff, (size_t)m * sizeof(int), c->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(d_last, 0xff, sizeof(int), c->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(d_hist, 0, (GW + 1) * sizeof(int), c->stream);
+  if (e != cudaSuccess) return ctx_cuda(c, e, "gf2 echelon: scratch");
 
   Gf2PanelOut h;
   std::vector<int> at, src, dst;
-  int i = 0;
+  int i = 0, epoch = 0;
+  const int head_grid = std::max(1, std::min((m + GF2_HEADS_THREADS - 1) / GF2_HEADS_THREADS,
+                                             c->num_sms * 2));
   for (int wc = 0; wc < nw && i < m; ++wc) {
     const int w = std::min(64, n - 64 * wc);
-    int pi = prof_begin(c, "gf2_panel");
-    gf2_panel_kernel<<<1, 1024, 0, c->stream>>>(D, ld, i, m, wc, w, d_act_row, d_act_pos, d_vals,
-                                                d_mult, d_out);
+    const uint64_t pmask = (w == 64) ? ~0ull : ((1ull << w) - 1ull);
+    int pi = prof_begin(c, "gf2_heads");
+    gf2_heads_kernel<<<head_grid, GF2_HEADS_THREADS, 0, c->stream>>>(D, ld, i, m, wc, pmask,
+                                                                     d_head, d_act, d_hist, d_last);
     prof_end(c, pi);
-    ctx_launched(c);
-    cudaError_t e = cudaMemcpyAsync(&h, d_out, sizeof h, cudaMemcpyDeviceToHost, c->stream);
+    pi = prof_begin(c, "gf2_search");
+    gf2_search_kernel<<<1, GF2_SEARCH_THREADS, GF2_SEARCH_SMEM, c->stream>>>(
+        D, ld, i, m, wc, w, pmask, d_head, d_act, d_hist, d_last, d_p2r, d_stamp, epoch++, d_U,
+        d_out);
+    prof_end(c, pi);
+    ctx_launched(c, 2);
+    e = cudaMemcpyAsync(&h, d_out, sizeof h, cudaMemcpyDeviceToHost, c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) return ctx_cuda(c, e, "gf2 echelon: panel");
     const int t = (int)h.t;
@@ -455,17 +622,14 @@ int gf2_echelon_dev(Ctx *c, int m, int n, uint64_t *D, size_t ld, size_t *rank_o
     const int r0 = i + t;
     const int r1 = (h.last_pos >= (uint32_t)r0) ? (int)h.last_pos : r0 - 1;
     const int below = r1 - r0 + 1;
-    if (below > 0) {
-      gf2_zero_kernel<<<std::min((below + 255) / 256, c->num_sms * 8), 256, 0, c->stream>>>(
-          d_L21, (size_t)below);
+    {
+      const int rows = r1 - i + 1;
+      pi = prof_begin(c, "gf2_solve");
+      gf2_solve_kernel<<<std::max(1, std::min((rows + 255) / 256, c->num_sms * 4)), 256, 0,
+                         c->stream>>>(D, ld, i, r1, wc, pmask, t, d_pcol, d_U, d_L11, d_L21);
+      prof_end(c, pi);
       ctx_launched(c);
     }
-    const uint64_t pmask = (w == 64) ? ~0ull : ((1ull << w) - 1ull);
-    const int nact = (int)h.nact;
-    gf2_panel_writeback_kernel<<<std::max(1, std::min((nact + 255) / 256, c->num_sms * 4)), 256,
-                                 0, c->stream>>>(D, ld, wc, ~pmask, nact, d_act_pos, d_vals,
-                                                 d_mult, i, t, d_L11, d_L21, r0);
-    ctx_launched(c);
     const int w1 = wc + 1;
     if (w1 < nw) {
       gf2_l11_solve_kernel<<<(nw - w1 + 127) / 128, 128, 0, c->stream>>>(D, ld, i, t, w1, nw,

@@ -59,3 +59,21 @@ def test_echelon_large(cuda):
     got, gr, gd = cuda.echelonize(p, A.copy())
     assert (gr, gd) == (wr, wd)
     assert np.array_equal(got, want)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("p", [3, 65521])
+def test_echelon_pivots_far_below(cuda, p):
+    """Pivots that lie hundreds of rows below the current row: the first 700
+    rows are zero in the leading columns, so the search reaches rows beyond
+    the block it keeps on chip, and the transpositions move rows across it."""
+    g = np.random.default_rng(5)
+    m, n = 1200, 150
+    A = gen.dense_zp(91, m, n, p)
+    A[:700, :40] = 0
+    A[g.choice(np.arange(700, m), size=300, replace=False), :12] = 0
+    A[::7, 70:75] = 0
+    want, wr, wd = oracle.echelon_zp(p, A)
+    got, gr, gd = cuda.echelonize(p, A.copy())
+    assert (gr, gd) == (wr, wd)
+    assert np.array_equal(got, want)

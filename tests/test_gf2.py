@@ -87,3 +87,17 @@ def test_gf2_echelon_against_oracle(cuda):
         want, wr = oracle.echelon_gf2(A, n)
         got, gr = cuda.echelonize_gf2(A.copy(), n)
         assert gr == wr and np.array_equal(got, want), (m, n)
+
+
+@pytest.mark.gpu
+def test_gf2_echelon_pivots_far_below(cuda):
+    """The first 4500 rows are zero in the leading columns, so pivots come
+    from rows beyond the block the search keeps on chip."""
+    m, n = 6000, 200
+    A = gen.dense_gf2(77, m, n)
+    A[:4500, 0] &= ~np.uint64((1 << 40) - 1)
+    A[4500:5200, 0] &= ~np.uint64(0xFFF)
+    want, wr = oracle.echelon_gf2(A, n)
+    got, gr = cuda.echelonize_gf2(A.copy(), n)
+    assert gr == wr
+    assert np.array_equal(got, want)
