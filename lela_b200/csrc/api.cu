@@ -187,6 +187,7 @@ int lela_cuda_destroy(lela_cuda_ctx *h) {
     if (c->stage[i]) cudaFree(c->stage[i]);
   for (int i = 0; i < 32; ++i)
     if (c->buf[i]) cudaFree(c->buf[i]);
+  if (c->batch_exec) cudaGraphExecDestroy(c->batch_exec);
   if (c->dstatus) cudaFree(c->dstatus);
   if (c->hstatus) cudaFreeHost(c->hstatus);
   for (auto &r : c->prof) {
@@ -483,33 +484,45 @@ int lela_cuda_echelon_zp_u32_batch(lela_cuda_ctx *h, size_t count, uint32_t *con
     cudaError_t e = cudaMemcpyAsync(d_items, small.data(), ns * sizeof(SmallItem),
                                     cudaMemcpyHostToDevice, c->stream);
     if (e != cudaSuccess) return ctx_cuda(c, e, "batch: items");
-    // one persistent launch, captured in a CUDA graph and replayed once
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
-    if ((st = echelon_small_batch_prepare(c))) return st;
-    const bool was_profiling = c->profile;
-    c->profile = false;  // no event records inside the capture
-    e = cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal);
-    c->profile = was_profiling;
-    if (e == cudaSuccess) c->profile = false;
-    if (e != cudaSuccess) return ctx_cuda(c, e, "batch: begin capture");
-    st = echelon_small_batch_dev(c, (int)ns, d_items, d_next, d_rank, d_det, d_status);
-    e = cudaStreamEndCapture(c->stream, &graph);
-    c->profile = was_profiling;
-    if (st) {
+    // one persistent launch, captured in a CUDA graph; the instantiated graph
+    // is kept in the handle and replayed by later calls with the same item
+    // count and buffer (the item array is refreshed above, outside the graph)
+    if (!(c->batch_exec && c->batch_ns == ns && c->batch_buf == buf)) {
+      if (c->batch_exec) cudaGraphExecDestroy(c->batch_exec);
+      c->batch_exec = nullptr;
+      cudaGraph_t graph = nullptr;
+      if ((st = echelon_small_batch_prepare(c))) return st;
+      const bool was_profiling = c->profile;
+      c->profile = false;  // no event records inside the capture
+      e = cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal);
+      if (e != cudaSuccess) {
+        c->profile = was_profiling;
+        return ctx_cuda(c, e, "batch: begin capture");
+      }
+      st = echelon_small_batch_dev(c, (int)ns, d_items, d_next, d_rank, d_det, d_status);
+      e = cudaStreamEndCapture(c->stream, &graph);
+      c->profile = was_profiling;
+      if (st) {
+        if (graph) cudaGraphDestroy(graph);
+        return st;
+      }
+      cudaGraphExec_t exec = nullptr;
+      if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
       if (graph) cudaGraphDestroy(graph);
-      return st;
+      if (e != cudaSuccess) return ctx_cuda(c, e, "batch: graph");
+      c->batch_exec = exec;
+      c->batch_ns = ns;
+      c->batch_buf = buf;
     }
-    if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
-    if (e == cudaSuccess) e = cudaGraphLaunch(exec, c->stream);
+    int pi = prof_begin(c, "echelon_small_batch_graph");
+    e = cudaGraphLaunch(c->batch_exec, c->stream);
+    prof_end(c, pi);
     std::vector<uint64_t> hr(ns);
     std::vector<uint32_t> hd(ns), hs(ns);
     if (e == cudaSuccess) e = cudaMemcpyAsync(hr.data(), d_rank, ns * 8, cudaMemcpyDeviceToHost, c->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(hd.data(), d_det, ns * 4, cudaMemcpyDeviceToHost, c->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(hs.data(), d_status, ns * 4, cudaMemcpyDeviceToHost, c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-    if (exec) cudaGraphExecDestroy(exec);
-    if (graph) cudaGraphDestroy(graph);
     if (e != cudaSuccess) return ctx_cuda(c, e, "batch: small blocks");
     for (size_t j = 0; j < ns; ++j) {
       const size_t i = small_idx[j];

@@ -60,6 +60,12 @@ struct Ctx {
   int gf2_kernel = GF2_AUTO;
   std::string last_error;
 
+  // Instantiated CUDA graph of the small-block batch launch, replayed while
+  // the item count and the batch buffer stay the same.
+  cudaGraphExec_t batch_exec = nullptr;
+  size_t batch_ns = 0;
+  void *batch_buf = nullptr;
+
   // Kernel launches issued through this handle (all kernels of the library).
   uint64_t launches = 0;
   // Optional per-kernel device timing: an event pair around each launch of

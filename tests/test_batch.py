@@ -59,3 +59,30 @@ def test_fl_batch(cuda):
         assert st[i] == 0
         assert (ranks[i], dets[i]) == (w["rank"], w["det"]), i
         assert np.array_equal(Rs[i].cpu().numpy().view(np.uint32), w["R"]), i
+
+
+@pytest.mark.gpu
+def test_echelon_batch_small_kernel_edges(cuda):
+    """The shared-memory kernel on tall blocks whose pivots lie more than 512
+    rows down (the search covers 512 rows per pass), and on composite moduli
+    where a pivot has no inverse (the reference's error, status != 0)."""
+    blocks, ps, wants = [], [], []
+    for i, (m, n, p) in enumerate([(1500, 20, 7), (900, 40, 65521), (700, 30, 2147483647),
+                                   (60, 50, 10), (40, 40, 12), (33, 17, 9)]):
+        A = gen.dense_zp(70 + i, m, n, p)
+        if m > 512:
+            A[: m - 100, :5] = 0               # the first columns' pivots far down
+        blocks.append(_dev(A)); ps.append(p)
+        try:
+            wants.append(oracle.echelon_zp(p, A))
+        except ArithmeticError:
+            wants.append(None)
+    ranks, dets, st = cuda.echelonize_batch(blocks, ps, [1] * len(blocks))
+    for i, want in enumerate(wants):
+        if want is None:
+            assert st[i] != 0, i
+            continue
+        E, r, d = want
+        assert st[i] == 0, i
+        assert (ranks[i], dets[i]) == (r, d), i
+        assert np.array_equal(blocks[i].cpu().numpy().view(np.uint32), E), i
