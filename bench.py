@@ -32,6 +32,7 @@ import statistics
 import subprocess
 import sys
 import tempfile
+import threading
 import time
 
 import numpy as np
@@ -314,13 +315,14 @@ def run_batch(args, cm, stream, torch, dev):
     """Batched workload (scaled to minutes): F4-shaped FL matrices with m
     log-uniform in [2000, 8000] plus dense Z/p echelon blocks of sizes
     log-uniform in [64, 4096], p in {251, 65521, 2^31-1}.
-    * ours: the FL matrices through the batched entry point (4 worker
+    * ours: the FL matrices through the batched entry point (8 worker
       streams, tensor-core gemms) and the dense blocks through one batched
       call whose kernel per block is chosen by the MLP cost model, trained
-      first on autotuner timings of a separate set of blocks;
-    * plain: the per-matrix pipeline -- one matrix at a time on one stream
-      with every gemm on the CUDA-core kernel and every dense block through
-      the panel pipeline."""
+      first on autotuner timings of a separate set of blocks (small blocks in
+      one persistent graph launch, the others over worker streams);
+    * plain: the per-matrix pipeline -- one matrix per call, one at a time on
+      one stream, with every gemm on the CUDA-core kernel and every dense
+      block through the panel pipeline."""
     import types
     from lela_b200 import gen
     from lela_b200 import selector as sel
@@ -346,7 +348,7 @@ def run_batch(args, cm, stream, torch, dev):
     t0 = time.perf_counter()
     tuner = sel.Autotuner(cm, reps=2)
     for i in range(24):
-        s = int(2 ** rng.uniform(6, 11.5))
+        s = int(2 ** rng.uniform(6, 12))
         tuner.tune_echelon(s, s, int(rng.choice(primes)), seed=9000 + i)
     X, y = sel.records_to_xy(tuner.records)
     model = sel.CostModel(cm, seed=1)
@@ -356,11 +358,31 @@ def run_batch(args, cm, stream, torch, dev):
                for A, p in dense]
     tune_s = time.perf_counter() - t0
 
+    # the dense blocks go through a second handle from a second host thread,
+    # concurrently with the FL batch (a handle serves one thread at a time)
+    from lela_b200 import CudaModule
+    cm_dense = CudaModule(torch.cuda.current_device())
+
     def ours():
         for w, (A, _) in zip(work, dense):
             w.copy_(A)
-        cm.fl_echelonize_batch(fl_items, [P] * len(fl_items), Rs, True, nworkers=4)
-        cm.echelonize_batch(work, [p for _, p in dense], kernels)
+        torch.cuda.synchronize()  # the copies are done before another stream reads them
+        failed = []
+
+        def dense_part():
+            try:
+                cm_dense.echelonize_batch(work, [p for _, p in dense], kernels)
+            except BaseException as e:  # re-raised on the calling thread
+                failed.append(e)
+
+        th = threading.Thread(target=dense_part)
+        th.start()
+        try:
+            cm.fl_echelonize_batch(fl_items, [P] * len(fl_items), Rs, True, nworkers=8)
+        finally:
+            th.join()
+        if failed:
+            raise failed[0]
 
     def plain():
         for w, (A, _) in zip(work, dense):
@@ -369,7 +391,8 @@ def run_batch(args, cm, stream, torch, dev):
         try:
             for X, R in zip(fl_items, Rs):
                 cm.fl_echelonize(P, X, True, False, R=R)
-            cm.echelonize_batch(work, [p for _, p in dense], [3] * len(dense))
+            for w, (_, p) in zip(work, dense):
+                cm.echelonize_batch([w], [p], [3])
         finally:
             cm.set_gemm_kernel(0)
 

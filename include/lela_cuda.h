@@ -200,8 +200,12 @@ int lela_cuda_echelon_gf2_dev (lela_cuda_ctx *ctx, size_t m, size_t n, uint64_t 
  * pipeline with tensor-core updates), 1 = batched shared-memory kernel,
  * 2 = panel pipeline with tensor-core updates, 3 = panel pipeline with
  * CUDA-core updates.  The shared-memory blocks are processed by one
- * persistent launch captured in a CUDA graph.  status[i] = 0 or
- * LELA_CUDA_PIVOT_NOT_INVERTIBLE. */
+ * persistent launch captured in a CUDA graph (the instantiated graph is kept
+ * in the handle and replayed while the count of such blocks stays the same);
+ * when two or more blocks take the panel pipeline they are spread over up to
+ * 8 worker handles with their own streams, concurrently with that launch, so
+ * the call first waits for the work already queued on the handle's stream.
+ * status[i] = 0 or LELA_CUDA_PIVOT_NOT_INVERTIBLE. */
 int lela_cuda_echelon_zp_u32_batch (lela_cuda_ctx *ctx, size_t count, uint32_t *const *A,
 				    const size_t *lda, const size_t *m, const size_t *n,
 				    const uint32_t *p, const int *kernel, size_t *rank,

@@ -471,6 +471,20 @@ int lela_cuda_echelon_zp_u32_batch(lela_cuda_ctx *h, size_t count, uint32_t *con
   }
   int st = ctx_clear_status(c);
   if (st) return st;
+  // big items run on worker handles (own streams) while the small ones run
+  // on this handle's stream; the caller's queued work must be done first
+  const int nworkers = (int)std::min<size_t>(big_idx.size(), 8);
+  if (nworkers > 1) {
+    while ((int)h->workers.size() < nworkers) {
+      lela_cuda_ctx *w = nullptr;
+      if ((st = lela_cuda_create(&w, c->device))) return ctx_fail(c, st, "batch: worker handle");
+      h->workers.push_back(w);
+    }
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return ctx_cuda(c, e, "batch: synchronize");
+  }
+  std::vector<uint64_t> hr(small.size());
+  std::vector<uint32_t> hd(small.size()), hs(small.size());
   if (!small.empty()) {
     const size_t ns = small.size();
     void *buf = nullptr;
@@ -517,11 +531,59 @@ int lela_cuda_echelon_zp_u32_batch(lela_cuda_ctx *h, size_t count, uint32_t *con
     int pi = prof_begin(c, "echelon_small_batch_graph");
     e = cudaGraphLaunch(c->batch_exec, c->stream);
     prof_end(c, pi);
-    std::vector<uint64_t> hr(ns);
-    std::vector<uint32_t> hd(ns), hs(ns);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(hr.data(), d_rank, ns * 8, cudaMemcpyDeviceToHost, c->stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(hd.data(), d_det, ns * 4, cudaMemcpyDeviceToHost, c->stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(hs.data(), d_status, ns * 4, cudaMemcpyDeviceToHost, c->stream);
+    if (e != cudaSuccess) return ctx_cuda(c, e, "batch: graph launch");
+    c->batch_rank = d_rank;
+    c->batch_det = d_det;
+    c->batch_status = d_status;
+  }
+  // big items: the panel pipeline, with the trailing-update gemm chosen per
+  // item (kernel 3: CUDA cores, else tensor cores); largest first over the
+  // workers when there are several
+  std::vector<size_t> order(big_idx);
+  std::sort(order.begin(), order.end(),
+            [&](size_t a, size_t b) { return m[a] * n[a] > m[b] * n[b]; });
+  std::atomic<size_t> next(0);
+  std::atomic<int> fatal(0);
+  auto run = [&](Ctx *wc) {
+    const int saved = wc->gemm_kernel;
+    for (size_t j = next++; j < order.size() && !fatal.load(); j = next++) {
+      const size_t i = order[j];
+      const int k = kernel ? kernel[i] : 0;
+      wc->gemm_kernel = (k == 3) ? GEMM_PLAIN : GEMM_TC;
+      size_t r = 0;
+      uint32_t d = 1;
+      int s = zp_echelon_dev(wc, (int)m[i], (int)n[i], p[i], A[i], lda[i], &r, &d, nullptr);
+      if (s == ST_OK && wc != c) s = ctx_check_status(wc, "echelon_zp_u32_batch");
+      if (s != ST_OK && s != ST_PIVOT) {
+        int none = 0;  // the first failure reports
+        if (fatal.compare_exchange_strong(none, s) && wc != c) c->last_error = wc->last_error;
+        break;
+      }
+      rank[i] = r;
+      det[i] = d;
+      status[i] = s;
+    }
+    wc->gemm_kernel = saved;
+  };
+  if (nworkers > 1) {
+    std::vector<std::thread> th;
+    for (int t = 0; t < nworkers; ++t)
+      th.emplace_back([&, t] {
+        cudaSetDevice(c->device);
+        run(&h->workers[t]->c);
+      });
+    for (auto &x : th) x.join();
+  } else {
+    run(c);
+  }
+  if (!small.empty()) {
+    const size_t ns = small.size();
+    cudaError_t e = cudaMemcpyAsync(hr.data(), c->batch_rank, ns * 8, cudaMemcpyDeviceToHost,
+                                    c->stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(hd.data(), c->batch_det, ns * 4, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(hs.data(), c->batch_status, ns * 4, cudaMemcpyDeviceToHost, c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) return ctx_cuda(c, e, "batch: small blocks");
     for (size_t j = 0; j < ns; ++j) {
@@ -531,22 +593,10 @@ int lela_cuda_echelon_zp_u32_batch(lela_cuda_ctx *h, size_t count, uint32_t *con
       status[i] = (int)hs[j];
     }
   }
-  const int saved = c->gemm_kernel;
-  for (size_t i : big_idx) {
-    const int k = kernel ? kernel[i] : 0;
-    c->gemm_kernel = (k == 3) ? GEMM_PLAIN : GEMM_TC;
-    size_t r = 0;
-    uint32_t d = 1;
-    int s = zp_echelon_dev(c, (int)m[i], (int)n[i], p[i], A[i], lda[i], &r, &d, nullptr);
-    if (s != ST_OK && s != ST_PIVOT) {
-      c->gemm_kernel = saved;
-      return s;
-    }
-    rank[i] = r;
-    det[i] = d;
-    status[i] = s;
+  if (fatal.load()) {
+    const std::string msg = c->last_error;
+    return ctx_fail(c, fatal.load(), msg.c_str());
   }
-  c->gemm_kernel = saved;
   return ctx_check_status(c, "echelon_zp_u32_batch");
 }
 

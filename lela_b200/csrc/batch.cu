@@ -8,9 +8,10 @@
 // 47-139 with DensePivotStrategy, pivot-strategy.tcc:19-42) and writes the
 // echelon form, rank and det back.  The launch has a fixed shape, so it can
 // be captured in a CUDA graph and replayed.  Larger blocks go through the
-// panel pipeline of echelon.cu; the kernel used for their trailing updates
-// (tensor-core or CUDA-core gemm) is chosen per block by the caller's
-// selector.  Faugere-Lachartre matrices are spread over worker threads, each
+// panel pipeline of echelon.cu, spread over worker handles with their own
+// streams while the persistent launch runs; the kernel used for their
+// trailing updates (tensor-core or CUDA-core gemm) is chosen per block by the
+// caller's selector.  Faugere-Lachartre matrices are spread over worker threads, each
 // with its own handle state and CUDA stream, so one matrix's host-side
 // steps overlap another's GPU work.
 #include <atomic>

@@ -65,6 +65,9 @@ struct Ctx {
   cudaGraphExec_t batch_exec = nullptr;
   size_t batch_ns = 0;
   void *batch_buf = nullptr;
+  // Device result arrays of the last small-block batch launch.
+  uint64_t *batch_rank = nullptr;
+  uint32_t *batch_det = nullptr, *batch_status = nullptr;
 
   // Kernel launches issued through this handle (all kernels of the library).
   uint64_t launches = 0;
