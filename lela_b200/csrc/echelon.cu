@@ -202,96 +202,124 @@ __global__ void __launch_bounds__(HEADS_THREADS)
 }
 
 // 2. The reference's pivot choice on the panel (see the file comment).
-// The rows at positions i0 .. i0+PW_R-1 form a window kept in shared memory
-// and eliminated eagerly, without division: when the pivot row P (pivot
-// value y) is chosen, every other window row W below it becomes
-// y W - W[col] P.  So a non-pivot window row holds S_t times its row
-// reduced by the t pivots so far (S_t = y_0 ... y_{t-1}) and pivot row k
-// holds S_k U_k; the pivot of a column is the first window row, by
-// position, with a nonzero there.  Rows below the window are touched only
-// when no window row has one and the head histogram says that one of them
-// may: they are then reduced by the same recurrence, in position order.
-// At the end the S_k and the pivots x_k = y_k / S_k are inverted in
+// The window: the first PW_R rows at or below i0, by position, with a nonzero
+// in the panel, kept in shared memory and eliminated eagerly without
+// division: when pivot row P (pivot value y) is chosen, every window row W
+// becomes y W - W[col] P.  So a window row holds S_t times its row reduced
+// by the t pivots so far (S_t = y_0 ... y_{t-1}); pivot rows move to PV,
+// holding S_k U_k.  Rows between window rows are zero in the panel and can
+// never hold a pivot.  The pivot of a column is the first window row, by
+// position, with a nonzero there; rows past the last window position are
+// reached only when no window row has one and the head histogram says one
+// of them may: they are then reduced by the same recurrence, in position
+// order.  At the end the S_k and the pivots x_k = y_k / S_k are inverted in
 // parallel.  Outputs: PanelOut; U (t x EW, row stride EW: the pivot rows'
 // final panel values) and the pivot inverses.  Resets *last_act to -1 and
 // hist[] to zero for the next panel.
 //
-// Window bookkeeping: perm[s] is the shared-memory slot of the row at
-// position i0 + s (double-buffered, rewritten each column), wrow[slot] its
-// row index in D.  Rows below the window are found through p2r / stamp and
-// carry in head[] a lower bound of the first nonzero column of their
-// reduced panel part; cnt[h] counts them by that bound.
-constexpr int PW_R = 80;                     // window rows
-constexpr int PW_FIND = (PW_R + 31) / 32;    // warps that test window rows
+// Bookkeeping: the window is a list of entries sorted by position, entry ->
+// shared-memory slot (perm) and position (ppos), double-buffered and
+// rewritten each column; wrow[slot] is the row index in D.  A transposition
+// (i, q) moves the row at position i to q: a window row keeps its entry
+// (with position q); a row outside the window (zero in the panel) is
+// recorded in p2r / stamp.  Rows past the window carry in head[] a lower
+// bound of the first nonzero column of their reduced panel part; cnt[h]
+// counts them by that bound.
+constexpr int PW_R = 80;                   // window rows
+constexpr int PW_FIND = (PW_R + 31) / 32;  // warps that test window rows
+constexpr size_t PW_SMEM = (size_t)PW_R * EW * 4;  // dynamic shared memory: the window rows
 
 template <class A>
 __global__ void __launch_bounds__(PS_THREADS)
     panel_search_kernel(const uint32_t *__restrict__ D, size_t ld, int i0, int m, int c0, int w,
-                        A ar, uint8_t *__restrict__ head,
-                        const uint8_t *__restrict__ act, int *__restrict__ hist,
-                        int *__restrict__ last_act, int *__restrict__ p2r, int *__restrict__ stamp,
-                        int epoch, uint32_t *__restrict__ Uout, uint32_t *__restrict__ xinv_out,
-                        PanelOut *out) {
-  __shared__ uint32_t Wv[PW_R][EW];
-  __shared__ int perm[2][PW_R];
+                        A ar, uint8_t *__restrict__ head, const uint8_t *__restrict__ act,
+                        int *__restrict__ hist, int *__restrict__ last_act, int *__restrict__ p2r,
+                        int *__restrict__ stamp, int epoch, uint32_t *__restrict__ Uout,
+                        uint32_t *__restrict__ xinv_out, PanelOut *out) {
+  extern __shared__ __align__(16) uint32_t dyn_w[];
+  uint32_t(*Wv)[EW] = reinterpret_cast<uint32_t(*)[EW]>(dyn_w);  // PW_R rows
+  __shared__ uint32_t PV[EW][EW];
+  __shared__ int perm[2][PW_R], ppos[2][PW_R];
   __shared__ int wrow[PW_R];
-  __shared__ uint32_t s_red[PS_FAST][EW];  // rows below the window, reduced (one per warp)
+  __shared__ uint32_t s_red[PS_FAST][EW];  // rows past the window, reduced (one per warp)
   __shared__ int s_pcol[EW];
   __shared__ uint32_t s_y[EW], s_S[EW], s_x[EW], s_sinv[EW];
   __shared__ int s_cnt[EW + 1];
   __shared__ int s_first[PS_FAST], s_wcnt[PS_FAST];
   __shared__ int s_list[PS_THREADS], s_lrow[PS_THREADS], s_lhead[PS_THREADS];
-  __shared__ int s_err, s_last, s_hi;
+  __shared__ int s_err, s_last, s_hi, s_wlast;
   const uint32_t p = ar.p;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-  const int nw = min(PW_R, m - i0);
-  const int wend = i0 + nw;  // first position below the window
 
-  for (int e = tid; e < nw * EW; e += PS_THREADS) {
-    const int k = e / EW, c = e % EW;
-    const uint32_t *src = D + (size_t)(i0 + k) * ld + c0;
-    cp_async4(&Wv[k][c], src + (c < w ? c : 0), c < w);
-  }
-  for (int k = tid; k < nw; k += PS_THREADS) {
-    perm[0][k] = k;
-    wrow[k] = i0 + k;
-  }
+  // the window: ordered compaction of the rows with a nonzero panel
+  int nl = 0;
+  if (tid == 0) s_wlast = m - 1;
   if (tid <= EW) {
     s_cnt[tid] = hist[tid];
     hist[tid] = 0;
   }
+  for (int base = i0; base < m && nl < PW_R; base += PS_THREADS) {
+    const int pos = base + tid;
+    const bool a = pos < m && act[pos];
+    const unsigned bal = __ballot_sync(0xffffffffu, a);
+    if (lane == 0) s_wcnt[wid] = __popc(bal);
+    __syncthreads();
+    int off = 0, cnt = 0;
+    for (int k = 0; k < PS_FAST; ++k) {
+      const int v = s_wcnt[k];
+      off += k < wid ? v : 0;
+      cnt += v;
+    }
+    off += __popc(bal & ((1u << lane) - 1u));
+    const int take = min(cnt, PW_R - nl);
+    if (a && off < take) {
+      const int slot = nl + off;
+      perm[0][slot] = slot;
+      ppos[0][slot] = pos;
+      wrow[slot] = pos;
+      const uint32_t *src = D + (size_t)pos * ld + c0;
+      for (int c = 0; c < EW; ++c) cp_async4(&Wv[slot][c], src + (c < w ? c : 0), c < w);
+      if (off == PW_R - 1 - nl) s_wlast = pos;
+    }
+    nl += take;
+    __syncthreads();  // s_wcnt is rewritten by the next pass
+  }
   cp_async_wait_all();
   __syncthreads();
-  for (int k = tid; k < nw; k += PS_THREADS) atomicSub(&s_cnt[head[i0 + k]], 1);
+  const int wlast = s_wlast;  // rows past it are outside the window
+  for (int k = tid; k < nl; k += PS_THREADS) atomicSub(&s_cnt[head[wrow[k]]], 1);
   __syncthreads();
 
   int cur = 0, i = i0, t = 0;
   uint32_t S = 1u % p;
   for (int col = 0; col < w && i < m; ++col) {
-    const int *pm = perm[cur];
-    // A. first window row at or below position i with a nonzero in col
+    const int *pm = perm[cur], *pp = ppos[cur];
+    int *pn = perm[cur ^ 1], *ppn = ppos[cur ^ 1];
+    // A. first window entry (by position) with a nonzero in col
     if (wid < PW_FIND) {
-      const int s = t + tid;
-      const bool nz = s < nw && Wv[pm[s]][col] != 0u;
+      const bool nz = tid < nl && Wv[pm[tid]][col] != 0u;
       const unsigned b = __ballot_sync(0xffffffffu, nz);
-      if (lane == 0) s_first[wid] = b ? s + __ffs(b) - 1 - lane : 0x7fffffff;
+      if (lane == 0) s_first[wid] = b ? tid + __ffs(b) - 1 : 0x7fffffff;
     }
     __syncthreads();
     int qs = 0x7fffffff;
     for (int k = 0; k < PW_FIND; ++k) qs = min(qs, s_first[k]);
+    const bool z = nl > 0 && pp[0] == i;  // the row at position i is window entry 0
+    const uint32_t *P;                    // the pivot row (S_t times reduced)
+    int q, drop;                          // pivot position; window entry leaving (-1: none)
+    bool relocate0 = false;               // entry 0 moves to position q, in place of qs
     if (qs == 0x7fffffff) {
-      // none in the window: rows below it whose bound allows a pivot here
+      // none in the window: rows past it whose bound allows a pivot here
       int cand = 0;
-      if (wend < m)
+      if (wlast < m - 1)
         for (int h = 0; h <= col; ++h) cand += s_cnt[h];
       __syncthreads();  // every thread has its count before s_cnt changes
       if (cand == 0) continue;
-      // scan them in position order: per pass the CTA lists the candidates
-      // among PS_THREADS positions (ordered compaction), then each warp
-      // reduces one of them by the t pivots, W <- y_k W - W[pcol_k] (S_k U_k),
-      // and records its exact head
+      // per pass the CTA lists the candidates among PS_THREADS positions
+      // (ordered compaction), then each warp reduces one of them by the t
+      // pivots, W <- y_k W - W[pcol_k] (S_k U_k), and records its exact head
       int found = -1, fw = 0;
-      for (int base = wend; base < m && cand > 0 && found < 0; base += PS_THREADS) {
+      for (int base = wlast + 1; base < m && cand > 0 && found < 0; base += PS_THREADS) {
         const int pos = base + tid;
         int r = -1, hr = HEAD_NONE;
         if (pos < m) {
@@ -326,9 +354,8 @@ __global__ void __launch_bounds__(PS_THREADS)
               const int pc = s_pcol[k];
               const uint32_t f = __shfl_sync(0xffffffffu, pc < 32 ? a0 : a1, pc & 31);
               const uint32_t nf = f ? p - f : 0u;
-              const uint32_t *P = Wv[pm[k]];
-              a0 = ar.dot2(s_y[k], a0, nf, P[lane]);
-              a1 = ar.dot2(s_y[k], a1, nf, P[lane + 32]);
+              a0 = ar.dot2(s_y[k], a0, nf, PV[k][lane]);
+              a1 = ar.dot2(s_y[k], a1, nf, PV[k][lane + 32]);
             }
             s_red[wid][lane] = a0;
             s_red[wid][lane + 32] = a1;
@@ -357,59 +384,85 @@ __global__ void __launch_bounds__(PS_THREADS)
         __syncthreads();
         continue;
       }
-      // the pivot comes from below the window: it takes the slot of position
-      // i, whose row goes to position `found` with the bound of its values
-      const int slot = pm[t];
+      // the pivot comes from past the window; the row at position i goes to
+      // position `found`: window entry 0 leaves the window (with the bound
+      // of its values), a row outside it is recorded in p2r
+      q = found;
+      P = s_red[fw];
+      drop = z ? 0 : -1;
       if (wid == 0) {
-        const uint32_t b0v = Wv[slot][lane], b1v = Wv[slot][lane + 32];
-        const unsigned b0 = __ballot_sync(0xffffffffu, b0v != 0u && lane > col);
-        const unsigned b1 = __ballot_sync(0xffffffffu, b1v != 0u && lane + 32 > col);
-        const int hd = b0 ? __ffs(b0) - 1 : (b1 ? 32 + __ffs(b1) - 1 : HEAD_NONE);
+        int hd = HEAD_NONE;
+        if (z) {
+          const uint32_t *E = Wv[pm[0]];
+          const unsigned b0 = __ballot_sync(0xffffffffu, E[lane] != 0u && lane > col);
+          const unsigned b1 = __ballot_sync(0xffffffffu, E[lane + 32] != 0u && lane + 32 > col);
+          hd = b0 ? __ffs(b0) - 1 : (b1 ? 32 + __ffs(b1) - 1 : HEAD_NONE);
+        }
         if (lane == 0) {
-          const int ri = wrow[slot], rq = row_at(found, p2r, stamp, epoch);
-          head[ri] = (uint8_t)hd;
-          atomicAdd(&s_cnt[hd], 1);
+          const int rq = row_at(q, p2r, stamp, epoch);
           atomicSub(&s_cnt[head[rq]], 1);
-          p2r[found] = ri;
-          stamp[found] = epoch;
-          wrow[slot] = rq;
+          int ri;
+          if (z) {
+            ri = wrow[pm[0]];
+            head[ri] = (uint8_t)hd;
+            atomicAdd(&s_cnt[hd], 1);
+          } else {
+            ri = row_at(i, p2r, stamp, epoch);
+          }
+          p2r[q] = ri;
+          stamp[q] = epoch;
         }
       }
-      __syncthreads();
-      if (tid < EW) Wv[slot][tid] = s_red[fw][tid];
-      if (tid == 0) s_first[0] = found;
-      __syncthreads();
-      qs = -1;  // marks "pivot now in slot pm[t]", transposition (i, found)
+    } else {
+      q = pp[qs];
+      P = Wv[pm[qs]];
+      drop = qs;
+      relocate0 = z && qs > 0;
+      if (!z && q != i && tid == 0) {  // the row at i is outside the window
+        p2r[q] = row_at(i, p2r, stamp, epoch);
+        stamp[q] = epoch;
+      }
     }
-    // B. pivot at position slot qp; eliminate the other window rows below
-    const int qp = qs < 0 ? t : qs;
-    const int tq = qs < 0 ? s_first[0] : i0 + qs;
-    const int ps = pm[qp];
-    const uint32_t y = Wv[ps][col];
+    // B. eliminate the window rows that stay, keep the pivot row in PV, and
+    // write the new entry list
+    const uint32_t y = P[col];
     {
       const int c = tid & (EW - 1);
       if (c > col && c < w) {
-        const uint32_t pc = Wv[ps][c];
-        for (int s = t + (tid >> 6); s < nw; s += PS_PARTS) {
-          if (s == qp) continue;
+        const uint32_t pc = P[c];
+        for (int s = tid >> 6; s < nl; s += PS_PARTS) {
+          if (s == drop) continue;
           const int pr = pm[s];
           const uint32_t a = Wv[pr][col];
           Wv[pr][c] = ar.dot2(y, Wv[pr][c], a ? p - a : 0u, pc);
         }
       }
     }
-    int *pn = perm[cur ^ 1];
-    for (int s = tid; s < nw; s += PS_THREADS) pn[s] = s == t ? pm[qp] : (s == qp ? pm[t] : pm[s]);
+    if (tid < EW) PV[t][tid] = P[tid];
+    const int nn = drop >= 0 ? nl - 1 : nl;
+    for (int s = tid; s < nn; s += PS_THREADS) {
+      int src, pos;
+      if (relocate0) {
+        src = s < drop - 1 ? s + 1 : (s == drop - 1 ? 0 : s + 1);
+        pos = s == drop - 1 ? q : pp[src];
+      } else {
+        src = (drop >= 0 && s >= drop) ? s + 1 : s;
+        pos = pp[src];
+      }
+      pn[s] = pm[src];
+      ppn[s] = pos;
+    }
     if (tid == 0) {
       s_pcol[t] = col;
       s_y[t] = y;
       s_S[t] = S;
       out->pcol[t] = (uint32_t)col;
       out->ti[t] = (uint32_t)i;
-      out->tq[t] = (uint32_t)tq;
+      out->tq[t] = (uint32_t)q;
     }
     __syncthreads();
     cur ^= 1;
+    nl = nn;
     S = ar.mul(S, y);
     ++i;
     ++t;
@@ -435,19 +488,19 @@ __global__ void __launch_bounds__(PS_THREADS)
     atomicMax(&s_hi, (int)out->tq[tid]);
   }
   __syncthreads();
-  // U_k = (S_k U_k) / S_k; the window keeps only the columns right of the
-  // latest pivot up to date, and U_k is zero left of its pivot column
+  // U_k = (S_k U_k) / S_k; entries left of the pivot column are not kept up
+  // to date, and U_k is zero there
   for (int e = tid; e < t * EW; e += PS_THREADS) {
     const int k = e / EW, c = e % EW;
-    Uout[e] = c < s_pcol[k] ? 0u : ar.mul(Wv[perm[cur][k]][c], s_sinv[k]);
+    Uout[e] = c < s_pcol[k] ? 0u : ar.mul(PV[k][c], s_sinv[k]);
   }
-  // last final position of a non-pivot row with a nonzero panel: window
-  // positions through their slots, positions below it up to the largest
-  // transposition target through p2r, beyond that rows have not moved
+  // last final position of a non-pivot row with a nonzero panel: the window
+  // entries, positions past the window up to the largest transposition target
+  // through p2r; beyond that rows have not moved
   const int hi = s_hi;
-  for (int s = t + tid; s < nw; s += PS_THREADS)
-    if (act[wrow[perm[cur][s]]]) atomicMax(&s_last, i0 + s);
-  for (int pos = max(wend, i) + tid; pos <= hi && pos < m; pos += PS_THREADS)
+  for (int s = tid; s < nl; s += PS_THREADS)
+    if (act[wrow[perm[cur][s]]]) atomicMax(&s_last, ppos[cur][s]);
+  for (int pos = max(wlast + 1, i) + tid; pos <= hi && pos < m; pos += PS_THREADS)
     if (act[row_at(pos, p2r, stamp, epoch)]) atomicMax(&s_last, pos);
   __syncthreads();
   if (tid == 0) {
@@ -595,6 +648,16 @@ int zp_echelon_dev(Ctx *c, int m, int n, uint32_t p, uint32_t *D, size_t ld, siz
   st = ctx_workspace(c, zp_gemm_workspace_bytes(p, m, n, EW), &gws);
   if (st) return st;
   const bool small = p < (1u << 16);
+  static std::once_flag once;
+  static cudaError_t attr_err = cudaSuccess;
+  std::call_once(once, [] {
+    attr_err = cudaFuncSetAttribute(panel_search_kernel<ArithSmall>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PW_SMEM);
+    if (attr_err == cudaSuccess)
+      attr_err = cudaFuncSetAttribute(panel_search_kernel<ArithWide>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PW_SMEM);
+  });
+  if (attr_err != cudaSuccess) return ctx_cuda(c, attr_err, "echelon: panel search attributes");
   const ArithSmall ars = ArithSmall::make(p);
   const ArithWide arw = ArithWide::make(p);
   cudaError_t e = cudaMemsetAsync(d_stamp, 0xff, (size_t)m * sizeof(int), c->stream);
@@ -614,11 +677,11 @@ int zp_echelon_dev(Ctx *c, int m, int n, uint32_t p, uint32_t *D, size_t ld, siz
     prof_end(c, pi);
     pi = prof_begin(c, "ech_search");
     if (small)
-      panel_search_kernel<<<1, PS_THREADS, 0, c->stream>>>(
+      panel_search_kernel<<<1, PS_THREADS, PW_SMEM, c->stream>>>(
           D, ld, i, m, c0, w, ars, d_head, d_act, d_hist, d_last, d_p2r, d_stamp, epoch, d_U,
           d_xinv, d_out);
     else
-      panel_search_kernel<<<1, PS_THREADS, 0, c->stream>>>(
+      panel_search_kernel<<<1, PS_THREADS, PW_SMEM, c->stream>>>(
           D, ld, i, m, c0, w, arw, d_head, d_act, d_hist, d_last, d_p2r, d_stamp, epoch, d_U,
           d_xinv, d_out);
     ++epoch;
