@@ -60,9 +60,10 @@ enum {
 
 /* Kernel choice for the Z/p gemm (lela_cuda_set_gemm_kernel). */
 enum {
-	LELA_CUDA_GEMM_AUTO = 0,   /* tensor-core kernel */
+	LELA_CUDA_GEMM_AUTO = 0,   /* small-K CUDA-core kernel for small problems, else tensor cores */
 	LELA_CUDA_GEMM_PLAIN = 1,  /* CUDA-core delayed-reduction kernel */
-	LELA_CUDA_GEMM_TC = 2      /* limb-split INT8 tcgen05 kernel */
+	LELA_CUDA_GEMM_TC = 2,     /* limb-split INT8 tcgen05 kernel */
+	LELA_CUDA_GEMM_SMALLK = 3  /* CUDA-core kernel for small K (unchecked sums when p < 2^28) */
 };
 
 /* ---------------------------------------------------------------- handle

@@ -25,7 +25,7 @@ _U = ctypes.c_uint32
 _I = ctypes.c_int
 
 OK, ERR_ARG, ERR_CUDA, ERR_NOMEM, DIAG, WRONG_FORM, PIVOT, TIMEOUT, UNSUPPORTED = range(9)
-GEMM_AUTO, GEMM_PLAIN, GEMM_TC = 0, 1, 2
+GEMM_AUTO, GEMM_PLAIN, GEMM_TC, GEMM_SMALLK = 0, 1, 2, 3
 
 
 class LELAError(Exception):

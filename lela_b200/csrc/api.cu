@@ -230,7 +230,7 @@ int lela_cuda_synchronize(lela_cuda_ctx *h) {
 }
 
 int lela_cuda_set_gemm_kernel(lela_cuda_ctx *h, int kernel) {
-  if (!h || kernel < GEMM_AUTO || kernel > GEMM_TC) return ST_ARG;
+  if (!h || kernel < GEMM_AUTO || kernel > GEMM_SMALLK) return ST_ARG;
   h->c.gemm_kernel = kernel;
   return ST_OK;
 }

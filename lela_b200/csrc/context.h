@@ -18,9 +18,10 @@ namespace lela {
 
 // Kernel families a caller (or the selector) can force.
 enum GemmKernel : int {
-  GEMM_AUTO = 0,   // tensor-core path when the shape allows it
-  GEMM_PLAIN = 1,  // CUDA-core 64-bit delayed-reduction gemm
-  GEMM_TC = 2,     // limb-split INT8 tcgen05 gemm
+  GEMM_AUTO = 0,    // small-K CUDA-core kernel below its crossover, else tensor cores
+  GEMM_PLAIN = 1,   // CUDA-core 64-bit delayed-reduction gemm (the plain GPU form)
+  GEMM_TC = 2,      // limb-split INT8 tcgen05 gemm
+  GEMM_SMALLK = 3,  // CUDA-core gemm for small K (no per-term wrap check when p < 2^28)
 };
 
 // GF(2) gemm kernels.

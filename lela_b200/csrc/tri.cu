@@ -19,6 +19,7 @@
 // reported and B is left unchanged (the reference leaves it partially
 // solved, which callers such as Faugere-Lachartre discard).
 #include <algorithm>
+#include <mutex>
 
 #include "common.cuh"
 #include "context.h"
@@ -164,38 +165,6 @@ __global__ void __launch_bounds__(64)
   for (int k = 0; k < TRI_NB; ++k) out[k * TRI_NB + j] = (j < nb) ? x[k] : 0u;
 }
 
-// B (nb x ncols) <- alpha * Tinv * B in place: one CTA per 64-column tile
-// (the tile is read completely before it is overwritten).
-__global__ void __launch_bounds__(256)
-    tri_apply_kernel(const uint32_t *__restrict__ Tinv, int nb, uint32_t *__restrict__ B,
-                     size_t ldb, int ncols, Modulus mod, uint32_t two64, uint32_t alpha) {
-  __shared__ uint32_t sT[TRI_NB][TRI_NB + 1];
-  __shared__ uint32_t sB[TRI_NB][TRI_NB + 1];
-  const int c0 = blockIdx.x * TRI_NB;
-  for (int e = threadIdx.x; e < TRI_NB * TRI_NB; e += blockDim.x) {
-    int r = e / TRI_NB, cc = e % TRI_NB;
-    sT[r][cc] = Tinv[r * TRI_NB + cc];
-    sB[r][cc] = (r < nb && c0 + cc < ncols) ? B[(size_t)r * ldb + c0 + cc] : 0u;
-  }
-  __syncthreads();
-  const int cc = threadIdx.x & 63, r4 = threadIdx.x >> 6;  // 4 row groups of 16 rows
-  if (c0 + cc >= ncols) return;
-#pragma unroll 1
-  for (int rr = 0; rr < 16; ++rr) {
-    const int r = r4 * 16 + rr;
-    if (r >= nb) break;
-    uint64_t s = 0;
-#pragma unroll 16
-    for (int k = 0; k < TRI_NB; ++k) {
-      uint64_t t = (uint64_t)sT[r][k] * sB[k][cc];
-      s += t;
-      if (s < t) s += two64;
-    }
-    uint32_t v = mod_reduce(s, mod);
-    B[(size_t)r * ldb + c0 + cc] = (alpha == 1u) ? v : mod_mul(v, alpha, mod);
-  }
-}
-
 // C <- beta * C for an m x n block (beta in [0, p)).
 __global__ void zp_scale2_kernel(uint32_t *C, size_t ldc, int M, int N, Modulus mod,
                                  uint32_t beta) {
@@ -237,18 +206,168 @@ struct TriLeaves {
   const uint32_t *tinv;
 };
 
-static int tri_apply_leaf(Ctx *c, const TriLeaves &L, int m, const uint32_t *A, size_t lda,
-                          uint32_t *B, size_t ldb, int n, uint32_t p, uint32_t alpha) {
+// Diagonal blocks of up to TB_NB rows in one launch: each CTA holds a
+// CT-column slice of the block's B in shared memory and runs the whole
+// block's substitution over its 64-row sub-blocks (upper: last first): the
+// sub-block's rows minus A's off-diagonal 64 x 64 tiles times the solved
+// sub-blocks, then times the inverted diagonal 64-block.  A thread owns a
+// register tile of RPT rows x 4 columns.  NOWRAP (p < 2^28): 64-term sums
+// cannot wrap, no per-term check.
+constexpr int TB_NB = 512;
+constexpr int TB_THREADS = 256;
+
+template <bool UPPER, bool NOWRAP, int CT>
+__global__ void __launch_bounds__(TB_THREADS)
+    tri_block_kernel(const uint32_t *__restrict__ A, size_t lda, const uint32_t *__restrict__ Tinv,
+                     int nb, uint32_t *__restrict__ B, size_t ldb, int ncols, Modulus mod,
+                     uint32_t two64, uint32_t alpha) {
+  constexpr int CG = CT / 4;              // column groups (4 columns each, stride CG)
+  constexpr int RG = TB_THREADS / CG;     // row groups
+  constexpr int RPT = TRI_NB / RG;        // rows per thread within a 64-row sub-block
+  extern __shared__ uint32_t Xs[];        // nb x CT
+  __shared__ uint32_t At[TRI_NB][TRI_NB + 1];
+  const int tid = threadIdx.x, cg = tid % CG, rg = tid / CG;
+  const int c0 = blockIdx.x * CT;
+  const uint32_t p = (uint32_t)mod.p;
+  // tiles come in through asynchronous copies (all in flight at once)
+  for (int e = tid; e < nb * CT; e += TB_THREADS) {
+    const int r = e / CT, cc = e % CT;
+    const bool ok = c0 + cc < ncols;
+    cp_async4(&Xs[e], ok ? B + (size_t)r * ldb + c0 + cc : B, ok);
+  }
+  cp_async_wait_all();
+  if (alpha != 1u)
+    for (int e = tid; e < nb * CT; e += TB_THREADS) Xs[e] = mod_mul(Xs[e], alpha, mod);
+  const int nsb = (nb + TRI_NB - 1) / TRI_NB;
+  for (int jj = 0; jj < nsb; ++jj) {
+    const int j = UPPER ? nsb - 1 - jj : jj;
+    const int r0 = j * TRI_NB, bj = min(TRI_NB, nb - r0);
+    __syncthreads();  // Xs written by the previous sub-block (or the load)
+    uint32_t y[RPT][4];
+#pragma unroll
+    for (int u = 0; u < RPT; ++u)
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        const int r = rg * RPT + u;
+        y[u][v] = r < bj ? Xs[(r0 + r) * CT + cg + CG * v] : 0u;
+      }
+    const int jlo = UPPER ? j + 1 : 0, jhi = UPPER ? nsb : j;
+    for (int j2 = jlo; j2 <= jhi; ++j2) {
+      // j2 < jhi (or > j for upper): an off-diagonal tile; the last pass
+      // (j2 == jhi) applies the inverted diagonal block to y
+      const bool diag = j2 == jhi;
+      const int k0 = diag ? r0 : j2 * TRI_NB, bk = diag ? bj : min(TRI_NB, nb - k0);
+      __syncthreads();  // At is free; for diag, every thread has read Xs below
+      if (diag) {
+#pragma unroll
+        for (int u = 0; u < RPT; ++u)
+#pragma unroll
+          for (int v = 0; v < 4; ++v) {
+            const int r = rg * RPT + u;
+            if (r < bj) Xs[(r0 + r) * CT + cg + CG * v] = y[u][v];
+          }
+        const uint32_t *T = Tinv + (size_t)j * TRI_NB * TRI_NB;
+        for (int e = tid; e < TRI_NB * TRI_NB; e += TB_THREADS)
+          cp_async4(&At[e / TRI_NB][e % TRI_NB], T + e, true);
+      } else {
+        for (int e = tid; e < TRI_NB * TRI_NB; e += TB_THREADS) {
+          const int rr = e / TRI_NB, kk = e % TRI_NB;
+          const bool ok = rr < bj && kk < bk;
+          cp_async4(&At[rr][kk], ok ? A + (size_t)(r0 + rr) * lda + k0 + kk : A, ok);
+        }
+      }
+      cp_async_wait_all();
+      __syncthreads();
+      uint64_t s[RPT][4];
+#pragma unroll
+      for (int u = 0; u < RPT; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) s[u][v] = 0;
+      for (int k = 0; k < bk; ++k) {
+        uint32_t xv[4], av[RPT];
+#pragma unroll
+        for (int v = 0; v < 4; ++v) xv[v] = Xs[(k0 + k) * CT + cg + CG * v];
+#pragma unroll
+        for (int u = 0; u < RPT; ++u) av[u] = At[rg * RPT + u][k];
+#pragma unroll
+        for (int u = 0; u < RPT; ++u)
+#pragma unroll
+          for (int v = 0; v < 4; ++v) {
+            const uint64_t t = (uint64_t)av[u] * xv[v];
+            s[u][v] += t;
+            if (!NOWRAP && s[u][v] < t) s[u][v] += two64;
+          }
+      }
+#pragma unroll
+      for (int u = 0; u < RPT; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+          const uint32_t w = mod_reduce(s[u][v], mod);
+          y[u][v] = diag ? w : (y[u][v] >= w ? y[u][v] - w : y[u][v] + (p - w));
+        }
+    }
+    __syncthreads();  // every thread has read the sub-block's right-hand sides
+#pragma unroll
+    for (int u = 0; u < RPT; ++u)
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        const int r = rg * RPT + u;
+        if (r < bj) Xs[(r0 + r) * CT + cg + CG * v] = y[u][v];
+      }
+  }
+  __syncthreads();
+  for (int e = tid; e < nb * CT; e += TB_THREADS) {
+    const int r = e / CT, cc = e % CT;
+    if (c0 + cc < ncols) B[(size_t)r * ldb + c0 + cc] = Xs[e];
+  }
+}
+
+static int tri_block(Ctx *c, const TriLeaves &L, bool upper, int m, const uint32_t *A, size_t lda,
+                     uint32_t *B, size_t ldb, int n, uint32_t p, uint32_t alpha) {
   if (n <= 0) return ST_OK;
+  static std::once_flag once;
+  static cudaError_t attr_err = cudaSuccess;
+  std::call_once(once, [] {
+    const void *fns[8] = {
+        (const void *)tri_block_kernel<true, true, 64>, (const void *)tri_block_kernel<true, false, 64>,
+        (const void *)tri_block_kernel<false, true, 64>, (const void *)tri_block_kernel<false, false, 64>,
+        (const void *)tri_block_kernel<true, true, 32>, (const void *)tri_block_kernel<true, false, 32>,
+        (const void *)tri_block_kernel<false, true, 32>, (const void *)tri_block_kernel<false, false, 32>};
+    for (int k = 0; k < 8 && attr_err == cudaSuccess; ++k)
+      attr_err = cudaFuncSetAttribute(fns[k], cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      TB_NB * (k < 4 ? 64 : 32) * 4);
+  });
+  if (attr_err != cudaSuccess) return ctx_cuda(c, attr_err, "cudaFuncSetAttribute(tri_block)");
   const size_t off = (size_t)(A - L.A_base) / (lda + 1);
   const uint32_t *T = L.tinv + (off / TRI_NB) * TRI_NB * TRI_NB;
-  int pi = prof_begin(c, "tri_apply");
-  tri_apply_kernel<<<(n + TRI_NB - 1) / TRI_NB, 256, 0, c->stream>>>(
-      T, m, B, ldb, n, make_modulus(p), two64_mod(p), alpha);
+  const Modulus mod = make_modulus(p);
+  const uint32_t t64 = two64_mod(p);
+  // 64-column slices when they still give every SM a CTA, else 32
+  const bool wide = n >= 64 * c->num_sms;
+  const int ct = wide ? 64 : 32;
+  const int grid = (n + ct - 1) / ct;
+  const size_t smem = (size_t)m * ct * 4;
+  const bool nowrap = p < (1u << 28);
+  int pi = prof_begin(c, "tri_block");
+#define TB_LAUNCH(U, W, C)                                                              \
+  tri_block_kernel<U, W, C><<<grid, TB_THREADS, smem, c->stream>>>(A, lda, T, m, B, ldb, n, \
+                                                                   mod, t64, alpha)
+  if (wide) {
+    if (upper && nowrap) TB_LAUNCH(true, true, 64);
+    else if (upper) TB_LAUNCH(true, false, 64);
+    else if (nowrap) TB_LAUNCH(false, true, 64);
+    else TB_LAUNCH(false, false, 64);
+  } else {
+    if (upper && nowrap) TB_LAUNCH(true, true, 32);
+    else if (upper) TB_LAUNCH(true, false, 32);
+    else if (nowrap) TB_LAUNCH(false, true, 32);
+    else TB_LAUNCH(false, false, 32);
+  }
+#undef TB_LAUNCH
   prof_end(c, pi);
   ctx_launched(c);
   cudaError_t e = cudaGetLastError();
-  return e == cudaSuccess ? ST_OK : ctx_cuda(c, e, "tri_apply launch");
+  return e == cudaSuccess ? ST_OK : ctx_cuda(c, e, "tri_block launch");
 }
 
 // Recursive solve (dinv is the inverted diagonal of the current sub-system).
@@ -256,7 +375,7 @@ static int trsm_rec(Ctx *c, const TriLeaves &TL, bool upper, int m, int n, uint3
                     uint32_t alpha, const uint32_t *A, size_t lda, const uint32_t *dinv,
                     uint32_t *B, size_t ldb, uint8_t *gemm_ws) {
   if (m <= 0) return ST_OK;
-  if (m <= TRI_NB) return tri_apply_leaf(c, TL, m, A, lda, B, ldb, n, p, alpha);
+  if (m <= TB_NB) return tri_block(c, TL, upper, m, A, lda, B, ldb, n, p, alpha);
   // split at a multiple of the leaf size, near the middle
   int l = ((m / 2 + TRI_NB - 1) / TRI_NB) * TRI_NB;
   if (l >= m) l = m - TRI_NB;

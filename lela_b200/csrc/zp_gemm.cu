@@ -37,6 +37,11 @@
 //    whose inner loop is exactly the reference's delayed-reduction dot
 //    (64-bit sum of 32x32-bit products, + 2^64 mod p on wrap-around, one
 //    final reduction).
+// 3. zp_gemm_smallk_kernel -- CUDA-core gemm for the small-K updates of the
+//    triangular solve and the echelon panels, where the tensor-core path's
+//    fixed cost (limb splits, tensor maps, pipeline start) dominates.  For
+//    p < 2^28 a 64-bit sum of 256 products cannot wrap, so the products are
+//    summed without checks and the sums reduced every 256 terms.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
@@ -511,6 +516,78 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// Same tiling as the plain kernel.  NOWRAP (p < 2^28): unchecked sums,
+// reduced modulo p after every 256 terms (256 (p-1)^2 < 2^64).
+template <bool NOWRAP>
+__global__ void __launch_bounds__(256)
+    zp_gemm_smallk_kernel(const uint32_t *__restrict__ A, size_t lda,
+                          const uint32_t *__restrict__ B, size_t ldb, uint32_t *__restrict__ C,
+                          size_t ldc, int M, int N, int K, Modulus mod, uint32_t two64,
+                          uint32_t alpha, uint32_t beta) {
+  __shared__ uint32_t As[PK][PT + 1];
+  __shared__ uint32_t Bs[PK][PT + 1];
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const int m0 = blockIdx.y * PT, n0 = blockIdx.x * PT;
+  uint64_t acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = 0;
+
+  for (int k0 = 0; k0 < K; k0 += PK) {
+#pragma unroll
+    for (int e = 0; e < (PT * PK) / 256; ++e) {
+      int idx = threadIdx.x + 256 * e;
+      int r = idx / PK, kk = idx % PK;
+      int gm = m0 + r, gk = k0 + kk;
+      As[kk][r] = (gm < M && gk < K) ? __ldg(A + (size_t)gm * lda + gk) : 0u;
+      int kr = idx / PT, c = idx % PT;
+      int gk2 = k0 + kr, gn = n0 + c;
+      Bs[kr][c] = (gk2 < K && gn < N) ? __ldg(B + (size_t)gk2 * ldb + gn) : 0u;
+    }
+    __syncthreads();
+#pragma unroll 8
+    for (int kk = 0; kk < PK; ++kk) {
+      uint32_t a[4], b[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i] = As[kk][ty + 16 * i];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) b[j] = Bs[kk][tx + 16 * j];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const uint64_t t = (uint64_t)a[i] * b[j];
+          if (NOWRAP) {
+            acc[i][j] += t;
+          } else {
+            const uint64_t s = acc[i][j] + t;
+            acc[i][j] = (s < t) ? s + two64 : s;
+          }
+        }
+    }
+    if (NOWRAP && ((k0 / PK) & 7) == 7)
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = mod_reduce(acc[i][j], mod);
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    int gm = m0 + ty + 16 * i;
+    if (gm >= M) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      int gn = n0 + tx + 16 * j;
+      if (gn >= N) continue;
+      uint32_t d = mod_reduce(acc[i][j], mod);
+      uint32_t c = beta ? C[(size_t)gm * ldc + gn] : 0u;
+      C[(size_t)gm * ldc + gn] = mod_axpby(alpha, d, beta, c, mod);
+    }
+  }
+}
+
 // Scale C <- beta * C (mod p), used when K = 0 or alpha = 0.
 __global__ void zp_scale_kernel(uint32_t *C, size_t ldc, int M, int N, Modulus mod,
                                 uint32_t beta) {
@@ -629,7 +706,31 @@ int zp_gemm_dev(Ctx *c, int kernel, int M, int N, int K, uint32_t p, uint32_t al
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? ST_OK : ctx_cuda(c, e, "zp_scale launch");
   }
-  if (kernel == GEMM_AUTO) kernel = c->gemm_kernel == GEMM_AUTO ? GEMM_TC : c->gemm_kernel;
+  if (kernel == GEMM_AUTO) kernel = c->gemm_kernel;
+  if (kernel == GEMM_AUTO) {
+    // small K: the CUDA-core kernel below its measured crossover with the
+    // tensor-core path (whose fixed and per-output costs grow with the limb
+    // count L)
+    const double work = (double)M * N * K;
+    const bool wide = zp_limbs_for(p) == 4;
+    const bool smallk = wide ? ((K <= 64 && work <= 4.0e9) || (K <= 256 && work <= 2.4e9))
+                             : ((K <= 32 && work <= 4.0e9) || (K <= 256 && work <= 6.0e8));
+    kernel = smallk ? GEMM_SMALLK : GEMM_TC;
+  }
+  if (kernel == GEMM_SMALLK) {
+    dim3 grid((N + PT - 1) / PT, (M + PT - 1) / PT);
+    int pi = prof_begin(c, "zp_gemm_smallk");
+    if (p < (1u << 28))
+      zp_gemm_smallk_kernel<true><<<grid, 256, 0, c->stream>>>(A, lda, B, ldb, C, ldc, M, N, K,
+                                                               mod, host_two64(p), alpha, beta);
+    else
+      zp_gemm_smallk_kernel<false><<<grid, 256, 0, c->stream>>>(A, lda, B, ldb, C, ldc, M, N, K,
+                                                                mod, host_two64(p), alpha, beta);
+    prof_end(c, pi);
+    ctx_launched(c);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? ST_OK : ctx_cuda(c, e, "zp_gemm_smallk launch");
+  }
   if (kernel == GEMM_PLAIN) {
     dim3 grid((N + PT - 1) / PT, (M + PT - 1) / PT);
     int pi = prof_begin(c, "zp_gemm_plain");

@@ -10,7 +10,7 @@ from lela_b200 import gen, api
 
 import props
 
-P_CASES = [2, 251, 256, 257, 65521, 65536, 65537, 2147483647, 4294967291]
+P_CASES = [2, 251, 256, 257, 65521, 65536, 65537, 268435455, 268435457, 2147483647, 4294967291]
 SHAPES = [(1, 1, 1), (17, 33, 5), (128, 128, 128), (130, 257, 300), (64, 300, 1000)]
 COEFFS = [(1, 1), ("m1", 1), (3, 0), (0, 5), (7, 11)]
 
@@ -20,7 +20,7 @@ def _coef(x, p):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("kernel", [api.GEMM_TC, api.GEMM_PLAIN])
+@pytest.mark.parametrize("kernel", [api.GEMM_TC, api.GEMM_PLAIN, api.GEMM_SMALLK, api.GEMM_AUTO])
 @pytest.mark.parametrize("p", P_CASES)
 def test_gemm_shapes_moduli(cuda, kernel, p):
     cuda.set_gemm_kernel(kernel)
