@@ -49,8 +49,9 @@ __global__ void diag_inverse_kernel(const uint32_t *__restrict__ A, size_t lda, 
 // triangular with inverted diagonal dinv (nullptr: unit diagonal).  The
 // column lives in registers; products accumulate in 64 bits with the
 // reference's wrap-around correction (+2^64 mod p) and one reduction per
-// entry.
-template <bool UPPER>
+// entry.  NOWRAP (p < 2^28): 64-term sums cannot wrap; two independent
+// partial sums per entry.
+template <bool UPPER, bool NOWRAP>
 __global__ void __launch_bounds__(128)
     tri_left_kernel(const uint32_t *__restrict__ T, size_t ldt, int nb,
                     const uint32_t *__restrict__ dinv, uint32_t *__restrict__ B, size_t ldb,
@@ -72,34 +73,32 @@ __global__ void __launch_bounds__(128)
     uint32_t v = (k < nb) ? B[(size_t)k * ldb + col] : 0u;
     x[k] = (alpha == 1u) ? v : mod_mul(v, alpha, mod);
   }
-  if (!UPPER) {
+  const bool unitd = dinv == nullptr;
 #pragma unroll
-    for (int k = 0; k < TRI_NB; ++k) {
-      uint64_t s = 0;
+  for (int kk = 0; kk < TRI_NB; ++kk) {
+    const int k = UPPER ? TRI_NB - 1 - kk : kk;
+    uint64_t s = 0, s2 = 0;
 #pragma unroll
-      for (int j = 0; j < k; ++j) {
-        uint64_t t = (uint64_t)sT[k][j] * x[j];
+    for (int j = 0; j < TRI_NB; ++j) {
+      if (UPPER ? j <= k : j >= k) continue;
+      const uint64_t t = (uint64_t)sT[k][j] * x[j];
+      if (NOWRAP) {
+        if (j & 1)
+          s2 += t;
+        else
+          s += t;
+      } else {
         s += t;
         if (s < t) s += two64;
       }
-      uint32_t r = mod_reduce(s, mod);
-      uint32_t v = x[k] >= r ? x[k] - r : x[k] + (p - r);
-      x[k] = (k < nb) ? mod_mul(v, sD[k], mod) : 0u;
     }
-  } else {
-#pragma unroll
-    for (int k = TRI_NB - 1; k >= 0; --k) {
-      uint64_t s = 0;
-#pragma unroll
-      for (int j = k + 1; j < TRI_NB; ++j) {
-        uint64_t t = (uint64_t)sT[k][j] * x[j];
-        s += t;
-        if (s < t) s += two64;
-      }
-      uint32_t r = mod_reduce(s, mod);
-      uint32_t v = x[k] >= r ? x[k] - r : x[k] + (p - r);
-      x[k] = (k < nb) ? mod_mul(v, sD[k], mod) : 0u;
+    uint32_t r = mod_reduce(s, mod);
+    if (NOWRAP) {
+      const uint32_t r2 = mod_reduce(s2, mod);
+      r = r + r2 >= p ? r + r2 - p : r + r2;
     }
+    const uint32_t v = x[k] >= r ? x[k] - r : x[k] + (p - r);
+    x[k] = (k < nb) ? (unitd ? v : mod_mul(v, sD[k], mod)) : 0u;
   }
 #pragma unroll
   for (int k = 0; k < TRI_NB; ++k)
@@ -183,15 +182,23 @@ int tri_left_block(Ctx *c, bool upper, int nb, const uint32_t *T, size_t ldt,
   if (nb <= 0 || ncols <= 0) return ST_OK;
   const Modulus mod = make_modulus(p);
   const uint32_t t64 = two64_mod(p);
-  const int threads = 128;
+  // 64-thread CTAs spread narrow right-hand sides over more SMs
+  const int threads = ncols >= 128 * c->num_sms ? 128 : 64;
   const int grid = (ncols + threads - 1) / threads;
+  const bool nowrap = p < (1u << 28);
   int pi = prof_begin(c, "tri_left");
-  if (upper)
-    tri_left_kernel<true><<<grid, threads, 0, c->stream>>>(T, ldt, nb, dinv, B, ldb, ncols, mod,
-                                                           t64, alpha);
+  if (upper && nowrap)
+    tri_left_kernel<true, true><<<grid, threads, 0, c->stream>>>(T, ldt, nb, dinv, B, ldb, ncols,
+                                                                 mod, t64, alpha);
+  else if (upper)
+    tri_left_kernel<true, false><<<grid, threads, 0, c->stream>>>(T, ldt, nb, dinv, B, ldb, ncols,
+                                                                  mod, t64, alpha);
+  else if (nowrap)
+    tri_left_kernel<false, true><<<grid, threads, 0, c->stream>>>(T, ldt, nb, dinv, B, ldb, ncols,
+                                                                  mod, t64, alpha);
   else
-    tri_left_kernel<false><<<grid, threads, 0, c->stream>>>(T, ldt, nb, dinv, B, ldb, ncols, mod,
-                                                            t64, alpha);
+    tri_left_kernel<false, false><<<grid, threads, 0, c->stream>>>(T, ldt, nb, dinv, B, ldb, ncols,
+                                                                   mod, t64, alpha);
   prof_end(c, pi);
   ctx_launched(c);
   cudaError_t e = cudaGetLastError();
