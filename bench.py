@@ -56,6 +56,8 @@ def parse():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fl", action="store_true")
+    ap.add_argument("--fl-only", action="store_true",
+                    help="run only the Faugere-Lachartre line (profiling aid)")
     ap.add_argument("--fl-m", type=int, default=20000)
     ap.add_argument("--fl-count", type=int, default=3)
     ap.add_argument("--no-gf2", action="store_true")
@@ -627,10 +629,24 @@ def run_ours(args):
         print(json.dumps(out), flush=True)
 
 
+def run_fl_only(args):
+    """Only the Faugere-Lachartre line (for kernel launch lists and
+    profiles): one process, one GPU; prints its JSON object."""
+    import torch
+    from lela_b200 import CudaModule
+    dev = torch.device("cuda", 0)
+    cm = CudaModule(0)
+    stream = torch.cuda.Stream(device=dev)
+    cm.set_stream(stream)
+    print(json.dumps(run_fl(args, cm, stream, torch, dev, 0)))
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.fl_only:
+        run_fl_only(args)
     else:
         run_ours(args)
 
