@@ -124,6 +124,14 @@ int lela_cuda_trsm_zp_u32 (lela_cuda_ctx *ctx, int upper, int diag_is_one, size_
 int lela_cuda_trsm_zp_u32_dev (lela_cuda_ctx *ctx, int upper, int diag_is_one, size_t m,
 			       size_t n, uint32_t p, uint32_t a, const uint32_t *A, size_t lda,
 			       uint32_t *B, size_t ldb, size_t *bad_idx);
+/* Diagonal-block solver of the trsm (and of the trsm steps inside
+ * Faugere-Lachartre); every choice gives the same B. */
+enum {
+	LELA_CUDA_TRSM_AUTO = 0,    /* inverse leaves when B is wide, else block substitution */
+	LELA_CUDA_TRSM_BLOCKS = 1,  /* 256-row blocks by substitution on CUDA cores */
+	LELA_CUDA_TRSM_INVERSE = 2  /* 512-row blocks inverted, applied by the tensor-core gemm */
+};
+int lela_cuda_set_trsm_kernel (lela_cuda_ctx *ctx, int kernel);
 
 /* ------------------------------------------------------- Z/p echelon form
  * A (m x n) <- its non-reduced row-echelon form, in place; *rank, *det =

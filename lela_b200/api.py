@@ -26,6 +26,7 @@ _I = ctypes.c_int
 
 OK, ERR_ARG, ERR_CUDA, ERR_NOMEM, DIAG, WRONG_FORM, PIVOT, TIMEOUT, UNSUPPORTED = range(9)
 GEMM_AUTO, GEMM_PLAIN, GEMM_TC, GEMM_SMALLK = 0, 1, 2, 3
+TRSM_AUTO, TRSM_BLOCKS, TRSM_INVERSE = 0, 1, 2
 
 
 class LELAError(Exception):
@@ -118,6 +119,7 @@ def _bind_optional(L):
         "lela_cuda_echelon_gf2": [_P, _S, _S, _P, _S, ctypes.POINTER(_S)],
         "lela_cuda_echelon_gf2_dev": [_P, _S, _S, _P, _S, ctypes.POINTER(_S)],
         "lela_cuda_set_gf2_kernel": [_P, _I],
+        "lela_cuda_set_trsm_kernel": [_P, _I],
     }
     for name, args in sigs.items():
         if hasattr(L, name):
@@ -313,6 +315,10 @@ class CudaModule:
     def set_gf2_kernel(self, kernel):
         """0 = auto (tensor cores), 1 = int8-expanded tcgen05, 2 = M4RM."""
         self._raise(self.L.lela_cuda_set_gf2_kernel(self.h, int(kernel)))
+
+    def set_trsm_kernel(self, kernel):
+        """0 = auto, 1 = 256-row block substitution, 2 = 512-row inverses on the tensor cores."""
+        self._raise(self.L.lela_cuda_set_trsm_kernel(self.h, int(kernel)))
 
     def gemm_gf2(self, A, B, C, n, k, a=1, b=1):
         """C <- a*A*B + b*C over GF(2) in place; packed uint64 rows (bit j of

@@ -369,6 +369,12 @@ int lela_cuda_set_gf2_kernel(lela_cuda_ctx *h, int kernel) {
   return ST_OK;
 }
 
+int lela_cuda_set_trsm_kernel(lela_cuda_ctx *h, int kernel) {
+  if (!h || kernel < TRSM_AUTO || kernel > TRSM_INVERSE) return ST_ARG;
+  h->c.trsm_kernel = kernel;
+  return ST_OK;
+}
+
 int lela_cuda_gemm_gf2_dev(lela_cuda_ctx *h, size_t m, size_t n, size_t k, int a,
                            const uint64_t *A, size_t lda, const uint64_t *B, size_t ldb, int b,
                            uint64_t *C, size_t ldc) {
@@ -727,6 +733,7 @@ int lela_cuda_fl_echelonize_zp_u32_batch(lela_cuda_ctx *h, size_t count, const s
     int st = lela_cuda_create(&w, c->device);
     if (st) return ctx_fail(c, st, "batch: worker handle");
     w->c.gemm_kernel = c->gemm_kernel;
+    w->c.trsm_kernel = c->trsm_kernel;
     h->workers.push_back(w);
   }
   // the caller's queued work must be done before the workers read inputs
@@ -741,6 +748,7 @@ int lela_cuda_fl_echelonize_zp_u32_batch(lela_cuda_ctx *h, size_t count, const s
   auto work = [&](lela_cuda_ctx *w) {
     cudaSetDevice(w->c.device);
     w->c.gemm_kernel = c->gemm_kernel;
+    w->c.trsm_kernel = c->trsm_kernel;
     for (size_t j = next++; j < count && !fatal.load(); j = next++) {
       const size_t i = order[j];
       size_t rows = 0, bad = 0;

@@ -31,6 +31,13 @@ enum Gf2Kernel : int {
   GF2_M4RM = 2,  // bit-packed four-Russians on CUDA cores
 };
 
+// Diagonal-block solvers of the Z/p trsm.
+enum TrsmKernel : int {
+  TRSM_AUTO = 0,     // inverse leaves for wide right-hand sides, else block substitution
+  TRSM_BLOCKS = 1,   // 256-row diagonal blocks by substitution on CUDA cores
+  TRSM_INVERSE = 2,  // 512-row diagonal blocks inverted, applied by the tensor-core gemm
+};
+
 struct Ctx {
   int device = 0;
   int num_sms = 148;
@@ -59,6 +66,7 @@ struct Ctx {
 
   int gemm_kernel = GEMM_AUTO;
   int gf2_kernel = GF2_AUTO;
+  int trsm_kernel = TRSM_AUTO;
   std::string last_error;
 
   // Instantiated CUDA graph of the small-block batch launch, replayed while
@@ -106,7 +114,9 @@ enum BufSlot : int {
   BUF_TINV = 15,      // inverted 64 x 64 diagonal blocks (trsm)
   BUF_BATCH = 16,     // batch item descriptors and results
   BUF_MLP = 17,       // cost-model scratch
-  BUF_COUNT = 18,
+  BUF_TRI_W = 18,     // inverted 512-row diagonal blocks (trsm)
+  BUF_TRI_T = 19,     // their assembly temporaries
+  BUF_COUNT = 20,
 };
 
 // Grow-only allocation helpers; return ST_OK or ST_NOMEM.

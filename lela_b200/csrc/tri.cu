@@ -8,7 +8,9 @@
 // reference's (split at l ~ m/2; lower: solve A11, B2 <- alpha*B2 - A21*B1,
 // solve A22 with coefficient 1; upper: A22 first, then B1 <- alpha*B1 -
 // A12*B2, then A11), with the off-diagonal updates on the limb-split
-// tensor-core gemm and 64-row diagonal leaves solved on CUDA cores.
+// tensor-core gemm.  The diagonal leaves are either 256-row blocks solved by
+// substitution on CUDA cores, or (from 1024 rows) 512-row blocks whose
+// inverses are built once and applied by the tensor-core gemm.
 //
 // Error behaviour.  With alpha = 0 the reference returns alpha*B = 0
 // without looking at A (:433-434); otherwise a diagonal entry that
@@ -44,13 +46,15 @@ __global__ void diag_inverse_kernel(const uint32_t *__restrict__ A, size_t lda, 
   }
 }
 
-// Left solve of one diagonal block: for every column of B (one thread per
-// column) x <- alpha * T^-1 x, T = nb x nb (nb <= 64) lower or upper
-// triangular with inverted diagonal dinv (nullptr: unit diagonal).  The
-// column lives in registers; products accumulate in 64 bits with the
-// reference's wrap-around correction (+2^64 mod p) and one reduction per
-// entry.  NOWRAP (p < 2^28): 64-term sums cannot wrap; two independent
-// partial sums per entry.
+// Left solve of one diagonal block: for every column of B,
+// x <- alpha * T^-1 x, T = nb x nb (nb <= 64) lower or upper triangular
+// with inverted diagonal dinv (nullptr: unit diagonal).  Four threads per
+// column: thread q holds the entries k = 4i + q in registers; for each k the
+// quad sums its partial products (two shuffles) and the owner of k
+// finishes x[k], so the sequential chain per thread is a quarter of the
+// triangle.  Products accumulate in 64 bits with the reference's
+// wrap-around correction (+2^64 mod p); NOWRAP (p < 2^28): the sums cannot
+// wrap, no check.
 template <bool UPPER, bool NOWRAP>
 __global__ void __launch_bounds__(128)
     tri_left_kernel(const uint32_t *__restrict__ T, size_t ldt, int nb,
@@ -64,55 +68,60 @@ __global__ void __launch_bounds__(128)
   }
   for (int e = threadIdx.x; e < TRI_NB; e += blockDim.x) sD[e] = (e < nb && dinv) ? dinv[e] : 1u;
   __syncthreads();
-  const int col = blockIdx.x * blockDim.x + threadIdx.x;
-  if (col >= ncols) return;
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+  const int col = gt >> 2, q = gt & 3;
+  const bool ok = col < ncols;  // every lane stays for the quad's shuffles
   const uint32_t p = (uint32_t)mod.p;
-  uint32_t x[TRI_NB];
+  uint32_t x[TRI_NB / 4];
 #pragma unroll
-  for (int k = 0; k < TRI_NB; ++k) {
-    uint32_t v = (k < nb) ? B[(size_t)k * ldb + col] : 0u;
-    x[k] = (alpha == 1u) ? v : mod_mul(v, alpha, mod);
+  for (int i = 0; i < TRI_NB / 4; ++i) {
+    const int k = 4 * i + q;
+    const uint32_t v = (ok && k < nb) ? B[(size_t)k * ldb + col] : 0u;
+    x[i] = (alpha == 1u) ? v : mod_mul(v, alpha, mod);
   }
   const bool unitd = dinv == nullptr;
 #pragma unroll
   for (int kk = 0; kk < TRI_NB; ++kk) {
     const int k = UPPER ? TRI_NB - 1 - kk : kk;
-    uint64_t s = 0, s2 = 0;
+    uint64_t s = 0;
 #pragma unroll
-    for (int j = 0; j < TRI_NB; ++j) {
-      if (UPPER ? j <= k : j >= k) continue;
-      const uint64_t t = (uint64_t)sT[k][j] * x[j];
-      if (NOWRAP) {
-        if (j & 1)
-          s2 += t;
-        else
-          s += t;
-      } else {
+    for (int i = 0; i < TRI_NB / 4; ++i) {
+      const int j = 4 * i + q;
+      if (UPPER ? j > k : j < k) {
+        const uint64_t t = (uint64_t)sT[k][j] * x[i];
         s += t;
-        if (s < t) s += two64;
+        if (!NOWRAP && s < t) s += two64;
       }
     }
-    uint32_t r = mod_reduce(s, mod);
-    if (NOWRAP) {
-      const uint32_t r2 = mod_reduce(s2, mod);
-      r = r + r2 >= p ? r + r2 - p : r + r2;
+    if (!NOWRAP) s = mod_reduce(s, mod);  // partial sums below 2^32, their sum below 2^34
+    s += __shfl_xor_sync(0xffffffffu, s, 1);
+    s += __shfl_xor_sync(0xffffffffu, s, 2);
+    if ((k & 3) == q) {
+      const uint32_t r = mod_reduce(s, mod);
+      const uint32_t xk = x[k >> 2];
+      const uint32_t v = xk >= r ? xk - r : xk + (p - r);
+      x[k >> 2] = (k < nb) ? (unitd ? v : mod_mul(v, sD[k], mod)) : 0u;
     }
-    const uint32_t v = x[k] >= r ? x[k] - r : x[k] + (p - r);
-    x[k] = (k < nb) ? (unitd ? v : mod_mul(v, sD[k], mod)) : 0u;
   }
+  if (ok)
 #pragma unroll
-  for (int k = 0; k < TRI_NB; ++k)
-    if (k < nb) B[(size_t)k * ldb + col] = x[k];
+    for (int i = 0; i < TRI_NB / 4; ++i) {
+      const int k = 4 * i + q;
+      if (k < nb) B[(size_t)k * ldb + col] = x[i];
+    }
 }
 
 // Inverses of all diagonal blocks at once: block b (rows/cols 64b ..
 // 64b+nb) of the triangular A; one CTA of 64 threads per block, thread j
-// solves T x = e_j with x in registers.  Out: Tinv[b] (64 x 64, zero padded).
+// solves T x = e_j with x in registers.  Out: the 64 x 64 inverse (zero
+// padded) at rows 64b.. of Tinv (row stride ldo), columns (64b mod cmod)..:
+// ldo = cmod = 64 stores the blocks one after the other; ldo = cmod = NB
+// places them on the diagonal of the NB-row block inverses.
 template <bool UPPER>
 __global__ void __launch_bounds__(64)
     tri_inv_blocks_kernel(const uint32_t *__restrict__ A, size_t lda, int m,
                           const uint32_t *__restrict__ dinv, uint32_t *__restrict__ Tinv,
-                          Modulus mod, uint32_t two64) {
+                          size_t ldo, int cmod, Modulus mod, uint32_t two64) {
   __shared__ uint32_t sT[TRI_NB][TRI_NB + 1];
   __shared__ uint32_t sD[TRI_NB];
   const int b = blockIdx.x;
@@ -159,9 +168,106 @@ __global__ void __launch_bounds__(64)
       x[k] = (k < nb) ? mod_mul(v, sD[k], mod) : 0u;
     }
   }
-  uint32_t *out = Tinv + (size_t)b * TRI_NB * TRI_NB;
+  uint32_t *out = Tinv + (size_t)r0 * ldo + r0 % cmod;
 #pragma unroll
-  for (int k = 0; k < TRI_NB; ++k) out[k * TRI_NB + j] = (j < nb) ? x[k] : 0u;
+  for (int k = 0; k < TRI_NB; ++k) out[(size_t)k * ldo + j] = (j < nb) ? x[k] : 0u;
+}
+
+// ----------------------------------------------------------- inverse leaves
+// For wide right-hand sides the diagonal blocks of TI_NB rows (aligned to
+// multiples of TI_NB from the top-left) are inverted once, and each leaf of
+// the recursion becomes B_leaf <- alpha * inv(A_leaf) * B_leaf on the
+// tensor-core gemm.  The triangular system has a unique solution (every
+// diagonal entry is a unit, checked first), so the result is the
+// substitution's.  The inverses are assembled from the 64-row ones by
+// doubling: for a block [[A11, A12], [0, A22]] with inverses I11, I22 of its
+// halves, inv = [[I11, -I11 A12 I22], [0, I22]] (lower: the off-diagonal
+// block is -I22 A21 I11).  W (rows x TI_NB) holds the inverse of leaf b in
+// its rows TI_NB b .., columns 0 ..; every level writes its off-diagonal
+// blocks in place.
+constexpr int TI_NB = 512;
+constexpr int MG_T = 64, MG_K = 32;
+
+// One operand of a batched merge product: entry (i, j) of instance z sits at
+// ptr[(z rs + ro + i) ld + (z cs + co) mod cmod + j].
+struct MergeOp {
+  const uint32_t *ptr;
+  size_t ld;
+  int rs, ro, cs, co, cmod;
+  __host__ __device__ const uint32_t *at(int z) const {
+    return ptr + (size_t)(z * rs + ro) * ld + (z * cs + co) % cmod;
+  }
+};
+
+// C_z <- alpha X_z Y_z (M x N, inner dimension K) for the instances
+// z = zbase + blockIdx.z; 64 x 64 tiles as the small-K gemm.  NOWRAP
+// (p < 2^28): unchecked sums reduced every 256 terms.
+template <bool NOWRAP>
+__global__ void __launch_bounds__(256)
+    tri_merge_kernel(MergeOp X, MergeOp Y, MergeOp Cop, int zbase, int M, int N, int K,
+                     Modulus mod, uint32_t two64, uint32_t alpha) {
+  __shared__ uint32_t Xs[MG_K][MG_T + 1];
+  __shared__ uint32_t Ys[MG_K][MG_T + 1];
+  const int z = zbase + blockIdx.z;
+  const uint32_t *__restrict__ Xp = X.at(z);
+  const uint32_t *__restrict__ Yp = Y.at(z);
+  uint32_t *Cp = const_cast<uint32_t *>(Cop.at(z));
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const int m0 = blockIdx.y * MG_T, n0 = blockIdx.x * MG_T;
+  uint64_t acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = 0;
+  for (int k0 = 0; k0 < K; k0 += MG_K) {
+#pragma unroll
+    for (int e = 0; e < (MG_T * MG_K) / 256; ++e) {
+      const int idx = threadIdx.x + 256 * e;
+      const int r = idx / MG_K, kk = idx % MG_K;
+      const int gm = m0 + r, gk = k0 + kk;
+      Xs[kk][r] = (gm < M && gk < K) ? Xp[(size_t)gm * X.ld + gk] : 0u;
+      const int kr = idx / MG_T, cc = idx % MG_T;
+      const int gk2 = k0 + kr, gn = n0 + cc;
+      Ys[kr][cc] = (gk2 < K && gn < N) ? Yp[(size_t)gk2 * Y.ld + gn] : 0u;
+    }
+    __syncthreads();
+#pragma unroll 8
+    for (int kk = 0; kk < MG_K; ++kk) {
+      uint32_t a[4], b[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i] = Xs[kk][ty + 16 * i];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) b[j] = Ys[kk][tx + 16 * j];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const uint64_t t = (uint64_t)a[i] * b[j];
+          if (NOWRAP) {
+            acc[i][j] += t;
+          } else {
+            const uint64_t s = acc[i][j] + t;
+            acc[i][j] = (s < t) ? s + two64 : s;
+          }
+        }
+    }
+    if (NOWRAP && ((k0 / MG_K) & 7) == 7)
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = mod_reduce(acc[i][j], mod);
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int gm = m0 + ty + 16 * i;
+    if (gm >= M) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int gn = n0 + tx + 16 * j;
+      if (gn < N) Cp[(size_t)gm * Cop.ld + gn] = mod_mul(mod_reduce(acc[i][j], mod), alpha, mod);
+    }
+  }
 }
 
 // C <- beta * C for an m x n block (beta in [0, p)).
@@ -182,9 +288,8 @@ int tri_left_block(Ctx *c, bool upper, int nb, const uint32_t *T, size_t ldt,
   if (nb <= 0 || ncols <= 0) return ST_OK;
   const Modulus mod = make_modulus(p);
   const uint32_t t64 = two64_mod(p);
-  // 64-thread CTAs spread narrow right-hand sides over more SMs
-  const int threads = ncols >= 128 * c->num_sms ? 128 : 64;
-  const int grid = (ncols + threads - 1) / threads;
+  const int threads = 128;  // 32 columns, four threads each
+  const int grid = (ncols * 4 + threads - 1) / threads;
   const bool nowrap = p < (1u << 28);
   int pi = prof_begin(c, "tri_left");
   if (upper && nowrap)
@@ -220,7 +325,7 @@ struct TriLeaves {
 // sub-blocks, then times the inverted diagonal 64-block.  A thread owns a
 // register tile of RPT rows x 4 columns.  NOWRAP (p < 2^28): 64-term sums
 // cannot wrap, no per-term check.
-constexpr int TB_NB = 512;
+constexpr int TB_NB = 256;
 constexpr int TB_THREADS = 256;
 
 template <bool UPPER, bool NOWRAP, int CT>
@@ -407,6 +512,90 @@ static int trsm_rec(Ctx *c, const TriLeaves &TL, bool upper, int m, int n, uint3
   }
 }
 
+// Off-diagonal blocks of the TI_NB-row diagonal block inverses, level by
+// level (block size s = 128, 256, .., TI_NB), on W whose diagonal 64-blocks
+// hold the 64-row inverses and whose other entries are zero.  T: scratch of
+// (m / TI_NB + 1) * (TI_NB / 2)^2 entries (the largest level's need).
+static int tri_inverse_levels(Ctx *c, bool upper, int m, uint32_t p, const uint32_t *A,
+                              size_t lda, uint32_t *W, uint32_t *T) {
+  const Modulus mod = make_modulus(p);
+  const uint32_t t64 = two64_mod(p);
+  const bool nowrap = p < (1u << 28);
+  constexpr int NOMOD = 1 << 30;
+  for (int s = 2 * TRI_NB; s <= TI_NB && s / 2 < m; s *= 2) {
+    const int h = s / 2;
+    const int nfull = m / s;
+    const int h2p = m - nfull * s - h;  // second half of the last, partial block
+    for (int pass = 0; pass < 2; ++pass) {
+      const int zbase = pass ? nfull : 0, nz = pass ? 1 : nfull, h2 = pass ? h2p : h;
+      if (nz <= 0 || h2 <= 0) continue;
+      const MergeOp Tz{T, (size_t)h, h, 0, 0, 0, NOMOD};
+      MergeOp X1, Y1, X2, C2;
+      int M1, N1, K1, M2, N2, K2;
+      if (upper) {
+        // T = A12 I22 (h x h2); W12 = -I11 T
+        X1 = {A, lda, s, 0, s, h, NOMOD};
+        Y1 = {W, (size_t)TI_NB, s, h, s, h, TI_NB};
+        X2 = {W, (size_t)TI_NB, s, 0, s, 0, TI_NB};
+        C2 = {W, (size_t)TI_NB, s, 0, s, h, TI_NB};
+        M1 = h, N1 = h2, K1 = h2, M2 = h, N2 = h2, K2 = h;
+      } else {
+        // T = A21 I11 (h2 x h); W21 = -I22 T
+        X1 = {A, lda, s, h, s, 0, NOMOD};
+        Y1 = {W, (size_t)TI_NB, s, 0, s, 0, TI_NB};
+        X2 = {W, (size_t)TI_NB, s, h, s, h, TI_NB};
+        C2 = {W, (size_t)TI_NB, s, h, s, 0, TI_NB};
+        M1 = h2, N1 = h, K1 = h, M2 = h2, N2 = h, K2 = h2;
+      }
+      const dim3 g1((N1 + MG_T - 1) / MG_T, (M1 + MG_T - 1) / MG_T, nz);
+      const dim3 g2((N2 + MG_T - 1) / MG_T, (M2 + MG_T - 1) / MG_T, nz);
+      if (nowrap) {
+        tri_merge_kernel<true><<<g1, 256, 0, c->stream>>>(X1, Y1, Tz, zbase, M1, N1, K1, mod, t64, 1u);
+        tri_merge_kernel<true><<<g2, 256, 0, c->stream>>>(X2, Tz, C2, zbase, M2, N2, K2, mod, t64, p - 1);
+      } else {
+        tri_merge_kernel<false><<<g1, 256, 0, c->stream>>>(X1, Y1, Tz, zbase, M1, N1, K1, mod, t64, 1u);
+        tri_merge_kernel<false><<<g2, 256, 0, c->stream>>>(X2, Tz, C2, zbase, M2, N2, K2, mod, t64, p - 1);
+      }
+      ctx_launched(c, 2);
+    }
+  }
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? ST_OK : ctx_cuda(c, e, "tri_merge launch");
+}
+
+// Recursion with inverse leaves: splits at multiples of TI_NB (so every leaf
+// is one of W's blocks; W points at the rows of A's top-left entry).
+static int trsm_rec_inv(Ctx *c, bool upper, int m, int n, uint32_t p, uint32_t alpha,
+                        const uint32_t *A, size_t lda, const uint32_t *W, uint32_t *B, size_t ldb,
+                        uint8_t *gemm_ws) {
+  if (m <= 0) return ST_OK;
+  if (m <= TI_NB) {
+    // in place: the tensor-core path converts B to limbs in the workspace
+    // before its first product, and with one K chunk (m <= TI_NB) each
+    // output tile is written once, after every product that reads B
+    return zp_gemm_dev(c, GEMM_TC, m, n, m, p, alpha, W, TI_NB, B, ldb, 0, B, ldb, gemm_ws);
+  }
+  const int l = ((m / 2 + TI_NB - 1) / TI_NB) * TI_NB;  // TI_NB <= l < m
+  const uint32_t *A12 = A + l, *A21 = A + (size_t)l * lda, *A22 = A21 + l;
+  const uint32_t *W2 = W + (size_t)l * TI_NB;
+  uint32_t *B1 = B, *B2 = B + (size_t)l * ldb;
+  int st;
+  if (!upper) {
+    if ((st = trsm_rec_inv(c, upper, l, n, p, alpha, A, lda, W, B1, ldb, gemm_ws))) return st;
+    if ((st = zp_gemm_dev(c, GEMM_AUTO, m - l, n, l, p, p - 1, A21, lda, B1, ldb, alpha, B2, ldb,
+                          gemm_ws)))
+      return st;
+    return trsm_rec_inv(c, upper, m - l, n, p, 1, A22, lda, W2, B2, ldb, gemm_ws);
+  } else {
+    if ((st = trsm_rec_inv(c, upper, m - l, n, p, alpha, A22, lda, W2, B2, ldb, gemm_ws)))
+      return st;
+    if ((st = zp_gemm_dev(c, GEMM_AUTO, l, n, m - l, p, p - 1, A12, lda, B2, ldb, alpha, B1, ldb,
+                          gemm_ws)))
+      return st;
+    return trsm_rec_inv(c, upper, l, n, p, 1, A, lda, W, B1, ldb, gemm_ws);
+  }
+}
+
 int zp_trsm_dev(Ctx *c, bool upper, bool unit, int m, int n, uint32_t p, uint32_t alpha,
                 const uint32_t *A, size_t lda, uint32_t *B, size_t ldb, size_t *bad_idx) {
   if (p < 2) return ctx_fail(c, ST_ARG, "modulus must be at least 2");
@@ -448,21 +637,54 @@ int zp_trsm_dev(Ctx *c, bool upper, bool unit, int m, int n, uint32_t p, uint32_
     }
   }
   if (n == 0) return ST_OK;
-  // inverses of all 64 x 64 diagonal blocks, in one launch
+  int kind = c->trsm_kernel;
+  if (kind == TRSM_AUTO) {
+    // inverse leaves from two leaves up (measured faster there for every
+    // width from 64 columns; a single leaf's set-up costs more than the
+    // substitution), and not when the caller forced a CUDA-core gemm
+    const bool tc = c->gemm_kernel == GEMM_AUTO || c->gemm_kernel == GEMM_TC;
+    kind = (tc && m >= 2 * TI_NB) ? TRSM_INVERSE : TRSM_BLOCKS;
+  }
+  // inverses of all 64 x 64 diagonal blocks, in one launch: one after the
+  // other for the block substitution, on the diagonal of W for the inverse
+  // leaves
   const int nblk = (m + TRI_NB - 1) / TRI_NB;
+  const uint32_t *dv = unit ? nullptr : dinv;
+  if (kind == TRSM_INVERSE) {
+    const int nleaf = (m + TI_NB - 1) / TI_NB;
+    void *wb = nullptr, *tb = nullptr;
+    if ((st = ctx_buffer(c, BUF_TRI_W, (size_t)nleaf * TI_NB * TI_NB * 4, &wb))) return st;
+    // T holds one (s/2)^2 product per block of a level: at most at s = TI_NB
+    const size_t tent = (size_t)(m / TI_NB + 1) * (TI_NB / 2) * (TI_NB / 2);
+    if ((st = ctx_buffer(c, BUF_TRI_T, tent * 4, &tb))) return st;
+    uint32_t *W = static_cast<uint32_t *>(wb);
+    cudaError_t e = cudaMemsetAsync(W, 0, (size_t)nleaf * TI_NB * TI_NB * 4, c->stream);
+    if (e != cudaSuccess) return ctx_cuda(c, e, "cudaMemsetAsync(trsm inverses)");
+    if (upper)
+      tri_inv_blocks_kernel<true><<<nblk, 64, 0, c->stream>>>(A, lda, m, dv, W, TI_NB, TI_NB,
+                                                              mod, two64_mod(p));
+    else
+      tri_inv_blocks_kernel<false><<<nblk, 64, 0, c->stream>>>(A, lda, m, dv, W, TI_NB, TI_NB,
+                                                               mod, two64_mod(p));
+    ctx_launched(c);
+    if ((st = tri_inverse_levels(c, upper, m, p, A, lda, W, static_cast<uint32_t *>(tb))))
+      return st;
+    void *w = nullptr;
+    // the largest update is about (m/2 + TI_NB) x n x (m/2 + TI_NB)
+    st = ctx_workspace(c, zp_gemm_workspace_bytes(p, m, n, (m + 1) / 2 + TI_NB), &w);
+    if (st) return st;
+    return trsm_rec_inv(c, upper, m, n, p, alpha, A, lda, W, B, ldb, static_cast<uint8_t *>(w));
+  }
   void *tb = nullptr;
   if ((st = ctx_buffer(c, BUF_TINV, (size_t)nblk * TRI_NB * TRI_NB * 4, &tb))) return st;
   uint32_t *tinv = static_cast<uint32_t *>(tb);
-  {
-    const uint32_t *dv = unit ? nullptr : dinv;
-    if (upper)
-      tri_inv_blocks_kernel<true><<<nblk, 64, 0, c->stream>>>(A, lda, m, dv, tinv, mod,
-                                                              two64_mod(p));
-    else
-      tri_inv_blocks_kernel<false><<<nblk, 64, 0, c->stream>>>(A, lda, m, dv, tinv, mod,
-                                                               two64_mod(p));
-    ctx_launched(c);
-  }
+  if (upper)
+    tri_inv_blocks_kernel<true><<<nblk, 64, 0, c->stream>>>(A, lda, m, dv, tinv, TRI_NB, TRI_NB,
+                                                            mod, two64_mod(p));
+  else
+    tri_inv_blocks_kernel<false><<<nblk, 64, 0, c->stream>>>(A, lda, m, dv, tinv, TRI_NB, TRI_NB,
+                                                             mod, two64_mod(p));
+  ctx_launched(c);
   void *w = nullptr;
   // the largest update is about (m/2) x n x (m/2)
   st = ctx_workspace(c, zp_gemm_workspace_bytes(p, m, n, (m + 1) / 2 + TRI_NB), &w);
