@@ -41,7 +41,11 @@
 //     of a pivot row, the L21 row otherwise); the panel becomes U_k in pivot
 //     row k and zero below;
 //  5. U12 = L11^-1 A12 on CUDA cores and A22 -= L21 U12 on the limb-split
-//     tensor-core gemm over the rows down to the last possibly nonzero row.
+//     tensor-core gemm over the rows down to the last possibly nonzero row,
+//     for the columns of the panel's block of EB columns; the columns right
+//     of the block get one such update per block, with the multipliers of
+//     all its panels (K up to EB instead of W: a quarter of the passes over
+//     the trailing matrix).
 // F4 Schur complements are staircase-shaped (rows sorted by head), so few
 // rows are touched per panel; dense matrices make every row active and the
 // scheme becomes ordinary blocked LU with LELA's pivot choice.
@@ -59,6 +63,7 @@
 namespace lela {
 
 constexpr int EW = 64;                     // panel width
+constexpr int EB = 4 * EW;                 // block of panels sharing one trailing update
 constexpr int PS_THREADS = 512;            // panel search CTA
 constexpr int PS_FAST = PS_THREADS / 32;   // positions tested per column by whole warps
 constexpr int PS_PARTS = PS_THREADS / EW;  // k-slices of a row-wide sum
@@ -543,15 +548,16 @@ __global__ void scatter_rows_kernel(uint32_t *__restrict__ D, size_t ld, int n,
 // reference's elimination steps on the panel part, pivot k applied with
 // multiplier l_k = v[pcol_k] / x_k (v: the row's current value) and
 // v -= l_k U_k.  Pivot row k takes the pivots before it (its L11 row, unit
-// lower, row stride EW; its panel becomes U_k); rows below take all t (their
-// L21 row of t entries; their panel becomes zero).
+// lower; its panel becomes U_k); rows below take all t (their L21 row; their
+// panel becomes zero).  Row i0 + r of L = [L11; L21] goes to
+// Lout[r * ldl + 0 .. t-1].
 constexpr int SOLVE_THREADS = 256;
 template <class A>
 __global__ void __launch_bounds__(SOLVE_THREADS)
     panel_solve_kernel(uint32_t *__restrict__ D, size_t ld, int i0, int r1, int c0, int w, int t,
                        const uint32_t *__restrict__ pcol, const uint32_t *__restrict__ Uin,
-                       const uint32_t *__restrict__ xinv, A ar,
-                       uint32_t *__restrict__ L11, uint32_t *__restrict__ L21) {
+                       const uint32_t *__restrict__ xinv, A ar, uint32_t *__restrict__ Lout,
+                       size_t ldl) {
   __shared__ uint32_t sU[EW][EW];
   __shared__ uint32_t sX[EW];
   __shared__ int sP[EW];
@@ -563,7 +569,6 @@ __global__ void __launch_bounds__(SOLVE_THREADS)
   }
   __syncthreads();
   const uint32_t p = ar.p;
-  const int r0 = i0 + t;
   const int warps = (gridDim.x * SOLVE_THREADS) >> 5;
   for (int pos = i0 + ((blockIdx.x * SOLVE_THREADS + tid) >> 5); pos <= r1; pos += warps) {
     uint32_t *row = D + (size_t)pos * ld + c0;
@@ -584,11 +589,11 @@ __global__ void __launch_bounds__(SOLVE_THREADS)
     }
     if (lane < w) row[lane] = a0;
     if (lane + 32 < w) row[lane + 32] = a1;
+    uint32_t *lr = Lout + (size_t)kk * ldl;
     if (kk < t) {
-      L11[kk * EW + lane] = lane < kk ? l0 : (lane == kk ? 1u : 0u);
-      L11[kk * EW + lane + 32] = lane + 32 < kk ? l1 : (lane + 32 == kk ? 1u : 0u);
+      if (lane < t) lr[lane] = lane < kk ? l0 : (lane == kk ? 1u : 0u);
+      if (lane + 32 < t) lr[lane + 32] = lane + 32 < kk ? l1 : (lane + 32 == kk ? 1u : 0u);
     } else {
-      uint32_t *lr = L21 + (size_t)(pos - r0) * t;
       if (lane < t) lr[lane] = l0;
       if (lane + 32 < t) lr[lane + 32] = l1;
     }
@@ -622,11 +627,11 @@ int zp_echelon_dev(Ctx *c, int m, int n, uint32_t p, uint32_t *D, size_t ld, siz
       (((size_t)2 * m + 4 * EW + 1 + EW + 1) * sizeof(int) + 255) & ~(size_t)255;
   const size_t h_bytes = ((size_t)2 * m + 255) & ~(size_t)255;
   const size_t sq_bytes = (size_t)EW * EW * 4;
-  const size_t l21_bytes = (size_t)m * EW * 4;
-  const size_t tmp_bytes = (size_t)2 * EW * n * 4;
+  const size_t l_bytes = (size_t)m * EB * 4;
+  const size_t tmp_bytes = (size_t)2 * EW * std::max(n, EB) * 4;
   void *base = nullptr;
   int st = ctx_buffer(c, BUF_ECH_0,
-                      out_bytes + i_bytes + h_bytes + 3 * sq_bytes + l21_bytes + tmp_bytes + 1024,
+                      out_bytes + i_bytes + h_bytes + 2 * sq_bytes + l_bytes + tmp_bytes + 1024,
                       &base);
   if (st) return st;
   uint8_t *b8 = static_cast<uint8_t *>(base);
@@ -640,12 +645,15 @@ int zp_echelon_dev(Ctx *c, int m, int n, uint32_t p, uint32_t *D, size_t ld, siz
   uint8_t *d_act = d_head + m;
   uint32_t *d_U = reinterpret_cast<uint32_t *>(b8 + out_bytes + i_bytes + h_bytes);
   uint32_t *d_xinv = d_U + EW * EW;  // pivot inverses (EW)
-  uint32_t *d_L11 = d_xinv + EW * EW;
-  uint32_t *d_L21 = d_L11 + EW * EW;
-  uint32_t *d_tmp = d_L21 + (size_t)m * EW;
+  uint32_t *d_L = d_xinv + EW * EW;  // the block's multipliers (m x EB)
+  uint32_t *d_tmp = d_L + (size_t)m * EB;
   const uint32_t *d_pcol = reinterpret_cast<const uint32_t *>(b8 + offsetof(PanelOut, pcol));
   void *gws = nullptr;
-  st = ctx_workspace(c, zp_gemm_workspace_bytes(p, m, n, EW), &gws);
+  // one size for the panel and block updates and the block's trsm (which
+  // takes the same workspace, so it must not grow it)
+  st = ctx_workspace(c, std::max(zp_gemm_workspace_bytes(p, m, n, EB),
+                                 zp_trsm_workspace_bytes(p, EB, n)),
+                     &gws);
   if (st) return st;
   const bool small = p < (1u << 16);
   static std::once_flag once;
@@ -669,8 +677,45 @@ int zp_echelon_dev(Ctx *c, int m, int n, uint32_t p, uint32_t *D, size_t ld, siz
   std::vector<int> at, src, dst;
   int i = 0, epoch = 0;
   const int head_grid = std::max(1, std::min((m + 7) / 8, c->num_sms * 2));
+  // Blocks of EB columns (delayed updates): a block's panels update only the
+  // block's columns; the columns right of it are updated once per block,
+  // U12 = L11^-1 A12 on the block's Tb pivot rows (from row ib) and
+  // A22 -= L21 U12 on the rows below, down to R.  L = [L11; L21] holds the
+  // block's multipliers: d_L row q (stride EB) belongs to the row at position
+  // q, panel k of the block fills columns Tb_k .. Tb_k + t_k - 1, and later
+  // panels' transpositions move d_L's rows with D's.  The result is the
+  // panel-by-panel one: the multipliers are the same, and the delayed update
+  // is the same Schur complement.  A block is delayed when the first panel
+  // with pivots has at least DELAY_ROWS rows to update below them (dense
+  // matrices); otherwise (staircase Schur complements, where few rows are
+  // touched) each panel updates all columns at once and the block solve is
+  // not paid.
+  constexpr int DELAY_ROWS = 512;
+  int ib = 0, Tb = 0, R = -1, b1 = 0, delayed = 0;
+  auto flush = [&]() -> int {
+    if (Tb == 0 || b1 >= n) return ST_OK;
+    int s = zp_trsm_dev(c, false, true, Tb, n - b1, p, 1, d_L + (size_t)ib * EB, EB,
+                        D + (size_t)ib * ld + b1, ld, nullptr);
+    if (s) return s;
+    const int rb = ib + Tb;
+    if (R < rb) return ST_OK;
+    int pi = prof_begin(c, "ech_block_update");
+    s = zp_gemm_dev(c, GEMM_AUTO, R - rb + 1, n - b1, Tb, p, p - 1, d_L + (size_t)rb * EB, EB,
+                    D + (size_t)ib * ld + b1, ld, 1, D + (size_t)rb * ld + b1, ld,
+                    static_cast<uint8_t *>(gws));
+    prof_end(c, pi);
+    return s;
+  };
   for (int c0 = 0; c0 < n && i < m; c0 += EW) {
     const int w = std::min(EW, n - c0);
+    if (c0 % EB == 0) {
+      if ((st = flush())) return st;
+      ib = i;
+      Tb = 0;
+      R = -1;
+      b1 = std::min(n, c0 + EB);
+      delayed = -1;  // decided at the block's first panel with pivots
+    }
     int pi = prof_begin(c, "ech_heads");
     panel_heads_kernel<<<head_grid, HEADS_THREADS, 0, c->stream>>>(D, ld, i, m, c0, w, d_head,
                                                                     d_act, d_hist, d_last);
@@ -716,35 +761,55 @@ int zp_echelon_dev(Ctx *c, int m, int n, uint32_t p, uint32_t *D, size_t ld, siz
       gather_rows_kernel<<<grid, 256, 0, c->stream>>>(D, ld, n, d_perm, cnt, d_tmp);
       scatter_rows_kernel<<<grid, 256, 0, c->stream>>>(D, ld, n, d_perm + cnt, cnt, d_tmp);
       ctx_launched(c, 2);
+      if (Tb > 0) {  // the multipliers of the block's earlier panels move too
+        dim3 gl((EB + 255) / 256, cnt);
+        gather_rows_kernel<<<gl, 256, 0, c->stream>>>(d_L, EB, EB, d_perm, cnt, d_tmp);
+        scatter_rows_kernel<<<gl, 256, 0, c->stream>>>(d_L, EB, EB, d_perm + cnt, cnt, d_tmp);
+        ctx_launched(c, 2);
+      }
     }
     // L11 / L21 and the panel's final values
     const int r0 = i + t;
     const int r1 = (h.last_pos >= (uint32_t)r0) ? (int)h.last_pos : r0 - 1;
     const int below = r1 - r0 + 1;
+    if (delayed < 0) {
+      delayed = below >= DELAY_ROWS;
+      if (delayed) {  // rows a panel's solve does not reach hold zero multipliers
+        e = cudaMemsetAsync(d_L + (size_t)i * EB, 0, (size_t)(m - i) * EB * 4, c->stream);
+        if (e != cudaSuccess) return ctx_cuda(c, e, "echelon: multipliers");
+      }
+    }
+    uint32_t *Lp = d_L + (size_t)i * EB + Tb;  // this panel's columns of L, from row i
     {
       const int groups = (r1 - i + 1 + SOLVE_THREADS / 32 - 1) / (SOLVE_THREADS / 32);
       pi = prof_begin(c, "ech_solve");
       const int sgrid = std::max(1, std::min(groups, c->num_sms * 8));
       if (small)
         panel_solve_kernel<<<sgrid, SOLVE_THREADS, 0, c->stream>>>(D, ld, i, r1, c0, w, t, d_pcol,
-                                                                   d_U, d_xinv, ars, d_L11, d_L21);
+                                                                   d_U, d_xinv, ars, Lp, EB);
       else
         panel_solve_kernel<<<sgrid, SOLVE_THREADS, 0, c->stream>>>(D, ld, i, r1, c0, w, t, d_pcol,
-                                                                   d_U, d_xinv, arw, d_L11, d_L21);
+                                                                   d_U, d_xinv, arw, Lp, EB);
       prof_end(c, pi);
       ctx_launched(c);
     }
-    const int rest = n - (c0 + w);
+    // the rest of the block's columns (delayed), or of all columns
+    const int rest = (delayed ? b1 : n) - (c0 + w);
     if (rest > 0) {
       uint32_t *U12 = D + (size_t)i * ld + c0 + w;
-      if ((st = tri_left_block(c, false, t, d_L11, EW, nullptr, U12, ld, rest, p, 1))) return st;
+      if ((st = tri_left_block(c, false, t, Lp, EB, nullptr, U12, ld, rest, p, 1))) return st;
       if (below > 0) {
         pi = prof_begin(c, "ech_update");
-        st = zp_gemm_dev(c, GEMM_AUTO, below, rest, t, p, p - 1, d_L21, (size_t)t, U12, ld, 1,
-                         D + (size_t)r0 * ld + c0 + w, ld, static_cast<uint8_t *>(gws));
+        st = zp_gemm_dev(c, GEMM_AUTO, below, rest, t, p, p - 1, Lp + (size_t)t * EB, EB, U12,
+                         ld, 1, D + (size_t)r0 * ld + c0 + w, ld, static_cast<uint8_t *>(gws));
         prof_end(c, pi);
         if (st) return st;
       }
+    }
+    if (delayed) {
+      // rows with multipliers: down to r1, and wherever a transposition moved one
+      R = std::max(R, std::max(r1, hi));
+      Tb += t;
     }
     det = (det * h.det) % p;
     if (pivot_cols)
@@ -752,6 +817,7 @@ int zp_echelon_dev(Ctx *c, int m, int n, uint32_t p, uint32_t *D, size_t ld, siz
     rank += t;
     i += t;
   }
+  if ((st = flush())) return st;
   *rank_out = rank;
   *det_out = (uint32_t)det;
   return ST_OK;

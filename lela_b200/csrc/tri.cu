@@ -596,6 +596,11 @@ static int trsm_rec_inv(Ctx *c, bool upper, int m, int n, uint32_t p, uint32_t a
   }
 }
 
+size_t zp_trsm_workspace_bytes(uint32_t p, int m, int n) {
+  // the largest update is about (m/2 + leaf) x n x (m/2 + leaf)
+  return zp_gemm_workspace_bytes(p, m, n, (m + 1) / 2 + std::max(TI_NB, TRI_NB));
+}
+
 int zp_trsm_dev(Ctx *c, bool upper, bool unit, int m, int n, uint32_t p, uint32_t alpha,
                 const uint32_t *A, size_t lda, uint32_t *B, size_t ldb, size_t *bad_idx) {
   if (p < 2) return ctx_fail(c, ST_ARG, "modulus must be at least 2");
@@ -670,9 +675,7 @@ int zp_trsm_dev(Ctx *c, bool upper, bool unit, int m, int n, uint32_t p, uint32_
     if ((st = tri_inverse_levels(c, upper, m, p, A, lda, W, static_cast<uint32_t *>(tb))))
       return st;
     void *w = nullptr;
-    // the largest update is about (m/2 + TI_NB) x n x (m/2 + TI_NB)
-    st = ctx_workspace(c, zp_gemm_workspace_bytes(p, m, n, (m + 1) / 2 + TI_NB), &w);
-    if (st) return st;
+    if ((st = ctx_workspace(c, zp_trsm_workspace_bytes(p, m, n), &w))) return st;
     return trsm_rec_inv(c, upper, m, n, p, alpha, A, lda, W, B, ldb, static_cast<uint8_t *>(w));
   }
   void *tb = nullptr;
@@ -686,9 +689,7 @@ int zp_trsm_dev(Ctx *c, bool upper, bool unit, int m, int n, uint32_t p, uint32_
                                                              mod, two64_mod(p));
   ctx_launched(c);
   void *w = nullptr;
-  // the largest update is about (m/2) x n x (m/2)
-  st = ctx_workspace(c, zp_gemm_workspace_bytes(p, m, n, (m + 1) / 2 + TRI_NB), &w);
-  if (st) return st;
+  if ((st = ctx_workspace(c, zp_trsm_workspace_bytes(p, m, n), &w))) return st;
   TriLeaves TL{A, tinv};
   return trsm_rec(c, TL, upper, m, n, p, alpha, A, lda, unit ? nullptr : dinv, B, ldb,
                   static_cast<uint8_t *>(w));

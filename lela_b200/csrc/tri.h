@@ -12,6 +12,10 @@ namespace lela {
 int zp_trsm_dev(Ctx *c, bool upper, bool unit, int m, int n, uint32_t p, uint32_t alpha,
                 const uint32_t *A, size_t lda, uint32_t *B, size_t ldb, size_t *bad_idx);
 
+// Workspace bytes zp_trsm_dev asks ctx_workspace for (either solver), so a
+// caller holding the workspace can size it once.
+size_t zp_trsm_workspace_bytes(uint32_t p, int m, int n);
+
 // One diagonal block (nb <= 64) solved on CUDA cores: B <- alpha*T^-1*B;
 // dinv = inverted diagonal (nullptr for a unit diagonal).
 int tri_left_block(Ctx *c, bool upper, int nb, const uint32_t *T, size_t ldt,

@@ -77,3 +77,24 @@ def test_echelon_pivots_far_below(cuda, p):
     got, gr, gd = cuda.echelonize(p, A.copy())
     assert (gr, gd) == (wr, wd)
     assert np.array_equal(got, want)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("p", [3, 2147483647])
+def test_echelon_blocks_far_pivots(cuda, p):
+    """Several blocks of panels (delayed trailing updates) with pivots far
+    below the current row across block boundaries, a block-wide band of zero
+    columns, dependent rows and rows that become zero mid-block."""
+    g = np.random.default_rng(11)
+    m, n = 1100, 900
+    A = gen.dense_zp(17, m, n, p)
+    A[:600, :300] = 0                      # the first block's pivots lie far below
+    A[:, 400:470] = 0                      # a panel and more without pivots
+    A[g.choice(np.arange(600, m), size=200, replace=False), :20] = 0
+    for r in g.choice(m, size=60, replace=False):
+        a, b = g.choice(m, size=2, replace=False)
+        A[r] = (A[a].astype(np.uint64) * 2 + A[b].astype(np.uint64) * 7) % p
+    want, wr, wd = oracle.echelon_zp(p, A)
+    got, gr, gd = cuda.echelonize(p, A.copy())
+    assert (gr, gd) == (wr, wd)
+    assert np.array_equal(got, want)
