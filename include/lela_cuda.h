@@ -124,6 +124,26 @@ int lela_cuda_trsm_zp_u32 (lela_cuda_ctx *ctx, int upper, int diag_is_one, size_
 int lela_cuda_trsm_zp_u32_dev (lela_cuda_ctx *ctx, int upper, int diag_is_one, size_t m,
 			       size_t n, uint32_t p, uint32_t a, const uint32_t *A, size_t lda,
 			       uint32_t *B, size_t ldb, size_t *bad_idx);
+/* The same solve with a sparse upper-triangular A (n x n) in CSR form:
+ * row r's entries are colidx/vals[rowptr[r] .. rowptr[r+1]), rowptr[0] = 0;
+ * B is n x ncols dense.  Replaces BLAS3::trsm on a SparseMatrix<uint32>
+ * operand, e.g. FaugereLachartre's A^-1 B (lela/algorithms/
+ * faugere-lachartre.tcc:791, UpperTriangular, diagIsOne = false), which
+ * runs _trsm<Ring, GenericModule::Tag>::trsm_impl (lela/blas/
+ * level3-generic.tcc:421-498) on the sparse rows.  Entries left of the
+ * diagonal are ignored (an upper solve never reads them); a missing
+ * diagonal entry is zero, reported like any singular diagonal
+ * (LELA_CUDA_DIAG_NOT_INVERTIBLE, largest such index).  A column index >= n
+ * returns LELA_CUDA_ERR_ARG.  A is expanded into a dense n x n device
+ * scratch copy (4 n^2 bytes).  The _dev form takes device arrays. */
+int lela_cuda_trsm_csr_upper_zp_u32 (lela_cuda_ctx *ctx, size_t n, size_t ncols, uint32_t p,
+				     uint32_t a, int diag_is_one, const uint64_t *rowptr,
+				     const uint32_t *colidx, const uint32_t *vals, uint32_t *B,
+				     size_t ldb, size_t *bad_idx);
+int lela_cuda_trsm_csr_upper_zp_u32_dev (lela_cuda_ctx *ctx, size_t n, size_t ncols, uint32_t p,
+					 uint32_t a, int diag_is_one, const uint64_t *rowptr,
+					 const uint32_t *colidx, const uint32_t *vals, uint32_t *B,
+					 size_t ldb, size_t *bad_idx);
 /* Diagonal-block solver of the trsm (and of the trsm steps inside
  * Faugere-Lachartre); every choice gives the same B. */
 enum {

@@ -106,6 +106,8 @@ def _bind_optional(L):
     sigs = {
         "lela_cuda_trsm_zp_u32": [_P, _I, _I, _S, _S, _U, _U, _P, _S, _P, _S, ctypes.POINTER(_S)],
         "lela_cuda_trsm_zp_u32_dev": [_P, _I, _I, _S, _S, _U, _U, _P, _S, _P, _S, ctypes.POINTER(_S)],
+        "lela_cuda_trsm_csr_upper_zp_u32": [_P, _S, _S, _U, _U, _I, _P, _P, _P, _P, _S, ctypes.POINTER(_S)],
+        "lela_cuda_trsm_csr_upper_zp_u32_dev": [_P, _S, _S, _U, _U, _I, _P, _P, _P, _P, _S, ctypes.POINTER(_S)],
         "lela_cuda_echelon_zp_u32": [_P, _S, _S, _U, _P, _S, ctypes.POINTER(_S), ctypes.POINTER(_U)],
         "lela_cuda_echelon_zp_u32_dev": [_P, _S, _S, _U, _P, _S, ctypes.POINTER(_S), ctypes.POINTER(_U)],
         "lela_cuda_fl_echelonize_zp_u32": [_P, _S, _S, _U, _P, _P, _P, _I, _I, _P, _S,
@@ -257,6 +259,27 @@ class CudaModule:
             st = self.L.lela_cuda_trsm_zp_u32(self.h, int(upper), int(diag_is_one), m, n, p, a % p,
                                               _ptr(A), A.strides[0] // 4, _ptr(B), B.strides[0] // 4,
                                               ctypes.byref(bad))
+        self._raise(st, bad.value)
+        return B
+
+    def trsm_csr_upper(self, p, a, n, rowptr, colidx, vals, B, diag_is_one=False):
+        """B <- a*A^-1*B mod p in place for an n x n upper-triangular A in CSR
+        form (BLAS3::trsm on a SparseMatrix, as in FaugereLachartre's A^-1 B);
+        numpy arrays (host) or torch CUDA tensors (device: rowptr int64,
+        colidx / vals int32, B int32).  Raises DiagonalEntryNotInvertible(idx)."""
+        _check(B.shape[0] == n and len(rowptr) == n + 1, "trsm_csr_upper: dimension mismatch")
+        ncols = B.shape[1]
+        bad = _S(0)
+        if _is_torch(B):
+            st = self.L.lela_cuda_trsm_csr_upper_zp_u32_dev(
+                self.h, n, ncols, p, a % p, int(diag_is_one), _dptr(rowptr), _dptr(colidx),
+                _dptr(vals), _dptr(B), B.stride(0), ctypes.byref(bad))
+        else:
+            _check(B.dtype == np.uint32 and rowptr.dtype == np.uint64 and colidx.dtype == np.uint32
+                   and vals.dtype == np.uint32, "trsm_csr_upper: uint64 rowptr, uint32 colidx/vals/B")
+            st = self.L.lela_cuda_trsm_csr_upper_zp_u32(
+                self.h, n, ncols, p, a % p, int(diag_is_one), _ptr(rowptr), _ptr(colidx),
+                _ptr(vals), _ptr(B), B.strides[0] // 4, ctypes.byref(bad))
         self._raise(st, bad.value)
         return B
 

@@ -801,6 +801,61 @@ int lela_cuda_echelon_zp_u32(lela_cuda_ctx *h, size_t m, size_t n, uint32_t p, u
   return st;
 }
 
+int lela_cuda_trsm_csr_upper_zp_u32(lela_cuda_ctx *h, size_t n, size_t ncols, uint32_t p,
+                                    uint32_t a, int diag_is_one, const uint64_t *rowptr,
+                                    const uint32_t *colidx, const uint32_t *vals, uint32_t *B,
+                                    size_t ldb, size_t *bad_idx) {
+  if (!h) return ST_ARG;
+  Ctx *c = &h->c;
+  if (n > (size_t)INT32_MAX || ncols > (size_t)INT32_MAX)
+    return ctx_fail(c, ST_ARG, "dimension too large");
+  if (p < 2) return ctx_fail(c, ST_ARG, "modulus must be at least 2");
+  if (n == 0) return ST_OK;
+  if (!rowptr || (ncols && !B)) return ctx_fail(c, ST_ARG, "null pointer");
+  if (ncols && ldb < ncols) return ctx_fail(c, ST_ARG, "leading dimension smaller than the row length");
+  const uint64_t nnz = rowptr[n];
+  if (nnz && (!colidx || !vals)) return ctx_fail(c, ST_ARG, "null pointer");
+  if (rowptr[0] != 0) return ctx_fail(c, ST_ARG, "row pointers must start at 0");
+  for (size_t r = 0; r < n; ++r)
+    if (rowptr[r + 1] < rowptr[r]) return ctx_fail(c, ST_ARG, "row pointers decrease");
+  for (uint64_t e = 0; e < nnz; ++e)
+    if (colidx[e] >= n) return ctx_fail(c, ST_ARG, "column index out of range");
+  cudaSetDevice(c->device);
+  void *dX = nullptr, *dB = nullptr;
+  int st = ctx_stage(c, 2, (n + 1) * 8 + nnz * 8 + 64, &dX);
+  if (!st && ncols) st = ctx_stage(c, 1, n * ncols * 4, &dB);
+  if (st) return st;
+  uint64_t *d_rowptr = (uint64_t *)dX;
+  uint32_t *d_col = (uint32_t *)(d_rowptr + n + 1);
+  uint32_t *d_val = d_col + nnz;
+  cudaError_t e = cudaMemcpyAsync(d_rowptr, rowptr, (n + 1) * 8, cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess && nnz)
+    e = cudaMemcpyAsync(d_col, colidx, nnz * 4, cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess && nnz)
+    e = cudaMemcpyAsync(d_val, vals, nnz * 4, cudaMemcpyHostToDevice, c->stream);
+  if (e != cudaSuccess) return ctx_cuda(c, e, "trsm csr: input copy");
+  if ((st = ctx_clear_status(c))) return st;
+  if (ncols && (st = h2d_matrix(c, dB, B, n, ncols, ldb, 4))) return st;
+  st = zp_trsm_csr_upper_dev(c, diag_is_one != 0, (int)n, (int)ncols, p, a, d_rowptr, d_col,
+                             d_val, (uint32_t *)dB, ncols, bad_idx);
+  if (!st && ncols) st = d2h_matrix(c, B, dB, n, ncols, ldb, 4);
+  if (!st) st = ctx_check_status(c, "trsm_csr_upper_zp_u32");
+  return st;
+}
+
+int lela_cuda_trsm_csr_upper_zp_u32_dev(lela_cuda_ctx *h, size_t n, size_t ncols, uint32_t p,
+                                        uint32_t a, int diag_is_one, const uint64_t *rowptr,
+                                        const uint32_t *colidx, const uint32_t *vals, uint32_t *B,
+                                        size_t ldb, size_t *bad_idx) {
+  if (!h) return ST_ARG;
+  Ctx *c = &h->c;
+  if (n > (size_t)INT32_MAX || ncols > (size_t)INT32_MAX)
+    return ctx_fail(c, ST_ARG, "dimension too large");
+  if (n && (!rowptr || (ncols && !B))) return ctx_fail(c, ST_ARG, "null pointer");
+  return zp_trsm_csr_upper_dev(c, diag_is_one != 0, (int)n, (int)ncols, p, a, rowptr, colidx,
+                               vals, B, ldb, bad_idx);
+}
+
 int lela_cuda_trsm_zp_u32_dev(lela_cuda_ctx *h, int upper, int diag_is_one, size_t m, size_t n,
                               uint32_t p, uint32_t a, const uint32_t *A, size_t lda, uint32_t *B,
                               size_t ldb, size_t *bad_idx) {

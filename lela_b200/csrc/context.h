@@ -116,7 +116,8 @@ enum BufSlot : int {
   BUF_MLP = 17,       // cost-model scratch
   BUF_TRI_W = 18,     // inverted 512-row diagonal blocks (trsm)
   BUF_TRI_T = 19,     // their assembly temporaries
-  BUF_COUNT = 20,
+  BUF_TRI_A = 20,     // dense copy of a sparse triangular operand
+  BUF_COUNT = 21,
 };
 
 // Grow-only allocation helpers; return ST_OK or ST_NOMEM.

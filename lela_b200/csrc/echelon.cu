@@ -66,7 +66,6 @@ constexpr int EW = 64;                     // panel width
 constexpr int EB = 4 * EW;                 // block of panels sharing one trailing update
 constexpr int PS_THREADS = 512;            // panel search CTA
 constexpr int PS_FAST = PS_THREADS / 32;   // positions tested per column by whole warps
-constexpr int PS_PARTS = PS_THREADS / EW;  // k-slices of a row-wide sum
 constexpr uint8_t HEAD_NONE = 64;
 
 struct PanelOut {
@@ -232,7 +231,10 @@ __global__ void __launch_bounds__(HEADS_THREADS)
 // counts them by that bound.
 constexpr int PW_R = 80;                   // window rows
 constexpr int PW_FIND = (PW_R + 31) / 32;  // warps that test window rows
-constexpr size_t PW_SMEM = (size_t)PW_R * EW * 4;  // dynamic shared memory: the window rows
+// window rows padded to EW + 1 words: a column read across rows (the pivot
+// test, the multipliers) then touches every bank once
+constexpr int PW_LD = EW + 1;
+constexpr size_t PW_SMEM = (size_t)PW_R * PW_LD * 4;  // dynamic shared memory: the window rows
 
 template <class A>
 __global__ void __launch_bounds__(PS_THREADS)
@@ -242,7 +244,7 @@ __global__ void __launch_bounds__(PS_THREADS)
                         int *__restrict__ stamp, int epoch, uint32_t *__restrict__ Uout,
                         uint32_t *__restrict__ xinv_out, PanelOut *out) {
   extern __shared__ __align__(16) uint32_t dyn_w[];
-  uint32_t(*Wv)[EW] = reinterpret_cast<uint32_t(*)[EW]>(dyn_w);  // PW_R rows
+  uint32_t(*Wv)[PW_LD] = reinterpret_cast<uint32_t(*)[PW_LD]>(dyn_w);  // PW_R rows
   __shared__ uint32_t PV[EW][EW];
   __shared__ int perm[2][PW_R], ppos[2][PW_R];
   __shared__ int wrow[PW_R];
@@ -432,14 +434,20 @@ __global__ void __launch_bounds__(PS_THREADS)
     // write the new entry list
     const uint32_t y = P[col];
     {
-      const int c = tid & (EW - 1);
-      if (c > col && c < w) {
-        const uint32_t pc = P[c];
-        for (int s = tid >> 6; s < nl; s += PS_PARTS) {
-          if (s == drop) continue;
-          const int pr = pm[s];
-          const uint32_t a = Wv[pr][col];
-          Wv[pr][c] = ar.dot2(y, Wv[pr][c], a ? p - a : 0u, pc);
+      // the ac live columns right of col, each taken by G threads that
+      // split the rows: every thread has work until the last columns
+      const int ac = w - col - 1;
+      if (ac > 0) {
+        const int G = PS_THREADS / ac;
+        if (tid < G * ac) {
+          const int c = col + 1 + tid % ac;
+          const uint32_t pc = P[c];
+          for (int s = tid / ac; s < nl; s += G) {
+            if (s == drop) continue;
+            const int pr = pm[s];
+            const uint32_t a = Wv[pr][col];
+            Wv[pr][c] = ar.dot2(y, Wv[pr][c], a ? p - a : 0u, pc);
+          }
         }
       }
     }

@@ -696,3 +696,60 @@ int zp_trsm_dev(Ctx *c, bool upper, bool unit, int m, int n, uint32_t p, uint32_
 }
 
 }  // namespace lela
+
+namespace lela {
+
+// ------------------------------------------------------- sparse operand
+// Upper-triangular A given as CSR (rowptr[n + 1], col, val) -> dense rows of
+// the zeroed n x n matrix A (one warp per row).  Entries left of the
+// diagonal are not part of an upper-triangular operand (the reference's
+// upper solve never reads them) and are skipped; values are taken mod p; a
+// column index >= n sets *bad.
+__global__ void csr_upper_to_dense_kernel(const uint64_t *__restrict__ rowptr,
+                                          const uint32_t *__restrict__ col,
+                                          const uint32_t *__restrict__ val, int n, uint32_t p,
+                                          uint32_t *__restrict__ A, size_t lda, uint32_t *bad) {
+  const int lane = threadIdx.x & 31;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  for (int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < n; r += warps) {
+    const uint64_t e0 = rowptr[r], e1 = rowptr[r + 1];
+    for (uint64_t e = e0 + lane; e < e1; e += 32) {
+      const uint32_t j = col[e];
+      if (j >= (uint32_t)n) {
+        atomicOr(bad, 1u);
+      } else if ((int)j >= r) {
+        A[(size_t)r * lda + j] = val[e] % p;
+      }
+    }
+  }
+}
+
+int zp_trsm_csr_upper_dev(Ctx *c, bool unit, int n, int ncols, uint32_t p, uint32_t alpha,
+                          const uint64_t *rowptr, const uint32_t *col, const uint32_t *val,
+                          uint32_t *B, size_t ldb, size_t *bad_idx) {
+  if (p < 2) return ctx_fail(c, ST_ARG, "modulus must be at least 2");
+  if (n < 0 || ncols < 0) return ctx_fail(c, ST_ARG, "negative dimension");
+  if (n == 0) return ST_OK;
+  if (ncols > 0 && ldb < (size_t)ncols)
+    return ctx_fail(c, ST_ARG, "leading dimension smaller than the row length");
+  void *buf = nullptr;
+  int st = ctx_buffer(c, BUF_TRI_A, (size_t)n * n * 4, &buf);
+  if (st) return st;
+  uint32_t *A = static_cast<uint32_t *>(buf);
+  cudaError_t e = cudaMemsetAsync(A, 0, (size_t)n * n * 4, c->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(c->dstatus + 3, 0, sizeof(uint32_t), c->stream);
+  if (e != cudaSuccess) return ctx_cuda(c, e, "trsm csr: scratch");
+  const int grid = std::max(1, std::min((n + 7) / 8, c->num_sms * 8));
+  csr_upper_to_dense_kernel<<<grid, 256, 0, c->stream>>>(rowptr, col, val, n, p, A, (size_t)n,
+                                                         c->dstatus + 3);
+  ctx_launched(c);
+  // the index check is read before the solve (one synchronisation)
+  e = cudaMemcpyAsync(c->hstatus + 3, c->dstatus + 3, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                      c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return ctx_cuda(c, e, "trsm csr: conversion");
+  if (c->hstatus[3]) return ctx_fail(c, ST_ARG, "column index out of range");
+  return zp_trsm_dev(c, true, unit, n, ncols, p, alpha, A, (size_t)n, B, ldb, bad_idx);
+}
+
+}  // namespace lela

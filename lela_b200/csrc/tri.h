@@ -12,6 +12,14 @@ namespace lela {
 int zp_trsm_dev(Ctx *c, bool upper, bool unit, int m, int n, uint32_t p, uint32_t alpha,
                 const uint32_t *A, size_t lda, uint32_t *B, size_t ldb, size_t *bad_idx);
 
+// B <- alpha * A^-1 * B for an n x n upper-triangular A in CSR form on the
+// device (the sparse pivot block of Faugere-Lachartre); A is expanded into
+// a dense scratch copy and solved by zp_trsm_dev.  Synchronises once to
+// check the column indices.
+int zp_trsm_csr_upper_dev(Ctx *c, bool unit, int n, int ncols, uint32_t p, uint32_t alpha,
+                          const uint64_t *rowptr, const uint32_t *col, const uint32_t *val,
+                          uint32_t *B, size_t ldb, size_t *bad_idx);
+
 // Workspace bytes zp_trsm_dev asks ctx_workspace for (either solver), so a
 // caller holding the workspace can size it once.
 size_t zp_trsm_workspace_bytes(uint32_t p, int m, int n);
