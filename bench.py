@@ -234,14 +234,17 @@ def run_fl(args, cm, stream, torch, dev, rank):
 
     cm.fl_echelonize(P, mats[0], True, False, R=R)  # warm-up
     cm.synchronize()
-    cm.profile_reset()
-    cm.profile(True)
     times, ranks = [], []
     for T in mats:
         t, rk, _ = timed(T)
         times.append(t)
         ranks.append(rk)
-    phases = {k.replace("fl_phase_", ""): round(cm.profile_read(k)[0] / len(mats), 2)
+    # phase breakdown from one more, untimed run with per-launch events on
+    # (the events themselves cost host time, so the timed runs go without)
+    cm.profile_reset()
+    cm.profile(True)
+    timed(mats[0])
+    phases = {k.replace("fl_phase_", ""): round(cm.profile_read(k)[0], 2)
               for k in ("fl_phase_trsm", "fl_phase_schur", "fl_phase_echelon", "fl_phase_reduce")}
     cm.profile(False)
     res.update({"ms_per_matrix": round(sum(times) / len(times), 2), "ms_each": [round(t, 2) for t in times],

@@ -46,15 +46,54 @@ __global__ void diag_inverse_kernel(const uint32_t *__restrict__ A, size_t lda, 
   }
 }
 
-// Left solve of one diagonal block: for every column of B,
-// x <- alpha * T^-1 x, T = nb x nb (nb <= 64) lower or upper triangular
-// with inverted diagonal dinv (nullptr: unit diagonal).  Four threads per
-// column: thread q holds the entries k = 4i + q in registers; for each k the
-// quad sums its partial products (two shuffles) and the owner of k
-// finishes x[k], so the sequential chain per thread is a quarter of the
-// triangle.  Products accumulate in 64 bits with the reference's
-// wrap-around correction (+2^64 mod p); NOWRAP (p < 2^28): the sums cannot
-// wrap, no check.
+// Solve T x = x in place for one column held by a quad of threads: thread q
+// holds the entries k = 4i + q (x[i]); T (nb x nb, nb <= 64, lower or upper
+// triangular) is in shared memory with its inverted diagonal sD (unitd: 1).
+// For each k the quad sums its partial products (two shuffles) and the owner
+// of k finishes x[k], so the sequential chain per thread is a quarter of the
+// triangle.  Products accumulate in 64 bits with the reference's wrap-around
+// correction (+2^64 mod p); NOWRAP (p < 2^28): the sums cannot wrap, no
+// check.  The k loop stays rolled (a fully unrolled 64-step body does not
+// fit the instruction cache); x[k / 4] is picked and written back by selects
+// over the 16 registers.  Entries from nb on are zero and never solved.
+template <bool UPPER, bool NOWRAP>
+__device__ __forceinline__ void tri_quad_solve(const uint32_t (*sT)[TRI_NB + 1],
+                                               const uint32_t *sD, bool unitd, int nb, int q,
+                                               uint32_t (&x)[TRI_NB / 4], const Modulus &mod,
+                                               uint32_t two64) {
+  const uint32_t p = (uint32_t)mod.p;
+#pragma unroll 1
+  for (int kk = 0; kk < nb; ++kk) {
+    const int k = UPPER ? nb - 1 - kk : kk;
+    uint64_t s = 0;
+#pragma unroll
+    for (int i = 0; i < TRI_NB / 4; ++i) {
+      const int j = 4 * i + q;
+      const uint64_t t = (UPPER ? j > k : j < k) ? (uint64_t)sT[k][j] * x[i] : 0ull;
+      s += t;
+      if (!NOWRAP && s < t) s += two64;
+    }
+    if (!NOWRAP) s = mod_reduce(s, mod);  // partial sums below 2^32, their sum below 2^34
+    s += __shfl_xor_sync(0xffffffffu, s, 1);
+    s += __shfl_xor_sync(0xffffffffu, s, 2);
+    const uint32_t r = mod_reduce(s, mod);
+    const int ik = k >> 2;
+    uint32_t xk = 0u;
+#pragma unroll
+    for (int i = 0; i < TRI_NB / 4; ++i) xk = (i == ik) ? x[i] : xk;
+    uint32_t v = xk >= r ? xk - r : xk + (p - r);
+    if (!unitd) v = mod_mul(v, sD[k], mod);
+    if ((k & 3) == q) {
+#pragma unroll
+      for (int i = 0; i < TRI_NB / 4; ++i)
+        if (i == ik) x[i] = v;
+    }
+  }
+}
+
+// Left solve of one diagonal block: for every column of B (a quad of
+// threads each), x <- alpha * T^-1 x, T = nb x nb (nb <= 64) lower or upper
+// triangular with inverted diagonal dinv (nullptr: unit diagonal).
 template <bool UPPER, bool NOWRAP>
 __global__ void __launch_bounds__(128)
     tri_left_kernel(const uint32_t *__restrict__ T, size_t ldt, int nb,
@@ -71,7 +110,6 @@ __global__ void __launch_bounds__(128)
   const int gt = blockIdx.x * blockDim.x + threadIdx.x;
   const int col = gt >> 2, q = gt & 3;
   const bool ok = col < ncols;  // every lane stays for the quad's shuffles
-  const uint32_t p = (uint32_t)mod.p;
   uint32_t x[TRI_NB / 4];
 #pragma unroll
   for (int i = 0; i < TRI_NB / 4; ++i) {
@@ -79,30 +117,7 @@ __global__ void __launch_bounds__(128)
     const uint32_t v = (ok && k < nb) ? B[(size_t)k * ldb + col] : 0u;
     x[i] = (alpha == 1u) ? v : mod_mul(v, alpha, mod);
   }
-  const bool unitd = dinv == nullptr;
-#pragma unroll
-  for (int kk = 0; kk < TRI_NB; ++kk) {
-    const int k = UPPER ? TRI_NB - 1 - kk : kk;
-    uint64_t s = 0;
-#pragma unroll
-    for (int i = 0; i < TRI_NB / 4; ++i) {
-      const int j = 4 * i + q;
-      if (UPPER ? j > k : j < k) {
-        const uint64_t t = (uint64_t)sT[k][j] * x[i];
-        s += t;
-        if (!NOWRAP && s < t) s += two64;
-      }
-    }
-    if (!NOWRAP) s = mod_reduce(s, mod);  // partial sums below 2^32, their sum below 2^34
-    s += __shfl_xor_sync(0xffffffffu, s, 1);
-    s += __shfl_xor_sync(0xffffffffu, s, 2);
-    if ((k & 3) == q) {
-      const uint32_t r = mod_reduce(s, mod);
-      const uint32_t xk = x[k >> 2];
-      const uint32_t v = xk >= r ? xk - r : xk + (p - r);
-      x[k >> 2] = (k < nb) ? (unitd ? v : mod_mul(v, sD[k], mod)) : 0u;
-    }
-  }
+  tri_quad_solve<UPPER, NOWRAP>(sT, sD, dinv == nullptr, nb, q, x, mod, two64);
   if (ok)
 #pragma unroll
     for (int i = 0; i < TRI_NB / 4; ++i) {
@@ -112,13 +127,13 @@ __global__ void __launch_bounds__(128)
 }
 
 // Inverses of all diagonal blocks at once: block b (rows/cols 64b ..
-// 64b+nb) of the triangular A; one CTA of 64 threads per block, thread j
-// solves T x = e_j with x in registers.  Out: the 64 x 64 inverse (zero
-// padded) at rows 64b.. of Tinv (row stride ldo), columns (64b mod cmod)..:
-// ldo = cmod = 64 stores the blocks one after the other; ldo = cmod = NB
-// places them on the diagonal of the NB-row block inverses.
+// 64b+nb) of the triangular A; one CTA of 256 threads per block, a quad per
+// column j solving T x = e_j.  Out: the 64 x 64 inverse (zero padded) at
+// rows 64b.. of Tinv (row stride ldo), columns (64b mod cmod)..: ldo = cmod
+// = 64 stores the blocks one after the other; ldo = cmod = NB places them
+// on the diagonal of the NB-row block inverses.
 template <bool UPPER>
-__global__ void __launch_bounds__(64)
+__global__ void __launch_bounds__(256)
     tri_inv_blocks_kernel(const uint32_t *__restrict__ A, size_t lda, int m,
                           const uint32_t *__restrict__ dinv, uint32_t *__restrict__ Tinv,
                           size_t ldo, int cmod, Modulus mod, uint32_t two64) {
@@ -134,43 +149,14 @@ __global__ void __launch_bounds__(64)
   }
   for (int e = threadIdx.x; e < TRI_NB; e += blockDim.x) sD[e] = (e < nb && dinv) ? dinv[r0 + e] : 1u;
   __syncthreads();
-  const int j = threadIdx.x;
-  const uint32_t p = (uint32_t)mod.p;
-  uint32_t x[TRI_NB];
+  const int j = threadIdx.x >> 2, q = threadIdx.x & 3;
+  uint32_t x[TRI_NB / 4];
 #pragma unroll
-  for (int k = 0; k < TRI_NB; ++k) x[k] = (k == j) ? 1u : 0u;
-  if (!UPPER) {
-#pragma unroll
-    for (int k = 0; k < TRI_NB; ++k) {
-      uint64_t s = 0;
-#pragma unroll
-      for (int q = 0; q < k; ++q) {
-        uint64_t t = (uint64_t)sT[k][q] * x[q];
-        s += t;
-        if (s < t) s += two64;
-      }
-      uint32_t r = mod_reduce(s, mod);
-      uint32_t v = x[k] >= r ? x[k] - r : x[k] + (p - r);
-      x[k] = (k < nb) ? mod_mul(v, sD[k], mod) : 0u;
-    }
-  } else {
-#pragma unroll
-    for (int k = TRI_NB - 1; k >= 0; --k) {
-      uint64_t s = 0;
-#pragma unroll
-      for (int q = k + 1; q < TRI_NB; ++q) {
-        uint64_t t = (uint64_t)sT[k][q] * x[q];
-        s += t;
-        if (s < t) s += two64;
-      }
-      uint32_t r = mod_reduce(s, mod);
-      uint32_t v = x[k] >= r ? x[k] - r : x[k] + (p - r);
-      x[k] = (k < nb) ? mod_mul(v, sD[k], mod) : 0u;
-    }
-  }
+  for (int i = 0; i < TRI_NB / 4; ++i) x[i] = (4 * i + q == j && j < nb) ? 1u : 0u;
+  tri_quad_solve<UPPER, false>(sT, sD, dinv == nullptr, nb, q, x, mod, two64);
   uint32_t *out = Tinv + (size_t)r0 * ldo + r0 % cmod;
 #pragma unroll
-  for (int k = 0; k < TRI_NB; ++k) out[(size_t)k * ldo + j] = (j < nb) ? x[k] : 0u;
+  for (int i = 0; i < TRI_NB / 4; ++i) out[(size_t)(4 * i + q) * ldo + j] = (j < nb) ? x[i] : 0u;
 }
 
 // ----------------------------------------------------------- inverse leaves
@@ -666,10 +652,10 @@ int zp_trsm_dev(Ctx *c, bool upper, bool unit, int m, int n, uint32_t p, uint32_
     cudaError_t e = cudaMemsetAsync(W, 0, (size_t)nleaf * TI_NB * TI_NB * 4, c->stream);
     if (e != cudaSuccess) return ctx_cuda(c, e, "cudaMemsetAsync(trsm inverses)");
     if (upper)
-      tri_inv_blocks_kernel<true><<<nblk, 64, 0, c->stream>>>(A, lda, m, dv, W, TI_NB, TI_NB,
+      tri_inv_blocks_kernel<true><<<nblk, 256, 0, c->stream>>>(A, lda, m, dv, W, TI_NB, TI_NB,
                                                               mod, two64_mod(p));
     else
-      tri_inv_blocks_kernel<false><<<nblk, 64, 0, c->stream>>>(A, lda, m, dv, W, TI_NB, TI_NB,
+      tri_inv_blocks_kernel<false><<<nblk, 256, 0, c->stream>>>(A, lda, m, dv, W, TI_NB, TI_NB,
                                                                mod, two64_mod(p));
     ctx_launched(c);
     if ((st = tri_inverse_levels(c, upper, m, p, A, lda, W, static_cast<uint32_t *>(tb))))
@@ -682,10 +668,10 @@ int zp_trsm_dev(Ctx *c, bool upper, bool unit, int m, int n, uint32_t p, uint32_
   if ((st = ctx_buffer(c, BUF_TINV, (size_t)nblk * TRI_NB * TRI_NB * 4, &tb))) return st;
   uint32_t *tinv = static_cast<uint32_t *>(tb);
   if (upper)
-    tri_inv_blocks_kernel<true><<<nblk, 64, 0, c->stream>>>(A, lda, m, dv, tinv, TRI_NB, TRI_NB,
+    tri_inv_blocks_kernel<true><<<nblk, 256, 0, c->stream>>>(A, lda, m, dv, tinv, TRI_NB, TRI_NB,
                                                             mod, two64_mod(p));
   else
-    tri_inv_blocks_kernel<false><<<nblk, 64, 0, c->stream>>>(A, lda, m, dv, tinv, TRI_NB, TRI_NB,
+    tri_inv_blocks_kernel<false><<<nblk, 256, 0, c->stream>>>(A, lda, m, dv, tinv, TRI_NB, TRI_NB,
                                                              mod, two64_mod(p));
   ctx_launched(c);
   void *w = nullptr;
