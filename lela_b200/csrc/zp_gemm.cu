@@ -113,16 +113,38 @@ __device__ __forceinline__ void mbar_drain(uint64_t *bar, uint32_t parity, uint3
   }
 }
 
+// How the product v (reduced) and C combine, chosen once per launch:
+// C <- v + C (alpha = 1, beta = 1: the gemm C += A*B), C <- C - v
+// (alpha = p - 1, beta = 1: the trsm and elimination updates), C <- alpha v
+// (beta = 0), or the general alpha v + beta C.  The first three skip the two
+// modular products of the general form (the epilogue is instruction-bound
+// when K is small).
+enum EpiMode : int { EPI_ADD = 0, EPI_SUB = 1, EPI_SET = 2, EPI_AXPBY = 3 };
+
+__device__ __forceinline__ uint32_t epi_combine(int mode, uint32_t v, uint32_t c,
+                                                const Modulus &mod, uint32_t alpha,
+                                                uint32_t beta) {
+  const uint32_t p = (uint32_t)mod.p;
+  if (mode == EPI_SET) return alpha == 1u ? v : mod_mul(alpha, v, mod);
+  if (mode == EPI_AXPBY) return mod_axpby(alpha, v, beta, c, mod);
+  if (c >= p) c = mod_reduce((uint64_t)c, mod);  // only for a caller's non-canonical C
+  if (mode == EPI_ADD) {
+    const uint32_t t = p - v;  // v + c mod p without overflow
+    return c >= t ? c - t : c + v;
+  }
+  return c >= v ? c - v : c + (p - v);
+}
+
 template <int L>
 __device__ __forceinline__ void epilogue_chunk(uint32_t tcol, int gm, int gn0, int M, int N,
                                                uint32_t *C, size_t ldc, const Modulus &mod,
-                                               uint32_t alpha, uint32_t beta);
+                                               uint32_t alpha, uint32_t beta, int mode);
 
 // L = 1: one product, P_00 < 2^31.
 template <>
 __device__ __forceinline__ void epilogue_chunk<1>(uint32_t tcol, int gm, int gn0, int M, int N,
                                                   uint32_t *C, size_t ldc, const Modulus &mod,
-                                                  uint32_t alpha, uint32_t beta) {
+                                                  uint32_t alpha, uint32_t beta, int mode) {
   uint32_t r[16];
   tmem_ld16(tcol, r);
   tmem_ld_wait();
@@ -133,8 +155,8 @@ __device__ __forceinline__ void epilogue_chunk<1>(uint32_t tcol, int gm, int gn0
       int gn = gn0 + i;
       if (gn < N) {
         uint32_t v = mod_reduce((uint64_t)r[i], mod);
-        uint32_t c = beta ? crow[gn] : 0u;
-        crow[gn] = mod_axpby(alpha, v, beta, c, mod);
+        const uint32_t c = mode != EPI_SET ? crow[gn] : 0u;
+        crow[gn] = epi_combine(mode, v, c, mod, alpha, beta);
       }
     }
   }
@@ -144,7 +166,7 @@ __device__ __forceinline__ void epilogue_chunk<1>(uint32_t tcol, int gm, int gn0
 template <>
 __device__ __forceinline__ void epilogue_chunk<2>(uint32_t tcol, int gm, int gn0, int M, int N,
                                                   uint32_t *C, size_t ldc, const Modulus &mod,
-                                                  uint32_t alpha, uint32_t beta) {
+                                                  uint32_t alpha, uint32_t beta, int mode) {
   constexpr int BN = TcCfg<2>::BN, NMMA = TcCfg<2>::NMMA;
   uint32_t p00[16], p01[16], p10[16], p11[16];
   tmem_ld16(tcol, p00);
@@ -160,8 +182,8 @@ __device__ __forceinline__ void epilogue_chunk<2>(uint32_t tcol, int gm, int gn0
       if (gn < N) {
         uint64_t v = ((uint64_t)p11[i] << 16) + (((uint64_t)p01[i] + p10[i]) << 8) + p00[i];
         uint32_t vr = mod_reduce(v, mod);
-        uint32_t c = beta ? crow[gn] : 0u;
-        crow[gn] = mod_axpby(alpha, vr, beta, c, mod);
+        const uint32_t c = mode != EPI_SET ? crow[gn] : 0u;
+        crow[gn] = epi_combine(mode, vr, c, mod, alpha, beta);
       }
     }
   }
@@ -173,7 +195,7 @@ __device__ __forceinline__ void epilogue_chunk<2>(uint32_t tcol, int gm, int gn0
 template <>
 __device__ __forceinline__ void epilogue_chunk<4>(uint32_t tcol, int gm, int gn0, int M, int N,
                                                   uint32_t *C, size_t ldc, const Modulus &mod,
-                                                  uint32_t alpha, uint32_t beta) {
+                                                  uint32_t alpha, uint32_t beta, int mode) {
   constexpr int BN = TcCfg<4>::BN, NMMA = TcCfg<4>::NMMA;
 #pragma unroll 1
   for (int h = 0; h < 16; h += 8) {
@@ -202,8 +224,8 @@ __device__ __forceinline__ void epilogue_chunk<4>(uint32_t tcol, int gm, int gn0
           uint32_t acc = mod_reduce(D[6][i], mod);
 #pragma unroll
           for (int s = 5; s >= 0; --s) acc = mod_reduce(((uint64_t)acc << 8) + D[s][i], mod);
-          uint32_t c = beta ? crow[gn] : 0u;
-          crow[gn] = mod_axpby(alpha, acc, beta, c, mod);
+          const uint32_t c = mode != EPI_SET ? crow[gn] : 0u;
+          crow[gn] = epi_combine(mode, acc, c, mod, alpha, beta);
         }
       }
     }
@@ -365,6 +387,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     const int row = q * 32 + lane;
     const int half = (warp - 2) >> 2;
     const int cbeg = half * (BN / 2), cend = cbeg + BN / 2;
+    const int emode = beta == 0u ? EPI_SET
+                      : (beta == 1u && alpha == 1u) ? EPI_ADD
+                      : (beta == 1u && alpha == (uint32_t)mod.p - 1u) ? EPI_SUB
+                                                                     : EPI_AXPBY;
     int it = 0;
     for (int t = blockIdx.x; t < num_tiles; t += gridDim.x, ++it) {
       int mb, nb;
@@ -378,7 +404,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
       if constexpr (OUT == 0) {
 #pragma unroll 1
         for (int c0 = cbeg; c0 < cend; c0 += 16)
-          epilogue_chunk<L>(tbase + c0, gm, nb * BN + c0, M, N, C, ldc, mod, alpha, beta);
+          epilogue_chunk<L>(tbase + c0, gm, nb * BN + c0, M, N, C, ldc, mod, alpha, beta, emode);
       } else {
         epilogue_gf2(tbase, gm, nb * BN, M, N, static_cast<uint64_t *>(Cv), ldc, alpha, beta,
                      cbeg, cend);
