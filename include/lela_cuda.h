@@ -241,7 +241,15 @@ int lela_cuda_echelon_zp_u32_batch (lela_cuda_ctx *ctx, size_t count, uint32_t *
 				    uint32_t *det, int *status);
 /* Faugere-Lachartre on `count` CSR matrices (arrays on the DEVICE; R[i] is a
  * device output of m[i] rows, stride ldr[i]), spread over nworkers threads
- * with their own streams.  status[i] as for the single call. */
+ * with their own streams, largest first.  status[i] as for the single call.
+ * Memory-budgeted queue: when the nworkers largest matrices may not fit in
+ * the budget together (estimate per matrix: 4 m n + 4 (m + n) m + 2 KB per
+ * row + 256 MB), a matrix starts only when its estimate fits beside those
+ * running (one that does not fit even alone runs alone), and each worker
+ * frees its device buffers after a matrix. */
+/* Budget of that queue in bytes; 0 (the default) = 90 % of the free device
+ * memory at the call plus what the worker handles already hold. */
+int lela_cuda_set_batch_memory_budget (lela_cuda_ctx *ctx, size_t bytes);
 int lela_cuda_fl_echelonize_zp_u32_batch (lela_cuda_ctx *ctx, size_t count, const size_t *m,
 					  const size_t *n, const uint32_t *p,
 					  const uint64_t *const *rowptr, const uint32_t *const *colidx,

@@ -122,6 +122,7 @@ def _bind_optional(L):
         "lela_cuda_echelon_gf2_dev": [_P, _S, _S, _P, _S, ctypes.POINTER(_S)],
         "lela_cuda_set_gf2_kernel": [_P, _I],
         "lela_cuda_set_trsm_kernel": [_P, _I],
+        "lela_cuda_set_batch_memory_budget": [_P, _S],
     }
     for name, args in sigs.items():
         if hasattr(L, name):
@@ -397,6 +398,10 @@ class CudaModule:
                 ctypes.cast(dt, _P), ctypes.cast(stt, _P))
         self._raise(st)
         return list(rk), list(dt), list(stt)
+
+    def set_batch_memory_budget(self, nbytes):
+        """Device-memory budget of fl_echelonize_batch (0 = automatic)."""
+        self._raise(self.L.lela_cuda_set_batch_memory_budget(self.h, int(nbytes)))
 
     def fl_echelonize_batch(self, Xs, ps, Rs, reduced=True, nworkers=4):
         """Faugere-Lachartre on many device CSR matrices (objects with m, n,

@@ -5,6 +5,8 @@
 
 #include <algorithm>
 #include <atomic>
+#include <condition_variable>
+#include <mutex>
 #include <cstdio>
 #include <cstring>
 #include <new>
@@ -713,6 +715,75 @@ int lela_cuda_fl_echelonize_zp_u32_dev(lela_cuda_ctx *h, size_t m, size_t n, uin
   return fl_finish(c, st, res, rank, det, out_rows, bad_row);
 }
 
+namespace {
+
+// Device bytes a handle holds in its grow-only buffers.
+size_t ctx_held_bytes(const Ctx *c) {
+  size_t s = c->ws_bytes + c->ws2_bytes;
+  for (int i = 0; i < 32; ++i) s += c->buf_bytes[i];
+  for (int i = 0; i < 4; ++i) s += c->stage_bytes[i];
+  return s;
+}
+
+// Free a handle's grow-only buffers (after its queued work).
+void ctx_trim(Ctx *c) {
+  cudaStreamSynchronize(c->stream);
+  if (c->ws) cudaFree(c->ws);
+  if (c->ws2) cudaFree(c->ws2);
+  c->ws = c->ws2 = nullptr;
+  c->ws_bytes = c->ws2_bytes = 0;
+  for (int i = 0; i < 32; ++i) {
+    if (c->buf[i]) cudaFree(c->buf[i]);
+    c->buf[i] = nullptr;
+    c->buf_bytes[i] = 0;
+  }
+  for (int i = 0; i < 4; ++i) {
+    if (c->stage[i]) cudaFree(c->stage[i]);
+    c->stage[i] = nullptr;
+    c->stage_bytes[i] = 0;
+  }
+}
+
+// Upper estimate of the device bytes one FL matrix needs on a handle: the
+// dense blocks A, B, C, D (4 m n), the gemm limb planes (at most 4 (m + n) m
+// for the Schur complement), the triangular-solve inverses and echelon
+// bookkeeping (about 2 KB per row), and fixed scratch.
+size_t fl_bytes_estimate(size_t m, size_t n) {
+  return 4 * m * n + 4 * (m + n) * m + 2048 * m + ((size_t)256 << 20);
+}
+
+// The memory-budgeted queue of a batch: an item starts only when its
+// estimate fits beside the items running (one that does not fit even alone
+// runs alone).
+struct MemQueue {
+  std::mutex mu;
+  std::condition_variable cv;
+  size_t budget = 0, used = 0;
+  int running = 0;
+  void acquire(size_t need) {
+    std::unique_lock<std::mutex> lk(mu);
+    cv.wait(lk, [&] { return running == 0 || used + need <= budget; });
+    used += need;
+    ++running;
+  }
+  void release(size_t need) {
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      used -= need;
+      --running;
+    }
+    cv.notify_all();
+  }
+};
+
+}  // namespace
+
+int lela_cuda_set_batch_memory_budget(lela_cuda_ctx *h, size_t bytes) {
+  if (!h) return ST_ARG;
+  h->c.batch_budget = bytes;
+  return ST_OK;
+}
+
 int lela_cuda_fl_echelonize_zp_u32_batch(lela_cuda_ctx *h, size_t count, const size_t *m,
                                          const size_t *n, const uint32_t *p,
                                          const uint64_t *const *rowptr,
@@ -743,20 +814,47 @@ int lela_cuda_fl_echelonize_zp_u32_batch(lela_cuda_ctx *h, size_t count, const s
   std::vector<size_t> order(count);
   for (size_t i = 0; i < count; ++i) order[i] = i;
   std::sort(order.begin(), order.end(), [&](size_t a, size_t b) { return m[a] * n[a] > m[b] * n[b]; });
+  // Memory budget: when the nworkers largest matrices may not fit together,
+  // items wait for room and each worker frees its buffers after an item.
+  MemQueue mq;
+  if (c->batch_budget) {
+    mq.budget = c->batch_budget;
+  } else {
+    size_t fr = 0, tot = 0;
+    e = cudaMemGetInfo(&fr, &tot);
+    if (e != cudaSuccess) return ctx_cuda(c, e, "batch: cudaMemGetInfo");
+    size_t held = 0;
+    for (int t = 0; t < nworkers; ++t) held += ctx_held_bytes(&h->workers[t]->c);
+    mq.budget = fr / 10 * 9 + held;
+  }
+  size_t peak = 0;
+  for (int j = 0; j < nworkers; ++j) peak += fl_bytes_estimate(m[order[j]], n[order[j]]);
+  const bool tight = peak > mq.budget;
   std::atomic<size_t> next(0);
   std::atomic<int> fatal(0);
   auto work = [&](lela_cuda_ctx *w) {
     cudaSetDevice(w->c.device);
     w->c.gemm_kernel = c->gemm_kernel;
     w->c.trsm_kernel = c->trsm_kernel;
+    if (tight) ctx_trim(&w->c);
     for (size_t j = next++; j < count && !fatal.load(); j = next++) {
       const size_t i = order[j];
+      const size_t need = fl_bytes_estimate(m[i], n[i]);
+      if (tight) mq.acquire(need);
+      if (fatal.load()) {  // another worker failed while this one waited
+        if (tight) mq.release(need);
+        break;
+      }
       size_t rows = 0, bad = 0;
       int st = lela_cuda_fl_echelonize_zp_u32_dev(w, m[i], n[i], p[i], rowptr[i], colidx[i],
                                                   vals[i], reduced, 0, R[i], ldr[i], &rank[i],
                                                   &det[i], &rows, &bad);
       status[i] = st;
       if (st != ST_OK && st != ST_WRONG_FORM && st != ST_DIAG && st != ST_PIVOT) fatal = st;
+      if (tight) {
+        ctx_trim(&w->c);
+        mq.release(need);
+      }
     }
   };
   std::vector<std::thread> th;

@@ -67,6 +67,9 @@ struct Ctx {
   int gemm_kernel = GEMM_AUTO;
   int gf2_kernel = GF2_AUTO;
   int trsm_kernel = TRSM_AUTO;
+  // Device-memory budget of the batched FL entry point (bytes; 0 = 90 % of
+  // the free memory plus what the worker handles already hold).
+  size_t batch_budget = 0;
   std::string last_error;
 
   // Instantiated CUDA graph of the small-block batch launch, replayed while

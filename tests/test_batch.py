@@ -86,3 +86,38 @@ def test_echelon_batch_small_kernel_edges(cuda):
         assert st[i] == 0, i
         assert (ranks[i], dets[i]) == (r, d), i
         assert np.array_equal(blocks[i].cpu().numpy().view(np.uint32), E), i
+
+
+@pytest.mark.gpu
+def test_fl_batch_memory_budget(cuda):
+    """The memory-budgeted queue: with a budget smaller than any matrix the
+    workers run one matrix at a time and free their buffers after each; the
+    results are those of the unbudgeted batch and of the oracle."""
+    import torch
+    p = 65521
+    Xs, Rs, wants = [], [], []
+    for i, m in enumerate([400, 900, 200, 650]):
+        X = gen.f4_matrix(170 + i, m, p)
+        wants.append(oracle.fl_echelonize_zp(p, X.m, X.n, X.rowptr, X.colidx, X.vals, 1, 0))
+        Xs.append(types.SimpleNamespace(m=X.m, n=X.n,
+                                        rowptr=torch.from_numpy(X.rowptr.view(np.int64)).cuda(),
+                                        colidx=_dev(X.colidx), vals=_dev(X.vals)))
+        Rs.append(torch.empty((X.m, X.n), dtype=torch.int32, device="cuda"))
+    cuda.set_batch_memory_budget(1)
+    try:
+        ranks, dets, st = cuda.fl_echelonize_batch(Xs, [p] * len(Xs), Rs, True, nworkers=3)
+    finally:
+        cuda.set_batch_memory_budget(0)
+    torch.cuda.synchronize()
+    for i, w in enumerate(wants):
+        assert st[i] == 0
+        assert (ranks[i], dets[i]) == (w["rank"], w["det"]), i
+        assert np.array_equal(Rs[i].cpu().numpy().view(np.uint32), w["R"]), i
+    # the same batch again under the automatic budget
+    for R in Rs:
+        R.zero_()
+    ranks, dets, st = cuda.fl_echelonize_batch(Xs, [p] * len(Xs), Rs, True, nworkers=3)
+    torch.cuda.synchronize()
+    for i, w in enumerate(wants):
+        assert st[i] == 0 and (ranks[i], dets[i]) == (w["rank"], w["det"]), i
+        assert np.array_equal(Rs[i].cpu().numpy().view(np.uint32), w["R"]), i
