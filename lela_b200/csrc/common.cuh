@@ -205,6 +205,12 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const void *tmap, uint64_
       : "memory");
 }
 
+// Prefetch the 128-byte line holding ptr into L2 (a hint; no data moves to
+// registers).
+__device__ __forceinline__ void prefetch_l2(const void *ptr) {
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(ptr));
+}
+
 __device__ __forceinline__ void prefetch_tmap(const void *tmap) {
   asm volatile("prefetch.tensormap [%0];" ::"l"((uint64_t)tmap) : "memory");
 }

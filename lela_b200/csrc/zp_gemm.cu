@@ -395,6 +395,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     for (int t = blockIdx.x; t < num_tiles; t += gridDim.x, ++it) {
       int mb, nb;
       tile_coords(t, tiles_m, tiles_n, mb, nb);
+      if (OUT == 0 && beta != 0u) {
+        // pull this thread's row segment of C into L2 while the tile's
+        // products run, so that the epilogue's loads of C hit L2
+        const int gm = mb * BM + row, gn0 = nb * BN + cbeg;
+        if (gm < M)
+          for (int cc = 0; cc < cend - cbeg; cc += 32)
+            if (gn0 + cc < N) prefetch_l2(C + (size_t)gm * ldc + gn0 + cc);
+      }
       const int a = it % ACC;
       const uint32_t aph = (uint32_t)(it / ACC) & 1u;
       if (!mbar_wait(&tfull[a], aph, err)) break;
