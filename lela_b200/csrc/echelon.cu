@@ -237,7 +237,7 @@ constexpr int PW_LD = EW + 1;
 constexpr size_t PW_SMEM = (size_t)PW_R * PW_LD * 4;  // dynamic shared memory: the window rows
 
 template <class A>
-__global__ void __launch_bounds__(PS_THREADS)
+__global__ void __launch_bounds__(PS_THREADS, 1)
     panel_search_kernel(const uint32_t *__restrict__ D, size_t ld, int i0, int m, int c0, int w,
                         A ar, uint8_t *__restrict__ head, const uint8_t *__restrict__ act,
                         int *__restrict__ hist, int *__restrict__ last_act, int *__restrict__ p2r,
@@ -253,6 +253,7 @@ __global__ void __launch_bounds__(PS_THREADS)
   __shared__ uint32_t s_y[EW], s_S[EW], s_x[EW], s_sinv[EW];
   __shared__ int s_cnt[EW + 1];
   __shared__ int s_first[PS_FAST], s_wcnt[PS_FAST];
+  __shared__ int s_fa[2][PW_FIND];  // phase A per column, by column parity
   __shared__ int s_list[PS_THREADS], s_lrow[PS_THREADS], s_lhead[PS_THREADS];
   __shared__ int s_err, s_last, s_hi, s_wlast;
   const uint32_t p = ar.p;
@@ -306,22 +307,27 @@ __global__ void __launch_bounds__(PS_THREADS)
     if (wid < PW_FIND) {
       const bool nz = tid < nl && Wv[pm[tid]][col] != 0u;
       const unsigned b = __ballot_sync(0xffffffffu, nz);
-      if (lane == 0) s_first[wid] = b ? tid + __ffs(b) - 1 : 0x7fffffff;
+      if (lane == 0) s_fa[col & 1][wid] = b ? tid + __ffs(b) - 1 : 0x7fffffff;
     }
     __syncthreads();
     int qs = 0x7fffffff;
-    for (int k = 0; k < PW_FIND; ++k) qs = min(qs, s_first[k]);
+    for (int k = 0; k < PW_FIND; ++k) qs = min(qs, s_fa[col & 1][k]);
     const bool z = nl > 0 && pp[0] == i;  // the row at position i is window entry 0
     const uint32_t *P;                    // the pivot row (S_t times reduced)
     int q, drop;                          // pivot position; window entry leaving (-1: none)
     bool relocate0 = false;               // entry 0 moves to position q, in place of qs
     if (qs == 0x7fffffff) {
       // none in the window: rows past it whose bound allows a pivot here
+      // (a warp-wide sum; every warp computes the same count)
       int cand = 0;
-      if (wlast < m - 1)
-        for (int h = 0; h <= col; ++h) cand += s_cnt[h];
-      __syncthreads();  // every thread has its count before s_cnt changes
+      if (wlast < m - 1) {
+        const int v = (lane <= col ? s_cnt[lane] : 0) + (lane + 32 <= col ? s_cnt[lane + 32] : 0);
+        cand = __reduce_add_sync(0xffffffffu, v);
+      }
+      // no barrier when there is no candidate: nothing shared changes, and
+      // the next column's phase A writes the other s_fa buffer
       if (cand == 0) continue;
+      __syncthreads();  // every thread has its count before s_cnt changes
       // per pass the CTA lists the candidates among PS_THREADS positions
       // (ordered compaction), then each warp reduces one of them by the t
       // pivots, W <- y_k W - W[pcol_k] (S_k U_k), and records its exact head
