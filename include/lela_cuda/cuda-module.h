@@ -178,6 +178,51 @@ class _trsm<Modular<uint32>, CUDAModule<uint32>::Tag>
 		return B;
 	}
 
+	// A stored by rows (SparseMatrix<uint32>), B dense: sparse rows of an
+	// upper-triangular A go to the CSR solve (FaugereLachartre's A^-1 B,
+	// lela/algorithms/faugere-lachartre.tcc:791); other rows and lower
+	// triangular A go to the parent module.
+	template <class Modules, class Matrix1, class Matrix2>
+	static Matrix2 &trsm_impl (const Modular<uint32> &F, Modules &M, uint32 a, const Matrix1 &A, Matrix2 &B,
+				   TriangularMatrixType type, bool diagIsOne,
+				   MatrixStorageTypes::Rows, MatrixStorageTypes::Dense)
+		{ return trsm_rows (F, M, a, A, B, type, diagIsOne,
+				    typename VectorTraits<Modular<uint32>, typename Matrix1::ConstRow>::RepresentationType ()); }
+
+	template <class Modules, class Matrix1, class Matrix2, class Rep>
+	static Matrix2 &trsm_rows (const Modular<uint32> &F, Modules &M, uint32 a, const Matrix1 &A, Matrix2 &B,
+				   TriangularMatrixType type, bool diagIsOne, Rep)
+		{ return _trsm<Modular<uint32>, CUDAModule<uint32>::Tag::Parent>::op (F, M, a, A, B, type, diagIsOne); }
+
+	template <class Modules, class Matrix1, class Matrix2>
+	static Matrix2 &trsm_rows (const Modular<uint32> &F, Modules &M, uint32 a, const Matrix1 &A, Matrix2 &B,
+				   TriangularMatrixType type, bool diagIsOne, VectorRepresentationTypes::Sparse)
+	{
+		if (type != UpperTriangular)
+			return _trsm<Modular<uint32>, CUDAModule<uint32>::Tag::Parent>::op (F, M, a, A, B, type, diagIsOne);
+		lela_check (A.coldim () == B.rowdim ());
+		lela_check (A.rowdim () == B.rowdim ());
+		const size_t m = A.rowdim (), n = B.coldim ();
+		if (m == 0)
+			return B;
+		std::vector<uint64_t> rowptr (m + 1, 0);
+		std::vector<uint32_t> colidx, vals;
+		size_t i = 0;
+		for (typename Matrix1::ConstRowIterator r = A.rowBegin (); r != A.rowEnd (); ++r, ++i) {
+			for (typename Matrix1::ConstRow::const_iterator e = r->begin (); e != r->end (); ++e) {
+				colidx.push_back ((uint32_t) (uint32) e->first);
+				vals.push_back ((uint32_t) e->second);
+			}
+			rowptr[i + 1] = colidx.size ();
+		}
+		size_t bad = 0;
+		int st = lela_cuda_trsm_csr_upper_zp_u32 (M.cuda.get (), m, n, F._modulus, a, diagIsOne, &rowptr[0],
+							  colidx.empty () ? 0 : &colidx[0], vals.empty () ? 0 : &vals[0],
+							  n ? &B[0][0] : 0, n ? B.disp () : 1, &bad);
+		lela_cuda_check (M.cuda.get (), st, bad);
+		return B;
+	}
+
 public:
 	template <class Modules, class Matrix1, class Matrix2>
 	static Matrix2 &op (const Modular<uint32> &F, Modules &M, uint32 a, const Matrix1 &A, Matrix2 &B,

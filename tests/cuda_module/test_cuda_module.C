@@ -112,6 +112,50 @@ static void test_trsm (uint32 p, size_t m, size_t n, bool upper, bool unit)
 	}
 }
 
+// trsm with a sparse upper-triangular A (SparseMatrix<uint32>, the operand
+// FaugereLachartre passes at faugere-lachartre.tcc:791): CUDAModule's CSR
+// path against GenericModule on the same sparse rows, and the singular
+// diagonal's index (a missing diagonal entry).
+static void test_trsm_sparse (uint32 p, size_t m, size_t n)
+{
+	Zp F (p);
+	Context<Zp, CUDAModule<uint32> > gpu (F);
+	Context<Zp, GenericModule<Zp> > cpu (F);
+	MersenneTwister MT (m * 5 + n);
+	SparseMatrix<uint32> A (m, m);
+	size_t i = 0;
+	for (SparseMatrix<uint32>::RowIterator r = A.rowBegin (); r != A.rowEnd (); ++r, ++i) {
+		r->push_back (SparseMatrix<uint32>::Row::value_type (i, MT.randomIntRange (1, p)));
+		for (size_t j = i + 1; j < m; ++j)
+			if (MT.randomDouble () < 0.05)
+				r->push_back (SparseMatrix<uint32>::Row::value_type (j, MT.randomIntRange (1, p)));
+	}
+	DenseMatrix<uint32> B (m, n), B2 (m, n);
+	fill (B, p, MT);
+	BLAS3::copy (cpu, B, B2);
+	BLAS3::trsm (gpu, 3, A, B, UpperTriangular, false);
+	BLAS3::trsm (cpu, 3, A, B2, UpperTriangular, false);
+	char what[160];
+	std::snprintf (what, sizeof what, "trsm sparse upper p=%u %zux%zu CUDAModule == GenericModule", p, m, n);
+	CHECK (same (B, B2), what);
+
+	// drop two diagonal entries: DiagonalEntryNotInvertible with LELA's index
+	SparseMatrix<uint32> S (m, m);
+	i = 0;
+	SparseMatrix<uint32>::ConstRowIterator ra = A.rowBegin ();
+	for (SparseMatrix<uint32>::RowIterator r = S.rowBegin (); r != S.rowEnd (); ++r, ++ra, ++i)
+		for (SparseMatrix<uint32>::ConstRow::const_iterator e = ra->begin (); e != ra->end (); ++e)
+			if (!(e->first == i && (i == 5 || i == m - 7)))
+				r->push_back (*e);
+	size_t gi = (size_t) -1, ci = (size_t) -2;
+	try { BLAS3::trsm (gpu, 1, S, B, UpperTriangular, false); }
+	catch (DiagonalEntryNotInvertible e) { gi = e.idx (); }
+	try { BLAS3::trsm (cpu, 1, S, B2, UpperTriangular, false); }
+	catch (DiagonalEntryNotInvertible e) { ci = e.idx (); }
+	std::snprintf (what, sizeof what, "trsm sparse DiagonalEntryNotInvertible(%zu) == reference (%zu)", gi, ci);
+	CHECK (gi == ci, what);
+}
+
 // The reference test's F4 staircase (tests/test-faugere-lachartre.C:142-175),
 // written here for SparseMatrix<uint32> rows.
 static void random_f4 (SparseMatrix<uint32> &A, uint32 p, MersenneTwister &MT, double density)
@@ -163,6 +207,8 @@ int main ()
 		test_trsm (65521, 130, 40, false, false);
 		test_trsm (2147483647u, 70, 9, true, true);
 		test_trsm (2147483647u, 70, 9, false, true);
+		test_trsm_sparse (65521, 300, 40);
+		test_trsm_sparse (2147483647u, 90, 7);
 		test_fl (65521, 96, 128, true);
 		test_fl (65521, 96, 128, false);
 		test_fl (2147483647u, 200, 300, true);
