@@ -10,10 +10,12 @@
  * diagIsOne) on DenseMatrix<uint32> operands run on the GPU through the C
  * ABI of include/lela_cuda.h, and FaugereLachartre<Modular<uint32>,
  * CUDAModule<uint32> >::echelonize runs the whole Faugere-Lachartre pipeline
- * there.  Operand combinations the GPU path does not take (sparse or
- * transposed operands) fall through to the parent module, exactly as an
- * unimplemented operation falls through LELA's module stack
- * (lela/blas/context.h:109-146).
+ * there; BLAS3::trsm also takes a sparse upper-triangular SparseMatrix<uint32>
+ * A.  With Context<GF2, CUDAModuleGF2>, BLAS3::gemm on DenseMatrix<bool>
+ * operands runs on the GPU.  Operand combinations the GPU path does not take
+ * (sparse gemm operands, sparse lower-triangular or transposed operands) fall
+ * through to the parent module, exactly as an unimplemented operation falls
+ * through LELA's module stack (lela/blas/context.h:109-146).
  *
  * Mechanism (the reference's own): a Modules class with a Tag whose Parent
  * is the next module (ZpModule<uint32>, lela/ring/modular.h:604-626), and
@@ -37,6 +39,7 @@
 #include "lela/matrix/dense.h"
 #include "lela/matrix/sparse.h"
 #include "lela/ring/modular.h"
+#include "lela/ring/gf2.h"
 #include "lela/util/error.h"
 #include "lela/algorithms/faugere-lachartre.h"
 
@@ -230,6 +233,86 @@ public:
 		{ return trsm_impl (F, M, a, A, B, type, diagIsOne,
 				    typename Matrix1::StorageType (),
 				    typename Matrix2::StorageType ()); }
+};
+
+} // namespace BLAS3
+
+/** The CUDA module over GF2: the GPU gemm on DenseMatrix<bool> operands
+ * (LELA's packed rows: 64-bit words, LittleEndian bit order, the layout
+ * without M4RI, lela/vector/bit-iterator.h:300-311); everything else is
+ * GenericModule<GF2>'s. */
+struct CUDAModuleGF2 : public GenericModule<GF2>
+{
+	struct Tag { typedef GenericModule<GF2>::Tag Parent; };
+
+	CUDAHandle cuda;
+
+	CUDAModuleGF2 (const GF2 &R) : GenericModule<GF2> (R) {}
+};
+
+namespace BLAS3
+{
+
+/** C <- a A B + b C over GF2 (replaces the generic Row*Row*Row gemm,
+ * lela/blas/level3-generic.tcc:243-263).  DenseMatrix<bool> operands are
+ * packed into contiguous words and go to lela_cuda_gemm_gf2; other matrix
+ * types go to the parent module. */
+template <>
+class _gemm<GF2, CUDAModuleGF2::Tag>
+{
+	static void pack (const DenseMatrix<bool> &M, std::vector<uint64_t> &w)
+	{
+		const size_t words = (M.coldim () + 63) / 64;
+		w.assign (M.rowdim () * words + 1, 0);
+		size_t i = 0;
+		for (DenseMatrix<bool>::ConstRowIterator r = M.rowBegin (); r != M.rowEnd (); ++r, ++i) {
+			DenseMatrix<bool>::ConstRow::const_word_iterator it = r->word_begin ();
+			for (size_t j = 0; j < words; ++j, ++it) {
+				uint64_t v = *it;
+				if (j == words - 1 && (M.coldim () & 63))
+					v &= (~0ULL) >> (64 - (M.coldim () & 63));
+				w[i * words + j] = v;
+			}
+		}
+	}
+
+	static void unpack (DenseMatrix<bool> &M, const std::vector<uint64_t> &w)
+	{
+		const size_t words = (M.coldim () + 63) / 64;
+		size_t i = 0;
+		for (DenseMatrix<bool>::RowIterator r = M.rowBegin (); r != M.rowEnd (); ++r, ++i) {
+			DenseMatrix<bool>::Row::word_iterator it = r->word_begin ();
+			for (size_t j = 0; j < words; ++j, ++it)
+				*it = w[i * words + j];
+		}
+	}
+
+public:
+	template <class Modules, class Matrix1, class Matrix2, class Matrix3>
+	static Matrix3 &op (const GF2 &F, Modules &M, bool a, const Matrix1 &A, const Matrix2 &B, bool b, Matrix3 &C)
+		{ return _gemm<GF2, CUDAModuleGF2::Tag::Parent>::op (F, M, a, A, B, b, C); }
+
+	template <class Modules>
+	static DenseMatrix<bool> &op (const GF2 &F, Modules &M, bool a, const DenseMatrix<bool> &A,
+				      const DenseMatrix<bool> &B, bool b, DenseMatrix<bool> &C)
+	{
+		lela_check (A.coldim () == B.rowdim ());
+		lela_check (A.rowdim () == C.rowdim ());
+		lela_check (B.coldim () == C.coldim ());
+		const size_t m = C.rowdim (), n = C.coldim (), k = A.coldim ();
+		if (m == 0 || n == 0)
+			return C;
+		std::vector<uint64_t> wa, wb, wc;
+		pack (A, wa);
+		pack (B, wb);
+		pack (C, wc);
+		const size_t kw = (k + 63) / 64, nw = (n + 63) / 64;
+		int st = lela_cuda_gemm_gf2 (M.cuda.get (), m, n, k, a ? 1 : 0, &wa[0], kw ? kw : 1, &wb[0], nw,
+					     b ? 1 : 0, &wc[0], nw);
+		lela_cuda_check (M.cuda.get (), st);
+		unpack (C, wc);
+		return C;
+	}
 };
 
 } // namespace BLAS3

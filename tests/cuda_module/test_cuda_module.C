@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "lela/ring/modular.h"
+#include "lela/ring/gf2.h"
 #include "lela/blas/context.h"
 #include "lela/blas/level3.h"
 #include "lela/matrix/dense.h"
@@ -156,6 +157,42 @@ static void test_trsm_sparse (uint32 p, size_t m, size_t n)
 	CHECK (gi == ci, what);
 }
 
+// GF(2) gemm on DenseMatrix<bool>: CUDAModuleGF2 against GenericModule<GF2>.
+static void test_gemm_gf2 (size_t m, size_t n, size_t k, bool a, bool b)
+{
+	GF2 F;
+	Context<GF2, CUDAModuleGF2> gpu (F);
+	Context<GF2, GenericModule<GF2> > cpu (F);
+	MersenneTwister MT (m * 3 + n * 5 + k);
+	DenseMatrix<bool> A (m, k), B (k, n), C (m, n), C2 (m, n);
+	for (size_t i = 0; i < m; ++i)
+		for (size_t j = 0; j < k; ++j)
+			A.setEntry (i, j, MT.randomIntRange (0, 2) != 0);
+	for (size_t i = 0; i < k; ++i)
+		for (size_t j = 0; j < n; ++j)
+			B.setEntry (i, j, MT.randomIntRange (0, 2) != 0);
+	for (size_t i = 0; i < m; ++i)
+		for (size_t j = 0; j < n; ++j) {
+			bool v = MT.randomIntRange (0, 2) != 0;
+			C.setEntry (i, j, v);
+			C2.setEntry (i, j, v);
+		}
+	BLAS3::gemm (gpu, a, A, B, b, C);
+	BLAS3::gemm (cpu, a, A, B, b, C2);
+	bool eq = true;
+	for (size_t i = 0; i < m && eq; ++i)
+		for (size_t j = 0; j < n; ++j) {
+			bool x, y;
+			C.getEntry (x, i, j);
+			C2.getEntry (y, i, j);
+			if (x != y) { eq = false; break; }
+		}
+	char what[160];
+	std::snprintf (what, sizeof what, "GF(2) gemm %zux%zux%zu a=%d b=%d CUDAModuleGF2 == GenericModule", m, n, k,
+		       (int) a, (int) b);
+	CHECK (eq, what);
+}
+
 // The reference test's F4 staircase (tests/test-faugere-lachartre.C:142-175),
 // written here for SparseMatrix<uint32> rows.
 static void random_f4 (SparseMatrix<uint32> &A, uint32 p, MersenneTwister &MT, double density)
@@ -207,6 +244,8 @@ int main ()
 		test_trsm (65521, 130, 40, false, false);
 		test_trsm (2147483647u, 70, 9, true, true);
 		test_trsm (2147483647u, 70, 9, false, true);
+		test_gemm_gf2 (130, 200, 257, true, true);
+		test_gemm_gf2 (64, 70, 129, true, false);
 		test_trsm_sparse (65521, 300, 40);
 		test_trsm_sparse (2147483647u, 90, 7);
 		test_fl (65521, 96, 128, true);
