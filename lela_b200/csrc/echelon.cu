@@ -230,7 +230,6 @@ __global__ void __launch_bounds__(HEADS_THREADS)
 // bound of the first nonzero column of their reduced panel part; cnt[h]
 // counts them by that bound.
 constexpr int PW_R = 80;                   // window rows
-constexpr int PW_FIND = (PW_R + 31) / 32;  // warps that test window rows
 // window rows padded to EW + 1 words: a column read across rows (the pivot
 // test, the multipliers) then touches every bank once
 constexpr int PW_LD = EW + 1;
@@ -253,7 +252,6 @@ __global__ void __launch_bounds__(PS_THREADS, 1)
   __shared__ uint32_t s_y[EW], s_S[EW], s_x[EW], s_sinv[EW];
   __shared__ int s_cnt[EW + 1];
   __shared__ int s_first[PS_FAST], s_wcnt[PS_FAST];
-  __shared__ int s_fa[2][PW_FIND];  // phase A per column, by column parity
   __shared__ int s_list[PS_THREADS], s_lrow[PS_THREADS], s_lhead[PS_THREADS];
   __shared__ int s_err, s_last, s_hi, s_wlast;
   const uint32_t p = ar.p;
@@ -303,15 +301,21 @@ __global__ void __launch_bounds__(PS_THREADS, 1)
   for (int col = 0; col < w && i < m; ++col) {
     const int *pm = perm[cur], *pp = ppos[cur];
     int *pn = perm[cur ^ 1], *ppn = ppos[cur ^ 1];
-    // A. first window entry (by position) with a nonzero in col
-    if (wid < PW_FIND) {
-      const bool nz = tid < nl && Wv[pm[tid]][col] != 0u;
-      const unsigned b = __ballot_sync(0xffffffffu, nz);
-      if (lane == 0) s_fa[col & 1][wid] = b ? tid + __ffs(b) - 1 : 0x7fffffff;
-    }
-    __syncthreads();
+    // A. first window entry (by position) with a nonzero in col.  Every warp
+    // finds it by itself: column col of the window and the entry list were
+    // last written before the previous column's closing barrier, and the
+    // work of this column (phase B) writes only columns right of col and the
+    // other list buffer, so no barrier is needed here
     int qs = 0x7fffffff;
-    for (int k = 0; k < PW_FIND; ++k) qs = min(qs, s_fa[col & 1][k]);
+    for (int base = 0; base < nl; base += 32) {
+      const int e = base + lane;
+      const bool nz = e < nl && Wv[pm[e]][col] != 0u;
+      const unsigned b = __ballot_sync(0xffffffffu, nz);
+      if (b) {
+        qs = base + __ffs(b) - 1;
+        break;
+      }
+    }
     const bool z = nl > 0 && pp[0] == i;  // the row at position i is window entry 0
     const uint32_t *P;                    // the pivot row (S_t times reduced)
     int q, drop;                          // pivot position; window entry leaving (-1: none)
@@ -324,8 +328,7 @@ __global__ void __launch_bounds__(PS_THREADS, 1)
         const int v = (lane <= col ? s_cnt[lane] : 0) + (lane + 32 <= col ? s_cnt[lane + 32] : 0);
         cand = __reduce_add_sync(0xffffffffu, v);
       }
-      // no barrier when there is no candidate: nothing shared changes, and
-      // the next column's phase A writes the other s_fa buffer
+      // no barrier when there is no candidate: nothing shared changes
       if (cand == 0) continue;
       __syncthreads();  // every thread has its count before s_cnt changes
       // per pass the CTA lists the candidates among PS_THREADS positions
