@@ -525,6 +525,24 @@ __global__ void gf2_l11_solve_kernel(uint64_t *__restrict__ D, size_t ld, int i0
     if (k < t) D[(size_t)(i0 + k) * ld + w] = x[k];
 }
 
+// The panel's multipliers into the block's rows of bits: rows i0..r1, the
+// t bits of L11 (pivot rows) or L21 (rows below) at bit offset off of the
+// row's GB words (the caller zeroed the block's rows).
+constexpr int GB = 4;  // panels (words) per block of delayed updates
+__global__ void gf2_deposit_kernel(uint64_t *__restrict__ Lb, int i0, int r1, int t, int off,
+                                   const uint64_t *__restrict__ L11,
+                                   const uint64_t *__restrict__ L21) {
+  const int r0 = i0 + t;
+  for (int pos = i0 + blockIdx.x * blockDim.x + threadIdx.x; pos <= r1;
+       pos += gridDim.x * blockDim.x) {
+    const uint64_t l = pos < r0 ? L11[pos - i0] : L21[pos - r0];
+    uint64_t *row = Lb + (size_t)pos * GB;
+    const int wq = off >> 6, sh = off & 63;
+    row[wq] |= l << sh;
+    if (sh && sh + t > 64) row[wq + 1] |= l >> (64 - sh);
+  }
+}
+
 int gf2_echelon_dev(Ctx *c, int m, int n, uint64_t *D, size_t ld, size_t *rank_out) {
   if (m < 0 || n < 0) return ctx_fail(c, ST_ARG, "negative dimension");
   const int nw = (n + 63) / 64;
@@ -540,9 +558,10 @@ int gf2_echelon_dev(Ctx *c, int m, int n, uint64_t *D, size_t ld, size_t *rank_o
       (((size_t)2 * m + 4 * GW + 1 + GW + 1) * sizeof(int) + 255) & ~(size_t)255;
   const size_t h_bytes = ((size_t)2 * m + 255) & ~(size_t)255;
   void *base = nullptr;
+  const size_t lb_bytes = (size_t)m * GB * 8 + (size_t)GB * GW * 8;  // block bits, panel L11s
   int st = ctx_buffer(c, BUF_GF2_0,
                       out_bytes + i_bytes + h_bytes + (size_t)m * 8 + 2 * GW * 8 +
-                          (size_t)2 * GW * nw * 8 + 1024,
+                          (size_t)2 * GW * std::max(nw, GB) * 8 + lb_bytes + 1024,
                       &base);
   if (st) return st;
   uint8_t *b8 = static_cast<uint8_t *>(base);
@@ -558,6 +577,8 @@ int gf2_echelon_dev(Ctx *c, int m, int n, uint64_t *D, size_t ld, size_t *rank_o
   uint64_t *d_L11 = d_L21 + m;
   uint64_t *d_U = d_L11 + GW;
   uint64_t *d_tmp = d_U + GW;
+  uint64_t *d_Lb = d_tmp + (size_t)2 * GW * std::max(nw, GB);  // m x GB words
+  uint64_t *d_L11s = d_Lb + (size_t)m * GB;                       // GB x GW words
   const uint32_t *d_pcol = reinterpret_cast<const uint32_t *>(b8 + offsetof(Gf2PanelOut, pcol));
   static std::once_flag once;
   static cudaError_t attr_err = cudaSuccess;
@@ -576,8 +597,50 @@ int gf2_echelon_dev(Ctx *c, int m, int n, uint64_t *D, size_t ld, size_t *rank_o
   int i = 0, epoch = 0;
   const int head_grid = std::max(1, std::min((m + GF2_HEADS_THREADS - 1) / GF2_HEADS_THREADS,
                                              c->num_sms * 2));
+  // Blocks of GB words (delayed updates), as in the Z/p form: when the
+  // block's first panel with pivots has at least DELAY_ROWS rows below it,
+  // the block's panels update only the block's words; the words right of it
+  // get, per block, U12 = L11^-1 A12 on the block's pivot rows (panel by
+  // panel: the earlier panels' part by a gemm, then the panel's own L11) and
+  // one C ^= L21 U12 with K = the block's pivots (up to 256 bits) on the rows
+  // below.  d_Lb row q (GB words) holds the multipliers of the row at
+  // position q, panel k of the block at bits Tb_k .. Tb_k + t_k - 1; later
+  // panels' transpositions move d_Lb's rows with D's.
+  constexpr int DELAY_ROWS = 512;
+  int ib = 0, Tb = 0, R = -1, bw1 = 0, delayed = 0, np = 0;
+  int pan_i[GB], pan_t[GB], pan_off[GB];
+  auto flush = [&]() -> int {
+    if (Tb == 0 || bw1 >= nw) return ST_OK;
+    const int nrest = n - 64 * bw1;  // bits right of the block
+    for (int j = 0; j < np; ++j) {
+      if (pan_off[j] > 0) {
+        int s = gf2_m4rm_dev(c, pan_t[j], nrest, pan_off[j], 1, d_Lb + (size_t)pan_i[j] * GB, GB,
+                             D + (size_t)ib * ld + bw1, ld, 1, D + (size_t)pan_i[j] * ld + bw1, ld);
+        if (s) return s;
+      }
+      gf2_l11_solve_kernel<<<(nw - bw1 + 127) / 128, 128, 0, c->stream>>>(
+          D, ld, pan_i[j], pan_t[j], bw1, nw, d_L11s + (size_t)j * GW);
+      ctx_launched(c);
+    }
+    const int rb = ib + Tb;
+    if (R < rb) return ST_OK;
+    int pi = prof_begin(c, "gf2_block_update");
+    int s = gf2_gemm_dev(c, GF2_AUTO, R - rb + 1, nrest, Tb, 1, d_Lb + (size_t)rb * GB, GB,
+                         D + (size_t)ib * ld + bw1, ld, 1, D + (size_t)rb * ld + bw1, ld);
+    prof_end(c, pi);
+    return s;
+  };
   for (int wc = 0; wc < nw && i < m; ++wc) {
     const int w = std::min(64, n - 64 * wc);
+    if (wc % GB == 0) {
+      if ((st = flush())) return st;
+      ib = i;
+      Tb = 0;
+      R = -1;
+      np = 0;
+      bw1 = std::min(nw, wc + GB);
+      delayed = -1;  // decided at the block's first panel with pivots
+    }
     const uint64_t pmask = (w == 64) ? ~0ull : ((1ull << w) - 1ull);
     int pi = prof_begin(c, "gf2_heads");
     gf2_heads_kernel<<<head_grid, GF2_HEADS_THREADS, 0, c->stream>>>(D, ld, i, m, wc, pmask,
@@ -618,10 +681,23 @@ int gf2_echelon_dev(Ctx *c, int m, int n, uint64_t *D, size_t ld, size_t *rank_o
       gf2_gather_rows_kernel<<<grid, 256, 0, c->stream>>>(D, ld, nw, d_perm, cnt, d_tmp);
       gf2_scatter_rows_kernel<<<grid, 256, 0, c->stream>>>(D, ld, nw, d_perm + cnt, cnt, d_tmp);
       ctx_launched(c, 2);
+      if (Tb > 0) {  // the block's earlier multipliers move with their rows
+        dim3 gl(1, cnt);
+        gf2_gather_rows_kernel<<<gl, 256, 0, c->stream>>>(d_Lb, GB, GB, d_perm, cnt, d_tmp);
+        gf2_scatter_rows_kernel<<<gl, 256, 0, c->stream>>>(d_Lb, GB, GB, d_perm + cnt, cnt, d_tmp);
+        ctx_launched(c, 2);
+      }
     }
     const int r0 = i + t;
     const int r1 = (h.last_pos >= (uint32_t)r0) ? (int)h.last_pos : r0 - 1;
     const int below = r1 - r0 + 1;
+    if (delayed < 0) {
+      delayed = below >= DELAY_ROWS && bw1 < nw;
+      if (delayed) {  // rows the panels' solves do not reach hold zero multipliers
+        e = cudaMemsetAsync(d_Lb + (size_t)i * GB, 0, (size_t)(m - i) * GB * 8, c->stream);
+        if (e != cudaSuccess) return ctx_cuda(c, e, "gf2 echelon: multipliers");
+      }
+    }
     {
       const int rows = r1 - i + 1;
       pi = prof_begin(c, "gf2_solve");
@@ -630,23 +706,42 @@ int gf2_echelon_dev(Ctx *c, int m, int n, uint64_t *D, size_t ld, size_t *rank_o
       prof_end(c, pi);
       ctx_launched(c);
     }
-    const int w1 = wc + 1;
-    if (w1 < nw) {
-      gf2_l11_solve_kernel<<<(nw - w1 + 127) / 128, 128, 0, c->stream>>>(D, ld, i, t, w1, nw,
-                                                                          d_L11);
+    if (delayed) {
+      const int rows = r1 - i + 1;
+      gf2_deposit_kernel<<<std::max(1, std::min((rows + 255) / 256, c->num_sms * 4)), 256, 0,
+                           c->stream>>>(d_Lb, i, r1, t, Tb, d_L11, d_L21);
+      e = cudaMemcpyAsync(d_L11s + (size_t)np * GW, d_L11, (size_t)t * 8, cudaMemcpyDeviceToDevice,
+                          c->stream);
+      if (e != cudaSuccess) return ctx_cuda(c, e, "gf2 echelon: panel multipliers");
+      ctx_launched(c);
+    }
+    // the rest of the block's words (delayed), or of all words
+    const int w1 = wc + 1, wend = delayed ? bw1 : nw;
+    if (w1 < wend) {
+      gf2_l11_solve_kernel<<<(wend - w1 + 127) / 128, 128, 0, c->stream>>>(D, ld, i, t, w1, wend,
+                                                                            d_L11);
       ctx_launched(c);
       if (below > 0) {
-        // rows r0..r1, trailing words: C ^= L21 (one word of t bits per row) * U12
+        // rows r0..r1, those words: C ^= L21 (one word of t bits per row) * U12
         pi = prof_begin(c, "gf2_update");
-        st = gf2_m4rm_dev(c, below, n - 64 * w1, t, 1, d_L21, 1, D + (size_t)i * ld + w1, ld, 1,
-                          D + (size_t)r0 * ld + w1, ld);
+        st = gf2_m4rm_dev(c, below, std::min(n, 64 * wend) - 64 * w1, t, 1, d_L21, 1,
+                          D + (size_t)i * ld + w1, ld, 1, D + (size_t)r0 * ld + w1, ld);
         prof_end(c, pi);
         if (st) return st;
       }
     }
+    if (delayed) {
+      pan_i[np] = i;
+      pan_t[np] = t;
+      pan_off[np] = Tb;
+      ++np;
+      R = std::max(R, std::max(r1, hi));
+      Tb += t;
+    }
     rank += t;
     i += t;
   }
+  if ((st = flush())) return st;
   *rank_out = rank;
   return ST_OK;
 }

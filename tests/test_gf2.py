@@ -101,3 +101,24 @@ def test_gf2_echelon_pivots_far_below(cuda):
     got, gr = cuda.echelonize_gf2(A.copy(), n)
     assert gr == wr
     assert np.array_equal(got, want)
+
+
+@pytest.mark.gpu
+def test_gf2_echelon_blocks(cuda):
+    """Several blocks of four word-panels with delayed trailing updates
+    (many rows below the pivots), rank-deficient and dense inputs, a band of
+    zero columns and pivots far below in the first block."""
+    for seed, (m, n, r) in enumerate([(1500, 1300, 1100), (1200, 2000, 1200), (2100, 700, 650)]):
+        A = gen.planted_rank_gf2(90 + seed, m, n, r)
+        if seed == 1:
+            A[:, 5] = 0                                   # a whole word column without pivots
+        want, wr = oracle.echelon_gf2(A, n)
+        got, gr = cuda.echelonize_gf2(A.copy(), n)
+        assert gr == wr, (m, n, r)
+        assert np.array_equal(got, want), (m, n, r)
+    m, n = 2500, 900
+    A = gen.dense_gf2(93, m, n)
+    A[:1800, :2] = 0                                      # the first panels' pivots far below
+    want, wr = oracle.echelon_gf2(A, n)
+    got, gr = cuda.echelonize_gf2(A.copy(), n)
+    assert gr == wr and np.array_equal(got, want)
