@@ -528,7 +528,7 @@ __global__ void gf2_l11_solve_kernel(uint64_t *__restrict__ D, size_t ld, int i0
 // The panel's multipliers into the block's rows of bits: rows i0..r1, the
 // t bits of L11 (pivot rows) or L21 (rows below) at bit offset off of the
 // row's GB words (the caller zeroed the block's rows).
-constexpr int GB = 4;  // panels (words) per block of delayed updates
+constexpr int GB = 8;  // panels (words) per block of delayed updates
 __global__ void gf2_deposit_kernel(uint64_t *__restrict__ Lb, int i0, int r1, int t, int off,
                                    const uint64_t *__restrict__ L11,
                                    const uint64_t *__restrict__ L21) {
@@ -614,8 +614,9 @@ int gf2_echelon_dev(Ctx *c, int m, int n, uint64_t *D, size_t ld, size_t *rank_o
     const int nrest = n - 64 * bw1;  // bits right of the block
     for (int j = 0; j < np; ++j) {
       if (pan_off[j] > 0) {
-        int s = gf2_m4rm_dev(c, pan_t[j], nrest, pan_off[j], 1, d_Lb + (size_t)pan_i[j] * GB, GB,
-                             D + (size_t)ib * ld + bw1, ld, 1, D + (size_t)pan_i[j] * ld + bw1, ld);
+        int s = gf2_gemm_dev(c, GF2_AUTO, pan_t[j], nrest, pan_off[j], 1,
+                             d_Lb + (size_t)pan_i[j] * GB, GB, D + (size_t)ib * ld + bw1, ld, 1,
+                             D + (size_t)pan_i[j] * ld + bw1, ld);
         if (s) return s;
       }
       gf2_l11_solve_kernel<<<(nw - bw1 + 127) / 128, 128, 0, c->stream>>>(
