@@ -602,7 +602,7 @@ int gf2_echelon_dev(Ctx *c, int m, int n, uint64_t *D, size_t ld, size_t *rank_o
   // the block's panels update only the block's words; the words right of it
   // get, per block, U12 = L11^-1 A12 on the block's pivot rows (panel by
   // panel: the earlier panels' part by a gemm, then the panel's own L11) and
-  // one C ^= L21 U12 with K = the block's pivots (up to 256 bits) on the rows
+  // one C ^= L21 U12 with K = the block's pivots (up to 64 GB bits) on the rows
   // below.  d_Lb row q (GB words) holds the multipliers of the row at
   // position q, panel k of the block at bits Tb_k .. Tb_k + t_k - 1; later
   // panels' transpositions move d_Lb's rows with D's.
