@@ -190,6 +190,7 @@ int lela_cuda_destroy(lela_cuda_ctx *h) {
   for (int i = 0; i < 32; ++i)
     if (c->buf[i]) cudaFree(c->buf[i]);
   if (c->batch_exec) cudaGraphExecDestroy(c->batch_exec);
+  if (c->panel_map) cudaFreeHost(c->panel_map);
   if (c->dstatus) cudaFree(c->dstatus);
   if (c->hstatus) cudaFreeHost(c->hstatus);
   for (auto &r : c->prof) {

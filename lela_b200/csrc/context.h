@@ -70,6 +70,10 @@ struct Ctx {
   // Device-memory budget of the batched FL entry point (bytes; 0 = 90 % of
   // the free memory plus what the worker handles already hold).
   size_t batch_budget = 0;
+  // Mapped (pinned, device-visible) host memory where the echelon panel
+  // search publishes its result and a sequence number; created on first use.
+  void *panel_map = nullptr, *panel_map_dev = nullptr;
+  uint32_t panel_seq = 0;
   std::string last_error;
 
   // Instantiated CUDA graph of the small-block batch launch, replayed while

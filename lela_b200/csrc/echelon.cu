@@ -50,8 +50,11 @@
 // rows are touched per panel; dense matrices make every row active and the
 // scheme becomes ordinary blocked LU with LELA's pivot choice.
 #include <algorithm>
+#include <atomic>
+#include <chrono>
 #include <cstddef>
 #include <mutex>
+#include <thread>
 #include <vector>
 
 #include "common.cuh"
@@ -241,7 +244,8 @@ __global__ void __launch_bounds__(PS_THREADS, 1)
                         A ar, uint8_t *__restrict__ head, const uint8_t *__restrict__ act,
                         int *__restrict__ hist, int *__restrict__ last_act, int *__restrict__ p2r,
                         int *__restrict__ stamp, int epoch, uint32_t *__restrict__ Uout,
-                        uint32_t *__restrict__ xinv_out, PanelOut *out) {
+                        uint32_t *__restrict__ xinv_out, PanelOut *out,
+                        PanelOut *hout, volatile uint32_t *hflag, uint32_t seq) {
   extern __shared__ __align__(16) uint32_t dyn_w[];
   uint32_t(*Wv)[PW_LD] = reinterpret_cast<uint32_t(*)[PW_LD]>(dyn_w);  // PW_R rows
   __shared__ uint32_t PV[EW][EW];
@@ -536,7 +540,22 @@ __global__ void __launch_bounds__(PS_THREADS, 1)
     out->last_pos = (uint32_t)(last >= 0 ? last : 0);
     out->det = det;
     *last_act = -1;
+    hout->t = (uint32_t)t;
+    hout->err = (uint32_t)s_err;
+    hout->last_pos = (uint32_t)(last >= 0 ? last : 0);
+    hout->det = det;
   }
+  // the result also goes to mapped host memory, then a sequence flag: the
+  // host waits on the flag instead of a copy and a stream synchronisation
+  __syncthreads();
+  for (int k = tid; k < t; k += PS_THREADS) {
+    hout->pcol[k] = out->pcol[k];
+    hout->ti[k] = out->ti[k];
+    hout->tq[k] = out->tq[k];
+  }
+  __threadfence_system();
+  __syncthreads();
+  if (tid == 0) *hflag = seq;
 }
 
 // Row permutation through a temporary: tmp[k] = D[src[k]], then
@@ -617,10 +636,24 @@ __global__ void __launch_bounds__(SOLVE_THREADS)
   }
 }
 
-static int sync_read(Ctx *c, const void *dev, void *host, size_t bytes, const char *what) {
-  cudaError_t e = cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, c->stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-  return e == cudaSuccess ? ST_OK : ctx_cuda(c, e, what);
+// Wait until the panel search has published sequence number seq in mapped
+// host memory (the work queued before it included), checking the stream for
+// errors now and then; bounded by PANEL_WAIT_S seconds.
+constexpr double PANEL_WAIT_S = 60.0;
+static int wait_panel(Ctx *c, volatile uint32_t *flag, uint32_t seq, const char *what) {
+  const auto t0 = std::chrono::steady_clock::now();
+  for (uint64_t spins = 1; *flag != seq; ++spins) {
+    if ((spins & 1023) == 0) {
+      const cudaError_t e = cudaStreamQuery(c->stream);
+      if (e != cudaSuccess && e != cudaErrorNotReady) return ctx_cuda(c, e, what);
+      if (e == cudaSuccess && *flag != seq) return ctx_fail(c, ST_CUDA, "echelon: panel result missing");
+      const double s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+      if (s > PANEL_WAIT_S) return ctx_fail(c, ST_TIMEOUT, "echelon: panel search did not finish");
+      std::this_thread::yield();
+    }
+  }
+  std::atomic_thread_fence(std::memory_order_acquire);
+  return ST_OK;
 }
 
 int zp_echelon_dev(Ctx *c, int m, int n, uint32_t p, uint32_t *D, size_t ld, size_t *rank_out,
@@ -685,6 +718,18 @@ int zp_echelon_dev(Ctx *c, int m, int n, uint32_t p, uint32_t *D, size_t ld, siz
   if (attr_err != cudaSuccess) return ctx_cuda(c, attr_err, "echelon: panel search attributes");
   const ArithSmall ars = ArithSmall::make(p);
   const ArithWide arw = ArithWide::make(p);
+  if (!c->panel_map) {
+    cudaError_t e0 = cudaHostAlloc(&c->panel_map, sizeof(PanelOut) + 64, cudaHostAllocMapped);
+    if (e0 == cudaSuccess) e0 = cudaHostGetDevicePointer(&c->panel_map_dev, c->panel_map, 0);
+    if (e0 != cudaSuccess) return ctx_cuda(c, e0, "echelon: mapped panel result");
+    *reinterpret_cast<volatile uint32_t *>(static_cast<char *>(c->panel_map) + sizeof(PanelOut)) = 0u;
+  }
+  const PanelOut *hmap = static_cast<const PanelOut *>(c->panel_map);
+  volatile uint32_t *hflag =
+      reinterpret_cast<volatile uint32_t *>(static_cast<char *>(c->panel_map) + sizeof(PanelOut));
+  PanelOut *hmap_dev = static_cast<PanelOut *>(c->panel_map_dev);
+  uint32_t *hflag_dev =
+      reinterpret_cast<uint32_t *>(static_cast<char *>(c->panel_map_dev) + sizeof(PanelOut));
   cudaError_t e = cudaMemsetAsync(d_stamp, 0xff, (size_t)m * sizeof(int), c->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(d_last, 0xff, sizeof(int), c->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(d_hist, 0, (EW + 1) * sizeof(int), c->stream);
@@ -737,19 +782,29 @@ int zp_echelon_dev(Ctx *c, int m, int n, uint32_t p, uint32_t *D, size_t ld, siz
     panel_heads_kernel<<<head_grid, HEADS_THREADS, 0, c->stream>>>(D, ld, i, m, c0, w, d_head,
                                                                     d_act, d_hist, d_last);
     prof_end(c, pi);
+    const uint32_t seq = ++c->panel_seq;
     pi = prof_begin(c, "ech_search");
     if (small)
       panel_search_kernel<<<1, PS_THREADS, PW_SMEM, c->stream>>>(
           D, ld, i, m, c0, w, ars, d_head, d_act, d_hist, d_last, d_p2r, d_stamp, epoch, d_U,
-          d_xinv, d_out);
+          d_xinv, d_out, hmap_dev, hflag_dev, seq);
     else
       panel_search_kernel<<<1, PS_THREADS, PW_SMEM, c->stream>>>(
           D, ld, i, m, c0, w, arw, d_head, d_act, d_hist, d_last, d_p2r, d_stamp, epoch, d_U,
-          d_xinv, d_out);
+          d_xinv, d_out, hmap_dev, hflag_dev, seq);
     ++epoch;
     prof_end(c, pi);
     ctx_launched(c, 2);
-    if ((st = sync_read(c, d_out, &h, sizeof h, "echelon: panel"))) return st;
+    if ((st = wait_panel(c, hflag, seq, "echelon: panel"))) return st;
+    h.t = hmap->t;
+    h.err = hmap->err;
+    h.last_pos = hmap->last_pos;
+    h.det = hmap->det;
+    for (uint32_t k = 0; k < h.t && k < (uint32_t)EW; ++k) {
+      h.pcol[k] = hmap->pcol[k];
+      h.ti[k] = hmap->ti[k];
+      h.tq[k] = hmap->tq[k];
+    }
     if (h.err) return ctx_fail(c, ST_PIVOT, "Could not invert pivot-element in the ring");
     const int t = (int)h.t;
     if (t == 0) continue;
