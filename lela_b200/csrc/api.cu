@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <condition_variable>
 #include <mutex>
 #include <cstdio>
@@ -105,6 +106,39 @@ int ctx_check_status(Ctx *c, const char *what) {
     snprintf(buf, sizeof buf, "%s: a device-side wait exceeded its limit", what);
     return ctx_fail(c, ST_TIMEOUT, buf);
   }
+  return ST_OK;
+}
+
+int ctx_panel_map(Ctx *c, void **host, void **dev) {
+  if (!c->panel_map) {
+    cudaError_t e = cudaHostAlloc(&c->panel_map, PANEL_MAP_BYTES, cudaHostAllocMapped);
+    if (e == cudaSuccess) e = cudaHostGetDevicePointer(&c->panel_map_dev, c->panel_map, 0);
+    if (e != cudaSuccess) {
+      if (c->panel_map) cudaFreeHost(c->panel_map);
+      c->panel_map = c->panel_map_dev = nullptr;
+      return ctx_cuda(c, e, "mapped panel result");
+    }
+    *reinterpret_cast<volatile uint32_t *>(static_cast<char *>(c->panel_map) + PANEL_FLAG_OFF) = 0u;
+    c->panel_seq = 0;
+  }
+  *host = c->panel_map;
+  *dev = c->panel_map_dev;
+  return ST_OK;
+}
+
+int ctx_wait_flag(Ctx *c, volatile uint32_t *flag, uint32_t seq, const char *what) {
+  const auto t0 = std::chrono::steady_clock::now();
+  for (uint64_t spins = 1; *flag != seq; ++spins) {
+    if ((spins & 1023) == 0) {
+      const cudaError_t e = cudaStreamQuery(c->stream);
+      if (e != cudaSuccess && e != cudaErrorNotReady) return ctx_cuda(c, e, what);
+      if (e == cudaSuccess && *flag != seq) return ctx_fail(c, ST_CUDA, "panel result missing");
+      const double s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+      if (s > 60.0) return ctx_fail(c, ST_TIMEOUT, "panel search did not finish");
+      std::this_thread::yield();
+    }
+  }
+  std::atomic_thread_fence(std::memory_order_acquire);
   return ST_OK;
 }
 

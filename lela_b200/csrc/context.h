@@ -141,6 +141,16 @@ int ctx_clear_status(Ctx *c);
 // a status code.
 int ctx_check_status(Ctx *c, const char *what);
 
+// Mapped (pinned, device-visible) host memory of PANEL_MAP_BYTES where a
+// panel search publishes its result (from offset 0) and then a sequence
+// number (a uint32 at PANEL_FLAG_OFF); allocated on first use.
+constexpr size_t PANEL_MAP_BYTES = 4096, PANEL_FLAG_OFF = 4032;
+int ctx_panel_map(Ctx *c, void **host, void **dev);
+// Spin until *flag == seq (the work queued before the publishing kernel
+// included), checking the handle's stream for errors now and then and
+// giving up after a minute.
+int ctx_wait_flag(Ctx *c, volatile uint32_t *flag, uint32_t seq, const char *what);
+
 // Profiling: prof_begin records the start event of a named kernel launch
 // (returns an index, or -1 when profiling is off); prof_end its end event.
 int prof_begin(Ctx *c, const char *name);

@@ -50,11 +50,8 @@
 // rows are touched per panel; dense matrices make every row active and the
 // scheme becomes ordinary blocked LU with LELA's pivot choice.
 #include <algorithm>
-#include <atomic>
-#include <chrono>
 #include <cstddef>
 #include <mutex>
-#include <thread>
 #include <vector>
 
 #include "common.cuh"
@@ -636,26 +633,6 @@ __global__ void __launch_bounds__(SOLVE_THREADS)
   }
 }
 
-// Wait until the panel search has published sequence number seq in mapped
-// host memory (the work queued before it included), checking the stream for
-// errors now and then; bounded by PANEL_WAIT_S seconds.
-constexpr double PANEL_WAIT_S = 60.0;
-static int wait_panel(Ctx *c, volatile uint32_t *flag, uint32_t seq, const char *what) {
-  const auto t0 = std::chrono::steady_clock::now();
-  for (uint64_t spins = 1; *flag != seq; ++spins) {
-    if ((spins & 1023) == 0) {
-      const cudaError_t e = cudaStreamQuery(c->stream);
-      if (e != cudaSuccess && e != cudaErrorNotReady) return ctx_cuda(c, e, what);
-      if (e == cudaSuccess && *flag != seq) return ctx_fail(c, ST_CUDA, "echelon: panel result missing");
-      const double s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-      if (s > PANEL_WAIT_S) return ctx_fail(c, ST_TIMEOUT, "echelon: panel search did not finish");
-      std::this_thread::yield();
-    }
-  }
-  std::atomic_thread_fence(std::memory_order_acquire);
-  return ST_OK;
-}
-
 int zp_echelon_dev(Ctx *c, int m, int n, uint32_t p, uint32_t *D, size_t ld, size_t *rank_out,
                    uint32_t *det_out, std::vector<int> *pivot_cols) {
   if (p < 2) return ctx_fail(c, ST_ARG, "modulus must be at least 2");
@@ -718,18 +695,13 @@ int zp_echelon_dev(Ctx *c, int m, int n, uint32_t p, uint32_t *D, size_t ld, siz
   if (attr_err != cudaSuccess) return ctx_cuda(c, attr_err, "echelon: panel search attributes");
   const ArithSmall ars = ArithSmall::make(p);
   const ArithWide arw = ArithWide::make(p);
-  if (!c->panel_map) {
-    cudaError_t e0 = cudaHostAlloc(&c->panel_map, sizeof(PanelOut) + 64, cudaHostAllocMapped);
-    if (e0 == cudaSuccess) e0 = cudaHostGetDevicePointer(&c->panel_map_dev, c->panel_map, 0);
-    if (e0 != cudaSuccess) return ctx_cuda(c, e0, "echelon: mapped panel result");
-    *reinterpret_cast<volatile uint32_t *>(static_cast<char *>(c->panel_map) + sizeof(PanelOut)) = 0u;
-  }
-  const PanelOut *hmap = static_cast<const PanelOut *>(c->panel_map);
-  volatile uint32_t *hflag =
-      reinterpret_cast<volatile uint32_t *>(static_cast<char *>(c->panel_map) + sizeof(PanelOut));
-  PanelOut *hmap_dev = static_cast<PanelOut *>(c->panel_map_dev);
-  uint32_t *hflag_dev =
-      reinterpret_cast<uint32_t *>(static_cast<char *>(c->panel_map_dev) + sizeof(PanelOut));
+  static_assert(sizeof(PanelOut) <= PANEL_FLAG_OFF, "panel result and flag share the mapped page");
+  void *mh = nullptr, *md = nullptr;
+  if ((st = ctx_panel_map(c, &mh, &md))) return st;
+  const PanelOut *hmap = static_cast<const PanelOut *>(mh);
+  volatile uint32_t *hflag = reinterpret_cast<volatile uint32_t *>(static_cast<char *>(mh) + PANEL_FLAG_OFF);
+  PanelOut *hmap_dev = static_cast<PanelOut *>(md);
+  uint32_t *hflag_dev = reinterpret_cast<uint32_t *>(static_cast<char *>(md) + PANEL_FLAG_OFF);
   cudaError_t e = cudaMemsetAsync(d_stamp, 0xff, (size_t)m * sizeof(int), c->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(d_last, 0xff, sizeof(int), c->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(d_hist, 0, (EW + 1) * sizeof(int), c->stream);
@@ -795,7 +767,7 @@ int zp_echelon_dev(Ctx *c, int m, int n, uint32_t p, uint32_t *D, size_t ld, siz
     ++epoch;
     prof_end(c, pi);
     ctx_launched(c, 2);
-    if ((st = wait_panel(c, hflag, seq, "echelon: panel"))) return st;
+    if ((st = ctx_wait_flag(c, hflag, seq, "echelon: panel"))) return st;
     h.t = hmap->t;
     h.err = hmap->err;
     h.last_pos = hmap->last_pos;

@@ -278,7 +278,8 @@ __global__ void __launch_bounds__(GF2_SEARCH_THREADS)
                       uint64_t pmask, uint8_t *__restrict__ head, const uint8_t *__restrict__ act,
                       int *__restrict__ hist, int *__restrict__ last_act, int *__restrict__ p2r,
                       int *__restrict__ stamp, int epoch, uint64_t *__restrict__ Uout,
-                      Gf2PanelOut *out) {
+                      Gf2PanelOut *out, Gf2PanelOut *hout, volatile uint32_t *hflag,
+                      uint32_t seq) {
   extern __shared__ __align__(16) uint8_t gdyn[];
   __shared__ uint64_t G[GW], M[GW];
   __shared__ int s_pcol[GW];
@@ -447,7 +448,19 @@ __global__ void __launch_bounds__(GF2_SEARCH_THREADS)
     out->t = (uint32_t)t;
     out->last_pos = (uint32_t)(last >= 0 ? last : 0);
     *last_act = -1;
+    hout->t = (uint32_t)t;
+    hout->last_pos = (uint32_t)(last >= 0 ? last : 0);
   }
+  // the result also goes to mapped host memory, then the sequence flag
+  __syncwarp();
+  for (int k = lane; k < t; k += 32) {
+    hout->ti[k] = out->ti[k];
+    hout->tq[k] = out->tq[k];
+    hout->pcol[k] = out->pcol[k];
+  }
+  __threadfence_system();
+  __syncwarp();
+  if (lane == 0) *hflag = seq;
 }
 
 // Rows i0..r1 at their final positions: the reference's elimination steps
@@ -587,6 +600,13 @@ int gf2_echelon_dev(Ctx *c, int m, int n, uint64_t *D, size_t ld, size_t *rank_o
                                     (int)GF2_SEARCH_SMEM);
   });
   if (attr_err != cudaSuccess) return ctx_cuda(c, attr_err, "gf2 echelon: search attributes");
+  static_assert(sizeof(Gf2PanelOut) <= PANEL_FLAG_OFF, "panel result and flag share the mapped page");
+  void *mh = nullptr, *md = nullptr;
+  if ((st = ctx_panel_map(c, &mh, &md))) return st;
+  const Gf2PanelOut *hmap = static_cast<const Gf2PanelOut *>(mh);
+  volatile uint32_t *hflag = reinterpret_cast<volatile uint32_t *>(static_cast<char *>(mh) + PANEL_FLAG_OFF);
+  Gf2PanelOut *hmap_dev = static_cast<Gf2PanelOut *>(md);
+  uint32_t *hflag_dev = reinterpret_cast<uint32_t *>(static_cast<char *>(md) + PANEL_FLAG_OFF);
   cudaError_t e = cudaMemsetAsync(d_stamp, 0xff, (size_t)m * sizeof(int), c->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(d_last, 0xff, sizeof(int), c->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(d_hist, 0, (GW + 1) * sizeof(int), c->stream);
@@ -647,15 +667,21 @@ int gf2_echelon_dev(Ctx *c, int m, int n, uint64_t *D, size_t ld, size_t *rank_o
     gf2_heads_kernel<<<head_grid, GF2_HEADS_THREADS, 0, c->stream>>>(D, ld, i, m, wc, pmask,
                                                                      d_head, d_act, d_hist, d_last);
     prof_end(c, pi);
+    const uint32_t seq = ++c->panel_seq;
     pi = prof_begin(c, "gf2_search");
     gf2_search_kernel<<<1, GF2_SEARCH_THREADS, GF2_SEARCH_SMEM, c->stream>>>(
         D, ld, i, m, wc, w, pmask, d_head, d_act, d_hist, d_last, d_p2r, d_stamp, epoch++, d_U,
-        d_out);
+        d_out, hmap_dev, hflag_dev, seq);
     prof_end(c, pi);
     ctx_launched(c, 2);
-    e = cudaMemcpyAsync(&h, d_out, sizeof h, cudaMemcpyDeviceToHost, c->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-    if (e != cudaSuccess) return ctx_cuda(c, e, "gf2 echelon: panel");
+    if ((st = ctx_wait_flag(c, hflag, seq, "gf2 echelon: panel"))) return st;
+    h.t = hmap->t;
+    h.last_pos = hmap->last_pos;
+    for (uint32_t k = 0; k < h.t && k < (uint32_t)GW; ++k) {
+      h.ti[k] = hmap->ti[k];
+      h.tq[k] = hmap->tq[k];
+      h.pcol[k] = hmap->pcol[k];
+    }
     const int t = (int)h.t;
     if (t == 0) continue;
     int hi = i;
