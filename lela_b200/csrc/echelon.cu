@@ -595,11 +595,12 @@ __global__ void __launch_bounds__(SOLVE_THREADS)
   __shared__ uint32_t sX[EW];
   __shared__ int sP[EW];
   const int tid = threadIdx.x, lane = tid & 31;
-  for (int e = tid; e < t * EW; e += SOLVE_THREADS) sU[e / EW][e % EW] = Uin[e];
+  for (int e = tid; e < t * EW; e += SOLVE_THREADS) cp_async4(&sU[e / EW][e % EW], Uin + e, true);
   if (tid < EW) {
     sX[tid] = tid < t ? xinv[tid] : 0u;
     sP[tid] = tid < t ? (int)pcol[tid] : 0;
   }
+  cp_async_wait_all();
   __syncthreads();
   const uint32_t p = ar.p;
   const int warps = (gridDim.x * SOLVE_THREADS) >> 5;

@@ -101,11 +101,15 @@ __global__ void __launch_bounds__(128)
                     int ncols, Modulus mod, uint32_t two64, uint32_t alpha) {
   __shared__ uint32_t sT[TRI_NB][TRI_NB + 1];
   __shared__ uint32_t sD[TRI_NB];
+  // asynchronous copies, all in flight at once (entries outside nb x nb are
+  // zero-filled)
   for (int e = threadIdx.x; e < TRI_NB * TRI_NB; e += blockDim.x) {
-    int r = e / TRI_NB, cc = e % TRI_NB;
-    sT[r][cc] = (r < nb && cc < nb) ? T[(size_t)r * ldt + cc] : 0u;
+    const int r = e / TRI_NB, cc = e % TRI_NB;
+    const bool in = r < nb && cc < nb;
+    cp_async4(&sT[r][cc], in ? T + (size_t)r * ldt + cc : T, in);
   }
   for (int e = threadIdx.x; e < TRI_NB; e += blockDim.x) sD[e] = (e < nb && dinv) ? dinv[e] : 1u;
+  cp_async_wait_all();
   __syncthreads();
   const int gt = blockIdx.x * blockDim.x + threadIdx.x;
   const int col = gt >> 2, q = gt & 3;
@@ -144,10 +148,12 @@ __global__ void __launch_bounds__(256)
   const int nb = min(TRI_NB, m - r0);
   const uint32_t *T = A + (size_t)r0 * lda + r0;
   for (int e = threadIdx.x; e < TRI_NB * TRI_NB; e += blockDim.x) {
-    int r = e / TRI_NB, cc = e % TRI_NB;
-    sT[r][cc] = (r < nb && cc < nb) ? T[(size_t)r * lda + cc] : 0u;
+    const int r = e / TRI_NB, cc = e % TRI_NB;
+    const bool in = r < nb && cc < nb;
+    cp_async4(&sT[r][cc], in ? T + (size_t)r * lda + cc : T, in);
   }
   for (int e = threadIdx.x; e < TRI_NB; e += blockDim.x) sD[e] = (e < nb && dinv) ? dinv[r0 + e] : 1u;
+  cp_async_wait_all();
   __syncthreads();
   const int j = threadIdx.x >> 2, q = threadIdx.x & 3;
   uint32_t x[TRI_NB / 4];
