@@ -206,7 +206,7 @@ __global__ void __launch_bounds__(HEADS_THREADS)
 }
 
 // 2. The reference's pivot choice on the panel (see the file comment).
-// The window: the first PW_R rows at or below i0, by position, with a nonzero
+// The window: the first wcap <= PW_R rows at or below i0, by position, with a nonzero
 // in the panel, kept in shared memory and eliminated eagerly without
 // division: when pivot row P (pivot value y) is chosen, every window row W
 // becomes y W - W[col] P.  So a window row holds S_t times its row reduced
@@ -242,7 +242,7 @@ __global__ void __launch_bounds__(PS_THREADS, 1)
                         int *__restrict__ hist, int *__restrict__ last_act, int *__restrict__ p2r,
                         int *__restrict__ stamp, int epoch, uint32_t *__restrict__ Uout,
                         uint32_t *__restrict__ xinv_out, PanelOut *out,
-                        PanelOut *hout, volatile uint32_t *hflag, uint32_t seq) {
+                        PanelOut *hout, volatile uint32_t *hflag, uint32_t seq, int wcap) {
   extern __shared__ __align__(16) uint32_t dyn_w[];
   uint32_t(*Wv)[PW_LD] = reinterpret_cast<uint32_t(*)[PW_LD]>(dyn_w);  // PW_R rows
   __shared__ uint32_t PV[EW][EW];
@@ -265,7 +265,7 @@ __global__ void __launch_bounds__(PS_THREADS, 1)
     s_cnt[tid] = hist[tid];
     hist[tid] = 0;
   }
-  for (int base = i0; base < m && nl < PW_R; base += PS_THREADS) {
+  for (int base = i0; base < m && nl < wcap; base += PS_THREADS) {
     const int pos = base + tid;
     const bool a = pos < m && act[pos];
     const unsigned bal = __ballot_sync(0xffffffffu, a);
@@ -278,7 +278,7 @@ __global__ void __launch_bounds__(PS_THREADS, 1)
       cnt += v;
     }
     off += __popc(bal & ((1u << lane) - 1u));
-    const int take = min(cnt, PW_R - nl);
+    const int take = min(cnt, wcap - nl);
     if (a && off < take) {
       const int slot = nl + off;
       perm[0][slot] = slot;
@@ -286,7 +286,7 @@ __global__ void __launch_bounds__(PS_THREADS, 1)
       wrow[slot] = pos;
       const uint32_t *src = D + (size_t)pos * ld + c0;
       for (int c = 0; c < EW; ++c) cp_async4(&Wv[slot][c], src + (c < w ? c : 0), c < w);
-      if (off == PW_R - 1 - nl) s_wlast = pos;
+      if (off == wcap - 1 - nl) s_wlast = pos;
     }
     nl += take;
     __syncthreads();  // s_wcnt is rewritten by the next pass
@@ -741,6 +741,11 @@ int zp_echelon_dev(Ctx *c, int m, int n, uint32_t p, uint32_t *D, size_t ld, siz
     prof_end(c, pi);
     return s;
   };
+  // window rows of the search: the full PW_R, or 64 when the previous panel
+  // had many rows below its pivots (dense matrices, where the first 64
+  // active rows nearly always hold the panel's pivots; the rows past the
+  // window stay reachable through the search's slower path)
+  int wcap = PW_R;
   for (int c0 = 0; c0 < n && i < m; c0 += EW) {
     const int w = std::min(EW, n - c0);
     if (c0 % EB == 0) {
@@ -760,11 +765,11 @@ int zp_echelon_dev(Ctx *c, int m, int n, uint32_t p, uint32_t *D, size_t ld, siz
     if (small)
       panel_search_kernel<<<1, PS_THREADS, PW_SMEM, c->stream>>>(
           D, ld, i, m, c0, w, ars, d_head, d_act, d_hist, d_last, d_p2r, d_stamp, epoch, d_U,
-          d_xinv, d_out, hmap_dev, hflag_dev, seq);
+          d_xinv, d_out, hmap_dev, hflag_dev, seq, wcap);
     else
       panel_search_kernel<<<1, PS_THREADS, PW_SMEM, c->stream>>>(
           D, ld, i, m, c0, w, arw, d_head, d_act, d_hist, d_last, d_p2r, d_stamp, epoch, d_U,
-          d_xinv, d_out, hmap_dev, hflag_dev, seq);
+          d_xinv, d_out, hmap_dev, hflag_dev, seq, wcap);
     ++epoch;
     prof_end(c, pi);
     ctx_launched(c, 2);
@@ -817,6 +822,7 @@ int zp_echelon_dev(Ctx *c, int m, int n, uint32_t p, uint32_t *D, size_t ld, siz
     const int r0 = i + t;
     const int r1 = (h.last_pos >= (uint32_t)r0) ? (int)h.last_pos : r0 - 1;
     const int below = r1 - r0 + 1;
+    wcap = below >= DELAY_ROWS ? EW : PW_R;
     if (delayed < 0) {
       delayed = below >= DELAY_ROWS;
       if (delayed) {  // rows a panel's solve does not reach hold zero multipliers
