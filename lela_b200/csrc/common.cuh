@@ -194,8 +194,8 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t by
 }
 
 // ------------------------------------------------------------------ TMA
-// 3-D tiled bulk tensor load global -> shared, completion counted on an
-// mbarrier (no multicast).
+// 3-D tiled bulk tensor load global -> shared of this CTA only, completion
+// counted on an mbarrier.
 __device__ __forceinline__ void tma_load_3d(void *dst, const void *tmap, uint64_t *bar, int c0,
                                             int c1, int c2) {
   asm volatile(
