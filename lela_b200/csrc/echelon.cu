@@ -555,25 +555,24 @@ __global__ void __launch_bounds__(PS_THREADS, 1)
   if (tid == 0) *hflag = seq;
 }
 
-// Row permutation through a temporary: tmp[k] = D[src[k]], then
-// D[dst[k]] = tmp[k] (full rows).
-__global__ void gather_rows_kernel(const uint32_t *__restrict__ D, size_t ld, int n,
-                                   const int *__restrict__ src, int cnt, uint32_t *__restrict__ tmp) {
-  for (int k = blockIdx.y; k < cnt; k += gridDim.y) {
-    const uint32_t *s = D + (size_t)src[k] * ld;
-    uint32_t *d = tmp + (size_t)k * n;
-    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
-      d[j] = s[j];
+// Row permutation in one launch: each CTA takes a slice of PERM_COLS
+// columns, reads that slice of every source row into shared memory, then
+// writes it to the destination rows (the CTAs own disjoint columns, so no
+// grid-wide ordering is needed).  cnt <= 2 * EW rows.
+constexpr int PERM_COLS = 64;
+__global__ void __launch_bounds__(256)
+    permute_rows_kernel(uint32_t *__restrict__ D, size_t ld, int n, const int *__restrict__ src,
+                        const int *__restrict__ dst, int cnt) {
+  __shared__ uint32_t sl[2 * EW][PERM_COLS];
+  const int c0 = blockIdx.x * PERM_COLS;
+  for (int e = threadIdx.x; e < cnt * PERM_COLS; e += blockDim.x) {
+    const int k = e / PERM_COLS, cc = e % PERM_COLS;
+    if (c0 + cc < n) sl[k][cc] = D[(size_t)src[k] * ld + c0 + cc];
   }
-}
-__global__ void scatter_rows_kernel(uint32_t *__restrict__ D, size_t ld, int n,
-                                    const int *__restrict__ dst, int cnt,
-                                    const uint32_t *__restrict__ tmp) {
-  for (int k = blockIdx.y; k < cnt; k += gridDim.y) {
-    uint32_t *d = D + (size_t)dst[k] * ld;
-    const uint32_t *s = tmp + (size_t)k * n;
-    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
-      d[j] = s[j];
+  __syncthreads();
+  for (int e = threadIdx.x; e < cnt * PERM_COLS; e += blockDim.x) {
+    const int k = e / PERM_COLS, cc = e % PERM_COLS;
+    if (c0 + cc < n) D[(size_t)dst[k] * ld + c0 + cc] = sl[k][cc];
   }
 }
 
@@ -656,10 +655,9 @@ int zp_echelon_dev(Ctx *c, int m, int n, uint32_t p, uint32_t *D, size_t ld, siz
   const size_t h_bytes = ((size_t)2 * m + 255) & ~(size_t)255;
   const size_t sq_bytes = (size_t)EW * EW * 4;
   const size_t l_bytes = (size_t)m * EB * 4;
-  const size_t tmp_bytes = (size_t)2 * EW * std::max(n, EB) * 4;
   void *base = nullptr;
   int st = ctx_buffer(c, BUF_ECH_0,
-                      out_bytes + i_bytes + h_bytes + 2 * sq_bytes + l_bytes + tmp_bytes + 1024,
+                      out_bytes + i_bytes + h_bytes + 2 * sq_bytes + l_bytes + 1024,
                       &base);
   if (st) return st;
   uint8_t *b8 = static_cast<uint8_t *>(base);
@@ -674,7 +672,6 @@ int zp_echelon_dev(Ctx *c, int m, int n, uint32_t p, uint32_t *D, size_t ld, siz
   uint32_t *d_U = reinterpret_cast<uint32_t *>(b8 + out_bytes + i_bytes + h_bytes);
   uint32_t *d_xinv = d_U + EW * EW;  // pivot inverses (EW)
   uint32_t *d_L = d_xinv + EW * EW;  // the block's multipliers (m x EB)
-  uint32_t *d_tmp = d_L + (size_t)m * EB;
   const uint32_t *d_pcol = reinterpret_cast<const uint32_t *>(b8 + offsetof(PanelOut, pcol));
   void *gws = nullptr;
   // one size for the panel and block updates and the block's trsm (which
@@ -807,15 +804,13 @@ int zp_echelon_dev(Ctx *c, int m, int n, uint32_t p, uint32_t *D, size_t ld, siz
       e = cudaMemcpyAsync(d_perm, both.data(), both.size() * sizeof(int), cudaMemcpyHostToDevice,
                           c->stream);
       if (e != cudaSuccess) return ctx_cuda(c, e, "echelon: permutation");
-      dim3 grid((n + 255) / 256, cnt);
-      gather_rows_kernel<<<grid, 256, 0, c->stream>>>(D, ld, n, d_perm, cnt, d_tmp);
-      scatter_rows_kernel<<<grid, 256, 0, c->stream>>>(D, ld, n, d_perm + cnt, cnt, d_tmp);
-      ctx_launched(c, 2);
+      permute_rows_kernel<<<(n + PERM_COLS - 1) / PERM_COLS, 256, 0, c->stream>>>(
+          D, ld, n, d_perm, d_perm + cnt, cnt);
+      ctx_launched(c);
       if (Tb > 0) {  // the multipliers of the block's earlier panels move too
-        dim3 gl((EB + 255) / 256, cnt);
-        gather_rows_kernel<<<gl, 256, 0, c->stream>>>(d_L, EB, EB, d_perm, cnt, d_tmp);
-        scatter_rows_kernel<<<gl, 256, 0, c->stream>>>(d_L, EB, EB, d_perm + cnt, cnt, d_tmp);
-        ctx_launched(c, 2);
+        permute_rows_kernel<<<(EB + PERM_COLS - 1) / PERM_COLS, 256, 0, c->stream>>>(
+            d_L, EB, EB, d_perm, d_perm + cnt, cnt);
+        ctx_launched(c);
       }
     }
     // L11 / L21 and the panel's final values

@@ -498,19 +498,25 @@ __global__ void gf2_solve_kernel(uint64_t *__restrict__ D, size_t ld, int i0, in
   }
 }
 
-__global__ void gf2_gather_rows_kernel(const uint64_t *__restrict__ D, size_t ld, int nw,
-                                       const int *__restrict__ src, int cnt,
-                                       uint64_t *__restrict__ tmp) {
-  for (int k = blockIdx.y; k < cnt; k += gridDim.y)
-    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nw; j += gridDim.x * blockDim.x)
-      tmp[(size_t)k * nw + j] = D[(size_t)src[k] * ld + j];
-}
-__global__ void gf2_scatter_rows_kernel(uint64_t *__restrict__ D, size_t ld, int nw,
-                                        const int *__restrict__ dst, int cnt,
-                                        const uint64_t *__restrict__ tmp) {
-  for (int k = blockIdx.y; k < cnt; k += gridDim.y)
-    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nw; j += gridDim.x * blockDim.x)
-      D[(size_t)dst[k] * ld + j] = tmp[(size_t)k * nw + j];
+// Row permutation in one launch: each CTA takes GF2_PERM_WORDS words of
+// every moved row, reads the source rows' slice into shared memory, then
+// writes it to the destination rows (CTAs own disjoint words, so no
+// grid-wide ordering is needed).  cnt <= 2 * GW rows.
+constexpr int GF2_PERM_WORDS = 16;
+__global__ void __launch_bounds__(256)
+    gf2_permute_rows_kernel(uint64_t *__restrict__ D, size_t ld, int nw,
+                            const int *__restrict__ src, const int *__restrict__ dst, int cnt) {
+  __shared__ uint64_t sl[2 * GW][GF2_PERM_WORDS];
+  const int w0 = blockIdx.x * GF2_PERM_WORDS;
+  for (int e = threadIdx.x; e < cnt * GF2_PERM_WORDS; e += blockDim.x) {
+    const int k = e / GF2_PERM_WORDS, j = e % GF2_PERM_WORDS;
+    if (w0 + j < nw) sl[k][j] = D[(size_t)src[k] * ld + w0 + j];
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < cnt * GF2_PERM_WORDS; e += blockDim.x) {
+    const int k = e / GF2_PERM_WORDS, j = e % GF2_PERM_WORDS;
+    if (w0 + j < nw) D[(size_t)dst[k] * ld + w0 + j] = sl[k][j];
+  }
 }
 
 // U12 = L11^-1 A12 over GF(2): pivot rows i0..i0+t-1, words from w1; row k
@@ -573,8 +579,7 @@ int gf2_echelon_dev(Ctx *c, int m, int n, uint64_t *D, size_t ld, size_t *rank_o
   void *base = nullptr;
   const size_t lb_bytes = (size_t)m * GB * 8 + (size_t)GB * GW * 8;  // block bits, panel L11s
   int st = ctx_buffer(c, BUF_GF2_0,
-                      out_bytes + i_bytes + h_bytes + (size_t)m * 8 + 2 * GW * 8 +
-                          (size_t)2 * GW * std::max(nw, GB) * 8 + lb_bytes + 1024,
+                      out_bytes + i_bytes + h_bytes + (size_t)m * 8 + 2 * GW * 8 + lb_bytes + 1024,
                       &base);
   if (st) return st;
   uint8_t *b8 = static_cast<uint8_t *>(base);
@@ -589,8 +594,7 @@ int gf2_echelon_dev(Ctx *c, int m, int n, uint64_t *D, size_t ld, size_t *rank_o
   uint64_t *d_L21 = reinterpret_cast<uint64_t *>(b8 + out_bytes + i_bytes + h_bytes);
   uint64_t *d_L11 = d_L21 + m;
   uint64_t *d_U = d_L11 + GW;
-  uint64_t *d_tmp = d_U + GW;
-  uint64_t *d_Lb = d_tmp + (size_t)2 * GW * std::max(nw, GB);  // m x GB words
+  uint64_t *d_Lb = d_U + GW;                 // m x GB words
   uint64_t *d_L11s = d_Lb + (size_t)m * GB;                       // GB x GW words
   const uint32_t *d_pcol = reinterpret_cast<const uint32_t *>(b8 + offsetof(Gf2PanelOut, pcol));
   static std::once_flag once;
@@ -704,15 +708,13 @@ int gf2_echelon_dev(Ctx *c, int m, int n, uint64_t *D, size_t ld, size_t *rank_o
       e = cudaMemcpyAsync(d_perm, both.data(), both.size() * sizeof(int), cudaMemcpyHostToDevice,
                           c->stream);
       if (e != cudaSuccess) return ctx_cuda(c, e, "gf2 echelon: permutation");
-      dim3 grid((nw + 255) / 256, cnt);
-      gf2_gather_rows_kernel<<<grid, 256, 0, c->stream>>>(D, ld, nw, d_perm, cnt, d_tmp);
-      gf2_scatter_rows_kernel<<<grid, 256, 0, c->stream>>>(D, ld, nw, d_perm + cnt, cnt, d_tmp);
-      ctx_launched(c, 2);
+      gf2_permute_rows_kernel<<<(nw + GF2_PERM_WORDS - 1) / GF2_PERM_WORDS, 256, 0,
+                                c->stream>>>(D, ld, nw, d_perm, d_perm + cnt, cnt);
+      ctx_launched(c);
       if (Tb > 0) {  // the block's earlier multipliers move with their rows
-        dim3 gl(1, cnt);
-        gf2_gather_rows_kernel<<<gl, 256, 0, c->stream>>>(d_Lb, GB, GB, d_perm, cnt, d_tmp);
-        gf2_scatter_rows_kernel<<<gl, 256, 0, c->stream>>>(d_Lb, GB, GB, d_perm + cnt, cnt, d_tmp);
-        ctx_launched(c, 2);
+        gf2_permute_rows_kernel<<<(GB + GF2_PERM_WORDS - 1) / GF2_PERM_WORDS, 256, 0,
+                                  c->stream>>>(d_Lb, GB, GB, d_perm, d_perm + cnt, cnt);
+        ctx_launched(c);
       }
     }
     const int r0 = i + t;
