@@ -100,7 +100,13 @@ int lela_cuda_profile_reset (lela_cuda_ctx *ctx);
  * Replaces BLAS3::gemm (lela/blas/level3.h:82) for Modular<uint32> and dense
  * operands: _gemm<Modular<uint32>, Tag> reached through StrassenModule ->
  * ZpModule -> GenericModule (lela/blas/level3-sw.h:25-62,
- * lela/blas/level3-generic.tcc:285-322). */
+ * lela/blas/level3-generic.tcc:285-322).
+ * The host-pointer form returns when C holds the result.  For tensor-core
+ * products with k <= 32768 and m >= 1024 it works in row blocks: B is
+ * copied first, then A's and C's rows block by block on a second stream of
+ * the handle, and each block's rows of C are copied back on a third while
+ * later blocks still arrive.  Page-locked host buffers let the copies
+ * overlap. */
 int lela_cuda_gemm_zp_u32 (lela_cuda_ctx *ctx, size_t m, size_t n, size_t k, uint32_t p,
 			   uint32_t a, const uint32_t *A, size_t lda, const uint32_t *B, size_t ldb,
 			   uint32_t b, uint32_t *C, size_t ldc);

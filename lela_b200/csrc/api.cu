@@ -91,6 +91,17 @@ int ctx_stage(Ctx *c, int slot, size_t bytes, void **out) {
   return st;
 }
 
+int ctx_pipe(Ctx *c) {
+  if (c->pipe_ev[2 * PIPE_MAX_BLOCKS + 2]) return ST_OK;  // the last one made
+  cudaError_t e = cudaSuccess;
+  if (!c->copy_in) e = cudaStreamCreateWithFlags(&c->copy_in, cudaStreamNonBlocking);
+  if (e == cudaSuccess && !c->copy_out)
+    e = cudaStreamCreateWithFlags(&c->copy_out, cudaStreamNonBlocking);
+  for (int i = 0; e == cudaSuccess && i < 2 * PIPE_MAX_BLOCKS + 3; ++i)
+    if (!c->pipe_ev[i]) e = cudaEventCreateWithFlags(&c->pipe_ev[i], cudaEventDisableTiming);
+  return e == cudaSuccess ? ST_OK : ctx_cuda(c, e, "copy streams");
+}
+
 int ctx_clear_status(Ctx *c) {
   cudaError_t e = cudaMemsetAsync(c->dstatus, 0, 16 * sizeof(uint32_t), c->stream);
   return e == cudaSuccess ? ST_OK : ctx_cuda(c, e, "cudaMemsetAsync(status)");
@@ -225,6 +236,10 @@ int lela_cuda_destroy(lela_cuda_ctx *h) {
     if (c->buf[i]) cudaFree(c->buf[i]);
   if (c->batch_exec) cudaGraphExecDestroy(c->batch_exec);
   if (c->panel_map) cudaFreeHost(c->panel_map);
+  for (auto e : c->pipe_ev)
+    if (e) cudaEventDestroy(e);
+  if (c->copy_in) cudaStreamDestroy(c->copy_in);
+  if (c->copy_out) cudaStreamDestroy(c->copy_out);
   if (c->dstatus) cudaFree(c->dstatus);
   if (c->hstatus) cudaFreeHost(c->hstatus);
   for (auto &r : c->prof) {
@@ -388,6 +403,13 @@ int lela_cuda_gemm_zp_u32(lela_cuda_ctx *h, size_t m, size_t n, size_t k, uint32
   if (!st && k) st = ctx_stage(c, 1, k * n * 4, &dB);
   if (!st) st = ctx_stage(c, 2, m * n * 4, &dC);
   if (!st) st = ctx_clear_status(c);
+  if (!st && zp_gemm_pipelined(c, (int)m, (int)n, (int)k, p, a)) {
+    // large tensor-core products: copies overlapped with the product
+    st = zp_gemm_host_rows(c, (int)m, (int)n, (int)k, p, a, A, lda, B, ldb, b, C, ldc,
+                           (uint32_t *)dA, (uint32_t *)dB, (uint32_t *)dC);
+    if (!st) st = ctx_check_status(c, "gemm_zp_u32");
+    return st;
+  }
   if (!st && k) st = h2d_matrix(c, dA, A, m, k, lda, 4);
   if (!st && k) st = h2d_matrix(c, dB, B, k, n, ldb, 4);
   // With b = 0 mod p the kernels never read C.

@@ -38,6 +38,9 @@ enum TrsmKernel : int {
   TRSM_INVERSE = 2,  // 512-row diagonal blocks inverted, applied by the tensor-core gemm
 };
 
+// Most row blocks of the pipelined host-pointer gemm.
+constexpr int PIPE_MAX_BLOCKS = 16;
+
 struct Ctx {
   int device = 0;
   int num_sms = 148;
@@ -59,6 +62,12 @@ struct Ctx {
   // Device staging buffers for the host-pointer entry points.
   void *stage[4] = {nullptr, nullptr, nullptr, nullptr};
   size_t stage_bytes[4] = {0, 0, 0, 0};
+  // Copy streams and events of the pipelined host-pointer gemm (created on
+  // first use): host->device on copy_in, device->host on copy_out; events
+  // [0, PIPE_MAX_BLOCKS) mark a row block's operands in, the next
+  // PIPE_MAX_BLOCKS its product done, then start, B in, copies out.
+  cudaStream_t copy_in = nullptr, copy_out = nullptr;
+  cudaEvent_t pipe_ev[2 * PIPE_MAX_BLOCKS + 3] = {};
 
   // Named grow-only device buffers of the algorithms (see BufSlot).
   void *buf[32] = {};
@@ -132,6 +141,9 @@ int ctx_buffer(Ctx *c, int slot, size_t bytes, void **out);
 int ctx_workspace(Ctx *c, size_t bytes, void **out);
 int ctx_workspace2(Ctx *c, size_t bytes, void **out);
 int ctx_stage(Ctx *c, int slot, size_t bytes, void **out);
+// Creates the copy streams and events of the pipelined host-pointer gemm
+// on first use.
+int ctx_pipe(Ctx *c);
 // Record a CUDA error (returns ST_CUDA) or a message (returns code).
 int ctx_fail(Ctx *c, int code, const char *msg);
 int ctx_cuda(Ctx *c, cudaError_t e, const char *what);

@@ -664,18 +664,25 @@ static int encode_3d(Ctx *c, CUtensorMap *tm, void *base, uint64_t d0, uint64_t 
 }
 
 template <int L>
+static int tc_attr(Ctx *c) {
+  static std::once_flag once;
+  static cudaError_t attr_err = cudaSuccess;
+  std::call_once(once, [] {
+    attr_err = cudaFuncSetAttribute(zp_gemm_tc_kernel<L, 0>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    TcLayout<L>::SMEM);
+  });
+  return attr_err == cudaSuccess ? ST_OK
+                                 : ctx_cuda(c, attr_err, "cudaFuncSetAttribute(zp_gemm_tc)");
+}
+
+template <int L>
 static int launch_tc(Ctx *c, int M, int N, int K, const Modulus &mod, uint32_t alpha,
                      const uint32_t *A, size_t lda, const uint32_t *B, size_t ldb, uint32_t beta,
                      uint32_t *C, size_t ldc, uint8_t *ws) {
   using Cfg = TcCfg<L>;
   using Lay = TcLayout<L>;
-  static std::once_flag once;
-  static cudaError_t attr_err = cudaSuccess;
-  std::call_once(once, [] {
-    attr_err = cudaFuncSetAttribute(zp_gemm_tc_kernel<L, 0>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, Lay::SMEM);
-  });
-  if (attr_err != cudaSuccess) return ctx_cuda(c, attr_err, "cudaFuncSetAttribute(zp_gemm_tc)");
+  if (int st = tc_attr<L>(c)) return st;
   const int tiles = ((M + BM - 1) / BM) * ((N + Cfg::BN - 1) / Cfg::BN);
   uint32_t b = beta;
   for (int k0 = 0; k0 < K; k0 += ZP_KCHUNK) {
@@ -720,6 +727,18 @@ size_t zp_gemm_workspace_bytes(uint32_t p, int M, int N, int K) {
   return (size_t)L * ((size_t)M + N) * Kp + 256;
 }
 
+int zp_gemm_pick(const Ctx *c, int M, int N, int K, uint32_t p) {
+  if (c->gemm_kernel != GEMM_AUTO) return c->gemm_kernel;
+  // small K: the CUDA-core kernel below its measured crossover with the
+  // tensor-core path (whose fixed and per-output costs grow with the limb
+  // count L)
+  const double work = (double)M * N * K;
+  const bool wide = zp_limbs_for(p) == 4;
+  const bool smallk = wide ? ((K <= 64 && work <= 4.0e9) || (K <= 256 && work <= 2.4e9))
+                           : ((K <= 32 && work <= 4.0e9) || (K <= 256 && work <= 6.0e8));
+  return smallk ? GEMM_SMALLK : GEMM_TC;
+}
+
 int zp_gemm_dev(Ctx *c, int kernel, int M, int N, int K, uint32_t p, uint32_t alpha,
                 const uint32_t *A, size_t lda, const uint32_t *B, size_t ldb, uint32_t beta,
                 uint32_t *C, size_t ldc, uint8_t *ws_override) {
@@ -740,17 +759,7 @@ int zp_gemm_dev(Ctx *c, int kernel, int M, int N, int K, uint32_t p, uint32_t al
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? ST_OK : ctx_cuda(c, e, "zp_scale launch");
   }
-  if (kernel == GEMM_AUTO) kernel = c->gemm_kernel;
-  if (kernel == GEMM_AUTO) {
-    // small K: the CUDA-core kernel below its measured crossover with the
-    // tensor-core path (whose fixed and per-output costs grow with the limb
-    // count L)
-    const double work = (double)M * N * K;
-    const bool wide = zp_limbs_for(p) == 4;
-    const bool smallk = wide ? ((K <= 64 && work <= 4.0e9) || (K <= 256 && work <= 2.4e9))
-                             : ((K <= 32 && work <= 4.0e9) || (K <= 256 && work <= 6.0e8));
-    kernel = smallk ? GEMM_SMALLK : GEMM_TC;
-  }
+  if (kernel == GEMM_AUTO) kernel = zp_gemm_pick(c, M, N, K, p);
   if (kernel == GEMM_SMALLK) {
     dim3 grid((N + PT - 1) / PT, (M + PT - 1) / PT);
     int pi = prof_begin(c, "zp_gemm_smallk");
@@ -786,6 +795,137 @@ int zp_gemm_dev(Ctx *c, int kernel, int M, int N, int K, uint32_t p, uint32_t al
     case 1: return launch_tc<1>(c, M, N, K, mod, alpha, A, lda, B, ldb, beta, C, ldc, ws);
     case 2: return launch_tc<2>(c, M, N, K, mod, alpha, A, lda, B, ldb, beta, C, ldc, ws);
     default: return launch_tc<4>(c, M, N, K, mod, alpha, A, lda, B, ldb, beta, C, ldc, ws);
+  }
+}
+
+// ============================================ pipelined host-pointer gemm
+//
+// The host-pointer gemm moves (M K + K N + 2 M N) * 4 bytes over the host
+// link for 2 M N K operations on the GPU: at 8192^3 the copies take about
+// ten times as long as the product.  The rows of C are therefore done in
+// blocks: B goes over first, then A's and C's rows block by block on the
+// copy_in stream; each block's product runs on the handle stream as soon as
+// its rows are in, and its rows of C go back on the copy_out stream while
+// later blocks still arrive (the two directions of the link run at once).
+// The result is the same product: every output element is computed by the
+// same kernel from the same operands, only the launches cover fewer rows.
+
+bool zp_gemm_pipelined(const Ctx *c, int M, int N, int K, uint32_t p, uint32_t alpha) {
+  return K > 0 && K <= ZP_KCHUNK && alpha % p != 0 && M >= 2 * PIPE_MIN_ROWS &&
+         zp_gemm_pick(c, M, N, K, p) == GEMM_TC;
+}
+
+template <int L>
+static int host_rows(Ctx *c, int M, int N, int K, const Modulus &mod, uint32_t alpha,
+                     const uint32_t *hA, size_t lda, const uint32_t *hB, size_t ldb,
+                     uint32_t beta, uint32_t *hC, size_t ldc, uint32_t *dA, uint32_t *dB,
+                     uint32_t *dC, uint8_t *ws) {
+  using Cfg = TcCfg<L>;
+  using Lay = TcLayout<L>;
+  if (int st = tc_attr<L>(c)) return st;
+  const int Kp = (K + 15) & ~15;
+  // row blocks: a multiple of the tile height, at most PIPE_MAX_BLOCKS
+  const int per = (M + PIPE_MAX_BLOCKS - 1) / PIPE_MAX_BLOCKS;
+  const int rb = std::max(PIPE_MIN_ROWS, (per + BM - 1) / BM * BM);
+  const int nblk = (M + rb - 1) / rb;
+  cudaEvent_t *ready = c->pipe_ev, *done = c->pipe_ev + PIPE_MAX_BLOCKS;
+  cudaEvent_t ev_start = c->pipe_ev[2 * PIPE_MAX_BLOCKS], ev_b = c->pipe_ev[2 * PIPE_MAX_BLOCKS + 1],
+              ev_out = c->pipe_ev[2 * PIPE_MAX_BLOCKS + 2];
+  const size_t rowA = (size_t)K * 4, rowC = (size_t)N * 4;
+  // the copies start after the work already queued on the handle stream
+  cudaError_t e = cudaEventRecord(ev_start, c->stream);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(c->copy_in, ev_start, 0);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(c->copy_out, ev_start, 0);
+  if (e == cudaSuccess)
+    e = cudaMemcpy2DAsync(dB, rowC, hB, ldb * 4, rowC, (size_t)K, cudaMemcpyHostToDevice,
+                          c->copy_in);
+  if (e == cudaSuccess) e = cudaEventRecord(ev_b, c->copy_in);
+  for (int j = 0; e == cudaSuccess && j < nblk; ++j) {
+    const int r0 = j * rb, rows = std::min(rb, M - r0);
+    e = cudaMemcpy2DAsync(dA + (size_t)r0 * K, rowA, hA + (size_t)r0 * lda, lda * 4, rowA,
+                          (size_t)rows, cudaMemcpyHostToDevice, c->copy_in);
+    if (e == cudaSuccess && beta)
+      e = cudaMemcpy2DAsync(dC + (size_t)r0 * N, rowC, hC + (size_t)r0 * ldc, ldc * 4, rowC,
+                            (size_t)rows, cudaMemcpyHostToDevice, c->copy_in);
+    if (e == cudaSuccess) e = cudaEventRecord(ready[j], c->copy_in);
+  }
+  // B's limb planes once; block j's A planes in their own part of the
+  // workspace, so that a block's split never overwrites planes an earlier
+  // block's kernel still reads
+  int st = ST_OK;
+  uint8_t *Bl = ws + (size_t)L * M * Kp;
+  CUtensorMap tmB;
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(c->stream, ev_b, 0);
+  if (e == cudaSuccess) {
+    int pi = prof_begin(c, "zp_split");
+    dim3 grid2((N + 31) / 32, (Kp + 63) / 64);
+    split_cols_kernel<L><<<grid2, 256, 0, c->stream>>>(dB, (size_t)N, K, N, Bl, Kp);
+    prof_end(c, pi);
+    ctx_launched(c);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess)
+    st = encode_3d(c, &tmB, Bl, (uint64_t)K, (uint64_t)N, L, (uint64_t)Kp, (uint64_t)N * Kp, BK,
+                   Cfg::BN, L);
+  for (int j = 0; e == cudaSuccess && !st && j < nblk; ++j) {
+    const int r0 = j * rb, rows = std::min(rb, M - r0);
+    uint8_t *Al = ws + (size_t)L * r0 * Kp;
+    e = cudaStreamWaitEvent(c->stream, ready[j], 0);
+    if (e != cudaSuccess) break;
+    const size_t total = (size_t)rows * ((K + 3) / 4);
+    const int sgrid = (int)std::min<size_t>((total + 255) / 256, (size_t)c->num_sms * 16);
+    int pi = prof_begin(c, "zp_split");
+    split_rows_kernel<L><<<sgrid, 256, 0, c->stream>>>(dA + (size_t)r0 * K, (size_t)K, rows, K,
+                                                       Al, Kp);
+    prof_end(c, pi);
+    CUtensorMap tmA;
+    st = encode_3d(c, &tmA, Al, (uint64_t)K, (uint64_t)rows, L, (uint64_t)Kp,
+                   (uint64_t)rows * Kp, BK, BM, L);
+    if (st) break;
+    const int tiles = ((rows + BM - 1) / BM) * ((N + Cfg::BN - 1) / Cfg::BN);
+    pi = prof_begin(c, "zp_gemm_tc");
+    zp_gemm_tc_kernel<L, 0><<<std::min(tiles, c->num_sms), TC_THREADS, Lay::SMEM, c->stream>>>(
+        tmA, tmB, dC + (size_t)r0 * N, (size_t)N, rows, N, K, mod, alpha, beta, c->dstatus);
+    prof_end(c, pi);
+    ctx_launched(c, 2);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaEventRecord(done[j], c->stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(c->copy_out, done[j], 0);
+    if (e == cudaSuccess)
+      e = cudaMemcpy2DAsync(hC + (size_t)r0 * ldc, ldc * 4, dC + (size_t)r0 * N, rowC, rowC,
+                            (size_t)rows, cudaMemcpyDeviceToHost, c->copy_out);
+  }
+  // the handle stream ends after the last copy out
+  if (e == cudaSuccess && !st) e = cudaEventRecord(ev_out, c->copy_out);
+  if (e == cudaSuccess && !st) e = cudaStreamWaitEvent(c->stream, ev_out, 0);
+  if (e != cudaSuccess || st) {
+    // copies already queued may still use the caller's buffers
+    cudaStreamSynchronize(c->copy_in);
+    cudaStreamSynchronize(c->copy_out);
+    return st ? st : ctx_cuda(c, e, "pipelined gemm");
+  }
+  return ST_OK;
+}
+
+int zp_gemm_host_rows(Ctx *c, int M, int N, int K, uint32_t p, uint32_t alpha,
+                      const uint32_t *hA, size_t lda, const uint32_t *hB, size_t ldb,
+                      uint32_t beta, uint32_t *hC, size_t ldc, uint32_t *dA, uint32_t *dB,
+                      uint32_t *dC) {
+  if (!zp_gemm_pipelined(c, M, N, K, p, alpha)) return ctx_fail(c, ST_ARG, "not a pipelined gemm");
+  if (int st = ctx_pipe(c)) return st;
+  void *w = nullptr;
+  if (int st = ctx_workspace(c, zp_gemm_workspace_bytes(p, M, N, K), &w)) return st;
+  uint8_t *ws = static_cast<uint8_t *>(w);
+  const Modulus mod = make_modulus(p);
+  alpha %= p;
+  beta %= p;
+  switch (zp_limbs_for(p)) {
+    case 1:
+      return host_rows<1>(c, M, N, K, mod, alpha, hA, lda, hB, ldb, beta, hC, ldc, dA, dB, dC, ws);
+    case 2:
+      return host_rows<2>(c, M, N, K, mod, alpha, hA, lda, hB, ldb, beta, hC, ldc, dA, dB, dC, ws);
+    default:
+      return host_rows<4>(c, M, N, K, mod, alpha, hA, lda, hB, ldb, beta, hC, ldc, dA, dB, dC, ws);
   }
 }
 

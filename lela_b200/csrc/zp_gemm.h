@@ -21,6 +21,26 @@ int zp_gemm_dev(Ctx *c, int kernel, int M, int N, int K, uint32_t p, uint32_t al
                 const uint32_t *A, size_t lda, const uint32_t *B, size_t ldb, uint32_t beta,
                 uint32_t *C, size_t ldc, uint8_t *ws_override);
 
+// The kernel GEMM_AUTO resolves to for this shape (the handle's forced
+// kernel, else the small-K crossover rule).
+int zp_gemm_pick(const Ctx *c, int M, int N, int K, uint32_t p);
+
+// Whether the host-pointer gemm of this shape is done in row blocks with
+// its copies overlapped (tensor-core path, one K chunk, at least two blocks
+// of PIPE_MIN_ROWS rows).
+constexpr int PIPE_MIN_ROWS = 512;
+bool zp_gemm_pipelined(const Ctx *c, int M, int N, int K, uint32_t p, uint32_t alpha);
+
+// C <- alpha*A*B + beta*C mod p with A, B, C in host memory (row strides
+// lda, ldb, ldc) through the device buffers dA (M x K), dB (K x N), dC
+// (M x N, packed): the row-block pipeline above.  Asynchronous on the
+// handle stream, which ends after the last copy back; the caller
+// synchronises it.  Only for shapes zp_gemm_pipelined accepts.
+int zp_gemm_host_rows(Ctx *c, int M, int N, int K, uint32_t p, uint32_t alpha,
+                      const uint32_t *hA, size_t lda, const uint32_t *hB, size_t ldb,
+                      uint32_t beta, uint32_t *hC, size_t ldc, uint32_t *dA, uint32_t *dB,
+                      uint32_t *dC);
+
 }  // namespace lela
 
 namespace lela {

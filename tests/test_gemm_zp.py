@@ -132,3 +132,26 @@ def test_gemm_8192_property(cuda):
     C0 = gen.dense_zp(23, n, n, p)
     C = cuda.gemm(p, 1, A, B, 1, C0.copy())
     assert props.freivalds_gemm(p, A, B, C0, C, 1, 1)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("p", [251, 65521, 2147483647])
+def test_gemm_host_row_blocks(cuda, p):
+    """Host-pointer gemms large enough for the row-block pipeline (copies on
+    two streams overlapped with the per-block products): ragged last
+    block, row strides larger than the rows, b = 0 (C never read) and
+    b != 0, one limb count per modulus."""
+    big = gen.dense_zp(31, 1300, 700, p)
+    A = big[3:1203, 10:310]                   # 1200 x 300, lda = 700
+    B = gen.dense_zp(32, 300, 520, p)
+    Cbig = gen.dense_zp(33, 1250, 600, p)
+    C = Cbig[20:1220, 40:560]                 # 1200 x 520, ldc = 600
+    for a, b in ((1, 1), (p - 1, 0), (7, 11)):
+        want = oracle.gemm_zp(p, A, B, C, a, b, threads=8)
+        before = Cbig.copy()
+        cuda.gemm(p, a, A, B, b, C)
+        assert np.array_equal(C, want), (p, a, b)
+        mask = np.ones_like(Cbig, dtype=bool)
+        mask[20:1220, 40:560] = False
+        assert np.array_equal(Cbig[mask], before[mask])
+        C[...] = want                         # next case starts from this C
