@@ -556,23 +556,27 @@ __global__ void __launch_bounds__(PS_THREADS, 1)
 }
 
 // Row permutation in one launch: each CTA takes a slice of PERM_COLS
-// columns, reads that slice of every source row into shared memory, then
-// writes it to the destination rows (the CTAs own disjoint columns, so no
-// grid-wide ordering is needed).  cnt <= 2 * EW rows.
-constexpr int PERM_COLS = 64;
-__global__ void __launch_bounds__(256)
+// columns of every moved row.  Its threads load all their elements of the
+// source rows at once (at most PERM_PER each, into registers), wait at the
+// barrier, then store them to the destination rows; the CTAs own disjoint
+// columns, so no grid-wide ordering is needed.  cnt <= 2 * EW rows.
+constexpr int PERM_THREADS = 256, PERM_COLS = 32;
+constexpr int PERM_PER = 2 * EW * PERM_COLS / PERM_THREADS;
+__global__ void __launch_bounds__(PERM_THREADS)
     permute_rows_kernel(uint32_t *__restrict__ D, size_t ld, int n, const int *__restrict__ src,
                         const int *__restrict__ dst, int cnt) {
-  __shared__ uint32_t sl[2 * EW][PERM_COLS];
-  const int c0 = blockIdx.x * PERM_COLS;
-  for (int e = threadIdx.x; e < cnt * PERM_COLS; e += blockDim.x) {
-    const int k = e / PERM_COLS, cc = e % PERM_COLS;
-    if (c0 + cc < n) sl[k][cc] = D[(size_t)src[k] * ld + c0 + cc];
+  const int c0 = blockIdx.x * PERM_COLS, total = cnt * PERM_COLS;
+  uint32_t v[PERM_PER];
+#pragma unroll
+  for (int u = 0; u < PERM_PER; ++u) {
+    const int e = threadIdx.x + u * PERM_THREADS, c = c0 + e % PERM_COLS;
+    v[u] = (e < total && c < n) ? D[(size_t)src[e / PERM_COLS] * ld + c] : 0u;
   }
   __syncthreads();
-  for (int e = threadIdx.x; e < cnt * PERM_COLS; e += blockDim.x) {
-    const int k = e / PERM_COLS, cc = e % PERM_COLS;
-    if (c0 + cc < n) D[(size_t)dst[k] * ld + c0 + cc] = sl[k][cc];
+#pragma unroll
+  for (int u = 0; u < PERM_PER; ++u) {
+    const int e = threadIdx.x + u * PERM_THREADS, c = c0 + e % PERM_COLS;
+    if (e < total && c < n) D[(size_t)dst[e / PERM_COLS] * ld + c] = v[u];
   }
 }
 
@@ -804,11 +808,11 @@ int zp_echelon_dev(Ctx *c, int m, int n, uint32_t p, uint32_t *D, size_t ld, siz
       e = cudaMemcpyAsync(d_perm, both.data(), both.size() * sizeof(int), cudaMemcpyHostToDevice,
                           c->stream);
       if (e != cudaSuccess) return ctx_cuda(c, e, "echelon: permutation");
-      permute_rows_kernel<<<(n + PERM_COLS - 1) / PERM_COLS, 256, 0, c->stream>>>(
+      permute_rows_kernel<<<(n + PERM_COLS - 1) / PERM_COLS, PERM_THREADS, 0, c->stream>>>(
           D, ld, n, d_perm, d_perm + cnt, cnt);
       ctx_launched(c);
       if (Tb > 0) {  // the multipliers of the block's earlier panels move too
-        permute_rows_kernel<<<(EB + PERM_COLS - 1) / PERM_COLS, 256, 0, c->stream>>>(
+        permute_rows_kernel<<<(EB + PERM_COLS - 1) / PERM_COLS, PERM_THREADS, 0, c->stream>>>(
             d_L, EB, EB, d_perm, d_perm + cnt, cnt);
         ctx_launched(c);
       }

@@ -499,23 +499,27 @@ __global__ void gf2_solve_kernel(uint64_t *__restrict__ D, size_t ld, int i0, in
 }
 
 // Row permutation in one launch: each CTA takes GF2_PERM_WORDS words of
-// every moved row, reads the source rows' slice into shared memory, then
-// writes it to the destination rows (CTAs own disjoint words, so no
-// grid-wide ordering is needed).  cnt <= 2 * GW rows.
-constexpr int GF2_PERM_WORDS = 16;
-__global__ void __launch_bounds__(256)
+// every moved row.  Its threads load all their words of the source rows at
+// once (at most GF2_PERM_PER each, into registers), wait at the barrier,
+// then store them to the destination rows; the CTAs own disjoint words, so
+// no grid-wide ordering is needed.  cnt <= 2 * GW rows.
+constexpr int GF2_PERM_THREADS = 256, GF2_PERM_WORDS = 16;
+constexpr int GF2_PERM_PER = 2 * GW * GF2_PERM_WORDS / GF2_PERM_THREADS;
+__global__ void __launch_bounds__(GF2_PERM_THREADS)
     gf2_permute_rows_kernel(uint64_t *__restrict__ D, size_t ld, int nw,
                             const int *__restrict__ src, const int *__restrict__ dst, int cnt) {
-  __shared__ uint64_t sl[2 * GW][GF2_PERM_WORDS];
-  const int w0 = blockIdx.x * GF2_PERM_WORDS;
-  for (int e = threadIdx.x; e < cnt * GF2_PERM_WORDS; e += blockDim.x) {
-    const int k = e / GF2_PERM_WORDS, j = e % GF2_PERM_WORDS;
-    if (w0 + j < nw) sl[k][j] = D[(size_t)src[k] * ld + w0 + j];
+  const int w0 = blockIdx.x * GF2_PERM_WORDS, total = cnt * GF2_PERM_WORDS;
+  uint64_t v[GF2_PERM_PER];
+#pragma unroll
+  for (int u = 0; u < GF2_PERM_PER; ++u) {
+    const int e = threadIdx.x + u * GF2_PERM_THREADS, w = w0 + e % GF2_PERM_WORDS;
+    v[u] = (e < total && w < nw) ? D[(size_t)src[e / GF2_PERM_WORDS] * ld + w] : 0ull;
   }
   __syncthreads();
-  for (int e = threadIdx.x; e < cnt * GF2_PERM_WORDS; e += blockDim.x) {
-    const int k = e / GF2_PERM_WORDS, j = e % GF2_PERM_WORDS;
-    if (w0 + j < nw) D[(size_t)dst[k] * ld + w0 + j] = sl[k][j];
+#pragma unroll
+  for (int u = 0; u < GF2_PERM_PER; ++u) {
+    const int e = threadIdx.x + u * GF2_PERM_THREADS, w = w0 + e % GF2_PERM_WORDS;
+    if (e < total && w < nw) D[(size_t)dst[e / GF2_PERM_WORDS] * ld + w] = v[u];
   }
 }
 
@@ -708,12 +712,12 @@ int gf2_echelon_dev(Ctx *c, int m, int n, uint64_t *D, size_t ld, size_t *rank_o
       e = cudaMemcpyAsync(d_perm, both.data(), both.size() * sizeof(int), cudaMemcpyHostToDevice,
                           c->stream);
       if (e != cudaSuccess) return ctx_cuda(c, e, "gf2 echelon: permutation");
-      gf2_permute_rows_kernel<<<(nw + GF2_PERM_WORDS - 1) / GF2_PERM_WORDS, 256, 0,
+      gf2_permute_rows_kernel<<<(nw + GF2_PERM_WORDS - 1) / GF2_PERM_WORDS, GF2_PERM_THREADS, 0,
                                 c->stream>>>(D, ld, nw, d_perm, d_perm + cnt, cnt);
       ctx_launched(c);
       if (Tb > 0) {  // the block's earlier multipliers move with their rows
-        gf2_permute_rows_kernel<<<(GB + GF2_PERM_WORDS - 1) / GF2_PERM_WORDS, 256, 0,
-                                  c->stream>>>(d_Lb, GB, GB, d_perm, d_perm + cnt, cnt);
+        gf2_permute_rows_kernel<<<(GB + GF2_PERM_WORDS - 1) / GF2_PERM_WORDS, GF2_PERM_THREADS,
+                                  0, c->stream>>>(d_Lb, GB, GB, d_perm, d_perm + cnt, cnt);
         ctx_launched(c);
       }
     }
