@@ -49,44 +49,79 @@ __global__ void diag_inverse_kernel(const uint32_t *__restrict__ A, size_t lda, 
 // Solve T x = x in place for one column held by a quad of threads: thread q
 // holds the entries k = 4i + q (x[i]); T (nb x nb, nb <= 64, lower or upper
 // triangular) is in shared memory with its inverted diagonal sD (unitd: 1).
-// For each k the quad sums its partial products (two shuffles) and the owner
-// of k finishes x[k], so the sequential chain per thread is a quarter of the
-// triangle.  Products accumulate in 64 bits with the reference's wrap-around
-// correction (+2^64 mod p); NOWRAP (p < 2^28): the sums cannot wrap, no
-// check.  The k loop stays rolled (a fully unrolled 64-step body does not
-// fit the instruction cache); x[k / 4] is picked and written back by selects
-// over the 16 registers.  Entries from nb on are zero and never solved.
+// Right-looking: each thread keeps, per entry it holds, the 64-bit sum of
+// the products T[j][k] x[k] of the entries already solved (the reference's
+// wrap-around correction, +2^64 mod p, when NOWRAP is false; with p < 2^28
+// the sums cannot wrap).  Step k: the owner of k reduces its sum and
+// finishes x[k], one shuffle hands x[k] to the quad, and every thread adds
+// T[j][k] x[k] into the sums of its entries j still to solve -- sixteen
+// independent multiply-adds, so the sequential chain per step is one
+// reduction, one shuffle and one multiply-add.  The entries of the current
+// group of four (k / 4) sit in slot CUR: after each group the registers
+// rotate by one, so no step needs a dynamic register index, and after the
+// sixteen groups they are back in place.  Entries from nb on are zero and
+// never solved.
 template <bool UPPER, bool NOWRAP>
 __device__ __forceinline__ void tri_quad_solve(const uint32_t (*sT)[TRI_NB + 1],
                                                const uint32_t *sD, bool unitd, int nb, int q,
                                                uint32_t (&x)[TRI_NB / 4], const Modulus &mod,
                                                uint32_t two64) {
+  constexpr int NI = TRI_NB / 4;
+  constexpr int CUR = UPPER ? NI - 1 : 0;  // slot s holds group (g + s - CUR) mod NI
   const uint32_t p = (uint32_t)mod.p;
+  const int qbase = (threadIdx.x & 31) & ~3;
+  const int last = (nb - 1) >> 2;  // last group with an entry
+  uint64_t acc[NI];
+#pragma unroll
+  for (int i = 0; i < NI; ++i) acc[i] = 0ull;
 #pragma unroll 1
-  for (int kk = 0; kk < nb; ++kk) {
-    const int k = UPPER ? nb - 1 - kk : kk;
-    uint64_t s = 0;
+  for (int gg = 0; gg < NI; ++gg) {
+    const int g = UPPER ? NI - 1 - gg : gg;
+    if (g <= last) {
 #pragma unroll
-    for (int i = 0; i < TRI_NB / 4; ++i) {
-      const int j = 4 * i + q;
-      const uint64_t t = (UPPER ? j > k : j < k) ? (uint64_t)sT[k][j] * x[i] : 0ull;
-      s += t;
-      if (!NOWRAP && s < t) s += two64;
+      for (int rr = 0; rr < 4; ++rr) {
+        const int r = UPPER ? 3 - rr : rr;
+        const int k = 4 * g + r;
+        if (k < nb) {
+          // every lane forms its candidate; the owner's (q == r) is x[k]
+          const uint32_t red = mod_reduce(acc[CUR], mod);
+          uint32_t v = x[CUR] >= red ? x[CUR] - red : x[CUR] + (p - red);
+          if (!unitd) v = mod_mul(v, sD[k], mod);
+          if (q == r) x[CUR] = v;
+          v = __shfl_sync(0xffffffffu, v, qbase + r);
+#pragma unroll
+          for (int sl = 0; sl < NI; ++sl) {
+            const int j = 4 * ((g + sl - CUR) & (NI - 1)) + q;
+            if (UPPER ? j < k : j > k) {
+              const uint64_t t = (uint64_t)sT[j][k] * v;
+              acc[sl] += t;
+              if (!NOWRAP && acc[sl] < t) acc[sl] += two64;
+            }
+          }
+        }
+      }
     }
-    if (!NOWRAP) s = mod_reduce(s, mod);  // partial sums below 2^32, their sum below 2^34
-    s += __shfl_xor_sync(0xffffffffu, s, 1);
-    s += __shfl_xor_sync(0xffffffffu, s, 2);
-    const uint32_t r = mod_reduce(s, mod);
-    const int ik = k >> 2;
-    uint32_t xk = 0u;
+    // the next group into slot CUR
+    if (UPPER) {
+      const uint32_t xe = x[NI - 1];
+      const uint64_t ae = acc[NI - 1];
 #pragma unroll
-    for (int i = 0; i < TRI_NB / 4; ++i) xk = (i == ik) ? x[i] : xk;
-    uint32_t v = xk >= r ? xk - r : xk + (p - r);
-    if (!unitd) v = mod_mul(v, sD[k], mod);
-    if ((k & 3) == q) {
+      for (int sl = NI - 1; sl > 0; --sl) {
+        x[sl] = x[sl - 1];
+        acc[sl] = acc[sl - 1];
+      }
+      x[0] = xe;
+      acc[0] = ae;
+    } else {
+      const uint32_t xe = x[0];
+      const uint64_t ae = acc[0];
 #pragma unroll
-      for (int i = 0; i < TRI_NB / 4; ++i)
-        if (i == ik) x[i] = v;
+      for (int sl = 0; sl < NI - 1; ++sl) {
+        x[sl] = x[sl + 1];
+        acc[sl] = acc[sl + 1];
+      }
+      x[NI - 1] = xe;
+      acc[NI - 1] = ae;
     }
   }
 }
