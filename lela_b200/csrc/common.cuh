@@ -307,6 +307,4 @@ __device__ __forceinline__ void tmem_ld_wait() {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-__device__ __forceinline__ bool elect_lane0() { return (threadIdx.x & 31) == 0; }
-
 }  // namespace lela

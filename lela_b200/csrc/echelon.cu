@@ -80,10 +80,6 @@ struct PanelOut {
   uint32_t tq[EW];
 };
 
-__device__ __forceinline__ uint32_t sub_mod(uint32_t a, uint32_t b, uint32_t p) {
-  return a >= b ? a - b : a + (p - b);
-}
-
 // Exact inverse of a unit x modulo p (any p < 2^32): extended Euclid on
 // unsigned remainders with 64-bit signed coefficients.  0 when gcd != 1.
 __device__ __forceinline__ uint32_t inv_exact_u32(uint32_t p, uint32_t x) {
@@ -159,14 +155,6 @@ struct ArithWide {
     return mod_dot2(a, b, c, d, mod, two64);
   }
 };
-
-// Delayed-reduction accumulator: 64-bit sum of u32 products, 2^64 mod p
-// added back whenever the sum wraps (the reference's ZpModule dot,
-// lela/blas/level1-modular.tcc:135-181).
-__device__ __forceinline__ void acc_add(uint64_t &s, uint64_t prod, uint32_t two64) {
-  s += prod;
-  if (s < prod) s += two64;
-}
 
 // 1. First nonzero column of each row's panel part, rows i0..m-1 (one warp
 // per row); the histogram of these heads (hist[0..64], which the caller
