@@ -46,6 +46,8 @@ def lib():
         L.oracle_gemm_zp_u32_threads.argtypes = [_I, _U, _S, _S, _S, _U, _P, _S, _P, _S, _U, _P, _S]
         L.oracle_trsm_zp_u32.argtypes = [_U, _I, _I, _S, _S, _U, _P, _S, _P, _S, ctypes.POINTER(_S)]
         L.oracle_echelon_zp_u32.argtypes = [_U, _S, _S, _P, _S, ctypes.POINTER(_S), ctypes.POINTER(_U)]
+        L.oracle_echelon_reduced_zp_u32.argtypes = [_U, _S, _S, _P, _S, ctypes.POINTER(_S),
+                                                    ctypes.POINTER(_U)]
         L.oracle_fl_echelonize_zp_u32.argtypes = [_U, _S, _S, _P, _P, _P, _I, _I, _P, _S,
                                                   ctypes.POINTER(_S), ctypes.POINTER(_U),
                                                   ctypes.POINTER(_S), ctypes.POINTER(_S)]
@@ -75,6 +77,8 @@ def ref():
         L.lela_ref_trsm_zp_u32.argtypes = [_U, _I, _I, _S, _S, _U, _P, _S, _P, _S, ctypes.POINTER(_S)]
         L.lela_ref_trsm_zp_u32_threads.argtypes = [_I, _U, _I, _I, _S, _S, _U, _P, _S, _P, _S]
         L.lela_ref_echelon_zp_u32.argtypes = [_U, _S, _S, _P, _S, ctypes.POINTER(_S), ctypes.POINTER(_U)]
+        L.lela_ref_echelon_reduced_zp_u32.argtypes = [_U, _S, _S, _P, _S, ctypes.POINTER(_S),
+                                                      ctypes.POINTER(_U)]
         L.lela_ref_elim_echelon_zp_u32.argtypes = [_U, _S, _S, _P, _S, ctypes.POINTER(_S), ctypes.POINTER(_U)]
         L.lela_ref_fl_echelonize_zp_u32.argtypes = [_U, _S, _S, _P, _P, _P, _I, _I, _P, _S,
                                                     ctypes.POINTER(_S), ctypes.POINTER(_U), ctypes.POINTER(_S)]
@@ -114,6 +118,16 @@ def echelon_zp(p, A):
     m, n = A.shape
     r = _S(0); d = _U(0)
     rc = lib().oracle_echelon_zp_u32(p, m, n, _ptr(A), n, ctypes.byref(r), ctypes.byref(d))
+    if rc:
+        raise ArithmeticError("pivot not invertible")
+    return A, r.value, d.value
+
+
+def echelon_reduced_zp(p, A):
+    A = _c(A, np.uint32).copy()
+    m, n = A.shape
+    r = _S(0); d = _U(0)
+    rc = lib().oracle_echelon_reduced_zp_u32(p, m, n, _ptr(A), n, ctypes.byref(r), ctypes.byref(d))
     if rc:
         raise ArithmeticError("pivot not invertible")
     return A, r.value, d.value
@@ -180,6 +194,15 @@ def ref_echelon_zp(p, A, classical=False):
     r = _S(0); d = _U(0)
     fn = ref().lela_ref_elim_echelon_zp_u32 if classical else ref().lela_ref_echelon_zp_u32
     if fn(p, m, n, _ptr(A), n, ctypes.byref(r), ctypes.byref(d)):
+        raise ArithmeticError("pivot not invertible")
+    return A, r.value, d.value
+
+
+def ref_echelon_reduced_zp(p, A):
+    A = _c(A, np.uint32).copy()
+    m, n = A.shape
+    r = _S(0); d = _U(0)
+    if ref().lela_ref_echelon_reduced_zp_u32(p, m, n, _ptr(A), n, ctypes.byref(r), ctypes.byref(d)):
         raise ArithmeticError("pivot not invertible")
     return A, r.value, d.value
 

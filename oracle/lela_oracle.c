@@ -254,6 +254,49 @@ int oracle_echelon_zp_u32 (uint32_t p, size_t m, size_t n, uint32_t *A, size_t l
 	return 0;
 }
 
+/* Reduced row-echelon form, GaussJordan::echelonize_reduced (lela/
+ * algorithms/gauss-jordan.tcc:434-466) through GaussJordanTransform
+ * (:27-230), as EchelonForm::echelonize (A, true) runs it on a dense
+ * matrix.  The recursion takes the columns left to right; in each it picks
+ * the first nonzero at or below the current row of the column as reduced
+ * by the earlier pivot rows -- the pivot rows and pivot values of the
+ * non-reduced form above -- and clears the column in every other row by
+ * adding multiples of the pivot row, whose entry keeps its value (:74-107:
+ * a_ii is set back, the transform's diagonal stays one).  So every pivot
+ * row of the result is its non-reduced row plus multiples of the later
+ * pivot rows, zero in their pivot columns, which determines it.  Restated
+ * as the non-reduced form followed by clearing upwards, the bottom pivot
+ * row first: R_j <- R_j - (R_j[c_i] / x_i) R_i for j < i. */
+int oracle_echelon_reduced_zp_u32 (uint32_t p, size_t m, size_t n, uint32_t *A, size_t lda,
+				   size_t *rank, uint32_t *det)
+{
+	int rc = oracle_echelon_zp_u32 (p, m, n, A, lda, rank, det);
+	if (rc)
+		return rc;
+	size_t r = *rank;
+	size_t *pc = (size_t *) malloc ((r ? r : 1) * sizeof (size_t));
+	for (size_t i = 0; i < r; ++i) {
+		size_t c = 0;
+		while (A[i * lda + c] == 0)
+			++c;
+		pc[i] = c;
+	}
+	for (size_t i = r; i-- > 0;) {
+		/* every pivot was inverted by the form above */
+		uint32_t negxinv = (p - oracle_inv_zp (p, A[i * lda + pc[i]])) % p;
+		for (size_t j = 0; j < i; ++j) {
+			uint32_t a = A[j * lda + pc[i]];
+			if (a == 0)
+				continue;
+			uint32_t f = mulmod (p, a, negxinv);
+			for (size_t c = pc[i]; c < n; ++c)
+				A[j * lda + c] = axpy_mod (p, A[j * lda + c], f, A[i * lda + c]);
+		}
+	}
+	free (pc);
+	return 0;
+}
+
 /* Faugere-Lachartre (lela/algorithms/faugere-lachartre.tcc:735-917).
  *
  * setup_splicer (:47-146) walks the rows: the head of a sparse row is its

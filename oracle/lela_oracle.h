@@ -43,6 +43,12 @@ int oracle_trsm_zp_u32 (uint32_t p, int upper, int diag_is_one, size_t m, size_t
 int oracle_echelon_zp_u32 (uint32_t p, size_t m, size_t n, uint32_t *A, size_t lda,
 			   size_t *rank, uint32_t *det);
 
+/* Reduced row echelon form in place (pivots keep their values; zeros above
+ * and below them); rank and det as above.  Returns 0, or -1 when a pivot is
+ * not invertible mod p. */
+int oracle_echelon_reduced_zp_u32 (uint32_t p, size_t m, size_t n, uint32_t *A, size_t lda,
+				   size_t *rank, uint32_t *det);
+
 /* Faugere-Lachartre echelon form of a CSR matrix.  R is dense m x n (ldr).
  * Returns 0; 1 with *bad_row on a malformed input (WrongMatrixForm);
  * 2 when the pivot block is singular (the reference returns early). */

@@ -247,6 +247,41 @@ int lela_ref_echelon_zp_u32 (uint32_t p, size_t m, size_t n, uint32_t *A, size_t
 	return 0;
 }
 
+/* Dense reduced row-echelon form as EchelonForm::echelonize (A, true) does
+ * it for a DenseMatrix (lela/solutions/echelon-form.h:115-123): L sized
+ * m x m, then GaussJordan::echelonize_reduced (lela/algorithms/
+ * gauss-jordan.tcc:434-466), whose transform GaussJordanTransform
+ * (:27-230) leaves every pivot at its value (no normalisation).  Rank and
+ * det (product of the pivots, taken from the leading entries as above). */
+int lela_ref_echelon_reduced_zp_u32 (uint32_t p, size_t m, size_t n, uint32_t *A, size_t lda, size_t *rank, uint32_t *det)
+{
+	Zp F (p);
+	Context<Zp> ctx (F);
+	DenseMatrix<uint32> MA (m, n);
+	if (m && n) load_dense (MA, A, lda);
+	GaussJordan<Zp> GJ (ctx);
+	GaussJordan<Zp>::Permutation P;
+	DenseMatrix<uint32> L (m, m);
+	size_t r = 0;
+	Zp::Element d;
+	try {
+		GJ.echelonize_reduced (MA, L, P, r, d);
+	} catch (...) {
+		return -1;
+	}
+	if (m && n) store_dense (MA, A, lda);
+	*rank = r;
+	Zp::Element pd = 1;
+	for (size_t i = 0; i < r; ++i) {
+		size_t c = 0;
+		while (c < n && MA[i][c] == 0) ++c;
+		if (c < n) F.mulin (pd, MA[i][c]);
+	}
+	*det = pd;
+	(void) d;
+	return 0;
+}
+
 /* Classical elimination Elimination::echelonize (lela/algorithms/
  * elimination.tcc:47-139), the reference's own cross-check for the
  * recursive GaussJordan result. */

@@ -4,8 +4,9 @@
 
 Needs oracle/_ref/liblela_ref.so (built by `make -C oracle ref` from the
 reference sources).  Inputs come from lela_b200.gen (seeded); outputs are
-what LELA itself computes: BLAS3::gemm, BLAS3::trsm, the dense echelon form
-of EchelonForm (GaussJordan + move_L), FaugereLachartre::echelonize in all
+what LELA itself computes: BLAS3::gemm, BLAS3::trsm, the dense echelon forms
+of EchelonForm (GaussJordan + move_L; reduced: GaussJordan::
+echelonize_reduced), FaugereLachartre::echelonize in all
 four modes, and the GF(2) gemm / echelon form.  Small cases store inputs
 and outputs; the larger ones store SHA-256 digests of inputs and outputs.
 """
@@ -110,6 +111,27 @@ def main():
         out.update({pre + "A": A, pre + "E": E, pre + "meta": np.array([p, st, r, d], dtype=np.uint64)})
         cases.append(pre)
     manifest["echelon"] = cases
+
+    # ---- dense reduced echelon form (EchelonForm::echelonize (A, true):
+    #      GaussJordan::echelonize_reduced)
+    cases = []
+    for i, (p, m, nn) in enumerate([(65521, 30, 40), (65521, 50, 30), (251, 40, 40), (2, 24, 70),
+                                    (65536, 12, 12), (2147483647, 33, 57), (4294967291, 20, 25),
+                                    (65521, 70, 9)]):
+        A = gen.dense_zp(600 + i, m, nn, p)
+        A[:, 3 % nn] = 0
+        if m > 20:
+            A[m - 8:] = (A[:8] * 3) % p     # rank deficiency
+        A[2] = 0                            # zero row
+        try:
+            E, r, d = oracle.ref_echelon_reduced_zp(p, A)
+            st = 0
+        except ArithmeticError:     # LELA cannot invert a pivot
+            E, r, d, st = A, 0, 0, 1
+        pre = "rech%d_" % i
+        out.update({pre + "A": A, pre + "E": E, pre + "meta": np.array([p, st, r, d], dtype=np.uint64)})
+        cases.append(pre)
+    manifest["echelon_reduced"] = cases
 
     # ---- Faugere-Lachartre, the reference test's matrix family and an
     #      F4-shaped matrix

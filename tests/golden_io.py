@@ -42,6 +42,13 @@ def echelon_cases():
         yield pre, p, st, r, d, z[pre + "A"], z[pre + "E"]
 
 
+def echelon_reduced_cases():
+    z, man = data()
+    for pre in man["echelon_reduced"]:
+        p, st, r, d = (int(x) for x in z[pre + "meta"])
+        yield pre, p, st, r, d, z[pre + "A"], z[pre + "E"]
+
+
 def fl_cases(with_inputs_only=True):
     """Faugere-Lachartre cases whose inputs are stored (the reference test's
     matrix family)."""

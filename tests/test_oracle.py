@@ -49,6 +49,17 @@ def test_golden_echelon():
         assert np.array_equal(got, E), pre
 
 
+def test_golden_echelon_reduced():
+    for pre, p, st, r, d, A, E in golden_io.echelon_reduced_cases():
+        if st:
+            with pytest.raises(ArithmeticError):
+                oracle.echelon_reduced_zp(p, A)
+            continue
+        got, gr, gd = oracle.echelon_reduced_zp(p, A)
+        assert (gr, gd) == (r, d), pre
+        assert np.array_equal(got, E), pre
+
+
 def test_golden_fl():
     for (pre, p, m, n, red, od, st, rank, det, rowptr, colidx, vals, R) in golden_io.fl_cases():
         got = oracle.fl_echelonize_zp(p, m, n, rowptr, colidx, vals, red, od)
@@ -167,6 +178,38 @@ def test_live_echelon(seed):
     e3, r3, d3 = oracle.ref_echelon_zp(p, A, classical=True)
     assert np.array_equal(e1, e2) and np.array_equal(e1, e3)
     assert (r1, d1) == (r2, d2) == (r3, d3)
+
+
+@need_ref
+@pytest.mark.parametrize("p", [2, 3, 251, 65521, 65536, 2147483647, 4294967291])
+def test_live_echelon_reduced(p):
+    """GaussJordan::echelonize_reduced against the restatement: full rank,
+    rank deficient (a product of thin factors), zero columns and rows, tall
+    and wide, and LELA's pivot-inversion failures (composite p, p >= 2^31)."""
+    rng = np.random.default_rng(p % 1000)
+    for (m, n) in ((1, 1), (7, 13), (13, 7), (40, 40), (64, 100), (100, 64)):
+        for kind in range(4):
+            A = gen.dense_zp(int(rng.integers(1 << 30)), m, n, p)
+            if kind == 1:
+                A[:, ::3] = 0
+            elif kind == 2:
+                r = max(1, min(m, n) // 3)
+                F = gen.dense_zp(1, m, r, p).astype(object) @ gen.dense_zp(2, r, n, p).astype(object)
+                A = (F % p).astype(np.uint32)
+            elif kind == 3:
+                A[m // 2:] = 0
+                A[:, :n // 2] = 0
+            try:
+                want = oracle.ref_echelon_reduced_zp(p, A)
+            except ArithmeticError:
+                want = None
+            try:
+                got = oracle.echelon_reduced_zp(p, A)
+            except ArithmeticError:
+                got = None
+            assert (want is None) == (got is None), (m, n, kind)
+            if want is not None:
+                assert np.array_equal(got[0], want[0]) and got[1:] == want[1:], (m, n, kind)
 
 
 @need_ref
