@@ -921,22 +921,24 @@ int lela_cuda_fl_echelonize_zp_u32_batch(lela_cuda_ctx *h, size_t count, const s
   return ST_OK;
 }
 
-int lela_cuda_echelon_zp_u32_dev(lela_cuda_ctx *h, size_t m, size_t n, uint32_t p, uint32_t *A,
-                                 size_t lda, size_t *rank, uint32_t *det) {
+// The dense echelon entry points: device (dev) or host pointers, the
+// non-reduced form or the reduced one.
+static int echelon_entry(lela_cuda_ctx *h, size_t m, size_t n, uint32_t p, uint32_t *A,
+                         size_t lda, size_t *rank, uint32_t *det, bool dev, bool reduced) {
   if (!h || !rank || !det) return ST_ARG;
   Ctx *c = &h->c;
+  const char *what = reduced ? "echelon_reduced_zp_u32" : "echelon_zp_u32";
   if (m > (size_t)INT32_MAX || n > (size_t)INT32_MAX) return ctx_fail(c, ST_ARG, "dimension too large");
-  if (m && n && !A) return ctx_fail(c, ST_ARG, "null pointer");
-  int st = zp_echelon_dev(c, (int)m, (int)n, p, A, lda, rank, det, nullptr);
-  if (!st) st = ctx_check_status(c, "echelon_zp_u32");
-  return st;
-}
-
-int lela_cuda_echelon_zp_u32(lela_cuda_ctx *h, size_t m, size_t n, uint32_t p, uint32_t *A,
-                             size_t lda, size_t *rank, uint32_t *det) {
-  if (!h || !rank || !det) return ST_ARG;
-  Ctx *c = &h->c;
-  if (m > (size_t)INT32_MAX || n > (size_t)INT32_MAX) return ctx_fail(c, ST_ARG, "dimension too large");
+  auto run = [&](uint32_t *D, size_t ld) {
+    return reduced ? zp_echelon_reduced_dev(c, (int)m, (int)n, p, D, ld, rank, det)
+                   : zp_echelon_dev(c, (int)m, (int)n, p, D, ld, rank, det, nullptr);
+  };
+  if (dev) {
+    if (m && n && !A) return ctx_fail(c, ST_ARG, "null pointer");
+    int st = run(A, lda);
+    if (!st) st = ctx_check_status(c, what);
+    return st;
+  }
   if (p < 2) return ctx_fail(c, ST_ARG, "modulus must be at least 2");
   if (m == 0 || n == 0) {
     *rank = 0;
@@ -950,10 +952,30 @@ int lela_cuda_echelon_zp_u32(lela_cuda_ctx *h, size_t m, size_t n, uint32_t p, u
   int st = ctx_stage(c, 0, m * n * 4, &dA);
   if (!st) st = ctx_clear_status(c);
   if (!st) st = h2d_matrix(c, dA, A, m, n, lda, 4);
-  if (!st) st = zp_echelon_dev(c, (int)m, (int)n, p, (uint32_t *)dA, n, rank, det, nullptr);
+  if (!st) st = run((uint32_t *)dA, n);
   if (!st) st = d2h_matrix(c, A, dA, m, n, lda, 4);
-  if (!st) st = ctx_check_status(c, "echelon_zp_u32");
+  if (!st) st = ctx_check_status(c, what);
   return st;
+}
+
+int lela_cuda_echelon_zp_u32_dev(lela_cuda_ctx *h, size_t m, size_t n, uint32_t p, uint32_t *A,
+                                 size_t lda, size_t *rank, uint32_t *det) {
+  return echelon_entry(h, m, n, p, A, lda, rank, det, true, false);
+}
+
+int lela_cuda_echelon_zp_u32(lela_cuda_ctx *h, size_t m, size_t n, uint32_t p, uint32_t *A,
+                             size_t lda, size_t *rank, uint32_t *det) {
+  return echelon_entry(h, m, n, p, A, lda, rank, det, false, false);
+}
+
+int lela_cuda_echelon_reduced_zp_u32_dev(lela_cuda_ctx *h, size_t m, size_t n, uint32_t p,
+                                         uint32_t *A, size_t lda, size_t *rank, uint32_t *det) {
+  return echelon_entry(h, m, n, p, A, lda, rank, det, true, true);
+}
+
+int lela_cuda_echelon_reduced_zp_u32(lela_cuda_ctx *h, size_t m, size_t n, uint32_t p,
+                                     uint32_t *A, size_t lda, size_t *rank, uint32_t *det) {
+  return echelon_entry(h, m, n, p, A, lda, rank, det, false, true);
 }
 
 int lela_cuda_trsm_csr_upper_zp_u32(lela_cuda_ctx *h, size_t n, size_t ncols, uint32_t p,

@@ -133,7 +133,8 @@ enum BufSlot : int {
   BUF_TRI_W = 18,     // inverted 512-row diagonal blocks (trsm)
   BUF_TRI_T = 19,     // their assembly temporaries
   BUF_TRI_A = 20,     // dense copy of a sparse triangular operand
-  BUF_COUNT = 21,
+  BUF_RED = 21,       // reduced echelon form: column maps, pivot block, solved columns
+  BUF_COUNT = 22,
 };
 
 // Grow-only allocation helpers; return ST_OK or ST_NOMEM.

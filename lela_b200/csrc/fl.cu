@@ -373,4 +373,93 @@ int zp_fl_echelonize_dev(Ctx *c, int m, int n, uint32_t p, const uint64_t *d_row
   return e == cudaSuccess ? ST_OK : ctx_cuda(c, e, "fl launch");
 }
 
+// ------------------------------------------------ reduced dense echelon form
+//
+// GaussJordan::echelonize_reduced (lela/algorithms/gauss-jordan.tcc:
+// 434-466), as EchelonForm::echelonize (A, true) runs it on a DenseMatrix
+// (lela/solutions/echelon-form.h:115-123).  Its recursion GaussJordanTransform
+// (:27-230) picks the pivots by the rule of the non-reduced form (the first
+// nonzero at or below the current row of the column reduced by the earlier
+// pivot rows) and clears each pivot column in every other row by adding
+// multiples of the pivot row, which keeps its pivot value x_i.  So pivot
+// row i of the result is the non-reduced row U_i plus multiples of the
+// later pivot rows, zero in their pivot columns: R = X U_P^-1 U, with U_P
+// the pivot columns of U (upper triangular, diagonal x_i) and X =
+// diag(x_i).  Here: the non-reduced form on the panels, then U_P and the
+// other columns U_N gathered, U_N <- U_P^-1 U_N (the triangular solve), and
+// one kernel writes row i back as x_i U_N[i] in the other columns, x_i at
+// its pivot column and zero at the other pivot columns.  Rows from the rank
+// on are zero already.
+
+// Rows 0..r-1 of D from the solved columns: colmap[c] >= 0 is c's column in
+// X, colmap[c] = -1 - j marks the pivot column of row j; the pivot values
+// are the diagonal of UP.
+__global__ void reduced_assemble_kernel(uint32_t *__restrict__ D, size_t ld, int r, int n,
+                                        const int *__restrict__ colmap,
+                                        const uint32_t *__restrict__ X, size_t ldx,
+                                        const uint32_t *__restrict__ UP, size_t ldp, Modulus mod) {
+  const size_t total = (size_t)r * n;
+  for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(idx / n), col = (int)(idx % n);
+    const int cm = colmap[col];
+    const uint32_t x = UP[(size_t)i * ldp + i];
+    D[(size_t)i * ld + col] =
+        cm >= 0 ? mod_mul(X[(size_t)i * ldx + cm], x, mod) : (-1 - cm == i ? x : 0u);
+  }
+}
+
+int zp_echelon_reduced_dev(Ctx *c, int m, int n, uint32_t p, uint32_t *D, size_t ld,
+                           size_t *rank, uint32_t *det) {
+  std::vector<int> piv;
+  int st = zp_echelon_dev(c, m, n, p, D, ld, rank, det, &piv);
+  if (st) return st;
+  const int r = (int)*rank;
+  if (r == 0) return ST_OK;
+  if ((int)piv.size() != r) return ctx_fail(c, ST_CUDA, "reduced echelon: pivot columns missing");
+  const int nrem = n - r;
+  std::vector<int> colmap(n, 0), cols(piv);
+  for (int j = 0; j < r; ++j) colmap[piv[j]] = -1 - j;
+  for (int col = 0, k = 0; col < n; ++col)
+    if (colmap[col] >= 0) {
+      colmap[col] = k++;
+      cols.push_back(col);
+    }
+  const size_t ibytes = ((size_t)2 * n * sizeof(int) + 255) & ~(size_t)255;
+  const size_t pbytes = (((size_t)r * r * 4) + 255) & ~(size_t)255;
+  void *vb = nullptr;
+  if ((st = ctx_buffer(c, BUF_RED, ibytes + pbytes + (size_t)r * std::max(nrem, 1) * 4, &vb)))
+    return st;
+  int *d_map = static_cast<int *>(vb), *d_cols = d_map + n;
+  uint32_t *UP = reinterpret_cast<uint32_t *>(static_cast<uint8_t *>(vb) + ibytes);
+  uint32_t *X = reinterpret_cast<uint32_t *>(static_cast<uint8_t *>(vb) + ibytes + pbytes);
+  cudaError_t e = cudaMemcpyAsync(d_map, colmap.data(), (size_t)n * sizeof(int),
+                                  cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(d_cols, cols.data(), (size_t)n * sizeof(int), cudaMemcpyHostToDevice,
+                        c->stream);
+  if (e != cudaSuccess) return ctx_cuda(c, e, "reduced echelon: columns");
+  auto gather = [&](const int *sel, int ncols, uint32_t *out, size_t ldo) {
+    const size_t total = (size_t)r * ncols;
+    const int grid = (int)std::min<size_t>((total + 255) / 256, (size_t)c->num_sms * 16);
+    gather_cols_kernel<<<grid, 256, 0, c->stream>>>(D, ld, r, sel, ncols, out, ldo);
+    ctx_launched(c);
+  };
+  gather(d_cols, r, UP, (size_t)r);
+  if (nrem > 0) {
+    gather(d_cols + r, nrem, X, (size_t)nrem);
+    size_t bad = 0;
+    if ((st = zp_trsm_dev(c, true, false, r, nrem, p, 1, UP, (size_t)r, X, (size_t)nrem, &bad)))
+      return st;
+  }
+  const size_t total = (size_t)r * n;
+  const int grid = (int)std::min<size_t>((total + 255) / 256, (size_t)c->num_sms * 16);
+  reduced_assemble_kernel<<<grid, 256, 0, c->stream>>>(D, ld, r, n, d_map, X,
+                                                       (size_t)std::max(nrem, 1), UP, (size_t)r,
+                                                       make_modulus(p));
+  ctx_launched(c);
+  e = cudaGetLastError();
+  return e == cudaSuccess ? ST_OK : ctx_cuda(c, e, "reduced echelon: assembly");
+}
+
 }  // namespace lela

@@ -98,3 +98,63 @@ def test_echelon_blocks_far_pivots(cuda, p):
     got, gr, gd = cuda.echelonize(p, A.copy())
     assert (gr, gd) == (wr, wd)
     assert np.array_equal(got, want)
+
+
+# ------------------------------------------------------------ reduced form
+# EchelonForm::echelonize (A, true) on a DenseMatrix: GaussJordan::
+# echelonize_reduced (lela/algorithms/gauss-jordan.tcc:434-466).
+
+@pytest.mark.gpu
+def test_echelon_reduced_golden(cuda):
+    for pre, p, st, r, d, A, E in golden_io.echelon_reduced_cases():
+        if st:
+            with pytest.raises(LELAError):
+                cuda.echelonize(p, A.copy(), reduced=True)
+            continue
+        got, gr, gd = cuda.echelonize(p, A.copy(), reduced=True)
+        assert (gr, gd) == (r, d), pre
+        assert np.array_equal(got, E), pre
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("p", [2, 3, 251, 65521, 2147483647])
+def test_echelon_reduced_against_oracle(cuda, p):
+    for seed, (m, n) in enumerate([(1, 1), (5, 9), (9, 5), (64, 64), (65, 130), (200, 90),
+                                   (150, 400), (333, 333)]):
+        for kind in ("dense", "structured"):
+            A = gen.dense_zp(seed, m, n, p) if kind == "dense" else _structured(seed, m, n, p)
+            want, wr, wd = oracle.echelon_reduced_zp(p, A)
+            got, gr, gd = cuda.echelonize(p, A.copy(), reduced=True)
+            assert (gr, gd) == (wr, wd), (p, m, n, kind)
+            assert np.array_equal(got, want), (p, m, n, kind)
+
+
+@pytest.mark.gpu
+def test_echelon_reduced_large(cuda):
+    """1400 x 1600, rank about 1090: the pivot block is solved through the
+    inverted 512-row diagonal blocks on the tensor cores."""
+    p = 65521
+    A = _structured(78, 1400, 1600, p)
+    want, wr, wd = oracle.echelon_reduced_zp(p, A)
+    assert wr >= 1024
+    got, gr, gd = cuda.echelonize(p, A.copy(), reduced=True)
+    assert (gr, gd) == (wr, wd)
+    assert np.array_equal(got, want)
+
+
+@pytest.mark.gpu
+def test_echelon_reduced_device(cuda):
+    """The _dev entry point on a torch CUDA view with a row stride."""
+    import torch
+    p = 251
+    A = _structured(79, 120, 170, p)
+    want, wr, wd = oracle.echelon_reduced_zp(p, A)
+    big = torch.zeros((120, 200), dtype=torch.int32, device="cuda")
+    big[:, 10:180] = torch.from_numpy(A.view(np.int32)).cuda()
+    view = big[:, 10:180]
+    _, gr, gd = cuda.echelonize(p, view, reduced=True)
+    cuda.synchronize()
+    host = big.cpu().numpy().view(np.uint32)
+    assert (gr, gd) == (wr, wd)
+    assert np.array_equal(host[:, 10:180], want)
+    assert not host[:, :10].any() and not host[:, 180:].any()
