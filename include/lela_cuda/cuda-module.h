@@ -10,8 +10,9 @@
  * diagIsOne) on DenseMatrix<uint32> operands run on the GPU through the C
  * ABI of include/lela_cuda.h, and FaugereLachartre<Modular<uint32>,
  * CUDAModule<uint32> >::echelonize runs the whole Faugere-Lachartre pipeline
- * there; BLAS3::trsm also takes a sparse upper-triangular SparseMatrix<uint32>
- * A.  With Context<GF2, CUDAModuleGF2>, BLAS3::gemm on DenseMatrix<bool>
+ * there, as does EchelonForm<Modular<uint32>, CUDAModule<uint32> >::echelonize
+ * for the dense echelon forms, reduced or not; BLAS3::trsm also takes a
+ * sparse upper-triangular SparseMatrix<uint32> A.  With Context<GF2, CUDAModuleGF2>, BLAS3::gemm on DenseMatrix<bool>
  * operands runs on the GPU.  Operand combinations the GPU path does not take
  * (sparse gemm operands, sparse lower-triangular or transposed operands) fall
  * through to the parent module, exactly as an unimplemented operation falls
@@ -32,6 +33,7 @@
 #define LELA_CUDA_CUDA_MODULE_H
 
 #include <cstdlib>
+#include <map>
 #include <vector>
 
 #include "lela/blas/context.h"
@@ -42,6 +44,9 @@
 #include "lela/ring/gf2.h"
 #include "lela/util/error.h"
 #include "lela/algorithms/faugere-lachartre.h"
+#include "lela/algorithms/elimination.h"
+#include "lela/algorithms/gauss-jordan.h"
+#include "lela/solutions/echelon-form.h"
 
 #include "../lela_cuda.h"
 
@@ -368,6 +373,117 @@ public:
 				if (dense[i * n + j])
 					r->push_back (typename Matrix::Row::value_type (j, dense[i * n + j]));
 		}
+	}
+};
+
+/** EchelonForm over Modular<uint32> with the CUDA module: the interface and
+ * the per-method control flow of lela/solutions/echelon-form.h:29-163.
+ * Dense matrices go to the GPU where the reference's method gives the
+ * GPU's result: the asymptotically fast Gauss-Jordan (the default for a
+ * DenseMatrix), reduced or not, and the standard method's non-reduced form
+ * (the same matrix, tests/test-gauss-jordan.C:91-99).  The Faugere-Lachartre
+ * method runs the GPU pipeline on a sparse copy of the rows.  The standard
+ * method's reduced form and every other matrix type take the reference's
+ * Elimination on this context, as in the reference. */
+template <>
+class EchelonForm<Modular<uint32>, CUDAModule<uint32> >
+{
+	typedef Modular<uint32> Ring;
+	typedef CUDAModule<uint32> Modules;
+
+	Context<Ring, Modules> _ctx;
+	Elimination<Ring, Modules> _elim;
+	DenseMatrix<uint32> L;
+	GaussJordan<Ring, Modules>::Permutation P;
+	std::map<const void *, size_t> _rank_table;
+
+	void gpu (DenseMatrix<uint32> &A, bool reduced, size_t &rank)
+	{
+		size_t m = A.rowdim (), n = A.coldim ();
+		uint32_t d = 1;
+		rank = 0;
+		if (m == 0 || n == 0)
+			return;
+		int st = (reduced ? lela_cuda_echelon_reduced_zp_u32 : lela_cuda_echelon_zp_u32)
+			(_ctx.M.cuda.get (), m, n, _ctx.F._modulus, &A[0][0], A.disp (), &rank, &d);
+		lela_cuda_check (_ctx.M.cuda.get (), st);
+	}
+
+public:
+	enum Method { METHOD_UNKNOWN, METHOD_STANDARD_GJ, METHOD_ASYMPTOTICALLY_FAST_GJ, METHOD_FAUGERE_LACHARTRE };
+
+	EchelonForm (Context<Ring, Modules> &ctx) : _ctx (ctx), _elim (ctx) {}
+
+	template <class Matrix>
+	Matrix &echelonize (Matrix &A, bool reduced = false, Method method = METHOD_STANDARD_GJ)
+	{
+		size_t rank = 0;
+		uint32 d;
+		switch (method) {
+		case METHOD_STANDARD_GJ:
+			if (reduced)
+				_elim.echelonize_reduced (A, L, P, rank, d, false);
+			else
+				_elim.echelonize (A, P, rank, d, false);
+			break;
+		case METHOD_FAUGERE_LACHARTRE:
+			{
+				FaugereLachartre<Ring, Modules> FL (_ctx);
+				FL.echelonize (A, A, rank, d, reduced);
+			}
+			break;
+		default:
+			throw LELAError ("Invalid method for choice of matrix");
+		}
+		_rank_table[&A] = rank;
+		return A;
+	}
+
+	DenseMatrix<uint32> &echelonize (DenseMatrix<uint32> &A, bool reduced = false, Method method = METHOD_ASYMPTOTICALLY_FAST_GJ)
+	{
+		size_t rank = 0;
+		uint32 d;
+		switch (method) {
+		case METHOD_STANDARD_GJ:
+			if (reduced)
+				_elim.echelonize_reduced (A, L, P, rank, d, false);
+			else
+				gpu (A, false, rank);
+			break;
+		case METHOD_ASYMPTOTICALLY_FAST_GJ:
+			gpu (A, reduced, rank);
+			break;
+		case METHOD_FAUGERE_LACHARTRE:
+			{
+				// the reference runs FL with its default (reduced) output here
+				const size_t m = A.rowdim (), n = A.coldim ();
+				SparseMatrix<uint32> X (m, n), R (m, n);
+				for (size_t i = 0; i < m; ++i)
+					for (size_t j = 0; j < n; ++j)
+						if (A[i][j] != 0)
+							X[i].push_back (SparseMatrix<uint32>::Row::value_type (j, A[i][j]));
+				FaugereLachartre<Ring, Modules> FL (_ctx);
+				FL.echelonize (R, X, rank, d);
+				for (size_t i = 0; i < m; ++i) {
+					for (size_t j = 0; j < n; ++j)
+						A[i][j] = 0;
+					for (SparseMatrix<uint32>::Row::const_iterator e = R[i].begin (); e != R[i].end (); ++e)
+						A[i][e->first] = e->second;
+				}
+			}
+			break;
+		default:
+			throw LELAError ("Invalid method for choice of matrix");
+		}
+		_rank_table[&A] = rank;
+		return A;
+	}
+
+	template <class Matrix>
+	size_t rank (const Matrix &A) const
+	{
+		std::map<const void *, size_t>::const_iterator it = _rank_table.find (&A);
+		return it == _rank_table.end () ? 0 : it->second;
 	}
 };
 

@@ -18,6 +18,7 @@
 #include "lela/matrix/sparse.h"
 #include "lela/randiter/mersenne-twister.h"
 #include "lela/algorithms/faugere-lachartre.h"
+#include "lela/solutions/echelon-form.h"
 #include "lela_cuda/cuda-module.h"
 
 using namespace LELA;
@@ -234,6 +235,44 @@ static void test_fl (uint32 p, size_t m, size_t n, bool reduced)
 	CHECK (r1 == r2 && d1 == d2 && BLAS3::equal (cpu, R1, R2), what);
 }
 
+// EchelonForm::echelonize on a DenseMatrix (lela/solutions/echelon-form.h:
+// 103-150) under both contexts, per method and reduced flag: a
+// rank-deficient matrix with a zero column, a zero row and dependent rows.
+typedef EchelonForm<Zp, CUDAModule<uint32> > EFg;
+typedef EchelonForm<Zp> EFc;
+
+static void test_echelon (uint32 p, size_t m, size_t n, bool reduced, int method)
+{
+	Zp F (p);
+	Context<Zp, CUDAModule<uint32> > gpu (F);
+	Context<Zp> cpu (F);
+	MersenneTwister MT (m * 7 + n + method);
+	DenseMatrix<uint32> A (m, n), B (m, n);
+	fill (A, p, MT);
+	for (size_t i = 0; i < m; ++i)
+		A.setEntry (i, 1, 0);
+	for (size_t j = 0; j < n; ++j) {
+		A.setEntry (2, j, 0);
+		A.setEntry (m - 1, j, (A[0][j] * (uint64_t) 3) % p);
+		A.setEntry (m - 2, j, (A[3][j] + (uint64_t) A[4][j]) % p);
+	}
+	BLAS3::copy (cpu, A, B);
+	EFg Eg (gpu);
+	EFc Ec (cpu);
+	Eg.echelonize (A, reduced, (EFg::Method) method);
+	Ec.echelonize (B, reduced, (EFc::Method) method);
+	// the reference's EchelonForm::rank does not compile when instantiated
+	// (operator[] on its const map, echelon-form.h:163): count B's rows
+	size_t rb = 0;
+	for (size_t i = 0; i < m; ++i)
+		for (size_t j = 0; j < n; ++j)
+			if (B[i][j] != 0) { ++rb; break; }
+	char what[200];
+	std::snprintf (what, sizeof what, "EchelonForm p=%u %zux%zu %s method %d: form and rank (%zu/%zu) equal",
+		       p, m, n, reduced ? "reduced" : "non-reduced", method, Eg.rank (A), rb);
+	CHECK (Eg.rank (A) == rb && BLAS3::equal (cpu, A, B), what);
+}
+
 int main ()
 {
 	try {
@@ -251,6 +290,11 @@ int main ()
 		test_fl (65521, 96, 128, true);
 		test_fl (65521, 96, 128, false);
 		test_fl (2147483647u, 200, 300, true);
+		test_echelon (65521, 90, 130, false, EFc::METHOD_ASYMPTOTICALLY_FAST_GJ);
+		test_echelon (65521, 90, 130, true, EFc::METHOD_ASYMPTOTICALLY_FAST_GJ);
+		test_echelon (251, 140, 70, true, EFc::METHOD_ASYMPTOTICALLY_FAST_GJ);
+		test_echelon (65521, 90, 130, false, EFc::METHOD_STANDARD_GJ);
+		test_echelon (65521, 60, 80, true, EFc::METHOD_STANDARD_GJ);
 	} catch (LELAError &e) {
 		std::printf ("FAIL: LELAError thrown\n");
 		return 2;
