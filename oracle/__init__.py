@@ -48,6 +48,8 @@ def lib():
         L.oracle_echelon_zp_u32.argtypes = [_U, _S, _S, _P, _S, ctypes.POINTER(_S), ctypes.POINTER(_U)]
         L.oracle_echelon_reduced_zp_u32.argtypes = [_U, _S, _S, _P, _S, ctypes.POINTER(_S),
                                                     ctypes.POINTER(_U)]
+        L.oracle_echelon_reduced_unit_zp_u32.argtypes = [_U, _S, _S, _P, _S, ctypes.POINTER(_S),
+                                                         ctypes.POINTER(_U)]
         L.oracle_fl_echelonize_zp_u32.argtypes = [_U, _S, _S, _P, _P, _P, _I, _I, _P, _S,
                                                   ctypes.POINTER(_S), ctypes.POINTER(_U),
                                                   ctypes.POINTER(_S), ctypes.POINTER(_S)]
@@ -79,6 +81,8 @@ def ref():
         L.lela_ref_echelon_zp_u32.argtypes = [_U, _S, _S, _P, _S, ctypes.POINTER(_S), ctypes.POINTER(_U)]
         L.lela_ref_echelon_reduced_zp_u32.argtypes = [_U, _S, _S, _P, _S, ctypes.POINTER(_S),
                                                       ctypes.POINTER(_U)]
+        L.lela_ref_elim_echelon_reduced_zp_u32.argtypes = [_U, _S, _S, _P, _S, ctypes.POINTER(_S),
+                                                           ctypes.POINTER(_U)]
         L.lela_ref_elim_echelon_zp_u32.argtypes = [_U, _S, _S, _P, _S, ctypes.POINTER(_S), ctypes.POINTER(_U)]
         L.lela_ref_fl_echelonize_zp_u32.argtypes = [_U, _S, _S, _P, _P, _P, _I, _I, _P, _S,
                                                     ctypes.POINTER(_S), ctypes.POINTER(_U), ctypes.POINTER(_S)]
@@ -123,11 +127,13 @@ def echelon_zp(p, A):
     return A, r.value, d.value
 
 
-def echelon_reduced_zp(p, A):
+def echelon_reduced_zp(p, A, unit=False):
+    """unit: the standard method's form (pivots 1)."""
     A = _c(A, np.uint32).copy()
     m, n = A.shape
     r = _S(0); d = _U(0)
-    rc = lib().oracle_echelon_reduced_zp_u32(p, m, n, _ptr(A), n, ctypes.byref(r), ctypes.byref(d))
+    fn = lib().oracle_echelon_reduced_unit_zp_u32 if unit else lib().oracle_echelon_reduced_zp_u32
+    rc = fn(p, m, n, _ptr(A), n, ctypes.byref(r), ctypes.byref(d))
     if rc:
         raise ArithmeticError("pivot not invertible")
     return A, r.value, d.value
@@ -198,11 +204,13 @@ def ref_echelon_zp(p, A, classical=False):
     return A, r.value, d.value
 
 
-def ref_echelon_reduced_zp(p, A):
+def ref_echelon_reduced_zp(p, A, unit=False):
+    """unit: Elimination::echelonize_reduced (the standard method)."""
     A = _c(A, np.uint32).copy()
     m, n = A.shape
     r = _S(0); d = _U(0)
-    if ref().lela_ref_echelon_reduced_zp_u32(p, m, n, _ptr(A), n, ctypes.byref(r), ctypes.byref(d)):
+    fn = ref().lela_ref_elim_echelon_reduced_zp_u32 if unit else ref().lela_ref_echelon_reduced_zp_u32
+    if fn(p, m, n, _ptr(A), n, ctypes.byref(r), ctypes.byref(d)):
         raise ArithmeticError("pivot not invertible")
     return A, r.value, d.value
 

@@ -297,6 +297,31 @@ int oracle_echelon_reduced_zp_u32 (uint32_t p, size_t m, size_t n, uint32_t *A, 
 	return 0;
 }
 
+/* The standard method's reduced form, Elimination::echelonize_reduced
+ * (lela/algorithms/elimination.tcc:143-265), as EchelonForm::echelonize
+ * (A, true, METHOD_STANDARD_GJ) runs it.  Row i: the first nonzero at or
+ * below it in the current column of the matrix reduced by the earlier
+ * pivot rows (the same pivots as above), scaled by the inverse of its pivot
+ * (:222), then cleared from every other row.  The result is the form above
+ * with each pivot row divided by its pivot; det is the product of the
+ * pivots before scaling. */
+int oracle_echelon_reduced_unit_zp_u32 (uint32_t p, size_t m, size_t n, uint32_t *A, size_t lda,
+					size_t *rank, uint32_t *det)
+{
+	int rc = oracle_echelon_reduced_zp_u32 (p, m, n, A, lda, rank, det);
+	if (rc)
+		return rc;
+	for (size_t i = 0; i < *rank; ++i) {
+		size_t c = 0;
+		while (A[i * lda + c] == 0)
+			++c;
+		uint32_t xinv = oracle_inv_zp (p, A[i * lda + c]);
+		for (; c < n; ++c)
+			A[i * lda + c] = mulmod (p, A[i * lda + c], xinv);
+	}
+	return 0;
+}
+
 /* Faugere-Lachartre (lela/algorithms/faugere-lachartre.tcc:735-917).
  *
  * setup_splicer (:47-146) walks the rows: the head of a sparse row is its

@@ -49,6 +49,11 @@ int oracle_echelon_zp_u32 (uint32_t p, size_t m, size_t n, uint32_t *A, size_t l
 int oracle_echelon_reduced_zp_u32 (uint32_t p, size_t m, size_t n, uint32_t *A, size_t lda,
 				   size_t *rank, uint32_t *det);
 
+/* The same with every pivot row divided by its pivot (pivots 1): the
+ * standard method's reduced form. */
+int oracle_echelon_reduced_unit_zp_u32 (uint32_t p, size_t m, size_t n, uint32_t *A, size_t lda,
+					size_t *rank, uint32_t *det);
+
 /* Faugere-Lachartre echelon form of a CSR matrix.  R is dense m x n (ldr).
  * Returns 0; 1 with *bad_row on a malformed input (WrongMatrixForm);
  * 2 when the pivot block is singular (the reference returns early). */

@@ -282,6 +282,35 @@ int lela_ref_echelon_reduced_zp_u32 (uint32_t p, size_t m, size_t n, uint32_t *A
 	return 0;
 }
 
+/* The standard method's reduced form, EchelonForm::echelonize (A, true,
+ * METHOD_STANDARD_GJ) on a DenseMatrix: Elimination::echelonize_reduced
+ * (lela/algorithms/elimination.tcc:143-265) with the default pivot
+ * strategy of a dense row (elimination.h:141-147) and no L, as
+ * lela/solutions/echelon-form.h:111 calls it.  Each pivot row is scaled
+ * by the inverse of its pivot (:222), so the pivots come out as 1.  det =
+ * the product of the pivots before scaling. */
+int lela_ref_elim_echelon_reduced_zp_u32 (uint32_t p, size_t m, size_t n, uint32_t *A, size_t lda, size_t *rank, uint32_t *det)
+{
+	Zp F (p);
+	Context<Zp> ctx (F);
+	DenseMatrix<uint32> MA (m, n);
+	if (m && n) load_dense (MA, A, lda);
+	Elimination<Zp> elim (ctx);
+	Elimination<Zp>::Permutation P;
+	DenseMatrix<uint32> L;
+	size_t r = 0;
+	Zp::Element d;
+	try {
+		elim.echelonize_reduced (MA, L, P, r, d, false);
+	} catch (...) {
+		return -1;
+	}
+	if (m && n) store_dense (MA, A, lda);
+	*rank = r;
+	*det = d;
+	return 0;
+}
+
 /* Classical elimination Elimination::echelonize (lela/algorithms/
  * elimination.tcc:47-139), the reference's own cross-check for the
  * recursive GaussJordan result. */

@@ -6,7 +6,8 @@ Needs oracle/_ref/liblela_ref.so (built by `make -C oracle ref` from the
 reference sources).  Inputs come from lela_b200.gen (seeded); outputs are
 what LELA itself computes: BLAS3::gemm, BLAS3::trsm, the dense echelon forms
 of EchelonForm (GaussJordan + move_L; reduced: GaussJordan::
-echelonize_reduced), FaugereLachartre::echelonize in all
+echelonize_reduced and Elimination::echelonize_reduced),
+FaugereLachartre::echelonize in all
 four modes, and the GF(2) gemm / echelon form.  Small cases store inputs
 and outputs; the larger ones store SHA-256 digests of inputs and outputs.
 """
@@ -114,7 +115,7 @@ def main():
 
     # ---- dense reduced echelon form (EchelonForm::echelonize (A, true):
     #      GaussJordan::echelonize_reduced)
-    cases = []
+    cases, units = [], []
     for i, (p, m, nn) in enumerate([(65521, 30, 40), (65521, 50, 30), (251, 40, 40), (2, 24, 70),
                                     (65536, 12, 12), (2147483647, 33, 57), (4294967291, 20, 25),
                                     (65521, 70, 9)]):
@@ -131,7 +132,18 @@ def main():
         pre = "rech%d_" % i
         out.update({pre + "A": A, pre + "E": E, pre + "meta": np.array([p, st, r, d], dtype=np.uint64)})
         cases.append(pre)
+        # the standard method's reduced form (Elimination::echelonize_reduced,
+        # pivots scaled to 1) of the same input
+        try:
+            E, r, d = oracle.ref_echelon_reduced_zp(p, A, unit=True)
+            st = 0
+        except ArithmeticError:
+            E, r, d, st = A, 0, 0, 1
+        pre = "rechu%d_" % i
+        out.update({pre + "A": A, pre + "E": E, pre + "meta": np.array([p, st, r, d], dtype=np.uint64)})
+        units.append(pre)
     manifest["echelon_reduced"] = cases
+    manifest["echelon_reduced_unit"] = units
 
     # ---- Faugere-Lachartre, the reference test's matrix family and an
     #      F4-shaped matrix

@@ -42,9 +42,10 @@ def echelon_cases():
         yield pre, p, st, r, d, z[pre + "A"], z[pre + "E"]
 
 
-def echelon_reduced_cases():
+def echelon_reduced_cases(unit=False):
+    """unit: the standard method's form (Elimination::echelonize_reduced)."""
     z, man = data()
-    for pre in man["echelon_reduced"]:
+    for pre in man["echelon_reduced_unit" if unit else "echelon_reduced"]:
         p, st, r, d = (int(x) for x in z[pre + "meta"])
         yield pre, p, st, r, d, z[pre + "A"], z[pre + "E"]
 

@@ -49,13 +49,14 @@ def test_golden_echelon():
         assert np.array_equal(got, E), pre
 
 
-def test_golden_echelon_reduced():
-    for pre, p, st, r, d, A, E in golden_io.echelon_reduced_cases():
+@pytest.mark.parametrize("unit", [False, True])
+def test_golden_echelon_reduced(unit):
+    for pre, p, st, r, d, A, E in golden_io.echelon_reduced_cases(unit):
         if st:
             with pytest.raises(ArithmeticError):
-                oracle.echelon_reduced_zp(p, A)
+                oracle.echelon_reduced_zp(p, A, unit)
             continue
-        got, gr, gd = oracle.echelon_reduced_zp(p, A)
+        got, gr, gd = oracle.echelon_reduced_zp(p, A, unit)
         assert (gr, gd) == (r, d), pre
         assert np.array_equal(got, E), pre
 
@@ -181,9 +182,11 @@ def test_live_echelon(seed):
 
 
 @need_ref
+@pytest.mark.parametrize("unit", [False, True])
 @pytest.mark.parametrize("p", [2, 3, 251, 65521, 65536, 2147483647, 4294967291])
-def test_live_echelon_reduced(p):
-    """GaussJordan::echelonize_reduced against the restatement: full rank,
+def test_live_echelon_reduced(p, unit):
+    """GaussJordan::echelonize_reduced (unit: Elimination::echelonize_reduced)
+    against the restatement: full rank,
     rank deficient (a product of thin factors), zero columns and rows, tall
     and wide, and LELA's pivot-inversion failures (composite p, p >= 2^31)."""
     rng = np.random.default_rng(p % 1000)
@@ -200,11 +203,11 @@ def test_live_echelon_reduced(p):
                 A[m // 2:] = 0
                 A[:, :n // 2] = 0
             try:
-                want = oracle.ref_echelon_reduced_zp(p, A)
+                want = oracle.ref_echelon_reduced_zp(p, A, unit)
             except ArithmeticError:
                 want = None
             try:
-                got = oracle.echelon_reduced_zp(p, A)
+                got = oracle.echelon_reduced_zp(p, A, unit)
             except ArithmeticError:
                 got = None
             assert (want is None) == (got is None), (m, n, kind)
