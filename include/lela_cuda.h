@@ -175,16 +175,22 @@ int lela_cuda_echelon_zp_u32_dev (lela_cuda_ctx *ctx, size_t m, size_t n, uint32
 				  uint32_t *A, size_t lda, size_t *rank, uint32_t *det);
 
 /* A (m x n) <- its reduced row-echelon form, in place: zero above and below
- * every pivot, pivots keeping their values, zero rows last; *rank and *det
- * as above.  Replaces EchelonForm::echelonize (A, true) on a DenseMatrix
- * (lela/solutions/echelon-form.h:115-123: GaussJordan::echelonize_reduced,
- * lela/algorithms/gauss-jordan.tcc:434-466, through GaussJordanTransform,
- * :27-230), whose pivot rows are those of the non-reduced form with the
- * later pivot columns cleared.  LELA_CUDA_PIVOT_NOT_INVERTIBLE as above. */
+ * every pivot, zero rows last; *rank and *det as above.
+ * unit_pivots = 0: the pivots keep their values, as EchelonForm::echelonize
+ * (A, true) leaves a DenseMatrix with its default method (lela/solutions/
+ * echelon-form.h:115-123: GaussJordan::echelonize_reduced, lela/algorithms/
+ * gauss-jordan.tcc:434-466, through GaussJordanTransform, :27-230), whose
+ * pivot rows are those of the non-reduced form with the later pivot columns
+ * cleared.  unit_pivots = 1: every pivot row divided by its pivot, as the
+ * standard method leaves it (echelon-form.h:108-111: Elimination::
+ * echelonize_reduced, lela/algorithms/elimination.tcc:143-265).
+ * LELA_CUDA_PIVOT_NOT_INVERTIBLE as above. */
 int lela_cuda_echelon_reduced_zp_u32 (lela_cuda_ctx *ctx, size_t m, size_t n, uint32_t p,
-				      uint32_t *A, size_t lda, size_t *rank, uint32_t *det);
+				      uint32_t *A, size_t lda, int unit_pivots, size_t *rank,
+				      uint32_t *det);
 int lela_cuda_echelon_reduced_zp_u32_dev (lela_cuda_ctx *ctx, size_t m, size_t n, uint32_t p,
-					  uint32_t *A, size_t lda, size_t *rank, uint32_t *det);
+					  uint32_t *A, size_t lda, int unit_pivots, size_t *rank,
+					  uint32_t *det);
 
 /* ------------------------------------------- Faugere-Lachartre echelon form
  * Echelon form of the F4 matrix X (m x n, CSR: rowptr[m+1], colidx, vals;

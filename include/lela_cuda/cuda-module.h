@@ -378,13 +378,12 @@ public:
 
 /** EchelonForm over Modular<uint32> with the CUDA module: the interface and
  * the per-method control flow of lela/solutions/echelon-form.h:29-163.
- * Dense matrices go to the GPU where the reference's method gives the
- * GPU's result: the asymptotically fast Gauss-Jordan (the default for a
- * DenseMatrix), reduced or not, and the standard method's non-reduced form
- * (the same matrix, tests/test-gauss-jordan.C:91-99).  The Faugere-Lachartre
- * method runs the GPU pipeline on a sparse copy of the rows.  The standard
- * method's reduced form and every other matrix type take the reference's
- * Elimination on this context, as in the reference. */
+ * Dense matrices go to the GPU for both Gauss-Jordan methods, reduced or
+ * not: the asymptotically fast one (the default for a DenseMatrix; reduced,
+ * the pivots keep their values) and the standard one (Elimination; reduced,
+ * the pivots come out as 1).  The Faugere-Lachartre method runs the GPU
+ * pipeline on a sparse copy of the rows.  Every other matrix type takes the
+ * reference's Elimination on this context, as in the reference. */
 template <>
 class EchelonForm<Modular<uint32>, CUDAModule<uint32> >
 {
@@ -397,15 +396,20 @@ class EchelonForm<Modular<uint32>, CUDAModule<uint32> >
 	GaussJordan<Ring, Modules>::Permutation P;
 	std::map<const void *, size_t> _rank_table;
 
-	void gpu (DenseMatrix<uint32> &A, bool reduced, size_t &rank)
+	// reduced: 0 = non-reduced, 1 = pivots keep their values (Gauss-Jordan),
+	// 2 = pivots 1 (Elimination)
+	void gpu (DenseMatrix<uint32> &A, int reduced, size_t &rank)
 	{
 		size_t m = A.rowdim (), n = A.coldim ();
 		uint32_t d = 1;
 		rank = 0;
 		if (m == 0 || n == 0)
 			return;
-		int st = (reduced ? lela_cuda_echelon_reduced_zp_u32 : lela_cuda_echelon_zp_u32)
-			(_ctx.M.cuda.get (), m, n, _ctx.F._modulus, &A[0][0], A.disp (), &rank, &d);
+		int st = reduced
+			? lela_cuda_echelon_reduced_zp_u32 (_ctx.M.cuda.get (), m, n, _ctx.F._modulus, &A[0][0],
+							    A.disp (), reduced == 2, &rank, &d)
+			: lela_cuda_echelon_zp_u32 (_ctx.M.cuda.get (), m, n, _ctx.F._modulus, &A[0][0], A.disp (),
+						    &rank, &d);
 		lela_cuda_check (_ctx.M.cuda.get (), st);
 	}
 
@@ -445,13 +449,13 @@ public:
 		uint32 d;
 		switch (method) {
 		case METHOD_STANDARD_GJ:
-			if (reduced)
-				_elim.echelonize_reduced (A, L, P, rank, d, false);
-			else
-				gpu (A, false, rank);
+			// Elimination: the non-reduced form equals Gauss-Jordan's
+			// (tests/test-gauss-jordan.C:91-99); its reduced form has
+			// unit pivots (lela/algorithms/elimination.tcc:222)
+			gpu (A, reduced ? 2 : 0, rank);
 			break;
 		case METHOD_ASYMPTOTICALLY_FAST_GJ:
-			gpu (A, reduced, rank);
+			gpu (A, reduced ? 1 : 0, rank);
 			break;
 		case METHOD_FAUGERE_LACHARTRE:
 			{

@@ -110,9 +110,9 @@ def _bind_optional(L):
         "lela_cuda_trsm_csr_upper_zp_u32_dev": [_P, _S, _S, _U, _U, _I, _P, _P, _P, _P, _S, ctypes.POINTER(_S)],
         "lela_cuda_echelon_zp_u32": [_P, _S, _S, _U, _P, _S, ctypes.POINTER(_S), ctypes.POINTER(_U)],
         "lela_cuda_echelon_zp_u32_dev": [_P, _S, _S, _U, _P, _S, ctypes.POINTER(_S), ctypes.POINTER(_U)],
-        "lela_cuda_echelon_reduced_zp_u32": [_P, _S, _S, _U, _P, _S, ctypes.POINTER(_S),
+        "lela_cuda_echelon_reduced_zp_u32": [_P, _S, _S, _U, _P, _S, _I, ctypes.POINTER(_S),
                                              ctypes.POINTER(_U)],
-        "lela_cuda_echelon_reduced_zp_u32_dev": [_P, _S, _S, _U, _P, _S, ctypes.POINTER(_S),
+        "lela_cuda_echelon_reduced_zp_u32_dev": [_P, _S, _S, _U, _P, _S, _I, ctypes.POINTER(_S),
                                                  ctypes.POINTER(_U)],
         "lela_cuda_fl_echelonize_zp_u32": [_P, _S, _S, _U, _P, _P, _P, _I, _I, _P, _S,
                                            ctypes.POINTER(_S), ctypes.POINTER(_U),
@@ -290,20 +290,22 @@ class CudaModule:
 
 
     # ------------------------------------------------------- echelon form
-    def echelonize(self, p, A, reduced=False):
+    def echelonize(self, p, A, reduced=False, unit_pivots=False):
         """A <- row-echelon form in place (EchelonForm::echelonize (A,
         reduced) on a DenseMatrix, LELA's pivot rule; reduced: zero above and
-        below the pivots, which keep their values); returns (A, rank, det)."""
+        below the pivots, which keep their values, or with unit_pivots are
+        divided out as the standard method does); returns (A, rank, det)."""
         m, n = A.shape
         r = _S(0)
         d = _U(0)
         name = "lela_cuda_echelon_reduced_zp_u32" if reduced else "lela_cuda_echelon_zp_u32"
+        extra = (int(bool(unit_pivots)),) if reduced else ()
         if _is_torch(A):
-            st = getattr(self.L, name + "_dev")(self.h, m, n, p, _dptr(A), A.stride(0),
+            st = getattr(self.L, name + "_dev")(self.h, m, n, p, _dptr(A), A.stride(0), *extra,
                                                 ctypes.byref(r), ctypes.byref(d))
         else:
             _check(A.dtype == np.uint32, "echelonize: uint32 matrix expected")
-            st = getattr(self.L, name)(self.h, m, n, p, _ptr(A), A.strides[0] // 4,
+            st = getattr(self.L, name)(self.h, m, n, p, _ptr(A), A.strides[0] // 4, *extra,
                                        ctypes.byref(r), ctypes.byref(d))
         self._raise(st)
         return A, r.value, d.value

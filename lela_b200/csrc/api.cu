@@ -924,13 +924,14 @@ int lela_cuda_fl_echelonize_zp_u32_batch(lela_cuda_ctx *h, size_t count, const s
 // The dense echelon entry points: device (dev) or host pointers, the
 // non-reduced form or the reduced one.
 static int echelon_entry(lela_cuda_ctx *h, size_t m, size_t n, uint32_t p, uint32_t *A,
-                         size_t lda, size_t *rank, uint32_t *det, bool dev, bool reduced) {
+                         size_t lda, size_t *rank, uint32_t *det, bool dev, bool reduced,
+                         bool unit = false) {
   if (!h || !rank || !det) return ST_ARG;
   Ctx *c = &h->c;
   const char *what = reduced ? "echelon_reduced_zp_u32" : "echelon_zp_u32";
   if (m > (size_t)INT32_MAX || n > (size_t)INT32_MAX) return ctx_fail(c, ST_ARG, "dimension too large");
   auto run = [&](uint32_t *D, size_t ld) {
-    return reduced ? zp_echelon_reduced_dev(c, (int)m, (int)n, p, D, ld, rank, det)
+    return reduced ? zp_echelon_reduced_dev(c, (int)m, (int)n, p, D, ld, unit, rank, det)
                    : zp_echelon_dev(c, (int)m, (int)n, p, D, ld, rank, det, nullptr);
   };
   if (dev) {
@@ -969,13 +970,15 @@ int lela_cuda_echelon_zp_u32(lela_cuda_ctx *h, size_t m, size_t n, uint32_t p, u
 }
 
 int lela_cuda_echelon_reduced_zp_u32_dev(lela_cuda_ctx *h, size_t m, size_t n, uint32_t p,
-                                         uint32_t *A, size_t lda, size_t *rank, uint32_t *det) {
-  return echelon_entry(h, m, n, p, A, lda, rank, det, true, true);
+                                         uint32_t *A, size_t lda, int unit_pivots, size_t *rank,
+                                         uint32_t *det) {
+  return echelon_entry(h, m, n, p, A, lda, rank, det, true, true, unit_pivots != 0);
 }
 
 int lela_cuda_echelon_reduced_zp_u32(lela_cuda_ctx *h, size_t m, size_t n, uint32_t p,
-                                     uint32_t *A, size_t lda, size_t *rank, uint32_t *det) {
-  return echelon_entry(h, m, n, p, A, lda, rank, det, false, true);
+                                     uint32_t *A, size_t lda, int unit_pivots, size_t *rank,
+                                     uint32_t *det) {
+  return echelon_entry(h, m, n, p, A, lda, rank, det, false, true, unit_pivots != 0);
 }
 
 int lela_cuda_trsm_csr_upper_zp_u32(lela_cuda_ctx *h, size_t n, size_t ncols, uint32_t p,

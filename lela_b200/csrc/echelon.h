@@ -17,10 +17,12 @@ int zp_echelon_dev(Ctx *c, int m, int n, uint32_t p, uint32_t *D, size_t ld, siz
 
 // Reduced row-echelon form of D in place as LELA's GaussJordan::
 // echelonize_reduced leaves it (pivots keep their values; zero above and
-// below them): the form above, then the pivot columns cleared upwards by one
-// triangular solve.  Same rank, det and errors.  Defined in fl.cu, beside
-// the column gather it shares with the reduced FL form.
+// below them), or with unit_pivots as Elimination::echelonize_reduced does
+// (each pivot row divided by its pivot): the form above, then the pivot
+// columns cleared upwards by one triangular solve.  Same rank, det and
+// errors.  Defined in fl.cu, beside the column gather it shares with the
+// reduced FL form.
 int zp_echelon_reduced_dev(Ctx *c, int m, int n, uint32_t p, uint32_t *D, size_t ld,
-                           size_t *rank, uint32_t *det);
+                           bool unit_pivots, size_t *rank, uint32_t *det);
 
 }  // namespace lela

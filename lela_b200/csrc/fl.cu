@@ -389,28 +389,34 @@ int zp_fl_echelonize_dev(Ctx *c, int m, int n, uint32_t p, const uint64_t *d_row
 // other columns U_N gathered, U_N <- U_P^-1 U_N (the triangular solve), and
 // one kernel writes row i back as x_i U_N[i] in the other columns, x_i at
 // its pivot column and zero at the other pivot columns.  Rows from the rank
-// on are zero already.
+// on are zero already.  The standard method's reduced form,
+// Elimination::echelonize_reduced (lela/algorithms/elimination.tcc:143-265),
+// picks the same pivots but scales each pivot row by the inverse of its
+// pivot (:222): R = U_P^-1 U (unit_pivots).
 
 // Rows 0..r-1 of D from the solved columns: colmap[c] >= 0 is c's column in
 // X, colmap[c] = -1 - j marks the pivot column of row j; the pivot values
-// are the diagonal of UP.
+// are the diagonal of UP.  unit: the pivots become 1 (row i not multiplied
+// back by its pivot).
 __global__ void reduced_assemble_kernel(uint32_t *__restrict__ D, size_t ld, int r, int n,
                                         const int *__restrict__ colmap,
                                         const uint32_t *__restrict__ X, size_t ldx,
-                                        const uint32_t *__restrict__ UP, size_t ldp, Modulus mod) {
+                                        const uint32_t *__restrict__ UP, size_t ldp, Modulus mod,
+                                        bool unit) {
   const size_t total = (size_t)r * n;
   for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total;
        idx += (size_t)gridDim.x * blockDim.x) {
     const int i = (int)(idx / n), col = (int)(idx % n);
     const int cm = colmap[col];
-    const uint32_t x = UP[(size_t)i * ldp + i];
+    const uint32_t x = unit ? 1u : UP[(size_t)i * ldp + i];
+    const uint32_t v = cm >= 0 ? X[(size_t)i * ldx + cm] : 0u;
     D[(size_t)i * ld + col] =
-        cm >= 0 ? mod_mul(X[(size_t)i * ldx + cm], x, mod) : (-1 - cm == i ? x : 0u);
+        cm >= 0 ? (unit ? v : mod_mul(v, x, mod)) : (-1 - cm == i ? x : 0u);
   }
 }
 
 int zp_echelon_reduced_dev(Ctx *c, int m, int n, uint32_t p, uint32_t *D, size_t ld,
-                           size_t *rank, uint32_t *det) {
+                           bool unit_pivots, size_t *rank, uint32_t *det) {
   std::vector<int> piv;
   int st = zp_echelon_dev(c, m, n, p, D, ld, rank, det, &piv);
   if (st) return st;
@@ -456,7 +462,7 @@ int zp_echelon_reduced_dev(Ctx *c, int m, int n, uint32_t p, uint32_t *D, size_t
   const int grid = (int)std::min<size_t>((total + 255) / 256, (size_t)c->num_sms * 16);
   reduced_assemble_kernel<<<grid, 256, 0, c->stream>>>(D, ld, r, n, d_map, X,
                                                        (size_t)std::max(nrem, 1), UP, (size_t)r,
-                                                       make_modulus(p));
+                                                       make_modulus(p), unit_pivots);
   ctx_launched(c);
   e = cudaGetLastError();
   return e == cudaSuccess ? ST_OK : ctx_cuda(c, e, "reduced echelon: assembly");

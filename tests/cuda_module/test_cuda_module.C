@@ -295,6 +295,7 @@ int main ()
 		test_echelon (251, 140, 70, true, EFc::METHOD_ASYMPTOTICALLY_FAST_GJ);
 		test_echelon (65521, 90, 130, false, EFc::METHOD_STANDARD_GJ);
 		test_echelon (65521, 60, 80, true, EFc::METHOD_STANDARD_GJ);
+		test_echelon (251, 140, 70, true, EFc::METHOD_STANDARD_GJ);
 	} catch (LELAError &e) {
 		std::printf ("FAIL: LELAError thrown\n");
 		return 2;

@@ -105,13 +105,16 @@ def test_echelon_blocks_far_pivots(cuda, p):
 # echelonize_reduced (lela/algorithms/gauss-jordan.tcc:434-466).
 
 @pytest.mark.gpu
-def test_echelon_reduced_golden(cuda):
-    for pre, p, st, r, d, A, E in golden_io.echelon_reduced_cases():
+@pytest.mark.parametrize("unit", [False, True])
+def test_echelon_reduced_golden(cuda, unit):
+    """unit: the standard method's form (Elimination::echelonize_reduced,
+    lela/algorithms/elimination.tcc:143-265), pivots scaled to 1."""
+    for pre, p, st, r, d, A, E in golden_io.echelon_reduced_cases(unit):
         if st:
             with pytest.raises(LELAError):
-                cuda.echelonize(p, A.copy(), reduced=True)
+                cuda.echelonize(p, A.copy(), reduced=True, unit_pivots=unit)
             continue
-        got, gr, gd = cuda.echelonize(p, A.copy(), reduced=True)
+        got, gr, gd = cuda.echelonize(p, A.copy(), reduced=True, unit_pivots=unit)
         assert (gr, gd) == (r, d), pre
         assert np.array_equal(got, E), pre
 
@@ -123,10 +126,11 @@ def test_echelon_reduced_against_oracle(cuda, p):
                                    (150, 400), (333, 333)]):
         for kind in ("dense", "structured"):
             A = gen.dense_zp(seed, m, n, p) if kind == "dense" else _structured(seed, m, n, p)
-            want, wr, wd = oracle.echelon_reduced_zp(p, A)
-            got, gr, gd = cuda.echelonize(p, A.copy(), reduced=True)
-            assert (gr, gd) == (wr, wd), (p, m, n, kind)
-            assert np.array_equal(got, want), (p, m, n, kind)
+            for unit in (False, True):
+                want, wr, wd = oracle.echelon_reduced_zp(p, A, unit)
+                got, gr, gd = cuda.echelonize(p, A.copy(), reduced=True, unit_pivots=unit)
+                assert (gr, gd) == (wr, wd), (p, m, n, kind, unit)
+                assert np.array_equal(got, want), (p, m, n, kind, unit)
 
 
 @pytest.mark.gpu
