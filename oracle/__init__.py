@@ -88,6 +88,9 @@ def ref():
                                                     ctypes.POINTER(_S), ctypes.POINTER(_U), ctypes.POINTER(_S)]
         L.lela_ref_gemm_gf2.argtypes = [_S, _S, _S, _I, _P, _S, _P, _S, _I, _P, _S]
         L.lela_ref_echelon_gf2.argtypes = [_S, _S, _P, _S, ctypes.POINTER(_S)]
+        L.lela_ref_detect_format.argtypes = [ctypes.c_char_p]
+        L.lela_ref_read_dumas.argtypes = [_U, ctypes.c_char_p, _S, ctypes.POINTER(_S), ctypes.POINTER(_S), _P]
+        L.lela_ref_write_dumas.argtypes = [_U, _S, _S, _P, _S, ctypes.c_char_p, _S, ctypes.POINTER(_S)]
         _ref = L
     return _ref
 
@@ -237,3 +240,33 @@ def ref_echelon_gf2(A, n):
     r = _S(0)
     ref().lela_ref_echelon_gf2(A.shape[0], n, _ptr(A), A.shape[1], ctypes.byref(r))
     return A, r.value
+
+
+# ------------------------------------------------ LELA's matrix I/O (live)
+
+def ref_detect_format(text):
+    """MatrixReader::detectFormat (lela/matrix/io.tcc:163-200)."""
+    return ref().lela_ref_detect_format(text.encode())
+
+
+def ref_read_dumas(p, text, cap=1 << 22):
+    """MatrixReader::read (FORMAT_DUMAS): (status, dense matrix or None);
+    status 0 ok, 1 InvalidMatrixInput, 2 another exception."""
+    m = _S(0); n = _S(0)
+    A = np.zeros(cap, dtype=np.uint32)
+    st = ref().lela_ref_read_dumas(p, text.encode(), cap, ctypes.byref(m), ctypes.byref(n), _ptr(A))
+    if st:
+        return st, None
+    return 0, A[:m.value * n.value].reshape(m.value, n.value).copy()
+
+
+def ref_write_dumas(p, A):
+    """MatrixWriter::write (FORMAT_DUMAS) of a dense matrix."""
+    A = _c(A, np.uint32)
+    m, n = A.shape
+    cap = 64 + 40 * int(np.count_nonzero(A)) + 64
+    buf = ctypes.create_string_buffer(cap)
+    ln = _S(0)
+    st = ref().lela_ref_write_dumas(p, m, n, _ptr(A), max(n, 1), buf, cap, ctypes.byref(ln))
+    assert st == 0
+    return buf.value.decode()

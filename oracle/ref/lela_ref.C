@@ -27,6 +27,10 @@
 #include "lela/algorithms/gauss-jordan.h"
 #include "lela/algorithms/elimination.h"
 #include "lela/util/error.h"
+#include "lela/matrix/io.h"
+
+#include <sstream>
+#include <string>
 
 using namespace LELA;
 
@@ -415,6 +419,62 @@ int lela_ref_echelon_gf2 (size_t m, size_t n, uint64_t *A, size_t lda, size_t *r
 	}
 	store_gf2 (MA, A, lda);
 	*rank = r;
+	return 0;
+}
+
+/* MatrixReader<Modular<uint32> >::detectFormat (lela/matrix/io.tcc:
+ * 163-200) on the start of text: the FileFormatTag (lela/matrix/io.h:37-41)
+ * as an int. */
+int lela_ref_detect_format (const char *text)
+{
+	std::istringstream is (text);
+	return (int) MatrixReader<Zp>::detectFormat (is);
+}
+
+/* MatrixReader::read (A, FORMAT_DUMAS) -> readDumas (lela/matrix/io.tcc:
+ * 233-268) into a DenseMatrix<uint32> over Z/p.  *m, *n: the declared
+ * size; the entries go to A (row stride n) when m * n <= cap.
+ * Returns 0, 1 for InvalidMatrixInput, 2 for any other exception, 3 when
+ * the matrix does not fit cap. */
+int lela_ref_read_dumas (uint32_t p, const char *text, size_t cap, size_t *m, size_t *n, uint32_t *A)
+{
+	Zp F (p);
+	MatrixReader<Zp> reader (F);
+	DenseMatrix<uint32> M;
+	std::istringstream is (text);
+	try {
+		reader.read (is, M, FORMAT_DUMAS);
+	} catch (InvalidMatrixInput &) {
+		return 1;
+	} catch (...) {
+		return 2;
+	}
+	*m = M.rowdim ();
+	*n = M.coldim ();
+	if (M.rowdim () * M.coldim () > cap)
+		return 3;
+	if (M.rowdim () && M.coldim ())
+		store_dense (M, A, M.coldim ());
+	return 0;
+}
+
+/* MatrixWriter::write (A, FORMAT_DUMAS) -> writeDumas (lela/matrix/io.tcc:
+ * 526-534) of a dense m x n matrix over Z/p.  The text (NUL-terminated)
+ * goes to buf when it fits cap bytes; *len = its length.  Returns 0, or 3
+ * when it does not fit. */
+int lela_ref_write_dumas (uint32_t p, size_t m, size_t n, const uint32_t *A, size_t lda, char *buf, size_t cap, size_t *len)
+{
+	Zp F (p);
+	MatrixWriter<Zp> writer (F);
+	DenseMatrix<uint32> M (m, n);
+	if (m && n) load_dense (M, A, lda);
+	std::ostringstream os;
+	writer.write (os, M, FORMAT_DUMAS);
+	std::string t = os.str ();
+	*len = t.size ();
+	if (t.size () + 1 > cap)
+		return 3;
+	std::memcpy (buf, t.c_str (), t.size () + 1);
 	return 0;
 }
 
