@@ -29,6 +29,7 @@ Where the reference's behaviour is undefined -- a column index of 0 with a
 row index in range, which it writes before the row -- this module raises
 InvalidMatrixInput.
 """
+import math
 import re
 
 import numpy as np
@@ -211,13 +212,185 @@ def write_sms(A):
     return "".join(out)
 
 
-def read(text, p, format=FORMAT_DETECT):
-    """MatrixReader::read: detects the format unless one is named; the SMS
-    format is read here, the other formats raise NotImplementedError."""
+def _ones(A):
+    """(i, j, value) of the nonzero entries in row order."""
+    rows, cols = np.nonzero(A)
+    return [(int(i), int(j), int(A[i, j])) for i, j in zip(rows, cols)]
+
+
+def _rows_listed(A):
+    return [", ".join(str(int(v)) for v in row) for row in A]
+
+
+def write(A, p, format=FORMAT_PRETTY):
+    """MatrixWriter::write of a dense matrix over Z/p (entries already
+    reduced) in LELA's text formats (lela/matrix/io.tcc:438-680):
+    FORMAT_TURNER (zero-based triples, then -1), FORMAT_ONE_BASED,
+    FORMAT_DUMAS, FORMAT_MAPLE, FORMAT_MATLAB, FORMAT_SAGE and FORMAT_PRETTY
+    (columns as wide as the decimal width of p, zeros as '.')."""
+    A = np.asarray(A)
+    m, n = A.shape
+    if format == FORMAT_TURNER:
+        return "".join("%d %d %d\n" % e for e in _ones(A)) + "-1\n"
+    if format == FORMAT_ONE_BASED:
+        return "".join("%d %d %d\n" % (i + 1, j + 1, v) for i, j, v in _ones(A))
+    if format == FORMAT_DUMAS:
+        return write_sms(A)
+    if format == FORMAT_MAPLE:
+        if m == 0:
+            return "[]"
+        return "[ " + "], ".join("[" + r for r in _rows_listed(A)) + "] ]\n"
+    if format == FORMAT_MATLAB:
+        if m == 0:
+            return "[]"
+        return "[ " + "; ".join(_rows_listed(A)) + "]\n"
+    if format == FORMAT_SAGE:
+        if m == 0:
+            return "matrix([])\n"
+        return "matrix([ " + " ],\n         ".join("[ " + r for r in _rows_listed(A)) + " ] ])\n"
+    if format == FORMAT_PRETTY:
+        if m == 0 or n == 0:
+            return "(empty %dx%d matrix)\n" % (m, n)
+        # ModularTraits<uint32>::element_width (lela/ring/modular.h:225-226)
+        w = int(math.ceil(math.log(float(p)) / math.log(10.0)))
+        out = []
+        for row in A:
+            cells = [(" " * (w - 1) + ". ") if int(v) == 0 else (str(int(v)).rjust(w) + " ") for v in row]
+            out.append("  [ " + "".join(cells) + "]\n")
+        return "".join(out)
+    raise ValueError("no writer for matrix format %d" % format)
+
+
+def _put(A, i, j, x):
+    """A.setEntry (i, j, x) of a matrix the reader does not resize: an index
+    outside it is undefined in the reference and an error here."""
+    if i >= A.shape[0] or j >= A.shape[1]:
+        raise InvalidMatrixInput("entry (%d, %d) outside %d x %d" % ((i, j) + A.shape))
+    A[i, j] = x
+
+
+def read_turner(text, p, shape):
+    """MatrixReader::readTurner (lela/matrix/io.tcc:202-231) into a zero m x n
+    matrix: one zero-based 'i j v' per line up to a row index of -1.  A line
+    that cannot be read as such sets nothing.  The reference reads the first
+    line into 32 bytes and the others with a limit of 80: a first line of 32
+    or more characters is cut to 31 and ends the input, a line of 80 or more
+    ends it unread (lines of 32 to 79 characters after the first overflow
+    the reference's buffer; they are read whole here)."""
+    A = np.zeros(shape, dtype=np.uint32)
+    lines = text.split("\n")
+    if text.endswith("\n"):
+        lines.pop()
+    for k, line in enumerate(lines):
+        limit = 31 if k == 0 else 79
+        last = len(line) > limit
+        if last and k > 0:
+            break
+        s = _Scanner(line[:limit] if last else line)
+        i = s.size()
+        if i == _SIZE_MAX:
+            break
+        j = s.size() if i is not None else None
+        x = s.integer() if j is not None else None
+        if x is not None and x % p:
+            _put(A, i, j, x % p)
+        if last:
+            break
+    return A
+
+
+def read_matlab(text, p, shape):
+    """MatrixReader::readMatlab (lela/matrix/io.tcc:276-341) into a zero m x n
+    matrix: '[', then values separated by ',' (next column) and ';' (next
+    row), then ']'.  Anything else, a value that does not start with a digit
+    or '-', or the end of the text before ']' raises InvalidMatrixInput (so
+    does '[]', which the reference's writer produces for an empty matrix)."""
+    A = np.zeros(shape, dtype=np.uint32)
+    s = _Scanner(text)
+    if s.char() != "[":
+        raise InvalidMatrixInput("Matlab matrix must start with '['")
+    i = j = 0
+    while True:
+        c = s.char()
+        if c is None or not (c.isdigit() or c == "-"):
+            raise InvalidMatrixInput("value expected")
+        s.i -= 1
+        x = s.integer()
+        if x is None:
+            raise InvalidMatrixInput("value expected")
+        if x % p:
+            _put(A, i, j, x % p)
+        c = s.char()
+        if c == ";":
+            i, j = i + 1, 0
+        elif c == "]":
+            break
+        elif c == ",":
+            j += 1
+        else:
+            raise InvalidMatrixInput("',', ';' or ']' expected")
+    return A
+
+
+def read_pretty(text, p, shape):
+    """MatrixReader::readPretty (lela/matrix/io.tcc:351-409) into a zero m x n
+    matrix: one row per '[ ... ]', entries separated by white space, '.' for
+    a zero.  A row that is not opened by '[' raises InvalidMatrixInput; the
+    end of the text closes an open row.  An entry that is neither a number,
+    '.' nor ']' raises InvalidMatrixInput here (the reference does not
+    terminate on it)."""
+    A = np.zeros(shape, dtype=np.uint32)
+    t, n = text, len(text)
+    k, i = 0, 0
+    while True:
+        while k < n and t[k].isspace():
+            k += 1
+        if k >= n:
+            break
+        if t[k] != "[":
+            raise InvalidMatrixInput("row must start with '['")
+        k += 1
+        j = 0
+        while True:
+            while k < n and t[k].isspace():
+                k += 1
+            if k >= n:
+                break
+            if t[k] == "]":
+                k += 1
+                break
+            if t[k] == ".":
+                k += 1
+                j += 1
+                continue
+            s = _Scanner(t)
+            s.i = k
+            x = s.integer()
+            if x is None:
+                raise InvalidMatrixInput("entry expected")
+            k = s.i
+            if x % p:
+                _put(A, i, j, x % p)
+            j += 1
+        i += 1
+    return A
+
+
+def read(text, p, format=FORMAT_DETECT, shape=None):
+    """MatrixReader::read: detects the format unless one is named.  SMS sets
+    the size; the Turner, Matlab and Pretty readers fill a zero matrix of the
+    given shape, as the reference fills the matrix it is handed.  The
+    reference reads no other format (one-based, Maple and Sage raise
+    NotImplemented there)."""
     if format == FORMAT_DETECT:
         format = detect_format(text)
     if format == FORMAT_UNKNOWN:
         raise UnrecognisedFormat()
     if format == FORMAT_DUMAS:
         return read_sms(text, p)
-    raise NotImplementedError("matrix format %d is not read by this module" % format)
+    readers = {FORMAT_TURNER: read_turner, FORMAT_MATLAB: read_matlab, FORMAT_PRETTY: read_pretty}
+    if format in readers:
+        if shape is None:
+            raise ValueError("this format does not carry the matrix size: give shape")
+        return readers[format](text, p, shape)
+    raise NotImplementedError("the reference reads no matrix format %d" % format)

@@ -91,6 +91,8 @@ def ref():
         L.lela_ref_detect_format.argtypes = [ctypes.c_char_p]
         L.lela_ref_read_dumas.argtypes = [_U, ctypes.c_char_p, _S, ctypes.POINTER(_S), ctypes.POINTER(_S), _P]
         L.lela_ref_write_dumas.argtypes = [_U, _S, _S, _P, _S, ctypes.c_char_p, _S, ctypes.POINTER(_S)]
+        L.lela_ref_write_matrix.argtypes = [_I, _U, _S, _S, _P, _S, ctypes.c_char_p, _S, ctypes.POINTER(_S)]
+        L.lela_ref_read_matrix.argtypes = [_I, _U, ctypes.c_char_p, _S, _S, _P]
         _ref = L
     return _ref
 
@@ -270,3 +272,22 @@ def ref_write_dumas(p, A):
     st = ref().lela_ref_write_dumas(p, m, n, _ptr(A), max(n, 1), buf, cap, ctypes.byref(ln))
     assert st == 0
     return buf.value.decode()
+
+
+def ref_write_matrix(fmt, p, A):
+    """MatrixWriter::write (format fmt, a FileFormatTag) of a dense matrix."""
+    A = _c(A, np.uint32)
+    m, n = A.shape
+    cap = 256 + 24 * m * max(n, 1)
+    buf = ctypes.create_string_buffer(cap)
+    ln = _S(0)
+    st = ref().lela_ref_write_matrix(fmt, p, m, n, _ptr(A), max(n, 1), buf, cap, ctypes.byref(ln))
+    assert st == 0
+    return buf.value.decode()
+
+
+def ref_read_matrix(fmt, p, text, m, n):
+    """MatrixReader::read (format fmt) into an m x n matrix: (status, A)."""
+    A = np.zeros((m, n), dtype=np.uint32)
+    st = ref().lela_ref_read_matrix(fmt, p, text.encode(), m, n, _ptr(A))
+    return st, (A if st == 0 else None)

@@ -458,10 +458,50 @@ int lela_ref_read_dumas (uint32_t p, const char *text, size_t cap, size_t *m, si
 	return 0;
 }
 
-/* MatrixWriter::write (A, FORMAT_DUMAS) -> writeDumas (lela/matrix/io.tcc:
- * 526-534) of a dense m x n matrix over Z/p.  The text (NUL-terminated)
- * goes to buf when it fits cap bytes; *len = its length.  Returns 0, or 3
- * when it does not fit. */
+/* MatrixReader::read (A, format) into a DenseMatrix<uint32> already sized
+ * m x n (the Turner, Matlab and Pretty readers do not resize; lela/matrix/
+ * io.tcc:202-231, 295-341, 351-409).  Returns 0, 1 for InvalidMatrixInput,
+ * 2 for any other exception; A (row stride n) receives the matrix. */
+int lela_ref_read_matrix (int format, uint32_t p, const char *text, size_t m, size_t n, uint32_t *A)
+{
+	Zp F (p);
+	MatrixReader<Zp> reader (F);
+	DenseMatrix<uint32> M (m, n);
+	std::istringstream is (text);
+	try {
+		reader.read (is, M, (FileFormatTag) format);
+	} catch (InvalidMatrixInput &) {
+		return 1;
+	} catch (...) {
+		return 2;
+	}
+	if (m && n)
+		store_dense (M, A, n);
+	return 0;
+}
+
+/* MatrixWriter::write (A, format) (lela/matrix/io.tcc:438-488 and the
+ * writers after it) of a dense m x n matrix over Z/p; format is a
+ * FileFormatTag (lela/matrix/io.h:37-41).  The text (NUL-terminated) goes
+ * to buf when it fits cap bytes; *len = its length.  Returns 0, or 3 when
+ * it does not fit. */
+int lela_ref_write_matrix (int format, uint32_t p, size_t m, size_t n, const uint32_t *A, size_t lda, char *buf, size_t cap, size_t *len)
+{
+	Zp F (p);
+	MatrixWriter<Zp> writer (F);
+	DenseMatrix<uint32> M (m, n);
+	if (m && n) load_dense (M, A, lda);
+	std::ostringstream os;
+	writer.write (os, M, (FileFormatTag) format);
+	std::string t = os.str ();
+	*len = t.size ();
+	if (t.size () + 1 > cap)
+		return 3;
+	std::memcpy (buf, t.c_str (), t.size () + 1);
+	return 0;
+}
+
+/* The same for FORMAT_DUMAS (writeDumas, io.tcc:526-534). */
 int lela_ref_write_dumas (uint32_t p, size_t m, size_t n, const uint32_t *A, size_t lda, char *buf, size_t cap, size_t *len)
 {
 	Zp F (p);

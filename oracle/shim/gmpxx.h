@@ -78,6 +78,21 @@ MPZ_CMP(<) MPZ_CMP(>) MPZ_CMP(<=) MPZ_CMP(>=) MPZ_CMP(==) MPZ_CMP(!=)
 #undef MPZ_CMP
 
 inline std::ostream &operator << (std::ostream &o, const mpz_class &a) { return o << a.get_str (); }
-inline std::istream &operator >> (std::istream &i, mpz_class &a) { std::string s; i >> s; a.parse (s.c_str ()); return i; }
+// Formatted input as GMP's: white space skipped, an optional sign, decimal
+// digits up to the first other character (left in the stream); failbit
+// when no digit follows.
+inline std::istream &operator >> (std::istream &i, mpz_class &a)
+{
+	std::istream::sentry se (i);
+	if (!se) return i;
+	std::string s;
+	int c = i.peek ();
+	if (c == '-' || c == '+') { s += (char) i.get (); c = i.peek (); }
+	bool any = false;
+	while (c >= '0' && c <= '9') { s += (char) i.get (); c = i.peek (); any = true; }
+	if (!any) { i.setstate (std::ios::failbit); return i; }
+	a.parse (s.c_str ());
+	return i;
+}
 inline mpz_class abs (const mpz_class &a) { return a.v < 0 ? -a : a; }
 #endif

@@ -4,9 +4,10 @@
 
 Needs oracle/_ref/liblela_ref.so (make -C oracle ref).  Records, for the
 cases below, what LELA's MatrixReader::detectFormat returns on a first
-line, what MatrixWriter::write (FORMAT_DUMAS) writes for small matrices
-from lela_b200.gen, and what MatrixReader::read (FORMAT_DUMAS) makes of
-hand-written SMS texts (status: 0 read, 1 InvalidMatrixInput).
+line, what MatrixWriter::write writes for small matrices from
+lela_b200.gen (FORMAT_DUMAS, and every text format), and what
+MatrixReader::read makes of hand-written texts in the SMS, Turner, Matlab
+and Pretty formats (status: 0 read, 1 InvalidMatrixInput).
 """
 import json
 import os
@@ -49,6 +50,23 @@ READ_CASES = [
 ]
 
 
+# (format, shape, text): the Turner (2), Matlab (6) and Pretty (8) readers
+OTHER_READS = [
+    (2, (2, 3), "0 0 3\n1 2 -1\n\n5\n1 1\n-1\n0 1 4\n"),
+    (2, (2, 2), "1 0 70000\n0 1 65521"),
+    (2, (3, 3), "0 0 1 and a first line past 31 chars\n1 1 1\n"),
+    (6, (2, 3), "[ 1, 0, 5; 0, 7, 0]\n"),
+    (6, (2, 2), "  [1,-2 ;3, 4 ]"),
+    (6, (2, 2), "[ 1, 2; 3, 4"),
+    (6, (2, 2), "[ 1 2 ]"),
+    (6, (1, 1), "[]"),
+    (6, (1, 2), "( 1, 2 )"),
+    (8, (2, 3), "  [     1     . 65520 ]\n  [     .     7     . ]\n"),
+    (8, (3, 2), "[1 .]\n[]\n[ -4 5"),
+    (8, (2, 2), "1 2\n"),
+]
+
+
 def main():
     assert oracle.have_ref(), "build oracle/_ref first (make -C oracle ref)"
     out = {"p": P, "detect": [], "write": [], "read": []}
@@ -61,6 +79,17 @@ def main():
     for text in READ_CASES:
         st, A = oracle.ref_read_dumas(P, text)
         out["read"].append({"text": text, "status": st, "A": None if A is None else A.tolist()})
+    out["write_all"] = []
+    for i, (p, m, n) in enumerate([(7, 2, 3), (65521, 3, 4), (4294967291, 2, 2), (10, 3, 3)]):
+        A = gen.dense_zp(950 + i, m, n, p)
+        A[A % 3 == 0] = 0
+        out["write_all"].append({"p": p, "A": A.tolist(),
+                                 "text": {str(fmt): oracle.ref_write_matrix(fmt, p, A) for fmt in range(2, 9)}})
+    out["read_other"] = []
+    for fmt, shape, text in OTHER_READS:
+        st, A = oracle.ref_read_matrix(fmt, P, text, *shape)
+        out["read_other"].append({"format": fmt, "shape": list(shape), "text": text, "status": st,
+                                  "A": None if A is None else A.tolist()})
     with open(os.path.join(HERE, "matrix_io_golden.json"), "w") as f:
         json.dump(out, f, indent=1)
     print("wrote", len(out["detect"]), "detections,", len(out["write"]), "writes,", len(out["read"]), "reads")

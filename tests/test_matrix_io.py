@@ -53,13 +53,17 @@ def test_golden_read():
 def test_read_detect_and_errors():
     """read () with FORMAT_DETECT: a real SMS header is FORMAT_UNKNOWN for
     the reference's patterns, so it raises UnrecognisedFormat; naming the
-    format reads it.  Formats the module does not read raise."""
+    format reads it.  Formats the reference does not read raise."""
     text = mio.write_sms(np.array([[1, 0], [0, 2]], dtype=np.uint32))
     with pytest.raises(mio.UnrecognisedFormat):
         mio.read(text, 7)
     assert np.array_equal(mio.read(text, 7, mio.FORMAT_DUMAS), [[1, 0], [0, 2]])
-    with pytest.raises(NotImplementedError):
+    assert mio.detect_format("tt dd gg\n") == mio.FORMAT_TURNER
+    with pytest.raises(ValueError):                      # Turner: the size must be given
         mio.read("tt dd gg\n", 7)
+    assert mio.detect_format("[:]\n") == mio.FORMAT_MAPLE
+    with pytest.raises(NotImplementedError):             # the reference reads no Maple
+        mio.read("[:]\n", 7)
     with pytest.raises(mio.InvalidMatrixInput):
         mio.read_sms("2 2 M\n1 0 5\n0 0 0\n", 7)   # column 0: undefined in the reference
 
@@ -134,3 +138,103 @@ def test_live_detect():
         line = "".join(rng.choice(alphabet, size=int(rng.integers(0, 40))))
         text = line + "\n1 1 1\n"
         assert mio.detect_format(text) == oracle.ref_detect_format(text), repr(line)
+
+
+def test_golden_write_all_formats():
+    for case in _golden()["write_all"]:
+        A = np.array(case["A"], dtype=np.uint32)
+        for fmt, text in case["text"].items():
+            assert mio.write(A, case["p"], int(fmt)) == text, fmt
+
+
+def test_golden_read_other_formats():
+    g = _golden()
+    for case in g["read_other"]:
+        try:
+            st, A = 0, mio.read(case["text"], g["p"], case["format"], tuple(case["shape"]))
+        except mio.InvalidMatrixInput:
+            st, A = 1, None
+        assert st == case["status"], case["text"]
+        if st == 0:
+            assert np.array_equal(A, np.array(case["A"], dtype=np.uint32)), case["text"]
+
+
+def _random_value(rng, p):
+    return int(rng.choice([0, 1, p - 1, p, -1, -p - 2, 1 << 40, int(rng.integers(-10**6, 10**6))]))
+
+
+@need_ref
+def test_live_read_turner():
+    """Short lines only: the reference overflows its 32-byte buffer on lines
+    of 32 to 79 characters after the first."""
+    rng = np.random.default_rng(21)
+    p = 65521
+    for _ in range(150):
+        m, n = int(rng.integers(1, 5)), int(rng.integers(1, 5))
+        lines = []
+        for _ in range(int(rng.integers(0, 9))):
+            r = rng.random()
+            if r < 0.75:
+                lines.append("%d %d %d" % (rng.integers(0, m), rng.integers(0, n), _random_value(rng, p) % (10**9)))
+            elif r < 0.85:
+                lines.append(rng.choice(["", "7", "1 2", "x 1 1", "  "]))
+            else:
+                lines.append("-1")
+        text = "\n".join(lines) + ("\n" if rng.random() < 0.7 else "")
+        st, want = oracle.ref_read_matrix(mio.FORMAT_TURNER, p, text, m, n)
+        assert st == 0
+        assert np.array_equal(mio.read(text, p, mio.FORMAT_TURNER, (m, n)), want), text
+
+
+@need_ref
+def test_live_read_matlab_pretty():
+    """Well-formed texts with random spacing and values, and ones cut short
+    or with a stray character, within the matrix bounds (the reference
+    writes outside them unchecked, and loops without end on a Pretty entry
+    that is not a number, '.' or ']')."""
+    rng = np.random.default_rng(22)
+    p = 65521
+    sp = lambda: rng.choice(["", " ", "  ", "\n", "\t"])
+    for trial in range(300):
+        m, n = int(rng.integers(1, 4)), int(rng.integers(1, 4))
+        vals = [[_random_value(rng, p) for _ in range(n)] for _ in range(m)]
+        if trial % 2 == 0:
+            fmt = mio.FORMAT_MATLAB
+            text = sp() + "[" + sp() + (sp() + ";" + sp()).join(
+                (sp() + "," + sp()).join(str(v) for v in row) for row in vals) + sp() + "]"
+            r = rng.random()
+            if r < 0.15:
+                text = text[:-1]
+            elif r < 0.3:
+                k = int(rng.integers(1, len(text)))
+                text = text[:k] + rng.choice(["x", ":", "(", "--"]) + text[k:]
+        else:
+            fmt = mio.FORMAT_PRETTY
+            rows = ["[" + " ".join("." if v % p == 0 and rng.random() < 0.5 else str(v) for v in row) + sp() + "]"
+                    for row in vals]
+            text = sp().join(r + "\n" for r in rows)
+            if rng.random() < 0.2:
+                text = text.rstrip()[:-1]
+        st, want = oracle.ref_read_matrix(fmt, p, text, m, n)
+        try:
+            got_st, got = 0, mio.read(text, p, fmt, (m, n))
+        except mio.InvalidMatrixInput:
+            got_st, got = 1, None
+        assert got_st == st, (fmt, text)
+        if st == 0:
+            assert np.array_equal(got, want), (fmt, text)
+
+
+@need_ref
+@pytest.mark.parametrize("p", [2, 7, 10, 251, 65521, 4294967291])
+def test_live_write_all_formats(p):
+    """Every text format; not m x 0 in the triple formats, where the
+    reference's raw iteration of a dense matrix crashes."""
+    for (m, n) in ((0, 0), (0, 3), (2, 0), (1, 1), (2, 3), (5, 4)):
+        A = gen.dense_zp(m * 10 + n, m, n, p) if m * n else np.zeros((m, n), dtype=np.uint32)
+        if m * n:
+            A[A % 3 == 0] = 0
+        for fmt in range(2, 9):
+            if m > 0 and n == 0 and fmt in (mio.FORMAT_TURNER, mio.FORMAT_ONE_BASED, mio.FORMAT_DUMAS):
+                continue
+            assert mio.write(A, p, fmt) == oracle.ref_write_matrix(fmt, p, A), (m, n, fmt)
