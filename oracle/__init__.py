@@ -55,6 +55,8 @@ def lib():
                                                   ctypes.POINTER(_S), ctypes.POINTER(_S)]
         L.oracle_gemm_gf2.argtypes = [_S, _S, _S, _I, _P, _S, _P, _S, _I, _P, _S]
         L.oracle_echelon_gf2.argtypes = [_S, _S, _P, _S, ctypes.POINTER(_S)]
+        L.oracle_pluq_zp_u32.argtypes = [_U, _S, _S, _P, _S, _P, ctypes.POINTER(_S), _P, ctypes.POINTER(_S),
+                                         ctypes.POINTER(_S), ctypes.POINTER(_U)]
         L.oracle_inv_zp.argtypes = [_U, _U]
         L.oracle_inv_zp.restype = _U
         _lib = L
@@ -93,6 +95,8 @@ def ref():
         L.lela_ref_write_dumas.argtypes = [_U, _S, _S, _P, _S, ctypes.c_char_p, _S, ctypes.POINTER(_S)]
         L.lela_ref_write_matrix.argtypes = [_I, _U, _S, _S, _P, _S, ctypes.c_char_p, _S, ctypes.POINTER(_S)]
         L.lela_ref_read_matrix.argtypes = [_I, _U, ctypes.c_char_p, _S, _S, _P]
+        L.lela_ref_pluq_zp_u32.argtypes = [_U, _S, _S, _P, _S, _P, ctypes.POINTER(_S), _P, ctypes.POINTER(_S),
+                                           ctypes.POINTER(_S), ctypes.POINTER(_U)]
         _ref = L
     return _ref
 
@@ -142,6 +146,24 @@ def echelon_reduced_zp(p, A, unit=False):
     if rc:
         raise ArithmeticError("pivot not invertible")
     return A, r.value, d.value
+
+
+def _pluq(fn, p, A):
+    A = _c(A, np.uint32).copy()
+    m, n = A.shape
+    k = max(min(m, n), 1)
+    P = np.zeros(2 * k, dtype=np.uint64); Q = np.zeros(2 * k, dtype=np.uint64)
+    np_ = _S(0); nq = _S(0); r = _S(0); d = _U(0)
+    if fn(p, m, n, _ptr(A), max(n, 1), _ptr(P), ctypes.byref(np_), _ptr(Q), ctypes.byref(nq),
+          ctypes.byref(r), ctypes.byref(d)):
+        raise ArithmeticError("pivot not invertible")
+    pairs = lambda X, c: [(int(X[2 * t]), int(X[2 * t + 1])) for t in range(c)]
+    return A, pairs(P, np_.value), pairs(Q, nq.value), r.value, d.value
+
+
+def pluq_zp(p, A):
+    """Elimination::pluq restated: (LU in place, P, Q, rank, det)."""
+    return _pluq(lib().oracle_pluq_zp_u32, p, A)
 
 
 def fl_echelonize_zp(p, m, n, rowptr, colidx, vals, reduced=True, only_D=False):
@@ -291,3 +313,8 @@ def ref_read_matrix(fmt, p, text, m, n):
     A = np.zeros((m, n), dtype=np.uint32)
     st = ref().lela_ref_read_matrix(fmt, p, text.encode(), m, n, _ptr(A))
     return st, (A if st == 0 else None)
+
+
+def ref_pluq_zp(p, A):
+    """Elimination::pluq (LELA): (LU in place, P, Q, rank, det)."""
+    return _pluq(ref().lela_ref_pluq_zp_u32, p, A)

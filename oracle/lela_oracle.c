@@ -322,6 +322,77 @@ int oracle_echelon_reduced_unit_zp_u32 (uint32_t p, size_t m, size_t n, uint32_t
 	return 0;
 }
 
+/* PLUQ decomposition, Elimination::pluq (lela/algorithms/elimination.tcc:
+ * 266-370) with DensePivotStrategy (lela/algorithms/pivot-strategy.tcc:
+ * 19-42).  Step i: the first column from i on, in the current column
+ * order, with a nonzero at or below row i, and its first such row; that row
+ * and that column are swapped into place (transpositions (i, row) and (i,
+ * col)), det is multiplied by the pivot x, and every row j below with a
+ * nonzero a in column i gets row j <- row j - (a / x) row i right of column
+ * i and L entry a / x in column i.  Stops when no pivot is left or i
+ * reaches the column count.  P and Q are returned reversed, as the
+ * reference returns them (:362-363), as pairs. */
+int oracle_pluq_zp_u32 (uint32_t p, size_t m, size_t n, uint32_t *A, size_t lda,
+			size_t *P, size_t *np, size_t *Q, size_t *nq, size_t *rank, uint32_t *det)
+{
+	size_t i, npp = 0, nqq = 0;
+	uint32_t d = 1 % p;
+	for (i = 0; i < m && i < n; ++i) {
+		size_t prow = m, pcol = i;
+		for (; pcol < n; ++pcol) {
+			for (size_t r = i; r < m; ++r)
+				if (A[r * lda + pcol] != 0) { prow = r; break; }
+			if (prow < m) break;
+		}
+		if (prow == m)
+			break;
+		if (prow != i) {
+			for (size_t c = 0; c < n; ++c) {
+				uint32_t t = A[i * lda + c];
+				A[i * lda + c] = A[prow * lda + c];
+				A[prow * lda + c] = t;
+			}
+			P[2 * npp] = i; P[2 * npp + 1] = prow; ++npp;
+		}
+		if (pcol != i) {
+			for (size_t r = 0; r < m; ++r) {
+				uint32_t t = A[r * lda + i];
+				A[r * lda + i] = A[r * lda + pcol];
+				A[r * lda + pcol] = t;
+			}
+			Q[2 * nqq] = i; Q[2 * nqq + 1] = pcol; ++nqq;
+		}
+		uint32_t x = A[i * lda + i];
+		d = mulmod (p, d, x);
+		uint32_t xinv = oracle_inv_zp (p, x);
+		if (xinv == 0)
+			return -1;
+		uint32_t negxinv = (p - xinv) % p;
+		for (size_t j = i + 1; j < m; ++j) {
+			uint32_t a = A[j * lda + i];
+			if (a == 0)
+				continue;
+			uint32_t f = mulmod (p, a, negxinv);
+			for (size_t c = i + 1; c < n; ++c)
+				A[j * lda + c] = axpy_mod (p, A[j * lda + c], f, A[i * lda + c]);
+			A[j * lda + i] = (p - f) % p;
+		}
+	}
+	for (size_t k = 0; k < npp / 2; ++k)
+		for (int h = 0; h < 2; ++h) {
+			size_t t = P[2 * k + h]; P[2 * k + h] = P[2 * (npp - 1 - k) + h]; P[2 * (npp - 1 - k) + h] = t;
+		}
+	for (size_t k = 0; k < nqq / 2; ++k)
+		for (int h = 0; h < 2; ++h) {
+			size_t t = Q[2 * k + h]; Q[2 * k + h] = Q[2 * (nqq - 1 - k) + h]; Q[2 * (nqq - 1 - k) + h] = t;
+		}
+	*np = npp;
+	*nq = nqq;
+	*rank = i;
+	*det = d;
+	return 0;
+}
+
 /* Faugere-Lachartre (lela/algorithms/faugere-lachartre.tcc:735-917).
  *
  * setup_splicer (:47-146) walks the rows: the head of a sparse row is its

@@ -54,6 +54,13 @@ int oracle_echelon_reduced_zp_u32 (uint32_t p, size_t m, size_t n, uint32_t *A, 
 int oracle_echelon_reduced_unit_zp_u32 (uint32_t p, size_t m, size_t n, uint32_t *A, size_t lda,
 					size_t *rank, uint32_t *det);
 
+/* PLUQ decomposition in place (L strictly below the diagonal, U on and
+ * above it); P and Q as transposition pairs (at most min(m, n) each), in
+ * the reference's order; rank, det = product of the pivots.  Returns 0, or
+ * -1 when a pivot is not invertible mod p. */
+int oracle_pluq_zp_u32 (uint32_t p, size_t m, size_t n, uint32_t *A, size_t lda,
+			size_t *P, size_t *np, size_t *Q, size_t *nq, size_t *rank, uint32_t *det);
+
 /* Faugere-Lachartre echelon form of a CSR matrix.  R is dense m x n (ldr).
  * Returns 0; 1 with *bad_row on a malformed input (WrongMatrixForm);
  * 2 when the pivot block is singular (the reference returns early). */

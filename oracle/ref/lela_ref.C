@@ -315,6 +315,38 @@ int lela_ref_elim_echelon_reduced_zp_u32 (uint32_t p, size_t m, size_t n, uint32
 	return 0;
 }
 
+/* Elimination::pluq (lela/algorithms/elimination.tcc:266-370) with the
+ * default pivot strategy of a dense row: A <- L and U in place (L strictly
+ * below the diagonal, unit diagonal implied), P and Q the row and column
+ * transpositions in the order the reference returns them (reversed at its
+ * end), as pairs in P[0..2*np), Q[0..2*nq).  The pair arrays hold at most
+ * min(m, n) transpositions each.  Returns 0, or -1 when a pivot is not
+ * invertible. */
+int lela_ref_pluq_zp_u32 (uint32_t p, size_t m, size_t n, uint32_t *A, size_t lda, size_t *P, size_t *np, size_t *Q, size_t *nq, size_t *rank, uint32_t *det)
+{
+	Zp F (p);
+	Context<Zp> ctx (F);
+	DenseMatrix<uint32> MA (m, n);
+	if (m && n) load_dense (MA, A, lda);
+	Elimination<Zp> elim (ctx);
+	Elimination<Zp>::Permutation PP, QQ;
+	size_t r = 0;
+	Zp::Element d;
+	try {
+		elim.pluq (MA, PP, QQ, r, d);
+	} catch (...) {
+		return -1;
+	}
+	if (m && n) store_dense (MA, A, lda);
+	for (size_t k = 0; k < PP.size (); ++k) { P[2 * k] = PP[k].first; P[2 * k + 1] = PP[k].second; }
+	for (size_t k = 0; k < QQ.size (); ++k) { Q[2 * k] = QQ[k].first; Q[2 * k + 1] = QQ[k].second; }
+	*np = PP.size ();
+	*nq = QQ.size ();
+	*rank = r;
+	*det = d;
+	return 0;
+}
+
 /* Classical elimination Elimination::echelonize (lela/algorithms/
  * elimination.tcc:47-139), the reference's own cross-check for the
  * recursive GaussJordan result. */

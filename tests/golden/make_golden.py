@@ -6,7 +6,7 @@ Needs oracle/_ref/liblela_ref.so (built by `make -C oracle ref` from the
 reference sources).  Inputs come from lela_b200.gen (seeded); outputs are
 what LELA itself computes: BLAS3::gemm, BLAS3::trsm, the dense echelon forms
 of EchelonForm (GaussJordan + move_L; reduced: GaussJordan::
-echelonize_reduced and Elimination::echelonize_reduced),
+echelonize_reduced and Elimination::echelonize_reduced), Elimination::pluq,
 FaugereLachartre::echelonize in all
 four modes, and the GF(2) gemm / echelon form.  Small cases store inputs
 and outputs; the larger ones store SHA-256 digests of inputs and outputs.
@@ -144,6 +144,25 @@ def main():
         units.append(pre)
     manifest["echelon_reduced"] = cases
     manifest["echelon_reduced_unit"] = units
+
+    # ---- PLUQ decomposition (Elimination::pluq)
+    cases = []
+    for i, (p, m, nn) in enumerate([(65521, 20, 30), (65521, 30, 20), (251, 25, 25), (2, 18, 40),
+                                    (65536, 10, 10), (2147483647, 16, 24)]):
+        A = gen.dense_zp(700 + i, m, nn, p)
+        A[:, 2] = 0
+        A[m - 4:] = (A[:4] * 5) % p       # rank deficiency
+        try:
+            E, P, Q, r, d = oracle.ref_pluq_zp(p, A)
+            st = 0
+        except ArithmeticError:
+            E, P, Q, r, d, st = A, [], [], 0, 0, 1
+        pre = "pluq%d_" % i
+        out.update({pre + "A": A, pre + "E": E, pre + "P": np.array(P, dtype=np.int64).reshape(-1, 2),
+                    pre + "Q": np.array(Q, dtype=np.int64).reshape(-1, 2),
+                    pre + "meta": np.array([p, st, r, d], dtype=np.uint64)})
+        cases.append(pre)
+    manifest["pluq"] = cases
 
     # ---- Faugere-Lachartre, the reference test's matrix family and an
     #      F4-shaped matrix

@@ -50,6 +50,15 @@ def echelon_reduced_cases(unit=False):
         yield pre, p, st, r, d, z[pre + "A"], z[pre + "E"]
 
 
+def pluq_cases():
+    z, man = data()
+    for pre in man["pluq"]:
+        p, st, r, d = (int(x) for x in z[pre + "meta"])
+        P = [tuple(int(v) for v in t) for t in z[pre + "P"]]
+        Q = [tuple(int(v) for v in t) for t in z[pre + "Q"]]
+        yield pre, p, st, r, d, z[pre + "A"], z[pre + "E"], P, Q
+
+
 def fl_cases(with_inputs_only=True):
     """Faugere-Lachartre cases whose inputs are stored (the reference test's
     matrix family)."""

@@ -61,6 +61,17 @@ def test_golden_echelon_reduced(unit):
         assert np.array_equal(got, E), pre
 
 
+def test_golden_pluq():
+    for pre, p, st, r, d, A, E, P, Q in golden_io.pluq_cases():
+        if st:
+            with pytest.raises(ArithmeticError):
+                oracle.pluq_zp(p, A)
+            continue
+        got, gP, gQ, gr, gd = oracle.pluq_zp(p, A)
+        assert (gr, gd) == (r, d) and gP == P and gQ == Q, pre
+        assert np.array_equal(got, E), pre
+
+
 def test_golden_fl():
     for (pre, p, m, n, red, od, st, rank, det, rowptr, colidx, vals, R) in golden_io.fl_cases():
         got = oracle.fl_echelonize_zp(p, m, n, rowptr, colidx, vals, red, od)
@@ -262,3 +273,35 @@ def test_live_gf2(seed):
     e1, r1 = oracle.echelon_gf2(E, n)
     e2, r2 = oracle.ref_echelon_gf2(E, n)
     assert r1 == r2 and np.array_equal(e1, e2)
+
+
+@need_ref
+@pytest.mark.parametrize("p", [2, 3, 251, 65521, 65536, 2147483647, 4294967291])
+def test_live_pluq(p):
+    """Elimination::pluq against the restatement: L and U, both permutations,
+    rank and det, on full-rank, rank-deficient, zero-column and zero-row
+    inputs, and LELA's pivot-inversion failures."""
+    rng = np.random.default_rng(p % 991)
+    for (m, n) in ((1, 1), (7, 13), (13, 7), (40, 40), (48, 80), (80, 48)):
+        for kind in range(4):
+            A = gen.dense_zp(int(rng.integers(1 << 30)), m, n, p)
+            if kind == 1:
+                A[:, ::3] = 0
+            elif kind == 2:
+                r = max(1, min(m, n) // 3)
+                F = gen.dense_zp(1, m, r, p).astype(object) @ gen.dense_zp(2, r, n, p).astype(object)
+                A = (F % p).astype(np.uint32)
+            elif kind == 3:
+                A[m // 2:] = 0
+                A[:, :n // 2] = 0
+            try:
+                want = oracle.ref_pluq_zp(p, A)
+            except ArithmeticError:
+                want = None
+            try:
+                got = oracle.pluq_zp(p, A)
+            except ArithmeticError:
+                got = None
+            assert (want is None) == (got is None), (m, n, kind)
+            if want is not None:
+                assert np.array_equal(got[0], want[0]) and got[1:] == want[1:], (m, n, kind)
