@@ -224,7 +224,10 @@ int lela_cuda_fl_echelonize_zp_u32_dev (lela_cuda_ctx *ctx, size_t m, size_t n, 
  * (lela/blas/level3-generic.tcc:243-263 -> lela/blas/level2-gf2.tcc:132-155),
  * with M4RI mzd_mul/mzd_addmul (lela/blas/level3-m4ri.tcc:78-80).
  * Kernels (lela_cuda_set_gf2_kernel): 0 = auto (tensor cores), 1 =
- * int8-expanded tcgen05, 2 = bit-packed four-Russians on CUDA cores. */
+ * int8-expanded tcgen05, 2 = bit-packed four-Russians on CUDA cores.
+ * When n is not a multiple of 64, the bits of each row's last word of C at
+ * columns >= n are left as they were (a strided view may keep the next
+ * columns of a wider matrix there). */
 int lela_cuda_set_gf2_kernel (lela_cuda_ctx *ctx, int kernel);
 int lela_cuda_gemm_gf2 (lela_cuda_ctx *ctx, size_t m, size_t n, size_t k, int a,
 			const uint64_t *A, size_t lda, const uint64_t *B, size_t ldb, int b,
@@ -313,7 +316,9 @@ int lela_cuda_mlp_adam (lela_cuda_ctx *ctx, float *params, const float *grad, fl
  *    limbs for p <= 2^8, 2^16, 2^32 (m = n = k = 4096 fits at p = 65521);
  *    larger problems return LELA_CUDA_ERR_ARG before any GPU work.
  *  - The first call on a device sets up that device (looks up the array's
- *    device address); make it before any stream capture.
+ *    device address); make it before any stream capture.  That set-up is
+ *    kept for the life of the process: do not call this entry point after
+ *    cudaDeviceReset, which invalidates the address it looked up.
  *  - All calls share the array and it keeps the last call's contents; calls
  *    whose GPU work overlaps (other streams or threads without ordering)
  *    race on it.  The call synchronises `stream` before returning. */

@@ -153,6 +153,20 @@ int ctx_wait_flag(Ctx *c, volatile uint32_t *flag, uint32_t seq, const char *wha
   return ST_OK;
 }
 
+int ctx_smem_attr(Ctx *c, const void *kernel, int bytes, const char *what) {
+  static std::mutex mu;
+  static std::vector<std::pair<int, const void *>> done;
+  std::lock_guard<std::mutex> lock(mu);
+  for (const auto &d : done)
+    if (d.first == c->device && d.second == kernel) return ST_OK;
+  DeviceScope scope(c);
+  const cudaError_t e =
+      cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e != cudaSuccess) return ctx_cuda(c, e, what);
+  done.emplace_back(c->device, kernel);
+  return ST_OK;
+}
+
 static cudaEvent_t pool_event(Ctx *c) {
   if (!c->event_pool.empty()) {
     cudaEvent_t e = c->event_pool.back();
@@ -359,6 +373,7 @@ int lela_cuda_gemm_zp_u32_dev(lela_cuda_ctx *h, size_t m, size_t n, size_t k, ui
                               size_t ldb, uint32_t b, uint32_t *C, size_t ldc) {
   if (!h) return ST_ARG;
   Ctx *c = &h->c;
+  DeviceScope ds(c);
   if (m > (size_t)INT32_MAX || n > (size_t)INT32_MAX || k > (size_t)INT32_MAX)
     return ctx_fail(c, ST_ARG, "dimension too large");
   if ((m && n && !C) || (m && k && n && (!A || !B))) return ctx_fail(c, ST_ARG, "null pointer");
@@ -396,7 +411,7 @@ int lela_cuda_gemm_zp_u32(lela_cuda_ctx *h, size_t m, size_t n, size_t k, uint32
   if (!C || (k && (!A || !B))) return ctx_fail(c, ST_ARG, "null pointer");
   if (ldc < n || (k && (lda < k || ldb < n)))
     return ctx_fail(c, ST_ARG, "leading dimension smaller than the row length");
-  cudaSetDevice(c->device);
+  DeviceScope ds(c);
   void *dA = nullptr, *dB = nullptr, *dC = nullptr;
   int st = ST_OK;
   if (!st && k) st = ctx_stage(c, 0, m * k * 4, &dA);
@@ -439,6 +454,7 @@ int lela_cuda_gemm_gf2_dev(lela_cuda_ctx *h, size_t m, size_t n, size_t k, int a
                            uint64_t *C, size_t ldc) {
   if (!h) return ST_ARG;
   Ctx *c = &h->c;
+  DeviceScope ds(c);
   if (m > (size_t)INT32_MAX || n > (size_t)INT32_MAX || k > (size_t)INT32_MAX)
     return ctx_fail(c, ST_ARG, "dimension too large");
   if ((m && n && !C) || (m && n && k && (!A || !B))) return ctx_fail(c, ST_ARG, "null pointer");
@@ -456,7 +472,7 @@ int lela_cuda_gemm_gf2(lela_cuda_ctx *h, size_t m, size_t n, size_t k, int a, co
   if (!C || (k && (!A || !B))) return ctx_fail(c, ST_ARG, "null pointer");
   if (ldc < nw || (k && (lda < kw || ldb < nw)))
     return ctx_fail(c, ST_ARG, "leading dimension smaller than the row length");
-  cudaSetDevice(c->device);
+  DeviceScope ds(c);
   void *dA = nullptr, *dB = nullptr, *dC = nullptr;
   int st = ST_OK;
   if (k) st = ctx_stage(c, 0, m * kw * 8, &dA);
@@ -465,7 +481,9 @@ int lela_cuda_gemm_gf2(lela_cuda_ctx *h, size_t m, size_t n, size_t k, int a, co
   if (!st) st = ctx_clear_status(c);
   if (!st && k) st = h2d_matrix(c, dA, A, m, kw, lda, 8);
   if (!st && k) st = h2d_matrix(c, dB, B, k, nw, ldb, 8);
-  if (!st && (b & 1)) st = h2d_matrix(c, dC, C, m, nw, ldc, 8);
+  // C is read when b = 1, and for the bits past column n of each row's last
+  // word, which the kernels leave as they were
+  if (!st && ((b & 1) || (n & 63))) st = h2d_matrix(c, dC, C, m, nw, ldc, 8);
   if (!st)
     st = gf2_gemm_dev(c, GF2_AUTO, (int)m, (int)n, (int)k, a, (const uint64_t *)dA, kw,
                       (const uint64_t *)dB, nw, b, (uint64_t *)dC, nw);
@@ -478,6 +496,7 @@ int lela_cuda_echelon_gf2_dev(lela_cuda_ctx *h, size_t m, size_t n, uint64_t *A,
                               size_t *rank) {
   if (!h || !rank) return ST_ARG;
   Ctx *c = &h->c;
+  DeviceScope ds(c);
   if (m > (size_t)INT32_MAX || n > (size_t)INT32_MAX) return ctx_fail(c, ST_ARG, "dimension too large");
   if (m && n && !A) return ctx_fail(c, ST_ARG, "null pointer");
   int st = gf2_echelon_dev(c, (int)m, (int)n, A, lda, rank);
@@ -497,7 +516,7 @@ int lela_cuda_echelon_gf2(lela_cuda_ctx *h, size_t m, size_t n, uint64_t *A, siz
   const size_t nw = (n + 63) / 64;
   if (!A) return ctx_fail(c, ST_ARG, "null pointer");
   if (lda < nw) return ctx_fail(c, ST_ARG, "leading dimension smaller than the row length");
-  cudaSetDevice(c->device);
+  DeviceScope ds(c);
   void *dA = nullptr;
   int st = ctx_stage(c, 0, m * nw * 8, &dA);
   if (!st) st = ctx_clear_status(c);
@@ -517,7 +536,7 @@ int lela_cuda_echelon_zp_u32_batch(lela_cuda_ctx *h, size_t count, uint32_t *con
   if (count == 0) return ST_OK;
   if (!A || !lda || !m || !n || !p || !rank || !det || !status)
     return ctx_fail(c, ST_ARG, "null pointer");
-  cudaSetDevice(c->device);
+  DeviceScope ds(c);
   std::vector<SmallItem> small;
   std::vector<size_t> small_idx, big_idx;
   for (size_t i = 0; i < count; ++i) {
@@ -671,6 +690,7 @@ int lela_cuda_mlp_forward(lela_cuda_ctx *h, const float *params, int nfeat, cons
                           size_t n, float *out) {
   if (!h) return ST_ARG;
   if (n > (size_t)INT32_MAX) return ctx_fail(&h->c, ST_ARG, "mlp: too many samples");
+  DeviceScope ds(&h->c);
   return mlp_forward_dev(&h->c, params, nfeat, X, (int)n, out);
 }
 
@@ -678,12 +698,14 @@ int lela_cuda_mlp_grad(lela_cuda_ctx *h, const float *params, int nfeat, const f
                        const float *target, size_t n, float *grad, float *loss) {
   if (!h) return ST_ARG;
   if (n > (size_t)INT32_MAX) return ctx_fail(&h->c, ST_ARG, "mlp: too many samples");
+  DeviceScope ds(&h->c);
   return mlp_grad_dev(&h->c, params, nfeat, X, target, (int)n, grad, loss);
 }
 
 int lela_cuda_mlp_adam(lela_cuda_ctx *h, float *params, const float *grad, float *m, float *v,
                        size_t count, int step, float lr) {
   if (!h || step < 1) return ST_ARG;
+  DeviceScope ds(&h->c);
   return mlp_adam_dev(&h->c, params, grad, m, v, (int)count, step, lr);
 }
 
@@ -713,7 +735,7 @@ int lela_cuda_fl_echelonize_zp_u32(lela_cuda_ctx *h, size_t m, size_t n, uint32_
     if (rowptr[r + 1] < rowptr[r]) return ctx_fail(c, ST_ARG, "row pointers decrease");
   for (uint64_t e = 0; e < nnz; ++e)
     if (colidx[e] >= n) return ctx_fail(c, ST_ARG, "column index out of range");
-  cudaSetDevice(c->device);
+  DeviceScope ds(c);
   std::vector<uint32_t> heads(m), hv(m);
   for (size_t r = 0; r < m; ++r) {
     const bool empty = rowptr[r + 1] == rowptr[r];
@@ -750,6 +772,7 @@ int lela_cuda_fl_echelonize_zp_u32_dev(lela_cuda_ctx *h, size_t m, size_t n, uin
                                        size_t *bad_row) {
   if (!h) return ST_ARG;
   Ctx *c = &h->c;
+  DeviceScope ds(c);
   if (m > (size_t)INT32_MAX || n > (size_t)INT32_MAX) return ctx_fail(c, ST_ARG, "dimension too large");
   if (p < 2) return ctx_fail(c, ST_ARG, "modulus must be at least 2");
   if (!rowptr || (m && (!R || ldr < n))) return ctx_fail(c, ST_ARG, "bad output or row pointers");
@@ -850,6 +873,7 @@ int lela_cuda_fl_echelonize_zp_u32_batch(lela_cuda_ctx *h, size_t count, const s
                                          size_t *rank, uint32_t *det, int *status) {
   if (!h) return ST_ARG;
   Ctx *c = &h->c;
+  DeviceScope ds(c);
   if (count == 0) return ST_OK;
   if (!m || !n || !p || !rowptr || !colidx || !vals || !R || !ldr || !rank || !det || !status)
     return ctx_fail(c, ST_ARG, "null pointer");
@@ -928,6 +952,7 @@ static int echelon_entry(lela_cuda_ctx *h, size_t m, size_t n, uint32_t p, uint3
                          bool unit = false) {
   if (!h || !rank || !det) return ST_ARG;
   Ctx *c = &h->c;
+  DeviceScope ds(c);
   const char *what = reduced ? "echelon_reduced_zp_u32" : "echelon_zp_u32";
   if (m > (size_t)INT32_MAX || n > (size_t)INT32_MAX) return ctx_fail(c, ST_ARG, "dimension too large");
   auto run = [&](uint32_t *D, size_t ld) {
@@ -948,7 +973,6 @@ static int echelon_entry(lela_cuda_ctx *h, size_t m, size_t n, uint32_t p, uint3
   }
   if (!A) return ctx_fail(c, ST_ARG, "null pointer");
   if (lda < n) return ctx_fail(c, ST_ARG, "leading dimension smaller than the row length");
-  cudaSetDevice(c->device);
   void *dA = nullptr;
   int st = ctx_stage(c, 0, m * n * 4, &dA);
   if (!st) st = ctx_clear_status(c);
@@ -1000,7 +1024,7 @@ int lela_cuda_trsm_csr_upper_zp_u32(lela_cuda_ctx *h, size_t n, size_t ncols, ui
     if (rowptr[r + 1] < rowptr[r]) return ctx_fail(c, ST_ARG, "row pointers decrease");
   for (uint64_t e = 0; e < nnz; ++e)
     if (colidx[e] >= n) return ctx_fail(c, ST_ARG, "column index out of range");
-  cudaSetDevice(c->device);
+  DeviceScope ds(c);
   void *dX = nullptr, *dB = nullptr;
   int st = ctx_stage(c, 2, (n + 1) * 8 + nnz * 8 + 64, &dX);
   if (!st && ncols) st = ctx_stage(c, 1, n * ncols * 4, &dB);
@@ -1029,6 +1053,7 @@ int lela_cuda_trsm_csr_upper_zp_u32_dev(lela_cuda_ctx *h, size_t n, size_t ncols
                                         size_t ldb, size_t *bad_idx) {
   if (!h) return ST_ARG;
   Ctx *c = &h->c;
+  DeviceScope ds(c);
   if (n > (size_t)INT32_MAX || ncols > (size_t)INT32_MAX)
     return ctx_fail(c, ST_ARG, "dimension too large");
   if (n && (!rowptr || (ncols && !B))) return ctx_fail(c, ST_ARG, "null pointer");
@@ -1041,6 +1066,7 @@ int lela_cuda_trsm_zp_u32_dev(lela_cuda_ctx *h, int upper, int diag_is_one, size
                               size_t ldb, size_t *bad_idx) {
   if (!h) return ST_ARG;
   Ctx *c = &h->c;
+  DeviceScope ds(c);
   if (m > (size_t)INT32_MAX || n > (size_t)INT32_MAX) return ctx_fail(c, ST_ARG, "dimension too large");
   if (m && (!A || (n && !B))) return ctx_fail(c, ST_ARG, "null pointer");
   return zp_trsm_dev(c, upper != 0, diag_is_one != 0, (int)m, (int)n, p, a, A, lda, B, ldb,
@@ -1057,7 +1083,7 @@ int lela_cuda_trsm_zp_u32(lela_cuda_ctx *h, int upper, int diag_is_one, size_t m
   if (m == 0) return ST_OK;
   if (!A || (n && !B)) return ctx_fail(c, ST_ARG, "null pointer");
   if (lda < m || (n && ldb < n)) return ctx_fail(c, ST_ARG, "leading dimension smaller than the row length");
-  cudaSetDevice(c->device);
+  DeviceScope ds(c);
   void *dA = nullptr, *dB = nullptr;
   int st = ctx_stage(c, 0, m * m * 4, &dA);
   if (!st && n) st = ctx_stage(c, 1, m * n * 4, &dB);

@@ -213,14 +213,8 @@ __global__ void __launch_bounds__(SB_THREADS)
 bool small_echelon_fits(int m, int n) { return (size_t)m * n * 4 <= (size_t)SMALL_SMEM; }
 
 int echelon_small_batch_prepare(Ctx *c) {
-  static std::once_flag once;
-  static cudaError_t attr_err = cudaSuccess;
-  std::call_once(once, [] {
-    attr_err = cudaFuncSetAttribute(echelon_small_batch_kernel,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, SMALL_SMEM);
-  });
-  return attr_err == cudaSuccess ? ST_OK
-                                 : ctx_cuda(c, attr_err, "cudaFuncSetAttribute(small batch)");
+  return ctx_smem_attr(c, (const void *)echelon_small_batch_kernel, SMALL_SMEM,
+                       "cudaFuncSetAttribute(small batch)");
 }
 
 int echelon_small_batch_dev(Ctx *c, int count, const SmallItem *d_items, unsigned *d_next,

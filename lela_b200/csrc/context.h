@@ -164,6 +164,29 @@ int ctx_panel_map(Ctx *c, void **host, void **dev);
 // giving up after a minute.
 int ctx_wait_flag(Ctx *c, volatile uint32_t *flag, uint32_t seq, const char *what);
 
+// Raise a kernel's dynamic shared-memory limit to `bytes` on the handle's
+// device.  The attribute belongs to the device that is current when it is
+// set, so it is set once per (device, kernel) pair, under a lock; handles on
+// different devices of one process each get their own.
+int ctx_smem_attr(Ctx *c, const void *kernel, int bytes, const char *what);
+
+// Makes the handle's device current for the life of the object and then
+// restores the caller's device (the device-pointer entry points run on the
+// handle's stream, which belongs to that device).
+struct DeviceScope {
+  int prev = -1;
+  bool changed = false;
+  explicit DeviceScope(const Ctx *c) {
+    if (cudaGetDevice(&prev) == cudaSuccess && prev != c->device)
+      changed = cudaSetDevice(c->device) == cudaSuccess;
+  }
+  ~DeviceScope() {
+    if (changed) cudaSetDevice(prev);
+  }
+  DeviceScope(const DeviceScope &) = delete;
+  DeviceScope &operator=(const DeviceScope &) = delete;
+};
+
 // Profiling: prof_begin records the start event of a named kernel launch
 // (returns an index, or -1 when profiling is off); prof_end its end event.
 int prof_begin(Ctx *c, const char *name);

@@ -673,16 +673,11 @@ int zp_echelon_dev(Ctx *c, int m, int n, uint32_t p, uint32_t *D, size_t ld, siz
                      &gws);
   if (st) return st;
   const bool small = p < (1u << 16);
-  static std::once_flag once;
-  static cudaError_t attr_err = cudaSuccess;
-  std::call_once(once, [] {
-    attr_err = cudaFuncSetAttribute(panel_search_kernel<ArithSmall>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PW_SMEM);
-    if (attr_err == cudaSuccess)
-      attr_err = cudaFuncSetAttribute(panel_search_kernel<ArithWide>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PW_SMEM);
-  });
-  if (attr_err != cudaSuccess) return ctx_cuda(c, attr_err, "echelon: panel search attributes");
+  if ((st = ctx_smem_attr(c, (const void *)panel_search_kernel<ArithSmall>, (int)PW_SMEM,
+                          "echelon: panel search attributes")) ||
+      (st = ctx_smem_attr(c, (const void *)panel_search_kernel<ArithWide>, (int)PW_SMEM,
+                          "echelon: panel search attributes")))
+    return st;
   const ArithSmall ars = ArithSmall::make(p);
   const ArithWide arw = ArithWide::make(p);
   static_assert(sizeof(PanelOut) <= PANEL_FLAG_OFF, "panel result and flag share the mapped page");

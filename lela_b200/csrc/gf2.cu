@@ -103,8 +103,12 @@ __global__ void __launch_bounds__(M4_THREADS)
     for (int w = 0; w < M4_BW; ++w) {
       const int gw = w0 + w;
       if (gw >= Nw) break;
-      uint64_t v = (beta ? crow[gw] : 0ull) ^ (alpha ? acc[i][w] : 0ull);
-      if (gw == Nw - 1) v &= tail_mask;
+      // bits of the last word at columns >= N keep their old values (they
+      // may belong to the next columns of a strided view)
+      const bool part = gw == Nw - 1 && tail_mask != ~0ull;
+      const uint64_t old = (beta || part) ? crow[gw] : 0ull;
+      uint64_t v = (beta ? old : 0ull) ^ (alpha ? acc[i][w] : 0ull);
+      if (part) v = (v & tail_mask) | (old & ~tail_mask);
       crow[gw] = v;
     }
   }
@@ -117,13 +121,9 @@ int gf2_m4rm_dev(Ctx *c, int M, int N, int K, int alpha, const uint64_t *A, size
   const uint64_t tail = (N & 63) ? ((1ull << (N & 63)) - 1ull) : ~0ull;
   dim3 grid((Nw + M4_BW - 1) / M4_BW, (M + M4_THREADS * M4_ROWS - 1) / (M4_THREADS * M4_ROWS));
   constexpr int smem = (4 * M4_BW * 256 + M4_KC * M4_BW) * 8;
-  static std::once_flag once;
-  static cudaError_t attr_err = cudaSuccess;
-  std::call_once(once, [] {
-    attr_err = cudaFuncSetAttribute(gf2_m4rm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)((4 * M4_BW * 256 + M4_KC * M4_BW) * 8));
-  });
-  if (attr_err != cudaSuccess) return ctx_cuda(c, attr_err, "cudaFuncSetAttribute(gf2_m4rm)");
+  if (int st = ctx_smem_attr(c, (const void *)gf2_m4rm_kernel, smem,
+                             "cudaFuncSetAttribute(gf2_m4rm)"))
+    return st;
   int pi = prof_begin(c, "gf2_m4rm");
   gf2_m4rm_kernel<<<grid, M4_THREADS, smem, c->stream>>>(A, lda, B, ldb, C, ldc, M, Nw, K, tail,
                                                          alpha, beta);
@@ -601,13 +601,9 @@ int gf2_echelon_dev(Ctx *c, int m, int n, uint64_t *D, size_t ld, size_t *rank_o
   uint64_t *d_Lb = d_U + GW;                 // m x GB words
   uint64_t *d_L11s = d_Lb + (size_t)m * GB;                       // GB x GW words
   const uint32_t *d_pcol = reinterpret_cast<const uint32_t *>(b8 + offsetof(Gf2PanelOut, pcol));
-  static std::once_flag once;
-  static cudaError_t attr_err = cudaSuccess;
-  std::call_once(once, [] {
-    attr_err = cudaFuncSetAttribute(gf2_search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)GF2_SEARCH_SMEM);
-  });
-  if (attr_err != cudaSuccess) return ctx_cuda(c, attr_err, "gf2 echelon: search attributes");
+  if ((st = ctx_smem_attr(c, (const void *)gf2_search_kernel, (int)GF2_SEARCH_SMEM,
+                          "gf2 echelon: search attributes")))
+    return st;
   static_assert(sizeof(Gf2PanelOut) <= PANEL_FLAG_OFF, "panel result and flag share the mapped page");
   void *mh = nullptr, *md = nullptr;
   if ((st = ctx_panel_map(c, &mh, &md))) return st;

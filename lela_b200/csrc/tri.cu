@@ -464,19 +464,17 @@ __global__ void __launch_bounds__(TB_THREADS)
 static int tri_block(Ctx *c, const TriLeaves &L, bool upper, int m, const uint32_t *A, size_t lda,
                      uint32_t *B, size_t ldb, int n, uint32_t p, uint32_t alpha) {
   if (n <= 0) return ST_OK;
-  static std::once_flag once;
-  static cudaError_t attr_err = cudaSuccess;
-  std::call_once(once, [] {
+  {
     const void *fns[8] = {
         (const void *)tri_block_kernel<true, true, 64>, (const void *)tri_block_kernel<true, false, 64>,
         (const void *)tri_block_kernel<false, true, 64>, (const void *)tri_block_kernel<false, false, 64>,
         (const void *)tri_block_kernel<true, true, 32>, (const void *)tri_block_kernel<true, false, 32>,
         (const void *)tri_block_kernel<false, true, 32>, (const void *)tri_block_kernel<false, false, 32>};
-    for (int k = 0; k < 8 && attr_err == cudaSuccess; ++k)
-      attr_err = cudaFuncSetAttribute(fns[k], cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      TB_NB * (k < 4 ? 64 : 32) * 4);
-  });
-  if (attr_err != cudaSuccess) return ctx_cuda(c, attr_err, "cudaFuncSetAttribute(tri_block)");
+    for (int k = 0; k < 8; ++k)
+      if (int st = ctx_smem_attr(c, fns[k], TB_NB * (k < 4 ? 64 : 32) * 4,
+                                 "cudaFuncSetAttribute(tri_block)"))
+        return st;
+  }
   const size_t off = (size_t)(A - L.A_base) / (lda + 1);
   const uint32_t *T = L.tinv + (off / TRI_NB) * TRI_NB * TRI_NB;
   const Modulus mod = make_modulus(p);

@@ -236,8 +236,8 @@ __device__ __forceinline__ void epilogue_chunk<4>(uint32_t tcol, int gm, int gn0
 // integer count of the row/column bit products; its parity is the GF(2)
 // product.  The 256 columns of a tile are packed into four 64-bit
 // LittleEndian words (bit j of word w = column 64w + j) and combined as
-// C <- (beta ? C : 0) XOR (alpha ? A*B : 0); bits at columns >= N are
-// cleared.
+// C <- (beta ? C : 0) XOR (alpha ? A*B : 0); bits of the last word at
+// columns >= N keep their old values.
 __device__ __forceinline__ void epilogue_gf2(uint32_t tcol, int gm, int gn0, int M, int N,
                                              uint64_t *C, size_t ldc_words, uint32_t alpha,
                                              uint32_t beta, int cbeg, int cend) {
@@ -257,8 +257,10 @@ __device__ __forceinline__ void epilogue_gf2(uint32_t tcol, int gm, int gn0, int
         const int valid = min(64, N - wcol);
         const uint64_t mask = valid == 64 ? ~0ull : ((1ull << valid) - 1ull);
         uint64_t *dst = C + (size_t)gm * ldc_words + (wcol >> 6);
-        const uint64_t old = beta ? *dst : 0ull;
-        *dst = (old ^ (alpha ? word : 0ull)) & mask;
+        const bool part = valid < 64;
+        const uint64_t old = (beta || part) ? *dst : 0ull;
+        const uint64_t v = (beta ? old : 0ull) ^ (alpha ? word : 0ull);
+        *dst = (v & mask) | (old & ~mask);
       }
       word = 0;
     }
@@ -665,15 +667,8 @@ static int encode_3d(Ctx *c, CUtensorMap *tm, void *base, uint64_t d0, uint64_t 
 
 template <int L>
 static int tc_attr(Ctx *c) {
-  static std::once_flag once;
-  static cudaError_t attr_err = cudaSuccess;
-  std::call_once(once, [] {
-    attr_err = cudaFuncSetAttribute(zp_gemm_tc_kernel<L, 0>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    TcLayout<L>::SMEM);
-  });
-  return attr_err == cudaSuccess ? ST_OK
-                                 : ctx_cuda(c, attr_err, "cudaFuncSetAttribute(zp_gemm_tc)");
+  return ctx_smem_attr(c, (const void *)zp_gemm_tc_kernel<L, 0>, TcLayout<L>::SMEM,
+                       "cudaFuncSetAttribute(zp_gemm_tc)");
 }
 
 template <int L>
@@ -960,7 +955,10 @@ int zp_gemm_host_rows(Ctx *c, int M, int N, int K, uint32_t p, uint32_t alpha,
 //  - The first call on a device does its set-up there, with that device
 //    current: it looks up the array's device address with
 //    cudaGetSymbolAddress and sets the kernels' shared-memory attribute.
-//    Make that first call before any stream capture.
+//    Make that first call before any stream capture.  The set-up is kept
+//    for the life of the process, so the entry point must not be called
+//    after cudaDeviceReset (which unloads the module the address and the
+//    attributes belong to).
 namespace lela {
 
 constexpr size_t NOALLOC_STATUS_BYTES = 256;
@@ -1121,13 +1119,9 @@ int gf2_gemm_tc_planes(Ctx *c, int M, int N, int K, const uint8_t *Ab, const uin
                        uint32_t alpha, uint32_t beta, uint64_t *C, size_t ldc_words) {
   using Cfg = TcCfg<1>;
   using Lay = TcLayout<1>;
-  static std::once_flag once;
-  static cudaError_t attr_err = cudaSuccess;
-  std::call_once(once, [] {
-    attr_err = cudaFuncSetAttribute(zp_gemm_tc_kernel<1, 1>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, Lay::SMEM);
-  });
-  if (attr_err != cudaSuccess) return ctx_cuda(c, attr_err, "cudaFuncSetAttribute(gf2 tc)");
+  if (int st = ctx_smem_attr(c, (const void *)zp_gemm_tc_kernel<1, 1>, Lay::SMEM,
+                             "cudaFuncSetAttribute(gf2 tc)"))
+    return st;
   CUtensorMap tmA, tmB;
   int st = encode_3d(c, &tmA, const_cast<uint8_t *>(Ab), (uint64_t)K, (uint64_t)M, 1,
                      (uint64_t)Kp, (uint64_t)M * Kp, BK, BM, 1);

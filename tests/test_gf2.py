@@ -122,3 +122,39 @@ def test_gf2_echelon_blocks(cuda):
     want, wr = oracle.echelon_gf2(A, n)
     got, gr = cuda.echelonize_gf2(A.copy(), n)
     assert gr == wr and np.array_equal(got, want)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kernel", KERNELS)
+def test_gf2_gemm_strided_c_keeps_neighbour_bits(cuda, kernel):
+    """C is the first 100 columns of a 256-column matrix (row stride 4
+    words): the product lands in bits 0..99, and bits 100..255 of every row
+    -- the rest of the last word and the two words after it -- keep their
+    values, whatever b is.  Host and device paths."""
+    import torch
+    m, n, k = 150, 100, 333
+    A = gen.dense_gf2(5, m, k)
+    B = gen.dense_gf2(6, k, n)
+    W = gen.dense_gf2(7, m, 256)
+    cuda.set_gf2_kernel(kernel)
+    try:
+        for a, b in ((1, 1), (1, 0), (0, 0)):
+            Cn = np.ascontiguousarray(W[:, :2])
+            Cn[:, 1] &= np.uint64((1 << 36) - 1)          # columns 0..99 only
+            want = oracle.gemm_gf2(A, B, Cn, k, n, a, b)
+            tail = ~np.uint64((1 << 36) - 1)
+            want[:, 1] |= W[:, 1] & tail
+            for dev in (False, True):
+                Wc = W.copy()
+                if dev:
+                    Wt = torch.from_numpy(Wc.view(np.int64)).cuda()
+                    cuda.gemm_gf2(torch.from_numpy(A.view(np.int64)).cuda(),
+                                  torch.from_numpy(B.view(np.int64)).cuda(), Wt[:, :2], n, k, a, b)
+                    torch.cuda.synchronize()
+                    Wc = Wt.cpu().numpy().view(np.uint64)
+                else:
+                    cuda.gemm_gf2(A, B, Wc[:, :2], n, k, a, b)
+                assert np.array_equal(Wc[:, :2], want), (kernel, a, b, dev)
+                assert np.array_equal(Wc[:, 2:], W[:, 2:]), (kernel, a, b, dev)
+    finally:
+        cuda.set_gf2_kernel(0)
