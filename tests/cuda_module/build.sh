@@ -6,7 +6,7 @@
 set -e
 HERE=$(cd "$(dirname "$0")" && pwd)
 ROOT=$(cd "$HERE/../.." && pwd)
-REF=${REF:-/root/reference}
+REF=${REF:-$(cd "$ROOT/.." && pwd)/reference}
 if [ ! -d "$REF/lela" ]; then echo "reference tree not present; keeping prebuilt binary (if any)"; exit 0; fi
 mkdir -p "$HERE/_build"
 g++ -std=gnu++98 -O2 -fno-strict-aliasing -w \
