@@ -58,11 +58,20 @@ def parse():
     ap.add_argument("--no-fl", action="store_true")
     ap.add_argument("--fl-only", action="store_true",
                     help="run only the Faugere-Lachartre line (profiling aid)")
+    ap.add_argument("--gemm-only", metavar="M,N,K",
+                    help="time only a Z/p gemm of this shape on the tensor cores (profiling aid)")
+    ap.add_argument("--gemm-p", type=int, default=P)
+    ap.add_argument("--gemm-tile", type=int, default=0,
+                    help="tile variant for --gemm-only: 0 auto, 1 wide, 2 two accumulator buffers")
     ap.add_argument("--fl-m", type=int, default=20000)
     ap.add_argument("--fl-count", type=int, default=3)
+    ap.add_argument("--no-fl-check", action="store_true",
+                    help="skip the reduced-echelon certificate of the last timed FL matrix")
+    ap.add_argument("--no-dense", action="store_true",
+                    help="skip the p = 2^31-1 gemm, trsm and dense echelon lines")
     ap.add_argument("--no-gf2", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
-    ap.add_argument("--batch-fl", type=int, default=12)
+    ap.add_argument("--batch-fl", type=int, default=16)
     ap.add_argument("--batch-dense", type=int, default=48)
     ap.add_argument("--gf2-n", type=int, default=16384)
     ap.add_argument("--gf2-ech-n", type=int, default=32768)
@@ -127,6 +136,60 @@ class ClockSampler:
                 "samples": len(rows), "samples_under_load": len(load)}
 
 
+class NvmlClockSampler:
+    """SM clock, power and clock-event reasons of this process's GPU read
+    through NVML every 5 ms from a thread (read-only queries), so that even
+    a timed region of a few tens of milliseconds gets samples.  The GPU is
+    found by its UUID; raises when NVML or the UUID is unavailable."""
+
+    def __init__(self, torch, dev):
+        import pynvml
+        self.nv = pynvml
+        pynvml.nvmlInit()
+        uuid = str(torch.cuda.get_device_properties(dev).uuid)
+        if not uuid.startswith("GPU-"):
+            uuid = "GPU-" + uuid
+        self.h = pynvml.nvmlDeviceGetHandleByUUID(uuid.encode() if isinstance(uuid, str) else uuid)
+        self.smax = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+        self.rows = []
+        self.stop_ev = threading.Event()
+        self.th = threading.Thread(target=self._run, daemon=True)
+        self.th.start()
+
+    def _run(self):
+        nv = self.nv
+        while not self.stop_ev.is_set():
+            try:
+                self.rows.append((nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM),
+                                  nv.nvmlDeviceGetPowerUsage(self.h) / 1000.0,
+                                  nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)))
+            except Exception:
+                pass
+            time.sleep(0.005)
+
+    def stop(self):
+        self.stop_ev.set()
+        self.th.join(timeout=2)
+        nv = self.nv
+        names = ((nv.nvmlClocksEventReasonHwSlowdown, "hw_slowdown"),
+                 (nv.nvmlClocksEventReasonHwThermalSlowdown, "hw_thermal_slowdown"),
+                 (nv.nvmlClocksEventReasonSwThermalSlowdown, "sw_thermal_slowdown"),
+                 (nv.nvmlClocksEventReasonSwPowerCap, "sw_power_cap"))
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": self.smax, "reasons": ["unsampled"]}
+        reasons = sorted({name for _, _, r in self.rows for bit, name in names if r & bit})
+        return {"sm_mhz": statistics.median(s for s, _, _ in self.rows), "sm_max_mhz": self.smax,
+                "reasons": reasons, "samples": len(self.rows),
+                "power_w_max": round(max(w for _, w, _ in self.rows), 1), "source": "NVML, 5 ms"}
+
+
+def clock_sampler(torch, dev, index):
+    try:
+        return NvmlClockSampler(torch, dev)
+    except Exception:
+        return ClockSampler(index)
+
+
 # --------------------------------------------------------------- helpers
 def max_over_ranks(torch, value, dev, world):
     """The slowest rank's time: MAX all-reduce over the process group (NCCL
@@ -172,6 +235,16 @@ def int8_peak_tops(torch, dev):
             return 2 * 1590.0, "2 x fallback bf16 1.59 PFLOP/s"
 
 
+def _hbm_peak():
+    """HBM copy bandwidth measured on this pool (MEASURED_PEAKS.json), else
+    the stated fallback."""
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        return float(peaks["hbm_gbs"]), "MEASURED_PEAKS.json hbm_gbs (measured)"
+    except Exception:
+        return 6650.0, "fallback 6.65 TB/s (MEASURED_PEAKS.json absent)"
+
+
 def cpu_baseline(n, threads):
     """LELA's own CPU gemm on a bounded sample: rows 0..r-1 of the n^3
     workload, ZpModule gemm row-sliced over all host threads."""
@@ -198,7 +271,34 @@ def cpu_baseline(n, threads):
 FL_DENSITY = 0.025
 
 
-def run_fl(args, cm, stream, torch, dev, rank):
+def fl_structure(X):
+    """Pivot structure of an F4 matrix as FaugereLachartre splits it
+    (setup_splicer, faugere-lachartre.tcc:47-146): pivot rows/columns and the
+    off-diagonal nonzeros of the pivot block A."""
+    heads = X.colidx[X.rowptr[:-1].astype(np.int64)].astype(np.int64)
+    piv = np.concatenate([[True], heads[1:] > heads[:-1]])
+    is_pc = np.zeros(X.n, dtype=bool)
+    is_pc[heads[piv]] = True
+    rows = np.repeat(np.arange(X.m), np.diff(X.rowptr).astype(np.int64))
+    in_a = piv[rows] & is_pc[X.colidx.astype(np.int64)]
+    npiv = int(piv.sum())
+    return npiv, int(in_a.sum()) - npiv
+
+
+def fl_algorithmic_ops(m, n, npiv, nnz_off_a, rank):
+    """Z/p operations of one reduced FL echelonization (multiply and add
+    counted separately): the sparse triangular solve 2 nnz_off(A) (n - npiv),
+    the Schur complement 2 (m - npiv) npiv (n - npiv), the echelon form of D
+    (mres x nres, rank r) 2 (mres nres r - (mres + nres) r^2 / 2 + r^3 / 3),
+    and the back-substitution r^2 (nres - r) + 2 npiv r (nres - r)."""
+    mres, nres, r = m - npiv, n - npiv, rank - npiv
+    parts = {"trsm": 2.0 * nnz_off_a * nres, "schur": 2.0 * mres * npiv * nres,
+             "echelon": 2.0 * (mres * nres * r - (mres + nres) * r * r / 2.0 + r ** 3 / 3.0),
+             "reduce": float(r) * r * (nres - r) + 2.0 * npiv * r * (nres - r)}
+    return parts
+
+
+def run_fl(args, cm, stream, torch, dev, rank, zp_peak=None):
     """FaugereLachartre::echelonize (reduced) on F4-shaped matrices over
     Z/65521: m rows, n = 1.2 m columns, 75% pivot rows, row density 2.5%,
     5% of the non-pivot rows dependent.  The CSR input and the dense output
@@ -215,8 +315,9 @@ def run_fl(args, cm, stream, torch, dev, rank):
     mats = []
     for s in range(args.fl_count):
         X = gen.f4_matrix(1000 + 17 * rank + s, m, P, density=FL_DENSITY)
+        npiv, nnz_off = fl_structure(X)
         T = types.SimpleNamespace(
-            m=X.m, n=X.n, nnz=X.nnz,
+            m=X.m, n=X.n, nnz=X.nnz, host=X, npiv=npiv, nnz_off=nnz_off,
             rowptr=torch.from_numpy(X.rowptr.view(np.int64)).to(dev),
             colidx=torch.from_numpy(X.colidx.view(np.int32)).to(dev),
             vals=torch.from_numpy(X.vals.view(np.int32)).to(dev))
@@ -249,6 +350,27 @@ def run_fl(args, cm, stream, torch, dev, rank):
     cm.profile(False)
     res.update({"ms_per_matrix": round(sum(times) / len(times), 2), "ms_each": [round(t, 2) for t in times],
                 "ranks": ranks, "phase_ms": phases, "nnz": [T.nnz for T in mats]})
+    # roofline of the whole matrix and of its phases: algorithmic Z/p
+    # operations over the time, against the two-limb Z/p peak (int8 peak / 4)
+    ops = [fl_algorithmic_ops(T.m, T.n, T.npiv, T.nnz_off, rk) for T, rk in zip(mats, ranks)]
+    tot = [sum(o.values()) for o in ops]
+    res["algorithmic_ops"] = {k: "%.3e" % ops[0][k] for k in ops[0]}
+    res["Zp_Top_s"] = round(sum(tot) / (sum(times) / 1e3) / 1e12, 2)
+    if zp_peak:
+        res["roofline"] = {"bound": "tensor", "peak_Zp_Top_s": round(zp_peak, 1),
+                           "frac": round(res["Zp_Top_s"] / zp_peak, 4),
+                           "phase_frac": {k: round(ops[0][k] / (phases[k] / 1e3) / 1e12 / zp_peak, 4)
+                                          for k in phases if phases[k] > 0},
+                           "counting": "fl_algorithmic_ops (trsm counted on the sparse A)"}
+    if not args.no_fl_check:
+        # the last timed matrix's output is still in R
+        from lela_b200 import certify
+        T = mats[-1]
+        err = certify.rref_certificate(torch, P, T.host, R[:T.m], ranks[-1])
+        res["checked"] = err is None
+        res["check"] = ("reduced-echelon certificate of matrix %d (echelon structure exact; "
+                        "row space by 2 random projections, error <= p^-2)" % (len(mats) - 1)
+                        + ("" if err is None else ": FAILED " + err))
     if not args.no_plain:
         cm.set_gemm_kernel(1)
         t, rk, _ = timed(mats[0])
@@ -259,7 +381,99 @@ def run_fl(args, cm, stream, torch, dev, rank):
     return res
 
 
-def run_gf2(args, cm, stream, torch, dev):
+def _event_ms(torch, stream, fn, reps):
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def run_dense(args, cm, stream, torch, dev, int8_peak):
+    """The other dense workloads, inputs resident in HBM, CUDA events on the
+    module's stream:
+    * gemm 8192^3 at p = 2^31 - 1 (four limbs: 16 limb products per output);
+    * trsm with the 8192 x 8192 unit-lower L (uniform off-diagonal entries)
+      and an 8192 x 4096 right-hand side, at p = 65521 and 2^31 - 1;
+    * the row-echelon form of a dense 8192 x 8192 matrix over Z/65521.
+    Each with its roofline: algorithmic Z/p operations per second against
+    the Z/p peak of its limb count (the int8 peak measured in this run /
+    limbs^2)."""
+    from lela_b200 import gen
+    n = 8192
+    out = {}
+    p31 = 2147483647
+    dA = torch.from_numpy(gen.dense_zp(21, n, n, p31).view(np.int32)).to(dev)
+    dB = torch.from_numpy(gen.dense_zp(22, n, n, p31).view(np.int32)).to(dev)
+    dC = torch.from_numpy(gen.dense_zp(23, n, n, p31).view(np.int32)).to(dev)
+    cm.gemm(p31, 1, dA, dB, 1, dC)
+    cm.profile_reset()
+    cm.profile(True)
+    ms = _event_ms(torch, stream, lambda: cm.gemm(p31, 1, dA, dB, 1, dC), 5)
+    tc_ms, tc_n = cm.profile_read("zp_gemm_tc")
+    cm.profile(False)
+    cm.synchronize()
+    kern = tc_ms / max(tc_n, 1)
+    zp = 2.0 * n ** 3 / (ms / 1e3) / 1e12
+    out["gemm_p31"] = {"workload": "gemm Z/2147483647 8192^3 C<-A*B+C", "ms": round(ms, 3),
+                       "Gop_s": round(zp * 1e3, 1), "limbs": 4,
+                       "roofline": {"bound": "tensor", "kernel": "zp_gemm_tc_kernel<4>",
+                                    "kernel_ms": round(kern, 3),
+                                    "achieved_int8_Tops": round(16 * 2.0 * n ** 3 / (kern / 1e3) / 1e12, 1),
+                                    "peak_int8_Tops": round(int8_peak, 1),
+                                    "frac": round(16 * 2.0 * n ** 3 / (kern / 1e3) / 1e12 / int8_peak, 4)}}
+    del dA, dB, dC
+    # trsm, both moduli
+    out["trsm"] = {}
+    for p, L in ((65521, 2), (p31, 4)):
+        Lm = torch.from_numpy(gen.unit_lower_zp(31, n, p).view(np.int32)).to(dev)
+        B0 = torch.from_numpy(gen.dense_zp(32, n, n // 2, p).view(np.int32)).to(dev)
+        B = B0.clone()
+        cm.trsm(p, 1, Lm, B, False, True)
+        times = []
+        for _ in range(3):
+            B.copy_(B0)
+            times.append(_event_ms(torch, stream, lambda: cm.trsm(p, 1, Lm, B, False, True), 1))
+        ms = min(times)
+        ops = float(n) * n * (n // 2)
+        peak = int8_peak / (L * L)
+        out["trsm"][str(p)] = {"workload": "trsm 8192x8192 unit-lower, 8192x4096 RHS, p=%d" % p,
+                               "ms": round(ms, 3), "Zp_Top_s": round(ops / (ms / 1e3) / 1e12, 2),
+                               "roofline": {"bound": "tensor", "peak_Zp_Top_s": round(peak, 1),
+                                            "frac": round(ops / (ms / 1e3) / 1e12 / peak, 4),
+                                            "counting": "m^2 n Z/p operations (triangle, multiply and add)"}}
+        del Lm, B0, B
+    # dense echelon form
+    E0 = torch.from_numpy(gen.dense_zp(33, n, n, P).view(np.int32)).to(dev)
+    E = E0.clone()
+    cm.echelonize(P, E)
+    times, rk = [], None
+    for _ in range(3):
+        E.copy_(E0)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        _, rk, _ = cm.echelonize(P, E)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    ms = min(times)
+    r = rk
+    ops = 2.0 * (n * n * r - (n + n) * r * r / 2.0 + r ** 3 / 3.0)
+    out["echelon"] = {"workload": "row-echelon form, dense 8192x8192 over Z/65521 (LELA pivot rule)",
+                      "ms": round(ms, 3), "rank": rk, "Zp_Top_s": round(ops / (ms / 1e3) / 1e12, 2),
+                      "roofline": {"bound": "tensor", "peak_Zp_Top_s": round(int8_peak / 4, 1),
+                                   "frac": round(ops / (ms / 1e3) / 1e12 / (int8_peak / 4), 4),
+                                   "counting": "2 (m n r - (m + n) r^2 / 2 + r^3 / 3)"}}
+    del E0, E
+    torch.cuda.empty_cache()
+    return out
+
+
+def run_gf2(args, cm, stream, torch, dev, int8_peak=None):
     """GF(2) workloads: packed gemm 16384^3 with Bernoulli(1/2) bits on both
     kernels (int8-expanded tensor cores, bit-packed four-Russians), and the
     echelon form of a 32768 x 32768 matrix of planted rank 30000 (product of
@@ -292,6 +506,16 @@ def run_gf2(args, cm, stream, torch, dev):
         res["gemm_%s_ms" % name] = round(ms, 3)
         res["gemm_%s_Tbitop_s" % name] = round(2.0 * n ** 3 / (ms / 1e3) / 1e12, 1)
     cm.set_gf2_kernel(0)
+    if int8_peak:
+        # one int8 multiply-add per bit product on the tensor cores; the
+        # packed operands and result are 3 n^2 / 8 bytes (HBM fraction of the
+        # algorithmic bytes against the copy bandwidth, for reference)
+        hbm = _hbm_peak()
+        res["roofline"] = {"bound": "tensor", "frac_tc": round(res["gemm_tc_Tbitop_s"] / int8_peak, 4),
+                           "peak_int8_Tops": round(int8_peak, 1),
+                           "hbm_frac_tc": round(3 * n * n / 8 / (res["gemm_tc_ms"] / 1e3) / 1e9 / hbm[0], 5),
+                           "hbm_frac_m4rm": round(3 * n * n / 8 / (res["gemm_m4rm_ms"] / 1e3) / 1e9 / hbm[0], 5),
+                           "hbm_peak_GBs": hbm[0], "hbm_peak_source": hbm[1]}
     del A, B, C
     # planted-rank echelon
     m, r = args.gf2_ech_n, args.gf2_ech_rank
@@ -310,73 +534,95 @@ def run_gf2(args, cm, stream, torch, dev):
     _, rank = cm.echelonize_gf2(D, m)
     e1.record(stream)
     cm.synchronize()
+    ems = e0.elapsed_time(e1)
+    ops = 2.0 * (m * m * rank - (m + m) * rank * rank / 2.0 + rank ** 3 / 3.0)
     res.update({"echelon_workload": "GF(2) echelon %d x %d, planted rank %d" % (m, m, r),
-                "echelon_ms": round(e0.elapsed_time(e1), 2), "echelon_rank": rank})
+                "echelon_ms": round(ems, 2), "echelon_rank": rank,
+                "echelon_Tbitop_s": round(ops / (ems / 1e3) / 1e12, 1)})
+    if int8_peak:
+        res["echelon_frac_tc"] = round(ops / (ems / 1e3) / 1e12 / int8_peak, 4)
     del D
     return res
 
 
 def run_batch(args, cm, stream, torch, dev):
-    """Batched workload (scaled to minutes): F4-shaped FL matrices with m
-    log-uniform in [2000, 8000] plus dense Z/p echelon blocks of sizes
+    """Batched workload: F4 matrices of the FL family (m uniform in
+    [20000, 24000], n = 1.2 m, density 2.5 %, p = 65521; the vectorised
+    generator gen.f4_matrix_fast) plus dense Z/p echelon blocks of sizes
     log-uniform in [64, 4096], p in {251, 65521, 2^31-1}.
     * ours: the FL matrices through the batched entry point (8 worker
       streams, tensor-core gemms) and the dense blocks through one batched
-      call whose kernel per block is chosen by the MLP cost model, trained
-      first on autotuner timings of a separate set of blocks (small blocks in
-      one persistent graph launch, the others over worker streams);
-    * plain: the per-matrix pipeline -- one matrix per call, one at a time on
-      one stream, with every gemm on the CUDA-core kernel and every dense
-      block through the panel pipeline."""
+      call whose kernel and tile variant per block are chosen by the MLP
+      cost model, trained first on autotuner timings of a separate set of
+      blocks (small blocks in one persistent graph launch, the others over
+      worker streams); both batches are stream-ordered on CUDA streams and
+      timed by CUDA events around them;
+    * per-matrix tensor cores: the same matrices and blocks one call at a
+      time on one stream, tensor-core gemms (the batching gain alone);
+    * plain: the per-matrix pipeline with every gemm on the CUDA-core kernel
+      and every dense block through the panel pipeline with CUDA-core
+      updates.
+    The selector's regret is measured on this batch's own dense blocks
+    (every candidate timed)."""
     import types
     from lela_b200 import gen
     from lela_b200 import selector as sel
     rng = np.random.default_rng(11)
     primes = [251, 65521, 2147483647]
     fl_items = []
+    t_gen = time.perf_counter()
     for i in range(args.batch_fl):
-        m = int(2 ** rng.uniform(math.log2(2000), math.log2(8000)))
-        X = gen.f4_matrix(3000 + i, m, P, density=FL_DENSITY)
+        m = int(rng.integers(20000, 24001))
+        X = gen.f4_matrix_fast(3000 + i, m, P, density=FL_DENSITY)
         fl_items.append(types.SimpleNamespace(
             m=X.m, n=X.n, rowptr=torch.from_numpy(X.rowptr.view(np.int64)).to(dev),
             colidx=torch.from_numpy(X.colidx.view(np.int32)).to(dev),
             vals=torch.from_numpy(X.vals.view(np.int32)).to(dev)))
+    t_gen = time.perf_counter() - t_gen
     dense = []
     for i in range(args.batch_dense):
-        s = int(2 ** rng.uniform(6, 12))
+        s_ = int(2 ** rng.uniform(6, 12))
         p = int(rng.choice(primes))
-        dense.append((torch.from_numpy(gen.dense_zp(4000 + i, s, s, p).view(np.int32)).to(dev), p))
+        dense.append((torch.from_numpy(gen.dense_zp(4000 + i, s_, s_, p).view(np.int32)).to(dev), p, s_, 4000 + i))
     Rs = [torch.empty((X.m, X.n), dtype=torch.int32, device=dev) for X in fl_items]
-    work = [torch.empty_like(A) for A, _ in dense]
+    work = [torch.empty_like(A) for A, _, _, _ in dense]
 
     # cost model from autotuner timings on separate blocks
     t0 = time.perf_counter()
     tuner = sel.Autotuner(cm, reps=2)
-    for i in range(24):
-        s = int(2 ** rng.uniform(6, 12))
-        tuner.tune_echelon(s, s, int(rng.choice(primes)), seed=9000 + i)
-    X, y = sel.records_to_xy(tuner.records)
+    for i in range(32):
+        s_ = int(2 ** rng.uniform(6, 12))
+        tuner.tune_echelon(s_, s_, int(rng.choice(primes)), seed=9000 + i)
+    X_, y_ = sel.records_to_xy(tuner.records)
     model = sel.CostModel(cm, seed=1)
-    model.fit(X, y, epochs=600)
+    model.fit(X_, y_, epochs=800)
     choose = sel.Selector(model)
-    kernels = [choose.choose("echelon", A.shape[0], A.shape[1], 0, 1.0, p.bit_length(), A.shape[0])
-               for A, p in dense]
+    kernels = [choose.choose("echelon", s_, s_, 0, 1.0, p.bit_length(), s_) for _, p, s_, _ in dense]
     tune_s = time.perf_counter() - t0
+    # the selector's regret on this batch's blocks: every candidate timed
+    judge = sel.Autotuner(cm, reps=2)
+    for _, p, s_, seed in dense:
+        judge.tune_echelon(s_, s_, p, seed=seed)
+    res_sel = sel.evaluate(choose, sel.group_blocks(judge.records))
 
-    # the dense blocks go through a second handle from a second host thread,
-    # concurrently with the FL batch (a handle serves one thread at a time)
     from lela_b200 import CudaModule
     cm_dense = CudaModule(torch.cuda.current_device())
+    s2 = torch.cuda.Stream(device=dev)
+    cm_dense.set_stream(s2)
 
     def ours():
-        for w, (A, _) in zip(work, dense):
+        for w, (A, _, _, _) in zip(work, dense):
             w.copy_(A)
-        torch.cuda.synchronize()  # the copies are done before another stream reads them
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        s2.wait_event(e0)
         failed = []
 
         def dense_part():
             try:
-                cm_dense.echelonize_batch(work, [p for _, p in dense], kernels)
+                cm_dense.echelonize_batch(work, [p for _, p, _, _ in dense], kernels)
             except BaseException as e:  # re-raised on the calling thread
                 failed.append(e)
 
@@ -388,40 +634,51 @@ def run_batch(args, cm, stream, torch, dev):
             th.join()
         if failed:
             raise failed[0]
+        stream.wait_stream(s2)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
 
-    def plain():
-        for w, (A, _) in zip(work, dense):
+    def one_at_a_time(gemm_kernel, dense_kernel):
+        for w, (A, _, _, _) in zip(work, dense):
             w.copy_(A)
-        cm.set_gemm_kernel(1)
+        torch.cuda.synchronize()
+        cm.set_gemm_kernel(gemm_kernel)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
         try:
+            e0.record(stream)
             for X, R in zip(fl_items, Rs):
                 cm.fl_echelonize(P, X, True, False, R=R)
-            for w, (_, p) in zip(work, dense):
-                cm.echelonize_batch([w], [p], [3])
+            for w, (_, p, _, _) in zip(work, dense):
+                cm.echelonize_batch([w], [p], [dense_kernel])
+            e1.record(stream)
+            torch.cuda.synchronize()
         finally:
             cm.set_gemm_kernel(0)
-
-    def timed(fn):
-        torch.cuda.synchronize()
-        cm.synchronize()
-        t = time.perf_counter()
-        fn()
-        cm.synchronize()
-        torch.cuda.synchronize()
-        return (time.perf_counter() - t) * 1e3
+        return e0.elapsed_time(e1)
 
     ours()
-    t_ours = min(timed(ours) for _ in range(4))
-    plain()
-    t_plain = timed(plain)
-    return {"workload": "%d F4 matrices (m log-uniform 2000-8000, p=65521) + %d dense echelon blocks "
-                        "(64-4096, p in {251, 65521, 2^31-1})" % (len(fl_items), len(dense)),
-            "unit": "ms/batch", "ms": round(t_ours, 1), "plain_ms": round(t_plain, 1),
-            "speedup_vs_plain": round(t_plain / t_ours, 2),
-            "selector": {"kernels": {str(k): kernels.count(k) for k in sorted(set(kernels))},
+    t_ours = min(ours() for _ in range(3))
+    t_tc = one_at_a_time(0, 2)
+    t_plain = one_at_a_time(1, 3)
+    cm_dense.close()
+    ms_ = [X.m for X in fl_items]
+    return {"workload": "%d F4 matrices (m uniform 20000-24000, n = 1.2 m, density 2.5%%, p=65521) + %d dense "
+                        "echelon blocks (64-4096 log-uniform, p in {251, 65521, 2^31-1})"
+                        % (len(fl_items), len(dense)),
+            "unit": "ms/batch", "ms": round(t_ours, 1),
+            "per_matrix_tc_ms": round(t_tc, 1), "batching_gain": round(t_tc / t_ours, 2),
+            "plain_ms": round(t_plain, 1), "speedup_vs_plain": round(t_plain / t_ours, 2),
+            "fl_m": ms_, "generation_s": round(t_gen, 1),
+            "selector": {"kernels": {sel.KERNEL_NAMES[("echelon", k)]: kernels.count(k) for k in sorted(set(kernels))},
                          "tuning_and_training_s": round(tune_s, 1),
-                         "names": {str(k): sel.KERNEL_NAMES[("echelon", k)] for k in (1, 2, 3)}},
-            "timing": "host wall clock around the synchronised batch (includes host orchestration)"}
+                         "regret_on_batch": round(res_sel["regret"], 4),
+                         "gain_vs_default_on_batch": round(res_sel["gain_vs_default"], 4),
+                         "exhaustive_ms": round(res_sel["exhaustive_ms"], 2),
+                         "selector_ms": round(res_sel["selector_ms"], 2)},
+            "timing": "CUDA events on the handle's stream around the stream-ordered batch calls (the FL "
+                      "workers and the dense blocks' second stream joined to it); best of 3"}
 
 
 def fl_cpu_baseline(m_target):
@@ -531,7 +788,7 @@ def run_ours(args):
         torch.distributed.barrier()
     torch.cuda.synchronize()
 
-    clocks = ClockSampler(local)
+    clocks = clock_sampler(torch, dev, local)
     cm.profile_reset()
     cm.profile(True)
     launches0 = cm.launch_count
@@ -613,10 +870,12 @@ def run_ours(args):
                       "ms_per_step": round(te * 1e3, 3),
                       "api": "lela_cuda_gemm_zp_u32 (host pointers, pinned)"}
 
+    if not args.no_dense:
+        out["dense"] = run_dense(args, cm, stream, torch, dev, peak)
     if not args.no_fl:
-        out["fl"] = run_fl(args, cm, stream, torch, dev, rank)
+        out["fl"] = run_fl(args, cm, stream, torch, dev, rank, zp_peak=peak / 4)
     if not args.no_gf2:
-        out["gf2"] = run_gf2(args, cm, stream, torch, dev)
+        out["gf2"] = run_gf2(args, cm, stream, torch, dev, peak)
     if not args.no_batch:
         out["batch"] = run_batch(args, cm, stream, torch, dev)
 
@@ -641,13 +900,49 @@ def run_fl_only(args):
     cm = CudaModule(0)
     stream = torch.cuda.Stream(device=dev)
     cm.set_stream(stream)
-    print(json.dumps(run_fl(args, cm, stream, torch, dev, 0)))
+    print(json.dumps(run_fl(args, cm, stream, torch, dev, 0, zp_peak=int8_peak_tops(torch, dev)[0] / 4)))
+
+
+def run_gemm_only(args):
+    """One Z/p gemm shape C <- C - A*B (the update form of the triangular
+    solve and the elimination) on the tensor-core kernel, inputs resident:
+    `steps` launches after `warmup`, CUDA events; prints one JSON object
+    (for kernel launch lists and profiles of a given shape)."""
+    import torch
+    from lela_b200 import CudaModule, gen
+    m, n, k = (int(x) for x in args.gemm_only.split(","))
+    p = args.gemm_p
+    dev = torch.device("cuda", 0)
+    cm = CudaModule(0)
+    stream = torch.cuda.Stream(device=dev)
+    cm.set_stream(stream)
+    cm.set_gemm_kernel(2)
+    cm.set_gemm_tile(args.gemm_tile)
+    t = lambda x: torch.from_numpy(x.view(np.int32)).to(dev)
+    dA, dB, dC = t(gen.dense_zp(1, m, k, p)), t(gen.dense_zp(2, k, n, p)), t(gen.dense_zp(3, m, n, p))
+    for _ in range(max(1, args.warmup)):
+        cm.gemm(p, p - 1, dA, dB, 1, dC)
+    cm.synchronize()
+    cm.profile_reset()
+    cm.profile(True)
+    ms = _event_ms(torch, stream, lambda: cm.gemm(p, p - 1, dA, dB, 1, dC), args.steps)
+    kms, kn = cm.profile_read("zp_gemm_tc")
+    cm.profile(False)
+    L = 1 if p <= 256 else (2 if p <= 65536 else 4)
+    kavg = kms / max(kn, 1)
+    print(json.dumps({"workload": "gemm C <- C - A*B, %dx%dx%d, p=%d" % (m, n, k, p), "tile": args.gemm_tile,
+                      "ms_per_gemm": round(ms, 4), "kernel_ms": round(kavg, 4),
+                      "int8_Tops": round(L * L * 2.0 * m * n * k / (kavg / 1e3) / 1e12, 1),
+                      "c_GBs": round(8.0 * m * n / (kavg / 1e3) / 1e9, 1)}))
+    cm.close()
 
 
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.gemm_only:
+        run_gemm_only(args)
     elif args.fl_only:
         run_fl_only(args)
     else:

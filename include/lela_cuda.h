@@ -80,6 +80,14 @@ void *lela_cuda_get_stream (lela_cuda_ctx *ctx);
  * kernel recorded (e.g. LELA_CUDA_ERR_TIMEOUT). */
 int lela_cuda_synchronize (lela_cuda_ctx *ctx);
 int lela_cuda_set_gemm_kernel (lela_cuda_ctx *ctx, int kernel);
+/* Tile variant of the tensor-core Z/p gemm: 0 = automatic (variant 1 for
+ * K <= 1024, else variant 0), 1 = variant 0 (wide tiles: 256 / 128 / 32
+ * columns for 1 / 2 / 4 limbs), 2 = variant 1 (128 / 64 columns for 1 / 2
+ * limbs with two TMEM accumulator buffers, so the epilogue of one tile
+ * overlaps the products of the next; four limbs always use variant 0).
+ * Every variant gives the same result.  No counterpart in the reference
+ * (a tuning knob of the GPU kernels). */
+int lela_cuda_set_gemm_tile (lela_cuda_ctx *ctx, int tile);
 const char *lela_cuda_status_string (int status);
 const char *lela_cuda_last_error (lela_cuda_ctx *ctx);
 /* Number of SMs of the handle's device. */
@@ -254,8 +262,10 @@ int lela_cuda_echelon_gf2_dev (lela_cuda_ctx *ctx, size_t m, size_t n, uint64_t 
  * host.  kernel[i] (or NULL = all 0): 0 = automatic (blocks that fit one
  * CTA's shared memory go to the batched kernel, the rest to the panel
  * pipeline with tensor-core updates), 1 = batched shared-memory kernel,
- * 2 = panel pipeline with tensor-core updates, 3 = panel pipeline with
- * CUDA-core updates.  The shared-memory blocks are processed by one
+ * 2 = panel pipeline with tensor-core updates (wide tiles), 3 = panel
+ * pipeline with CUDA-core updates, 4 = panel pipeline with tensor-core
+ * updates on tiles with two accumulator buffers (see
+ * lela_cuda_set_gemm_tile).  The shared-memory blocks are processed by one
  * persistent launch captured in a CUDA graph (the instantiated graph is kept
  * in the handle and replayed while the count of such blocks stays the same);
  * when two or more blocks take the panel pipeline they are spread over up to
@@ -273,7 +283,9 @@ int lela_cuda_echelon_zp_u32_batch (lela_cuda_ctx *ctx, size_t count, uint32_t *
  * the budget together (estimate per matrix: 4 m n + 4 (m + n) m + 2 KB per
  * row + 256 MB), a matrix starts only when its estimate fits beside those
  * running (one that does not fit even alone runs alone), and each worker
- * frees its device buffers after a matrix. */
+ * frees its device buffers after a matrix.  The batch is stream-ordered on
+ * the handle's stream: the workers start after the work queued there, and
+ * work queued there after the call starts after the batch. */
 /* Budget of that queue in bytes; 0 (the default) = 90 % of the free device
  * memory at the call plus what the worker handles already hold. */
 int lela_cuda_set_batch_memory_budget (lela_cuda_ctx *ctx, size_t bytes);

@@ -26,6 +26,7 @@ _I = ctypes.c_int
 
 OK, ERR_ARG, ERR_CUDA, ERR_NOMEM, DIAG, WRONG_FORM, PIVOT, TIMEOUT, UNSUPPORTED = range(9)
 GEMM_AUTO, GEMM_PLAIN, GEMM_TC, GEMM_SMALLK = 0, 1, 2, 3
+GEMM_TILE_AUTO, GEMM_TILE_WIDE, GEMM_TILE_DOUBLE = 0, 1, 2
 TRSM_AUTO, TRSM_BLOCKS, TRSM_INVERSE = 0, 1, 2
 
 
@@ -125,6 +126,7 @@ def _bind_optional(L):
         "lela_cuda_echelon_gf2": [_P, _S, _S, _P, _S, ctypes.POINTER(_S)],
         "lela_cuda_echelon_gf2_dev": [_P, _S, _S, _P, _S, ctypes.POINTER(_S)],
         "lela_cuda_set_gf2_kernel": [_P, _I],
+        "lela_cuda_set_gemm_tile": [_P, _I],
         "lela_cuda_set_trsm_kernel": [_P, _I],
         "lela_cuda_set_batch_memory_budget": [_P, _S],
     }
@@ -201,6 +203,12 @@ class CudaModule:
         self._raise(self.L.lela_cuda_set_gemm_kernel(self.h, int(kernel)))
 
     @property
+    def set_gemm_tile(self, tile):
+        """Tensor-core tile variant: 0 = automatic, 1 = wide tiles (one
+        accumulator buffer), 2 = narrower tiles with two accumulator buffers
+        (one and two limbs).  Results do not depend on it."""
+        self._raise(self.L.lela_cuda_set_gemm_tile(self.h, int(tile)))
+
     def num_sms(self):
         return self.L.lela_cuda_num_sms(self.h)
 

@@ -301,6 +301,12 @@ int lela_cuda_set_gemm_kernel(lela_cuda_ctx *h, int kernel) {
   return ST_OK;
 }
 
+int lela_cuda_set_gemm_tile(lela_cuda_ctx *h, int tile) {
+  if (!h || tile < GEMM_TILE_AUTO || tile > GEMM_TILE_DOUBLE) return ST_ARG;
+  h->c.gemm_tile = tile;
+  return ST_OK;
+}
+
 const char *lela_cuda_status_string(int s) {
   switch (s) {
     case ST_OK: return "ok";
@@ -621,19 +627,21 @@ int lela_cuda_echelon_zp_u32_batch(lela_cuda_ctx *h, size_t count, uint32_t *con
     c->batch_status = d_status;
   }
   // big items: the panel pipeline, with the trailing-update gemm chosen per
-  // item (kernel 3: CUDA cores, else tensor cores); largest first over the
-  // workers when there are several
+  // item (kernel 3: CUDA cores; 4: tensor cores, two-accumulator tiles;
+  // else tensor cores, wide tiles); largest first over the workers when
+  // there are several
   std::vector<size_t> order(big_idx);
   std::sort(order.begin(), order.end(),
             [&](size_t a, size_t b) { return m[a] * n[a] > m[b] * n[b]; });
   std::atomic<size_t> next(0);
   std::atomic<int> fatal(0);
   auto run = [&](Ctx *wc) {
-    const int saved = wc->gemm_kernel;
+    const int saved = wc->gemm_kernel, saved_tile = wc->gemm_tile;
     for (size_t j = next++; j < order.size() && !fatal.load(); j = next++) {
       const size_t i = order[j];
       const int k = kernel ? kernel[i] : 0;
       wc->gemm_kernel = (k == 3) ? GEMM_PLAIN : GEMM_TC;
+      wc->gemm_tile = (k == 4) ? GEMM_TILE_DOUBLE : (k == 2 ? GEMM_TILE_WIDE : GEMM_TILE_AUTO);
       size_t r = 0;
       uint32_t d = 1;
       int s = zp_echelon_dev(wc, (int)m[i], (int)n[i], p[i], A[i], lda[i], &r, &d, nullptr);
@@ -648,6 +656,7 @@ int lela_cuda_echelon_zp_u32_batch(lela_cuda_ctx *h, size_t count, uint32_t *con
       status[i] = s;
     }
     wc->gemm_kernel = saved;
+    wc->gemm_tile = saved_tile;
   };
   if (nworkers > 1) {
     std::vector<std::thread> th;
@@ -888,9 +897,16 @@ int lela_cuda_fl_echelonize_zp_u32_batch(lela_cuda_ctx *h, size_t count, const s
     w->c.trsm_kernel = c->trsm_kernel;
     h->workers.push_back(w);
   }
-  // the caller's queued work must be done before the workers read inputs
-  cudaError_t e = cudaStreamSynchronize(c->stream);
-  if (e != cudaSuccess) return ctx_cuda(c, e, "batch: synchronize");
+  // Stream order: the workers' streams wait for the work queued on the
+  // caller's stream so far, and the caller's stream waits for the workers'
+  // at the end, so events on the caller's stream bracket the whole batch.
+  cudaEvent_t start = nullptr;
+  cudaError_t e = cudaEventCreateWithFlags(&start, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventRecord(start, c->stream);
+  for (int t = 0; e == cudaSuccess && t < nworkers; ++t)
+    e = cudaStreamWaitEvent(h->workers[t]->c.stream, start, 0);
+  if (start) cudaEventDestroy(start);
+  if (e != cudaSuccess) return ctx_cuda(c, e, "batch: stream order");
   // largest matrices first
   std::vector<size_t> order(count);
   for (size_t i = 0; i < count; ++i) order[i] = i;
@@ -941,7 +957,15 @@ int lela_cuda_fl_echelonize_zp_u32_batch(lela_cuda_ctx *h, size_t count, const s
   std::vector<std::thread> th;
   for (int t = 0; t < nworkers; ++t) th.emplace_back(work, h->workers[t]);
   for (auto &x : th) x.join();
+  for (int t = 0; e == cudaSuccess && t < nworkers; ++t) {
+    cudaEvent_t end = nullptr;
+    e = cudaEventCreateWithFlags(&end, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventRecord(end, h->workers[t]->c.stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(c->stream, end, 0);
+    if (end) cudaEventDestroy(end);
+  }
   if (fatal.load()) return ctx_fail(c, fatal.load(), "batch: a worker failed");
+  if (e != cudaSuccess) return ctx_cuda(c, e, "batch: stream order");
   return ST_OK;
 }
 

@@ -24,6 +24,17 @@ enum GemmKernel : int {
   GEMM_SMALLK = 3,  // CUDA-core gemm for small K (no per-term wrap check when p < 2^28)
 };
 
+// Tile variant of the tensor-core gemm (TcCfg in zp_gemm.cu): variant 0
+// (wide tiles, one accumulator buffer for two and four limbs) or variant 1
+// (narrower tiles, two accumulator buffers, so that a tile's epilogue
+// overlaps the next tile's products); four limbs have variant 0 only.
+enum GemmTile : int {
+  GEMM_TILE_AUTO = 0,    // variant 1 up to GEMM_TILE_DOUBLE_MAX_K, else variant 0
+  GEMM_TILE_WIDE = 1,    // variant 0
+  GEMM_TILE_DOUBLE = 2,  // variant 1
+};
+constexpr int GEMM_TILE_DOUBLE_MAX_K = 1024;
+
 // GF(2) gemm kernels.
 enum Gf2Kernel : int {
   GF2_AUTO = 0,  // tensor cores
@@ -74,6 +85,7 @@ struct Ctx {
   size_t buf_bytes[32] = {};
 
   int gemm_kernel = GEMM_AUTO;
+  int gemm_tile = GEMM_TILE_AUTO;
   int gf2_kernel = GF2_AUTO;
   int trsm_kernel = TRSM_AUTO;
   // Device-memory budget of the batched FL entry point (bytes; 0 = 90 % of
@@ -134,7 +146,9 @@ enum BufSlot : int {
   BUF_TRI_T = 19,     // their assembly temporaries
   BUF_TRI_A = 20,     // dense copy of a sparse triangular operand
   BUF_RED = 21,       // reduced echelon form: column maps, pivot block, solved columns
-  BUF_COUNT = 22,
+  BUF_TRI_OCC = 22,   // occupancy of a sparse triangular operand's 64 x 64 tiles
+  BUF_FL_KR = 23,     // Faugere-Lachartre: per-row column ranges of A and C
+  BUF_COUNT = 24,
 };
 
 // Grow-only allocation helpers; return ST_OK or ST_NOMEM.

@@ -433,18 +433,33 @@ __global__ void __launch_bounds__(PS_THREADS, 1)
     const uint32_t y = P[col];
     {
       // the ac live columns right of col, each taken by G threads that
-      // split the rows: every thread has work until the last columns
+      // split the rows: every thread has work until the last columns.  The
+      // rows are taken four at a time, all their loads issued before any
+      // store (a store to the window may alias a later row's loads, so the
+      // compiler would otherwise keep one row's load-compute-store chain
+      // behind the previous one's)
       const int ac = w - col - 1;
       if (ac > 0) {
         const int G = PS_THREADS / ac;
         if (tid < G * ac) {
           const int c = col + 1 + tid % ac;
           const uint32_t pc = P[c];
-          for (int s = tid / ac; s < nl; s += G) {
-            if (s == drop) continue;
-            const int pr = pm[s];
-            const uint32_t a = Wv[pr][col];
-            Wv[pr][c] = ar.dot2(y, Wv[pr][c], a ? p - a : 0u, pc);
+          for (int s0 = tid / ac; s0 < nl; s0 += 4 * G) {
+            int pr[4];
+            uint32_t av[4], wv[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+              const int s = s0 + u * G;
+              pr[u] = (s < nl && s != drop) ? pm[s] : -1;
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+              av[u] = pr[u] >= 0 ? Wv[pr[u]][col] : 0u;
+              wv[u] = pr[u] >= 0 ? Wv[pr[u]][c] : 0u;
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+              if (pr[u] >= 0) Wv[pr[u]][c] = ar.dot2(y, wv[u], av[u] ? p - av[u] : 0u, pc);
           }
         }
       }

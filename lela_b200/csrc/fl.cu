@@ -13,11 +13,14 @@
 //      runs on the host over the row heads.
 //  split (MatrixGrid1, :766)  One scatter kernel places every stored entry
 //      into dense A (pivot rows x pivot columns, upper triangular), B, C, D.
-//  B <- A^-1 B (:791)  Dense trsm (tri.cu): tensor-core updates, CUDA-core
-//      leaves.  A singular diagonal makes the reference return early
+//  B <- A^-1 B (:791)  Dense trsm (tri.cu): tensor-core updates, inverse
+//      leaves; the updates skip A's empty tiles (its nonzeros lie in a band
+//      above the diagonal), using the per-row column ranges the split
+//      records.  A singular diagonal makes the reference return early
 //      (:792-799); reported here as LELA_CUDA_DIAG_NOT_INVERTIBLE with rank
 //      and det as the reference leaves them.
-//  D <- D - C B (:805)  Limb-split INT8 tensor-core gemm (zp_gemm.cu).
+//  D <- D - C B (:805)  Limb-split INT8 tensor-core gemm (zp_gemm.cu),
+//      each 128-row tile over the K blocks its rows of C can touch.
 //  echelon(D) (:822, then setup_splicer on it, :833)  echelon.cu; its pivots
 //      multiply det and add to the rank.
 //  reduced (:851-902)  D1 | D2 split by D's pivot columns, D2 <- D1^-1 D2
@@ -38,20 +41,28 @@
 namespace lela {
 
 // Row r of X: pos[r] = index of r among pivot rows (>= 0) or -(1 + index
-// among non-pivot rows); column c: cpos likewise.
+// among non-pivot rows); column c: cpos likewise.  Also, per row of A (a
+// pivot row) and of C (a non-pivot row), the range [first, last + 1) of its
+// pivot columns holding entries ((0, 0) when none): the products with A
+// and C skip the K blocks outside them.
 __global__ void fl_split_kernel(const uint64_t *__restrict__ rowptr,
                                 const uint32_t *__restrict__ colidx,
                                 const uint32_t *__restrict__ vals, int m,
                                 const int *__restrict__ rpos, const int *__restrict__ cpos,
                                 uint32_t *A, size_t npiv, uint32_t *B, size_t nres, uint32_t *C,
-                                uint32_t *D) {
+                                uint32_t *D, int2 *krA, int2 *krC) {
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   for (int r = warp; r < m; r += nwarps) {
     const int rp = rpos[r];
+    int lo = 0x7fffffff, hi = -1;
     for (uint64_t e = rowptr[r] + lane; e < rowptr[r + 1]; e += 32) {
       const int cp = cpos[colidx[e]];
       const uint32_t v = vals[e];
+      if (cp >= 0) {
+        lo = min(lo, cp);
+        hi = max(hi, cp);
+      }
       if (rp >= 0) {
         if (cp >= 0) A[(size_t)rp * npiv + cp] = v;
         else B[(size_t)rp * nres + (-1 - cp)] = v;
@@ -59,6 +70,16 @@ __global__ void fl_split_kernel(const uint64_t *__restrict__ rowptr,
         if (cp >= 0) C[(size_t)(-1 - rp) * npiv + cp] = v;
         else D[(size_t)(-1 - rp) * nres + (-1 - cp)] = v;
       }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+      hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    }
+    if (lane == 0) {
+      const int2 v = hi >= 0 ? make_int2(lo, hi + 1) : make_int2(0, 0);
+      if (rp >= 0) krA[rp] = v;
+      else krC[-1 - rp] = v;
     }
   }
 }
@@ -196,6 +217,9 @@ int zp_fl_echelonize_dev(Ctx *c, int m, int n, uint32_t p, const uint64_t *d_row
   if ((st = ctx_buffer(c, BUF_FL_IDX, idx_words * sizeof(int), &vI))) return st;
   uint32_t *A = (uint32_t *)vA, *B = (uint32_t *)vB, *C = (uint32_t *)vC, *D = (uint32_t *)vD;
   int *d_rpos = (int *)vI, *d_cpos = d_rpos + m, *d_aux = d_cpos + n;
+  void *vK = nullptr;
+  if ((st = ctx_buffer(c, BUF_FL_KR, ((size_t)npiv + mres + 1) * sizeof(int2), &vK))) return st;
+  int2 *krA = static_cast<int2 *>(vK), *krC = krA + npiv;
   cudaMemsetAsync(A, 0, szA * 4, c->stream);
   cudaMemsetAsync(B, 0, szB * 4, c->stream);
   cudaMemsetAsync(C, 0, szC * 4, c->stream);
@@ -206,7 +230,7 @@ int zp_fl_echelonize_dev(Ctx *c, int m, int n, uint32_t p, const uint64_t *d_row
     int grid = std::min((m * 32 + 255) / 256, c->num_sms * 16);
     int pi = prof_begin(c, "fl_split");
     fl_split_kernel<<<grid, 256, 0, c->stream>>>(d_rowptr, d_colidx, d_vals, m, d_rpos, d_cpos, A,
-                                                 npiv, B, nres, C, D);
+                                                 npiv, B, nres, C, D, krA, krC);
     prof_end(c, pi);
     ctx_launched(c);
   }
@@ -215,7 +239,7 @@ int zp_fl_echelonize_dev(Ctx *c, int m, int n, uint32_t p, const uint64_t *d_row
   size_t bad = 0;
   int ph = prof_begin(c, "fl_phase_trsm");
   if (npiv > 0) {
-    st = zp_trsm_dev(c, true, false, npiv, nres, p, 1, A, npiv, B, nres, &bad);
+    st = zp_trsm_dev(c, true, false, npiv, nres, p, 1, A, npiv, B, nres, &bad, true, krA);
     if (st == ST_DIAG) {
       res->bad_row = bad;
       return st;  // the reference returns early (rank, det as set so far)
@@ -227,7 +251,7 @@ int zp_fl_echelonize_dev(Ctx *c, int m, int n, uint32_t p, const uint64_t *d_row
   ph = prof_begin(c, "fl_phase_schur");
   if (mres > 0 && nres > 0 && npiv > 0)
     if ((st = zp_gemm_dev(c, GEMM_AUTO, mres, nres, npiv, p, p - 1, C, npiv, B, nres, 1, D, nres,
-                          nullptr)))
+                          nullptr, krC, 0)))
       return st;
   prof_end(c, ph);
   // ---- echelon form of D

@@ -12,6 +12,15 @@
 // substitution on CUDA cores, or (from 1024 rows) 512-row blocks whose
 // inverses are built once and applied by the tensor-core gemm.
 //
+// Sparse operands.  When the caller says A may be sparse (Faugere-
+// Lachartre's pivot block, the CSR entry point), the occupancy of A's 64 x 64
+// tiles is read once (one kernel, one copy to the host), and every
+// off-diagonal update of the recursion runs only over the bounding box of
+// the occupied tiles of its block of A: the rows of B outside the box get
+// no update (only the alpha scaling), and the columns outside it multiply
+// zero.  The result is the same; for F4 pivot blocks, whose nonzeros lie in
+// a band above the diagonal, the update work drops by about 3x at m = 20000.
+//
 // Error behaviour.  With alpha = 0 the reference returns alpha*B = 0
 // without looking at A (:433-434); otherwise a diagonal entry that
 // Modular<uint32>::inv cannot invert throws DiagonalEntryNotInvertible(idx)
@@ -22,6 +31,7 @@
 // solved, which callers such as Faugere-Lachartre discard).
 #include <algorithm>
 #include <mutex>
+#include <vector>
 
 #include "common.cuh"
 #include "context.h"
@@ -44,6 +54,31 @@ __global__ void diag_inverse_kernel(const uint32_t *__restrict__ A, size_t lda, 
       atomicMax(&status[2], (uint32_t)i + 1);
     }
   }
+}
+
+// occ[bi * tn + bj] = 1 when tile (bi, bj) (TRI_NB x TRI_NB) of the m x m
+// matrix A holds a nonzero entry.  Tiles on the other side of the diagonal
+// than the triangle are not read (0).  One CTA of 256 threads per tile;
+// warp w reads 8 of its rows, two 128-byte segments per row.
+__global__ void __launch_bounds__(256)
+    tile_occupancy_kernel(const uint32_t *__restrict__ A, size_t lda, int m, int tn, bool upper,
+                          uint8_t *__restrict__ occ) {
+  const int bi = blockIdx.y, bj = blockIdx.x;
+  if (upper ? bj < bi : bj > bi) {
+    if (threadIdx.x == 0) occ[(size_t)bi * tn + bj] = 0;
+    return;
+  }
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int c0 = bj * TRI_NB + lane, c1 = c0 + 32;
+  bool nz = false;
+  for (int rr = 0; rr < TRI_NB / 8; ++rr) {
+    const int r = bi * TRI_NB + w * (TRI_NB / 8) + rr;
+    if (r >= m) break;
+    const uint32_t *row = A + (size_t)r * lda;
+    nz |= (c0 < m && row[c0] != 0u) || (c1 < m && row[c1] != 0u);
+  }
+  nz = __syncthreads_or(nz);
+  if (threadIdx.x == 0) occ[(size_t)bi * tn + bj] = nz ? 1 : 0;
 }
 
 // Solve T x = x in place for one column held by a quad of threads: thread q
@@ -507,10 +542,99 @@ static int tri_block(Ctx *c, const TriLeaves &L, bool upper, int m, const uint32
   return e == cudaSuccess ? ST_OK : ctx_cuda(c, e, "tri_block launch");
 }
 
-// Recursive solve (dinv is the inverted diagonal of the current sub-system).
-static int trsm_rec(Ctx *c, const TriLeaves &TL, bool upper, int m, int n, uint32_t p,
-                    uint32_t alpha, const uint32_t *A, size_t lda, const uint32_t *dinv,
-                    uint32_t *B, size_t ldb, uint8_t *gemm_ws) {
+// Occupied TRI_NB-tiles of A (host copy): a summed-area table over the
+// tile grid answers "which rows / columns of this block hold nonzeros".
+struct TileMap {
+  int tn = 0;
+  std::vector<int> S;            // (tn + 1)^2 prefix counts
+  const int2 *kr = nullptr;      // per-row column ranges of A (device), or null
+  int count(int i0, int i1, int j0, int j1) const {
+    const int w = tn + 1;
+    return S[(size_t)i1 * w + j1] - S[(size_t)i0 * w + j1] - S[(size_t)i1 * w + j0] +
+           S[(size_t)i0 * w + j0];
+  }
+  // Bounding box, in entries, of the occupied tiles of rows [r0, r1) x
+  // columns [c0, c1) of A (r0, c0 multiples of TRI_NB); false when empty.
+  bool box(int r0, int r1, int c0, int c1, int &br0, int &br1, int &bc0, int &bc1) const {
+    const int i0 = r0 / TRI_NB, i1 = (r1 + TRI_NB - 1) / TRI_NB;
+    const int j0 = c0 / TRI_NB, j1 = (c1 + TRI_NB - 1) / TRI_NB;
+    if (count(i0, i1, j0, j1) == 0) return false;
+    int a = i0, b = i1, x = j0, y = j1;
+    while (count(a, a + 1, j0, j1) == 0) ++a;
+    while (count(b - 1, b, j0, j1) == 0) --b;
+    while (count(i0, i1, x, x + 1) == 0) ++x;
+    while (count(i0, i1, y - 1, y) == 0) --y;
+    br0 = a * TRI_NB;
+    br1 = std::min(r1, b * TRI_NB);
+    bc0 = x * TRI_NB;
+    bc1 = std::min(c1, y * TRI_NB);
+    return true;
+  }
+};
+
+static int build_tile_map(Ctx *c, bool upper, int m, const uint32_t *A, size_t lda, TileMap *tm) {
+  const int tn = (m + TRI_NB - 1) / TRI_NB;
+  void *buf = nullptr;
+  int st = ctx_buffer(c, BUF_TRI_OCC, (size_t)tn * tn, &buf);
+  if (st) return st;
+  uint8_t *d_occ = static_cast<uint8_t *>(buf);
+  tile_occupancy_kernel<<<dim3(tn, tn), 256, 0, c->stream>>>(A, lda, m, tn, upper, d_occ);
+  ctx_launched(c);
+  std::vector<uint8_t> occ((size_t)tn * tn);
+  cudaError_t e = cudaMemcpyAsync(occ.data(), d_occ, occ.size(), cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return ctx_cuda(c, e, "trsm: tile occupancy");
+  tm->tn = tn;
+  const int w = tn + 1;
+  tm->S.assign((size_t)w * w, 0);
+  for (int i = 0; i < tn; ++i)
+    for (int j = 0; j < tn; ++j)
+      tm->S[(size_t)(i + 1) * w + j + 1] = occ[(size_t)i * tn + j] + tm->S[(size_t)i * w + j + 1] +
+                                           tm->S[(size_t)(i + 1) * w + j] - tm->S[(size_t)i * w + j];
+  return ST_OK;
+}
+
+// The off-diagonal update of the recursion, Bd <- alpha Bd - Ablk Bs, where
+// Ablk (rows x cols) is the block of A at rows ar, columns ac of the whole
+// matrix.  With a tile map only its occupied bounding box is multiplied; the
+// other rows of Bd are scaled by alpha (nothing to do for alpha = 1).
+static int tri_update(Ctx *c, const TileMap *tm, int ar, int ac, int rows, int cols, int n,
+                      uint32_t p, uint32_t alpha, const uint32_t *Ablk, size_t lda,
+                      const uint32_t *Bs, uint32_t *Bd, size_t ldb, uint8_t *gemm_ws) {
+  if (!tm)
+    return zp_gemm_dev(c, GEMM_AUTO, rows, n, cols, p, p - 1, Ablk, lda, Bs, ldb, alpha, Bd, ldb,
+                       gemm_ws);
+  int r0, r1, c0, c1;
+  const bool any = tm->box(ar, ar + rows, ac, ac + cols, r0, r1, c0, c1);
+  if (!any) {
+    r0 = r1 = ar;
+    c0 = c1 = ac;
+  }
+  const int lo = r0 - ar, hi = r1 - ar;  // rows of Bd that get a product
+  if (alpha != 1u && n > 0) {
+    const Modulus mod = make_modulus(p);
+    auto scale = [&](int a, int b) {
+      if (b <= a) return;
+      const size_t total = (size_t)(b - a) * n;
+      const int grid = (int)std::min<size_t>((total + 255) / 256, (size_t)c->num_sms * 8);
+      zp_scale2_kernel<<<grid, 256, 0, c->stream>>>(Bd + (size_t)a * ldb, ldb, b - a, n, mod, alpha);
+      ctx_launched(c);
+    };
+    scale(0, lo);
+    scale(hi, rows);
+  }
+  if (!any) return ST_OK;
+  return zp_gemm_dev(c, GEMM_AUTO, hi - lo, n, c1 - c0, p, p - 1,
+                     Ablk + (size_t)lo * lda + (c0 - ac), lda, Bs + (size_t)(c0 - ac) * ldb, ldb,
+                     alpha, Bd + (size_t)lo * ldb, ldb, gemm_ws,
+                     tm->kr ? tm->kr + (ar + lo) : nullptr, c0);
+}
+
+// Recursive solve (dinv is the inverted diagonal of the current sub-system,
+// whose top-left entry is A's entry (off, off)).
+static int trsm_rec(Ctx *c, const TriLeaves &TL, const TileMap *tm, int off, bool upper, int m,
+                    int n, uint32_t p, uint32_t alpha, const uint32_t *A, size_t lda,
+                    const uint32_t *dinv, uint32_t *B, size_t ldb, uint8_t *gemm_ws) {
   if (m <= 0) return ST_OK;
   if (m <= TB_NB) return tri_block(c, TL, upper, m, A, lda, B, ldb, n, p, alpha);
   // split at a multiple of the leaf size, near the middle
@@ -520,20 +644,21 @@ static int trsm_rec(Ctx *c, const TriLeaves &TL, bool upper, int m, int n, uint3
   uint32_t *B1 = B, *B2 = B + (size_t)l * ldb;
   int st;
   if (!upper) {
-    if ((st = trsm_rec(c, TL, upper, l, n, p, alpha, A11, lda, dinv, B1, ldb, gemm_ws))) return st;
-    if ((st = zp_gemm_dev(c, GEMM_AUTO, m - l, n, l, p, p - 1, A21, lda, B1, ldb, alpha, B2, ldb,
-                          gemm_ws)))
+    if ((st = trsm_rec(c, TL, tm, off, upper, l, n, p, alpha, A11, lda, dinv, B1, ldb, gemm_ws)))
       return st;
-    return trsm_rec(c, TL, upper, m - l, n, p, 1, A22, lda, dinv ? dinv + l : nullptr, B2, ldb,
-                    gemm_ws);
+    if ((st = tri_update(c, tm, off + l, off, m - l, l, n, p, alpha, A21, lda, B1, B2, ldb,
+                         gemm_ws)))
+      return st;
+    return trsm_rec(c, TL, tm, off + l, upper, m - l, n, p, 1, A22, lda,
+                    dinv ? dinv + l : nullptr, B2, ldb, gemm_ws);
   } else {
-    if ((st = trsm_rec(c, TL, upper, m - l, n, p, alpha, A22, lda, dinv ? dinv + l : nullptr, B2,
-                       ldb, gemm_ws)))
+    if ((st = trsm_rec(c, TL, tm, off + l, upper, m - l, n, p, alpha, A22, lda,
+                       dinv ? dinv + l : nullptr, B2, ldb, gemm_ws)))
       return st;
-    if ((st = zp_gemm_dev(c, GEMM_AUTO, l, n, m - l, p, p - 1, A12, lda, B2, ldb, alpha, B1, ldb,
-                          gemm_ws)))
+    if ((st = tri_update(c, tm, off, off + l, l, m - l, n, p, alpha, A12, lda, B2, B1, ldb,
+                         gemm_ws)))
       return st;
-    return trsm_rec(c, TL, upper, l, n, p, 1, A11, lda, dinv, B1, ldb, gemm_ws);
+    return trsm_rec(c, TL, tm, off, upper, l, n, p, 1, A11, lda, dinv, B1, ldb, gemm_ws);
   }
 }
 
@@ -589,10 +714,11 @@ static int tri_inverse_levels(Ctx *c, bool upper, int m, uint32_t p, const uint3
 }
 
 // Recursion with inverse leaves: splits at multiples of TI_NB (so every leaf
-// is one of W's blocks; W points at the rows of A's top-left entry).
-static int trsm_rec_inv(Ctx *c, bool upper, int m, int n, uint32_t p, uint32_t alpha,
-                        const uint32_t *A, size_t lda, const uint32_t *W, uint32_t *B, size_t ldb,
-                        uint8_t *gemm_ws) {
+// is one of W's blocks; W points at the rows of A's top-left entry, which is
+// A's entry (off, off)).
+static int trsm_rec_inv(Ctx *c, const TileMap *tm, int off, bool upper, int m, int n, uint32_t p,
+                        uint32_t alpha, const uint32_t *A, size_t lda, const uint32_t *W,
+                        uint32_t *B, size_t ldb, uint8_t *gemm_ws) {
   if (m <= 0) return ST_OK;
   if (m <= TI_NB) {
     // in place: the tensor-core path converts B to limbs in the workspace
@@ -606,18 +732,20 @@ static int trsm_rec_inv(Ctx *c, bool upper, int m, int n, uint32_t p, uint32_t a
   uint32_t *B1 = B, *B2 = B + (size_t)l * ldb;
   int st;
   if (!upper) {
-    if ((st = trsm_rec_inv(c, upper, l, n, p, alpha, A, lda, W, B1, ldb, gemm_ws))) return st;
-    if ((st = zp_gemm_dev(c, GEMM_AUTO, m - l, n, l, p, p - 1, A21, lda, B1, ldb, alpha, B2, ldb,
-                          gemm_ws)))
+    if ((st = trsm_rec_inv(c, tm, off, upper, l, n, p, alpha, A, lda, W, B1, ldb, gemm_ws)))
       return st;
-    return trsm_rec_inv(c, upper, m - l, n, p, 1, A22, lda, W2, B2, ldb, gemm_ws);
+    if ((st = tri_update(c, tm, off + l, off, m - l, l, n, p, alpha, A21, lda, B1, B2, ldb,
+                         gemm_ws)))
+      return st;
+    return trsm_rec_inv(c, tm, off + l, upper, m - l, n, p, 1, A22, lda, W2, B2, ldb, gemm_ws);
   } else {
-    if ((st = trsm_rec_inv(c, upper, m - l, n, p, alpha, A22, lda, W2, B2, ldb, gemm_ws)))
+    if ((st = trsm_rec_inv(c, tm, off + l, upper, m - l, n, p, alpha, A22, lda, W2, B2, ldb,
+                           gemm_ws)))
       return st;
-    if ((st = zp_gemm_dev(c, GEMM_AUTO, l, n, m - l, p, p - 1, A12, lda, B2, ldb, alpha, B1, ldb,
-                          gemm_ws)))
+    if ((st = tri_update(c, tm, off, off + l, l, m - l, n, p, alpha, A12, lda, B2, B1, ldb,
+                         gemm_ws)))
       return st;
-    return trsm_rec_inv(c, upper, l, n, p, 1, A, lda, W, B1, ldb, gemm_ws);
+    return trsm_rec_inv(c, tm, off, upper, l, n, p, 1, A, lda, W, B1, ldb, gemm_ws);
   }
 }
 
@@ -627,7 +755,8 @@ size_t zp_trsm_workspace_bytes(uint32_t p, int m, int n) {
 }
 
 int zp_trsm_dev(Ctx *c, bool upper, bool unit, int m, int n, uint32_t p, uint32_t alpha,
-                const uint32_t *A, size_t lda, uint32_t *B, size_t ldb, size_t *bad_idx) {
+                const uint32_t *A, size_t lda, uint32_t *B, size_t ldb, size_t *bad_idx,
+                bool sparse, const int2 *row_kr) {
   if (p < 2) return ctx_fail(c, ST_ARG, "modulus must be at least 2");
   if (m < 0 || n < 0) return ctx_fail(c, ST_ARG, "negative dimension");
   if (m == 0) return ST_OK;
@@ -675,6 +804,14 @@ int zp_trsm_dev(Ctx *c, bool upper, bool unit, int m, int n, uint32_t p, uint32_
     const bool tc = c->gemm_kernel == GEMM_AUTO || c->gemm_kernel == GEMM_TC;
     kind = (tc && m >= 2 * TI_NB) ? TRSM_INVERSE : TRSM_BLOCKS;
   }
+  // occupied tiles of a possibly sparse A (bounding boxes of the updates)
+  TileMap map;
+  const TileMap *tm = nullptr;
+  if (sparse && m > TRI_NB) {
+    if ((st = build_tile_map(c, upper, m, A, lda, &map))) return st;
+    map.kr = row_kr;
+    tm = &map;
+  }
   // inverses of all 64 x 64 diagonal blocks, in one launch: one after the
   // other for the block substitution, on the diagonal of W for the inverse
   // leaves
@@ -701,7 +838,8 @@ int zp_trsm_dev(Ctx *c, bool upper, bool unit, int m, int n, uint32_t p, uint32_
       return st;
     void *w = nullptr;
     if ((st = ctx_workspace(c, zp_trsm_workspace_bytes(p, m, n), &w))) return st;
-    return trsm_rec_inv(c, upper, m, n, p, alpha, A, lda, W, B, ldb, static_cast<uint8_t *>(w));
+    return trsm_rec_inv(c, tm, 0, upper, m, n, p, alpha, A, lda, W, B, ldb,
+                        static_cast<uint8_t *>(w));
   }
   void *tb = nullptr;
   if ((st = ctx_buffer(c, BUF_TINV, (size_t)nblk * TRI_NB * TRI_NB * 4, &tb))) return st;
@@ -716,7 +854,7 @@ int zp_trsm_dev(Ctx *c, bool upper, bool unit, int m, int n, uint32_t p, uint32_
   void *w = nullptr;
   if ((st = ctx_workspace(c, zp_trsm_workspace_bytes(p, m, n), &w))) return st;
   TriLeaves TL{A, tinv};
-  return trsm_rec(c, TL, upper, m, n, p, alpha, A, lda, unit ? nullptr : dinv, B, ldb,
+  return trsm_rec(c, TL, tm, 0, upper, m, n, p, alpha, A, lda, unit ? nullptr : dinv, B, ldb,
                   static_cast<uint8_t *>(w));
 }
 
@@ -726,26 +864,38 @@ namespace lela {
 
 // ------------------------------------------------------- sparse operand
 // Upper-triangular A given as CSR (rowptr[n + 1], col, val) -> dense rows of
-// the zeroed n x n matrix A (one warp per row).  Entries left of the
+// the zeroed n x n matrix A (one warp per row), and per row the column range
+// [first, last + 1) of its stored entries on or right of the diagonal (the
+// solve's updates skip the K blocks outside it).  Entries left of the
 // diagonal are not part of an upper-triangular operand (the reference's
 // upper solve never reads them) and are skipped; values are taken mod p; a
 // column index >= n sets *bad.
 __global__ void csr_upper_to_dense_kernel(const uint64_t *__restrict__ rowptr,
                                           const uint32_t *__restrict__ col,
                                           const uint32_t *__restrict__ val, int n, uint32_t p,
-                                          uint32_t *__restrict__ A, size_t lda, uint32_t *bad) {
+                                          uint32_t *__restrict__ A, size_t lda, uint32_t *bad,
+                                          int2 *__restrict__ kr) {
   const int lane = threadIdx.x & 31;
   const int warps = (gridDim.x * blockDim.x) >> 5;
   for (int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < n; r += warps) {
     const uint64_t e0 = rowptr[r], e1 = rowptr[r + 1];
+    int lo = 0x7fffffff, hi = -1;
     for (uint64_t e = e0 + lane; e < e1; e += 32) {
       const uint32_t j = col[e];
       if (j >= (uint32_t)n) {
         atomicOr(bad, 1u);
       } else if ((int)j >= r) {
         A[(size_t)r * lda + j] = val[e] % p;
+        lo = min(lo, (int)j);
+        hi = max(hi, (int)j);
       }
     }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+      hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    }
+    if (lane == 0) kr[r] = hi >= 0 ? make_int2(lo, hi + 1) : make_int2(0, 0);
   }
 }
 
@@ -758,15 +908,17 @@ int zp_trsm_csr_upper_dev(Ctx *c, bool unit, int n, int ncols, uint32_t p, uint3
   if (ncols > 0 && ldb < (size_t)ncols)
     return ctx_fail(c, ST_ARG, "leading dimension smaller than the row length");
   void *buf = nullptr;
-  int st = ctx_buffer(c, BUF_TRI_A, (size_t)n * n * 4, &buf);
+  const size_t abytes = ((size_t)n * n * 4 + 255) & ~(size_t)255;
+  int st = ctx_buffer(c, BUF_TRI_A, abytes + (size_t)n * sizeof(int2), &buf);
   if (st) return st;
   uint32_t *A = static_cast<uint32_t *>(buf);
+  int2 *kr = reinterpret_cast<int2 *>(static_cast<uint8_t *>(buf) + abytes);
   cudaError_t e = cudaMemsetAsync(A, 0, (size_t)n * n * 4, c->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(c->dstatus + 3, 0, sizeof(uint32_t), c->stream);
   if (e != cudaSuccess) return ctx_cuda(c, e, "trsm csr: scratch");
   const int grid = std::max(1, std::min((n + 7) / 8, c->num_sms * 8));
   csr_upper_to_dense_kernel<<<grid, 256, 0, c->stream>>>(rowptr, col, val, n, p, A, (size_t)n,
-                                                         c->dstatus + 3);
+                                                         c->dstatus + 3, kr);
   ctx_launched(c);
   // the index check is read before the solve (one synchronisation)
   e = cudaMemcpyAsync(c->hstatus + 3, c->dstatus + 3, sizeof(uint32_t), cudaMemcpyDeviceToHost,
@@ -774,7 +926,7 @@ int zp_trsm_csr_upper_dev(Ctx *c, bool unit, int n, int ncols, uint32_t p, uint3
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return ctx_cuda(c, e, "trsm csr: conversion");
   if (c->hstatus[3]) return ctx_fail(c, ST_ARG, "column index out of range");
-  return zp_trsm_dev(c, true, unit, n, ncols, p, alpha, A, (size_t)n, B, ldb, bad_idx);
+  return zp_trsm_dev(c, true, unit, n, ncols, p, alpha, A, (size_t)n, B, ldb, bad_idx, true, kr);
 }
 
 }  // namespace lela

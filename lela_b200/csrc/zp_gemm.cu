@@ -56,18 +56,37 @@
 namespace lela {
 
 // ------------------------------------------------------------ tile configs
-template <int L>
+//
+// TcCfg<L, T>: tile variant T of the L-limb kernel.  BN = columns of C per
+// tile, NMMA = L * BN (the N of one MMA: the L limbs of B stacked), STAGES
+// = depth of the shared-memory ring, ACC = accumulator buffers in TMEM
+// (each L * NMMA columns; at most 512 in all).  With ACC = 2 the epilogue
+// of one tile overlaps the MMAs of the next; with ACC = 1 the MMAs wait for
+// the epilogue to drain TMEM, but each MMA is wider (more operations per
+// byte of shared memory read).  Variant 0 suits large K, variant 1 the short
+// K of the triangular-solve and elimination updates; the autotuner and the
+// caller can force either.  Four limbs have variant 0 only: with two
+// accumulators a tile would be 16 columns wide, 8 per epilogue thread.
+template <int L, int T>
 struct TcCfg;
 template <>
-struct TcCfg<1> {
+struct TcCfg<1, 0> {
   static constexpr int BN = 256, NMMA = 256, STAGES = 4, ACC = 2;
 };
 template <>
-struct TcCfg<2> {
+struct TcCfg<1, 1> {
+  static constexpr int BN = 128, NMMA = 128, STAGES = 6, ACC = 2;
+};
+template <>
+struct TcCfg<2, 0> {
   static constexpr int BN = 128, NMMA = 256, STAGES = 3, ACC = 1;
 };
 template <>
-struct TcCfg<4> {
+struct TcCfg<2, 1> {
+  static constexpr int BN = 64, NMMA = 128, STAGES = 4, ACC = 2;
+};
+template <>
+struct TcCfg<4, 0> {
   static constexpr int BN = 32, NMMA = 128, STAGES = 2, ACC = 1;
 };
 
@@ -79,9 +98,11 @@ constexpr int TMEM_COLS = 512;
 constexpr int TC_EPI_THREADS = 256;
 constexpr int TC_THREADS = 64 + TC_EPI_THREADS;
 
-template <int L>
+template <int L, int T>
 struct TcLayout {
-  using Cfg = TcCfg<L>;
+  using Cfg = TcCfg<L, T>;
+  static_assert(Cfg::NMMA == L * Cfg::BN, "the B operand stacks the L limbs");
+  static_assert(Cfg::ACC * L * Cfg::NMMA <= TMEM_COLS, "accumulators exceed TMEM");
   static constexpr int A_BYTES = L * BM * BK;
   static constexpr int B_BYTES = Cfg::NMMA * BK;
   static constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
@@ -89,6 +110,7 @@ struct TcLayout {
   // full[S], empty[S], tfull[ACC], tempty[ACC], done, tmem base
   static constexpr int BAR_BYTES = 8 * (2 * Cfg::STAGES + 2 * Cfg::ACC + 1) + 8;
   static constexpr int SMEM = BAR_OFF + BAR_BYTES + 1024;
+  static_assert(SMEM <= 227 * 1024, "shared memory per CTA exceeded");
 };
 
 __device__ __forceinline__ void tile_coords(int t, int tiles_m, int tiles_n, int &mb, int &nb) {
@@ -135,69 +157,64 @@ __device__ __forceinline__ uint32_t epi_combine(int mode, uint32_t v, uint32_t c
   return c >= v ? c - v : c + (p - v);
 }
 
-template <int L>
-__device__ __forceinline__ void epilogue_chunk(uint32_t tcol, int gm, int gn0, int M, int N,
-                                               uint32_t *C, size_t ldc, const Modulus &mod,
-                                               uint32_t alpha, uint32_t beta, int mode);
+// The reduced products of 16 consecutive columns of one row, from the
+// TMEM accumulators of a tile (tcol: the column of the first one in the
+// accumulator of A-limb 0, B-limb 0).  Warp-collective: every lane of the
+// warp runs it (tcgen05.ld is .sync.aligned).
+template <int L, int BN, int NMMA>
+__device__ __forceinline__ void chunk_products(uint32_t tcol, uint32_t (&v)[16],
+                                               const Modulus &mod);
 
 // L = 1: one product, P_00 < 2^31.
 template <>
-__device__ __forceinline__ void epilogue_chunk<1>(uint32_t tcol, int gm, int gn0, int M, int N,
-                                                  uint32_t *C, size_t ldc, const Modulus &mod,
-                                                  uint32_t alpha, uint32_t beta, int mode) {
+__device__ __forceinline__ void chunk_products<1, 256, 256>(uint32_t tcol, uint32_t (&v)[16],
+                                                            const Modulus &mod) {
   uint32_t r[16];
   tmem_ld16(tcol, r);
   tmem_ld_wait();
-  if (gm < M) {
-    uint32_t *crow = C + (size_t)gm * ldc;
 #pragma unroll
-    for (int i = 0; i < 16; ++i) {
-      int gn = gn0 + i;
-      if (gn < N) {
-        uint32_t v = mod_reduce((uint64_t)r[i], mod);
-        const uint32_t c = mode != EPI_SET ? crow[gn] : 0u;
-        crow[gn] = epi_combine(mode, v, c, mod, alpha, beta);
-      }
-    }
-  }
+  for (int i = 0; i < 16; ++i) v[i] = mod_reduce((uint64_t)r[i], mod);
+}
+template <>
+__device__ __forceinline__ void chunk_products<1, 128, 128>(uint32_t tcol, uint32_t (&v)[16],
+                                                            const Modulus &mod) {
+  chunk_products<1, 256, 256>(tcol, v, mod);
 }
 
 // L = 2: A*B = 2^16 P_11 + 2^8 (P_01 + P_10) + P_00 < 2^48.
-template <>
-__device__ __forceinline__ void epilogue_chunk<2>(uint32_t tcol, int gm, int gn0, int M, int N,
-                                                  uint32_t *C, size_t ldc, const Modulus &mod,
-                                                  uint32_t alpha, uint32_t beta, int mode) {
-  constexpr int BN = TcCfg<2>::BN, NMMA = TcCfg<2>::NMMA;
+template <int BN, int NMMA>
+__device__ __forceinline__ void chunk_products2(uint32_t tcol, uint32_t (&v)[16],
+                                                const Modulus &mod) {
   uint32_t p00[16], p01[16], p10[16], p11[16];
   tmem_ld16(tcol, p00);
   tmem_ld16(tcol + BN, p01);
   tmem_ld16(tcol + NMMA, p10);
   tmem_ld16(tcol + NMMA + BN, p11);
   tmem_ld_wait();
-  if (gm < M) {
-    uint32_t *crow = C + (size_t)gm * ldc;
 #pragma unroll
-    for (int i = 0; i < 16; ++i) {
-      int gn = gn0 + i;
-      if (gn < N) {
-        uint64_t v = ((uint64_t)p11[i] << 16) + (((uint64_t)p01[i] + p10[i]) << 8) + p00[i];
-        uint32_t vr = mod_reduce(v, mod);
-        const uint32_t c = mode != EPI_SET ? crow[gn] : 0u;
-        crow[gn] = epi_combine(mode, vr, c, mod, alpha, beta);
-      }
-    }
+  for (int i = 0; i < 16; ++i) {
+    const uint64_t x = ((uint64_t)p11[i] << 16) + (((uint64_t)p01[i] + p10[i]) << 8) + p00[i];
+    v[i] = mod_reduce(x, mod);
   }
+}
+template <>
+__device__ __forceinline__ void chunk_products<2, 128, 256>(uint32_t tcol, uint32_t (&v)[16],
+                                                            const Modulus &mod) {
+  chunk_products2<128, 256>(tcol, v, mod);
+}
+template <>
+__device__ __forceinline__ void chunk_products<2, 64, 128>(uint32_t tcol, uint32_t (&v)[16],
+                                                           const Modulus &mod) {
+  chunk_products2<64, 128>(tcol, v, mod);
 }
 
 // L = 4: D_s = sum_{i+j=s} P_ij < 2^33, Horner in s with a reduction per
 // step ((r < 2^32) * 2^8 + D_s < 2^41).  Eight columns at a time to keep the
 // seven 64-bit partial sums in registers.
-template <>
-__device__ __forceinline__ void epilogue_chunk<4>(uint32_t tcol, int gm, int gn0, int M, int N,
-                                                  uint32_t *C, size_t ldc, const Modulus &mod,
-                                                  uint32_t alpha, uint32_t beta, int mode) {
-  constexpr int BN = TcCfg<4>::BN, NMMA = TcCfg<4>::NMMA;
-#pragma unroll 1
+template <int BN, int NMMA>
+__device__ __forceinline__ void chunk_products4(uint32_t tcol, uint32_t (&v)[16],
+                                                const Modulus &mod) {
+#pragma unroll
   for (int h = 0; h < 16; h += 8) {
     uint64_t D[7][8];
 #pragma unroll
@@ -215,19 +232,58 @@ __device__ __forceinline__ void epilogue_chunk<4>(uint32_t tcol, int gm, int gn0
         for (int i = 0; i < 8; ++i) D[li + lj][i] += r[i];
       }
     }
-    if (gm < M) {
-      uint32_t *crow = C + (size_t)gm * ldc;
 #pragma unroll
-      for (int i = 0; i < 8; ++i) {
-        int gn = gn0 + h + i;
-        if (gn < N) {
-          uint32_t acc = mod_reduce(D[6][i], mod);
+    for (int i = 0; i < 8; ++i) {
+      uint32_t acc = mod_reduce(D[6][i], mod);
 #pragma unroll
-          for (int s = 5; s >= 0; --s) acc = mod_reduce(((uint64_t)acc << 8) + D[s][i], mod);
-          const uint32_t c = mode != EPI_SET ? crow[gn] : 0u;
-          crow[gn] = epi_combine(mode, acc, c, mod, alpha, beta);
-        }
-      }
+      for (int s = 5; s >= 0; --s) acc = mod_reduce(((uint64_t)acc << 8) + D[s][i], mod);
+      v[h + i] = acc;
+    }
+  }
+}
+template <>
+__device__ __forceinline__ void chunk_products<4, 32, 128>(uint32_t tcol, uint32_t (&v)[16],
+                                                           const Modulus &mod) {
+  chunk_products4<32, 128>(tcol, v, mod);
+}
+
+// C row segments in registers.  load_c reads n consecutive entries of row
+// `crow` from column gn (entries at columns >= N read as 0; crow == nullptr:
+// a row past M); 16-byte loads where the row and column allow (vec: C and
+// its row stride 16-byte aligned).  store_c writes them back.
+template <int NV>
+__device__ __forceinline__ void load_c(uint32_t (&c)[NV], const uint32_t *crow, int gn, int N,
+                                       bool vec) {
+  static_assert(NV % 4 == 0, "whole vectors");
+#pragma unroll
+  for (int j = 0; j < NV / 4; ++j) {
+    const int g = gn + 4 * j;
+    if (crow != nullptr && vec && g + 3 < N) {
+      const uint4 u = *reinterpret_cast<const uint4 *>(crow + g);
+      c[4 * j] = u.x;
+      c[4 * j + 1] = u.y;
+      c[4 * j + 2] = u.z;
+      c[4 * j + 3] = u.w;
+    } else {
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+        c[4 * j + i] = (crow != nullptr && g + i < N) ? crow[g + i] : 0u;
+    }
+  }
+}
+template <int NV>
+__device__ __forceinline__ void store_c(const uint32_t (&c)[NV], uint32_t *crow, int gn, int N,
+                                        bool vec) {
+  if (crow == nullptr) return;
+#pragma unroll
+  for (int j = 0; j < NV / 4; ++j) {
+    const int g = gn + 4 * j;
+    if (vec && g + 3 < N) {
+      *reinterpret_cast<uint4 *>(crow + g) = make_uint4(c[4 * j], c[4 * j + 1], c[4 * j + 2], c[4 * j + 3]);
+    } else {
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+        if (g + i < N) crow[g + i] = c[4 * j + i];
     }
   }
 }
@@ -267,16 +323,57 @@ __device__ __forceinline__ void epilogue_gf2(uint32_t tcol, int gm, int gn0, int
   }
 }
 
-template <int L, int OUT>
+// K blocks [kb0, kb1) of the row tile starting at row m0: all of K, or,
+// with per-row ranges kr (row r of A is zero outside columns [kr[r].x,
+// kr[r].y) of the whole matrix; kbase = the whole matrix's column of this
+// product's K = 0), the blocks covering the union of the tile's rows'
+// ranges.  A tile whose rows are zero in all of K keeps one block: its
+// product is zero either way.  Warp-collective (the warp's lanes share the
+// rows), so every lane of the calling warp runs it.
+__device__ __forceinline__ void tile_kblocks(const int2 *__restrict__ kr, int kbase, int m0, int M,
+                                             int K, int &kb0, int &kb1) {
+  const int nkb = (K + BK - 1) / BK;
+  kb0 = 0;
+  kb1 = nkb;
+  if (kr == nullptr) return;
+  int lo = 0x7fffffff, hi = -0x7fffffff;
+  const int lane = threadIdx.x & 31;
+  for (int r = m0 + lane; r < min(M, m0 + BM); r += 32) {
+    const int2 v = kr[r];
+    if (v.y > v.x) {
+      lo = min(lo, v.x);
+      hi = max(hi, v.y);
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+    hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+  }
+  if (hi <= lo) {  // no row of the tile has a nonzero anywhere
+    kb1 = 1;
+    return;
+  }
+  lo = max(lo - kbase, 0);
+  hi = min(hi - kbase, K);
+  if (hi <= lo) {  // none inside this product's K range
+    kb1 = 1;
+    return;
+  }
+  kb0 = lo / BK;
+  kb1 = (hi + BK - 1) / BK;
+}
+
+template <int L, int OUT, int T = 0>
 __global__ void __launch_bounds__(TC_THREADS, 1)
     zp_gemm_tc_kernel(const __grid_constant__ CUtensorMap tmA,
                       const __grid_constant__ CUtensorMap tmB, void *__restrict__ Cv,
                       size_t ldc, int M, int N, int K, Modulus mod, uint32_t alpha, uint32_t beta,
-                      uint32_t *err) {
-  static_assert(OUT == 0 || L == 1, "GF(2) output uses one limb");
+                      uint32_t *err, const int2 *__restrict__ kr = nullptr, int kbase = 0) {
+  static_assert(OUT == 0 || (L == 1 && T == 0), "GF(2) output uses one limb, variant 0");
   uint32_t *C = static_cast<uint32_t *>(Cv);
-  using Cfg = TcCfg<L>;
-  using Lay = TcLayout<L>;
+  using Cfg = TcCfg<L, T>;
+  using Lay = TcLayout<L, T>;
   constexpr int S = Cfg::STAGES, ACC = Cfg::ACC, BN = Cfg::BN, NMMA = Cfg::NMMA;
   constexpr uint32_t IDESC = idesc_u8_s32(BM, NMMA);
 
@@ -291,7 +388,6 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(done + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int num_kb = (K + BK - 1) / BK;
   const int tiles_m = (M + BM - 1) / BM, tiles_n = (N + BN - 1) / BN;
   const int num_tiles = tiles_m * tiles_n;
 
@@ -316,16 +412,20 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
   const uint32_t tmem = *tmem_slot;
 
   if (warp == 0) {
-    if (lane == 0) {
-      // ---------------------------------------------------------- producer
-      uint32_t s = 0, ph = 0;
-      uint32_t issued = 0, last_ph[S];
-      for (int i = 0; i < S; ++i) last_ph[i] = 0;
-      bool ok = true;
-      for (int t = blockIdx.x; t < num_tiles && ok; t += gridDim.x) {
-        int mb, nb;
-        tile_coords(t, tiles_m, tiles_n, mb, nb);
-        for (int kb = 0; kb < num_kb; ++kb) {
+    // ------------------------------------------------------------ producer
+    // The whole warp walks the tiles (their K ranges are warp-collective);
+    // lane 0 issues the loads, and its status is shared each tile so that
+    // the lanes leave together.
+    uint32_t s = 0, ph = 0;
+    uint32_t issued = 0, last_ph[S];
+    for (int i = 0; i < S; ++i) last_ph[i] = 0;
+    bool ok = true;
+    for (int t = blockIdx.x; t < num_tiles; t += gridDim.x) {
+      int mb, nb, kb0, kb1;
+      tile_coords(t, tiles_m, tiles_n, mb, nb);
+      tile_kblocks(kr, kbase, mb * BM, M, K, kb0, kb1);
+      if (lane == 0) {
+        for (int kb = kb0; kb < kb1; ++kb) {
           if (!mbar_wait(&empty[s], ph ^ 1, err)) { ok = false; break; }
           uint8_t *sa = smem + s * Lay::STAGE_BYTES;
           uint8_t *sb = sa + Lay::A_BYTES;
@@ -337,25 +437,30 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
           if (++s == S) { s = 0; ph ^= 1; }
         }
       }
-      if (!ok) {
-        // Wait for the loads already in flight before the block may exit.
-        for (int i = 0; i < S; ++i)
-          if (issued & (1u << i)) mbar_drain(&full[i], last_ph[i], err);
-      }
+      if (!__shfl_sync(0xffffffffu, ok ? 1 : 0, 0)) break;
+    }
+    if (lane == 0 && !ok) {
+      // Wait for the loads already in flight before the block may exit.
+      for (int i = 0; i < S; ++i)
+        if (issued & (1u << i)) mbar_drain(&full[i], last_ph[i], err);
     }
   } else if (warp == 1) {
-    if (lane == 0) {
-      // --------------------------------------------------------- MMA issue
-      uint32_t s = 0, ph = 0;
-      int it = 0;
-      bool ok = true;
-      for (int t = blockIdx.x; t < num_tiles && ok; t += gridDim.x, ++it) {
+    // ----------------------------------------------------------- MMA issue
+    // As the producer: the warp walks the tiles, lane 0 issues the MMAs.
+    uint32_t s = 0, ph = 0;
+    int it = 0;
+    bool ok = true;
+    for (int t = blockIdx.x; t < num_tiles; t += gridDim.x, ++it) {
+      int mb, nb, kb0, kb1;
+      tile_coords(t, tiles_m, tiles_n, mb, nb);
+      tile_kblocks(kr, kbase, mb * BM, M, K, kb0, kb1);
+      if (lane == 0) {
         const int a = it % ACC;
         const uint32_t aph = (uint32_t)(it / ACC) & 1u;
-        if (!mbar_wait(&tempty[a], aph ^ 1, err)) { ok = false; break; }
+        if (!mbar_wait(&tempty[a], aph ^ 1, err)) ok = false;
         tc_fence_after();
         const uint32_t dbase = tmem + (uint32_t)(a * L * NMMA);
-        for (int kb = 0; kb < num_kb; ++kb) {
+        for (int kb = kb0; kb < kb1 && ok; ++kb) {
           if (!mbar_wait(&full[s], ph, err)) { ok = false; break; }
           tc_fence_after();
           uint8_t *sa = smem + s * Lay::STAGE_BYTES;
@@ -369,15 +474,17 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
               // +32 bytes of K inside the 128-byte swizzled row = +2 in the
               // descriptor's (address >> 4) field.
               mma_u8(dbase + (uint32_t)(l * NMMA), ad + 2 * kk, bd + 2 * kk, IDESC,
-                     (kb | kk) != 0);
+                     (kb != kb0 || kk != 0) ? 1u : 0u);
             }
           }
           mma_commit(&empty[s]);
           if (++s == S) { s = 0; ph ^= 1; }
         }
-        if (!ok) break;
-        mma_commit(&tfull[a]);
+        if (ok) mma_commit(&tfull[a]);
       }
+      if (!__shfl_sync(0xffffffffu, ok ? 1 : 0, 0)) break;
+    }
+    if (lane == 0) {
       // All MMAs of this thread must finish before TMEM is released.
       mma_commit(done);
       mbar_drain(done, 0, err);
@@ -388,39 +495,62 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     const int q = warp & 3;  // TMEM lane quadrant this warp may access
     const int row = q * 32 + lane;
     const int half = (warp - 2) >> 2;
-    const int cbeg = half * (BN / 2), cend = cbeg + BN / 2;
+    const int cbeg = half * (BN / 2);
     const int emode = beta == 0u ? EPI_SET
                       : (beta == 1u && alpha == 1u) ? EPI_ADD
                       : (beta == 1u && alpha == (uint32_t)mod.p - 1u) ? EPI_SUB
                                                                      : EPI_AXPBY;
+    const bool readc = emode != EPI_SET;
+    const bool vec = ((reinterpret_cast<uintptr_t>(C) & 15u) == 0) && ((ldc & 3u) == 0);
     int it = 0;
     for (int t = blockIdx.x; t < num_tiles; t += gridDim.x, ++it) {
       int mb, nb;
       tile_coords(t, tiles_m, tiles_n, mb, nb);
-      if (OUT == 0 && beta != 0u) {
-        // pull this thread's row segment of C into L2 while the tile's
-        // products run, so that the epilogue's loads of C hit L2
-        const int gm = mb * BM + row, gn0 = nb * BN + cbeg;
-        if (gm < M)
-          for (int cc = 0; cc < cend - cbeg; cc += 32)
-            if (gn0 + cc < N) prefetch_l2(C + (size_t)gm * ldc + gn0 + cc);
-      }
       const int a = it % ACC;
       const uint32_t aph = (uint32_t)(it / ACC) & 1u;
-      if (!mbar_wait(&tfull[a], aph, err)) break;
-      tc_fence_after();
-      const uint32_t tbase = tmem + (uint32_t)(a * L * NMMA) + ((uint32_t)(q * 32) << 16);
       const int gm = mb * BM + row;
+      const uint32_t tbase = tmem + (uint32_t)(a * L * NMMA) + ((uint32_t)(q * 32) << 16);
       if constexpr (OUT == 0) {
-#pragma unroll 1
-        for (int c0 = cbeg; c0 < cend; c0 += 16)
-          epilogue_chunk<L>(tbase + c0, gm, nb * BN + c0, M, N, C, ldc, mod, alpha, beta, emode);
+        // This thread's row segment: W = BN / 2 columns from gn0, in blocks
+        // of EPB columns.  C's block 0 is loaded before the accumulator is
+        // ready (its latency hides behind the tile's MMAs), block b + 1
+        // while block b is combined; TMEM is released after its last read,
+        // before the last block's stores.
+        constexpr int W = BN / 2;
+        constexpr int EPB = W < 32 ? W : 32;
+        constexpr int NB = W / EPB;
+        const int gn0 = nb * BN + cbeg;
+        uint32_t *crow = gm < M ? C + (size_t)gm * ldc : nullptr;
+        uint32_t cb[2][EPB];
+        if (readc) load_c<EPB>(cb[0], crow, gn0, N, vec);
+        if (!mbar_wait(&tfull[a], aph, err)) break;
+        tc_fence_after();
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
+          uint32_t(&cur)[EPB] = cb[b & 1];
+          if (b + 1 < NB && readc) load_c<EPB>(cb[(b + 1) & 1], crow, gn0 + (b + 1) * EPB, N, vec);
+#pragma unroll
+          for (int h = 0; h < EPB / 16; ++h) {
+            uint32_t v[16];
+            chunk_products<L, BN, NMMA>(tbase + (uint32_t)(cbeg + b * EPB + 16 * h), v, mod);
+#pragma unroll
+            for (int i = 0; i < 16; ++i)
+              cur[16 * h + i] = epi_combine(emode, v[i], readc ? cur[16 * h + i] : 0u, mod, alpha, beta);
+          }
+          if (b == NB - 1) {
+            tc_fence_before();
+            mbar_arrive(&tempty[a]);
+          }
+          store_c<EPB>(cur, crow, gn0 + b * EPB, N, vec);
+        }
       } else {
+        if (!mbar_wait(&tfull[a], aph, err)) break;
+        tc_fence_after();
         epilogue_gf2(tbase, gm, nb * BN, M, N, static_cast<uint64_t *>(Cv), ldc, alpha, beta,
-                     cbeg, cend);
+                     cbeg, cbeg + BN / 2);
+        tc_fence_before();
+        mbar_arrive(&tempty[a]);
       }
-      tc_fence_before();
-      mbar_arrive(&tempty[a]);
     }
   }
 
@@ -665,19 +795,19 @@ static int encode_3d(Ctx *c, CUtensorMap *tm, void *base, uint64_t d0, uint64_t 
   return ST_OK;
 }
 
-template <int L>
+template <int L, int T = 0>
 static int tc_attr(Ctx *c) {
-  return ctx_smem_attr(c, (const void *)zp_gemm_tc_kernel<L, 0>, TcLayout<L>::SMEM,
+  return ctx_smem_attr(c, (const void *)zp_gemm_tc_kernel<L, 0, T>, TcLayout<L, T>::SMEM,
                        "cudaFuncSetAttribute(zp_gemm_tc)");
 }
 
-template <int L>
+template <int L, int T>
 static int launch_tc(Ctx *c, int M, int N, int K, const Modulus &mod, uint32_t alpha,
                      const uint32_t *A, size_t lda, const uint32_t *B, size_t ldb, uint32_t beta,
-                     uint32_t *C, size_t ldc, uint8_t *ws) {
-  using Cfg = TcCfg<L>;
-  using Lay = TcLayout<L>;
-  if (int st = tc_attr<L>(c)) return st;
+                     uint32_t *C, size_t ldc, uint8_t *ws, const int2 *kr, int kbase) {
+  using Cfg = TcCfg<L, T>;
+  using Lay = TcLayout<L, T>;
+  if (int st = tc_attr<L, T>(c)) return st;
   const int tiles = ((M + BM - 1) / BM) * ((N + Cfg::BN - 1) / Cfg::BN);
   uint32_t b = beta;
   for (int k0 = 0; k0 < K; k0 += ZP_KCHUNK) {
@@ -704,8 +834,8 @@ static int launch_tc(Ctx *c, int M, int N, int K, const Modulus &mod, uint32_t a
     if (st) return st;
     const int grid = std::min(tiles, c->num_sms);
     int pi = prof_begin(c, "zp_gemm_tc");
-    zp_gemm_tc_kernel<L, 0><<<grid, TC_THREADS, Lay::SMEM, c->stream>>>(tmA, tmB, C, ldc, M, N, kc, mod,
-                                                              alpha, b, c->dstatus);
+    zp_gemm_tc_kernel<L, 0, T><<<grid, TC_THREADS, Lay::SMEM, c->stream>>>(
+        tmA, tmB, C, ldc, M, N, kc, mod, alpha, b, c->dstatus, kr, kbase + k0);
     prof_end(c, pi);
     ctx_launched(c);
     b = 1;
@@ -722,6 +852,13 @@ size_t zp_gemm_workspace_bytes(uint32_t p, int M, int N, int K) {
   return (size_t)L * ((size_t)M + N) * Kp + 256;
 }
 
+int zp_gemm_tile_pick(const Ctx *c, int K, uint32_t p) {
+  if (zp_limbs_for(p) == 4) return 0;  // one variant for four limbs
+  if (c->gemm_tile == GEMM_TILE_WIDE) return 0;
+  if (c->gemm_tile == GEMM_TILE_DOUBLE) return 1;
+  return K <= GEMM_TILE_DOUBLE_MAX_K ? 1 : 0;
+}
+
 int zp_gemm_pick(const Ctx *c, int M, int N, int K, uint32_t p) {
   if (c->gemm_kernel != GEMM_AUTO) return c->gemm_kernel;
   // small K: the CUDA-core kernel below its measured crossover with the
@@ -736,7 +873,7 @@ int zp_gemm_pick(const Ctx *c, int M, int N, int K, uint32_t p) {
 
 int zp_gemm_dev(Ctx *c, int kernel, int M, int N, int K, uint32_t p, uint32_t alpha,
                 const uint32_t *A, size_t lda, const uint32_t *B, size_t ldb, uint32_t beta,
-                uint32_t *C, size_t ldc, uint8_t *ws_override) {
+                uint32_t *C, size_t ldc, uint8_t *ws_override, const int2 *kr, int kbase) {
   if (p < 2) return ctx_fail(c, ST_ARG, "modulus must be at least 2");
   if (M < 0 || N < 0 || K < 0) return ctx_fail(c, ST_ARG, "negative dimension");
   if (M == 0 || N == 0) return ST_OK;
@@ -786,10 +923,16 @@ int zp_gemm_dev(Ctx *c, int kernel, int M, int N, int K, uint32_t p, uint32_t al
     if (st) return st;
     ws = static_cast<uint8_t *>(w);
   }
+  const bool t1 = zp_gemm_tile_pick(c, K, p) == 1;
   switch (zp_limbs_for(p)) {
-    case 1: return launch_tc<1>(c, M, N, K, mod, alpha, A, lda, B, ldb, beta, C, ldc, ws);
-    case 2: return launch_tc<2>(c, M, N, K, mod, alpha, A, lda, B, ldb, beta, C, ldc, ws);
-    default: return launch_tc<4>(c, M, N, K, mod, alpha, A, lda, B, ldb, beta, C, ldc, ws);
+    case 1:
+      return t1 ? launch_tc<1, 1>(c, M, N, K, mod, alpha, A, lda, B, ldb, beta, C, ldc, ws, kr, kbase)
+                : launch_tc<1, 0>(c, M, N, K, mod, alpha, A, lda, B, ldb, beta, C, ldc, ws, kr, kbase);
+    case 2:
+      return t1 ? launch_tc<2, 1>(c, M, N, K, mod, alpha, A, lda, B, ldb, beta, C, ldc, ws, kr, kbase)
+                : launch_tc<2, 0>(c, M, N, K, mod, alpha, A, lda, B, ldb, beta, C, ldc, ws, kr, kbase);
+    default:
+      return launch_tc<4, 0>(c, M, N, K, mod, alpha, A, lda, B, ldb, beta, C, ldc, ws, kr, kbase);
   }
 }
 
@@ -815,8 +958,8 @@ static int host_rows(Ctx *c, int M, int N, int K, const Modulus &mod, uint32_t a
                      const uint32_t *hA, size_t lda, const uint32_t *hB, size_t ldb,
                      uint32_t beta, uint32_t *hC, size_t ldc, uint32_t *dA, uint32_t *dB,
                      uint32_t *dC, uint8_t *ws) {
-  using Cfg = TcCfg<L>;
-  using Lay = TcLayout<L>;
+  using Cfg = TcCfg<L, 0>;
+  using Lay = TcLayout<L, 0>;
   if (int st = tc_attr<L>(c)) return st;
   const int Kp = (K + 15) & ~15;
   // row blocks: a multiple of the tile height, at most PIPE_MAX_BLOCKS
@@ -990,13 +1133,13 @@ int noalloc_setup(int dev, NoallocDevice *out) {
     e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) return ST_CUDA;
     e = cudaFuncSetAttribute(zp_gemm_tc_kernel<1, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             TcLayout<1>::SMEM);
+                             TcLayout<1, 0>::SMEM);
     if (e == cudaSuccess)
       e = cudaFuncSetAttribute(zp_gemm_tc_kernel<2, 0>,
-                               cudaFuncAttributeMaxDynamicSharedMemorySize, TcLayout<2>::SMEM);
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, TcLayout<2, 0>::SMEM);
     if (e == cudaSuccess)
       e = cudaFuncSetAttribute(zp_gemm_tc_kernel<4, 0>,
-                               cudaFuncAttributeMaxDynamicSharedMemorySize, TcLayout<4>::SMEM);
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, TcLayout<4, 0>::SMEM);
     if (e != cudaSuccess) return ST_CUDA;
     if (!g_noalloc_encode) {
       void *fn = nullptr;
@@ -1029,8 +1172,8 @@ template <int L>
 int noalloc_launch(cudaStream_t s, const NoallocDevice &d, int M, int N, int K,
                    const Modulus &mod, uint32_t alpha, const uint32_t *A, size_t lda,
                    const uint32_t *B, size_t ldb, uint32_t beta, uint32_t *C, size_t ldc) {
-  using Cfg = TcCfg<L>;
-  using Lay = TcLayout<L>;
+  using Cfg = TcCfg<L, 0>;
+  using Lay = TcLayout<L, 0>;
   uint32_t *err = reinterpret_cast<uint32_t *>(d.base);
   uint8_t *planes = d.base + NOALLOC_STATUS_BYTES;
   const int tiles = ((M + BM - 1) / BM) * ((N + Cfg::BN - 1) / Cfg::BN);
@@ -1117,8 +1260,8 @@ namespace lela {
 // the one-limb tensor-core kernel with the bit-packing epilogue.
 int gf2_gemm_tc_planes(Ctx *c, int M, int N, int K, const uint8_t *Ab, const uint8_t *Bb, int Kp,
                        uint32_t alpha, uint32_t beta, uint64_t *C, size_t ldc_words) {
-  using Cfg = TcCfg<1>;
-  using Lay = TcLayout<1>;
+  using Cfg = TcCfg<1, 0>;
+  using Lay = TcLayout<1, 0>;
   if (int st = ctx_smem_attr(c, (const void *)zp_gemm_tc_kernel<1, 1>, Lay::SMEM,
                              "cudaFuncSetAttribute(gf2 tc)"))
     return st;

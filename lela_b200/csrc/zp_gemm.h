@@ -3,6 +3,8 @@
 #include <cstddef>
 #include <cstdint>
 
+#include <cuda_runtime.h>
+
 #include "context.h"
 
 namespace lela {
@@ -16,14 +18,23 @@ size_t zp_gemm_workspace_bytes(uint32_t p, int M, int N, int K);
 // C <- alpha*A*B + beta*C mod p on the handle's stream (asynchronous).
 // kernel: GEMM_AUTO, GEMM_PLAIN or GEMM_TC.  ws_override, when non-null,
 // is used instead of the handle workspace for the limb planes and must hold
-// zp_gemm_workspace_bytes(p, M, N, K) bytes.
+// zp_gemm_workspace_bytes(p, M, N, K) bytes.  kr (device, optional): per
+// row r of A, a column range [kr[r].x, kr[r].y) of the whole matrix outside
+// which row r is zero (y <= x: the row is zero), and kbase the whole
+// matrix's column of A's column 0; the tensor-core kernel then multiplies,
+// per 128-row tile, only the K blocks its rows can touch (the other
+// kernels ignore it: the result is the same).
 int zp_gemm_dev(Ctx *c, int kernel, int M, int N, int K, uint32_t p, uint32_t alpha,
                 const uint32_t *A, size_t lda, const uint32_t *B, size_t ldb, uint32_t beta,
-                uint32_t *C, size_t ldc, uint8_t *ws_override);
+                uint32_t *C, size_t ldc, uint8_t *ws_override, const int2 *kr = nullptr,
+                int kbase = 0);
 
 // The kernel GEMM_AUTO resolves to for this shape (the handle's forced
 // kernel, else the small-K crossover rule).
 int zp_gemm_pick(const Ctx *c, int M, int N, int K, uint32_t p);
+// The tensor-core tile variant (0 or 1) for this K and modulus: the
+// handle's forced variant, else variant 1 up to GEMM_TILE_DOUBLE_MAX_K.
+int zp_gemm_tile_pick(const Ctx *c, int K, uint32_t p);
 
 // Whether the host-pointer gemm of this shape is done in row blocks with
 // its copies overlapped (tensor-core path, one K chunk, at least two blocks

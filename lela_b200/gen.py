@@ -220,3 +220,97 @@ def f4_matrix_small(seed, m, n, p, density=0.1):
     rowptr = np.zeros(m + 1, dtype=np.uint64)
     rowptr[1:] = np.cumsum(lens)
     return CSR(m, n, rowptr, np.concatenate(rows_c), np.concatenate(rows_v))
+
+
+def f4_matrix_fast(seed, m, p, n=None, density=None, pivot_frac=0.75, dep_frac=0.05):
+    """The F4 family of f4_matrix (same pivot structure, density, value
+    distribution and planted dependencies), generated with whole-array
+    operations so that matrices with m in the tens of thousands take well
+    under a second.  The offsets right of each row's leading column are
+    cumulative sums of geometric gaps (strictly increasing, clustered
+    towards the leading column) instead of sorted distinct exponential
+    draws, so for a given seed the matrix differs from f4_matrix's."""
+    g = rng(seed)
+    n = int(1.2 * m) if n is None else int(n)
+    if density is None:
+        density = float(g.uniform(0.01, 0.04))
+    npiv = max(0, min(int(round(pivot_frac * m)), n, m))
+    nnp = m - npiv
+    lead = np.sort(g.choice(n, size=npiv, replace=False)) if npiv else np.zeros(0, np.int64)
+    owner = np.sort(g.integers(0, npiv, size=nnp)) if (npiv and nnp) else np.zeros(0, np.int64)
+    counts = np.bincount(owner, minlength=npiv) if npiv else np.zeros(0, np.int64)
+    heads = np.repeat(lead, counts + 1).astype(np.int64) if npiv else np.zeros(0, np.int64)
+    is_piv = np.zeros(len(heads), dtype=bool)
+    if npiv:
+        starts = np.concatenate([[0], np.cumsum(counts + 1)[:-1]])
+        is_piv[starts] = True
+    mm = len(heads)
+    k = max(1, int(round(density * n)))
+    room = n - heads - 1
+    # gaps with mean room / (4 k): the k offsets spread over about a quarter
+    # of the room, more densely near the leading column
+    mean_gap = np.maximum(1.0, room / (4.0 * k))
+    gaps = 1 + np.floor(g.exponential(size=(mm, k)) * (mean_gap[:, None] - 1.0 + 1e-9)).astype(np.int64)
+    off = np.cumsum(gaps, axis=1) - 1
+    valid = off < room[:, None]
+    cols = heads[:, None] + 1 + off
+    vals = g.integers(1, p, size=(mm, k), dtype=np.uint32)
+    lead_v = np.where(is_piv, 1, g.integers(1, p, size=mm)).astype(np.uint32)
+    lens = 1 + valid.sum(axis=1)
+    rowptr = np.zeros(mm + 1, dtype=np.uint64)
+    rowptr[1:] = np.cumsum(lens)
+    colidx = np.empty(int(rowptr[-1]), dtype=np.uint32)
+    vv = np.empty(int(rowptr[-1]), dtype=np.uint32)
+    first = rowptr[:-1].astype(np.int64)
+    colidx[first] = heads
+    vv[first] = lead_v
+    body = np.ones(int(rowptr[-1]), dtype=bool)
+    body[first] = False
+    colidx[body] = cols[valid]
+    vv[body] = vals[valid]
+    X = CSR(mm, n, rowptr, colidx, vv)
+    # planted dependencies: c1 * (pivot row of the same head) + c2 * (a later
+    # pivot row), as in f4_matrix
+    np_rows = np.nonzero(~is_piv)[0]
+    ndep = int(round(dep_frac * len(np_rows)))
+    if not (ndep and npiv > 1):
+        return X
+    piv_rows = np.nonzero(is_piv)[0]
+    piv_of = np.searchsorted(lead, heads)  # index among pivot rows of each row's head
+    rows_c = {}
+    for r in g.choice(np_rows, size=ndep, replace=False):
+        i1 = int(piv_of[r])
+        if i1 + 1 >= npiv:
+            continue
+        r1, r2 = int(piv_rows[i1]), int(piv_rows[int(g.integers(i1 + 1, npiv))])
+        c1, c2 = int(g.integers(1, p)), int(g.integers(1, p))
+        a0, a1 = int(rowptr[r1]), int(rowptr[r1 + 1])
+        b0, b1 = int(rowptr[r2]), int(rowptr[r2 + 1])
+        cc = np.concatenate([colidx[a0:a1], colidx[b0:b1]]).astype(np.int64)
+        vals2 = np.concatenate([(vv[a0:a1].astype(np.uint64) * c1) % p,
+                                (vv[b0:b1].astype(np.uint64) * c2) % p])
+        u, inv = np.unique(cc, return_inverse=True)
+        acc = np.zeros(len(u), dtype=np.uint64)
+        np.add.at(acc, inv, vals2)
+        acc %= p
+        keep = acc != 0
+        rows_c[int(r)] = (u[keep].astype(np.uint32), acc[keep].astype(np.uint32))
+    if not rows_c:
+        return X
+    lens = np.diff(rowptr).astype(np.int64)
+    for r, (c_, v_) in rows_c.items():
+        lens[r] = len(c_)
+    rp2 = np.zeros(mm + 1, dtype=np.uint64)
+    rp2[1:] = np.cumsum(lens)
+    ci2 = np.empty(int(rp2[-1]), dtype=np.uint32)
+    v2 = np.empty(int(rp2[-1]), dtype=np.uint32)
+    keep_rows = np.ones(mm, dtype=bool)
+    keep_rows[list(rows_c)] = False
+    src_rows = np.repeat(keep_rows, np.diff(rowptr).astype(np.int64))
+    dst_rows = np.repeat(keep_rows, lens)
+    ci2[dst_rows] = colidx[src_rows]
+    v2[dst_rows] = vv[src_rows]
+    for r, (c_, v_) in rows_c.items():
+        ci2[int(rp2[r]):int(rp2[r + 1])] = c_
+        v2[int(rp2[r]):int(rp2[r + 1])] = v_
+    return CSR(mm, n, rp2, ci2, v2)

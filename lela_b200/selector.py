@@ -1,17 +1,20 @@
 """Autotuner and learned kernel selector.
 
 Several kernels compute the same exact result for a block (Z/p gemm on the
-tensor cores or on CUDA cores; GF(2) gemm int8-expanded on the tensor cores
-or bit-packed four-Russians; a dense echelon block in one CTA's shared
-memory or through the panel pipeline with tensor-core or CUDA-core
-updates).  Which is fastest depends on the block.
+tensor cores, with wide tiles or with tiles of two accumulator buffers, or
+on CUDA cores, plain or small-K; GF(2) gemm int8-expanded on the tensor
+cores or bit-packed four-Russians; a dense echelon block in one CTA's shared
+memory or through the panel pipeline with tensor-core updates of either
+tile variant or CUDA-core updates).  Which is fastest depends on the block.
 
-* ``Autotuner`` times every candidate on a block (exhaustive search) and
-  records ``{op, features, kernel, ms}`` lines (JSONL).
-* ``CostModel`` is a fully connected FP32 network (13 -> 64 -> 64 -> 1,
-  ReLU) that predicts log time from the block features and the kernel.  It
-  is trained on the GPU by the library's own forward / backward / Adam
-  kernels (``lela_cuda_mlp_*``) from the autotuner's records.
+* ``Autotuner`` times every candidate (kernel and tile variant) on a block
+  (exhaustive search) and records ``{op, features, kernel, ms}`` lines
+  (JSONL).
+* ``CostModel`` is a fully connected FP32 network (14 -> 64 -> 64 -> 1,
+  ReLU) that predicts log time from the block features and a description
+  of the candidate (operation, kernel family, tile variant).  It is trained
+  on the GPU by the library's own forward / backward / Adam kernels
+  (``lela_cuda_mlp_*``) from the autotuner's records.
 * ``Selector`` picks the candidate with the smallest predicted time, and
   falls back to exhaustive tuning when no model is loaded.
 
@@ -26,24 +29,43 @@ import numpy as np
 
 from . import api
 
-# (op, kernel) categories, one-hot in the features
-CATEGORIES = [("gemm", 1), ("gemm", 2), ("gf2_gemm", 1), ("gf2_gemm", 2),
-              ("echelon", 1), ("echelon", 2), ("echelon", 3)]
-KERNEL_NAMES = {("gemm", 1): "zp CUDA-core", ("gemm", 2): "zp tensor-core",
+# Candidates per operation: kernel id -> (kernel family, tile variant).
+# Families: "plain" (CUDA-core delayed-reduction products), "small" (a
+# CUDA-core kernel for small work: the small-K gemm, bit-packed
+# four-Russians, the one-CTA shared-memory echelon), "tc" (tensor cores).
+# Tiles (tensor cores): "wide" (one accumulator buffer for two and four
+# limbs) or "double" (two buffers, the epilogue overlapping the next tile).
+# The ids are the ones the library takes: lela_cuda_set_gemm_kernel /
+# set_gemm_tile for gemm, lela_cuda_set_gf2_kernel, and the per-block
+# kernel of lela_cuda_echelon_zp_u32_batch.
+KERNELS = {
+    "gemm": {1: ("plain", None), 2: ("tc", "wide"), 3: ("small", None), 4: ("tc", "double")},
+    "gf2_gemm": {1: ("tc", "wide"), 2: ("small", None)},
+    "echelon": {1: ("small", None), 2: ("tc", "wide"), 3: ("plain", None), 4: ("tc", "double")},
+}
+KERNEL_NAMES = {("gemm", 1): "zp CUDA-core (plain)", ("gemm", 2): "zp tensor-core, wide tiles",
+                ("gemm", 3): "zp CUDA-core small-K", ("gemm", 4): "zp tensor-core, double-buffered tiles",
                 ("gf2_gemm", 1): "gf2 tensor-core", ("gf2_gemm", 2): "gf2 four-Russians",
-                ("echelon", 1): "echelon shared-memory batch", ("echelon", 2): "echelon panels, TC updates",
-                ("echelon", 3): "echelon panels, CUDA-core updates"}
+                ("echelon", 1): "echelon shared-memory batch",
+                ("echelon", 2): "echelon panels, TC updates (wide tiles)",
+                ("echelon", 3): "echelon panels, CUDA-core updates",
+                ("echelon", 4): "echelon panels, TC updates (double-buffered tiles)"}
 DEFAULT = {"gemm": 2, "gf2_gemm": 1, "echelon": 2}   # the choice without a model
-NFEAT = 6 + len(CATEGORIES)
+OPS = ("gemm", "gf2_gemm", "echelon")
+FAMILIES = ("plain", "small", "tc")
+NFEAT = 6 + len(OPS) + len(FAMILIES) + 2
 
 
-def candidates(op, m, n, k):
+def candidates(op, m, n, k, pbits=16):
+    """Kernel ids worth timing for this block (four-limb moduli have one
+    tensor-core tile variant; the shared-memory echelon kernel takes blocks
+    of at most 200 KB)."""
     if op == "gemm":
-        return [1, 2]
+        return [1, 2, 3] + ([4] if pbits <= 16 else [])
     if op == "gf2_gemm":
         return [1, 2]
     if op == "echelon":
-        c = [2, 3]
+        c = [2, 3] + ([4] if pbits <= 16 else [])
         if m * n * 4 <= 200 * 1024:
             c.insert(0, 1)
         return c
@@ -52,12 +74,15 @@ def candidates(op, m, n, k):
 
 def features(op, kernel, m, n, k, density, pbits, pivots):
     """Numeric block features (m, n, k, density, bits of p, pivot count,
-    log-scaled) followed by the one-hot (op, kernel) category."""
+    log-scaled), then the candidate: one-hot operation, one-hot kernel
+    family, and the tile variant (wide, double) of a tensor-core kernel."""
     lg = lambda v: math.log2(max(1.0, float(v))) / 16.0
     f = [lg(m), lg(n), lg(k), float(density), float(pbits) / 32.0, lg(pivots)]
-    onehot = [0.0] * len(CATEGORIES)
-    onehot[CATEGORIES.index((op, kernel))] = 1.0
-    return f + onehot
+    fam, tile = KERNELS[op][kernel]
+    f += [1.0 if op == o else 0.0 for o in OPS]
+    f += [1.0 if fam == x else 0.0 for x in FAMILIES]
+    f += [1.0 if tile == "wide" else 0.0, 1.0 if tile == "double" else 0.0]
+    return f
 
 
 class CostModel:
@@ -175,10 +200,10 @@ class Autotuner:
         t = lambda x: torch.from_numpy(x.view(np.int32)).cuda()
         A, B, C = t(gen.dense_zp(seed, m, k, p)), t(gen.dense_zp(seed + 1, k, n, p)), t(gen.dense_zp(seed + 2, m, n, p))
         out = {}
-        for kern in candidates("gemm", m, n, k):
-            self.cm.set_gemm_kernel(kern)
+        for kern in candidates("gemm", m, n, k, p.bit_length()):
+            set_gemm_choice(self.cm, kern)
             out[kern] = self._time(lambda: self.cm.gemm(p, 1, A, B, 1, C))
-        self.cm.set_gemm_kernel(0)
+        set_gemm_choice(self.cm, 0)
         return self._record("gemm", m, n, k, 1.0, p.bit_length(), 0, out)
 
     def tune_gf2_gemm(self, m, n, k, seed=0):
@@ -203,7 +228,7 @@ class Autotuner:
         src = torch.from_numpy(gen.dense_zp(seed, m, n, p).view(np.int32)).cuda()
         work = torch.empty_like(src)
         out = {}
-        for kern in candidates("echelon", m, n, 0):
+        for kern in candidates("echelon", m, n, 0, p.bit_length()):
             def run():
                 work.copy_(src)
                 self.cm.echelonize_batch([work], [p], kernels=[kern])
@@ -238,6 +263,14 @@ def group_blocks(records):
     return blocks
 
 
+def set_gemm_choice(cm, kern):
+    """Apply a gemm kernel id of KERNELS (0: the library's automatic
+    choice) to a module handle."""
+    kernel, tile = {0: (0, 0), 1: (1, 0), 2: (2, 1), 3: (3, 0), 4: (2, 2)}[kern]
+    cm.set_gemm_kernel(kernel)
+    cm.set_gemm_tile(tile)
+
+
 class Selector:
     """Pick a kernel per block: the cost model's argmin, else exhaustive."""
 
@@ -245,7 +278,7 @@ class Selector:
         self.model, self.tuner = model, tuner
 
     def choose(self, op, m, n, k, density, pbits, pivots):
-        cands = candidates(op, m, n, k)
+        cands = candidates(op, m, n, k, pbits)
         if self.model is None:
             return DEFAULT[op]
         X = [features(op, c, m, n, k, density, pbits, pivots) for c in cands]

@@ -155,3 +155,40 @@ def test_gemm_host_row_blocks(cuda, p):
         mask[20:1220, 40:560] = False
         assert np.array_equal(Cbig[mask], before[mask])
         C[...] = want                         # next case starts from this C
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("tile", [api.GEMM_TILE_WIDE, api.GEMM_TILE_DOUBLE])
+@pytest.mark.parametrize("p", [251, 65521, 2147483647])
+def test_gemm_tile_variants(cuda, tile, p):
+    """Both tensor-core tile variants (one accumulator buffer / two) on
+    ragged shapes, every epilogue mode (C += AB, C -= AB, C = aAB,
+    aAB + bC), and device matrices whose row strides and column offsets
+    are not multiples of four entries (the epilogue's 16-byte loads and
+    stores fall back to single entries there)."""
+    import torch
+    cuda.set_gemm_kernel(api.GEMM_TC)
+    cuda.set_gemm_tile(tile)
+    dev = lambda x: torch.from_numpy(np.ascontiguousarray(x).view(np.int32)).cuda()
+    try:
+        for si, (m, n, k) in enumerate([(130, 257, 300), (300, 130, 40), (257, 515, 2100),
+                                        (129, 67, 5)]):
+            A = gen.dense_zp(70 + si, m, k, p)
+            B = gen.dense_zp(80 + si, k, n, p)
+            for ci, (a, b) in enumerate([(1, 1), (p - 1, 1), (3, 0), (7, 11)]):
+                C = gen.dense_zp(90 + 10 * si + ci, m, n, p)
+                want = oracle.gemm_zp(p, A, B, C, a, b)
+                got = cuda.gemm(p, a, A, B, b, C.copy())
+                assert np.array_equal(got, want), (tile, p, m, n, k, a, b, "host")
+                # device: C a view at column 1 of a wider matrix (stride n + 3)
+                W = np.zeros((m, n + 3), dtype=np.uint32)
+                W[:, 1:n + 1] = C
+                dW = dev(W)
+                cuda.gemm(p, a, dev(A), dev(B), b, dW[:, 1:n + 1])
+                cuda.synchronize()
+                gw = dW.cpu().numpy().view(np.uint32)
+                assert np.array_equal(gw[:, 1:n + 1], want), (tile, p, m, n, k, a, b, "view")
+                assert not gw[:, 0].any() and not gw[:, n + 1:].any()
+    finally:
+        cuda.set_gemm_kernel(api.GEMM_AUTO)
+        cuda.set_gemm_tile(api.GEMM_TILE_AUTO)

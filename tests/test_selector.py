@@ -54,32 +54,34 @@ def test_mlp_training_reduces_loss(cuda):
 
 @pytest.mark.gpu
 def test_selector_gain_and_regret(cuda):
-    """Autotune a family of blocks (every candidate timed), train the cost
-    model on half of them, and evaluate on the other half: the model's picks
-    must beat the fixed default choices and stay close to exhaustive
-    tuning."""
+    """Autotune a family of blocks (every candidate kernel and tile variant
+    timed), train the cost model on two thirds of them, and evaluate on the
+    held-out third: the model's picks must beat the fixed default choices
+    and stay within 15 % of exhaustive tuning (total time of the held-out
+    blocks)."""
     tuner = sel.Autotuner(cuda, reps=3)
     rng = np.random.default_rng(5)
-    for i in range(28):
-        s = int(2 ** rng.uniform(5, 11))
-        tuner.tune_gemm(s, int(2 ** rng.uniform(5, 11)), int(2 ** rng.uniform(5, 11)),
-                        int(rng.choice([251, 65521, 2147483647])), seed=i)
-    for i in range(16):
+    for i in range(48):
+        m, n = int(2 ** rng.uniform(6, 12)), int(2 ** rng.uniform(6, 12))
+        k = int(2 ** rng.uniform(4, 12)) if i % 2 else int(2 ** rng.uniform(4, 8))
+        tuner.tune_gemm(m, n, k, int(rng.choice([251, 65521, 2147483647])), seed=i)
+    for i in range(20):
         tuner.tune_gf2_gemm(int(2 ** rng.uniform(6, 12)), int(2 ** rng.uniform(6, 12)),
                             int(2 ** rng.uniform(6, 12)), seed=i)
-    for i in range(16):
-        s = int(2 ** rng.uniform(5, 9.5))
-        tuner.tune_echelon(s, s, int(rng.choice([251, 65521, 2147483647])), seed=i)
+    for i in range(24):
+        s_ = int(2 ** rng.uniform(5, 10))
+        tuner.tune_echelon(s_, s_, int(rng.choice([251, 65521, 2147483647])), seed=i)
     blocks = sel.group_blocks(tuner.records)
     keys = sorted(blocks)
     rng.shuffle(keys)
+    held = set(keys[::3])
     train = [r for r in tuner.records
-             if (r["op"], r["m"], r["n"], r["k"], r["density"], r["pbits"], r["pivots"]) in set(keys[::2])]
-    test_blocks = {k: blocks[k] for k in keys[1::2]}
+             if (r["op"], r["m"], r["n"], r["k"], r["density"], r["pbits"], r["pivots"]) not in held]
+    test_blocks = {k: blocks[k] for k in held}
     X, y = sel.records_to_xy(train)
     model = sel.CostModel(cuda, seed=6)
-    model.fit(X, y, epochs=800, lr=3e-3)
+    model.fit(X, y, epochs=1500, lr=3e-3)
     res = sel.evaluate(sel.Selector(model), test_blocks)
     print(res)
     assert res["gain_vs_default"] > 1.0
-    assert res["regret"] < 0.5
+    assert res["regret"] <= 0.15

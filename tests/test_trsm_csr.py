@@ -85,3 +85,39 @@ def test_trsm_csr_upper_device_and_errors(cuda):
     bad_dev = torch.from_numpy(bad.view(np.int32)).cuda()
     with pytest.raises(PreconditionFailed):
         cuda.trsm_csr_upper(p, 1, n, dev[0], bad_dev, dev[2], dev[3].clone())
+
+
+def _banded_upper(seed, n, p, unit, band, holes):
+    """Upper triangular with nonzeros only within `band` columns right of the
+    diagonal, minus square holes (row0, col0, size) -- the shape of F4 pivot
+    blocks, whose 64 x 64 tiles away from the diagonal are mostly zero."""
+    U = gen.upper_zp(seed, n, p, unit=unit)
+    i, j = np.indices((n, n))
+    U[(j - i) > band] = 0
+    for r0, c0, s in holes:
+        U[r0:r0 + s, c0:c0 + s] = np.where(np.eye(s, dtype=bool) & (r0 == c0), U[r0:r0 + s, c0:c0 + s], 0)
+    return U.astype(np.uint32)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kernel", [1, 2])
+@pytest.mark.parametrize("p", [65521, 2147483647])
+def test_trsm_csr_upper_banded(cuda, kernel, p):
+    """Banded sparse operands (most off-diagonal tiles empty): the updates
+    are trimmed to the occupied tiles' bounding boxes; alpha != 1 (rows of
+    B outside a box are only scaled), for both diagonal-block solvers."""
+    from lela_b200 import api
+    cuda.set_trsm_kernel(kernel)
+    try:
+        for n, ncols, band, holes in [(1500, 130, 300, [(0, 600, 400)]),
+                                      (2600, 70, 700, [(1024, 1100, 300), (100, 400, 200)]),
+                                      (700, 33, 0, [])]:
+            U = _banded_upper(n + band, n, p, False, band, holes)
+            rowptr, colidx, vals = _csr(U)
+            B = gen.dense_zp(n + 7, n, ncols, p)
+            for a in (1, 12345):
+                want, _ = oracle.trsm_zp(p, U, B, 1, 0, a)
+                got = cuda.trsm_csr_upper(p, a, n, rowptr, colidx, vals, B.copy(), False)
+                assert np.array_equal(got, want), (kernel, p, n, band, a)
+    finally:
+        cuda.set_trsm_kernel(api.TRSM_AUTO)
