@@ -55,7 +55,8 @@ enum {
 	LELA_CUDA_WRONG_MATRIX_FORM = 5,
 	LELA_CUDA_PIVOT_NOT_INVERTIBLE = 6,
 	LELA_CUDA_ERR_TIMEOUT = 7,
-	LELA_CUDA_ERR_UNSUPPORTED = 8
+	LELA_CUDA_ERR_UNSUPPORTED = 8,
+	LELA_CUDA_ERR_CAPACITY = 9  /* an output array is too small; see the call */
 };
 
 /* Kernel choice for the Z/p gemm (lela_cuda_set_gemm_kernel). */
@@ -224,6 +225,34 @@ int lela_cuda_fl_echelonize_zp_u32_dev (lela_cuda_ctx *ctx, size_t m, size_t n, 
 					const uint32_t *vals, int reduced, int only_D, uint32_t *R,
 					size_t ldr, size_t *rank, uint32_t *det, size_t *out_rows,
 					size_t *bad_row);
+/* The same, with R returned as CSR rows -- the SparseMatrix<uint32> the
+ * reference writes (faugere-lachartre.tcc:860-911): R_rowptr[*out_rows + 1]
+ * (room for m + 1 entries), R_colidx / R_vals with room for R_cap entries,
+ * column indices strictly increasing within a row.  No dense m x n array
+ * is formed (at m = 120000 that would be 69 GB).  *R_nnz = the result's
+ * entries.  When R_cap < *R_nnz the call writes R_rowptr, returns
+ * LELA_CUDA_ERR_CAPACITY and keeps the result in the handle until its next
+ * Faugere-Lachartre call: lela_cuda_fl_csr_fetch copies the entries out
+ * then.  Other statuses as above.  _csr takes host arrays, _csr_dev device
+ * arrays (asynchronous apart from one synchronisation that sizes the
+ * result). */
+int lela_cuda_fl_echelonize_zp_u32_csr (lela_cuda_ctx *ctx, size_t m, size_t n, uint32_t p,
+					const uint64_t *rowptr, const uint32_t *colidx,
+					const uint32_t *vals, int reduced, int only_D,
+					uint64_t *R_rowptr, uint32_t *R_colidx, uint32_t *R_vals,
+					size_t R_cap, size_t *R_nnz, size_t *rank, uint32_t *det,
+					size_t *out_rows, size_t *bad_row);
+int lela_cuda_fl_echelonize_zp_u32_csr_dev (lela_cuda_ctx *ctx, size_t m, size_t n, uint32_t p,
+					    const uint64_t *rowptr, const uint32_t *colidx,
+					    const uint32_t *vals, int reduced, int only_D,
+					    uint64_t *R_rowptr, uint32_t *R_colidx, uint32_t *R_vals,
+					    size_t R_cap, size_t *R_nnz, size_t *rank, uint32_t *det,
+					    size_t *out_rows, size_t *bad_row);
+/* Copies the kept CSR result's column indices and values (cap >= its entry
+ * count) into host (device = 0) or device (device != 0) arrays.  No
+ * counterpart in the reference. */
+int lela_cuda_fl_csr_fetch (lela_cuda_ctx *ctx, uint32_t *colidx, uint32_t *vals, size_t cap,
+			    int device);
 
 /* ----------------------------------------------------------------- GF(2)
  * Packed rows (bit j of 64-bit word w = column 64w + j), strides in words.

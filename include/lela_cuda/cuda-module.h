@@ -349,12 +349,22 @@ public:
 			}
 			rowptr[i + 1] = colidx.size ();
 		}
-		std::vector<uint32_t> dense (m * n + 1);
-		size_t rk = 0, rows = 0, bad = 0;
+		// the result comes back as CSR rows (no dense m x n array); the
+		// first guess of its size is twice X's entries, and a larger result
+		// is fetched from the handle after the call
+		std::vector<uint64_t> rrow (m + 1, 0);
+		std::vector<uint32_t> rcol (2 * colidx.size () + 1), rval (2 * colidx.size () + 1);
+		size_t rk = 0, rows = 0, bad = 0, nnz = 0;
 		uint32_t d = 1;
-		int st = lela_cuda_fl_echelonize_zp_u32 (ctx.M.cuda.get (), m, n, ctx.F._modulus, &rowptr[0],
-							 colidx.empty () ? 0 : &colidx[0], vals.empty () ? 0 : &vals[0],
-							 reduced, only_D, &dense[0], n, &rk, &d, &rows, &bad);
+		int st = lela_cuda_fl_echelonize_zp_u32_csr (ctx.M.cuda.get (), m, n, ctx.F._modulus, &rowptr[0],
+							     colidx.empty () ? 0 : &colidx[0], vals.empty () ? 0 : &vals[0],
+							     reduced, only_D, &rrow[0], &rcol[0], &rval[0], rcol.size (),
+							     &nnz, &rk, &d, &rows, &bad);
+		if (st == LELA_CUDA_ERR_CAPACITY) {
+			rcol.resize (nnz);
+			rval.resize (nnz);
+			st = lela_cuda_fl_csr_fetch (ctx.M.cuda.get (), &rcol[0], &rval[0], nnz, 0);
+		}
 		rank = rk;
 		det = d;
 		if (st == LELA_CUDA_WRONG_MATRIX_FORM)
@@ -369,9 +379,8 @@ public:
 			r->clear ();
 			if (i >= rows)
 				continue;
-			for (size_t j = 0; j < n; ++j)
-				if (dense[i * n + j])
-					r->push_back (typename Matrix::Row::value_type (j, dense[i * n + j]));
+			for (uint64_t e = rrow[i]; e < rrow[i + 1]; ++e)
+				r->push_back (typename Matrix::Row::value_type (rcol[e], rval[e]));
 		}
 	}
 };

@@ -24,7 +24,7 @@ _S = ctypes.c_size_t
 _U = ctypes.c_uint32
 _I = ctypes.c_int
 
-OK, ERR_ARG, ERR_CUDA, ERR_NOMEM, DIAG, WRONG_FORM, PIVOT, TIMEOUT, UNSUPPORTED = range(9)
+OK, ERR_ARG, ERR_CUDA, ERR_NOMEM, DIAG, WRONG_FORM, PIVOT, TIMEOUT, UNSUPPORTED, ERR_CAPACITY = range(10)
 GEMM_AUTO, GEMM_PLAIN, GEMM_TC, GEMM_SMALLK = 0, 1, 2, 3
 GEMM_TILE_AUTO, GEMM_TILE_WIDE, GEMM_TILE_DOUBLE = 0, 1, 2
 TRSM_AUTO, TRSM_BLOCKS, TRSM_INVERSE = 0, 1, 2
@@ -121,6 +121,15 @@ def _bind_optional(L):
         "lela_cuda_fl_echelonize_zp_u32_dev": [_P, _S, _S, _U, _P, _P, _P, _I, _I, _P, _S,
                                                ctypes.POINTER(_S), ctypes.POINTER(_U),
                                                ctypes.POINTER(_S), ctypes.POINTER(_S)],
+        "lela_cuda_fl_echelonize_zp_u32_csr": [_P, _S, _S, _U, _P, _P, _P, _I, _I, _P, _P, _P, _S,
+                                               ctypes.POINTER(_S), ctypes.POINTER(_S),
+                                               ctypes.POINTER(_U), ctypes.POINTER(_S),
+                                               ctypes.POINTER(_S)],
+        "lela_cuda_fl_echelonize_zp_u32_csr_dev": [_P, _S, _S, _U, _P, _P, _P, _I, _I, _P, _P, _P, _S,
+                                                   ctypes.POINTER(_S), ctypes.POINTER(_S),
+                                                   ctypes.POINTER(_U), ctypes.POINTER(_S),
+                                                   ctypes.POINTER(_S)],
+        "lela_cuda_fl_csr_fetch": [_P, _P, _P, _S, _I],
         "lela_cuda_gemm_gf2": [_P, _S, _S, _S, _I, _P, _S, _P, _S, _I, _P, _S],
         "lela_cuda_gemm_gf2_dev": [_P, _S, _S, _S, _I, _P, _S, _P, _S, _I, _P, _S],
         "lela_cuda_echelon_gf2": [_P, _S, _S, _P, _S, ctypes.POINTER(_S)],
@@ -350,6 +359,56 @@ class CudaModule:
         self._raise(st, bad.value)
         return R[:rows.value], rk.value, det.value
 
+
+    def fl_echelonize_csr(self, p, X, reduced=True, only_D=False, cap=None):
+        """FaugereLachartre::echelonize with the result as CSR rows (the
+        SparseMatrix the reference writes; no dense m x n array).  X as for
+        fl_echelonize (numpy arrays: host path; torch CUDA tensors: device
+        path, output tensors on the device).  Returns (R, rank, det) with R
+        a gen.CSR of out_rows rows (host) or an object with m, n, rowptr,
+        colidx, vals tensors (device).  cap: first guess of the entry count
+        (the result is fetched again when it holds more)."""
+        m, n = X.m, X.n
+        rk, det, rows, bad, nnz = _S(0), _U(0), _S(0), _S(0), _S(0)
+        if _is_torch(X.rowptr):
+            import torch
+            import types
+            dev = X.rowptr.device
+            cap = int(cap if cap is not None else max(1, 2 * int(X.colidx.numel())))
+            rp = torch.empty(m + 1, dtype=torch.int64, device=dev)
+            ci = torch.empty(max(cap, 1), dtype=torch.int32, device=dev)
+            va = torch.empty(max(cap, 1), dtype=torch.int32, device=dev)
+            st = self.L.lela_cuda_fl_echelonize_zp_u32_csr_dev(
+                self.h, m, n, p, _dptr(X.rowptr), _dptr(X.colidx), _dptr(X.vals), int(reduced),
+                int(only_D), _dptr(rp), _dptr(ci), _dptr(va), cap, ctypes.byref(nnz),
+                ctypes.byref(rk), ctypes.byref(det), ctypes.byref(rows), ctypes.byref(bad))
+            if st == ERR_CAPACITY:
+                ci = torch.empty(max(nnz.value, 1), dtype=torch.int32, device=dev)
+                va = torch.empty(max(nnz.value, 1), dtype=torch.int32, device=dev)
+                st = self.L.lela_cuda_fl_csr_fetch(self.h, _dptr(ci), _dptr(va), nnz.value, 1)
+            self._raise(st, bad.value)
+            R = types.SimpleNamespace(m=rows.value, n=n, rowptr=rp[:rows.value + 1],
+                                      colidx=ci[:nnz.value], vals=va[:nnz.value])
+            return R, rk.value, det.value
+        rowptr = np.ascontiguousarray(X.rowptr, dtype=np.uint64)
+        colidx = np.ascontiguousarray(X.colidx, dtype=np.uint32)
+        vals = np.ascontiguousarray(X.vals, dtype=np.uint32)
+        cap = int(cap if cap is not None else max(1, 2 * len(colidx)))
+        rp = np.zeros(m + 1, dtype=np.uint64)
+        ci = np.zeros(max(cap, 1), dtype=np.uint32)
+        va = np.zeros(max(cap, 1), dtype=np.uint32)
+        st = self.L.lela_cuda_fl_echelonize_zp_u32_csr(
+            self.h, m, n, p, _ptr(rowptr), _ptr(colidx), _ptr(vals), int(reduced), int(only_D),
+            _ptr(rp), _ptr(ci), _ptr(va), cap, ctypes.byref(nnz), ctypes.byref(rk),
+            ctypes.byref(det), ctypes.byref(rows), ctypes.byref(bad))
+        if st == ERR_CAPACITY:
+            ci = np.zeros(max(nnz.value, 1), dtype=np.uint32)
+            va = np.zeros(max(nnz.value, 1), dtype=np.uint32)
+            st = self.L.lela_cuda_fl_csr_fetch(self.h, _ptr(ci), _ptr(va), nnz.value, 0)
+        self._raise(st, bad.value)
+        from .gen import CSR
+        return (CSR(rows.value, n, rp[:rows.value + 1], ci[:nnz.value], va[:nnz.value]),
+                rk.value, det.value)
 
     # ------------------------------------------------------------- GF(2)
     def set_gf2_kernel(self, kernel):

@@ -318,6 +318,7 @@ const char *lela_cuda_status_string(int s) {
     case ST_PIVOT: return "pivot not invertible in the ring";
     case ST_TIMEOUT: return "device-side wait timed out";
     case ST_UNSUPPORTED: return "unsupported";
+    case ST_CAPACITY: return "output capacity too small";
     default: return "unknown status";
   }
 }
@@ -728,6 +729,117 @@ static int fl_finish(Ctx *c, int st, const FlResult &r, size_t *rank, uint32_t *
   return st;
 }
 
+// Host CSR input of the Faugere-Lachartre entry points: checked, copied to
+// the device (BUF_FL_X), row heads taken on the host.
+struct FlHostInput {
+  uint64_t *d_rowptr = nullptr;
+  uint32_t *d_col = nullptr, *d_val = nullptr;
+  std::vector<uint32_t> heads, hv;
+};
+
+static int fl_host_input(Ctx *c, size_t m, size_t n, const uint64_t *rowptr,
+                         const uint32_t *colidx, const uint32_t *vals, FlHostInput *in) {
+  const uint64_t nnz = rowptr[m];
+  if (nnz && (!colidx || !vals)) return ctx_fail(c, ST_ARG, "null pointer");
+  for (size_t r = 0; r < m; ++r)
+    if (rowptr[r + 1] < rowptr[r]) return ctx_fail(c, ST_ARG, "row pointers decrease");
+  for (uint64_t e = 0; e < nnz; ++e)
+    if (colidx[e] >= n) return ctx_fail(c, ST_ARG, "column index out of range");
+  in->heads.assign(m, 0);
+  in->hv.assign(m, 0);
+  for (size_t r = 0; r < m; ++r) {
+    const bool empty = rowptr[r + 1] == rowptr[r];
+    in->heads[r] = empty ? 0 : colidx[rowptr[r]];
+    in->hv[r] = empty ? 0 : vals[rowptr[r]];
+  }
+  void *dX = nullptr;
+  const size_t xbytes = (m + 1) * 8 + nnz * 8 + 64;
+  int st = ctx_buffer(c, BUF_FL_X, xbytes, &dX);
+  if (st) return st;
+  in->d_rowptr = (uint64_t *)dX;
+  in->d_col = (uint32_t *)(in->d_rowptr + m + 1);
+  in->d_val = in->d_col + nnz;
+  cudaError_t e = cudaMemcpyAsync(in->d_rowptr, rowptr, (m + 1) * 8, cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess && nnz)
+    e = cudaMemcpyAsync(in->d_col, colidx, nnz * 4, cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess && nnz)
+    e = cudaMemcpyAsync(in->d_val, vals, nnz * 4, cudaMemcpyHostToDevice, c->stream);
+  if (e != cudaSuccess) return ctx_cuda(c, e, "fl: input copy");
+  return ST_OK;
+}
+
+// Copies a CSR result out (kind: cudaMemcpyDeviceToHost or ToDevice):
+// the row pointers always, the entries when cap allows (else
+// ST_CAPACITY: the result stays in the handle for lela_cuda_fl_csr_fetch).
+static int fl_csr_out(Ctx *c, const FlCsr &csr, size_t rows, cudaMemcpyKind kind,
+                      uint64_t *R_rowptr, uint32_t *R_colidx, uint32_t *R_vals, size_t R_cap,
+                      size_t *R_nnz) {
+  if (R_nnz) *R_nnz = csr.nnz;
+  cudaError_t e = cudaMemcpyAsync(R_rowptr, csr.rowptr, (rows + 1) * 8, kind, c->stream);
+  if (e == cudaSuccess && csr.nnz && csr.nnz <= R_cap) {
+    e = cudaMemcpyAsync(R_colidx, csr.colidx, csr.nnz * 4, kind, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(R_vals, csr.vals, csr.nnz * 4, kind, c->stream);
+  }
+  if (e != cudaSuccess) return ctx_cuda(c, e, "fl: csr output copy");
+  if (csr.nnz > R_cap) {
+    e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return ctx_cuda(c, e, "fl: csr output copy");
+    return ctx_fail(c, ST_CAPACITY, "fl: the CSR result has more entries than the output arrays hold");
+  }
+  return ST_OK;
+}
+
+int lela_cuda_fl_echelonize_zp_u32_csr(lela_cuda_ctx *h, size_t m, size_t n, uint32_t p,
+                                       const uint64_t *rowptr, const uint32_t *colidx,
+                                       const uint32_t *vals, int reduced, int only_D,
+                                       uint64_t *R_rowptr, uint32_t *R_colidx, uint32_t *R_vals,
+                                       size_t R_cap, size_t *R_nnz, size_t *rank, uint32_t *det,
+                                       size_t *out_rows, size_t *bad_row) {
+  if (!h) return ST_ARG;
+  Ctx *c = &h->c;
+  if (m > (size_t)INT32_MAX || n > (size_t)INT32_MAX) return ctx_fail(c, ST_ARG, "dimension too large");
+  if (p < 2) return ctx_fail(c, ST_ARG, "modulus must be at least 2");
+  if (!rowptr || !R_rowptr || (R_cap && (!R_colidx || !R_vals)))
+    return ctx_fail(c, ST_ARG, "bad output or row pointers");
+  DeviceScope ds(c);
+  FlHostInput in;
+  int st = fl_host_input(c, m, n, rowptr, colidx, vals, &in);
+  if (!st) st = ctx_clear_status(c);
+  if (st) return st;
+  FlResult res{};
+  FlCsr csr;
+  st = zp_fl_echelonize_dev(c, (int)m, (int)n, p, in.d_rowptr, in.d_col, in.d_val, rowptr,
+                            in.heads.data(), in.hv.data(), reduced != 0, only_D != 0, nullptr, 0,
+                            &res, &csr);
+  if (st == ST_OK)
+    st = fl_csr_out(c, csr, res.out_rows, cudaMemcpyDeviceToHost, R_rowptr, R_colidx, R_vals,
+                    R_cap, R_nnz);
+  if (st == ST_CAPACITY) {
+    fl_finish(c, ST_OK, res, rank, det, out_rows, bad_row);
+    return ST_CAPACITY;
+  }
+  return fl_finish(c, st, res, rank, det, out_rows, bad_row);
+}
+
+int lela_cuda_fl_csr_fetch(lela_cuda_ctx *h, uint32_t *colidx, uint32_t *vals, size_t cap,
+                           int device) {
+  if (!h) return ST_ARG;
+  Ctx *c = &h->c;
+  if (c->fl_csr_nnz == (size_t)-1) return ctx_fail(c, ST_ARG, "fl: no CSR result kept");
+  const size_t nnz = c->fl_csr_nnz;
+  if (nnz > cap) return ctx_fail(c, ST_CAPACITY, "fl: the CSR result has more entries than cap");
+  if (nnz && (!colidx || !vals)) return ctx_fail(c, ST_ARG, "null pointer");
+  if (!nnz) return ST_OK;
+  DeviceScope ds(c);
+  const size_t col_bytes = (nnz * 4 + 255) & ~(size_t)255;
+  const uint8_t *b = static_cast<const uint8_t *>(c->buf[BUF_FL_CSR_V]);
+  const cudaMemcpyKind kind = device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  cudaError_t e = cudaMemcpyAsync(colidx, b, nnz * 4, kind, c->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(vals, b + col_bytes, nnz * 4, kind, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  return e == cudaSuccess ? ST_OK : ctx_cuda(c, e, "fl: csr fetch");
+}
+
 int lela_cuda_fl_echelonize_zp_u32(lela_cuda_ctx *h, size_t m, size_t n, uint32_t p,
                                    const uint64_t *rowptr, const uint32_t *colidx,
                                    const uint32_t *vals, int reduced, int only_D, uint32_t *R,
@@ -801,6 +913,47 @@ int lela_cuda_fl_echelonize_zp_u32_dev(lela_cuda_ctx *h, size_t m, size_t n, uin
   FlResult res{};
   st = zp_fl_echelonize_dev(c, (int)m, (int)n, p, rowptr, colidx, vals, hrow.data(), heads.data(),
                             hv.data(), reduced != 0, only_D != 0, R, ldr, &res);
+  return fl_finish(c, st, res, rank, det, out_rows, bad_row);
+}
+
+int lela_cuda_fl_echelonize_zp_u32_csr_dev(lela_cuda_ctx *h, size_t m, size_t n, uint32_t p,
+                                           const uint64_t *rowptr, const uint32_t *colidx,
+                                           const uint32_t *vals, int reduced, int only_D,
+                                           uint64_t *R_rowptr, uint32_t *R_colidx,
+                                           uint32_t *R_vals, size_t R_cap, size_t *R_nnz,
+                                           size_t *rank, uint32_t *det, size_t *out_rows,
+                                           size_t *bad_row) {
+  if (!h) return ST_ARG;
+  Ctx *c = &h->c;
+  DeviceScope ds(c);
+  if (m > (size_t)INT32_MAX || n > (size_t)INT32_MAX) return ctx_fail(c, ST_ARG, "dimension too large");
+  if (p < 2) return ctx_fail(c, ST_ARG, "modulus must be at least 2");
+  if (!rowptr || !R_rowptr || (R_cap && (!R_colidx || !R_vals)))
+    return ctx_fail(c, ST_ARG, "bad output or row pointers");
+  std::vector<uint64_t> hrow(m + 1);
+  std::vector<uint32_t> heads(m), hv(m);
+  void *dH = nullptr;
+  int st = ctx_buffer(c, BUF_FL_HEADS, 2 * (m + 1) * 4 + 64, &dH);
+  if (st) return st;
+  uint32_t *d_heads = (uint32_t *)dH, *d_hv = d_heads + m + 1;
+  if ((st = fl_row_heads_dev(c, (int)m, rowptr, colidx, vals, d_heads, d_hv))) return st;
+  cudaError_t e = cudaMemcpyAsync(hrow.data(), rowptr, (m + 1) * 8, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess && m)
+    e = cudaMemcpyAsync(heads.data(), d_heads, m * 4, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess && m) e = cudaMemcpyAsync(hv.data(), d_hv, m * 4, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return ctx_cuda(c, e, "fl: row heads");
+  FlResult res{};
+  FlCsr csr;
+  st = zp_fl_echelonize_dev(c, (int)m, (int)n, p, rowptr, colidx, vals, hrow.data(), heads.data(),
+                            hv.data(), reduced != 0, only_D != 0, nullptr, 0, &res, &csr);
+  if (st == ST_OK)
+    st = fl_csr_out(c, csr, res.out_rows, cudaMemcpyDeviceToDevice, R_rowptr, R_colidx, R_vals,
+                    R_cap, R_nnz);
+  if (st == ST_CAPACITY) {
+    fl_finish(c, ST_OK, res, rank, det, out_rows, bad_row);
+    return ST_CAPACITY;
+  }
   return fl_finish(c, st, res, rank, det, out_rows, bad_row);
 }
 

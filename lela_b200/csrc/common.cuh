@@ -18,6 +18,7 @@ enum : int {
   ST_PIVOT = 6,        // pivot not invertible in the ring (echelon)
   ST_TIMEOUT = 7,      // a bounded device-side wait expired
   ST_UNSUPPORTED = 8,  // configuration not supported by this build
+  ST_CAPACITY = 9,     // an output array is too small (the result is kept)
 };
 
 // Device-side error flags written by kernels (bit mask, OR-ed).

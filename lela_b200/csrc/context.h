@@ -95,6 +95,9 @@ struct Ctx {
   // search publishes its result and a sequence number; created on first use.
   void *panel_map = nullptr, *panel_map_dev = nullptr;
   uint32_t panel_seq = 0;
+  // Entries of the last Faugere-Lachartre CSR result kept in BUF_FL_CSR_V
+  // (SIZE_MAX: none), for lela_cuda_fl_csr_fetch.
+  size_t fl_csr_nnz = (size_t)-1;
   std::string last_error;
 
   // Instantiated CUDA graph of the small-block batch launch, replayed while
@@ -148,7 +151,9 @@ enum BufSlot : int {
   BUF_RED = 21,       // reduced echelon form: column maps, pivot block, solved columns
   BUF_TRI_OCC = 22,   // occupancy of a sparse triangular operand's 64 x 64 tiles
   BUF_FL_KR = 23,     // Faugere-Lachartre: per-row column ranges of A and C
-  BUF_COUNT = 24,
+  BUF_FL_CSR_P = 24,  // Faugere-Lachartre CSR output: row counts, row pointers, scan scratch
+  BUF_FL_CSR_V = 25,  // Faugere-Lachartre CSR output: column indices and values
+  BUF_COUNT = 26,
 };
 
 // Grow-only allocation helpers; return ST_OK or ST_NOMEM.

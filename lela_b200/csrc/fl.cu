@@ -28,6 +28,8 @@
 //      pivot-column order (the reduced row-echelon form is unique).
 //  non-reduced / only_D (:867-874, :906-911)  as the reference's
 //      MatrixGrid4/5 write them (see oracle/lela_oracle.c for the exact rows).
+#include <cub/device/device_scan.cuh>
+
 #include <algorithm>
 #include <vector>
 
@@ -120,6 +122,76 @@ __global__ void fl_assemble_kernel(uint32_t *__restrict__ R, size_t ldr, int row
   }
 }
 
+// CSR form of the rows fl_assemble_kernel writes (same plan), one warp per
+// row.  Count pass: cnt[o] = nonzero values of the row's source plus its
+// unit entry.  Fill pass (row pointers = exclusive sums of the counts): the
+// nonzero values in column order, the unit entry in its sorted place (the
+// value columns vcols are increasing and never hold the unit column).
+__global__ void fl_csr_count_kernel(int rows, const int *__restrict__ kind,
+                                    const int *__restrict__ src_row,
+                                    const int *__restrict__ unit_col,
+                                    const uint32_t *__restrict__ M1, size_t ld1,
+                                    const uint32_t *__restrict__ M2, size_t ld2, int nv,
+                                    uint64_t *__restrict__ cnt) {
+  const int lane = threadIdx.x & 31;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  for (int o = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; o < rows; o += warps) {
+    const int k = kind[o];
+    int c = 0;
+    if (k == 1 || k == 2) {
+      const uint32_t *src = k == 1 ? M1 + (size_t)src_row[o] * ld1 : M2 + (size_t)src_row[o] * ld2;
+      for (int j = lane; j < nv; j += 32) c += src[j] != 0u;
+      c = __reduce_add_sync(0xffffffffu, c);
+    }
+    if (lane == 0) cnt[o] = (uint64_t)c + ((k != 0 && unit_col[o] >= 0) ? 1u : 0u);
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) cnt[rows] = 0;
+}
+
+__global__ void fl_csr_fill_kernel(int rows, const int *__restrict__ kind,
+                                   const int *__restrict__ src_row,
+                                   const int *__restrict__ unit_col,
+                                   const uint32_t *__restrict__ M1, size_t ld1,
+                                   const uint32_t *__restrict__ M2, size_t ld2,
+                                   const int *__restrict__ vcols, int nv,
+                                   const uint64_t *__restrict__ rowptr,
+                                   uint32_t *__restrict__ colidx, uint32_t *__restrict__ vals) {
+  const int lane = threadIdx.x & 31;
+  const unsigned below = (1u << lane) - 1u;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  for (int o = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; o < rows; o += warps) {
+    const int k = kind[o];
+    if (k == 0) continue;
+    const uint64_t base = rowptr[o];
+    const int u = unit_col[o];
+    int before = 0;  // nonzero values left of the unit column
+    if (k == 1 || k == 2) {
+      const uint32_t *src = k == 1 ? M1 + (size_t)src_row[o] * ld1 : M2 + (size_t)src_row[o] * ld2;
+      if (u >= 0) {
+        for (int j = lane; j < nv; j += 32) before += (src[j] != 0u && vcols[j] < u);
+        before = __reduce_add_sync(0xffffffffu, before);
+      }
+      uint64_t run = 0;
+      for (int j0 = 0; j0 < nv; j0 += 32) {
+        const int j = j0 + lane;
+        const uint32_t v = j < nv ? src[j] : 0u;
+        const unsigned bal = __ballot_sync(0xffffffffu, v != 0u);
+        if (v != 0u) {
+          const int col = vcols[j];
+          const uint64_t at = base + run + __popc(bal & below) + ((u >= 0 && col > u) ? 1 : 0);
+          colidx[at] = (uint32_t)col;
+          vals[at] = v;
+        }
+        run += __popc(bal);
+      }
+    }
+    if (lane == 0 && u >= 0) {
+      colidx[base + before] = (uint32_t)u;
+      vals[base + before] = 1u;
+    }
+  }
+}
+
 __global__ void fl_heads_kernel(int m, const uint64_t *__restrict__ rowptr,
                                 const uint32_t *__restrict__ colidx,
                                 const uint32_t *__restrict__ vals, uint32_t *heads,
@@ -142,6 +214,54 @@ int fl_row_heads_dev(Ctx *c, int m, const uint64_t *d_rowptr, const uint32_t *d_
   return e == cudaSuccess ? ST_OK : ctx_cuda(c, e, "fl heads launch");
 }
 
+// The output rows of an assembly plan (kind, src_row, unit_col, vcols as
+// for fl_assemble_kernel, at d_plan) as CSR in the handle's buffers:
+// counts, exclusive scan (CUB), one synchronisation to size the entries,
+// fill.
+static int fl_assemble_csr(Ctx *c, int rows, const int *d_plan, const uint32_t *M1, size_t ld1,
+                           const uint32_t *M2, size_t ld2, int nv, FlCsr *csr) {
+  size_t temp = 0;
+  cudaError_t e = cub::DeviceScan::ExclusiveSum(nullptr, temp, (const uint64_t *)nullptr,
+                                                (uint64_t *)nullptr, rows + 1, c->stream);
+  if (e != cudaSuccess) return ctx_cuda(c, e, "fl: csr scan size");
+  const size_t cnt_bytes = ((size_t)(rows + 1) * 8 + 255) & ~(size_t)255;
+  void *vP = nullptr;
+  int st = ctx_buffer(c, BUF_FL_CSR_P, 2 * cnt_bytes + temp + 256, &vP);
+  if (st) return st;
+  uint8_t *b = static_cast<uint8_t *>(vP);
+  uint64_t *cnt = reinterpret_cast<uint64_t *>(b);
+  uint64_t *rowptr = reinterpret_cast<uint64_t *>(b + cnt_bytes);
+  void *d_temp = b + 2 * cnt_bytes;
+  const int *kind = d_plan, *srow = d_plan + rows, *ucol = d_plan + 2 * rows, *vcols = d_plan + 3 * rows;
+  const int grid = std::max(1, std::min((rows + 7) / 8, c->num_sms * 16));
+  int pi = prof_begin(c, "fl_assemble");
+  fl_csr_count_kernel<<<grid, 256, 0, c->stream>>>(rows, kind, srow, ucol, M1, ld1, M2, ld2, nv, cnt);
+  ctx_launched(c);
+  e = cub::DeviceScan::ExclusiveSum(d_temp, temp, cnt, rowptr, rows + 1, c->stream);
+  if (e != cudaSuccess) return ctx_cuda(c, e, "fl: csr scan");
+  uint64_t nnz = 0;
+  e = cudaMemcpyAsync(&nnz, rowptr + rows, 8, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return ctx_cuda(c, e, "fl: csr size");
+  void *vV = nullptr;
+  const size_t col_bytes = ((size_t)nnz * 4 + 255) & ~(size_t)255;
+  if ((st = ctx_buffer(c, BUF_FL_CSR_V, col_bytes + (size_t)nnz * 4 + 256, &vV))) return st;
+  uint32_t *colidx = static_cast<uint32_t *>(vV);
+  uint32_t *vals = reinterpret_cast<uint32_t *>(static_cast<uint8_t *>(vV) + col_bytes);
+  fl_csr_fill_kernel<<<grid, 256, 0, c->stream>>>(rows, kind, srow, ucol, M1, ld1, M2, ld2, vcols,
+                                                  nv, rowptr, colidx, vals);
+  ctx_launched(c);
+  prof_end(c, pi);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return ctx_cuda(c, e, "fl: csr fill");
+  csr->rowptr = rowptr;
+  csr->colidx = colidx;
+  csr->vals = vals;
+  csr->nnz = (size_t)nnz;
+  c->fl_csr_nnz = (size_t)nnz;
+  return ST_OK;
+}
+
 static int upload(Ctx *c, void *dst, const void *src, size_t bytes, const char *what) {
   if (!bytes) return ST_OK;
   cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->stream);
@@ -152,7 +272,8 @@ int zp_fl_echelonize_dev(Ctx *c, int m, int n, uint32_t p, const uint64_t *d_row
                          const uint32_t *d_colidx, const uint32_t *d_vals,
                          const uint64_t *h_rowptr, const uint32_t *h_heads,
                          const uint32_t *h_headvals, bool reduced, bool only_D, uint32_t *R,
-                         size_t ldr, FlResult *res) {
+                         size_t ldr, FlResult *res, FlCsr *csr) {
+  c->fl_csr_nnz = (size_t)-1;  // a kept CSR result is replaced by this call's
   res->rank = 0;
   res->det = 1 % p;
   res->out_rows = 0;
@@ -385,13 +506,25 @@ int zp_fl_echelonize_dev(Ctx *c, int m, int n, uint32_t p, const uint64_t *d_row
     if ((st = ctx_buffer(c, BUF_MISC, plan.size() * sizeof(int) + 64, &vP))) return st;
     int *d_plan = (int *)vP;
     if ((st = upload(c, d_plan, plan.data(), plan.size() * sizeof(int), "fl: plan"))) return st;
-    const int grid = std::min(out_rows, c->num_sms * 16);
-    int pi = prof_begin(c, "fl_assemble");
-    fl_assemble_kernel<<<grid, 256, 0, c->stream>>>(R, ldr, out_rows, n, d_plan, d_plan + out_rows,
-                                                    d_plan + 2 * out_rows, M1, ld1, M2, ld2,
-                                                    d_plan + 3 * out_rows, nv);
-    prof_end(c, pi);
-    ctx_launched(c);
+    if (csr) {
+      if ((st = fl_assemble_csr(c, out_rows, d_plan, M1, ld1, M2, ld2, nv, csr))) return st;
+    } else {
+      const int grid = std::min(out_rows, c->num_sms * 16);
+      int pi = prof_begin(c, "fl_assemble");
+      fl_assemble_kernel<<<grid, 256, 0, c->stream>>>(R, ldr, out_rows, n, d_plan, d_plan + out_rows,
+                                                      d_plan + 2 * out_rows, M1, ld1, M2, ld2,
+                                                      d_plan + 3 * out_rows, nv);
+      prof_end(c, pi);
+      ctx_launched(c);
+    }
+  } else if (csr) {
+    void *vP = nullptr;
+    if ((st = ctx_buffer(c, BUF_FL_CSR_P, 64, &vP))) return st;
+    csr->rowptr = static_cast<uint64_t *>(vP);
+    csr->nnz = 0;
+    cudaError_t e = cudaMemsetAsync(csr->rowptr, 0, 8, c->stream);
+    if (e != cudaSuccess) return ctx_cuda(c, e, "fl: csr output");
+    c->fl_csr_nnz = 0;
   }
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? ST_OK : ctx_cuda(c, e, "fl launch");

@@ -100,3 +100,50 @@ def test_fl_device_path(cuda):
     torch.cuda.synchronize()
     assert (gr, gd) == (want["rank"], want["det"])
     assert np.array_equal(R.cpu().numpy().view(np.uint32), want["R"])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("red,od", MODES)
+def test_fl_csr_output(cuda, red, od):
+    """The CSR form of the result (the SparseMatrix the reference writes)
+    against the dense one and the oracle: same rows, column indices strictly
+    increasing, every stored value nonzero; host and device paths; a first
+    guess of the capacity that is too small (the kept result is fetched)."""
+    import torch
+    p = 65521
+    for seed, m in ((1, 900), (2, 1500)):
+        X = gen.f4_matrix(300 + seed, m, p)
+        want = oracle.fl_echelonize_zp(p, X.m, X.n, X.rowptr, X.colidx, X.vals, red, od)
+        for cap in (None, 5):
+            R, gr, gd = cuda.fl_echelonize_csr(p, X, red, od, cap=cap)
+            assert (gr, gd) == (want["rank"], want["det"]), (m, red, od, cap)
+            assert R.m == want["R"].shape[0]
+            assert np.array_equal(R.to_dense(), want["R"]), (m, red, od, cap)
+            rows = np.repeat(np.arange(R.m), np.diff(R.rowptr).astype(np.int64))
+            d = np.diff(R.colidx.astype(np.int64))
+            assert (d[rows[1:] == rows[:-1]] > 0).all()
+            assert (R.vals != 0).all()
+        T = types.SimpleNamespace(m=X.m, n=X.n,
+                                  rowptr=torch.from_numpy(X.rowptr.view(np.int64)).cuda(),
+                                  colidx=torch.from_numpy(X.colidx.view(np.int32)).cuda(),
+                                  vals=torch.from_numpy(X.vals.view(np.int32)).cuda())
+        Rd, gr, gd = cuda.fl_echelonize_csr(p, T, red, od, cap=7)
+        torch.cuda.synchronize()
+        assert (gr, gd) == (want["rank"], want["det"])
+        Rh = gen.CSR(Rd.m, X.n, Rd.rowptr.cpu().numpy().view(np.uint64),
+                     Rd.colidx.cpu().numpy().view(np.uint32), Rd.vals.cpu().numpy().view(np.uint32))
+        assert np.array_equal(Rh.to_dense(), want["R"])
+
+
+@pytest.mark.gpu
+def test_fl_csr_edge_cases(cuda):
+    """Empty results (all rows zero; no D rows with only_D) and the fetch
+    without a kept result."""
+    p = 65521
+    for D in (np.zeros((3, 5), np.uint32), np.array([[0, 4, 0, 7]], np.uint32)):
+        X = gen.CSR.from_dense(D)
+        for red, od in MODES:
+            want = oracle.fl_echelonize_zp(p, X.m, X.n, X.rowptr, X.colidx, X.vals, red, od)
+            R, gr, gd = cuda.fl_echelonize_csr(p, X, red, od)
+            assert (gr, gd) == (want["rank"], want["det"])
+            assert np.array_equal(R.to_dense(), want["R"].reshape(R.m, X.n)), (D.shape, red, od)
