@@ -201,6 +201,23 @@ int lela_cuda_echelon_reduced_zp_u32_dev (lela_cuda_ctx *ctx, size_t m, size_t n
 					  uint32_t *A, size_t lda, int unit_pivots, size_t *rank,
 					  uint32_t *det);
 
+/* PLUQ decomposition of the m x n matrix A in place: replaces
+ * Elimination::pluq (lela/algorithms/elimination.h:196-209,
+ * elimination.tcc:266-370) with DensePivotStrategy.  On return A holds U on
+ * and above the diagonal (its columns in Q's order) and the multipliers of
+ * L below it, as the reference leaves them; P and Q receive the row and
+ * column transpositions as pairs (P[2t], P[2t+1]) in the reference's order
+ * (reversed, elimination.tcc:362-363), *np / *nq pairs each (room for
+ * min(m, n) pairs); *rank and *det = product of the pivots.
+ * LELA_CUDA_PIVOT_NOT_INVERTIBLE when a pivot cannot be inverted (A then
+ * unspecified).  The _dev form takes A on the device (P, Q on the host). */
+int lela_cuda_pluq_zp_u32 (lela_cuda_ctx *ctx, size_t m, size_t n, uint32_t p, uint32_t *A,
+			   size_t lda, size_t *P, size_t *np, size_t *Q, size_t *nq, size_t *rank,
+			   uint32_t *det);
+int lela_cuda_pluq_zp_u32_dev (lela_cuda_ctx *ctx, size_t m, size_t n, uint32_t p, uint32_t *A,
+			       size_t lda, size_t *P, size_t *np, size_t *Q, size_t *nq,
+			       size_t *rank, uint32_t *det);
+
 /* ------------------------------------------- Faugere-Lachartre echelon form
  * Echelon form of the F4 matrix X (m x n, CSR: rowptr[m+1], colidx, vals;
  * column indices strictly increasing within a row, stored values in [0,p)).

@@ -130,6 +130,10 @@ def _bind_optional(L):
                                                    ctypes.POINTER(_U), ctypes.POINTER(_S),
                                                    ctypes.POINTER(_S)],
         "lela_cuda_fl_csr_fetch": [_P, _P, _P, _S, _I],
+        "lela_cuda_pluq_zp_u32": [_P, _S, _S, _U, _P, _S, _P, ctypes.POINTER(_S), _P,
+                                  ctypes.POINTER(_S), ctypes.POINTER(_S), ctypes.POINTER(_U)],
+        "lela_cuda_pluq_zp_u32_dev": [_P, _S, _S, _U, _P, _S, _P, ctypes.POINTER(_S), _P,
+                                      ctypes.POINTER(_S), ctypes.POINTER(_S), ctypes.POINTER(_U)],
         "lela_cuda_gemm_gf2": [_P, _S, _S, _S, _I, _P, _S, _P, _S, _I, _P, _S],
         "lela_cuda_gemm_gf2_dev": [_P, _S, _S, _S, _I, _P, _S, _P, _S, _I, _P, _S],
         "lela_cuda_echelon_gf2": [_P, _S, _S, _P, _S, ctypes.POINTER(_S)],
@@ -327,6 +331,29 @@ class CudaModule:
         self._raise(st)
         return A, r.value, d.value
 
+
+    def pluq(self, p, A):
+        """Elimination::pluq in place: A <- L below the diagonal and U on and
+        above it (columns in Q's order); returns (A, P, Q, rank, det) with P
+        and Q lists of transposition pairs in the reference's order.  Host
+        numpy uint32 matrix or torch CUDA tensor."""
+        m, n = A.shape
+        k = max(min(m, n), 1)
+        P = np.zeros(2 * k, dtype=np.uint64)
+        Q = np.zeros(2 * k, dtype=np.uint64)
+        np_, nq, r, d = _S(0), _S(0), _S(0), _U(0)
+        if _is_torch(A):
+            st = self.L.lela_cuda_pluq_zp_u32_dev(self.h, m, n, p, _dptr(A), A.stride(0), _ptr(P),
+                                                  ctypes.byref(np_), _ptr(Q), ctypes.byref(nq),
+                                                  ctypes.byref(r), ctypes.byref(d))
+        else:
+            _check(A.dtype == np.uint32, "pluq: uint32 matrix expected")
+            st = self.L.lela_cuda_pluq_zp_u32(self.h, m, n, p, _ptr(A), A.strides[0] // 4, _ptr(P),
+                                              ctypes.byref(np_), _ptr(Q), ctypes.byref(nq),
+                                              ctypes.byref(r), ctypes.byref(d))
+        self._raise(st)
+        pairs = lambda X, c: [(int(X[2 * t]), int(X[2 * t + 1])) for t in range(c)]
+        return A, pairs(P, np_.value), pairs(Q, nq.value), r.value, d.value
 
     # ------------------------------------------------- Faugere-Lachartre
     def fl_echelonize(self, p, X, reduced=True, only_D=False, R=None):

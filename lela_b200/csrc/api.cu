@@ -1160,6 +1160,56 @@ static int echelon_entry(lela_cuda_ctx *h, size_t m, size_t n, uint32_t p, uint3
   return st;
 }
 
+static int pluq_entry(lela_cuda_ctx *h, size_t m, size_t n, uint32_t p, uint32_t *A, size_t lda,
+                      size_t *P, size_t *np, size_t *Q, size_t *nq, size_t *rank, uint32_t *det,
+                      bool dev) {
+  if (!h || !rank || !det || !np || !nq) return ST_ARG;
+  Ctx *c = &h->c;
+  DeviceScope ds(c);
+  if (m > (size_t)INT32_MAX || n > (size_t)INT32_MAX) return ctx_fail(c, ST_ARG, "dimension too large");
+  if (p < 2) return ctx_fail(c, ST_ARG, "modulus must be at least 2");
+  if (m && n && (!A || lda < n || !P || !Q))
+    return ctx_fail(c, ST_ARG, "bad matrix or permutation arrays");
+  std::vector<std::pair<int, int>> vp, vq;
+  int st = ctx_clear_status(c);
+  if (st) return st;
+  uint32_t *dA = A;
+  size_t ld = lda;
+  if (!dev && m && n) {
+    void *s = nullptr;
+    if ((st = ctx_stage(c, 0, m * n * 4, &s))) return st;
+    dA = static_cast<uint32_t *>(s);
+    ld = n;
+    if ((st = h2d_matrix(c, dA, A, m, n, lda, 4))) return st;
+  }
+  st = zp_pluq_dev(c, (int)m, (int)n, p, dA, ld, &vp, &vq, rank, det);
+  if (st == ST_PIVOT) return ctx_fail(c, ST_PIVOT, "Could not invert pivot-element in the ring");
+  if (st) return st;
+  if (!dev && m && n && (st = d2h_matrix(c, A, dA, m, n, lda, 4))) return st;
+  for (size_t t = 0; t < vp.size(); ++t) {
+    P[2 * t] = (size_t)vp[t].first;
+    P[2 * t + 1] = (size_t)vp[t].second;
+  }
+  for (size_t t = 0; t < vq.size(); ++t) {
+    Q[2 * t] = (size_t)vq[t].first;
+    Q[2 * t + 1] = (size_t)vq[t].second;
+  }
+  *np = vp.size();
+  *nq = vq.size();
+  return ctx_check_status(c, "pluq_zp_u32");
+}
+
+int lela_cuda_pluq_zp_u32(lela_cuda_ctx *h, size_t m, size_t n, uint32_t p, uint32_t *A, size_t lda,
+                          size_t *P, size_t *np, size_t *Q, size_t *nq, size_t *rank, uint32_t *det) {
+  return pluq_entry(h, m, n, p, A, lda, P, np, Q, nq, rank, det, false);
+}
+
+int lela_cuda_pluq_zp_u32_dev(lela_cuda_ctx *h, size_t m, size_t n, uint32_t p, uint32_t *A,
+                              size_t lda, size_t *P, size_t *np, size_t *Q, size_t *nq,
+                              size_t *rank, uint32_t *det) {
+  return pluq_entry(h, m, n, p, A, lda, P, np, Q, nq, rank, det, true);
+}
+
 int lela_cuda_echelon_zp_u32_dev(lela_cuda_ctx *h, size_t m, size_t n, uint32_t p, uint32_t *A,
                                  size_t lda, size_t *rank, uint32_t *det) {
   return echelon_entry(h, m, n, p, A, lda, rank, det, true, false);

@@ -153,7 +153,8 @@ enum BufSlot : int {
   BUF_FL_KR = 23,     // Faugere-Lachartre: per-row column ranges of A and C
   BUF_FL_CSR_P = 24,  // Faugere-Lachartre CSR output: row counts, row pointers, scan scratch
   BUF_FL_CSR_V = 25,  // Faugere-Lachartre CSR output: column indices and values
-  BUF_COUNT = 26,
+  BUF_PLUQ = 26,      // PLUQ: kept multipliers, assembled output, column order
+  BUF_COUNT = 27,
 };
 
 // Grow-only allocation helpers; return ST_OK or ST_NOMEM.

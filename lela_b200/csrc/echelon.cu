@@ -641,7 +641,7 @@ __global__ void __launch_bounds__(SOLVE_THREADS)
 }
 
 int zp_echelon_dev(Ctx *c, int m, int n, uint32_t p, uint32_t *D, size_t ld, size_t *rank_out,
-                   uint32_t *det_out, std::vector<int> *pivot_cols) {
+                   uint32_t *det_out, std::vector<int> *pivot_cols, EchelonKeep *keep) {
   if (p < 2) return ctx_fail(c, ST_ARG, "modulus must be at least 2");
   if (m < 0 || n < 0) return ctx_fail(c, ST_ARG, "negative dimension");
   if (m > 0 && n > 0 && ld < (size_t)n) return ctx_fail(c, ST_ARG, "leading dimension too small");
@@ -703,6 +703,10 @@ int zp_echelon_dev(Ctx *c, int m, int n, uint32_t p, uint32_t *D, size_t ld, siz
   PanelOut *hmap_dev = static_cast<PanelOut *>(md);
   uint32_t *hflag_dev = reinterpret_cast<uint32_t *>(static_cast<char *>(md) + PANEL_FLAG_OFF);
   cudaError_t e = cudaMemsetAsync(d_stamp, 0xff, (size_t)m * sizeof(int), c->stream);
+  if (e == cudaSuccess && keep) {
+    keep->swaps.clear();
+    e = cudaMemsetAsync(keep->L, 0, (size_t)m * keep->ldL * 4, c->stream);
+  }
   if (e == cudaSuccess) e = cudaMemsetAsync(d_last, 0xff, sizeof(int), c->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(d_hist, 0, (EW + 1) * sizeof(int), c->stream);
   if (e != cudaSuccess) return ctx_cuda(c, e, "echelon: scratch");
@@ -814,6 +818,12 @@ int zp_echelon_dev(Ctx *c, int m, int n, uint32_t p, uint32_t *D, size_t ld, siz
             d_L, EB, EB, d_perm, d_perm + cnt, cnt);
         ctx_launched(c);
       }
+      if (keep && rank > 0) {  // and every earlier pivot's kept multipliers
+        permute_rows_kernel<<<((int)rank + PERM_COLS - 1) / PERM_COLS, PERM_THREADS, 0,
+                              c->stream>>>(keep->L, keep->ldL, (int)rank, d_perm, d_perm + cnt,
+                                           cnt);
+        ctx_launched(c);
+      }
     }
     // L11 / L21 and the panel's final values
     const int r0 = i + t;
@@ -840,6 +850,14 @@ int zp_echelon_dev(Ctx *c, int m, int n, uint32_t p, uint32_t *D, size_t ld, siz
                                                                    d_U, d_xinv, arw, Lp, EB);
       prof_end(c, pi);
       ctx_launched(c);
+    }
+    if (keep) {
+      // this panel's multipliers (rows i..r1) into columns rank.. of L
+      e = cudaMemcpy2DAsync(keep->L + (size_t)i * keep->ldL + rank, keep->ldL * 4, Lp, EB * 4,
+                            (size_t)t * 4, (size_t)(r1 - i + 1), cudaMemcpyDeviceToDevice,
+                            c->stream);
+      if (e != cudaSuccess) return ctx_cuda(c, e, "pluq: multipliers");
+      for (int k = 0; k < t; ++k) keep->swaps.emplace_back((int)h.ti[k], (int)h.tq[k]);
     }
     // the rest of the block's columns (delayed), or of all columns
     const int rest = (delayed ? b1 : n) - (c0 + w);
@@ -869,6 +887,90 @@ int zp_echelon_dev(Ctx *c, int m, int n, uint32_t p, uint32_t *D, size_t ld, siz
   *rank_out = rank;
   *det_out = (uint32_t)det;
   return ST_OK;
+}
+
+// ---------------------------------------------------------------- PLUQ
+//
+// Elimination::pluq (lela/algorithms/elimination.tcc:266-370) with
+// DensePivotStrategy: at step i the first column, in the current column
+// order, with a nonzero at or below row i, and its first such row, are
+// swapped into place (transpositions (i, row) and (i, column)); det is
+// multiplied by the pivot x; every row j below gets row_j - (a / x) row_i
+// right of the pivot and keeps a / x below the diagonal.  A column passed
+// over at step i is zero at and below row i and stays so, so the pivots are
+// those of the non-reduced echelon form: the same rows, transpositions and
+// values (the eliminations are the same field operations).  The echelon
+// pipeline therefore runs with its multipliers kept (EchelonKeep); Q
+// follows on the host from the pivot columns, and one gather writes L
+// below the diagonal and U, its columns in Q's order, on and above it.
+
+__global__ void pluq_assemble_kernel(const uint32_t *__restrict__ U, size_t ldu,
+                                     const uint32_t *__restrict__ L, size_t ldl,
+                                     const int *__restrict__ qcol, int m, int n, int r,
+                                     uint32_t *__restrict__ out) {
+  const size_t total = (size_t)m * n;
+  for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (size_t)gridDim.x * blockDim.x) {
+    const int q = (int)(idx / n), j = (int)(idx % n);
+    out[idx] = j < min(q, r) ? L[(size_t)q * ldl + j] : U[(size_t)q * ldu + qcol[j]];
+  }
+}
+
+int zp_pluq_dev(Ctx *c, int m, int n, uint32_t p, uint32_t *D, size_t ld,
+                std::vector<std::pair<int, int>> *P, std::vector<std::pair<int, int>> *Q,
+                size_t *rank, uint32_t *det) {
+  P->clear();
+  Q->clear();
+  if (p < 2) return ctx_fail(c, ST_ARG, "modulus must be at least 2");
+  if (m < 0 || n < 0) return ctx_fail(c, ST_ARG, "negative dimension");
+  if (m == 0 || n == 0) {
+    *rank = 0;
+    *det = 1 % p;
+    return ST_OK;
+  }
+  const int rmax = std::min(m, n);
+  const size_t l_bytes = ((size_t)m * rmax * 4 + 255) & ~(size_t)255;
+  const size_t o_bytes = ((size_t)m * n * 4 + 255) & ~(size_t)255;
+  void *buf = nullptr;
+  int st = ctx_buffer(c, BUF_PLUQ, l_bytes + o_bytes + (size_t)n * sizeof(int) + 256, &buf);
+  if (st) return st;
+  uint8_t *b8 = static_cast<uint8_t *>(buf);
+  EchelonKeep keep;
+  keep.L = reinterpret_cast<uint32_t *>(b8);
+  keep.ldL = (size_t)rmax;
+  uint32_t *out = reinterpret_cast<uint32_t *>(b8 + l_bytes);
+  int *d_qcol = reinterpret_cast<int *>(b8 + l_bytes + o_bytes);
+  std::vector<int> piv;
+  if ((st = zp_echelon_dev(c, m, n, p, D, ld, rank, det, &piv, &keep))) return st;
+  const int r = (int)*rank;
+  for (const auto &sw : keep.swaps)
+    if (sw.first != sw.second) P->push_back(sw);
+  std::vector<int> qcol(n), where(n);  // position -> column, column -> position
+  for (int j = 0; j < n; ++j) qcol[j] = where[j] = j;
+  for (int i = 0; i < r; ++i) {
+    const int pos = where[piv[i]];
+    if (pos != i) {
+      std::swap(qcol[i], qcol[pos]);
+      where[qcol[i]] = i;
+      where[qcol[pos]] = pos;
+      Q->emplace_back(i, pos);
+    }
+  }
+  std::reverse(P->begin(), P->end());  // the reference returns them reversed (:362-363)
+  std::reverse(Q->begin(), Q->end());
+  cudaError_t e = cudaMemcpyAsync(d_qcol, qcol.data(), (size_t)n * sizeof(int),
+                                  cudaMemcpyHostToDevice, c->stream);
+  if (e != cudaSuccess) return ctx_cuda(c, e, "pluq: column order");
+  const size_t total = (size_t)m * n;
+  const int grid = (int)std::min<size_t>((total + 255) / 256, (size_t)c->num_sms * 16);
+  pluq_assemble_kernel<<<grid, 256, 0, c->stream>>>(D, ld, keep.L, keep.ldL, d_qcol, m, n, r, out);
+  ctx_launched(c);
+  e = cudaMemcpy2DAsync(D, ld * 4, out, (size_t)n * 4, (size_t)n * 4, (size_t)m,
+                        cudaMemcpyDeviceToDevice, c->stream);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  // the host vector qcol must outlive the copy above
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  return e == cudaSuccess ? ST_OK : ctx_cuda(c, e, "pluq: assembly");
 }
 
 }  // namespace lela

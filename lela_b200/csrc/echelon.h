@@ -2,6 +2,7 @@
 #pragma once
 #include <cstddef>
 #include <cstdint>
+#include <utility>
 #include <vector>
 
 #include "context.h"
@@ -12,8 +13,27 @@ namespace lela {
 // pivot rule (see echelon.cu): rank, det = product of the pivots, and the
 // pivot columns in order (optional).  Synchronises the stream per block.
 // Returns ST_PIVOT when a pivot is not invertible in Modular<uint32>.
+// PLUQ bookkeeping (optional): every panel's multipliers kept in L (m x
+// ldL, zeroed here; column k holds pivot k's multipliers, rows moved with
+// the row transpositions), and the row transpositions (current row, pivot
+// row) in order, those of equal rows included.
+struct EchelonKeep {
+  uint32_t *L = nullptr;
+  size_t ldL = 0;
+  std::vector<std::pair<int, int>> swaps;
+};
+
 int zp_echelon_dev(Ctx *c, int m, int n, uint32_t p, uint32_t *D, size_t ld, size_t *rank,
-                   uint32_t *det, std::vector<int> *pivot_cols);
+                   uint32_t *det, std::vector<int> *pivot_cols, EchelonKeep *keep = nullptr);
+
+// PLUQ decomposition of D in place with LELA's Elimination::pluq semantics
+// (see echelon.cu): U above and on the diagonal in the permuted column
+// order, the multipliers of L below it; P and Q as transposition pairs in
+// the reference's (reversed) order.  ST_PIVOT when a pivot is not
+// invertible in Modular<uint32>.
+int zp_pluq_dev(Ctx *c, int m, int n, uint32_t p, uint32_t *D, size_t ld,
+                std::vector<std::pair<int, int>> *P, std::vector<std::pair<int, int>> *Q,
+                size_t *rank, uint32_t *det);
 
 // Reduced row-echelon form of D in place as LELA's GaussJordan::
 // echelonize_reduced leaves it (pivots keep their values; zero above and
