@@ -65,6 +65,8 @@ def parse():
                     help="tile variant for --gemm-only: 0 auto, 1 wide, 2 two accumulator buffers")
     ap.add_argument("--fl-m", type=int, default=20000)
     ap.add_argument("--fl-count", type=int, default=3)
+    ap.add_argument("--fl-big", type=int, default=120000,
+                    help="rows of the one large FL matrix (CSR output; 0 = skip)")
     ap.add_argument("--no-fl-check", action="store_true",
                     help="skip the reduced-echelon certificate of the last timed FL matrix")
     ap.add_argument("--no-dense", action="store_true",
@@ -473,6 +475,62 @@ def run_dense(args, cm, stream, torch, dev, int8_peak):
     return out
 
 
+def run_fl_big(args, torch, dev, zp_peak=None):
+    """One F4 matrix at the top of the FL family's range (m = args.fl_big,
+    n = 1.2 m, density 2.5 %, p = 65521), generated on the device
+    (gen.f4_matrix_torch), echelonized (reduced) with the result as CSR rows
+    -- no dense m x n array, which would be 69 GB at m = 120000.  A warm-up
+    run (device buffers grow to size), then one timed run (CUDA events on
+    the handle's stream), then the reduced-echelon certificate of its
+    result.  Runs on its own handle, closed afterwards."""
+    from lela_b200 import CudaModule, certify, gen
+    m = args.fl_big
+    res = {"workload": "FL reduced echelon form, CSR output, F4-shaped, p=65521, m=%d, n=%d, density %.3f"
+                       % (m, int(1.2 * m), FL_DENSITY), "unit": "ms/matrix"}
+    cm = CudaModule(torch.cuda.current_device())
+    try:
+        stream = torch.cuda.Stream(device=dev)
+        cm.set_stream(stream)
+        t0 = time.perf_counter()
+        X = gen.f4_matrix_torch(7000, m, P, dev, density=FL_DENSITY)
+        torch.cuda.synchronize()
+        res["generation_s"] = round(time.perf_counter() - t0, 1)
+        res["nnz"] = X.nnz
+        torch.cuda.empty_cache()
+        R, rk, det = cm.fl_echelonize_csr(P, X, True, False)
+        cap = int(R.colidx.numel())
+        del R
+        torch.cuda.empty_cache()
+        cm.profile_reset()
+        cm.profile(True)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        R, rk, det = cm.fl_echelonize_csr(P, X, True, False, cap=cap)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        phases = {k.replace("fl_phase_", ""): round(cm.profile_read(k)[0], 1)
+                  for k in ("fl_phase_trsm", "fl_phase_schur", "fl_phase_echelon", "fl_phase_reduce")}
+        cm.profile(False)
+        res.update({"ms": round(ms, 1), "rank": rk, "R_nnz": int(R.colidx.numel()),
+                    "phase_ms_profiled": phases,
+                    "timing": "CUDA events around one call (after a warm-up call); phases from the same "
+                              "call's per-launch events"})
+        err = certify.rref_certificate_csr(torch, P, X, R, rk)
+        res["checked"] = err is None
+        res["check"] = "reduced-echelon certificate (CSR form; 2 random projections)" + \
+                       ("" if err is None else ": FAILED " + err)
+        del R, X
+    except Exception as ex:  # reported in the line, the other workloads still run
+        res["error"] = "%s: %s" % (type(ex).__name__, ex)
+    finally:
+        cm.close()
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+    return res
+
+
 def run_gf2(args, cm, stream, torch, dev, int8_peak=None):
     """GF(2) workloads: packed gemm 16384^3 with Bernoulli(1/2) bits on both
     kernels (int8-expanded tensor cores, bit-packed four-Russians), and the
@@ -764,6 +822,8 @@ def run_ours(args):
     from lela_b200 import gen, CudaModule
 
     n = args.n
+    # the largest FL matrix first, before the other workloads hold device memory
+    fl_big = run_fl_big(args, torch, dev) if (args.fl_big and not args.no_fl) else None
     cm = CudaModule(local)
     stream = torch.cuda.Stream(device=dev)
     cm.set_stream(stream)
@@ -874,6 +934,8 @@ def run_ours(args):
         out["dense"] = run_dense(args, cm, stream, torch, dev, peak)
     if not args.no_fl:
         out["fl"] = run_fl(args, cm, stream, torch, dev, rank, zp_peak=peak / 4)
+        if fl_big is not None:
+            out["fl"]["large"] = fl_big
     if not args.no_gf2:
         out["gf2"] = run_gf2(args, cm, stream, torch, dev, peak)
     if not args.no_batch:

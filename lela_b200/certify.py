@@ -65,3 +65,67 @@ def rref_certificate(torch, p, X, R, rank, trials=2, seed=0):
         if bool((torch.remainder(red, p) != 0).any()):
             return "w^T X is not in R's row space (trial %d)" % t
     return None
+
+
+def rref_certificate_csr(torch, p, X, R, rank, trials=2, seed=0, chunk=1 << 26):
+    """rref_certificate for a result given as CSR rows on the device (R with
+    m, n and tensors rowptr (int64), colidx, vals (int32 storage), as
+    CudaModule.fl_echelonize_csr returns it) and X as device CSR tensors of
+    the same form: (1) rows 0..rank-1 are nonempty, their first entries lie
+    in strictly increasing columns and are 1, each such pivot column holds
+    no other entry, rows from rank on are empty; (2) for random w, w^T X
+    minus its combination of R's rows by the pivot-column entries is zero
+    (float64 sums on the device, exact below 2^53: p < 2^16 and fewer than
+    2^21 rows).  Entries are processed about `chunk` at a time, so results
+    with billions of entries fit beside the matrices.  Returns an error
+    string or None."""
+    dev = R.rowptr.device
+    rp = R.rowptr.to(torch.int64)
+    lens = rp[1:] - rp[:-1]
+    if int((lens > 0).sum()) != rank or (rank and not bool((lens[:rank] > 0).all())):
+        return "nonempty rows do not match the rank"
+    if rank == 0:
+        return None
+    heads = R.colidx[rp[:rank]].to(torch.int64)
+    if rank > 1 and not bool((heads[1:] > heads[:-1]).all()):
+        return "leading columns not strictly increasing"
+    if not bool((R.vals[rp[:rank]] == 1).all()):
+        return "a leading entry is not 1"
+    is_pc = torch.zeros(R.n, dtype=torch.bool, device=dev)
+    is_pc[heads] = True
+
+    def row_chunks(rowptr, m):
+        """(r0, r1, e0, e1): consecutive rows holding about `chunk` entries."""
+        r0 = 0
+        while r0 < m:
+            e0 = int(rowptr[r0])
+            r1 = int(torch.searchsorted(rowptr, torch.tensor(e0 + chunk, device=dev), right=True)) - 1
+            r1 = min(m, max(r1, r0 + 1))
+            yield r0, r1, e0, int(rowptr[r1])
+            r0 = r1
+
+    pc_entries = 0
+    for r0, r1, e0, e1 in row_chunks(rp, R.m):
+        pc_entries += int(is_pc[R.colidx[e0:e1].to(torch.int64)].sum())
+    if pc_entries != rank:
+        return "a pivot column has another nonzero"
+    xrp = X.rowptr.to(torch.int64)
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    for t in range(trials):
+        w = torch.randint(0, p, (X.m,), generator=g, device=dev, dtype=torch.int64)
+        v = torch.zeros(X.n, dtype=torch.float64, device=dev)
+        for r0, r1, e0, e1 in row_chunks(xrp, X.m):
+            rows = torch.repeat_interleave(torch.arange(r0, r1, device=dev), xrp[r0 + 1:r1 + 1] - xrp[r0:r1])
+            prod = (w[rows] * X.vals[e0:e1].to(torch.int64)) % p
+            v.index_add_(0, X.colidx[e0:e1].to(torch.int64), prod.to(torch.float64))
+        v = torch.remainder(v, p)
+        coef = v[heads]                         # per pivot row
+        acc = torch.zeros(R.n, dtype=torch.float64, device=dev)
+        for r0, r1, e0, e1 in row_chunks(rp, min(R.m, rank)):
+            rows = torch.repeat_interleave(torch.arange(r0, r1, device=dev), rp[r0 + 1:r1 + 1] - rp[r0:r1])
+            acc.index_add_(0, R.colidx[e0:e1].to(torch.int64),
+                           coef[rows] * R.vals[e0:e1].to(torch.float64))
+        if bool((torch.remainder(v - torch.remainder(acc, p), p) != 0).any()):
+            return "w^T X is not in R's row space (trial %d)" % t
+    return None

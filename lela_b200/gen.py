@@ -314,3 +314,103 @@ def f4_matrix_fast(seed, m, p, n=None, density=None, pivot_frac=0.75, dep_frac=0
         ci2[int(rp2[r]):int(rp2[r + 1])] = c_
         v2[int(rp2[r]):int(rp2[r + 1])] = v_
     return CSR(mm, n, rp2, ci2, v2)
+
+
+def f4_matrix_torch(seed, m, p, device, n=None, density=0.025, pivot_frac=0.75, dep_frac=0.05):
+    """f4_matrix_fast's family generated on a torch device (for matrices
+    too large for host-side generation: m = 120000 has about 4.3e8
+    nonzeros).  Same structure -- staircase of pivot rows with leading 1,
+    non-pivot rows copying a pivot row's leading column right after it,
+    clustered nonzeros right of the leading column, values uniform in
+    [1, p), dep_frac of the non-pivot rows planted as combinations of two
+    pivot rows -- from torch's generator, so the matrix differs from the
+    numpy generators' for the same seed.  Returns an object with m, n and
+    CSR tensors rowptr (int64), colidx, vals (int32 storage) on the
+    device."""
+    import types
+    import torch
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    n = int(1.2 * m) if n is None else int(n)
+    npiv = max(0, min(int(round(pivot_frac * m)), n, m))
+    nnp = m - npiv
+    lead = torch.sort(torch.randperm(n, generator=g, device=device)[:npiv]).values
+    owner = torch.sort(torch.randint(0, npiv, (nnp,), generator=g, device=device)).values
+    counts = torch.bincount(owner, minlength=npiv)
+    heads = torch.repeat_interleave(lead, counts + 1)
+    starts = torch.cumsum(counts + 1, 0) - (counts + 1)
+    is_piv = torch.zeros(len(heads), dtype=torch.bool, device=device)
+    is_piv[starts] = True
+    mm = len(heads)
+    k = max(1, int(round(density * n)))
+    room = (n - heads - 1).to(torch.float32)
+    mean_gap = torch.clamp(room / (4.0 * k), min=1.0)
+    rowptr = torch.zeros(mm + 1, dtype=torch.int64, device=device)
+    cols_all, vals_all, lens = [], [], torch.empty(mm, dtype=torch.int64, device=device)
+    step = max(1, (1 << 26) // k)  # rows per chunk: about 6.7e7 draws at a time
+    for r0 in range(0, mm, step):
+        r1 = min(mm, r0 + step)
+        e = torch.empty((r1 - r0, k), dtype=torch.float32, device=device).exponential_(generator=g)
+        gaps = 1 + torch.floor(e * (mean_gap[r0:r1, None] - 1.0 + 1e-6)).to(torch.int64)
+        off = torch.cumsum(gaps, 1) - 1
+        del e, gaps
+        valid = off < (n - heads[r0:r1] - 1)[:, None]
+        c = heads[r0:r1, None] + 1 + off
+        v = torch.randint(1, p, (r1 - r0, k), generator=g, device=device, dtype=torch.int64)
+        lv = torch.where(is_piv[r0:r1], torch.ones_like(heads[r0:r1]),
+                         torch.randint(1, p, (r1 - r0,), generator=g, device=device))
+        # each row: its head, then its valid offsets
+        c = torch.cat([heads[r0:r1, None], torch.where(valid, c, -1)], 1)
+        v = torch.cat([lv[:, None], v], 1)
+        keep = c >= 0
+        lens[r0:r1] = keep.sum(1)
+        cols_all.append(c[keep].to(torch.int32))
+        vals_all.append(v[keep].to(torch.int32))
+        del c, v, keep, valid, off
+    rowptr[1:] = torch.cumsum(lens, 0)
+    colidx = torch.cat(cols_all)
+    vals = torch.cat(vals_all)
+    del cols_all, vals_all
+    # planted dependencies: c1 * (pivot row of the same head) + c2 * (a later pivot row)
+    np_rows = torch.nonzero(~is_piv).flatten()
+    ndep = int(round(dep_frac * len(np_rows)))
+    if ndep and npiv > 1:
+        piv_rows = torch.nonzero(is_piv).flatten()
+        piv_of = torch.searchsorted(lead, heads)
+        pick = np_rows[torch.randperm(len(np_rows), generator=g, device=device)[:ndep]]
+        repl = {}
+        for r in pick.tolist():
+            i1 = int(piv_of[r])
+            if i1 + 1 >= npiv:
+                continue
+            i2 = int(torch.randint(i1 + 1, npiv, (1,), generator=g, device=device))
+            c1, c2 = (int(x) for x in torch.randint(1, p, (2,), generator=g, device=device))
+            r1_, r2_ = int(piv_rows[i1]), int(piv_rows[i2])
+            a0, a1 = int(rowptr[r1_]), int(rowptr[r1_ + 1])
+            b0, b1 = int(rowptr[r2_]), int(rowptr[r2_ + 1])
+            cc = torch.cat([colidx[a0:a1], colidx[b0:b1]]).to(torch.int64)
+            vv = torch.cat([vals[a0:a1].to(torch.int64) * c1 % p, vals[b0:b1].to(torch.int64) * c2 % p])
+            u, inv = torch.unique(cc, return_inverse=True)
+            acc = torch.zeros(len(u), dtype=torch.int64, device=device).index_add_(0, inv, vv) % p
+            nz = acc != 0
+            repl[r] = (u[nz].to(torch.int32), acc[nz].to(torch.int32))
+        if repl:
+            new_lens = lens.clone()
+            for r, (cc, _) in repl.items():
+                new_lens[r] = len(cc)
+            rp2 = torch.zeros(mm + 1, dtype=torch.int64, device=device)
+            rp2[1:] = torch.cumsum(new_lens, 0)
+            keep_row = torch.ones(mm, dtype=torch.bool, device=device)
+            keep_row[torch.tensor(list(repl), device=device)] = False
+            src_keep = torch.repeat_interleave(keep_row, lens)
+            dst_keep = torch.repeat_interleave(keep_row, new_lens)
+            ci2 = torch.empty(int(rp2[-1]), dtype=torch.int32, device=device)
+            v2 = torch.empty_like(ci2)
+            ci2[dst_keep] = colidx[src_keep]
+            v2[dst_keep] = vals[src_keep]
+            for r, (cc, vv) in repl.items():
+                ci2[int(rp2[r]):int(rp2[r + 1])] = cc
+                v2[int(rp2[r]):int(rp2[r + 1])] = vv
+            rowptr, colidx, vals = rp2, ci2, v2
+    return types.SimpleNamespace(m=mm, n=n, rowptr=rowptr, colidx=colidx, vals=vals,
+                                 nnz=int(rowptr[-1]))

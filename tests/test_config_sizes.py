@@ -152,3 +152,26 @@ def test_fl_m20000_certificate(cuda):
     torch.cuda.synchronize()
     assert drank == rank
     assert torch.equal(D, R)
+
+
+@pytest.mark.gpu
+def test_fl_csr_output_m20000(cuda):
+    """The CSR output path at the benchmark's size, on a matrix generated on
+    the device (gen.f4_matrix_torch): the CSR certificate, and equality with
+    the dense output of the same matrix (expanded on the device)."""
+    import torch
+    from lela_b200 import certify
+    p, m = 65521, 20000
+    X = gen.f4_matrix_torch(77, m, p, "cuda", density=0.025)
+    Rc, rank, det = cuda.fl_echelonize_csr(p, X, True, False)
+    torch.cuda.synchronize()
+    err = certify.rref_certificate_csr(torch, p, X, Rc, rank)
+    assert err is None, err
+    Rd, rank2, det2 = cuda.fl_echelonize(p, X, True, False)
+    torch.cuda.synchronize()
+    assert (rank2, det2) == (rank, det)
+    rp = Rc.rowptr.to(torch.int64)
+    rows = torch.repeat_interleave(torch.arange(Rc.m, device="cuda"), rp[1:] - rp[:-1])
+    E = torch.zeros((Rd.shape[0], X.n), dtype=torch.int32, device="cuda")
+    E[rows, Rc.colidx.to(torch.int64)] = Rc.vals
+    assert torch.equal(E, Rd)
