@@ -247,24 +247,54 @@ def _hbm_peak():
         return 6650.0, "fallback 6.65 TB/s (MEASURED_PEAKS.json absent)"
 
 
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+class CpuGemmSampler:
+    """LELA's own CPU gemm (oracle/_ref, else the C restatement) on row
+    slices of the n^3 workload: rows 0..r-1 of A and C against all of B,
+    row-sliced over `threads` host threads (row slices are independent, so
+    the result equals a single call's).  Shared by the cpu_baseline leg and
+    the reference arm, so both sample the same way."""
+
+    def __init__(self, n, threads):
+        import oracle
+        from lela_b200 import gen
+        self.oracle, self.gen, self.n, self.threads = oracle, gen, n, threads
+        self.B = gen.dense_zp(102, n, n, P)
+        self.kind = "reference" if oracle.have_ref() else "port"
+
+    def run(self, rows):
+        A = self.gen.dense_zp(101, rows, self.n, P)
+        C = self.gen.dense_zp(103, rows, self.n, P)
+        t0 = time.perf_counter()
+        if self.kind == "reference":
+            self.oracle.ref_gemm_zp(P, A, self.B, C, 1, 1, threads=self.threads)
+        else:
+            self.oracle.gemm_zp(P, A, self.B, C, 1, 1, threads=self.threads)
+        return time.perf_counter() - t0
+
+    def rows_for(self, seconds):
+        """Rows (a multiple of the thread count) that take about `seconds`."""
+        t1 = self.run(self.threads)  # calibration: one row per thread
+        return self.threads * max(1, int(seconds / max(t1, 1e-3)))
+
+
 def cpu_baseline(n, threads):
-    """LELA's own CPU gemm on a bounded sample: rows 0..r-1 of the n^3
-    workload, ZpModule gemm row-sliced over all host threads."""
-    import oracle
-    from lela_b200 import gen
-    rows = max(64, 8 * threads)
-    A = gen.dense_zp(101, rows, n, P)
-    B = gen.dense_zp(102, n, n, P)
-    C = gen.dense_zp(103, rows, n, P)
-    if oracle.have_ref():
-        fn, kind = (lambda: oracle.ref_gemm_zp(P, A, B, C, 1, 1, threads=threads)), "reference"
-    else:
-        fn, kind = (lambda: oracle.gemm_zp(P, A, B, C, 1, 1, threads=threads)), "port"
-    t0 = time.perf_counter()
-    fn()
-    t = time.perf_counter() - t0
+    """LELA's own CPU gemm on a bounded sample of the n^3 workload (about
+    12 s of work), all host threads."""
+    s = CpuGemmSampler(n, threads)
+    rows = s.rows_for(12.0)
+    t = s.run(rows)
     return {"value": round(2 * rows * n * n / t / 1e9, 4), "unit": "Gop/s", "cores": threads,
-            "kind": kind,
+            "kind": s.kind, "cpu": cpu_model(),
             "sample": "rows 0-%d of the %d^3 gemm (%dx%dx%d), LELA ZpModule gemm row-sliced over %d threads, %.1f s"
                       % (rows - 1, n, rows, n, n, threads, t)}
 
@@ -741,22 +771,30 @@ def run_batch(args, cm, stream, torch, dev):
 
 def fl_cpu_baseline(m_target):
     """LELA's own FaugereLachartre (oracle/_ref) on the same matrix family at
-    m = 1000 and 2000, single-threaded (LELA has no threading), fitted as
-    c*m^3 and extrapolated; labelled as such."""
+    m = 1000, 2000 and 3000, single-threaded (LELA has no threading), fitted
+    as c*m^3 by least squares over the three points and extrapolated to the
+    bench's size; labelled as such.  (LELA needs about 40 s at m = 4000 and
+    9 min at m = 8000 on one core of this build's CPU, which is why the
+    bench stops at 3000.)"""
     import oracle
     from lela_b200 import gen
     if not oracle.have_ref():
         return {"unavailable": "oracle/_ref not built"}
     pts = []
-    for m in (1000, 2000):
+    for m in (1000, 2000, 3000):
         X = gen.f4_matrix(500 + m, m, P, density=FL_DENSITY)
         t0 = time.perf_counter()
         oracle.ref_fl_echelonize_zp(P, X.m, X.n, X.rowptr, X.colidx, X.vals, 1, 0)
         pts.append((m, time.perf_counter() - t0))
-    c = pts[-1][1] / pts[-1][0] ** 3
-    return {"kind": "reference", "cores": 1, "measured_s": {str(m): round(t, 3) for m, t in pts},
+    x = np.array([float(m) ** 3 for m, _ in pts])
+    y = np.array([t for _, t in pts])
+    c = float((x * y).sum() / (x * x).sum())
+    rel = [round(float(t / (c * xx)), 3) for t, xx in zip(y, x)]
+    return {"kind": "reference", "cores": 1, "cpu": cpu_model(),
+            "measured_s": {str(m): round(t, 3) for m, t in pts},
+            "fit": "t = c m^3, least squares over the measured points, c = %.3e s; measured / fit = %s" % (c, rel),
             "extrapolated_ms_per_matrix": round(c * m_target ** 3 * 1e3, 1),
-            "extrapolation": "c*m^3 with c from the m=2000 run, at m=%d" % m_target}
+            "extrapolation": "fitted c*m^3 at m=%d (extrapolated, not measured)" % m_target}
 
 
 # ------------------------------------------------------------ reference
@@ -767,26 +805,12 @@ def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
         return
-    import oracle
-    from lela_b200 import gen
     threads = os.cpu_count() or 1
     n = args.n
-    B = gen.dense_zp(102, n, n, P)
-    kind = "reference" if oracle.have_ref() else "port"
-
-    def run(rows):
-        A = gen.dense_zp(101, rows, n, P)
-        C = gen.dense_zp(103, rows, n, P)
-        t0 = time.perf_counter()
-        if kind == "reference":
-            oracle.ref_gemm_zp(P, A, B, C, 1, 1, threads=threads)
-        else:
-            oracle.gemm_zp(P, A, B, C, 1, 1, threads=threads)
-        return time.perf_counter() - t0
-
-    t1 = run(threads)  # calibration: one row per thread
+    sampler = CpuGemmSampler(n, threads)
+    kind, run = sampler.kind, sampler.run
     budget = 120.0 / max(1, args.steps + args.warmup)
-    rows = threads * max(1, int(budget / max(t1, 1e-3)))
+    rows = sampler.rows_for(budget)
     for _ in range(args.warmup):
         run(rows)
     tot = 0.0
@@ -801,6 +825,7 @@ def run_reference(args):
             "config": {"workload": "gemm Z/65521 %d^3 C<-A*B+C" % n, "p": P, "m": n, "n": n, "k": n,
                        "parallelism": "host threads (row slices)"},
             "cpu_baseline": {"value": round(v, 4), "unit": "Gop/s", "cores": threads, "kind": kind,
+                             "cpu": cpu_model(),
                              "sample": "rows 0-%d of the %d^3 gemm per step (LELA ZpModule gemm, row-sliced)"
                                        % (rows - 1, n)},
             "e2e": {"value": round(v, 4), "unit": "Gop/s", "h2d_bytes_per_step": 0,
