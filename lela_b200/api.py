@@ -215,13 +215,13 @@ class CudaModule:
     def set_gemm_kernel(self, kernel):
         self._raise(self.L.lela_cuda_set_gemm_kernel(self.h, int(kernel)))
 
-    @property
     def set_gemm_tile(self, tile):
         """Tensor-core tile variant: 0 = automatic, 1 = wide tiles (one
         accumulator buffer), 2 = narrower tiles with two accumulator buffers
         (one and two limbs).  Results do not depend on it."""
         self._raise(self.L.lela_cuda_set_gemm_tile(self.h, int(tile)))
 
+    @property
     def num_sms(self):
         return self.L.lela_cuda_num_sms(self.h)
 

@@ -94,8 +94,10 @@ def _banded_upper(seed, n, p, unit, band, holes):
     U = gen.upper_zp(seed, n, p, unit=unit)
     i, j = np.indices((n, n))
     U[(j - i) > band] = 0
-    for r0, c0, s in holes:
-        U[r0:r0 + s, c0:c0 + s] = np.where(np.eye(s, dtype=bool) & (r0 == c0), U[r0:r0 + s, c0:c0 + s], 0)
+    for r0, c0, s in holes:  # the diagonal stays (the system stays regular)
+        hole = np.zeros((n, n), dtype=bool)
+        hole[r0:r0 + s, c0:c0 + s] = True
+        U[hole & (i != j)] = 0
     return U.astype(np.uint32)
 
 
