@@ -82,7 +82,7 @@ void *lela_cuda_get_stream (lela_cuda_ctx *ctx);
 int lela_cuda_synchronize (lela_cuda_ctx *ctx);
 int lela_cuda_set_gemm_kernel (lela_cuda_ctx *ctx, int kernel);
 /* Tile variant of the tensor-core Z/p gemm: 0 = automatic (variant 1 for
- * K <= 1024, else variant 0), 1 = variant 0 (wide tiles: 256 / 128 / 32
+ * one and two limbs, variant 0 for four), 1 = variant 0 (wide tiles: 256 / 128 / 32
  * columns for 1 / 2 / 4 limbs), 2 = variant 1 (128 / 64 columns for 1 / 2
  * limbs with two TMEM accumulator buffers, so the epilogue of one tile
  * overlaps the products of the next; four limbs always use variant 0).

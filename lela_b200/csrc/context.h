@@ -29,11 +29,10 @@ enum GemmKernel : int {
 // (narrower tiles, two accumulator buffers, so that a tile's epilogue
 // overlaps the next tile's products); four limbs have variant 0 only.
 enum GemmTile : int {
-  GEMM_TILE_AUTO = 0,    // variant 1 up to GEMM_TILE_DOUBLE_MAX_K, else variant 0
+  GEMM_TILE_AUTO = 0,    // variant 1 for one and two limbs, else variant 0
   GEMM_TILE_WIDE = 1,    // variant 0
   GEMM_TILE_DOUBLE = 2,  // variant 1
 };
-constexpr int GEMM_TILE_DOUBLE_MAX_K = 1024;
 
 // GF(2) gemm kernels.
 enum Gf2Kernel : int {

@@ -63,9 +63,10 @@ namespace lela {
 // (each L * NMMA columns; at most 512 in all).  With ACC = 2 the epilogue
 // of one tile overlaps the MMAs of the next; with ACC = 1 the MMAs wait for
 // the epilogue to drain TMEM, but each MMA is wider (more operations per
-// byte of shared memory read).  Variant 0 suits large K, variant 1 the short
-// K of the triangular-solve and elimination updates; the autotuner and the
-// caller can force either.  Four limbs have variant 0 only: with two
+// byte of shared memory read).  Variant 1 is the default for one and two
+// limbs (as fast as variant 0 at K = 8192 and faster at the short K of the
+// triangular-solve and elimination updates); the autotuner and the caller
+// can force either.  Four limbs have variant 0 only: with two
 // accumulators a tile would be 16 columns wide, 8 per epilogue thread.
 template <int L, int T>
 struct TcCfg;
@@ -853,10 +854,13 @@ size_t zp_gemm_workspace_bytes(uint32_t p, int M, int N, int K) {
 }
 
 int zp_gemm_tile_pick(const Ctx *c, int K, uint32_t p) {
+  (void)K;
   if (zp_limbs_for(p) == 4) return 0;  // one variant for four limbs
   if (c->gemm_tile == GEMM_TILE_WIDE) return 0;
-  if (c->gemm_tile == GEMM_TILE_DOUBLE) return 1;
-  return K <= GEMM_TILE_DOUBLE_MAX_K ? 1 : 0;
+  // variant 1 by default: measured on the B200 (kernel ms, p = 65521),
+  // 1.750 against 1.735 (the previous one-buffer kernel) and 2.068 (variant
+  // 0) at 8192^3, and 0.116 against 0.168 (variant 0) at 4096 x 4096 x 256
+  return 1;
 }
 
 int zp_gemm_pick(const Ctx *c, int M, int N, int K, uint32_t p) {

@@ -33,7 +33,7 @@ int zp_gemm_dev(Ctx *c, int kernel, int M, int N, int K, uint32_t p, uint32_t al
 // kernel, else the small-K crossover rule).
 int zp_gemm_pick(const Ctx *c, int M, int N, int K, uint32_t p);
 // The tensor-core tile variant (0 or 1) for this K and modulus: the
-// handle's forced variant, else variant 1 up to GEMM_TILE_DOUBLE_MAX_K.
+// handle's forced variant, else variant 1 for one and two limbs.
 int zp_gemm_tile_pick(const Ctx *c, int K, uint32_t p);
 
 // Whether the host-pointer gemm of this shape is done in row blocks with
