@@ -144,14 +144,18 @@ __device__ __forceinline__ void mbar_drain(uint64_t *bar, uint32_t parity, uint3
 // when K is small).
 enum EpiMode : int { EPI_ADD = 0, EPI_SUB = 1, EPI_SET = 2, EPI_AXPBY = 3 };
 
-__device__ __forceinline__ uint32_t epi_combine(int mode, uint32_t v, uint32_t c,
-                                                const Modulus &mod, uint32_t alpha,
-                                                uint32_t beta) {
+// The mode is a template parameter: the epilogue's tile loop is
+// instantiated once per mode and the launch runs one of them, so the hot
+// code holds no per-element branches (the epilogue shares each
+// sub-partition's instruction cache with the TMA and MMA warps).
+template <int MODE>
+__device__ __forceinline__ uint32_t epi_combine(uint32_t v, uint32_t c, const Modulus &mod,
+                                                uint32_t alpha, uint32_t beta) {
   const uint32_t p = (uint32_t)mod.p;
-  if (mode == EPI_SET) return alpha == 1u ? v : mod_mul(alpha, v, mod);
-  if (mode == EPI_AXPBY) return mod_axpby(alpha, v, beta, c, mod);
+  if constexpr (MODE == EPI_SET) return alpha == 1u ? v : mod_mul(alpha, v, mod);
+  if constexpr (MODE == EPI_AXPBY) return mod_axpby(alpha, v, beta, c, mod);
   if (c >= p) c = mod_reduce((uint64_t)c, mod);  // only for a caller's non-canonical C
-  if (mode == EPI_ADD) {
+  if constexpr (MODE == EPI_ADD) {
     const uint32_t t = p - v;  // v + c mod p without overflow
     return c >= t ? c - t : c + v;
   }
@@ -365,6 +369,60 @@ __device__ __forceinline__ void tile_kblocks(const int2 *__restrict__ kr, int kb
   kb1 = (hi + BK - 1) / BK;
 }
 
+// Epilogue of the Z/p product for one thread (TMEM lane `row` of quadrant
+// q, columns cbeg.. of each tile) over this CTA's tiles.  This thread's row
+// segment of a tile: W = BN / 2 columns from gn0, in blocks of EPB columns.
+// C's block 0 is loaded before the accumulator is ready (its latency hides
+// behind the tile's MMAs), block b + 1 while block b is combined; TMEM is
+// released after its last read, before the last block's stores.
+template <int L, int T, int MODE>
+__device__ __noinline__ void epilogue_tiles(uint32_t tmem, uint64_t *tfull, uint64_t *tempty,
+                                               uint32_t *err, uint32_t *C, size_t ldc, int M,
+                                               int N, int tiles_m, int tiles_n, int num_tiles,
+                                               const Modulus &mod, uint32_t alpha, uint32_t beta,
+                                               int row, int q, int cbeg) {
+  using Cfg = TcCfg<L, T>;
+  constexpr int ACC = Cfg::ACC, BN = Cfg::BN, NMMA = Cfg::NMMA;
+  constexpr int W = BN / 2;
+  constexpr int EPB = W < 32 ? W : 32;
+  constexpr int NB = W / EPB;
+  constexpr bool READC = MODE != EPI_SET;
+  const bool vec = ((reinterpret_cast<uintptr_t>(C) & 15u) == 0) && ((ldc & 3u) == 0);
+  int it = 0;
+  for (int t = blockIdx.x; t < num_tiles; t += gridDim.x, ++it) {
+    int mb, nb;
+    tile_coords(t, tiles_m, tiles_n, mb, nb);
+    const int a = it % ACC;
+    const uint32_t aph = (uint32_t)(it / ACC) & 1u;
+    const int gm = mb * BM + row;
+    const uint32_t tbase = tmem + (uint32_t)(a * L * NMMA) + ((uint32_t)(q * 32) << 16);
+    const int gn0 = nb * BN + cbeg;
+    uint32_t *crow = gm < M ? C + (size_t)gm * ldc : nullptr;
+    uint32_t cb[2][EPB];
+    if (READC) load_c<EPB>(cb[0], crow, gn0, N, vec);
+    if (!mbar_wait(&tfull[a], aph, err)) return;
+    tc_fence_after();
+#pragma unroll
+    for (int b = 0; b < NB; ++b) {
+      uint32_t(&cur)[EPB] = cb[b & 1];
+      if (b + 1 < NB && READC) load_c<EPB>(cb[(b + 1) & 1], crow, gn0 + (b + 1) * EPB, N, vec);
+#pragma unroll
+      for (int h = 0; h < EPB / 16; ++h) {
+        uint32_t v[16];
+        chunk_products<L, BN, NMMA>(tbase + (uint32_t)(cbeg + b * EPB + 16 * h), v, mod);
+#pragma unroll
+        for (int i = 0; i < 16; ++i)
+          cur[16 * h + i] = epi_combine<MODE>(v[i], READC ? cur[16 * h + i] : 0u, mod, alpha, beta);
+      }
+      if (b == NB - 1) {
+        tc_fence_before();
+        mbar_arrive(&tempty[a]);
+      }
+      store_c<EPB>(cur, crow, gn0 + b * EPB, N, vec);
+    }
+  }
+}
+
 template <int L, int OUT, int T = 0>
 __global__ void __launch_bounds__(TC_THREADS, 1)
     zp_gemm_tc_kernel(const __grid_constant__ CUtensorMap tmA,
@@ -497,54 +555,30 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     const int row = q * 32 + lane;
     const int half = (warp - 2) >> 2;
     const int cbeg = half * (BN / 2);
-    const int emode = beta == 0u ? EPI_SET
-                      : (beta == 1u && alpha == 1u) ? EPI_ADD
-                      : (beta == 1u && alpha == (uint32_t)mod.p - 1u) ? EPI_SUB
-                                                                     : EPI_AXPBY;
-    const bool readc = emode != EPI_SET;
-    const bool vec = ((reinterpret_cast<uintptr_t>(C) & 15u) == 0) && ((ldc & 3u) == 0);
-    int it = 0;
-    for (int t = blockIdx.x; t < num_tiles; t += gridDim.x, ++it) {
-      int mb, nb;
-      tile_coords(t, tiles_m, tiles_n, mb, nb);
-      const int a = it % ACC;
-      const uint32_t aph = (uint32_t)(it / ACC) & 1u;
-      const int gm = mb * BM + row;
-      const uint32_t tbase = tmem + (uint32_t)(a * L * NMMA) + ((uint32_t)(q * 32) << 16);
-      if constexpr (OUT == 0) {
-        // This thread's row segment: W = BN / 2 columns from gn0, in blocks
-        // of EPB columns.  C's block 0 is loaded before the accumulator is
-        // ready (its latency hides behind the tile's MMAs), block b + 1
-        // while block b is combined; TMEM is released after its last read,
-        // before the last block's stores.
-        constexpr int W = BN / 2;
-        constexpr int EPB = W < 32 ? W : 32;
-        constexpr int NB = W / EPB;
-        const int gn0 = nb * BN + cbeg;
-        uint32_t *crow = gm < M ? C + (size_t)gm * ldc : nullptr;
-        uint32_t cb[2][EPB];
-        if (readc) load_c<EPB>(cb[0], crow, gn0, N, vec);
-        if (!mbar_wait(&tfull[a], aph, err)) break;
-        tc_fence_after();
-#pragma unroll
-        for (int b = 0; b < NB; ++b) {
-          uint32_t(&cur)[EPB] = cb[b & 1];
-          if (b + 1 < NB && readc) load_c<EPB>(cb[(b + 1) & 1], crow, gn0 + (b + 1) * EPB, N, vec);
-#pragma unroll
-          for (int h = 0; h < EPB / 16; ++h) {
-            uint32_t v[16];
-            chunk_products<L, BN, NMMA>(tbase + (uint32_t)(cbeg + b * EPB + 16 * h), v, mod);
-#pragma unroll
-            for (int i = 0; i < 16; ++i)
-              cur[16 * h + i] = epi_combine(emode, v[i], readc ? cur[16 * h + i] : 0u, mod, alpha, beta);
-          }
-          if (b == NB - 1) {
-            tc_fence_before();
-            mbar_arrive(&tempty[a]);
-          }
-          store_c<EPB>(cur, crow, gn0 + b * EPB, N, vec);
-        }
-      } else {
+    if constexpr (OUT == 0) {
+      const int emode = beta == 0u ? EPI_SET
+                        : (beta == 1u && alpha == 1u) ? EPI_ADD
+                        : (beta == 1u && alpha == (uint32_t)mod.p - 1u) ? EPI_SUB
+                                                                       : EPI_AXPBY;
+#define LELA_EPI(MODE)                                                                          \
+  epilogue_tiles<L, T, MODE>(tmem, tfull, tempty, err, C, ldc, M, N, tiles_m, tiles_n, num_tiles, \
+                             mod, alpha, beta, row, q, cbeg)
+      switch (emode) {
+        case EPI_ADD: LELA_EPI(EPI_ADD); break;
+        case EPI_SUB: LELA_EPI(EPI_SUB); break;
+        case EPI_SET: LELA_EPI(EPI_SET); break;
+        default: LELA_EPI(EPI_AXPBY); break;
+      }
+#undef LELA_EPI
+    } else {
+      int it = 0;
+      for (int t = blockIdx.x; t < num_tiles; t += gridDim.x, ++it) {
+        int mb, nb;
+        tile_coords(t, tiles_m, tiles_n, mb, nb);
+        const int a = it % ACC;
+        const uint32_t aph = (uint32_t)(it / ACC) & 1u;
+        const int gm = mb * BM + row;
+        const uint32_t tbase = tmem + (uint32_t)(a * L * NMMA) + ((uint32_t)(q * 32) << 16);
         if (!mbar_wait(&tfull[a], aph, err)) break;
         tc_fence_after();
         epilogue_gf2(tbase, gm, nb * BN, M, N, static_cast<uint64_t *>(Cv), ldc, alpha, beta,
@@ -854,12 +888,15 @@ size_t zp_gemm_workspace_bytes(uint32_t p, int M, int N, int K) {
 }
 
 int zp_gemm_tile_pick(const Ctx *c, int K, uint32_t p) {
-  (void)K;
-  if (zp_limbs_for(p) == 4) return 0;  // one variant for four limbs
+  const int L = zp_limbs_for(p);
+  if (L == 4) return 0;  // one variant for four limbs
   if (c->gemm_tile == GEMM_TILE_WIDE) return 0;
-  // variant 1 by default: measured on the B200 (kernel ms, p = 65521),
-  // 1.750 against 1.735 (the previous one-buffer kernel) and 2.068 (variant
-  // 0) at 8192^3, and 0.116 against 0.168 (variant 0) at 4096 x 4096 x 256
+  if (c->gemm_tile == GEMM_TILE_DOUBLE) return 1;
+  // Measured on the B200 (kernel ms, epilogue instantiated per combine
+  // mode): two limbs, variant 0 / variant 1: 1.411 / 1.690 at 8192^3,
+  // 0.0906 / 0.0901 at 4096 x 4096 x 256, 0.231 / 0.223 at 5000 x 9000 x 64;
+  // one limb, 0.131 / 0.082 at 4096 x 4096 x 256.
+  if (L == 2) return K >= 512 ? 0 : 1;
   return 1;
 }
 
