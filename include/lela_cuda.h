@@ -81,8 +81,8 @@ void *lela_cuda_get_stream (lela_cuda_ctx *ctx);
  * kernel recorded (e.g. LELA_CUDA_ERR_TIMEOUT). */
 int lela_cuda_synchronize (lela_cuda_ctx *ctx);
 int lela_cuda_set_gemm_kernel (lela_cuda_ctx *ctx, int kernel);
-/* Tile variant of the tensor-core Z/p gemm: 0 = automatic (variant 1 for
- * one and two limbs, variant 0 for four), 1 = variant 0 (wide tiles: 256 / 128 / 32
+/* Tile variant of the tensor-core Z/p gemm: 0 = automatic (variant 0 for
+ * two limbs at k >= 512 and for four limbs, else variant 1), 1 = variant 0 (wide tiles: 256 / 128 / 32
  * columns for 1 / 2 / 4 limbs), 2 = variant 1 (128 / 64 columns for 1 / 2
  * limbs with two TMEM accumulator buffers, so the epilogue of one tile
  * overlaps the products of the next; four limbs always use variant 0).
@@ -139,6 +139,41 @@ int lela_cuda_trsm_zp_u32 (lela_cuda_ctx *ctx, int upper, int diag_is_one, size_
 int lela_cuda_trsm_zp_u32_dev (lela_cuda_ctx *ctx, int upper, int diag_is_one, size_t m,
 			       size_t n, uint32_t p, uint32_t a, const uint32_t *A, size_t lda,
 			       uint32_t *B, size_t ldb, size_t *bad_idx);
+/* ------------------------------------- other Modular<T> element types
+ * The Z/p gemm and trsm for matrices of Modular<uint8>, Modular<uint16>,
+ * Modular<float> and Modular<double> elements (and Modular<uint32>, which
+ * forwards to the _u32 entry points above).  elem is one of
+ * LELA_CUDA_ELEM_*; A, B, C point to elements of that type, leading
+ * dimensions count elements.  Element representation as in the reference
+ * (lela/ring/modular.h:115-330): uint8 / uint16 hold 0 .. p-1; float /
+ * double hold the symmetric representative -p/2 .. p/2 (integral values).
+ * The scalars a, b are residues 0 .. p-1.  Moduli as the reference's
+ * ModularTraits<T>::valid_modulus: p < 2^8, 2^16, 4096 (float), 2^26
+ * (double); others return LELA_CUDA_ERR_ARG.  The results equal the
+ * reference's BLAS3::gemm / BLAS3::trsm on Context<Modular<T>> (its float
+ * and double gemm, lela/blas/level3-modular.tcc:25-122, is exact Z/p
+ * arithmetic); for an even p the residue p/2 is stored as +p/2 (the
+ * reference can give either sign).  Errors as for the _u32 forms. */
+enum lela_cuda_elem {
+	LELA_CUDA_ELEM_U8 = 1,
+	LELA_CUDA_ELEM_U16 = 2,
+	LELA_CUDA_ELEM_U32 = 4,
+	LELA_CUDA_ELEM_F32 = 5,
+	LELA_CUDA_ELEM_F64 = 6
+};
+int lela_cuda_gemm_zp (lela_cuda_ctx *ctx, int elem, size_t m, size_t n, size_t k, uint32_t p,
+		       uint32_t a, const void *A, size_t lda, const void *B, size_t ldb, uint32_t b,
+		       void *C, size_t ldc);
+int lela_cuda_gemm_zp_dev (lela_cuda_ctx *ctx, int elem, size_t m, size_t n, size_t k, uint32_t p,
+			   uint32_t a, const void *A, size_t lda, const void *B, size_t ldb,
+			   uint32_t b, void *C, size_t ldc);
+int lela_cuda_trsm_zp (lela_cuda_ctx *ctx, int elem, int upper, int diag_is_one, size_t m,
+		       size_t n, uint32_t p, uint32_t a, const void *A, size_t lda, void *B,
+		       size_t ldb, size_t *bad_idx);
+int lela_cuda_trsm_zp_dev (lela_cuda_ctx *ctx, int elem, int upper, int diag_is_one, size_t m,
+			   size_t n, uint32_t p, uint32_t a, const void *A, size_t lda, void *B,
+			   size_t ldb, size_t *bad_idx);
+
 /* The same solve with a sparse upper-triangular A (n x n) in CSR form:
  * row r's entries are colidx/vals[rowptr[r] .. rowptr[r+1]), rowptr[0] = 0;
  * B is n x ncols dense.  Replaces BLAS3::trsm on a SparseMatrix<uint32>

@@ -12,7 +12,9 @@
  * CUDAModule<uint32> >::echelonize runs the whole Faugere-Lachartre pipeline
  * there, as does EchelonForm<Modular<uint32>, CUDAModule<uint32> >::echelonize
  * for the dense echelon forms, reduced or not; BLAS3::trsm also takes a
- * sparse upper-triangular SparseMatrix<uint32> A.  With Context<GF2, CUDAModuleGF2>, BLAS3::gemm on DenseMatrix<bool>
+ * sparse upper-triangular SparseMatrix<uint32> A.  With Context<Modular<T>,
+ * CUDAModule<T> > for T = uint8, uint16, float or double, BLAS3::gemm and
+ * BLAS3::trsm on DenseMatrix<T> operands run on the GPU.  With Context<GF2, CUDAModuleGF2>, BLAS3::gemm on DenseMatrix<bool>
  * operands runs on the GPU.  Operand combinations the GPU path does not take
  * (sparse gemm operands, sparse lower-triangular or transposed operands) fall
  * through to the parent module, exactly as an unimplemented operation falls
@@ -239,6 +241,125 @@ public:
 				    typename Matrix1::StorageType (),
 				    typename Matrix2::StorageType ()); }
 };
+
+} // namespace BLAS3
+
+/** The CUDA module over Modular<uint8>, Modular<uint16>, Modular<float> and
+ * Modular<double>: GPU gemm and trsm on dense operands (lela_cuda_gemm_zp,
+ * lela_cuda_trsm_zp, which convert the elements to residues on the device
+ * and back); everything else is ZpModule<Element>'s. */
+template <class Element> struct CUDAElemCode;
+template <> struct CUDAElemCode<uint8> { enum { value = LELA_CUDA_ELEM_U8 }; };
+template <> struct CUDAElemCode<uint16> { enum { value = LELA_CUDA_ELEM_U16 }; };
+template <> struct CUDAElemCode<float> { enum { value = LELA_CUDA_ELEM_F32 }; };
+template <> struct CUDAElemCode<double> { enum { value = LELA_CUDA_ELEM_F64 }; };
+
+template <class Element>
+struct CUDAModule : public ZpModule<Element>
+{
+	struct Tag { typedef typename ZpModule<Element>::Tag Parent; };
+
+	CUDAHandle cuda;
+
+	CUDAModule (const Modular<Element> &R) : ZpModule<Element> (R) {}
+};
+
+/** A scalar of Modular<Element> as the residue the C ABI takes (the float
+ * and double representatives can be negative). */
+template <class Element>
+inline uint32_t cuda_residue (const Modular<Element> &F, const Element &a)
+{
+	if (a < 0)
+		return (uint32_t) ((long long) a + (long long) F._modulus);
+	return (uint32_t) a;
+}
+
+namespace BLAS3
+{
+
+template <class Element>
+class CUDAGemmElem
+{
+	typedef typename CUDAModule<Element>::Tag Tag;
+
+	template <class Modules, class Matrix1, class Matrix2, class Matrix3>
+	static Matrix3 &gemm_impl (const Modular<Element> &F, Modules &M, Element a, const Matrix1 &A, const Matrix2 &B, Element b, Matrix3 &C,
+				   MatrixStorageTypes::Generic, MatrixStorageTypes::Generic, MatrixStorageTypes::Generic)
+		{ return _gemm<Modular<Element>, typename Tag::Parent>::op (F, M, a, A, B, b, C); }
+
+	template <class Modules, class Matrix1, class Matrix2, class Matrix3>
+	static Matrix3 &gemm_impl (const Modular<Element> &F, Modules &M, Element a, const Matrix1 &A, const Matrix2 &B, Element b, Matrix3 &C,
+				   MatrixStorageTypes::Dense, MatrixStorageTypes::Dense, MatrixStorageTypes::Dense)
+	{
+		lela_check (A.coldim () == B.rowdim ());
+		lela_check (A.rowdim () == C.rowdim ());
+		lela_check (B.coldim () == C.coldim ());
+		size_t m = C.rowdim (), n = C.coldim (), k = A.coldim ();
+		if (m == 0 || n == 0)
+			return C;
+		const Element *pa = k ? &A[0][0] : 0, *pb = k ? &B[0][0] : 0;
+		int st = lela_cuda_gemm_zp (M.cuda.get (), CUDAElemCode<Element>::value, m, n, k,
+					    (uint32_t) F._modulus, cuda_residue (F, a), pa, k ? A.disp () : 1,
+					    pb, k ? B.disp () : 1, cuda_residue (F, b), &C[0][0], C.disp ());
+		lela_cuda_check (M.cuda.get (), st);
+		return C;
+	}
+
+public:
+	template <class Modules, class Matrix1, class Matrix2, class Matrix3>
+	static Matrix3 &op (const Modular<Element> &F, Modules &M, Element a, const Matrix1 &A, const Matrix2 &B, Element b, Matrix3 &C)
+		{ return gemm_impl (F, M, a, A, B, b, C,
+				    typename Matrix1::StorageType (),
+				    typename Matrix2::StorageType (),
+				    typename Matrix3::StorageType ()); }
+};
+
+template <class Element>
+class CUDATrsmElem
+{
+	typedef typename CUDAModule<Element>::Tag Tag;
+
+	template <class Modules, class Matrix1, class Matrix2>
+	static Matrix2 &trsm_impl (const Modular<Element> &F, Modules &M, Element a, const Matrix1 &A, Matrix2 &B,
+				   TriangularMatrixType type, bool diagIsOne,
+				   MatrixStorageTypes::Generic, MatrixStorageTypes::Generic)
+		{ return _trsm<Modular<Element>, typename Tag::Parent>::op (F, M, a, A, B, type, diagIsOne); }
+
+	template <class Modules, class Matrix1, class Matrix2>
+	static Matrix2 &trsm_impl (const Modular<Element> &F, Modules &M, Element a, const Matrix1 &A, Matrix2 &B,
+				   TriangularMatrixType type, bool diagIsOne,
+				   MatrixStorageTypes::Dense, MatrixStorageTypes::Dense)
+	{
+		lela_check (A.coldim () == B.rowdim ());
+		lela_check (A.rowdim () == B.rowdim ());
+		size_t m = A.rowdim (), n = B.coldim ();
+		if (m == 0)
+			return B;
+		size_t bad = 0;
+		int st = lela_cuda_trsm_zp (M.cuda.get (), CUDAElemCode<Element>::value, type == UpperTriangular, diagIsOne,
+					    m, n, (uint32_t) F._modulus, cuda_residue (F, a), &A[0][0], A.disp (),
+					    n ? &B[0][0] : 0, n ? B.disp () : 1, &bad);
+		lela_cuda_check (M.cuda.get (), st, bad);
+		return B;
+	}
+
+public:
+	template <class Modules, class Matrix1, class Matrix2>
+	static Matrix2 &op (const Modular<Element> &F, Modules &M, Element a, const Matrix1 &A, Matrix2 &B,
+			    TriangularMatrixType type, bool diagIsOne)
+		{ return trsm_impl (F, M, a, A, B, type, diagIsOne,
+				    typename Matrix1::StorageType (),
+				    typename Matrix2::StorageType ()); }
+};
+
+template <> class _gemm<Modular<uint8>, CUDAModule<uint8>::Tag> : public CUDAGemmElem<uint8> {};
+template <> class _gemm<Modular<uint16>, CUDAModule<uint16>::Tag> : public CUDAGemmElem<uint16> {};
+template <> class _gemm<Modular<float>, CUDAModule<float>::Tag> : public CUDAGemmElem<float> {};
+template <> class _gemm<Modular<double>, CUDAModule<double>::Tag> : public CUDAGemmElem<double> {};
+template <> class _trsm<Modular<uint8>, CUDAModule<uint8>::Tag> : public CUDATrsmElem<uint8> {};
+template <> class _trsm<Modular<uint16>, CUDAModule<uint16>::Tag> : public CUDATrsmElem<uint16> {};
+template <> class _trsm<Modular<float>, CUDAModule<float>::Tag> : public CUDATrsmElem<float> {};
+template <> class _trsm<Modular<double>, CUDAModule<double>::Tag> : public CUDATrsmElem<double> {};
 
 } // namespace BLAS3
 

@@ -105,6 +105,10 @@ def load_library():
 def _bind_optional(L):
     """Argument types of the entry points added alongside gemm."""
     sigs = {
+        "lela_cuda_gemm_zp": [_P, _I, _S, _S, _S, _U, _U, _P, _S, _P, _S, _U, _P, _S],
+        "lela_cuda_gemm_zp_dev": [_P, _I, _S, _S, _S, _U, _U, _P, _S, _P, _S, _U, _P, _S],
+        "lela_cuda_trsm_zp": [_P, _I, _I, _I, _S, _S, _U, _U, _P, _S, _P, _S, ctypes.POINTER(_S)],
+        "lela_cuda_trsm_zp_dev": [_P, _I, _I, _I, _S, _S, _U, _U, _P, _S, _P, _S, ctypes.POINTER(_S)],
         "lela_cuda_trsm_zp_u32": [_P, _I, _I, _S, _S, _U, _U, _P, _S, _P, _S, ctypes.POINTER(_S)],
         "lela_cuda_trsm_zp_u32_dev": [_P, _I, _I, _S, _S, _U, _U, _P, _S, _P, _S, ctypes.POINTER(_S)],
         "lela_cuda_trsm_csr_upper_zp_u32": [_P, _S, _S, _U, _U, _I, _P, _P, _P, _P, _S, ctypes.POINTER(_S)],
@@ -154,6 +158,33 @@ def _ptr(a):
 
 def _dptr(t):
     return ctypes.c_void_p(t.data_ptr())
+
+
+# Element types of Modular<T> (include/lela_cuda.h, enum lela_cuda_elem).
+ELEM_U8, ELEM_U16, ELEM_U32, ELEM_F32, ELEM_F64 = 1, 2, 4, 5, 6
+
+
+def _elem_of(X):
+    """(element code, bytes per element) of a numpy array or torch tensor:
+    uint8, uint16 (torch int16 / uint16), uint32 (torch int32), float32,
+    float64 -- the element types of Modular<uint8/uint16/uint32/float/double>."""
+    if _is_torch(X):
+        import torch
+        table = {torch.uint8: ELEM_U8, torch.int16: ELEM_U16, torch.int32: ELEM_U32,
+                 torch.float32: ELEM_F32, torch.float64: ELEM_F64}
+        if hasattr(torch, "uint16"):
+            table[torch.uint16] = ELEM_U16
+        if hasattr(torch, "uint32"):
+            table[torch.uint32] = ELEM_U32
+        code = table.get(X.dtype)
+        _check(code is not None, "unsupported element type %s" % X.dtype)
+        return code, X.element_size()
+    table = {np.dtype(np.uint8): ELEM_U8, np.dtype(np.uint16): ELEM_U16,
+             np.dtype(np.uint32): ELEM_U32, np.dtype(np.float32): ELEM_F32,
+             np.dtype(np.float64): ELEM_F64}
+    code = table.get(X.dtype)
+    _check(code is not None, "unsupported element type %s" % X.dtype)
+    return code, X.itemsize
 
 
 class CudaModule:
@@ -247,7 +278,30 @@ class CudaModule:
     # ---------------------------------------------------------- Z/p gemm
     def gemm(self, p, a, A, B, b, C):
         """C <- a*A*B + b*C mod p in place (BLAS3::gemm); returns C.
-        Host numpy uint32 matrices or torch CUDA tensors (int32/uint32)."""
+        Host numpy matrices or torch CUDA tensors of one element type:
+        uint32 (torch int32), or the element types of Modular<uint8>,
+        Modular<uint16>, Modular<float>, Modular<double> (uint8, uint16,
+        float32, float64; float entries are the symmetric representatives
+        -p/2 .. p/2)."""
+        elem, es = _elem_of(C)
+        if elem != ELEM_U32:
+            _check(_elem_of(A)[0] == elem and _elem_of(B)[0] == elem, "gemm: mixed element types")
+            m, n = C.shape
+            k = A.shape[1]
+            _check(A.shape[0] == m and B.shape == (k, n), "gemm: dimension mismatch")
+            if _is_torch(C):
+                st = self.L.lela_cuda_gemm_zp_dev(self.h, elem, m, n, k, p, a % p, _dptr(A),
+                                                  A.stride(0), _dptr(B), B.stride(0), b % p,
+                                                  _dptr(C), C.stride(0))
+            else:
+                _check(C.flags.c_contiguous or C.strides[1] == es, "gemm: rows of C must be contiguous")
+                A = np.ascontiguousarray(A)
+                B = np.ascontiguousarray(B)
+                st = self.L.lela_cuda_gemm_zp(self.h, elem, m, n, k, p, a % p, _ptr(A), A.strides[0] // es,
+                                              _ptr(B), B.strides[0] // es, b % p, _ptr(C),
+                                              C.strides[0] // es)
+            self._raise(st)
+            return C
         if _is_torch(C):
             m, n = C.shape
             k = A.shape[1]
@@ -276,6 +330,21 @@ class CudaModule:
         _check(A.shape == (m, m) and B.shape[0] == m, "trsm: dimension mismatch")
         n = B.shape[1]
         bad = _S(0)
+        elem, es = _elem_of(B)
+        if elem != ELEM_U32:
+            _check(_elem_of(A)[0] == elem, "trsm: mixed element types")
+            if _is_torch(B):
+                st = self.L.lela_cuda_trsm_zp_dev(self.h, elem, int(upper), int(diag_is_one), m, n, p,
+                                                  a % p, _dptr(A), A.stride(0), _dptr(B), B.stride(0),
+                                                  ctypes.byref(bad))
+            else:
+                _check(B.flags.c_contiguous or B.strides[1] == es, "trsm: rows of B must be contiguous")
+                A = np.ascontiguousarray(A)
+                st = self.L.lela_cuda_trsm_zp(self.h, elem, int(upper), int(diag_is_one), m, n, p,
+                                              a % p, _ptr(A), A.strides[0] // es, _ptr(B),
+                                              B.strides[0] // es, ctypes.byref(bad))
+            self._raise(st, bad.value)
+            return B
         if _is_torch(B):
             st = self.L.lela_cuda_trsm_zp_u32_dev(self.h, int(upper), int(diag_is_one), m, n, p,
                                                   a % p, _dptr(A), A.stride(0), _dptr(B), B.stride(0),

@@ -19,6 +19,7 @@
 #include "common.cuh"
 #include "context.h"
 #include "echelon.h"
+#include "elem.h"
 #include "fl.h"
 #include "gf2.h"
 #include "mlp.h"
@@ -1322,6 +1323,156 @@ int lela_cuda_trsm_zp_u32(lela_cuda_ctx *h, int upper, int diag_is_one, size_t m
                      m, (uint32_t *)dB, n, bad_idx);
   if (!st && n) st = d2h_matrix(c, B, dB, m, n, ldb, 4);
   if (!st) st = ctx_check_status(c, "trsm_zp_u32");
+  return st;
+}
+
+// ------------------------------------------ other Modular<T> element types
+// The operands go to uint32 residues in BUF_ELEM (each part aligned to 256
+// bytes), the uint32 path computes, the result goes back to type T.
+
+static size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+static int gemm_elem_dev(Ctx *c, int elem, size_t m, size_t n, size_t k, uint32_t p, uint32_t a,
+                         const void *A, size_t lda, const void *B, size_t ldb, uint32_t b, void *C,
+                         size_t ldc) {
+  const size_t ba = al256(m * k * 4), bb = al256(k * n * 4), bc = al256(m * n * 4);
+  void *buf = nullptr;
+  int st = ctx_buffer(c, BUF_ELEM, ba + bb + bc, &buf);
+  if (st) return st;
+  uint32_t *uA = static_cast<uint32_t *>(buf);
+  uint32_t *uB = reinterpret_cast<uint32_t *>(static_cast<char *>(buf) + ba);
+  uint32_t *uC = reinterpret_cast<uint32_t *>(static_cast<char *>(buf) + ba + bb);
+  if (k) {
+    if ((st = elem_to_u32(c, elem, A, lda, uA, k, (int)m, (int)k, p))) return st;
+    if ((st = elem_to_u32(c, elem, B, ldb, uB, n, (int)k, (int)n, p))) return st;
+  }
+  // with b = 0 mod p the kernels never read C
+  if (b % p != 0 && (st = elem_to_u32(c, elem, C, ldc, uC, n, (int)m, (int)n, p))) return st;
+  if ((st = zp_gemm_dev(c, GEMM_AUTO, (int)m, (int)n, (int)k, p, a, uA, k, uB, n, b, uC, n,
+                        nullptr)))
+    return st;
+  return elem_from_u32(c, elem, uC, n, C, ldc, (int)m, (int)n, p);
+}
+
+static int gemm_elem_args(Ctx *c, int elem, size_t m, size_t n, size_t k, uint32_t p,
+                          const void *A, size_t lda, const void *B, size_t ldb, const void *C,
+                          size_t ldc) {
+  if (int st = elem_check_modulus(c, elem, p)) return st;
+  if (m > (size_t)INT32_MAX || n > (size_t)INT32_MAX || k > (size_t)INT32_MAX)
+    return ctx_fail(c, ST_ARG, "dimension too large");
+  if (m == 0 || n == 0) return ST_OK;
+  if (!C || (k && (!A || !B))) return ctx_fail(c, ST_ARG, "null pointer");
+  if (ldc < n || (k && (lda < k || ldb < n)))
+    return ctx_fail(c, ST_ARG, "leading dimension smaller than the row length");
+  return ST_OK;
+}
+
+int lela_cuda_gemm_zp_dev(lela_cuda_ctx *h, int elem, size_t m, size_t n, size_t k, uint32_t p,
+                          uint32_t a, const void *A, size_t lda, const void *B, size_t ldb,
+                          uint32_t b, void *C, size_t ldc) {
+  if (!h) return ST_ARG;
+  if (elem == LELA_CUDA_ELEM_U32)
+    return lela_cuda_gemm_zp_u32_dev(h, m, n, k, p, a, static_cast<const uint32_t *>(A), lda,
+                                     static_cast<const uint32_t *>(B), ldb, b,
+                                     static_cast<uint32_t *>(C), ldc);
+  Ctx *c = &h->c;
+  DeviceScope ds(c);
+  if (int st = gemm_elem_args(c, elem, m, n, k, p, A, lda, B, ldb, C, ldc)) return st;
+  if (m == 0 || n == 0) return ST_OK;
+  return gemm_elem_dev(c, elem, m, n, k, p, a, A, lda, B, ldb, b, C, ldc);
+}
+
+int lela_cuda_gemm_zp(lela_cuda_ctx *h, int elem, size_t m, size_t n, size_t k, uint32_t p,
+                      uint32_t a, const void *A, size_t lda, const void *B, size_t ldb, uint32_t b,
+                      void *C, size_t ldc) {
+  if (!h) return ST_ARG;
+  if (elem == LELA_CUDA_ELEM_U32)
+    return lela_cuda_gemm_zp_u32(h, m, n, k, p, a, static_cast<const uint32_t *>(A), lda,
+                                 static_cast<const uint32_t *>(B), ldb, b,
+                                 static_cast<uint32_t *>(C), ldc);
+  Ctx *c = &h->c;
+  if (int st = gemm_elem_args(c, elem, m, n, k, p, A, lda, B, ldb, C, ldc)) return st;
+  if (m == 0 || n == 0) return ST_OK;
+  DeviceScope ds(c);
+  const size_t es = elem_size(elem);
+  void *dA = nullptr, *dB = nullptr, *dC = nullptr;
+  int st = ST_OK;
+  if (!st && k) st = ctx_stage(c, 0, m * k * es, &dA);
+  if (!st && k) st = ctx_stage(c, 1, k * n * es, &dB);
+  if (!st) st = ctx_stage(c, 2, m * n * es, &dC);
+  if (!st) st = ctx_clear_status(c);
+  if (!st && k) st = h2d_matrix(c, dA, A, m, k, lda, es);
+  if (!st && k) st = h2d_matrix(c, dB, B, k, n, ldb, es);
+  if (!st && (b % p) != 0) st = h2d_matrix(c, dC, C, m, n, ldc, es);
+  if (!st) st = gemm_elem_dev(c, elem, m, n, k, p, a, dA, k, dB, n, b, dC, n);
+  if (!st) st = d2h_matrix(c, C, dC, m, n, ldc, es);
+  if (!st) st = ctx_check_status(c, "gemm_zp");
+  return st;
+}
+
+static int trsm_elem_dev(Ctx *c, int elem, bool upper, bool unit, size_t m, size_t n, uint32_t p,
+                         uint32_t a, const void *A, size_t lda, void *B, size_t ldb,
+                         size_t *bad_idx) {
+  const size_t ba = al256(m * m * 4), bb = al256(m * n * 4);
+  void *buf = nullptr;
+  int st = ctx_buffer(c, BUF_ELEM, ba + bb, &buf);
+  if (st) return st;
+  uint32_t *uA = static_cast<uint32_t *>(buf);
+  uint32_t *uB = reinterpret_cast<uint32_t *>(static_cast<char *>(buf) + ba);
+  if ((st = elem_to_u32(c, elem, A, lda, uA, m, (int)m, (int)m, p))) return st;
+  if ((st = elem_to_u32(c, elem, B, ldb, uB, n, (int)m, (int)n, p))) return st;
+  if ((st = zp_trsm_dev(c, upper, unit, (int)m, (int)n, p, a, uA, m, uB, n, bad_idx))) return st;
+  return elem_from_u32(c, elem, uB, n, B, ldb, (int)m, (int)n, p);
+}
+
+static int trsm_elem_args(Ctx *c, int elem, size_t m, size_t n, uint32_t p, const void *A,
+                          size_t lda, const void *B, size_t ldb) {
+  if (int st = elem_check_modulus(c, elem, p)) return st;
+  if (m > (size_t)INT32_MAX || n > (size_t)INT32_MAX) return ctx_fail(c, ST_ARG, "dimension too large");
+  if (m == 0) return ST_OK;
+  if (!A || (n && !B)) return ctx_fail(c, ST_ARG, "null pointer");
+  if (lda < m || (n && ldb < n)) return ctx_fail(c, ST_ARG, "leading dimension smaller than the row length");
+  return ST_OK;
+}
+
+int lela_cuda_trsm_zp_dev(lela_cuda_ctx *h, int elem, int upper, int diag_is_one, size_t m,
+                          size_t n, uint32_t p, uint32_t a, const void *A, size_t lda, void *B,
+                          size_t ldb, size_t *bad_idx) {
+  if (!h) return ST_ARG;
+  if (elem == LELA_CUDA_ELEM_U32)
+    return lela_cuda_trsm_zp_u32_dev(h, upper, diag_is_one, m, n, p, a,
+                                     static_cast<const uint32_t *>(A), lda,
+                                     static_cast<uint32_t *>(B), ldb, bad_idx);
+  Ctx *c = &h->c;
+  DeviceScope ds(c);
+  if (int st = trsm_elem_args(c, elem, m, n, p, A, lda, B, ldb)) return st;
+  if (m == 0) return ST_OK;
+  return trsm_elem_dev(c, elem, upper != 0, diag_is_one != 0, m, n, p, a, A, lda, B, ldb, bad_idx);
+}
+
+int lela_cuda_trsm_zp(lela_cuda_ctx *h, int elem, int upper, int diag_is_one, size_t m, size_t n,
+                      uint32_t p, uint32_t a, const void *A, size_t lda, void *B, size_t ldb,
+                      size_t *bad_idx) {
+  if (!h) return ST_ARG;
+  if (elem == LELA_CUDA_ELEM_U32)
+    return lela_cuda_trsm_zp_u32(h, upper, diag_is_one, m, n, p, a,
+                                 static_cast<const uint32_t *>(A), lda, static_cast<uint32_t *>(B),
+                                 ldb, bad_idx);
+  Ctx *c = &h->c;
+  if (int st = trsm_elem_args(c, elem, m, n, p, A, lda, B, ldb)) return st;
+  if (m == 0) return ST_OK;
+  DeviceScope ds(c);
+  const size_t es = elem_size(elem);
+  void *dA = nullptr, *dB = nullptr;
+  int st = ctx_stage(c, 0, m * m * es, &dA);
+  if (!st && n) st = ctx_stage(c, 1, m * n * es, &dB);
+  if (!st) st = ctx_clear_status(c);
+  if (!st) st = h2d_matrix(c, dA, A, m, m, lda, es);
+  if (!st && n) st = h2d_matrix(c, dB, B, m, n, ldb, es);
+  if (!st)
+    st = trsm_elem_dev(c, elem, upper != 0, diag_is_one != 0, m, n, p, a, dA, m, dB, n, bad_idx);
+  if (!st && n) st = d2h_matrix(c, B, dB, m, n, ldb, es);
+  if (!st) st = ctx_check_status(c, "trsm_zp");
   return st;
 }
 

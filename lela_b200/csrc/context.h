@@ -29,7 +29,7 @@ enum GemmKernel : int {
 // (narrower tiles, two accumulator buffers, so that a tile's epilogue
 // overlaps the next tile's products); four limbs have variant 0 only.
 enum GemmTile : int {
-  GEMM_TILE_AUTO = 0,    // variant 1 for one and two limbs, else variant 0
+  GEMM_TILE_AUTO = 0,    // variant 0 for two limbs at K >= 512 and four limbs, else variant 1
   GEMM_TILE_WIDE = 1,    // variant 0
   GEMM_TILE_DOUBLE = 2,  // variant 1
 };
@@ -153,7 +153,8 @@ enum BufSlot : int {
   BUF_FL_CSR_P = 24,  // Faugere-Lachartre CSR output: row counts, row pointers, scan scratch
   BUF_FL_CSR_V = 25,  // Faugere-Lachartre CSR output: column indices and values
   BUF_PLUQ = 26,      // PLUQ: kept multipliers, assembled output, column order
-  BUF_COUNT = 27,
+  BUF_ELEM = 27,      // uint32 copies of Modular<uint8/uint16/float/double> operands
+  BUF_COUNT = 28,
 };
 
 // Grow-only allocation helpers; return ST_OK or ST_NOMEM.

@@ -95,6 +95,8 @@ def ref():
         L.lela_ref_write_dumas.argtypes = [_U, _S, _S, _P, _S, ctypes.c_char_p, _S, ctypes.POINTER(_S)]
         L.lela_ref_write_matrix.argtypes = [_I, _U, _S, _S, _P, _S, ctypes.c_char_p, _S, ctypes.POINTER(_S)]
         L.lela_ref_read_matrix.argtypes = [_I, _U, ctypes.c_char_p, _S, _S, _P]
+        L.lela_ref_gemm_zp_elem.argtypes = [_I, _U, _S, _S, _S, _U, _P, _S, _P, _S, _U, _P, _S]
+        L.lela_ref_trsm_zp_elem.argtypes = [_I, _U, _I, _I, _S, _S, _U, _P, _S, _P, _S, ctypes.POINTER(_S)]
         L.lela_ref_pluq_zp_u32.argtypes = [_U, _S, _S, _P, _S, _P, ctypes.POINTER(_S), _P, ctypes.POINTER(_S),
                                            ctypes.POINTER(_S), ctypes.POINTER(_U)]
         _ref = L
@@ -124,6 +126,49 @@ def trsm_zp(p, A, B, upper, diag_is_one, a=1):
     bad = _S(0)
     rc = lib().oracle_trsm_zp_u32(p, int(upper), int(diag_is_one), m, n, a, _ptr(A), m, _ptr(B), n, ctypes.byref(bad))
     return B, (bad.value if rc else None)
+
+
+# Other Modular<T> element types (lela/ring/modular.h:115-330): uint8 and
+# uint16 hold residues 0 .. p-1, float and double the symmetric
+# representative (ModularTraits<float>::reduce: fmod, then shift_up v < -p/2
+# -> v + p, then shift_down v > p/2 -> v - p).  Their gemm and trsm are exact
+# Z/p arithmetic (lela/blas/level3-modular.tcc:25-122 keeps every partial sum
+# below the mantissa), so the restatement runs the uint32 restatement on the
+# residues and stores the result in the type's representation.
+ELEM_CODES = {np.dtype(np.uint8): 1, np.dtype(np.uint16): 2, np.dtype(np.float32): 5,
+              np.dtype(np.float64): 6}
+
+
+def to_residues(X, p):
+    """Elements of Modular<T> (T = X.dtype) as uint32 residues."""
+    X = np.asarray(X)
+    if X.dtype.kind == "f":
+        v = X.astype(np.int64)
+        return np.where(v < 0, v + p, v).astype(np.uint32)
+    return X.astype(np.uint32)
+
+
+def from_residues(R, p, dtype):
+    """uint32 residues as elements of Modular<dtype> (for float / double the
+    representative in [-p/2, p/2]; +p/2 for the residue p/2 of an even p)."""
+    dtype = np.dtype(dtype)
+    R = np.asarray(R, dtype=np.int64)
+    if dtype.kind == "f":
+        return np.where(2 * R > p, R - p, R).astype(dtype)
+    return R.astype(dtype)
+
+
+def gemm_zp_elem(p, A, B, C, a=1, b=1):
+    dt = np.asarray(C).dtype
+    R = gemm_zp(p, to_residues(A, p), to_residues(B, p), to_residues(C, p), a, b)
+    return from_residues(R, p, dt)
+
+
+def trsm_zp_elem(p, A, B, upper, diag_is_one, a=1):
+    """Returns (B', bad_idx or None)."""
+    dt = np.asarray(B).dtype
+    R, bad = trsm_zp(p, to_residues(A, p), to_residues(B, p), upper, diag_is_one, a)
+    return from_residues(R, p, dt), bad
 
 
 def echelon_zp(p, A):
@@ -218,6 +263,27 @@ def ref_trsm_zp(p, A, B, upper, diag_is_one, a=1, threads=1):
         return B, None
     bad = _S(0)
     rc = ref().lela_ref_trsm_zp_u32(p, int(upper), int(diag_is_one), m, n, a, _ptr(A), m, _ptr(B), n, ctypes.byref(bad))
+    return B, (bad.value if rc else None)
+
+
+def ref_gemm_zp_elem(p, A, B, C, a=1, b=1):
+    """LELA's BLAS3::gemm on Context<Modular<T> >, T = the arrays' dtype."""
+    dt = np.asarray(C).dtype
+    A = _c(A, dt); B = _c(B, dt); C = _c(C, dt).copy()
+    m, k = A.shape; n = B.shape[1]
+    rc = ref().lela_ref_gemm_zp_elem(ELEM_CODES[dt], p, m, n, k, a, _ptr(A), k, _ptr(B), n, b, _ptr(C), n)
+    assert rc == 0, rc
+    return C
+
+
+def ref_trsm_zp_elem(p, A, B, upper, diag_is_one, a=1):
+    dt = np.asarray(B).dtype
+    A = _c(A, dt); B = _c(B, dt).copy()
+    m = A.shape[0]; n = B.shape[1]
+    bad = _S(0)
+    rc = ref().lela_ref_trsm_zp_elem(ELEM_CODES[dt], p, int(upper), int(diag_is_one), m, n, a,
+                                     _ptr(A), m, _ptr(B), n, ctypes.byref(bad))
+    assert rc in (0, 1), rc
     return B, (bad.value if rc else None)
 
 

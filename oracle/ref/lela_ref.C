@@ -125,6 +125,69 @@ void run_jobs (std::vector<SliceJob> &jobs)
 	for (size_t t = 0; t < jobs.size (); ++t) pthread_join (th[t], 0);
 }
 
+// Other element types of Modular<T> (lela/ring/modular.h:115-330).  A
+// scalar given as a residue r becomes T's representative: r itself for the
+// unsigned types, r or r - p (whichever lies in [-p/2, p/2]) for float and
+// double, whose ModularTraits keep the symmetric range.
+template <class T> T elem_of (uint32_t r, uint32_t p) { return (T) r; }
+template <> float elem_of<float> (uint32_t r, uint32_t p)
+	{ return 2ULL * r > p ? (float) ((long long) r - (long long) p) : (float) r; }
+template <> double elem_of<double> (uint32_t r, uint32_t p)
+	{ return 2ULL * r > p ? (double) ((long long) r - (long long) p) : (double) r; }
+
+template <class T>
+void load_t (DenseMatrix<T> &M, const T *src, size_t ld)
+{
+	for (size_t i = 0; i < M.rowdim (); ++i)
+		for (size_t j = 0; j < M.coldim (); ++j)
+			M[i][j] = src[i * ld + j];
+}
+
+template <class T>
+void store_t (const DenseMatrix<T> &M, T *dst, size_t ld)
+{
+	for (size_t i = 0; i < M.rowdim (); ++i)
+		for (size_t j = 0; j < M.coldim (); ++j)
+			dst[i * ld + j] = M[i][j];
+}
+
+// BLAS3::gemm on Context<Modular<T> > (the default module stack).
+template <class T>
+void gemm_t (uint32_t p, size_t m, size_t n, size_t k, uint32_t a, const void *A, size_t lda,
+	     const void *B, size_t ldb, uint32_t b, void *C, size_t ldc)
+{
+	Modular<T> F (p);
+	Context<Modular<T> > ctx (F);
+	DenseMatrix<T> MA (m, k), MB (k, n), MC (m, n);
+	if (m && k) load_t (MA, (const T *) A, lda);
+	if (k && n) load_t (MB, (const T *) B, ldb);
+	if (m && n) load_t (MC, (const T *) C, ldc);
+	BLAS3::gemm (ctx, elem_of<T> (a, p), MA, MB, elem_of<T> (b, p), MC);
+	if (m && n) store_t (MC, (T *) C, ldc);
+}
+
+// BLAS3::trsm on Context<Modular<T> >; 1 with *bad_idx on
+// DiagonalEntryNotInvertible (B then as LELA left it).
+template <class T>
+int trsm_t (uint32_t p, int upper, int diag_is_one, size_t m, size_t n, uint32_t a, const void *A,
+	    size_t lda, void *B, size_t ldb, size_t *bad_idx)
+{
+	Modular<T> F (p);
+	Context<Modular<T> > ctx (F);
+	DenseMatrix<T> MA (m, m), MB (m, n);
+	if (m) load_t (MA, (const T *) A, lda);
+	if (m && n) load_t (MB, (const T *) B, ldb);
+	int ret = 0;
+	try {
+		BLAS3::trsm (ctx, elem_of<T> (a, p), MA, MB, upper ? UpperTriangular : LowerTriangular, diag_is_one != 0);
+	} catch (DiagonalEntryNotInvertible &e) {
+		if (bad_idx) *bad_idx = e.idx ();
+		ret = 1;
+	}
+	if (m && n) store_t (MB, (T *) B, ldb);
+	return ret;
+}
+
 } // namespace
 
 extern "C" {
@@ -548,6 +611,45 @@ int lela_ref_write_dumas (uint32_t p, size_t m, size_t n, const uint32_t *A, siz
 		return 3;
 	std::memcpy (buf, t.c_str (), t.size () + 1);
 	return 0;
+}
+
+/* BLAS3::gemm and BLAS3::trsm over Modular<uint8> (elem 1), Modular<uint16>
+ * (2), Modular<float> (5) and Modular<double> (6) with the default module
+ * stack (as tests/test-blas-zp-module.C:161-168 runs them).  Matrices hold
+ * elements of that type; a and b are residues.  Returns -1 for an unknown
+ * type or an exception other than DiagonalEntryNotInvertible. */
+int lela_ref_gemm_zp_elem (int elem, uint32_t p, size_t m, size_t n, size_t k, uint32_t a,
+			   const void *A, size_t lda, const void *B, size_t ldb, uint32_t b,
+			   void *C, size_t ldc)
+{
+	try {
+		switch (elem) {
+		case 1: gemm_t<uint8> (p, m, n, k, a, A, lda, B, ldb, b, C, ldc); break;
+		case 2: gemm_t<uint16> (p, m, n, k, a, A, lda, B, ldb, b, C, ldc); break;
+		case 5: gemm_t<float> (p, m, n, k, a, A, lda, B, ldb, b, C, ldc); break;
+		case 6: gemm_t<double> (p, m, n, k, a, A, lda, B, ldb, b, C, ldc); break;
+		default: return -1;
+		}
+	} catch (...) {
+		return -1;
+	}
+	return 0;
+}
+
+int lela_ref_trsm_zp_elem (int elem, uint32_t p, int upper, int diag_is_one, size_t m, size_t n,
+			   uint32_t a, const void *A, size_t lda, void *B, size_t ldb, size_t *bad_idx)
+{
+	try {
+		switch (elem) {
+		case 1: return trsm_t<uint8> (p, upper, diag_is_one, m, n, a, A, lda, B, ldb, bad_idx);
+		case 2: return trsm_t<uint16> (p, upper, diag_is_one, m, n, a, A, lda, B, ldb, bad_idx);
+		case 5: return trsm_t<float> (p, upper, diag_is_one, m, n, a, A, lda, B, ldb, bad_idx);
+		case 6: return trsm_t<double> (p, upper, diag_is_one, m, n, a, A, lda, B, ldb, bad_idx);
+		default: return -1;
+		}
+	} catch (...) {
+		return -1;
+	}
 }
 
 } // extern "C"

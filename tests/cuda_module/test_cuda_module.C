@@ -273,6 +273,64 @@ static void test_echelon (uint32 p, size_t m, size_t n, bool reduced, int method
 	CHECK (Eg.rank (A) == rb && BLAS3::equal (cpu, A, B), what);
 }
 
+// The other element types (tests/test-blas-zp-module.C:161-168): gemm and
+// trsm with Context<Modular<T>, CUDAModule<T> > against the default module
+// stack of Modular<T> (odd moduli: the representatives are unique).
+template <class T>
+static void fill_t (const Modular<T> &F, DenseMatrix<T> &A, MersenneTwister &MT, bool nonzero = false)
+{
+	for (size_t i = 0; i < A.rowdim (); ++i)
+		for (size_t j = 0; j < A.coldim (); ++j) {
+			T x;
+			F.init (x, (integer) MT.randomIntRange (nonzero ? 1 : 0, (uint32) F._modulus));
+			A.setEntry (i, j, x);
+		}
+}
+
+template <class T>
+static bool same_t (const DenseMatrix<T> &A, const DenseMatrix<T> &B)
+{
+	for (size_t i = 0; i < A.rowdim (); ++i)
+		for (size_t j = 0; j < A.coldim (); ++j)
+			if (A[i][j] != B[i][j])
+				return false;
+	return true;
+}
+
+template <class T>
+static void test_elem (const char *name, uint32 p, size_t m, size_t n, size_t k)
+{
+	Modular<T> F (p);
+	Context<Modular<T>, CUDAModule<T> > gpu (F);
+	Context<Modular<T> > cpu (F);
+	MersenneTwister MT (p + m);
+	DenseMatrix<T> A (m, k), B (k, n), C (m, n), C2 (m, n);
+	fill_t (F, A, MT); fill_t (F, B, MT); fill_t (F, C, MT);
+	BLAS3::copy (cpu, C, C2);
+	T a, b;
+	F.init (a, (integer) 3);
+	F.init (b, (integer) (p - 1));
+	BLAS3::gemm (gpu, a, A, B, b, C);
+	BLAS3::gemm (cpu, a, A, B, b, C2);
+	char what[160];
+	std::snprintf (what, sizeof what, "gemm %s p=%u %zux%zux%zu CUDAModule == default modules", name, p, m, n, k);
+	CHECK (same_t (C, C2), what);
+
+	DenseMatrix<T> L (m, m), X (m, n), X2 (m, n);
+	for (size_t i = 0; i < m; ++i)
+		for (size_t j = 0; j < m; ++j) {
+			T x;
+			F.init (x, (integer) (j < i ? MT.randomIntRange (0, p) : (j == i ? MT.randomIntRange (1, p) : 0)));
+			L.setEntry (i, j, x);
+		}
+	fill_t (F, X, MT);
+	BLAS3::copy (cpu, X, X2);
+	BLAS3::trsm (gpu, a, L, X, LowerTriangular, false);
+	BLAS3::trsm (cpu, a, L, X2, LowerTriangular, false);
+	std::snprintf (what, sizeof what, "trsm %s p=%u %zux%zu lower CUDAModule == default modules", name, p, m, n);
+	CHECK (same_t (X, X2), what);
+}
+
 int main ()
 {
 	try {
@@ -296,6 +354,12 @@ int main ()
 		test_echelon (65521, 90, 130, false, EFc::METHOD_STANDARD_GJ);
 		test_echelon (65521, 60, 80, true, EFc::METHOD_STANDARD_GJ);
 		test_echelon (251, 140, 70, true, EFc::METHOD_STANDARD_GJ);
+		test_elem<uint8> ("Modular<uint8>", 251, 50, 30, 50);
+		test_elem<uint16> ("Modular<uint16>", 65521, 50, 30, 50);
+		test_elem<float> ("Modular<float>", 2039, 50, 30, 50);
+		test_elem<float> ("Modular<float>", 4093, 70, 20, 90);
+		test_elem<double> ("Modular<double>", 33554393, 50, 30, 50);
+		test_elem<double> ("Modular<double>", 67108859, 70, 20, 90);
 	} catch (LELAError &e) {
 		std::printf ("FAIL: LELAError thrown\n");
 		return 2;
