@@ -52,6 +52,7 @@
 #include <algorithm>
 #include <cstddef>
 #include <mutex>
+#include <type_traits>
 #include <vector>
 
 #include "common.cuh"
@@ -222,6 +223,7 @@ constexpr int PW_R = 80;                   // window rows
 // test, the multipliers) then touches every bank once
 constexpr int PW_LD = EW + 1;
 constexpr size_t PW_SMEM = (size_t)PW_R * PW_LD * 4;  // dynamic shared memory: the window rows
+constexpr int PW_EU = (PW_R + 31) / 32;  // window list entries per lane
 
 template <class A>
 __global__ void __launch_bounds__(PS_THREADS, 1)
@@ -238,7 +240,7 @@ __global__ void __launch_bounds__(PS_THREADS, 1)
   __shared__ int wrow[PW_R];
   __shared__ uint32_t s_red[PS_FAST][EW];  // rows past the window, reduced (one per warp)
   __shared__ int s_pcol[EW];
-  __shared__ uint32_t s_y[EW], s_S[EW], s_x[EW], s_sinv[EW];
+  __shared__ uint32_t s_y[EW], s_S[EW], s_x[EW], s_sinv[EW], s_yinv[EW];
   __shared__ int s_cnt[EW + 1];
   __shared__ int s_first[PS_FAST], s_wcnt[PS_FAST];
   __shared__ int s_list[PS_THREADS], s_lrow[PS_THREADS], s_lhead[PS_THREADS];
@@ -272,18 +274,21 @@ __global__ void __launch_bounds__(PS_THREADS, 1)
       perm[0][slot] = slot;
       ppos[0][slot] = pos;
       wrow[slot] = pos;
-      const uint32_t *src = D + (size_t)pos * ld + c0;
-      for (int c = 0; c < EW; ++c) cp_async4(&Wv[slot][c], src + (c < w ? c : 0), c < w);
+      atomicSub(&s_cnt[head[pos]], 1);  // the window's rows leave the counts
       if (off == wcap - 1 - nl) s_wlast = pos;
     }
     nl += take;
     __syncthreads();  // s_wcnt is rewritten by the next pass
   }
+  // the window rows' panel values: all threads, consecutive lanes on
+  // consecutive columns of a row (coalesced reads)
+  for (int e = tid; e < nl * EW; e += PS_THREADS) {
+    const int slot = e / EW, c = e % EW;
+    cp_async4(&Wv[slot][c], D + (size_t)wrow[slot] * ld + c0 + (c < w ? c : 0), c < w);
+  }
   cp_async_wait_all();
   __syncthreads();
   const int wlast = s_wlast;  // rows past it are outside the window
-  for (int k = tid; k < nl; k += PS_THREADS) atomicSub(&s_cnt[head[wrow[k]]], 1);
-  __syncthreads();
 
   int cur = 0, i = i0, t = 0;
   uint32_t S = 1u % p;
@@ -432,37 +437,50 @@ __global__ void __launch_bounds__(PS_THREADS, 1)
     // write the new entry list
     const uint32_t y = P[col];
     {
-      // the ac live columns right of col, each taken by G threads that
-      // split the rows: every thread has work until the last columns.  The
-      // rows are taken four at a time, all their loads issued before any
-      // store (a store to the window may alias a later row's loads, so the
-      // compiler would otherwise keep one row's load-compute-store chain
-      // behind the previous one's)
-      const int ac = w - col - 1;
-      if (ac > 0) {
-        const int G = PS_THREADS / ac;
-        if (tid < G * ac) {
-          const int c = col + 1 + tid % ac;
-          const uint32_t pc = P[c];
-          for (int s0 = tid / ac; s0 < nl; s0 += 4 * G) {
-            int pr[4];
-            uint32_t av[4], wv[4];
+      // Warp wid takes the columns col + 1 + wid, col + 17 + wid, ..; lane
+      // takes the list entries lane, lane + 32, lane + 64.  An entry's
+      // multiplier W[col] is loaded once for all of the warp's columns, and
+      // two columns are in flight at a time (their loads issued before
+      // their stores).
+      // NU groups of 32 entries, NU fixed per instantiation (the window
+      // shrinks by one entry per pivot, so most columns need one or two)
+      auto elim = [&](auto nu_c) {
+        constexpr int NU = decltype(nu_c)::value;
+        int pr[NU];
+        uint32_t na[NU];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-              const int s = s0 + u * G;
-              pr[u] = (s < nl && s != drop) ? pm[s] : -1;
-            }
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-              av[u] = pr[u] >= 0 ? Wv[pr[u]][col] : 0u;
-              wv[u] = pr[u] >= 0 ? Wv[pr[u]][c] : 0u;
-            }
-#pragma unroll
-            for (int u = 0; u < 4; ++u)
-              if (pr[u] >= 0) Wv[pr[u]][c] = ar.dot2(y, wv[u], av[u] ? p - av[u] : 0u, pc);
-          }
+        for (int u = 0; u < NU; ++u) {
+          const int s = lane + 32 * u;
+          pr[u] = (s < nl && s != drop) ? pm[s] : -1;
+          const uint32_t a = pr[u] >= 0 ? Wv[pr[u]][col] : 0u;
+          na[u] = a ? p - a : 0u;
         }
-      }
+        for (int c = col + 1 + wid; c < w; c += 2 * PS_FAST) {
+          const int c2 = c + PS_FAST;
+          const bool two = c2 < w;
+          const uint32_t pc = P[c], pc2 = two ? P[c2] : 0u;
+          uint32_t wv[NU], wv2[NU];
+#pragma unroll
+          for (int u = 0; u < NU; ++u) {
+            wv[u] = pr[u] >= 0 ? Wv[pr[u]][c] : 0u;
+            wv2[u] = (pr[u] >= 0 && two) ? Wv[pr[u]][c2] : 0u;
+          }
+#pragma unroll
+          for (int u = 0; u < NU; ++u)
+            if (pr[u] >= 0) {
+              Wv[pr[u]][c] = ar.dot2(y, wv[u], na[u], pc);
+              if (two) Wv[pr[u]][c2] = ar.dot2(y, wv2[u], na[u], pc2);
+            }
+        }
+      };
+      static_assert(PW_EU == 3, "the dispatch below covers three groups");
+      const int nu = (nl + 31) >> 5;
+      if (nu <= 1)
+        elim(std::integral_constant<int, 1>{});
+      else if (nu == 2)
+        elim(std::integral_constant<int, 2>{});
+      else
+        elim(std::integral_constant<int, 3>{});
     }
     if (tid < EW) PV[t][tid] = P[tid];
     const int nn = drop >= 0 ? nl - 1 : nl;
@@ -503,15 +521,24 @@ __global__ void __launch_bounds__(PS_THREADS, 1)
     s_hi = i - 1;
   }
   __syncthreads();
+  // For p < 2^31 the reference's inverse is the exact one, so x_k^-1 =
+  // S_k y_k^-1, and the two inversions of pivot k run side by side (threads
+  // k and 64 + k); for larger p the reference's inverse of x_k itself.
+  const bool exact_inv = p < 0x80000000u;
   if (tid < t) {
-    const uint32_t si = inv_exact_u32(p, s_S[tid]);
+    s_sinv[tid] = inv_exact_u32(p, s_S[tid]);
+    atomicMax(&s_hi, (int)out->tq[tid]);
+  } else if (exact_inv && tid >= EW && tid < EW + t) {
+    s_yinv[tid - EW] = inv_exact_u32(p, s_y[tid - EW]);
+  }
+  __syncthreads();
+  if (tid < t) {
+    const uint32_t si = s_sinv[tid];
     const uint32_t x = ar.mul(s_y[tid], si);
-    const uint32_t xi = lela_inv_u32(p, x);
-    s_sinv[tid] = si;
+    const uint32_t xi = exact_inv ? ar.mul(s_S[tid], s_yinv[tid]) : lela_inv_u32(p, x);
     s_x[tid] = x;
     xinv_out[tid] = xi;
     if (si == 0u || xi == 0u) atomicOr(&s_err, 1);
-    atomicMax(&s_hi, (int)out->tq[tid]);
   }
   __syncthreads();
   // U_k = (S_k U_k) / S_k; entries left of the pivot column are not kept up
@@ -529,12 +556,19 @@ __global__ void __launch_bounds__(PS_THREADS, 1)
   for (int pos = max(wlast + 1, i) + tid; pos <= hi && pos < m; pos += PS_THREADS)
     if (act[row_at(pos, p2r, stamp, epoch)]) atomicMax(&s_last, pos);
   __syncthreads();
+  // the panel's determinant factor: product of the x_k, by warp 0
+  uint32_t det = 1u % p;
+  if (wid == 0) {
+    uint32_t v = lane < t ? s_x[lane] : 1u % p;
+    if (lane + 32 < t) v = ar.mul(v, s_x[lane + 32]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = ar.mul(v, __shfl_xor_sync(0xffffffffu, v, o));
+    det = v;
+  }
   if (tid == 0) {
     const int la = *last_act;
     int last = s_last;
     if (la > hi) last = max(last, la);
-    uint32_t det = 1u % p;
-    for (int k = 0; k < t; ++k) det = ar.mul(det, s_x[k]);
     out->t = (uint32_t)t;
     out->err = (uint32_t)s_err;
     out->last_pos = (uint32_t)(last >= 0 ? last : 0);

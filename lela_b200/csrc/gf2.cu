@@ -40,11 +40,12 @@ namespace lela {
 
 // ------------------------------------------------------------------ M4RM
 constexpr int M4_BW = 8;      // words of C per CTA
-constexpr int M4_ROWS = 4;    // rows of C per thread
 constexpr int M4_THREADS = 256;
 constexpr int M4_KC = 32;     // rows of B per table round (4 tables of 8)
 
-// C[r, w0 .. w0+8) for the CTA's rows; tables T[g][w][s] in shared memory.
+// C[r, w0 .. w0+8) for the CTA's rows (M4_ROWS per thread); tables
+// T[g][w][s] in shared memory.
+template <int M4_ROWS>
 __global__ void __launch_bounds__(M4_THREADS)
     gf2_m4rm_kernel(const uint64_t *__restrict__ A, size_t lda, const uint64_t *__restrict__ B,
                     size_t ldb, uint64_t *__restrict__ C, size_t ldc, int M, int Nw, int K,
@@ -119,14 +120,26 @@ int gf2_m4rm_dev(Ctx *c, int M, int N, int K, int alpha, const uint64_t *A, size
   if (M <= 0 || N <= 0) return ST_OK;
   const int Nw = (N + 63) / 64;
   const uint64_t tail = (N & 63) ? ((1ull << (N & 63)) - 1ull) : ~0ull;
-  dim3 grid((Nw + M4_BW - 1) / M4_BW, (M + M4_THREADS * M4_ROWS - 1) / (M4_THREADS * M4_ROWS));
   constexpr int smem = (4 * M4_BW * 256 + M4_KC * M4_BW) * 8;
-  if (int st = ctx_smem_attr(c, (const void *)gf2_m4rm_kernel, smem,
+  if (int st = ctx_smem_attr(c, (const void *)gf2_m4rm_kernel<4>, smem,
                              "cudaFuncSetAttribute(gf2_m4rm)"))
     return st;
+  if (int st = ctx_smem_attr(c, (const void *)gf2_m4rm_kernel<1>, smem,
+                             "cudaFuncSetAttribute(gf2_m4rm)"))
+    return st;
+  // four rows per thread; one when that leaves fewer than two CTAs per SM
+  // (narrow C: the tables are then built by more CTAs, but all SMs work)
+  const int gx = (Nw + M4_BW - 1) / M4_BW;
+  const bool wide = (size_t)gx * ((M + M4_THREADS * 4 - 1) / (M4_THREADS * 4)) >= 2u * c->num_sms;
+  const int rows_cta = M4_THREADS * (wide ? 4 : 1);
+  dim3 grid(gx, (M + rows_cta - 1) / rows_cta);
   int pi = prof_begin(c, "gf2_m4rm");
-  gf2_m4rm_kernel<<<grid, M4_THREADS, smem, c->stream>>>(A, lda, B, ldb, C, ldc, M, Nw, K, tail,
-                                                         alpha, beta);
+  if (wide)
+    gf2_m4rm_kernel<4><<<grid, M4_THREADS, smem, c->stream>>>(A, lda, B, ldb, C, ldc, M, Nw, K,
+                                                              tail, alpha, beta);
+  else
+    gf2_m4rm_kernel<1><<<grid, M4_THREADS, smem, c->stream>>>(A, lda, B, ldb, C, ldc, M, Nw, K,
+                                                              tail, alpha, beta);
   prof_end(c, pi);
   ctx_launched(c);
   cudaError_t e = cudaGetLastError();
@@ -638,7 +651,9 @@ int gf2_echelon_dev(Ctx *c, int m, int n, uint64_t *D, size_t ld, size_t *rank_o
     const int nrest = n - 64 * bw1;  // bits right of the block
     for (int j = 0; j < np; ++j) {
       if (pan_off[j] > 0) {
-        int s = gf2_gemm_dev(c, GF2_AUTO, pan_t[j], nrest, pan_off[j], 1,
+        // M = this panel's pivots (<= 64 rows): the four-Russians kernel,
+        // which needs no byte expansion of the wide B
+        int s = gf2_gemm_dev(c, GF2_M4RM, pan_t[j], nrest, pan_off[j], 1,
                              d_Lb + (size_t)pan_i[j] * GB, GB, D + (size_t)ib * ld + bw1, ld, 1,
                              D + (size_t)pan_i[j] * ld + bw1, ld);
         if (s) return s;
