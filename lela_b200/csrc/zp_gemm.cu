@@ -903,12 +903,15 @@ int zp_gemm_tile_pick(const Ctx *c, int K, uint32_t p) {
 int zp_gemm_pick(const Ctx *c, int M, int N, int K, uint32_t p) {
   if (c->gemm_kernel != GEMM_AUTO) return c->gemm_kernel;
   // small K: the CUDA-core kernel below its measured crossover with the
-  // tensor-core path (whose fixed and per-output costs grow with the limb
-  // count L)
+  // tensor-core path, which has a fixed cost of about 20 us (limb split and
+  // launch) and then runs far faster.  Measured on the B200 (us per call,
+  // small-K / tensor cores, p = 65521): 8000 x 448 x 64: 57.8 / 31.3;
+  // 8000 x 64 x 64: 14.9 / 20.6; 4000 x 200 x 40: 23.9 / 20.4; p = 2^31 - 1,
+  // 8000 x 448 x 64: 104.8 / 76.4 -- a crossover near 3e7 multiply-adds,
+  // higher for narrow C (the tensor cores' tiles are 64 or more columns wide)
   const double work = (double)M * N * K;
-  const bool wide = zp_limbs_for(p) == 4;
-  const bool smallk = wide ? ((K <= 64 && work <= 4.0e9) || (K <= 256 && work <= 2.4e9))
-                           : ((K <= 32 && work <= 4.0e9) || (K <= 256 && work <= 6.0e8));
+  const bool smallk = K <= 256 && (work <= 2.5e7 || (N <= 96 && work <= 6.0e7));
+  (void)p;
   return smallk ? GEMM_SMALLK : GEMM_TC;
 }
 
