@@ -58,6 +58,8 @@ def parse():
     ap.add_argument("--no-fl", action="store_true")
     ap.add_argument("--fl-only", action="store_true",
                     help="run only the Faugere-Lachartre line (profiling aid)")
+    ap.add_argument("--gf2-only", action="store_true",
+                    help="run only the GF(2) gemm and echelon line (profiling aid)")
     ap.add_argument("--gemm-only", metavar="M,N,K",
                     help="time only a Z/p gemm of this shape on the tensor cores (profiling aid)")
     ap.add_argument("--gemm-p", type=int, default=P)
@@ -991,6 +993,19 @@ def run_fl_only(args):
     print(json.dumps(run_fl(args, cm, stream, torch, dev, 0, zp_peak=int8_peak_tops(torch, dev)[0] / 4)))
 
 
+def run_gf2_only(args):
+    """Only the GF(2) line (for kernel launch lists): one process, one GPU;
+    prints its JSON object."""
+    import torch
+    from lela_b200 import CudaModule
+    dev = torch.device("cuda", 0)
+    cm = CudaModule(0)
+    stream = torch.cuda.Stream(device=dev)
+    cm.set_stream(stream)
+    print(json.dumps(run_gf2(args, cm, stream, torch, dev, int8_peak_tops(torch, dev)[0])))
+    cm.close()
+
+
 def run_gemm_only(args):
     """One Z/p gemm shape C <- C - A*B (the update form of the triangular
     solve and the elimination) on the tensor-core kernel, inputs resident:
@@ -1033,6 +1048,8 @@ def main():
         run_gemm_only(args)
     elif args.fl_only:
         run_fl_only(args)
+    elif args.gf2_only:
+        run_gf2_only(args)
     else:
         run_ours(args)
 

@@ -242,9 +242,6 @@ int gf2_gemm_dev(Ctx *c, int kernel, int M, int N, int K, int alpha, const uint6
 //  * U12 = L11^-1 A12 and the M4RM trailing update C ^= L21 U12.
 constexpr int GW = 64;
 constexpr uint8_t GF2_HEAD_NONE = 64;
-constexpr int GF2_WIN = 4096;  // positions staged in shared memory by the search
-constexpr int GF2_SEARCH_THREADS = 256;
-constexpr size_t GF2_SEARCH_SMEM = (size_t)GF2_WIN * 13;
 
 struct Gf2PanelOut {
   uint32_t t, pad0, last_pos, pad;
@@ -256,10 +253,12 @@ __device__ __forceinline__ int gf2_row_at(int pos, const int *p2r, const int *st
 }
 
 constexpr int GF2_HEADS_THREADS = 256;
+// hist counts only the rows from position hist0 on (those the search reads
+// lazily, past its register window).
 __global__ void __launch_bounds__(GF2_HEADS_THREADS)
     gf2_heads_kernel(const uint64_t *__restrict__ D, size_t ld, int i0, int m, int wc,
                      uint64_t pmask, uint8_t *__restrict__ head, uint8_t *__restrict__ act,
-                     int *hist, int *last) {
+                     int *hist, int *last, int hist0) {
   __shared__ int s_last;
   __shared__ int s_hist[GW + 1];
   if (threadIdx.x == 0) s_last = -1;
@@ -271,7 +270,7 @@ __global__ void __launch_bounds__(GF2_HEADS_THREADS)
     const int h = v ? __ffsll((long long)v) - 1 : GF2_HEAD_NONE;
     head[r] = (uint8_t)h;
     act[r] = v != 0ull;
-    atomicAdd(&s_hist[h], 1);
+    if (r >= hist0) atomicAdd(&s_hist[h], 1);
     if (v) my_last = r;
   }
   if (my_last >= 0) atomicMax(&s_last, my_last);
@@ -280,100 +279,152 @@ __global__ void __launch_bounds__(GF2_HEADS_THREADS)
   if (threadIdx.x <= GW && s_hist[threadIdx.x]) atomicAdd(&hist[threadIdx.x], s_hist[threadIdx.x]);
 }
 
-// The CTA stages the words of positions i0 .. i0+GF2_WIN-1 in shared
-// memory; then one warp searches.  The head of a row is a lower bound of the
-// first set bit of its reduced word (exact when set by a bulk scan); cnt[h]
-// counts the non-pivot rows at or below the current row whose bound is h.
-// Outputs: Gf2PanelOut, U (the pivot rows' final words).  Resets *last_act
-// and hist[] for the next panel.
-__global__ void __launch_bounds__(GF2_SEARCH_THREADS)
+// One warp.  The words of positions i0 .. i0 + GF2_WR - 1 (the window) sit
+// in registers, lane l holding positions i0 + l + 32 u, and are eliminated
+// eagerly: when the pivot of column c is chosen, every other window row at
+// or below the current position with bit c set gets the pivot word XOR-ed
+// in, so the pivot of a column is the first window position at or below
+// the current one with the bit set (one ballot per 32 positions), and a
+// pivot row's word is its final U_k (reduced by the pivots before it, as the
+// reference's elimination leaves it).  Rows past the window are tested
+// lazily: the pivot rows are also kept as a reduced basis g_k (bit pcol_j of
+// g_k is delta_kj) with, per column c, the mask M[c] = (1 << c) | sum_k
+// g_k[c] << pcol_k, so bit c of a row reduced by all pivots so far is
+// parity(v & M[c]); head[] holds a lower bound of the first set bit of each
+// such row's reduced word and cnt[h] counts them by that bound, so the scan
+// past the window runs only when a row there may hold the pivot.  Outputs:
+// Gf2PanelOut, U (the pivot rows' final words).  Resets *last_act and
+// hist[] for the next panel.
+constexpr int GF2_WR = 128;               // window positions (registers)
+constexpr int GF2_WU = GF2_WR / 32;       // per lane
+__global__ void __launch_bounds__(32)
     gf2_search_kernel(const uint64_t *__restrict__ D, size_t ld, int i0, int m, int wc, int w,
                       uint64_t pmask, uint8_t *__restrict__ head, const uint8_t *__restrict__ act,
                       int *__restrict__ hist, int *__restrict__ last_act, int *__restrict__ p2r,
                       int *__restrict__ stamp, int epoch, uint64_t *__restrict__ Uout,
                       Gf2PanelOut *out, Gf2PanelOut *hout, volatile uint32_t *hflag,
                       uint32_t seq) {
-  extern __shared__ __align__(16) uint8_t gdyn[];
-  __shared__ uint64_t G[GW], M[GW];
-  __shared__ int s_pcol[GW];
+  __shared__ uint64_t G[GW], M[GW], s_U[GW];
+  __shared__ int s_pcol[GW], s_ti[GW], s_tq[GW];
   __shared__ int s_cnt[GW + 1];
-  uint64_t *sword = reinterpret_cast<uint64_t *>(gdyn);
-  int *srow = reinterpret_cast<int *>(gdyn + (size_t)GF2_WIN * 8);
-  uint8_t *shead = gdyn + (size_t)GF2_WIN * 12;
-  const int nwin = min(GF2_WIN, m - i0);
-  for (int k = threadIdx.x; k < nwin; k += blockDim.x) {
-    cp_async8(&sword[k], D + (size_t)(i0 + k) * ld + wc, true);
-    srow[k] = i0 + k;
-    shead[k] = head[i0 + k];
-  }
-  cp_async_wait_all();
-  __syncthreads();
-  for (int k = threadIdx.x; k < nwin; k += blockDim.x) sword[k] &= pmask;
-  __syncthreads();
-  if (threadIdx.x >= 32) return;
   const int lane = threadIdx.x;
-  auto in_win = [&](int pos) { return pos - i0 < nwin; };
-  auto word_at = [&](int pos) -> uint64_t {
-    return in_win(pos) ? sword[pos - i0]
-                       : D[(size_t)gf2_row_at(pos, p2r, stamp, epoch) * ld + wc] & pmask;
-  };
-  auto head_at = [&](int pos) -> int {
-    return in_win(pos) ? shead[pos - i0] : head[gf2_row_at(pos, p2r, stamp, epoch)];
-  };
-  auto set_head = [&](int pos, int h) {
-    if (in_win(pos))
-      shead[pos - i0] = (uint8_t)h;
-    else
-      head[gf2_row_at(pos, p2r, stamp, epoch)] = (uint8_t)h;
-  };
+  const int wend = min(i0 + GF2_WR, m);  // positions past the window start here
+  // cnt: the rows from wend on (the heads kernel counted only those)
   for (int h = lane; h <= GW; h += 32) {
     s_cnt[h] = hist[h];
     hist[h] = 0;
   }
+  __syncwarp();
+  uint64_t wv[GF2_WU];
+  int wr[GF2_WU];  // row index at the position (-1: past the matrix)
+#pragma unroll
+  for (int u = 0; u < GF2_WU; ++u) {
+    const int pos = i0 + lane + 32 * u;
+    wr[u] = pos < m ? pos : -1;  // no transposition has touched this panel yet
+    wv[u] = pos < m ? D[(size_t)pos * ld + wc] & pmask : 0ull;
+  }
   M[lane] = 1ull << lane;
   M[lane + 32] = 1ull << (lane + 32);
   __syncwarp();
+  auto pick64 = [&](int g) -> uint64_t {
+    uint64_t v = wv[0];
+#pragma unroll
+    for (int u = 1; u < GF2_WU; ++u)
+      if (g == u) v = wv[u];
+    return v;
+  };
+  auto pickr = [&](int g) -> int {
+    int v = wr[0];
+#pragma unroll
+    for (int u = 1; u < GF2_WU; ++u)
+      if (g == u) v = wr[u];
+    return v;
+  };
+  // The basis g_k and masks M: pivot U at column c makes g_k ^= U where g_k
+  // has bit c, and M[c'] ^= M[c] for the columns c' > c where U has a bit.
+  // Only the scan past the window uses them, so they are built when it first
+  // runs (replaying the pivots so far) and kept from then on.
+  auto basis_add = [&](uint64_t U, int c, int k) {
+    const uint64_t mcol = M[c], b = 1ull << c;
+    __syncwarp();
+    if (lane < k && (G[lane] & b)) G[lane] ^= U;
+    if (lane + 32 < k && (G[lane + 32] & b)) G[lane + 32] ^= U;
+    for (int cc = lane; cc < w; cc += 32)
+      if (cc > c && ((U >> cc) & 1ull)) M[cc] ^= mcol;
+    __syncwarp();
+    if (lane == 0) G[k] = U;
+    __syncwarp();
+  };
+  bool basis = false;
   int i = i0, t = 0;
   for (int col = 0; col < w && i < m; ++col) {
-    const uint64_t mc = M[col];
-    int q = -1;
-    {
-      const int pos = i + lane;
-      int nz = 0;
-      if (pos < m) {
-        const int hr = head_at(pos);
-        if (hr <= col) {
-          nz = __popcll(word_at(pos) & mc) & 1;
-          if (!nz) {
-            set_head(pos, col + 1);
-            atomicSub(&s_cnt[hr], 1);
-            atomicAdd(&s_cnt[col + 1], 1);
+    const uint64_t bit = 1ull << col;
+    // first window position at or below i with bit col set
+    int qi = -1;
+#pragma unroll
+    for (int u = 0; u < GF2_WU; ++u) {
+      const int pos = i0 + lane + 32 * u;
+      const unsigned b = __ballot_sync(0xffffffffu, pos >= i && (wv[u] & bit) != 0ull);
+      if (qi < 0 && b) qi = 32 * u + __ffs(b) - 1;
+    }
+    int q;
+    uint64_t U;
+    if (qi >= 0) {
+      q = i0 + qi;
+      U = __shfl_sync(0xffffffffu, pick64(qi >> 5), qi & 31);
+      // eliminate the other window rows at or below i
+#pragma unroll
+      for (int u = 0; u < GF2_WU; ++u) {
+        const int e = lane + 32 * u;
+        if (i0 + e >= i && e != qi && (wv[u] & bit)) wv[u] ^= U;
+      }
+      // transposition (i, q) inside the window: the row at i (bit col clear,
+      // so not changed above) and the pivot row trade places
+      if (q != i) {
+        const int ei = i - i0;
+        const uint64_t vi = __shfl_sync(0xffffffffu, pick64(ei >> 5), ei & 31);
+        const int ri = __shfl_sync(0xffffffffu, pickr(ei >> 5), ei & 31);
+        const int rq = __shfl_sync(0xffffffffu, pickr(qi >> 5), qi & 31);
+#pragma unroll
+        for (int u = 0; u < GF2_WU; ++u) {
+          const int e = lane + 32 * u;
+          if (e == ei) {
+            wv[u] = U;
+            wr[u] = rq;
+          } else if (e == qi) {
+            wv[u] = vi;
+            wr[u] = ri;
           }
         }
       }
-      const unsigned b = __ballot_sync(0xffffffffu, nz);
-      if (b) q = i + __ffs(b) - 1;
-    }
-    __syncwarp();
-    if (q < 0) {
+    } else {
+      // none in the window: rows past it whose bound allows a pivot here
       int cand = 0;
       for (int h = lane; h <= col; h += 32) cand += s_cnt[h];
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) cand += __shfl_xor_sync(0xffffffffu, cand, o);
-      __syncwarp();
-      for (int base = i + 32; base < m && cand > 0; base += 32) {
+      if (cand == 0) continue;  // no pivot in this column
+      if (!basis) {
+        for (int k = 0; k < t; ++k) basis_add(s_U[k], s_pcol[k], k);
+        basis = true;
+      }
+      q = -1;
+      uint64_t v = 0ull;
+      for (int base = wend; base < m && cand > 0; base += 32) {
         const int pos = base + lane;
         int is_cand = 0, hit = 0;
+        uint64_t pv = 0ull;
         if (pos < m) {
-          const int hr = head_at(pos);
+          const int r = gf2_row_at(pos, p2r, stamp, epoch);
+          const int hr = head[r];
           if (hr <= col) {
             is_cand = 1;
-            const uint64_t v = word_at(pos);
+            pv = D[(size_t)r * ld + wc] & pmask;
             int c = col;
-            while (c < w && !(__popcll(v & M[c]) & 1)) ++c;
+            while (c < w && !(__popcll(pv & M[c]) & 1)) ++c;
             const int hn = c < w ? c : GF2_HEAD_NONE;
-            set_head(pos, hn);
             if (hn != hr) {
+              head[r] = (uint8_t)hn;
               atomicSub(&s_cnt[hr], 1);
               atomicAdd(&s_cnt[hn], 1);
             }
@@ -383,63 +434,50 @@ __global__ void __launch_bounds__(GF2_SEARCH_THREADS)
         cand -= __popc(__ballot_sync(0xffffffffu, is_cand));
         const unsigned hb = __ballot_sync(0xffffffffu, hit);
         if (hb) {
-          q = base + __ffs(hb) - 1;
+          const int l = __ffs(hb) - 1;
+          q = base + l;
+          v = __shfl_sync(0xffffffffu, pv, l);
           break;
         }
       }
       __syncwarp();
       if (q < 0) continue;  // no pivot in this column
-    }
-    // the pivot row reduced by the pivots so far: U = v ^ sum_{k: v bit pcol_k} g_k
-    const uint64_t v = word_at(q);
-    uint64_t x = 0;
-    if (lane < t && ((v >> s_pcol[lane]) & 1ull)) x ^= G[lane];
-    if (lane + 32 < t && ((v >> s_pcol[lane + 32]) & 1ull)) x ^= G[lane + 32];
+      // the pivot row reduced by the pivots so far: U = v ^ sum_{k: v bit pcol_k} g_k
+      uint64_t x = 0;
+      if (lane < t && ((v >> s_pcol[lane]) & 1ull)) x ^= G[lane];
+      if (lane + 32 < t && ((v >> s_pcol[lane + 32]) & 1ull)) x ^= G[lane + 32];
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) x ^= __shfl_xor_sync(0xffffffffu, x, o);
-    const uint64_t U = v ^ x;
-    // basis and masks: g_k ^= U where g_k has bit col; M[c] ^= M[col] (which
-    // holds bit col and the pivot columns whose g has bit col) for the
-    // columns c > col where U has a bit
-    __syncwarp();
-    if (lane < t && ((G[lane] >> col) & 1ull)) G[lane] ^= U;
-    if (lane + 32 < t && ((G[lane + 32] >> col) & 1ull)) G[lane + 32] ^= U;
-    for (int c = lane; c < w; c += 32)
-      if (c > col && ((U >> c) & 1ull)) M[c] ^= mc;
-    if (lane == 0) {
-      G[t] = U;
-      s_pcol[t] = col;
-      Uout[t] = U;
-      out->pcol[t] = (uint32_t)col;
-      out->ti[t] = (uint32_t)i;
-      out->tq[t] = (uint32_t)q;
-      atomicSub(&s_cnt[head_at(q)], 1);
-      // transposition (i, q): inside the window the entries swap; a pivot
-      // from beyond it takes slot i and the row it displaces goes to
-      // position q in the global maps (with its head bound)
-      const int ki = i - i0;
-      if (q != i) {
-        if (in_win(q)) {
-          const int kq = q - i0;
-          const uint64_t tw = sword[ki];
-          const int tr = srow[ki];
-          const uint8_t th = shead[ki];
-          sword[ki] = sword[kq];
-          srow[ki] = srow[kq];
-          shead[ki] = shead[kq];
-          sword[kq] = tw;
-          srow[kq] = tr;
-          shead[kq] = th;
-        } else {
-          const int ap = gf2_row_at(q, p2r, stamp, epoch);
-          const int ri = srow[ki];
-          head[ri] = shead[ki];
-          p2r[q] = ri;
-          stamp[q] = epoch;
-          sword[ki] = v;
-          srow[ki] = ap;
-        }
+      for (int o = 16; o > 0; o >>= 1) x ^= __shfl_xor_sync(0xffffffffu, x, o);
+      U = v ^ x;
+      // transposition (i, q): the pivot row takes position i; the window row
+      // there (bit col clear, reduced by every pivot) goes to position q, with
+      // the bound of its reduced word
+      const int ei = i - i0;
+      const uint64_t vi = __shfl_sync(0xffffffffu, pick64(ei >> 5), ei & 31);
+      const int ri = __shfl_sync(0xffffffffu, pickr(ei >> 5), ei & 31);
+      const int ap = gf2_row_at(q, p2r, stamp, epoch);  // before the maps change
+      __syncwarp();
+      if (lane == 0) {
+        const int hv = vi ? __ffsll((long long)vi) - 1 : GF2_HEAD_NONE;
+        atomicSub(&s_cnt[head[ap]], 1);  // the pivot row leaves the counts
+        head[ri] = (uint8_t)hv;
+        atomicAdd(&s_cnt[hv], 1);
+        p2r[q] = ri;
+        stamp[q] = epoch;
       }
+#pragma unroll
+      for (int u = 0; u < GF2_WU; ++u)
+        if (lane + 32 * u == ei) {
+          wv[u] = U;
+          wr[u] = ap;
+        }
+    }
+    if (basis) basis_add(U, col, t);
+    if (lane == 0) {
+      s_U[t] = U;
+      s_pcol[t] = col;
+      s_ti[t] = i;
+      s_tq[t] = q;
     }
     __syncwarp();
     ++i;
@@ -447,12 +485,17 @@ __global__ void __launch_bounds__(GF2_SEARCH_THREADS)
   }
   // last final position of a non-pivot row with a nonzero word
   int hi = i - 1;
-  for (int k = lane; k < t; k += 32) hi = max(hi, (int)out->tq[k]);
+  for (int k = lane; k < t; k += 32) hi = max(hi, s_tq[k]);
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
   int last = -1;
-  for (int pos = i + lane; pos <= hi && pos < m; pos += 32)
-    if (act[in_win(pos) ? srow[pos - i0] : gf2_row_at(pos, p2r, stamp, epoch)]) last = pos;
+#pragma unroll
+  for (int u = 0; u < GF2_WU; ++u) {
+    const int pos = i0 + lane + 32 * u;
+    if (pos >= i && pos <= hi && wr[u] >= 0 && act[wr[u]]) last = max(last, pos);
+  }
+  for (int pos = max(i, wend) + lane; pos <= hi && pos < m; pos += 32)
+    if (act[gf2_row_at(pos, p2r, stamp, epoch)]) last = max(last, pos);
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) last = max(last, __shfl_xor_sync(0xffffffffu, last, o));
   if (lane == 0) {
@@ -464,12 +507,14 @@ __global__ void __launch_bounds__(GF2_SEARCH_THREADS)
     hout->t = (uint32_t)t;
     hout->last_pos = (uint32_t)(last >= 0 ? last : 0);
   }
-  // the result also goes to mapped host memory, then the sequence flag
+  // the outputs; the result also goes to mapped host memory, then the
+  // sequence flag
   __syncwarp();
   for (int k = lane; k < t; k += 32) {
-    hout->ti[k] = out->ti[k];
-    hout->tq[k] = out->tq[k];
-    hout->pcol[k] = out->pcol[k];
+    Uout[k] = s_U[k];
+    out->ti[k] = hout->ti[k] = (uint32_t)s_ti[k];
+    out->tq[k] = hout->tq[k] = (uint32_t)s_tq[k];
+    out->pcol[k] = hout->pcol[k] = (uint32_t)s_pcol[k];
   }
   __threadfence_system();
   __syncwarp();
@@ -614,9 +659,6 @@ int gf2_echelon_dev(Ctx *c, int m, int n, uint64_t *D, size_t ld, size_t *rank_o
   uint64_t *d_Lb = d_U + GW;                 // m x GB words
   uint64_t *d_L11s = d_Lb + (size_t)m * GB;                       // GB x GW words
   const uint32_t *d_pcol = reinterpret_cast<const uint32_t *>(b8 + offsetof(Gf2PanelOut, pcol));
-  if ((st = ctx_smem_attr(c, (const void *)gf2_search_kernel, (int)GF2_SEARCH_SMEM,
-                          "gf2 echelon: search attributes")))
-    return st;
   static_assert(sizeof(Gf2PanelOut) <= PANEL_FLAG_OFF, "panel result and flag share the mapped page");
   void *mh = nullptr, *md = nullptr;
   if ((st = ctx_panel_map(c, &mh, &md))) return st;
@@ -683,12 +725,12 @@ int gf2_echelon_dev(Ctx *c, int m, int n, uint64_t *D, size_t ld, size_t *rank_o
     }
     const uint64_t pmask = (w == 64) ? ~0ull : ((1ull << w) - 1ull);
     int pi = prof_begin(c, "gf2_heads");
-    gf2_heads_kernel<<<head_grid, GF2_HEADS_THREADS, 0, c->stream>>>(D, ld, i, m, wc, pmask,
-                                                                     d_head, d_act, d_hist, d_last);
+    gf2_heads_kernel<<<head_grid, GF2_HEADS_THREADS, 0, c->stream>>>(
+        D, ld, i, m, wc, pmask, d_head, d_act, d_hist, d_last, i + GF2_WR);
     prof_end(c, pi);
     const uint32_t seq = ++c->panel_seq;
     pi = prof_begin(c, "gf2_search");
-    gf2_search_kernel<<<1, GF2_SEARCH_THREADS, GF2_SEARCH_SMEM, c->stream>>>(
+    gf2_search_kernel<<<1, 32, 0, c->stream>>>(
         D, ld, i, m, wc, w, pmask, d_head, d_act, d_hist, d_last, d_p2r, d_stamp, epoch++, d_U,
         d_out, hmap_dev, hflag_dev, seq);
     prof_end(c, pi);
