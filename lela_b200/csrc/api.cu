@@ -487,6 +487,13 @@ int lela_cuda_gemm_gf2(lela_cuda_ctx *h, size_t m, size_t n, size_t k, int a, co
   if (!st && k) st = ctx_stage(c, 1, k * nw * 8, &dB);
   if (!st) st = ctx_stage(c, 2, m * nw * 8, &dC);
   if (!st) st = ctx_clear_status(c);
+  if (!st && gf2_gemm_pipelined(c, (int)m, (int)n, (int)k, a)) {
+    // large tensor-core products: copies overlapped with the product
+    st = gf2_gemm_host_rows(c, (int)m, (int)n, (int)k, A, lda, B, ldb, b, C, ldc,
+                            (uint64_t *)dA, (uint64_t *)dB, (uint64_t *)dC);
+    if (!st) st = ctx_check_status(c, "gemm_gf2");
+    return st;
+  }
   if (!st && k) st = h2d_matrix(c, dA, A, m, kw, lda, 8);
   if (!st && k) st = h2d_matrix(c, dB, B, k, nw, ldb, 8);
   // C is read when b = 1, and for the bits past column n of each row's last

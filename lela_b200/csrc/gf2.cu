@@ -39,13 +39,12 @@
 namespace lela {
 
 // ------------------------------------------------------------------ M4RM
-constexpr int M4_BW = 8;      // words of C per CTA
 constexpr int M4_THREADS = 256;
 constexpr int M4_KC = 32;     // rows of B per table round (4 tables of 8)
 
-// C[r, w0 .. w0+8) for the CTA's rows (M4_ROWS per thread); tables
+// C[r, w0 .. w0+M4_BW) for the CTA's rows (M4_ROWS per thread); tables
 // T[g][w][s] in shared memory.
-template <int M4_ROWS>
+template <int M4_ROWS, int M4_BW>
 __global__ void __launch_bounds__(M4_THREADS)
     gf2_m4rm_kernel(const uint64_t *__restrict__ A, size_t lda, const uint64_t *__restrict__ B,
                     size_t ldb, uint64_t *__restrict__ C, size_t ldc, int M, int Nw, int K,
@@ -120,26 +119,31 @@ int gf2_m4rm_dev(Ctx *c, int M, int N, int K, int alpha, const uint64_t *A, size
   if (M <= 0 || N <= 0) return ST_OK;
   const int Nw = (N + 63) / 64;
   const uint64_t tail = (N & 63) ? ((1ull << (N & 63)) - 1ull) : ~0ull;
-  constexpr int smem = (4 * M4_BW * 256 + M4_KC * M4_BW) * 8;
-  if (int st = ctx_smem_attr(c, (const void *)gf2_m4rm_kernel<4>, smem,
+  // Eight words and four rows per thread per CTA; one row when that leaves
+  // fewer than two CTAs per SM; two words as well when even that does (few
+  // rows, e.g. a panel's 64 pivot rows against a wide B: the tables, which
+  // dominate there, are then built by four times as many CTAs, each a
+  // quarter of them).
+  auto smem_for = [](int bw) { return (4 * bw * 256 + M4_KC * bw) * 8; };
+  if (int st = ctx_smem_attr(c, (const void *)gf2_m4rm_kernel<4, 8>, smem_for(8),
                              "cudaFuncSetAttribute(gf2_m4rm)"))
     return st;
-  if (int st = ctx_smem_attr(c, (const void *)gf2_m4rm_kernel<1>, smem,
+  if (int st = ctx_smem_attr(c, (const void *)gf2_m4rm_kernel<1, 8>, smem_for(8),
                              "cudaFuncSetAttribute(gf2_m4rm)"))
     return st;
-  // four rows per thread; one when that leaves fewer than two CTAs per SM
-  // (narrow C: the tables are then built by more CTAs, but all SMs work)
-  const int gx = (Nw + M4_BW - 1) / M4_BW;
-  const bool wide = (size_t)gx * ((M + M4_THREADS * 4 - 1) / (M4_THREADS * 4)) >= 2u * c->num_sms;
-  const int rows_cta = M4_THREADS * (wide ? 4 : 1);
-  dim3 grid(gx, (M + rows_cta - 1) / rows_cta);
+  const size_t enough = 2u * c->num_sms;
+  const int gx8 = (Nw + 7) / 8, gx2 = (Nw + 1) / 2;
+  const int gy4 = (M + M4_THREADS * 4 - 1) / (M4_THREADS * 4), gy1 = (M + M4_THREADS - 1) / M4_THREADS;
   int pi = prof_begin(c, "gf2_m4rm");
-  if (wide)
-    gf2_m4rm_kernel<4><<<grid, M4_THREADS, smem, c->stream>>>(A, lda, B, ldb, C, ldc, M, Nw, K,
-                                                              tail, alpha, beta);
+  if ((size_t)gx8 * gy4 >= enough)
+    gf2_m4rm_kernel<4, 8><<<dim3(gx8, gy4), M4_THREADS, smem_for(8), c->stream>>>(
+        A, lda, B, ldb, C, ldc, M, Nw, K, tail, alpha, beta);
+  else if ((size_t)gx8 * gy1 >= enough)
+    gf2_m4rm_kernel<1, 8><<<dim3(gx8, gy1), M4_THREADS, smem_for(8), c->stream>>>(
+        A, lda, B, ldb, C, ldc, M, Nw, K, tail, alpha, beta);
   else
-    gf2_m4rm_kernel<1><<<grid, M4_THREADS, smem, c->stream>>>(A, lda, B, ldb, C, ldc, M, Nw, K,
-                                                              tail, alpha, beta);
+    gf2_m4rm_kernel<1, 2><<<dim3(gx2, gy1), M4_THREADS, smem_for(2), c->stream>>>(
+        A, lda, B, ldb, C, ldc, M, Nw, K, tail, alpha, beta);
   prof_end(c, pi);
   ctx_launched(c);
   cudaError_t e = cudaGetLastError();
@@ -219,6 +223,96 @@ int gf2_gemm_dev(Ctx *c, int kernel, int M, int N, int K, int alpha, const uint6
     ctx_launched(c, 2);
     if ((st = gf2_gemm_tc_planes(c, M, N, kc, Ab, Bb, Kp, 1u, b, C, ldc))) return st;
     b = 1;
+  }
+  return ST_OK;
+}
+
+// ---------------------------------------------- host-pointer row blocks
+constexpr int GF2_PIPE_MIN_ROWS = 512;
+
+bool gf2_gemm_pipelined(const Ctx *c, int M, int N, int K, int alpha) {
+  const int kernel = c->gf2_kernel == GF2_AUTO ? GF2_TC : c->gf2_kernel;
+  return kernel == GF2_TC && (alpha & 1) && K > 0 && K <= ZP_KCHUNK && N > 0 &&
+         M >= 2 * GF2_PIPE_MIN_ROWS;
+}
+
+int gf2_gemm_host_rows(Ctx *c, int M, int N, int K, const uint64_t *hA, size_t lda,
+                       const uint64_t *hB, size_t ldb, int beta, uint64_t *hC, size_t ldc,
+                       uint64_t *dA, uint64_t *dB, uint64_t *dC) {
+  if (!gf2_gemm_pipelined(c, M, N, K, 1)) return ctx_fail(c, ST_ARG, "not a pipelined gemm");
+  if (int st = ctx_pipe(c)) return st;
+  const int Kp = (K + 63) & ~63;
+  const int Kw = (K + 63) / 64, Nw = (N + 63) / 64;
+  void *w = nullptr;
+  if (int st = ctx_workspace(c, (size_t)(M + N) * Kp + 256, &w)) return st;
+  uint8_t *Ab = static_cast<uint8_t *>(w), *Bb = Ab + (size_t)M * Kp;
+  // row blocks: a multiple of 128 rows (the tensor-core tile), at most
+  // PIPE_MAX_BLOCKS of them
+  const int per = (M + PIPE_MAX_BLOCKS - 1) / PIPE_MAX_BLOCKS;
+  const int rb = std::max(GF2_PIPE_MIN_ROWS, (per + 127) / 128 * 128);
+  const int nblk = (M + rb - 1) / rb;
+  cudaEvent_t *ready = c->pipe_ev, *done = c->pipe_ev + PIPE_MAX_BLOCKS;
+  cudaEvent_t ev_start = c->pipe_ev[2 * PIPE_MAX_BLOCKS], ev_b = c->pipe_ev[2 * PIPE_MAX_BLOCKS + 1],
+              ev_out = c->pipe_ev[2 * PIPE_MAX_BLOCKS + 2];
+  const size_t rowA = (size_t)Kw * 8, rowB = (size_t)Nw * 8;
+  // C's rows come in when b = 1, and for the bits past column N of each
+  // row's last word, which the product leaves as they were
+  const bool cin = (beta & 1) || (N & 63);
+  cudaError_t e = cudaEventRecord(ev_start, c->stream);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(c->copy_in, ev_start, 0);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(c->copy_out, ev_start, 0);
+  if (e == cudaSuccess)
+    e = cudaMemcpy2DAsync(dB, rowB, hB, ldb * 8, rowB, (size_t)K, cudaMemcpyHostToDevice,
+                          c->copy_in);
+  if (e == cudaSuccess) e = cudaEventRecord(ev_b, c->copy_in);
+  for (int j = 0; e == cudaSuccess && j < nblk; ++j) {
+    const int r0 = j * rb, rows = std::min(rb, M - r0);
+    e = cudaMemcpy2DAsync(dA + (size_t)r0 * Kw, rowA, hA + (size_t)r0 * lda, lda * 8, rowA,
+                          (size_t)rows, cudaMemcpyHostToDevice, c->copy_in);
+    if (e == cudaSuccess && cin)
+      e = cudaMemcpy2DAsync(dC + (size_t)r0 * Nw, rowB, hC + (size_t)r0 * ldc, ldc * 8, rowB,
+                            (size_t)rows, cudaMemcpyHostToDevice, c->copy_in);
+    if (e == cudaSuccess) e = cudaEventRecord(ready[j], c->copy_in);
+  }
+  // B's bytes once; each block's A bytes in its own part of the workspace
+  int st = ST_OK;
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(c->stream, ev_b, 0);
+  if (e == cudaSuccess) {
+    int pi = prof_begin(c, "gf2_unpack");
+    gf2_unpack_cols_kernel<<<dim3(Nw, Kp / 64), 64, 0, c->stream>>>(dB, (size_t)Nw, 0, K, N, Bb, Kp);
+    prof_end(c, pi);
+    ctx_launched(c);
+    e = cudaGetLastError();
+  }
+  for (int j = 0; e == cudaSuccess && !st && j < nblk; ++j) {
+    const int r0 = j * rb, rows = std::min(rb, M - r0);
+    uint8_t *Aj = Ab + (size_t)r0 * Kp;
+    e = cudaStreamWaitEvent(c->stream, ready[j], 0);
+    if (e != cudaSuccess) break;
+    const size_t total = (size_t)rows * ((K + 3) / 4);
+    const int grid = (int)std::min<size_t>((total + 255) / 256, (size_t)c->num_sms * 16);
+    int pi = prof_begin(c, "gf2_unpack");
+    gf2_unpack_rows_kernel<<<grid, 256, 0, c->stream>>>(dA + (size_t)r0 * Kw, (size_t)Kw, rows, 0,
+                                                        K, Aj, Kp);
+    prof_end(c, pi);
+    ctx_launched(c);
+    st = gf2_gemm_tc_planes(c, rows, N, K, Aj, Bb, Kp, 1u, (uint32_t)(beta & 1),
+                            dC + (size_t)r0 * Nw, (size_t)Nw);
+    if (st) break;
+    e = cudaEventRecord(done[j], c->stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(c->copy_out, done[j], 0);
+    if (e == cudaSuccess)
+      e = cudaMemcpy2DAsync(hC + (size_t)r0 * ldc, ldc * 8, dC + (size_t)r0 * Nw, rowB, rowB,
+                            (size_t)rows, cudaMemcpyDeviceToHost, c->copy_out);
+  }
+  // the handle stream ends after the last copy out
+  if (e == cudaSuccess && !st) e = cudaEventRecord(ev_out, c->copy_out);
+  if (e == cudaSuccess && !st) e = cudaStreamWaitEvent(c->stream, ev_out, 0);
+  if (e != cudaSuccess || st) {
+    // copies already queued may still use the caller's buffers
+    cudaStreamSynchronize(c->copy_in);
+    cudaStreamSynchronize(c->copy_out);
+    return st ? st : ctx_cuda(c, e, "pipelined gf2 gemm");
   }
   return ST_OK;
 }
@@ -581,29 +675,29 @@ __global__ void __launch_bounds__(GF2_PERM_THREADS)
   }
 }
 
-// U12 = L11^-1 A12 over GF(2): pivot rows i0..i0+t-1, words from w1; row k
-// gets the XOR of the earlier pivot rows j whose bit is set in L11[k].
-// One thread per word with the t words of the column in registers.
-__global__ void gf2_l11_solve_kernel(uint64_t *__restrict__ D, size_t ld, int i0, int t, int w1,
-                                     int nw, const uint64_t *__restrict__ L11) {
-  __shared__ uint64_t sL[GW];
-  if (threadIdx.x < GW) sL[threadIdx.x] = threadIdx.x < t ? L11[threadIdx.x] : 0ull;
-  __syncthreads();
-  const int w = w1 + blockIdx.x * blockDim.x + threadIdx.x;
-  if (w >= nw) return;
-  uint64_t x[GW];
-#pragma unroll
-  for (int k = 0; k < GW; ++k) x[k] = k < t ? D[(size_t)(i0 + k) * ld + w] : 0ull;
-#pragma unroll
-  for (int k = 1; k < GW; ++k) {
-    const uint64_t lk = sL[k];
-#pragma unroll
-    for (int j = 0; j < k; ++j)
-      if ((lk >> j) & 1ull) x[k] ^= x[j];
+// U12 = L11^-1 A12 over GF(2): pivot rows i0..i0+t-1, words w1 .. nw-1;
+// row k gets the XOR of the earlier pivot rows j whose bit is set in
+// L11[k].  One warp per word, lane l holding rows l and l + 32: step k hands
+// the finished row k to the warp (one shuffle) and the later rows whose
+// L11 row has bit k XOR it in (right-looking, 64 short steps per word
+// instead of a thread's 2016 dependent XORs).
+constexpr int GF2_L11_THREADS = 256;
+__global__ void __launch_bounds__(GF2_L11_THREADS)
+    gf2_l11_solve_kernel(uint64_t *__restrict__ D, size_t ld, int i0, int t, int w1, int nw,
+                         const uint64_t *__restrict__ L11) {
+  const int lane = threadIdx.x & 31;
+  const int w = w1 + (int)((blockIdx.x * (size_t)GF2_L11_THREADS + threadIdx.x) >> 5);
+  if (w >= nw) return;  // whole warps
+  const uint64_t l0 = lane < t ? L11[lane] : 0ull, l1 = lane + 32 < t ? L11[lane + 32] : 0ull;
+  uint64_t x0 = lane < t ? D[(size_t)(i0 + lane) * ld + w] : 0ull;
+  uint64_t x1 = lane + 32 < t ? D[(size_t)(i0 + lane + 32) * ld + w] : 0ull;
+  for (int k = 0; k < t - 1; ++k) {
+    const uint64_t xk = __shfl_sync(0xffffffffu, k < 32 ? x0 : x1, k & 31);
+    if (lane > k && ((l0 >> k) & 1ull)) x0 ^= xk;
+    if ((l1 >> k) & 1ull) x1 ^= xk;  // L11 is strictly lower: bit k set means k < the row
   }
-#pragma unroll
-  for (int k = 0; k < GW; ++k)
-    if (k < t) D[(size_t)(i0 + k) * ld + w] = x[k];
+  if (lane < t) D[(size_t)(i0 + lane) * ld + w] = x0;
+  if (lane + 32 < t) D[(size_t)(i0 + lane + 32) * ld + w] = x1;
 }
 
 // The panel's multipliers into the block's rows of bits: rows i0..r1, the
@@ -700,8 +794,9 @@ int gf2_echelon_dev(Ctx *c, int m, int n, uint64_t *D, size_t ld, size_t *rank_o
                              D + (size_t)pan_i[j] * ld + bw1, ld);
         if (s) return s;
       }
-      gf2_l11_solve_kernel<<<(nw - bw1 + 127) / 128, 128, 0, c->stream>>>(
-          D, ld, pan_i[j], pan_t[j], bw1, nw, d_L11s + (size_t)j * GW);
+      gf2_l11_solve_kernel<<<(nw - bw1 + GF2_L11_THREADS / 32 - 1) / (GF2_L11_THREADS / 32),
+                             GF2_L11_THREADS, 0, c->stream>>>(D, ld, pan_i[j], pan_t[j], bw1, nw,
+                                                              d_L11s + (size_t)j * GW);
       ctx_launched(c);
     }
     const int rb = ib + Tb;
@@ -804,8 +899,8 @@ int gf2_echelon_dev(Ctx *c, int m, int n, uint64_t *D, size_t ld, size_t *rank_o
     // the rest of the block's words (delayed), or of all words
     const int w1 = wc + 1, wend = delayed ? bw1 : nw;
     if (w1 < wend) {
-      gf2_l11_solve_kernel<<<(wend - w1 + 127) / 128, 128, 0, c->stream>>>(D, ld, i, t, w1, wend,
-                                                                            d_L11);
+      gf2_l11_solve_kernel<<<(wend - w1 + GF2_L11_THREADS / 32 - 1) / (GF2_L11_THREADS / 32),
+                             GF2_L11_THREADS, 0, c->stream>>>(D, ld, i, t, w1, wend, d_L11);
       ctx_launched(c);
       if (below > 0) {
         // rows r0..r1, those words: C ^= L21 (one word of t bits per row) * U12

@@ -158,3 +158,32 @@ def test_gf2_gemm_strided_c_keeps_neighbour_bits(cuda, kernel):
                 assert np.array_equal(Wc[:, 2:], W[:, 2:]), (kernel, a, b, dev)
     finally:
         cuda.set_gf2_kernel(0)
+
+
+@pytest.mark.gpu
+def test_gf2_gemm_host_row_blocks(cuda):
+    """The host-pointer GF(2) gemm of a large tensor-core shape works in row
+    blocks with its copies overlapped: ragged blocks (1500 rows), a partial
+    last word of C (700 columns: the bits past column 700 of a row of C are
+    kept), b = 0 and 1, and host rows wider than the matrices (views of
+    larger arrays)."""
+    m, n, k = 1500, 700, 300
+    nw, kw = (n + 63) // 64, (k + 63) // 64
+    A = gen.dense_gf2(141, m, k)
+    B = gen.dense_gf2(142, k, n)
+    for b in (0, 1):
+        W = gen.dense_gf2(143 + b, m, n + 128)  # C = its first nw words
+        C = W[:, :nw]
+        tail = np.uint64((1 << (n % 64)) - 1)
+        C0 = C.copy()
+        C0[:, -1] &= tail
+        want = oracle.gemm_gf2(A, B, C0, k, n, 1, b)
+        before = W.copy()
+        Aw = np.zeros((m, kw + 3), dtype=np.uint64)
+        Aw[:, :kw] = A
+        cuda.gemm_gf2(Aw[:, :kw], B, C, n, k, 1, b)
+        got = W[:, :nw]
+        assert np.array_equal(got[:, :-1], want[:, :-1]), b
+        assert np.array_equal(got[:, -1] & tail, want[:, -1] & tail), b
+        assert np.array_equal(got[:, -1] & ~tail, before[:, nw - 1] & ~tail), b  # bits past n kept
+        assert np.array_equal(W[:, nw:], before[:, nw:]), b
