@@ -997,9 +997,10 @@ void ctx_trim(Ctx *c) {
 // Upper estimate of the device bytes one FL matrix needs on a handle: the
 // dense blocks A, B, C, D (4 m n), the gemm limb planes (at most 4 (m + n) m
 // for the Schur complement), the triangular-solve inverses and echelon
-// bookkeeping (about 2 KB per row), and fixed scratch.
+// bookkeeping (about 5 KB per row: the echelon's block multipliers are 4 KB),
+// and fixed scratch.
 size_t fl_bytes_estimate(size_t m, size_t n) {
-  return 4 * m * n + 4 * (m + n) * m + 2048 * m + ((size_t)256 << 20);
+  return 4 * m * n + 4 * (m + n) * m + 5120 * m + ((size_t)256 << 20);
 }
 
 // The memory-budgeted queue of a batch: an item starts only when its

@@ -44,8 +44,8 @@
 //     tensor-core gemm over the rows down to the last possibly nonzero row,
 //     for the columns of the panel's block of EB columns; the columns right
 //     of the block get one such update per block, with the multipliers of
-//     all its panels (K up to EB = 8 W instead of W: an eighth of the passes
-//     over the trailing matrix).
+//     all its panels (K up to EB = 16 W instead of W: a sixteenth of the
+//     passes over the trailing matrix).
 // F4 Schur complements are staircase-shaped (rows sorted by head), so few
 // rows are touched per panel; dense matrices make every row active and the
 // scheme becomes ordinary blocked LU with LELA's pivot choice.
@@ -64,7 +64,7 @@
 namespace lela {
 
 constexpr int EW = 64;                     // panel width
-constexpr int EB = 8 * EW;                 // block of panels sharing one trailing update
+constexpr int EB = 16 * EW;                // block of panels sharing one trailing update
 constexpr int PS_THREADS = 512;            // panel search CTA
 constexpr int PS_FAST = PS_THREADS / 32;   // positions tested per column by whole warps
 constexpr uint8_t HEAD_NONE = 64;
