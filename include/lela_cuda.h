@@ -86,6 +86,7 @@ int lela_cuda_set_gemm_kernel (lela_cuda_ctx *ctx, int kernel);
  * columns for 1 / 2 / 4 limbs), 2 = variant 1 (128 / 64 columns for 1 / 2
  * limbs with two TMEM accumulator buffers, so the epilogue of one tile
  * overlaps the products of the next; four limbs always use variant 0).
+ * For one limb the number of epilogue warps is chosen by k.
  * Every variant gives the same result.  No counterpart in the reference
  * (a tuning knob of the GPU kernels). */
 int lela_cuda_set_gemm_tile (lela_cuda_ctx *ctx, int tile);

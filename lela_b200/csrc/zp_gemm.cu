@@ -60,35 +60,42 @@ namespace lela {
 // TcCfg<L, T>: tile variant T of the L-limb kernel.  BN = columns of C per
 // tile, NMMA = L * BN (the N of one MMA: the L limbs of B stacked), STAGES
 // = depth of the shared-memory ring, ACC = accumulator buffers in TMEM
-// (each L * NMMA columns; at most 512 in all).  With ACC = 2 the epilogue
-// of one tile overlaps the MMAs of the next; with ACC = 1 the MMAs wait for
-// the epilogue to drain TMEM, but each MMA is wider (more operations per
-// byte of shared memory read).  Variant 1 is the default for one and two
-// limbs (as fast as variant 0 at K = 8192 and faster at the short K of the
-// triangular-solve and elimination updates); the autotuner and the caller
-// can force either.  Four limbs have variant 0 only: with two
-// accumulators a tile would be 16 columns wide, 8 per epilogue thread.
+// (each L * NMMA columns; at most 512 in all), EPI = epilogue warps.  With
+// ACC = 2 the epilogue of one tile overlaps the MMAs of the next; with ACC =
+// 1 the MMAs wait for the epilogue to drain TMEM, but each MMA is wider
+// (more operations per byte of shared memory read).  The caller sees two
+// shapes, wide (one limb: 256 columns; two limbs: 128 columns, one
+// accumulator) and double-buffered (128 / 64 columns, two accumulators).
+// Two limbs use 16 epilogue warps, one limb 16 or 8 chosen by K
+// (zp_gemm_tile_pick): at short K the epilogue is most of a tile's time,
+// and a tcgen05.ld wait covers all of a warp's outstanding TMEM loads, so
+// only more warps hide their latency.  Four limbs have variant 0 only: with two accumulators a
+// tile would be 16 columns wide, 8 per epilogue thread.
 template <int L, int T>
 struct TcCfg;
 template <>
 struct TcCfg<1, 0> {
-  static constexpr int BN = 256, NMMA = 256, STAGES = 4, ACC = 2;
+  static constexpr int BN = 256, NMMA = 256, STAGES = 4, ACC = 2, EPI = 8;
 };
 template <>
 struct TcCfg<1, 1> {
-  static constexpr int BN = 128, NMMA = 128, STAGES = 6, ACC = 2;
+  static constexpr int BN = 128, NMMA = 128, STAGES = 6, ACC = 2, EPI = 16;
+};
+template <>
+struct TcCfg<1, 2> {
+  static constexpr int BN = 128, NMMA = 128, STAGES = 6, ACC = 2, EPI = 8;
 };
 template <>
 struct TcCfg<2, 0> {
-  static constexpr int BN = 128, NMMA = 256, STAGES = 3, ACC = 1;
+  static constexpr int BN = 128, NMMA = 256, STAGES = 3, ACC = 1, EPI = 16;
 };
 template <>
 struct TcCfg<2, 1> {
-  static constexpr int BN = 64, NMMA = 128, STAGES = 4, ACC = 2;
+  static constexpr int BN = 64, NMMA = 128, STAGES = 4, ACC = 2, EPI = 16;
 };
 template <>
 struct TcCfg<4, 0> {
-  static constexpr int BN = 32, NMMA = 128, STAGES = 2, ACC = 1;
+  static constexpr int BN = 32, NMMA = 128, STAGES = 2, ACC = 1, EPI = 8;
 };
 
 constexpr int BM = 128;         // rows of C per tile (UMMA M)
@@ -101,15 +108,21 @@ constexpr int BK = 128;         // bytes (= limb elements) of K per stage
 // 2.42 GB and the kernel took 4 % longer.
 constexpr int GROUP_M = 16;
 constexpr int TMEM_COLS = 512;
-// warp 0: TMA, warp 1: MMA, warps 2-9: epilogue (two per TMEM lane quadrant)
-constexpr int TC_EPI_THREADS = 256;
-constexpr int TC_THREADS = 64 + TC_EPI_THREADS;
+// warp 0: TMA, warp 1: MMA, warps 2 .. 2 + EPI - 1: epilogue (EPI / 4 per
+// TMEM lane quadrant, each on BN / (EPI / 4) columns of a tile)
+template <int L, int T>
+constexpr int tc_threads() {
+  return 64 + 32 * TcCfg<L, T>::EPI;
+}
 
 template <int L, int T>
 struct TcLayout {
   using Cfg = TcCfg<L, T>;
   static_assert(Cfg::NMMA == L * Cfg::BN, "the B operand stacks the L limbs");
   static_assert(Cfg::ACC * L * Cfg::NMMA <= TMEM_COLS, "accumulators exceed TMEM");
+  static_assert(Cfg::EPI % 4 == 0 && Cfg::BN % (Cfg::EPI / 4) == 0 &&
+                    (Cfg::BN / (Cfg::EPI / 4)) % 16 == 0,
+                "whole lane quadrants, 16-column chunks per epilogue warp");
   static constexpr int A_BYTES = L * BM * BK;
   static constexpr int B_BYTES = Cfg::NMMA * BK;
   static constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
@@ -142,6 +155,26 @@ __device__ __forceinline__ void mbar_drain(uint64_t *bar, uint32_t parity, uint3
   }
 }
 
+// Reduction for one and two limbs (p <= 2^16): 32-bit Barrett with mu =
+// floor(2^32 / p), whose quotient estimate for v < 2^32 is the quotient or
+// one less, and c32 = 2^32 mod p for the high word of a two-limb product.
+struct Mod32 {
+  uint32_t p, mu, c32;
+  __device__ __forceinline__ static Mod32 make(uint32_t p) {
+    Mod32 m;
+    m.p = p;
+    m.mu = (uint32_t)((1ull << 32) / p);
+    m.c32 = (uint32_t)((1ull << 32) % p);
+    return m;
+  }
+  // v mod p, up to one multiple of p too large (r < 2p)
+  __device__ __forceinline__ uint32_t lazy(uint32_t v) const { return v - __umulhi(v, mu) * p; }
+  __device__ __forceinline__ uint32_t full(uint32_t v) const {
+    const uint32_t r = lazy(v);
+    return r >= p ? r - p : r;
+  }
+};
+
 // How the product v (reduced) and C combine, chosen once per launch:
 // C <- v + C (alpha = 1, beta = 1: the gemm C += A*B), C <- C - v
 // (alpha = p - 1, beta = 1: the trsm and elimination updates), C <- alpha v
@@ -154,13 +187,27 @@ enum EpiMode : int { EPI_ADD = 0, EPI_SUB = 1, EPI_SET = 2, EPI_AXPBY = 3 };
 // instantiated once per mode and the launch runs one of them, so the hot
 // code holds no per-element branches (the epilogue shares each
 // sub-partition's instruction cache with the TMA and MMA warps).
-template <int MODE>
+// SMALL: p <= 2^16 (one and two limbs), where every product of two
+// residues fits in 32 bits and the 32-bit reduction serves.
+template <int MODE, bool SMALL>
 __device__ __forceinline__ uint32_t epi_combine(uint32_t v, uint32_t c, const Modulus &mod,
-                                                uint32_t alpha, uint32_t beta) {
-  const uint32_t p = (uint32_t)mod.p;
-  if constexpr (MODE == EPI_SET) return alpha == 1u ? v : mod_mul(alpha, v, mod);
-  if constexpr (MODE == EPI_AXPBY) return mod_axpby(alpha, v, beta, c, mod);
-  if (c >= p) c = mod_reduce((uint64_t)c, mod);  // only for a caller's non-canonical C
+                                                const Mod32 &m32, uint32_t alpha,
+                                                uint32_t beta) {
+  const uint32_t p = SMALL ? m32.p : (uint32_t)mod.p;
+  auto mul = [&](uint32_t a, uint32_t b) -> uint32_t {
+    if constexpr (SMALL) return m32.full(a * b);
+    else return mod_mul(a, b, mod);
+  };
+  if constexpr (MODE == EPI_SET) return alpha == 1u ? v : mul(alpha, v);
+  if constexpr (MODE == EPI_AXPBY) {
+    if constexpr (SMALL) {
+      const uint32_t r = mul(alpha, v) + mul(beta, c >= p ? m32.full(c) : c);
+      return r >= p ? r - p : r;
+    } else {
+      return mod_axpby(alpha, v, beta, c, mod);
+    }
+  }
+  if (c >= p) c = SMALL ? m32.full(c) : mod_reduce((uint64_t)c, mod);  // a caller's non-canonical C
   if constexpr (MODE == EPI_ADD) {
     const uint32_t t = p - v;  // v + c mod p without overflow
     return c >= t ? c - t : c + v;
@@ -171,91 +218,79 @@ __device__ __forceinline__ uint32_t epi_combine(uint32_t v, uint32_t c, const Mo
 // The reduced products of 16 consecutive columns of one row, from the
 // TMEM accumulators of a tile (tcol: the column of the first one in the
 // accumulator of A-limb 0, B-limb 0).  Warp-collective: every lane of the
-// warp runs it (tcgen05.ld is .sync.aligned).
+// warp runs it (tcgen05.ld is .sync.aligned).  The limb products P_ij are
+// below 255^2 * 32768 < 2^31 (one K chunk).
 template <int L, int BN, int NMMA>
 __device__ __forceinline__ void chunk_products(uint32_t tcol, uint32_t (&v)[16],
-                                               const Modulus &mod);
-
-// L = 1: one product, P_00 < 2^31.
-template <>
-__device__ __forceinline__ void chunk_products<1, 256, 256>(uint32_t tcol, uint32_t (&v)[16],
-                                                            const Modulus &mod) {
-  uint32_t r[16];
-  tmem_ld16(tcol, r);
-  tmem_ld_wait();
+                                               const Modulus &mod, const Mod32 &m32) {
+  if constexpr (L == 1) {
+    // one product P_00
+    uint32_t r[16];
+    tmem_ld16(tcol, r);
+    tmem_ld_wait();
 #pragma unroll
-  for (int i = 0; i < 16; ++i) v[i] = mod_reduce((uint64_t)r[i], mod);
-}
-template <>
-__device__ __forceinline__ void chunk_products<1, 128, 128>(uint32_t tcol, uint32_t (&v)[16],
-                                                            const Modulus &mod) {
-  chunk_products<1, 256, 256>(tcol, v, mod);
-}
-
-// L = 2: A*B = 2^16 P_11 + 2^8 (P_01 + P_10) + P_00 < 2^48.
-template <int BN, int NMMA>
-__device__ __forceinline__ void chunk_products2(uint32_t tcol, uint32_t (&v)[16],
-                                                const Modulus &mod) {
-  uint32_t p00[16], p01[16], p10[16], p11[16];
-  tmem_ld16(tcol, p00);
-  tmem_ld16(tcol + BN, p01);
-  tmem_ld16(tcol + NMMA, p10);
-  tmem_ld16(tcol + NMMA + BN, p11);
-  tmem_ld_wait();
+    for (int i = 0; i < 16; ++i) v[i] = m32.full(r[i]);
+  } else if constexpr (L == 2) {
+    // x = 2^16 P_11 + 2^8 (P_01 + P_10) + P_00 < 2^48, as hi 2^32 + lo:
+    // x = lo + hi c32 (mod p), and (lo mod p, < 2p) + hi c32 < 2^32 for
+    // p <= 2^16 (p = 2^16 has c32 = 0)
+    uint32_t p00[16], p01[16], p10[16], p11[16];
+    tmem_ld16(tcol, p00);
+    tmem_ld16(tcol + BN, p01);
+    tmem_ld16(tcol + NMMA, p10);
+    tmem_ld16(tcol + NMMA + BN, p11);
+    tmem_ld_wait();
 #pragma unroll
-  for (int i = 0; i < 16; ++i) {
-    const uint64_t x = ((uint64_t)p11[i] << 16) + (((uint64_t)p01[i] + p10[i]) << 8) + p00[i];
-    v[i] = mod_reduce(x, mod);
-  }
-}
-template <>
-__device__ __forceinline__ void chunk_products<2, 128, 256>(uint32_t tcol, uint32_t (&v)[16],
-                                                            const Modulus &mod) {
-  chunk_products2<128, 256>(tcol, v, mod);
-}
-template <>
-__device__ __forceinline__ void chunk_products<2, 64, 128>(uint32_t tcol, uint32_t (&v)[16],
-                                                           const Modulus &mod) {
-  chunk_products2<64, 128>(tcol, v, mod);
-}
-
-// L = 4: D_s = sum_{i+j=s} P_ij < 2^33, Horner in s with a reduction per
-// step ((r < 2^32) * 2^8 + D_s < 2^41).  Eight columns at a time to keep the
-// seven 64-bit partial sums in registers.
-template <int BN, int NMMA>
-__device__ __forceinline__ void chunk_products4(uint32_t tcol, uint32_t (&v)[16],
-                                                const Modulus &mod) {
+    for (int i = 0; i < 16; ++i) {
+      const uint64_t x = ((uint64_t)p11[i] << 16) + ((uint64_t)(p01[i] + p10[i]) << 8) + p00[i];
+      const uint32_t t = m32.lazy((uint32_t)x) + (uint32_t)(x >> 32) * m32.c32;
+      v[i] = m32.full(t);
+    }
+  } else {
+    // L = 4: x = sum_s 2^(8s) D_s with D_s = sum_{i+j=s} P_ij, gathered as
+    // x = F_a + 2^24 F_b + 2^48 D_6 (F_a = D_0 + 2^8 D_1 + 2^16 D_2 < 2^49,
+    // F_b likewise from D_3..D_5, D_6 = P_33 < 2^31), then three steps of
+    // Horner in 2^24 with one reduction each ((r < 2^32) 2^24 + F < 2^57).
+    // Eight columns at a time; the sixteen limb products in two waits.
 #pragma unroll
-  for (int h = 0; h < 16; h += 8) {
-    uint64_t D[7][8];
+    for (int h = 0; h < 16; h += 8) {
+      uint64_t Fa[8], Fb[8];
+      uint32_t D6[8];
 #pragma unroll
-    for (int s = 0; s < 7; ++s)
+      for (int i = 0; i < 8; ++i) {
+        Fa[i] = 0;
+        Fb[i] = 0;
+      }
 #pragma unroll
-      for (int i = 0; i < 8; ++i) D[s][i] = 0;
+      for (int half = 0; half < 2; ++half) {
+        uint32_t r[2][4][8];
 #pragma unroll
-    for (int li = 0; li < 4; ++li) {
+        for (int a = 0; a < 2; ++a)
 #pragma unroll
-      for (int lj = 0; lj < 4; ++lj) {
-        uint32_t r[8];
-        tmem_ld8(tcol + h + li * NMMA + lj * BN, r);
+          for (int lj = 0; lj < 4; ++lj)
+            tmem_ld8(tcol + h + (2 * half + a) * NMMA + lj * BN, r[a][lj]);
         tmem_ld_wait();
 #pragma unroll
-        for (int i = 0; i < 8; ++i) D[li + lj][i] += r[i];
+        for (int a = 0; a < 2; ++a)
+#pragma unroll
+          for (int lj = 0; lj < 4; ++lj) {
+            const int sd = 2 * half + a + lj;  // the digit of this limb product
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+              if (sd == 6) D6[i] = r[a][lj][i];
+              else if (sd < 3) Fa[i] += (uint64_t)r[a][lj][i] << (8 * sd);
+              else Fb[i] += (uint64_t)r[a][lj][i] << (8 * (sd - 3));
+            }
+          }
+      }
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        uint32_t acc = mod_reduce((uint64_t)D6[i], mod);
+        acc = mod_reduce(((uint64_t)acc << 24) + Fb[i], mod);
+        v[h + i] = mod_reduce(((uint64_t)acc << 24) + Fa[i], mod);
       }
     }
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      uint32_t acc = mod_reduce(D[6][i], mod);
-#pragma unroll
-      for (int s = 5; s >= 0; --s) acc = mod_reduce(((uint64_t)acc << 8) + D[s][i], mod);
-      v[h + i] = acc;
-    }
   }
-}
-template <>
-__device__ __forceinline__ void chunk_products<4, 32, 128>(uint32_t tcol, uint32_t (&v)[16],
-                                                           const Modulus &mod) {
-  chunk_products4<32, 128>(tcol, v, mod);
 }
 
 // C row segments in registers.  load_c reads n consecutive entries of row
@@ -377,7 +412,8 @@ __device__ __forceinline__ void tile_kblocks(const int2 *__restrict__ kr, int kb
 
 // Epilogue of the Z/p product for one thread (TMEM lane `row` of quadrant
 // q, columns cbeg.. of each tile) over this CTA's tiles.  This thread's row
-// segment of a tile: W = BN / 2 columns from gn0, in blocks of EPB columns.
+// segment of a tile: W = BN / (EPI / 4) columns from gn0, in blocks of EPB
+// columns.
 // C's block 0 is loaded before the accumulator is ready (its latency hides
 // behind the tile's MMAs), block b + 1 while block b is combined; TMEM is
 // released after its last read, before the last block's stores.
@@ -389,10 +425,11 @@ __device__ __noinline__ void epilogue_tiles(uint32_t tmem, uint64_t *tfull, uint
                                                int row, int q, int cbeg) {
   using Cfg = TcCfg<L, T>;
   constexpr int ACC = Cfg::ACC, BN = Cfg::BN, NMMA = Cfg::NMMA;
-  constexpr int W = BN / 2;
+  constexpr int W = BN / (Cfg::EPI / 4);
   constexpr int EPB = W < 32 ? W : 32;
   constexpr int NB = W / EPB;
   constexpr bool READC = MODE != EPI_SET;
+  const Mod32 m32 = Mod32::make(L < 4 ? (uint32_t)mod.p : 3u);
   const bool vec = ((reinterpret_cast<uintptr_t>(C) & 15u) == 0) && ((ldc & 3u) == 0);
   int it = 0;
   for (int t = blockIdx.x; t < num_tiles; t += gridDim.x, ++it) {
@@ -415,10 +452,11 @@ __device__ __noinline__ void epilogue_tiles(uint32_t tmem, uint64_t *tfull, uint
 #pragma unroll
       for (int h = 0; h < EPB / 16; ++h) {
         uint32_t v[16];
-        chunk_products<L, BN, NMMA>(tbase + (uint32_t)(cbeg + b * EPB + 16 * h), v, mod);
+        chunk_products<L, BN, NMMA>(tbase + (uint32_t)(cbeg + b * EPB + 16 * h), v, mod, m32);
 #pragma unroll
         for (int i = 0; i < 16; ++i)
-          cur[16 * h + i] = epi_combine<MODE>(v[i], READC ? cur[16 * h + i] : 0u, mod, alpha, beta);
+          cur[16 * h + i] =
+              epi_combine<MODE, (L < 4)>(v[i], READC ? cur[16 * h + i] : 0u, mod, m32, alpha, beta);
       }
       if (b == NB - 1) {
         tc_fence_before();
@@ -430,7 +468,7 @@ __device__ __noinline__ void epilogue_tiles(uint32_t tmem, uint64_t *tfull, uint
 }
 
 template <int L, int OUT, int T = 0>
-__global__ void __launch_bounds__(TC_THREADS, 1)
+__global__ void __launch_bounds__(tc_threads<L, T>(), 1)
     zp_gemm_tc_kernel(const __grid_constant__ CUtensorMap tmA,
                       const __grid_constant__ CUtensorMap tmB, void *__restrict__ Cv,
                       size_t ldc, int M, int N, int K, Modulus mod, uint32_t alpha, uint32_t beta,
@@ -463,7 +501,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     }
     for (int a = 0; a < ACC; ++a) {
       mbar_init(&tfull[a], 1);
-      mbar_init(&tempty[a], TC_EPI_THREADS);
+      mbar_init(&tempty[a], 32 * Cfg::EPI);
     }
     mbar_init(done, 1);
     fence_barrier_init();
@@ -556,11 +594,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     }
   } else {
     // ------------------------------------------------------------ epilogue
-    // warps 2..9: two warps per TMEM lane quadrant, each on half the columns
+    // EPI / 4 warps per TMEM lane quadrant, each on a BN / (EPI / 4) column
+    // part of every tile
     const int q = warp & 3;  // TMEM lane quadrant this warp may access
     const int row = q * 32 + lane;
-    const int half = (warp - 2) >> 2;
-    const int cbeg = half * (BN / 2);
+    const int part = (warp - 2) >> 2;
+    const int cbeg = part * (BN / (Cfg::EPI / 4));
     if constexpr (OUT == 0) {
       const int emode = beta == 0u ? EPI_SET
                         : (beta == 1u && alpha == 1u) ? EPI_ADD
@@ -588,7 +627,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         if (!mbar_wait(&tfull[a], aph, err)) break;
         tc_fence_after();
         epilogue_gf2(tbase, gm, nb * BN, M, N, static_cast<uint64_t *>(Cv), ldc, alpha, beta,
-                     cbeg, cbeg + BN / 2);
+                     cbeg, cbeg + BN / (Cfg::EPI / 4));
         tc_fence_before();
         mbar_arrive(&tempty[a]);
       }
@@ -875,7 +914,7 @@ static int launch_tc(Ctx *c, int M, int N, int K, const Modulus &mod, uint32_t a
     if (st) return st;
     const int grid = std::min(tiles, c->num_sms);
     int pi = prof_begin(c, "zp_gemm_tc");
-    zp_gemm_tc_kernel<L, 0, T><<<grid, TC_THREADS, Lay::SMEM, c->stream>>>(
+    zp_gemm_tc_kernel<L, 0, T><<<grid, tc_threads<L, T>(), Lay::SMEM, c->stream>>>(
         tmA, tmB, C, ldc, M, N, kc, mod, alpha, b, c->dstatus, kr, kbase + k0);
     prof_end(c, pi);
     ctx_launched(c);
@@ -896,14 +935,17 @@ size_t zp_gemm_workspace_bytes(uint32_t p, int M, int N, int K) {
 int zp_gemm_tile_pick(const Ctx *c, int K, uint32_t p) {
   const int L = zp_limbs_for(p);
   if (L == 4) return 0;  // one variant for four limbs
-  if (c->gemm_tile == GEMM_TILE_WIDE) return 0;
-  if (c->gemm_tile == GEMM_TILE_DOUBLE) return 1;
-  // Measured on the B200 (kernel ms, epilogue instantiated per combine
-  // mode): two limbs, variant 0 / variant 1: 1.411 / 1.690 at 8192^3,
-  // 0.0906 / 0.0901 at 4096 x 4096 x 256, 0.231 / 0.223 at 5000 x 9000 x 64;
-  // one limb, 0.131 / 0.082 at 4096 x 4096 x 256.
-  if (L == 2) return K >= 512 ? 0 : 1;
-  return 1;
+  // Measured on the B200 (kernel ms, M = N = 8192, p = 65521 / 251, the
+  // 32-bit reductions of the epilogue): two limbs, wide tiles with 8 / 16
+  // epilogue warps: 1.346 / 1.338 at K = 8192 (with the earlier 64-bit
+  // reduction 8 / 16 warps took 0.351 / 0.318 at K = 512 and 0.543 / 0.496
+  // at 2048).  One limb, double-buffered tiles with 8 / 16 warps: 0.256 /
+  // 0.256 at K = 2048, 0.284 / 0.322 at 3072, 0.596 / 0.642 at 8192 (0.316
+  // / 0.249 at 512 with the earlier reduction).
+  const bool wide = c->gemm_tile == GEMM_TILE_WIDE ||
+                    (c->gemm_tile == GEMM_TILE_AUTO && L == 2 && K >= 512);
+  if (L == 2) return wide ? 0 : 1;
+  return wide ? 0 : (K <= 2048 ? 1 : 2);
 }
 
 int zp_gemm_pick(const Ctx *c, int M, int N, int K, uint32_t p) {
@@ -973,14 +1015,14 @@ int zp_gemm_dev(Ctx *c, int kernel, int M, int N, int K, uint32_t p, uint32_t al
     if (st) return st;
     ws = static_cast<uint8_t *>(w);
   }
-  const bool t1 = zp_gemm_tile_pick(c, K, p) == 1;
+  const int tv = zp_gemm_tile_pick(c, K, p);
+#define LELA_TC(L, T) launch_tc<L, T>(c, M, N, K, mod, alpha, A, lda, B, ldb, beta, C, ldc, ws, kr, kbase)
   switch (zp_limbs_for(p)) {
     case 1:
-      return t1 ? launch_tc<1, 1>(c, M, N, K, mod, alpha, A, lda, B, ldb, beta, C, ldc, ws, kr, kbase)
-                : launch_tc<1, 0>(c, M, N, K, mod, alpha, A, lda, B, ldb, beta, C, ldc, ws, kr, kbase);
+      return tv == 0 ? LELA_TC(1, 0) : tv == 1 ? LELA_TC(1, 1) : LELA_TC(1, 2);
     case 2:
-      return t1 ? launch_tc<2, 1>(c, M, N, K, mod, alpha, A, lda, B, ldb, beta, C, ldc, ws, kr, kbase)
-                : launch_tc<2, 0>(c, M, N, K, mod, alpha, A, lda, B, ldb, beta, C, ldc, ws, kr, kbase);
+      return tv == 0 ? LELA_TC(2, 0) : LELA_TC(2, 1);
+#undef LELA_TC
     default:
       return launch_tc<4, 0>(c, M, N, K, mod, alpha, A, lda, B, ldb, beta, C, ldc, ws, kr, kbase);
   }
@@ -1072,7 +1114,7 @@ static int host_rows(Ctx *c, int M, int N, int K, const Modulus &mod, uint32_t a
     if (st) break;
     const int tiles = ((rows + BM - 1) / BM) * ((N + Cfg::BN - 1) / Cfg::BN);
     pi = prof_begin(c, "zp_gemm_tc");
-    zp_gemm_tc_kernel<L, 0><<<std::min(tiles, c->num_sms), TC_THREADS, Lay::SMEM, c->stream>>>(
+    zp_gemm_tc_kernel<L, 0><<<std::min(tiles, c->num_sms), tc_threads<L, 0>(), Lay::SMEM, c->stream>>>(
         tmA, tmB, dC + (size_t)r0 * N, (size_t)N, rows, N, K, mod, alpha, beta, c->dstatus);
     prof_end(c, pi);
     ctx_launched(c, 2);
@@ -1244,7 +1286,7 @@ int noalloc_launch(cudaStream_t s, const NoallocDevice &d, int M, int N, int K,
         !noalloc_map(&tmB, Bl, (uint64_t)kc, (uint64_t)N, L, (uint64_t)Kp, (uint64_t)N * Kp,
                      BK, Cfg::BN, L))
       return ST_CUDA;
-    zp_gemm_tc_kernel<L, 0><<<std::min(tiles, d.num_sms), TC_THREADS, Lay::SMEM, s>>>(
+    zp_gemm_tc_kernel<L, 0><<<std::min(tiles, d.num_sms), tc_threads<L, 0>(), Lay::SMEM, s>>>(
         tmA, tmB, C, ldc, M, N, kc, mod, alpha, b, err);
     b = 1;
   }
@@ -1324,7 +1366,7 @@ int gf2_gemm_tc_planes(Ctx *c, int M, int N, int K, const uint8_t *Ab, const uin
   if (st) return st;
   const int tiles = ((M + BM - 1) / BM) * ((N + Cfg::BN - 1) / Cfg::BN);
   int pi = prof_begin(c, "gf2_gemm_tc");
-  zp_gemm_tc_kernel<1, 1><<<std::min(tiles, c->num_sms), TC_THREADS, Lay::SMEM, c->stream>>>(
+  zp_gemm_tc_kernel<1, 1><<<std::min(tiles, c->num_sms), tc_threads<1, 0>(), Lay::SMEM, c->stream>>>(
       tmA, tmB, C, ldc_words, M, N, K, make_modulus(2), alpha, beta, c->dstatus);
   prof_end(c, pi);
   ctx_launched(c);

@@ -32,8 +32,11 @@ int zp_gemm_dev(Ctx *c, int kernel, int M, int N, int K, uint32_t p, uint32_t al
 // The kernel GEMM_AUTO resolves to for this shape (the handle's forced
 // kernel, else the small-K crossover rule).
 int zp_gemm_pick(const Ctx *c, int M, int N, int K, uint32_t p);
-// The tensor-core tile variant (0 or 1) for this K and modulus: the
-// handle's forced variant, else variant 1 for one and two limbs.
+// The tensor-core tile variant (TcCfg<L, T>'s T: 0, 1, or 2 for one limb)
+// for this K and modulus: the handle's forced shape (wide or
+// double-buffered), else wide for two limbs at K >= 512 and four limbs,
+// double-buffered otherwise; for one limb the number of epilogue warps
+// follows K.
 int zp_gemm_tile_pick(const Ctx *c, int K, uint32_t p);
 
 // Whether the host-pointer gemm of this shape is done in row blocks with
