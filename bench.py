@@ -44,8 +44,8 @@ METRIC = "Z/p gemm Gop/s at 8192^3 (Modular<uint32>, p=65521), bit-exact"
 # DRAM bytes of one launch of the tensor-core gemm at 8192^3, p = 65521 (two
 # limbs, wide tiles), from an ncu capture of
 # `python bench.py --gemm-only 8192,8192,8192 --steps 3 --warmup 2`:
-# dram__bytes_read.sum 1205.2 MB + dram__bytes_write.sum 256.1 MB.
-TC_TRAFFIC_8192 = 1205210000 + 256114944
+# dram__bytes_read.sum 1315.0 MB + dram__bytes_write.sum 261.4 MB.
+TC_TRAFFIC_8192 = 1315042304 + 261354496
 P = 65521
 N = 8192
 
@@ -913,7 +913,7 @@ def run_ours(args):
                 "traffic": TC_TRAFFIC_8192 if n == 8192 else None,
                 "traffic_unit": "bytes per launch",
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch of this "
-                                  "kernel at 8192^3 (one pass, --clock-control none), 1205 + 256 MB; "
+                                  "kernel at 8192^3 (one pass, --clock-control none), 1315 + 261 MB; "
                                   "algorithmic bytes 805 MB (limb planes 268 MB, C read and written)",
                 "ops_per_launch": "4 limb products x 2*8192^3 int8 multiply-adds = %.3e" % (L * L * 2.0 * n ** 3),
                 "kernel_ms_avg": round(tc_avg, 4), "split_ms_avg": round(sp_ms / max(sp_n, 1), 4),
