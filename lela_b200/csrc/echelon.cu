@@ -72,7 +72,7 @@ constexpr uint8_t HEAD_NONE = 64;
 struct PanelOut {
   uint32_t t;         // pivots found in the panel
   uint32_t err;       // 1: a pivot is not invertible in Modular<uint32>
-  uint32_t pad0;
+  uint32_t uinv;      // 1: U_P^-1 written (the rows to solve take panel_solve_inv_kernel)
   uint32_t last_pos;  // largest final position of a non-pivot row with a nonzero panel (or 0)
   uint32_t det;       // product of the panel's pivots
   uint32_t pad[3];
@@ -138,6 +138,16 @@ struct ArithSmall {
     const uint32_t r = red(a * b) + red(c * d);
     return r >= p ? r - p : r;
   }
+  // s += a*b for a sum of products reduced once at the end (red64): each
+  // product is below 2^32, so up to 2^16 of them fit
+  __device__ __forceinline__ void acc(uint64_t &s, uint32_t a, uint32_t b) const {
+    s += (uint64_t)a * b;
+  }
+  // s mod p for s < 2^48: (s mod 2^32 reduced) + (s / 2^32) (2^32 mod p)
+  __device__ __forceinline__ uint32_t red64(uint64_t s) const {
+    const uint32_t c32 = 0u - mu * p;
+    return red(red((uint32_t)s) + (uint32_t)(s >> 32) * c32);
+  }
 };
 struct ArithWide {
   Modulus mod;
@@ -155,7 +165,72 @@ struct ArithWide {
   __device__ __forceinline__ uint32_t dot2(uint32_t a, uint32_t b, uint32_t c, uint32_t d) const {
     return mod_dot2(a, b, c, d, mod, two64);
   }
+  // s += a*b modulo p: on a wrap past 2^64 the lost 2^64 comes back as
+  // 2^64 mod p (the sum then stays below 2^64: it is below the product)
+  __device__ __forceinline__ void acc(uint64_t &s, uint32_t a, uint32_t b) const {
+    const uint64_t x = (uint64_t)a * b;
+    s += x;
+    if (s < x) s += two64;
+  }
+  __device__ __forceinline__ uint32_t red64(uint64_t s) const { return mod_reduce(s, mod); }
 };
+
+// Inverse of a 64 x 64 triangular matrix X (row stride LD, shared memory)
+// in place by doubling: the inverse of [[A, B], [0, C]] is [[A^-1, -A^-1 B
+// C^-1], [0, C^-1]] (lower: [[A^-1, 0], [-C^-1 B A^-1, C^-1]]), so the
+// diagonal blocks of sizes 1, 2, 4, .., 32 are inverted level by level,
+// each level two products of b x b blocks (through T, 32 b entries) over
+// all pairs at once.  On entry the diagonal holds the inverses of the
+// diagonal entries and the rest of the triangle the matrix's entries, the
+// other triangle zero (the products run over whole blocks, zeros included).
+// Every thread of the CTA calls it (12 barriers).  A
+// triangular matrix with unit diagonal entries has one inverse over Z/p,
+// so the result is the one any substitution gives.
+template <class A, bool UPPER, int LD, int B>
+__device__ __forceinline__ void tri64_invert_level(uint32_t (*X)[LD], uint32_t *T, const A &ar,
+                                                   int tid, int nthreads) {
+  // products over whole b x b blocks (the zero triangle included): fixed
+  // trip counts, unrolled
+  constexpr int n = (EW / (2 * B)) * B * B;
+  const uint32_t p = ar.p;
+  for (int e = tid; e < n; e += nthreads) {
+    const int q = e / (B * B), ii = (e / B) % B, jj = e % B, r = 2 * B * q;
+    uint64_t acc = 0;
+#pragma unroll
+    for (int kk = 0; kk < B; ++kk) {
+      if constexpr (UPPER) ar.acc(acc, X[r + ii][r + B + kk], X[r + B + kk][r + B + jj]);  // B C^-1
+      else ar.acc(acc, X[r + B + ii][r + kk], X[r + kk][r + jj]);                          // B A^-1
+    }
+    T[e] = ar.red64(acc);
+  }
+  __syncthreads();
+  for (int e = tid; e < n; e += nthreads) {
+    const int q = e / (B * B), ii = (e / B) % B, jj = e % B, r = 2 * B * q;
+    const uint32_t *Tq = T + q * B * B;
+    uint64_t acc = 0;
+#pragma unroll
+    for (int kk = 0; kk < B; ++kk) {
+      if constexpr (UPPER) ar.acc(acc, X[r + ii][r + kk], Tq[kk * B + jj]);  // -A^-1 (B C^-1)
+      else ar.acc(acc, X[r + B + ii][r + B + kk], Tq[kk * B + jj]);         // -C^-1 (B A^-1)
+    }
+    const uint32_t v = ar.red64(acc);
+    if constexpr (UPPER) X[r + ii][r + B + jj] = v ? p - v : 0u;
+    else X[r + B + ii][r + jj] = v ? p - v : 0u;
+  }
+  __syncthreads();
+}
+
+template <class A, bool UPPER, int LD>
+__device__ void tri64_invert(uint32_t (*X)[LD], uint32_t *T, const A &ar, int tid,
+                             int nthreads) {
+  static_assert(EW == 64, "six levels");
+  tri64_invert_level<A, UPPER, LD, 1>(X, T, ar, tid, nthreads);
+  tri64_invert_level<A, UPPER, LD, 2>(X, T, ar, tid, nthreads);
+  tri64_invert_level<A, UPPER, LD, 4>(X, T, ar, tid, nthreads);
+  tri64_invert_level<A, UPPER, LD, 8>(X, T, ar, tid, nthreads);
+  tri64_invert_level<A, UPPER, LD, 16>(X, T, ar, tid, nthreads);
+  tri64_invert_level<A, UPPER, LD, 32>(X, T, ar, tid, nthreads);
+}
 
 // 1. First nonzero column of each row's panel part, rows i0..m-1 (one warp
 // per row); the histogram of these heads (hist[0..64], which the caller
@@ -224,6 +299,8 @@ constexpr int PW_R = 80;                   // window rows
 constexpr int PW_LD = EW + 1;
 constexpr size_t PW_SMEM = (size_t)PW_R * PW_LD * 4;  // dynamic shared memory: the window rows
 constexpr int PW_EU = (PW_R + 31) / 32;  // window list entries per lane
+// rows to solve from which the panel's multipliers come from U_P^-1
+constexpr int SOLVE_INV_ROWS = 768;
 
 template <class A>
 __global__ void __launch_bounds__(PS_THREADS, 1)
@@ -231,8 +308,9 @@ __global__ void __launch_bounds__(PS_THREADS, 1)
                         A ar, uint8_t *__restrict__ head, const uint8_t *__restrict__ act,
                         int *__restrict__ hist, int *__restrict__ last_act, int *__restrict__ p2r,
                         int *__restrict__ stamp, int epoch, uint32_t *__restrict__ Uout,
-                        uint32_t *__restrict__ xinv_out, PanelOut *out,
-                        PanelOut *hout, volatile uint32_t *hflag, uint32_t seq, int wcap) {
+                        uint32_t *__restrict__ xinv_out, uint32_t *__restrict__ Uinv_out,
+                        PanelOut *out, PanelOut *hout, volatile uint32_t *hflag, uint32_t seq,
+                        int wcap) {
   extern __shared__ __align__(16) uint32_t dyn_w[];
   uint32_t(*Wv)[PW_LD] = reinterpret_cast<uint32_t(*)[PW_LD]>(dyn_w);  // PW_R rows
   __shared__ uint32_t PV[EW][EW];
@@ -240,11 +318,11 @@ __global__ void __launch_bounds__(PS_THREADS, 1)
   __shared__ int wrow[PW_R];
   __shared__ uint32_t s_red[PS_FAST][EW];  // rows past the window, reduced (one per warp)
   __shared__ int s_pcol[EW];
-  __shared__ uint32_t s_y[EW], s_S[EW], s_x[EW], s_sinv[EW], s_yinv[EW];
+  __shared__ uint32_t s_y[EW], s_S[EW], s_x[EW], s_sinv[EW], s_yinv[EW], s_xi[EW];
   __shared__ int s_cnt[EW + 1];
   __shared__ int s_first[PS_FAST], s_wcnt[PS_FAST];
   __shared__ int s_list[PS_THREADS], s_lrow[PS_THREADS], s_lhead[PS_THREADS];
-  __shared__ int s_err, s_last, s_hi, s_wlast;
+  __shared__ int s_err, s_last, s_hi, s_wlast, s_uinv;
   const uint32_t p = ar.p;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
 
@@ -537,6 +615,7 @@ __global__ void __launch_bounds__(PS_THREADS, 1)
     const uint32_t x = ar.mul(s_y[tid], si);
     const uint32_t xi = exact_inv ? ar.mul(s_S[tid], s_yinv[tid]) : lela_inv_u32(p, x);
     s_x[tid] = x;
+    s_xi[tid] = xi;
     xinv_out[tid] = xi;
     if (si == 0u || xi == 0u) atomicOr(&s_err, 1);
   }
@@ -569,6 +648,10 @@ __global__ void __launch_bounds__(PS_THREADS, 1)
     const int la = *last_act;
     int last = s_last;
     if (la > hi) last = max(last, la);
+    // the rows the panel's solve takes: i0 .. max(last, i0 + t - 1)
+    const int rows = max(last, i0 + t - 1) - i0 + 1;
+    s_uinv = exact_inv && t > 0 && rows >= SOLVE_INV_ROWS;
+    out->uinv = hout->uinv = (uint32_t)s_uinv;
     out->t = (uint32_t)t;
     out->err = (uint32_t)s_err;
     out->last_pos = (uint32_t)(last >= 0 ? last : 0);
@@ -590,6 +673,31 @@ __global__ void __launch_bounds__(PS_THREADS, 1)
   __threadfence_system();
   __syncthreads();
   if (tid == 0) *hflag = seq;
+  // After the flag, so that it overlaps the host's handling of the result
+  // (its only reader is the next kernel on the stream): for p < 2^31 (exact
+  // pivot inverses), when at least SOLVE_INV_ROWS rows are to be solved (it
+  // costs a few microseconds), the inverse of U_P, the t x t upper triangular matrix of
+  // the pivot rows at the pivot columns (U_P[k][j] = U_k[pcol_j], diagonal
+  // x_k), padded to 64 x 64 with the identity.  A row's multipliers are then
+  // a_P U_P^-1 (a_P: its values at the pivot columns), all at once.  In the
+  // window's shared memory, now free.
+  if (s_uinv) {
+    uint32_t(*X)[PW_LD] = Wv;
+    uint32_t *T = dyn_w + EW * PW_LD;
+    static_assert(EW * PW_LD + 32 * EW / 2 <= PW_R * PW_LD, "inverse scratch fits the window");
+    for (int e = tid; e < EW * EW; e += PS_THREADS) {
+      const int k = e / EW, j = e % EW;
+      uint32_t v;
+      if (k >= t || j >= t) v = k == j ? 1u : 0u;
+      else if (j < k) v = 0u;
+      else if (j == k) v = s_xi[k];
+      else v = ar.mul(PV[k][s_pcol[j]], s_sinv[k]);
+      X[k][j] = v;
+    }
+    __syncthreads();
+    tri64_invert<A, true, PW_LD>(X, T, ar, tid, PS_THREADS);
+    for (int e = tid; e < t * EW; e += PS_THREADS) Uinv_out[e] = X[e / EW][e % EW];
+  }
 }
 
 // Row permutation in one launch: each CTA takes a slice of PERM_COLS
@@ -674,6 +782,66 @@ __global__ void __launch_bounds__(SOLVE_THREADS)
   }
 }
 
+// The same results for p < 2^31 from the inverse of U_P (the search's
+// Uinv, t x EW): a row's multipliers are l = a_P U_P^-1 (a_P: the row's
+// values at the pivot columns), one dot product of length t per lane
+// instead of t dependent elimination steps.  A pivot row k (position i0 +
+// k) keeps multipliers l_j for j < k and 1 at k (a_P = sum_{j<k} l_j U_P[j] +
+// U_P[k]), and its panel becomes U_k; every other row's panel becomes zero
+// (each panel column either holds a pivot, eliminated from all rows below
+// it, or was zero at and below the pivot row when it was reached).
+template <class A>
+__global__ void __launch_bounds__(SOLVE_THREADS)
+    panel_solve_inv_kernel(uint32_t *__restrict__ D, size_t ld, int i0, int r1, int c0, int w,
+                           int t, const uint32_t *__restrict__ pcol,
+                           const uint32_t *__restrict__ Uin, const uint32_t *__restrict__ Uinv,
+                           A ar, uint32_t *__restrict__ Lout, size_t ldl) {
+  __shared__ uint32_t sUi[EW][EW];
+  __shared__ int sP[EW];
+  const int tid = threadIdx.x, lane = tid & 31;
+  for (int e = tid; e < t * EW; e += SOLVE_THREADS) cp_async4(&sUi[e / EW][e % EW], Uinv + e, true);
+  if (tid < EW) sP[tid] = tid < t ? (int)pcol[tid] : 0;
+  cp_async_wait_all();
+  __syncthreads();
+  const int pc0 = sP[lane], pc1 = sP[lane + 32];
+  const int warps = (gridDim.x * SOLVE_THREADS) >> 5;
+  for (int pos = i0 + ((blockIdx.x * SOLVE_THREADS + tid) >> 5); pos <= r1; pos += warps) {
+    uint32_t *row = D + (size_t)pos * ld + c0;
+    const uint32_t a0 = lane < w ? row[lane] : 0u, a1 = lane + 32 < w ? row[lane + 32] : 0u;
+    // the row's values at the pivot columns: lane j holds a[pcol_j], a[pcol_{j+32}]
+    const uint32_t x0 = __shfl_sync(0xffffffffu, a0, pc0 & 31);
+    const uint32_t x1 = __shfl_sync(0xffffffffu, a1, pc0 & 31);
+    const uint32_t y0 = __shfl_sync(0xffffffffu, a0, pc1 & 31);
+    const uint32_t y1 = __shfl_sync(0xffffffffu, a1, pc1 & 31);
+    const uint32_t ap0 = lane < t ? (pc0 < 32 ? x0 : x1) : 0u;
+    const uint32_t ap1 = lane + 32 < t ? (pc1 < 32 ? y0 : y1) : 0u;
+    uint32_t l0 = 0u, l1 = 0u;  // multipliers k = lane, lane + 32
+    if (__any_sync(0xffffffffu, (ap0 | ap1) != 0u)) {
+      uint64_t s0 = 0, s1 = 0;
+      for (int j = 0; j < t; ++j) {
+        const uint32_t f = __shfl_sync(0xffffffffu, j < 32 ? ap0 : ap1, j & 31);
+        ar.acc(s0, f, sUi[j][lane]);
+        ar.acc(s1, f, sUi[j][lane + 32]);
+      }
+      l0 = ar.red64(s0);
+      l1 = ar.red64(s1);
+    }
+    const int kk = pos - i0;
+    uint32_t *lr = Lout + (size_t)kk * ldl;
+    if (kk < t) {
+      if (lane < w) row[lane] = Uin[(size_t)kk * EW + lane];
+      if (lane + 32 < w) row[lane + 32] = Uin[(size_t)kk * EW + lane + 32];
+      if (lane < t) lr[lane] = lane < kk ? l0 : (lane == kk ? 1u : 0u);
+      if (lane + 32 < t) lr[lane + 32] = lane + 32 < kk ? l1 : (lane + 32 == kk ? 1u : 0u);
+    } else {
+      if (lane < w) row[lane] = 0u;
+      if (lane + 32 < w) row[lane + 32] = 0u;
+      if (lane < t) lr[lane] = l0;
+      if (lane + 32 < t) lr[lane + 32] = l1;
+    }
+  }
+}
+
 int zp_echelon_dev(Ctx *c, int m, int n, uint32_t p, uint32_t *D, size_t ld, size_t *rank_out,
                    uint32_t *det_out, std::vector<int> *pivot_cols, EchelonKeep *keep) {
   if (p < 2) return ctx_fail(c, ST_ARG, "modulus must be at least 2");
@@ -698,7 +866,7 @@ int zp_echelon_dev(Ctx *c, int m, int n, uint32_t p, uint32_t *D, size_t ld, siz
   const size_t l_bytes = (size_t)m * EB * 4;
   void *base = nullptr;
   int st = ctx_buffer(c, BUF_ECH_0,
-                      out_bytes + i_bytes + h_bytes + 2 * sq_bytes + l_bytes + 1024,
+                      out_bytes + i_bytes + h_bytes + 3 * sq_bytes + l_bytes + 1024,
                       &base);
   if (st) return st;
   uint8_t *b8 = static_cast<uint8_t *>(base);
@@ -712,7 +880,8 @@ int zp_echelon_dev(Ctx *c, int m, int n, uint32_t p, uint32_t *D, size_t ld, siz
   uint8_t *d_act = d_head + m;
   uint32_t *d_U = reinterpret_cast<uint32_t *>(b8 + out_bytes + i_bytes + h_bytes);
   uint32_t *d_xinv = d_U + EW * EW;  // pivot inverses (EW)
-  uint32_t *d_L = d_xinv + EW * EW;  // the block's multipliers (m x EB)
+  uint32_t *d_Uinv = d_xinv + EW * EW;  // U_P^-1 (t x EW), p < 2^31
+  uint32_t *d_L = d_Uinv + EW * EW;  // the block's multipliers (m x EB)
   const uint32_t *d_pcol = reinterpret_cast<const uint32_t *>(b8 + offsetof(PanelOut, pcol));
   void *gws = nullptr;
   // one size for the panel and block updates and the block's trsm (which
@@ -802,16 +971,17 @@ int zp_echelon_dev(Ctx *c, int m, int n, uint32_t p, uint32_t *D, size_t ld, siz
     if (small)
       panel_search_kernel<<<1, PS_THREADS, PW_SMEM, c->stream>>>(
           D, ld, i, m, c0, w, ars, d_head, d_act, d_hist, d_last, d_p2r, d_stamp, epoch, d_U,
-          d_xinv, d_out, hmap_dev, hflag_dev, seq, wcap);
+          d_xinv, d_Uinv, d_out, hmap_dev, hflag_dev, seq, wcap);
     else
       panel_search_kernel<<<1, PS_THREADS, PW_SMEM, c->stream>>>(
           D, ld, i, m, c0, w, arw, d_head, d_act, d_hist, d_last, d_p2r, d_stamp, epoch, d_U,
-          d_xinv, d_out, hmap_dev, hflag_dev, seq, wcap);
+          d_xinv, d_Uinv, d_out, hmap_dev, hflag_dev, seq, wcap);
     ++epoch;
     prof_end(c, pi);
     ctx_launched(c, 2);
     if ((st = ctx_wait_flag(c, hflag, seq, "echelon: panel"))) return st;
     h.t = hmap->t;
+    h.uinv = hmap->uinv;
     h.err = hmap->err;
     h.last_pos = hmap->last_pos;
     h.det = hmap->det;
@@ -876,7 +1046,15 @@ int zp_echelon_dev(Ctx *c, int m, int n, uint32_t p, uint32_t *D, size_t ld, siz
       const int groups = (r1 - i + 1 + SOLVE_THREADS / 32 - 1) / (SOLVE_THREADS / 32);
       pi = prof_begin(c, "ech_solve");
       const int sgrid = std::max(1, std::min(groups, c->num_sms * 8));
-      if (small)
+      // U_P^-1 when the search wrote it (p < 2^31: exact pivot inverses, and
+      // many rows), else the elimination steps
+      if (h.uinv && small)
+        panel_solve_inv_kernel<<<sgrid, SOLVE_THREADS, 0, c->stream>>>(
+            D, ld, i, r1, c0, w, t, d_pcol, d_U, d_Uinv, ars, Lp, EB);
+      else if (h.uinv)
+        panel_solve_inv_kernel<<<sgrid, SOLVE_THREADS, 0, c->stream>>>(
+            D, ld, i, r1, c0, w, t, d_pcol, d_U, d_Uinv, arw, Lp, EB);
+      else if (small)
         panel_solve_kernel<<<sgrid, SOLVE_THREADS, 0, c->stream>>>(D, ld, i, r1, c0, w, t, d_pcol,
                                                                    d_U, d_xinv, ars, Lp, EB);
       else
