@@ -842,6 +842,57 @@ __global__ void __launch_bounds__(SOLVE_THREADS)
   }
 }
 
+// U12 = L11^-1 A12 for one panel, in place, one thread per column of A12:
+// forward substitution with the unit lower L11 (the panel's multipliers of
+// its pivot rows, row stride ldl) in shared memory, the column's t values in
+// registers (the loops fully unrolled, so every index is a constant):
+// x_k = a_k - sum_{j<k} L11[k][j] x_j, one reduction per k.
+constexpr int U12_THREADS = 128;
+template <class A>
+__global__ void __launch_bounds__(U12_THREADS)
+    panel_u12_kernel(const uint32_t *__restrict__ L, size_t ldl, int t, uint32_t *__restrict__ B,
+                     size_t ldb, int ncols, A ar) {
+  __shared__ __align__(16) uint32_t sL[EW][EW];
+  {
+    constexpr int PER = EW * EW / U12_THREADS;
+    uint32_t v[PER];
+#pragma unroll
+    for (int u = 0; u < PER; ++u) {
+      const int e = threadIdx.x + u * U12_THREADS, k = e / EW, j = e % EW;
+      v[u] = (k < t && j < k) ? L[(size_t)k * ldl + j] : 0u;
+    }
+#pragma unroll
+    for (int u = 0; u < PER; ++u) {
+      const int e = threadIdx.x + u * U12_THREADS;
+      sL[e / EW][e % EW] = v[u];
+    }
+  }
+  __syncthreads();
+  const int c = blockIdx.x * U12_THREADS + threadIdx.x;
+  if (c >= ncols) return;
+  const uint32_t p = ar.p;
+  constexpr bool SMALL = std::is_same<A, ArithSmall>::value;
+  uint32_t x[EW];
+#pragma unroll
+  for (int k = 0; k < EW; ++k) x[k] = k < t ? B[(size_t)k * ldb + c] : 0u;
+#pragma unroll
+  for (int k = 1; k < EW; ++k) {
+    if (k < t) {
+      uint64_t s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+#pragma unroll
+      for (int j = 0; j < k; ++j) {
+        if (!SMALL || (j & 3) == 0) ar.acc(s0, sL[k][j], x[j]);
+        else if ((j & 3) == 1) ar.acc(s1, sL[k][j], x[j]);
+        else if ((j & 3) == 2) ar.acc(s2, sL[k][j], x[j]);
+        else ar.acc(s3, sL[k][j], x[j]);
+      }
+      const uint32_t v = ar.red64(s0 + s1 + s2 + s3);
+      x[k] = x[k] >= v ? x[k] - v : x[k] + (p - v);
+      B[(size_t)k * ldb + c] = x[k];
+    }
+  }
+}
+
 int zp_echelon_dev(Ctx *c, int m, int n, uint32_t p, uint32_t *D, size_t ld, size_t *rank_out,
                    uint32_t *det_out, std::vector<int> *pivot_cols, EchelonKeep *keep) {
   if (p < 2) return ctx_fail(c, ST_ARG, "modulus must be at least 2");
@@ -1075,7 +1126,14 @@ int zp_echelon_dev(Ctx *c, int m, int n, uint32_t p, uint32_t *D, size_t ld, siz
     const int rest = (delayed ? b1 : n) - (c0 + w);
     if (rest > 0) {
       uint32_t *U12 = D + (size_t)i * ld + c0 + w;
-      if ((st = tri_left_block(c, false, t, Lp, EB, nullptr, U12, ld, rest, p, 1))) return st;
+      pi = prof_begin(c, "ech_u12");
+      const int ugrid = (rest + U12_THREADS - 1) / U12_THREADS;
+      if (small)
+        panel_u12_kernel<<<ugrid, U12_THREADS, 0, c->stream>>>(Lp, EB, t, U12, ld, rest, ars);
+      else
+        panel_u12_kernel<<<ugrid, U12_THREADS, 0, c->stream>>>(Lp, EB, t, U12, ld, rest, arw);
+      prof_end(c, pi);
+      ctx_launched(c);
       if (below > 0) {
         pi = prof_begin(c, "ech_update");
         st = zp_gemm_dev(c, GEMM_AUTO, below, rest, t, p, p - 1, Lp + (size_t)t * EB, EB, U12,
