@@ -287,7 +287,8 @@ __global__ void __launch_bounds__(HEADS_THREADS)
 //
 // Bookkeeping: the window is a list of entries sorted by position, entry ->
 // shared-memory slot (perm) and position (ppos), double-buffered and
-// rewritten each column; wrow[slot] is the row index in D.  A transposition
+// rewritten each column (or, when only its first entry leaves, read from one
+// entry further on); wrow[slot] is the row index in D.  A transposition
 // (i, q) moves the row at position i to q: a window row keeps its entry
 // (with position q); a row outside the window (zero in the panel) is
 // recorded in p2r / stamp.  Rows past the window carry in head[] a lower
@@ -368,10 +369,10 @@ __global__ void __launch_bounds__(PS_THREADS, 1)
   __syncthreads();
   const int wlast = s_wlast;  // rows past it are outside the window
 
-  int cur = 0, i = i0, t = 0;
+  int cur = 0, off = 0, i = i0, t = 0;  // the entry list: perm[cur] / ppos[cur] from off
   uint32_t S = 1u % p;
   for (int col = 0; col < w && i < m; ++col) {
-    const int *pm = perm[cur], *pp = ppos[cur];
+    const int *pm = perm[cur] + off, *pp = ppos[cur] + off;
     int *pn = perm[cur ^ 1], *ppn = ppos[cur ^ 1];
     // A. first window entry (by position) with a nonzero in col.  Every warp
     // finds it by itself: column col of the window and the entry list were
@@ -562,7 +563,11 @@ __global__ void __launch_bounds__(PS_THREADS, 1)
     }
     if (tid < EW) PV[t][tid] = P[tid];
     const int nn = drop >= 0 ? nl - 1 : nl;
-    for (int s = tid; s < nn; s += PS_THREADS) {
+    // the new entry list; when entry 0 leaves and nothing moves (a pivot at
+    // the row at position i, the usual case) it is the old list from its
+    // second entry, and nothing is copied
+    const bool shift = drop == 0 && !relocate0;
+    for (int s = tid; s < nn && !shift; s += PS_THREADS) {
       int src, pos;
       if (relocate0) {
         src = s < drop - 1 ? s + 1 : (s == drop - 1 ? 0 : s + 1);
@@ -583,7 +588,12 @@ __global__ void __launch_bounds__(PS_THREADS, 1)
       out->tq[t] = (uint32_t)q;
     }
     __syncthreads();
-    cur ^= 1;
+    if (shift) {
+      ++off;
+    } else {
+      cur ^= 1;
+      off = 0;
+    }
     nl = nn;
     S = ar.mul(S, y);
     ++i;
@@ -631,7 +641,7 @@ __global__ void __launch_bounds__(PS_THREADS, 1)
   // through p2r; beyond that rows have not moved
   const int hi = s_hi;
   for (int s = tid; s < nl; s += PS_THREADS)
-    if (act[wrow[perm[cur][s]]]) atomicMax(&s_last, ppos[cur][s]);
+    if (act[wrow[perm[cur][off + s]]]) atomicMax(&s_last, ppos[cur][off + s]);
   for (int pos = max(wlast + 1, i) + tid; pos <= hi && pos < m; pos += PS_THREADS)
     if (act[row_at(pos, p2r, stamp, epoch)]) atomicMax(&s_last, pos);
   __syncthreads();

@@ -85,6 +85,13 @@ template <>
 struct TcCfg<1, 2> {
   static constexpr int BN = 128, NMMA = 128, STAGES = 6, ACC = 2, EPI = 8;
 };
+// the GF(2) product at short K (one limb of 0/1 bytes, parity epilogue):
+// wide tiles with 16 epilogue warps, 64 columns (one output word) each
+template <>
+struct TcCfg<1, 3> {
+  static constexpr int BN = 256, NMMA = 256, STAGES = 4, ACC = 2, EPI = 16;
+};
+constexpr int GF2_TC_T = 3;
 template <>
 struct TcCfg<2, 0> {
   static constexpr int BN = 128, NMMA = 256, STAGES = 3, ACC = 1, EPI = 16;
@@ -473,7 +480,7 @@ __global__ void __launch_bounds__(tc_threads<L, T>(), 1)
                       const __grid_constant__ CUtensorMap tmB, void *__restrict__ Cv,
                       size_t ldc, int M, int N, int K, Modulus mod, uint32_t alpha, uint32_t beta,
                       uint32_t *err, const int2 *__restrict__ kr = nullptr, int kbase = 0) {
-  static_assert(OUT == 0 || (L == 1 && T == 0), "GF(2) output uses one limb, variant 0");
+  static_assert(OUT == 0 || (L == 1 && (T == 0 || T == GF2_TC_T)), "GF(2) output uses one limb");
   uint32_t *C = static_cast<uint32_t *>(Cv);
   using Cfg = TcCfg<L, T>;
   using Lay = TcLayout<L, T>;
@@ -1350,11 +1357,12 @@ namespace lela {
 // C (packed GF(2) words) <- (beta ? C : 0) XOR (alpha ? A*B : 0) from 0/1
 // byte planes Ab (M x Kp, K-major) and Bb (N x Kp, K-major) of K columns:
 // the one-limb tensor-core kernel with the bit-packing epilogue.
-int gf2_gemm_tc_planes(Ctx *c, int M, int N, int K, const uint8_t *Ab, const uint8_t *Bb, int Kp,
-                       uint32_t alpha, uint32_t beta, uint64_t *C, size_t ldc_words) {
-  using Cfg = TcCfg<1, 0>;
-  using Lay = TcLayout<1, 0>;
-  if (int st = ctx_smem_attr(c, (const void *)zp_gemm_tc_kernel<1, 1>, Lay::SMEM,
+template <int T>
+static int gf2_tc_launch(Ctx *c, int M, int N, int K, const uint8_t *Ab, const uint8_t *Bb,
+                         int Kp, uint32_t alpha, uint32_t beta, uint64_t *C, size_t ldc_words) {
+  using Cfg = TcCfg<1, T>;
+  using Lay = TcLayout<1, T>;
+  if (int st = ctx_smem_attr(c, (const void *)zp_gemm_tc_kernel<1, 1, T>, Lay::SMEM,
                              "cudaFuncSetAttribute(gf2 tc)"))
     return st;
   CUtensorMap tmA, tmB;
@@ -1366,12 +1374,23 @@ int gf2_gemm_tc_planes(Ctx *c, int M, int N, int K, const uint8_t *Ab, const uin
   if (st) return st;
   const int tiles = ((M + BM - 1) / BM) * ((N + Cfg::BN - 1) / Cfg::BN);
   int pi = prof_begin(c, "gf2_gemm_tc");
-  zp_gemm_tc_kernel<1, 1><<<std::min(tiles, c->num_sms), tc_threads<1, 0>(), Lay::SMEM, c->stream>>>(
-      tmA, tmB, C, ldc_words, M, N, K, make_modulus(2), alpha, beta, c->dstatus);
+  zp_gemm_tc_kernel<1, 1, T><<<std::min(tiles, c->num_sms), tc_threads<1, T>(), Lay::SMEM,
+                               c->stream>>>(tmA, tmB, C, ldc_words, M, N, K, make_modulus(2),
+                                            alpha, beta, c->dstatus);
   prof_end(c, pi);
   ctx_launched(c);
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? ST_OK : ctx_cuda(c, e, "gf2 tc launch");
+}
+
+// 16 epilogue warps at short K (the echelon's block updates, K <= 512 bits:
+// the 32768^2 echelon 62.0 -> 58.4 ms), 8 at long K (16384^3: 3.358 against
+// 3.371 ms)
+int gf2_gemm_tc_planes(Ctx *c, int M, int N, int K, const uint8_t *Ab, const uint8_t *Bb, int Kp,
+                       uint32_t alpha, uint32_t beta, uint64_t *C, size_t ldc_words) {
+  if (K <= 4096)
+    return gf2_tc_launch<GF2_TC_T>(c, M, N, K, Ab, Bb, Kp, alpha, beta, C, ldc_words);
+  return gf2_tc_launch<0>(c, M, N, K, Ab, Bb, Kp, alpha, beta, C, ldc_words);
 }
 
 }  // namespace lela
