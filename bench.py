@@ -67,6 +67,8 @@ def parse():
                     help="run only the GF(2) gemm and echelon line (profiling aid)")
     ap.add_argument("--gemm-only", metavar="M,N,K",
                     help="time only a Z/p gemm of this shape on the tensor cores (profiling aid)")
+    ap.add_argument("--echelon-only", type=int, metavar="N", default=0,
+                    help="only a dense N x N row-echelon form over Z/65521 (for launch lists)")
     ap.add_argument("--gemm-p", type=int, default=P)
     ap.add_argument("--gemm-tile", type=int, default=0,
                     help="tile variant for --gemm-only: 0 auto, 1 wide, 2 two accumulator buffers")
@@ -1049,6 +1051,29 @@ def run_gemm_only(args):
     cm.close()
 
 
+def run_echelon_only(args):
+    """One dense N x N row-echelon form over Z/65521 (the dense echelon line
+    at another size): a warm-up call, then `steps` calls timed by CUDA events
+    on the module's stream; prints one JSON object."""
+    import torch
+    from lela_b200 import CudaModule, gen
+    n = args.echelon_only
+    dev = torch.device("cuda", 0)
+    cm = CudaModule(0)
+    stream = torch.cuda.Stream(device=dev)
+    cm.set_stream(stream)
+    E0 = torch.from_numpy(gen.dense_zp(33, n, n, P).view(np.int32)).to(dev)
+    E = E0.clone()
+    _, rk, _ = cm.echelonize(P, E)
+    times = []
+    for _ in range(max(1, args.steps)):
+        E.copy_(E0)
+        times.append(_event_ms(torch, stream, lambda: cm.echelonize(P, E), 1))
+    print(json.dumps({"workload": "row-echelon form, dense %dx%d over Z/65521" % (n, n),
+                      "ms": round(min(times), 3), "rank": rk}))
+    cm.close()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -1059,6 +1084,8 @@ def main():
         run_fl_only(args)
     elif args.gf2_only:
         run_gf2_only(args)
+    elif args.echelon_only:
+        run_echelon_only(args)
     else:
         run_ours(args)
 
