@@ -852,12 +852,16 @@ __global__ void __launch_bounds__(SOLVE_THREADS)
   }
 }
 
-// U12 = L11^-1 A12 for one panel, in place, one thread per column of A12:
-// forward substitution with the unit lower L11 (the panel's multipliers of
-// its pivot rows, row stride ldl) in shared memory, the column's t values in
-// registers (the loops fully unrolled, so every index is a constant):
-// x_k = a_k - sum_{j<k} L11[k][j] x_j, one reduction per k.
+// U12 = L11^-1 A12 for one panel, in place: forward substitution x_k = a_k -
+// sum_{j<k} L11[k][j] x_j with the unit lower L11 (the panel's multipliers of
+// its pivot rows, row stride ldl) in shared memory.  Four lanes per column
+// of A12, lane l holding the column's entries j = l mod 4 in registers (the
+// loops fully unrolled, so every register index is a constant): per k each
+// lane sums its share of the products, two shuffles add the four shares, and
+// the owner of entry k updates it.  The same field operations as any
+// substitution with a unit diagonal.
 constexpr int U12_THREADS = 128;
+constexpr int U12_COLS = U12_THREADS / 4;
 template <class A>
 __global__ void __launch_bounds__(U12_THREADS)
     panel_u12_kernel(const uint32_t *__restrict__ L, size_t ldl, int t, uint32_t *__restrict__ B,
@@ -878,28 +882,39 @@ __global__ void __launch_bounds__(U12_THREADS)
     }
   }
   __syncthreads();
-  const int c = blockIdx.x * U12_THREADS + threadIdx.x;
-  if (c >= ncols) return;
+  const int l4 = threadIdx.x & 3;
+  const int c = blockIdx.x * U12_COLS + (threadIdx.x >> 2);
+  const bool valid = c < ncols;  // every lane stays for the shuffles
   const uint32_t p = ar.p;
-  constexpr bool SMALL = std::is_same<A, ArithSmall>::value;
-  uint32_t x[EW];
+  uint32_t x[EW / 4];  // x[i]: entry 4 i + l4
 #pragma unroll
-  for (int k = 0; k < EW; ++k) x[k] = k < t ? B[(size_t)k * ldb + c] : 0u;
+  for (int i = 0; i < EW / 4; ++i) {
+    const int j = 4 * i + l4;
+    x[i] = (valid && j < t) ? B[(size_t)j * ldb + c] : 0u;
+  }
 #pragma unroll
   for (int k = 1; k < EW; ++k) {
     if (k < t) {
-      uint64_t s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+      // entries j >= k still hold a_j, but L11[k][j] is zero there
+      uint64_t acc = 0;
 #pragma unroll
-      for (int j = 0; j < k; ++j) {
-        if (!SMALL || (j & 3) == 0) ar.acc(s0, sL[k][j], x[j]);
-        else if ((j & 3) == 1) ar.acc(s1, sL[k][j], x[j]);
-        else if ((j & 3) == 2) ar.acc(s2, sL[k][j], x[j]);
-        else ar.acc(s3, sL[k][j], x[j]);
+      for (int i = 0; i <= (k - 1) / 4; ++i) ar.acc(acc, sL[k][4 * i + l4], x[i]);
+      uint32_t v = ar.red64(acc);
+#pragma unroll
+      for (int o = 1; o <= 2; o <<= 1) {  // v + w mod p without overflow (any p < 2^32)
+        const uint32_t nw = p - __shfl_xor_sync(0xffffffffu, v, o);
+        v = v >= nw ? v - nw : v + (p - nw);
       }
-      const uint32_t v = ar.red64(s0 + s1 + s2 + s3);
-      x[k] = x[k] >= v ? x[k] - v : x[k] + (p - v);
-      B[(size_t)k * ldb + c] = x[k];
+      if (l4 == (k & 3)) {
+        const uint32_t a = x[k >> 2];
+        x[k >> 2] = a >= v ? a - v : a + (p - v);
+      }
     }
+  }
+#pragma unroll
+  for (int i = 0; i < EW / 4; ++i) {
+    const int j = 4 * i + l4;
+    if (valid && j >= 1 && j < t) B[(size_t)j * ldb + c] = x[i];
   }
 }
 
@@ -1137,7 +1152,7 @@ int zp_echelon_dev(Ctx *c, int m, int n, uint32_t p, uint32_t *D, size_t ld, siz
     if (rest > 0) {
       uint32_t *U12 = D + (size_t)i * ld + c0 + w;
       pi = prof_begin(c, "ech_u12");
-      const int ugrid = (rest + U12_THREADS - 1) / U12_THREADS;
+      const int ugrid = (rest + U12_COLS - 1) / U12_COLS;
       if (small)
         panel_u12_kernel<<<ugrid, U12_THREADS, 0, c->stream>>>(Lp, EB, t, U12, ld, rest, ars);
       else
