@@ -178,6 +178,13 @@ int ctx_check_status(Ctx *c, const char *what);
 // panel search publishes its result (from offset 0) and then a sequence
 // number (a uint32 at PANEL_FLAG_OFF); allocated on first use.
 constexpr size_t PANEL_MAP_BYTES = 4096, PANEL_FLAG_OFF = 4032;
+// a panel's row-transposition lists (source rows, then destination rows) are
+// staged here by the host and copied to the device on the stream: a copy
+// from pinned memory, so the host does not wait for it.  The host writes the
+// next panel's lists only after that panel's search has signalled, which the
+// stream orders after the previous copy.
+constexpr size_t PANEL_PERM_OFF = 1024, PANEL_PERM_INTS = 256;
+static_assert(PANEL_PERM_OFF + PANEL_PERM_INTS * 4 <= PANEL_FLAG_OFF, "staging below the flag");
 int ctx_panel_map(Ctx *c, void **host, void **dev);
 // Spin until *flag == seq (the work queued before the publishing kernel
 // included), checking the handle's stream for errors now and then and

@@ -978,6 +978,8 @@ int zp_echelon_dev(Ctx *c, int m, int n, uint32_t p, uint32_t *D, size_t ld, siz
   void *mh = nullptr, *md = nullptr;
   if ((st = ctx_panel_map(c, &mh, &md))) return st;
   const PanelOut *hmap = static_cast<const PanelOut *>(mh);
+  int *hperm = reinterpret_cast<int *>(static_cast<char *>(mh) + PANEL_PERM_OFF);
+  static_assert(sizeof(PanelOut) <= PANEL_PERM_OFF && 2 * (2 * EW) <= (int)PANEL_PERM_INTS, "staging layout");
   volatile uint32_t *hflag = reinterpret_cast<volatile uint32_t *>(static_cast<char *>(mh) + PANEL_FLAG_OFF);
   PanelOut *hmap_dev = static_cast<PanelOut *>(md);
   uint32_t *hflag_dev = reinterpret_cast<uint32_t *>(static_cast<char *>(md) + PANEL_FLAG_OFF);
@@ -1085,9 +1087,11 @@ int zp_echelon_dev(Ctx *c, int m, int n, uint32_t p, uint32_t *D, size_t ld, siz
     const int cnt = (int)src.size();
     if (cnt > 2 * EW) return ctx_fail(c, ST_ARG, "echelon: permutation larger than expected");
     if (cnt > 0) {
-      std::vector<int> both(src);
-      both.insert(both.end(), dst.begin(), dst.end());
-      e = cudaMemcpyAsync(d_perm, both.data(), both.size() * sizeof(int), cudaMemcpyHostToDevice,
+      for (int k = 0; k < cnt; ++k) {
+        hperm[k] = src[k];
+        hperm[cnt + k] = dst[k];
+      }
+      e = cudaMemcpyAsync(d_perm, hperm, (size_t)2 * cnt * sizeof(int), cudaMemcpyHostToDevice,
                           c->stream);
       if (e != cudaSuccess) return ctx_cuda(c, e, "echelon: permutation");
       permute_rows_kernel<<<(n + PERM_COLS - 1) / PERM_COLS, PERM_THREADS, 0, c->stream>>>(

@@ -757,6 +757,8 @@ int gf2_echelon_dev(Ctx *c, int m, int n, uint64_t *D, size_t ld, size_t *rank_o
   void *mh = nullptr, *md = nullptr;
   if ((st = ctx_panel_map(c, &mh, &md))) return st;
   const Gf2PanelOut *hmap = static_cast<const Gf2PanelOut *>(mh);
+  int *hperm = reinterpret_cast<int *>(static_cast<char *>(mh) + PANEL_PERM_OFF);
+  static_assert(sizeof(Gf2PanelOut) <= PANEL_PERM_OFF && 2 * (2 * GW) <= (int)PANEL_PERM_INTS, "staging layout");
   volatile uint32_t *hflag = reinterpret_cast<volatile uint32_t *>(static_cast<char *>(mh) + PANEL_FLAG_OFF);
   Gf2PanelOut *hmap_dev = static_cast<Gf2PanelOut *>(md);
   uint32_t *hflag_dev = reinterpret_cast<uint32_t *>(static_cast<char *>(md) + PANEL_FLAG_OFF);
@@ -855,9 +857,11 @@ int gf2_echelon_dev(Ctx *c, int m, int n, uint64_t *D, size_t ld, size_t *rank_o
     const int cnt = (int)src.size();
     if (cnt > 2 * GW) return ctx_fail(c, ST_ARG, "gf2 echelon: permutation larger than expected");
     if (cnt > 0) {
-      std::vector<int> both(src);
-      both.insert(both.end(), dst.begin(), dst.end());
-      e = cudaMemcpyAsync(d_perm, both.data(), both.size() * sizeof(int), cudaMemcpyHostToDevice,
+      for (int k = 0; k < cnt; ++k) {
+        hperm[k] = src[k];
+        hperm[cnt + k] = dst[k];
+      }
+      e = cudaMemcpyAsync(d_perm, hperm, (size_t)2 * cnt * sizeof(int), cudaMemcpyHostToDevice,
                           c->stream);
       if (e != cudaSuccess) return ctx_cuda(c, e, "gf2 echelon: permutation");
       gf2_permute_rows_kernel<<<(nw + GF2_PERM_WORDS - 1) / GF2_PERM_WORDS, GF2_PERM_THREADS, 0,
