@@ -32,14 +32,17 @@
 //     P with pivot value y), so no inverse is on this sequential path; rows
 //     below the window are reduced only when the head histogram says one of
 //     them may hold a pivot the window lacks.  The pivot inverses and the
-//     pivot rows U_k come out of parallel inversions at the end;
+//     pivot rows U_k come out of parallel inversions at the end, and, after
+//     the host has been signalled and when many rows are to be solved, the
+//     inverse of the pivot block U_P (the pivot rows at the pivot columns);
 //  3. the host replays the recorded transpositions and moves the affected
 //     rows (at most two per pivot) with one gather;
-//  4. panel_solve_kernel (all SMs, one warp per row): for every row from the
-//     first pivot to the last possibly nonzero row, the reference's
-//     elimination steps on its panel part give its multipliers (the L11 row
-//     of a pivot row, the L21 row otherwise); the panel becomes U_k in pivot
-//     row k and zero below;
+//  4. panel_solve_inv_kernel / panel_solve_kernel (all SMs, one warp per
+//     row): for every row from the first pivot to the last possibly nonzero
+//     row, its multipliers (the L11 row of a pivot row, the L21 row
+//     otherwise): a_P U_P^-1 from its entries a_P at the pivot columns, or
+//     the reference's elimination steps on its panel part; the panel becomes
+//     U_k in pivot row k and zero below;
 //  5. U12 = L11^-1 A12 on CUDA cores and A22 -= L21 U12 on the limb-split
 //     tensor-core gemm over the rows down to the last possibly nonzero row,
 //     for the columns of the panel's block of EB columns; the columns right
