@@ -57,6 +57,8 @@ def lib():
         L.oracle_echelon_gf2.argtypes = [_S, _S, _P, _S, ctypes.POINTER(_S)]
         L.oracle_pluq_zp_u32.argtypes = [_U, _S, _S, _P, _S, _P, ctypes.POINTER(_S), _P, ctypes.POINTER(_S),
                                          ctypes.POINTER(_S), ctypes.POINTER(_U)]
+        L.oracle_echelon_reduced_L_zp_u32.argtypes = [_U, _S, _S, _P, _S, _P, _S, _P, ctypes.POINTER(_S),
+                                                      ctypes.POINTER(_S), ctypes.POINTER(_U)]
         L.oracle_inv_zp.argtypes = [_U, _U]
         L.oracle_inv_zp.restype = _U
         _lib = L
@@ -99,6 +101,9 @@ def ref():
         L.lela_ref_trsm_zp_elem.argtypes = [_I, _U, _I, _I, _S, _S, _U, _P, _S, _P, _S, ctypes.POINTER(_S)]
         L.lela_ref_pluq_zp_u32.argtypes = [_U, _S, _S, _P, _S, _P, ctypes.POINTER(_S), _P, ctypes.POINTER(_S),
                                            ctypes.POINTER(_S), ctypes.POINTER(_U)]
+        L.lela_ref_elim_echelon_reduced_L_zp_u32.argtypes = [_U, _S, _S, _P, _S, _P, _S, _P,
+                                                             ctypes.POINTER(_S), ctypes.POINTER(_S),
+                                                             ctypes.POINTER(_U)]
         _ref = L
     return _ref
 
@@ -209,6 +214,24 @@ def _pluq(fn, p, A):
 def pluq_zp(p, A):
     """Elimination::pluq restated: (LU in place, P, Q, rank, det)."""
     return _pluq(lib().oracle_pluq_zp_u32, p, A)
+
+
+def _echelon_L(fn, p, A):
+    A = _c(A, np.uint32).copy()
+    m, n = A.shape
+    L = np.zeros((m, m), dtype=np.uint32)
+    P = np.zeros(2 * max(min(m, n), 1), dtype=np.uint64)
+    np_ = _S(0); r = _S(0); d = _U(0)
+    if fn(p, m, n, _ptr(A), max(n, 1), _ptr(L), max(m, 1), _ptr(P), ctypes.byref(np_),
+          ctypes.byref(r), ctypes.byref(d)):
+        raise ArithmeticError("pivot not invertible")
+    return A, L, [(int(P[2 * t]), int(P[2 * t + 1])) for t in range(np_.value)], r.value, d.value
+
+
+def echelon_reduced_L_zp(p, A):
+    """Elimination::echelonize_reduced with compute_L, restated:
+    (R, L, P, rank, det) with R = L P A."""
+    return _echelon_L(lib().oracle_echelon_reduced_L_zp_u32, p, A)
 
 
 def fl_echelonize_zp(p, m, n, rowptr, colidx, vals, reduced=True, only_D=False):
@@ -384,3 +407,9 @@ def ref_read_matrix(fmt, p, text, m, n):
 def ref_pluq_zp(p, A):
     """Elimination::pluq (LELA): (LU in place, P, Q, rank, det)."""
     return _pluq(ref().lela_ref_pluq_zp_u32, p, A)
+
+
+def ref_echelon_reduced_L_zp(p, A):
+    """Elimination::echelonize_reduced with compute_L (LELA):
+    (R, L, P, rank, det)."""
+    return _echelon_L(ref().lela_ref_elim_echelon_reduced_L_zp_u32, p, A)

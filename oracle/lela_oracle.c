@@ -322,6 +322,82 @@ int oracle_echelon_reduced_unit_zp_u32 (uint32_t p, size_t m, size_t n, uint32_t
 	return 0;
 }
 
+/* The standard method's reduced form with its transform,
+ * Elimination::echelonize_reduced (A, L, P, rank, det, true) (lela/
+ * algorithms/elimination.tcc:143-265), step by step as the reference takes
+ * it.  L (m x m, leading dimension ldl) starts as the identity (:176-184).
+ * Step i: the first column from the current one with a nonzero at or below
+ * row i, and its first such row; when that row is not i, rows i and it are
+ * swapped in A, and in L both rows and columns (:203-210), and the pair is
+ * recorded; det is multiplied by the pivot x; row i of A and of L is scaled
+ * by 1/x (:221-227); every other row j with a nonzero a in the pivot column
+ * gets row j <- row j - a row i, in A and in L (:229-244).  So at the end
+ * A = L P A_in, P the transpositions applied in order.  P holds them as
+ * pairs in the reference's order (not reversed).  Returns 0, or -1 when a
+ * pivot is not invertible (the reference throws). */
+int oracle_echelon_reduced_L_zp_u32 (uint32_t p, size_t m, size_t n, uint32_t *A, size_t lda,
+				     uint32_t *L, size_t ldl, size_t *P, size_t *np,
+				     size_t *rank, uint32_t *det)
+{
+	size_t i, c, npp = 0;
+	uint32_t d = 1 % p;
+	for (i = 0; i < m; ++i)
+		for (c = 0; c < m; ++c)
+			L[i * ldl + c] = (i == c) ? 1 % p : 0;
+	size_t pc = 0;
+	for (i = 0; i < m && pc < n; ++i, ++pc) {
+		size_t prow = m;
+		for (; pc < n; ++pc) {
+			for (size_t r = i; r < m; ++r)
+				if (A[r * lda + pc] != 0) { prow = r; break; }
+			if (prow < m) break;
+		}
+		if (prow == m)
+			break;
+		if (prow != i) {
+			for (c = 0; c < n; ++c) {
+				uint32_t t = A[i * lda + c];
+				A[i * lda + c] = A[prow * lda + c];
+				A[prow * lda + c] = t;
+			}
+			for (c = 0; c < m; ++c) {
+				uint32_t t = L[i * ldl + c];
+				L[i * ldl + c] = L[prow * ldl + c];
+				L[prow * ldl + c] = t;
+			}
+			for (c = 0; c < m; ++c) {
+				uint32_t t = L[c * ldl + i];
+				L[c * ldl + i] = L[c * ldl + prow];
+				L[c * ldl + prow] = t;
+			}
+			P[2 * npp] = i; P[2 * npp + 1] = prow; ++npp;
+		}
+		uint32_t x = A[i * lda + pc];
+		d = mulmod (p, d, x);
+		uint32_t xinv = oracle_inv_zp (p, x);
+		if (xinv == 0)
+			return -1;
+		for (c = 0; c < n; ++c)
+			A[i * lda + c] = mulmod (p, A[i * lda + c], xinv);
+		for (c = 0; c < m; ++c)
+			L[i * ldl + c] = mulmod (p, L[i * ldl + c], xinv);
+		for (size_t j = 0; j < m; ++j) {
+			uint32_t a = A[j * lda + pc];
+			if (j == i || a == 0)
+				continue;
+			uint32_t nega = (p - a) % p;
+			for (c = 0; c < n; ++c)
+				A[j * lda + c] = axpy_mod (p, A[j * lda + c], nega, A[i * lda + c]);
+			for (c = 0; c < m; ++c)
+				L[j * ldl + c] = axpy_mod (p, L[j * ldl + c], nega, L[i * ldl + c]);
+		}
+	}
+	*np = npp;
+	*rank = i;
+	*det = d;
+	return 0;
+}
+
 /* PLUQ decomposition, Elimination::pluq (lela/algorithms/elimination.tcc:
  * 266-370) with DensePivotStrategy (lela/algorithms/pivot-strategy.tcc:
  * 19-42).  Step i: the first column from i on, in the current column

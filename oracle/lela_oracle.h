@@ -54,6 +54,14 @@ int oracle_echelon_reduced_zp_u32 (uint32_t p, size_t m, size_t n, uint32_t *A, 
 int oracle_echelon_reduced_unit_zp_u32 (uint32_t p, size_t m, size_t n, uint32_t *A, size_t lda,
 					size_t *rank, uint32_t *det);
 
+/* The standard method's reduced form (pivots 1) with its transform: A <- R,
+ * L (m x m, ldl) <- the matrix with R = L P A_in, P the row transpositions
+ * as pairs (at most min(m, n)) in the order they were applied.  Returns 0,
+ * or -1 when a pivot is not invertible mod p. */
+int oracle_echelon_reduced_L_zp_u32 (uint32_t p, size_t m, size_t n, uint32_t *A, size_t lda,
+				     uint32_t *L, size_t ldl, size_t *P, size_t *np,
+				     size_t *rank, uint32_t *det);
+
 /* PLUQ decomposition in place (L strictly below the diagonal, U on and
  * above it); P and Q as transposition pairs (at most min(m, n) each), in
  * the reference's order; rank, det = product of the pivots.  Returns 0, or

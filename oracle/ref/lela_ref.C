@@ -378,6 +378,36 @@ int lela_ref_elim_echelon_reduced_zp_u32 (uint32_t p, size_t m, size_t n, uint32
 	return 0;
 }
 
+/* Elimination::echelonize_reduced (A, L, P, rank, det, true) (lela/
+ * algorithms/elimination.tcc:143-265) with the default pivot strategy of a
+ * dense row: A <- its reduced form (pivots 1), L (m x m, dense) <- the
+ * transform with A_out = L P A_in, P the row transpositions as pairs in the
+ * reference's order (at most min(m, n)).  Returns 0, or -1 when a pivot is
+ * not invertible. */
+int lela_ref_elim_echelon_reduced_L_zp_u32 (uint32_t p, size_t m, size_t n, uint32_t *A, size_t lda, uint32_t *L, size_t ldl, size_t *P, size_t *np, size_t *rank, uint32_t *det)
+{
+	Zp F (p);
+	Context<Zp> ctx (F);
+	DenseMatrix<uint32> MA (m, n), ML (m, m);
+	if (m && n) load_dense (MA, A, lda);
+	Elimination<Zp> elim (ctx);
+	Elimination<Zp>::Permutation PP;
+	size_t r = 0;
+	Zp::Element d;
+	try {
+		elim.echelonize_reduced (MA, ML, PP, r, d, true);
+	} catch (...) {
+		return -1;
+	}
+	if (m && n) store_dense (MA, A, lda);
+	if (m) store_dense (ML, L, ldl);
+	for (size_t k = 0; k < PP.size (); ++k) { P[2 * k] = PP[k].first; P[2 * k + 1] = PP[k].second; }
+	*np = PP.size ();
+	*rank = r;
+	*det = d;
+	return 0;
+}
+
 /* Elimination::pluq (lela/algorithms/elimination.tcc:266-370) with the
  * default pivot strategy of a dense row: A <- L and U in place (L strictly
  * below the diagonal, unit diagonal implied), P and Q the row and column

@@ -84,3 +84,17 @@ def gf2_echelon_cases():
     for pre in man["gf2_echelon"]:
         m, n, r = (int(x) for x in z[pre + "meta"])
         yield pre, m, n, r, z[pre + "A"], z[pre + "E"]
+
+
+def transform_cases():
+    """Elimination::echelonize_reduced with compute_L, as LELA computed it
+    (tests/golden/make_transform_golden.py): (pre, p, status, rank, det, A,
+    R, L, P)."""
+    if "transform" not in _cache:
+        _cache["transform"] = dict(np.load(os.path.join(HERE, "transform_golden.npz")))
+    z = _cache["transform"]
+    for pre in z["names"]:
+        pre = str(pre)
+        p, st, r, d = (int(x) for x in z[pre + "meta"])
+        P = [tuple(int(v) for v in t) for t in z[pre + "P"]]
+        yield pre, p, st, r, d, z[pre + "A"], z[pre + "R"], z[pre + "L"], P

@@ -72,6 +72,46 @@ def test_golden_pluq():
         assert np.array_equal(got, E), pre
 
 
+def test_golden_transform():
+    """Elimination::echelonize_reduced with compute_L: R, L, P, rank, det and
+    LELA's failures, against LELA's own results."""
+    n = 0
+    for pre, p, st, r, d, A, R, L, P in golden_io.transform_cases():
+        if st:
+            with pytest.raises(ArithmeticError):
+                oracle.echelon_reduced_L_zp(p, A)
+            continue
+        gR, gL, gP, gr, gd = oracle.echelon_reduced_L_zp(p, A)
+        assert (gr, gd) == (r, d) and gP == P, pre
+        assert np.array_equal(gR, R) and np.array_equal(gL, L), pre
+        n += 1
+    assert n >= 100
+
+
+def test_transform_identity():
+    """R = L P A, with L = [[X, 0], [Y, I]] in the rank's blocks, and R the
+    standard method's reduced form (p < 2^31, where Modular<uint32>'s
+    inverse is exact)."""
+    rng = np.random.default_rng(5)
+    for p in (2, 251, 65521, 2147483647):
+        for (m, n) in ((1, 1), (6, 9), (9, 6), (30, 30), (25, 60)):
+            for kind in range(3):
+                A = gen.dense_zp(int(rng.integers(1 << 30)), m, n, p)
+                if kind == 1:
+                    A[:, ::2] = 0
+                elif kind == 2:
+                    A[m // 3:] = (A[: m - m // 3] * 3) % p
+                R, L, P, r, d = oracle.echelon_reduced_L_zp(p, A)
+                B = A.astype(object)
+                for a, b in P:
+                    B[[a, b]] = B[[b, a]]
+                assert np.array_equal((L.astype(object).dot(B) % p).astype(np.uint32), R)
+                assert not L[:r, r:].any()
+                assert np.array_equal(L[r:, r:], np.eye(m - r, dtype=np.uint32))
+                R2, r2, d2 = oracle.echelon_reduced_zp(p, A, unit=True)
+                assert np.array_equal(R, R2) and (r, d) == (r2, d2)
+
+
 def test_golden_fl():
     for (pre, p, m, n, red, od, st, rank, det, rowptr, colidx, vals, R) in golden_io.fl_cases():
         got = oracle.fl_echelonize_zp(p, m, n, rowptr, colidx, vals, red, od)
@@ -305,3 +345,36 @@ def test_live_pluq(p):
             assert (want is None) == (got is None), (m, n, kind)
             if want is not None:
                 assert np.array_equal(got[0], want[0]) and got[1:] == want[1:], (m, n, kind)
+
+
+@need_ref
+@pytest.mark.parametrize("p", [2, 3, 251, 65521, 65536, 2147483647, 4294967291])
+def test_live_transform(p):
+    """Elimination::echelonize_reduced (compute_L = true) against the
+    restatement: R, L, P, rank and det on full-rank, rank-deficient,
+    zero-column and zero-row inputs, and LELA's pivot-inversion failures."""
+    rng = np.random.default_rng(p % 983)
+    for (m, n) in ((1, 1), (2, 7), (7, 13), (13, 7), (40, 40), (48, 80), (80, 48)):
+        for kind in range(4):
+            A = gen.dense_zp(int(rng.integers(1 << 30)), m, n, p)
+            if kind == 1:
+                A[:, ::3] = 0
+            elif kind == 2:
+                r = max(1, min(m, n) // 3)
+                F = gen.dense_zp(1, m, r, p).astype(object) @ gen.dense_zp(2, r, n, p).astype(object)
+                A = (F % p).astype(np.uint32)
+            elif kind == 3:
+                A[m // 2:] = 0
+                A[:, :n // 2] = 0
+            try:
+                want = oracle.ref_echelon_reduced_L_zp(p, A)
+            except ArithmeticError:
+                want = None
+            try:
+                got = oracle.echelon_reduced_L_zp(p, A)
+            except ArithmeticError:
+                got = None
+            assert (want is None) == (got is None), (m, n, kind)
+            if want is not None:
+                assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1]), (m, n, kind)
+                assert got[2:] == want[2:], (m, n, kind)
