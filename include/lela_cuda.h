@@ -254,6 +254,31 @@ int lela_cuda_pluq_zp_u32_dev (lela_cuda_ctx *ctx, size_t m, size_t n, uint32_t 
 			       size_t lda, size_t *P, size_t *np, size_t *Q, size_t *nq,
 			       size_t *rank, uint32_t *det);
 
+/* The standard method's reduced row-echelon form together with its
+ * transform: replaces Elimination::echelonize_reduced (A, L, P, rank, det,
+ * compute_L = true) (lela/algorithms/elimination.h:108-162,
+ * elimination.tcc:143-265) with DensePivotStrategy.  On return A (m x n)
+ * holds the reduced form with unit pivots (as lela_cuda_echelon_reduced_
+ * zp_u32 with unit_pivots = 1), L (m x m, row stride ldl >= m) the matrix
+ * with A_out = L P A_in, where P applies the row transpositions
+ * (P[2t], P[2t+1]), t < *np, in that order (the reference's order, not
+ * reversed; room for min(m, n) pairs).  L is [[X, 0], [Y, I]] in blocks of
+ * *rank rows and columns.  *det = product of the pivots before scaling.
+ * p must be below 2^31 (LELA_CUDA_ERR_ARG otherwise): above it
+ * Modular<uint32>::inv works in wrapped 32-bit ints and returns no true
+ * inverse, so the reference itself produces no transform.
+ * LELA_CUDA_PIVOT_NOT_INVERTIBLE when a pivot cannot be inverted (a
+ * composite p; A and L unspecified).  The _dev form takes A and L on the
+ * device (P on the host). */
+int lela_cuda_echelon_reduced_transform_zp_u32 (lela_cuda_ctx *ctx, size_t m, size_t n,
+						uint32_t p, uint32_t *A, size_t lda, uint32_t *L,
+						size_t ldl, size_t *P, size_t *np, size_t *rank,
+						uint32_t *det);
+int lela_cuda_echelon_reduced_transform_zp_u32_dev (lela_cuda_ctx *ctx, size_t m, size_t n,
+						    uint32_t p, uint32_t *A, size_t lda, uint32_t *L,
+						    size_t ldl, size_t *P, size_t *np, size_t *rank,
+						    uint32_t *det);
+
 /* ------------------------------------------- Faugere-Lachartre echelon form
  * Echelon form of the F4 matrix X (m x n, CSR: rowptr[m+1], colidx, vals;
  * column indices strictly increasing within a row, stored values in [0,p)).

@@ -138,6 +138,12 @@ def _bind_optional(L):
                                   ctypes.POINTER(_S), ctypes.POINTER(_S), ctypes.POINTER(_U)],
         "lela_cuda_pluq_zp_u32_dev": [_P, _S, _S, _U, _P, _S, _P, ctypes.POINTER(_S), _P,
                                       ctypes.POINTER(_S), ctypes.POINTER(_S), ctypes.POINTER(_U)],
+        "lela_cuda_echelon_reduced_transform_zp_u32": [_P, _S, _S, _U, _P, _S, _P, _S, _P,
+                                                       ctypes.POINTER(_S), ctypes.POINTER(_S),
+                                                       ctypes.POINTER(_U)],
+        "lela_cuda_echelon_reduced_transform_zp_u32_dev": [_P, _S, _S, _U, _P, _S, _P, _S, _P,
+                                                           ctypes.POINTER(_S), ctypes.POINTER(_S),
+                                                           ctypes.POINTER(_U)],
         "lela_cuda_gemm_gf2": [_P, _S, _S, _S, _I, _P, _S, _P, _S, _I, _P, _S],
         "lela_cuda_gemm_gf2_dev": [_P, _S, _S, _S, _I, _P, _S, _P, _S, _I, _P, _S],
         "lela_cuda_echelon_gf2": [_P, _S, _S, _P, _S, ctypes.POINTER(_S)],
@@ -423,6 +429,33 @@ class CudaModule:
         self._raise(st)
         pairs = lambda X, c: [(int(X[2 * t]), int(X[2 * t + 1])) for t in range(c)]
         return A, pairs(P, np_.value), pairs(Q, nq.value), r.value, d.value
+
+    def echelon_reduced_transform(self, p, A, L=None):
+        """Elimination::echelonize_reduced (A, L, P, rank, det, compute_L =
+        true): A <- its reduced form with unit pivots, in place; returns (A,
+        L, P, rank, det) with A_out = L P A_in, L m x m, and P a list of
+        transposition pairs in the order applied.  Host numpy uint32 matrix,
+        or torch CUDA tensor (then L is a device tensor too).  p < 2^31."""
+        m, n = A.shape
+        P = np.zeros(2 * max(min(m, n), 1), dtype=np.uint64)
+        np_, r, d = _S(0), _S(0), _U(0)
+        if _is_torch(A):
+            import torch
+            if L is None:
+                L = torch.empty((m, m), dtype=A.dtype, device=A.device)
+            st = self.L.lela_cuda_echelon_reduced_transform_zp_u32_dev(
+                self.h, m, n, p, _dptr(A), max(A.stride(0), 1), _dptr(L), max(L.stride(0), 1),
+                _ptr(P), ctypes.byref(np_), ctypes.byref(r), ctypes.byref(d))
+        else:
+            _check(A.dtype == np.uint32, "echelon_reduced_transform: uint32 matrix expected")
+            if L is None:
+                L = np.zeros((m, m), dtype=np.uint32)
+            st = self.L.lela_cuda_echelon_reduced_transform_zp_u32(
+                self.h, m, n, p, _ptr(A), max(A.strides[0] // 4, n, 1), _ptr(L),
+                max(L.strides[0] // 4, m, 1), _ptr(P), ctypes.byref(np_), ctypes.byref(r),
+                ctypes.byref(d))
+        self._raise(st)
+        return A, L, [(int(P[2 * t]), int(P[2 * t + 1])) for t in range(np_.value)], r.value, d.value
 
     # ------------------------------------------------- Faugere-Lachartre
     def fl_echelonize(self, p, X, reduced=True, only_D=False, R=None):

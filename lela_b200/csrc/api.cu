@@ -1219,6 +1219,62 @@ int lela_cuda_pluq_zp_u32_dev(lela_cuda_ctx *h, size_t m, size_t n, uint32_t p, 
   return pluq_entry(h, m, n, p, A, lda, P, np, Q, nq, rank, det, true);
 }
 
+static int transform_entry(lela_cuda_ctx *h, size_t m, size_t n, uint32_t p, uint32_t *A,
+                           size_t lda, uint32_t *L, size_t ldl, size_t *P, size_t *np,
+                           size_t *rank, uint32_t *det, bool dev) {
+  if (!h || !rank || !det || !np) return ST_ARG;
+  Ctx *c = &h->c;
+  DeviceScope ds(c);
+  if (m > (size_t)INT32_MAX || n > (size_t)INT32_MAX) return ctx_fail(c, ST_ARG, "dimension too large");
+  if (p < 2) return ctx_fail(c, ST_ARG, "modulus must be at least 2");
+  if (m && (!L || ldl < m)) return ctx_fail(c, ST_ARG, "bad transform array");
+  if (m && n && (!A || lda < n || !P)) return ctx_fail(c, ST_ARG, "bad matrix or permutation array");
+  std::vector<std::pair<int, int>> vp;
+  int st = ctx_clear_status(c);
+  if (st) return st;
+  uint32_t *dA = A, *dL = L;
+  size_t ld = lda, ldL = ldl;
+  if (!dev && m) {
+    void *s = nullptr;
+    if (n) {
+      if ((st = ctx_stage(c, 0, m * n * 4, &s))) return st;
+      dA = static_cast<uint32_t *>(s);
+      ld = n;
+      if ((st = h2d_matrix(c, dA, A, m, n, lda, 4))) return st;
+    }
+    if ((st = ctx_stage(c, 1, m * m * 4, &s))) return st;
+    dL = static_cast<uint32_t *>(s);
+    ldL = m;
+  }
+  st = zp_echelon_transform_dev(c, (int)m, (int)n, p, dA, ld, dL, ldL, &vp, rank, det);
+  if (st == ST_PIVOT) return ctx_fail(c, ST_PIVOT, "Could not invert pivot-element in the ring");
+  if (st) return st;
+  if (!dev && m) {
+    if (n && (st = d2h_matrix(c, A, dA, m, n, lda, 4))) return st;
+    if ((st = d2h_matrix(c, L, dL, m, m, ldl, 4))) return st;
+  }
+  for (size_t t = 0; t < vp.size(); ++t) {
+    P[2 * t] = (size_t)vp[t].first;
+    P[2 * t + 1] = (size_t)vp[t].second;
+  }
+  *np = vp.size();
+  return ctx_check_status(c, "echelon_reduced_transform_zp_u32");
+}
+
+int lela_cuda_echelon_reduced_transform_zp_u32(lela_cuda_ctx *h, size_t m, size_t n, uint32_t p,
+                                               uint32_t *A, size_t lda, uint32_t *L, size_t ldl,
+                                               size_t *P, size_t *np, size_t *rank,
+                                               uint32_t *det) {
+  return transform_entry(h, m, n, p, A, lda, L, ldl, P, np, rank, det, false);
+}
+
+int lela_cuda_echelon_reduced_transform_zp_u32_dev(lela_cuda_ctx *h, size_t m, size_t n,
+                                                   uint32_t p, uint32_t *A, size_t lda,
+                                                   uint32_t *L, size_t ldl, size_t *P, size_t *np,
+                                                   size_t *rank, uint32_t *det) {
+  return transform_entry(h, m, n, p, A, lda, L, ldl, P, np, rank, det, true);
+}
+
 int lela_cuda_echelon_zp_u32_dev(lela_cuda_ctx *h, size_t m, size_t n, uint32_t p, uint32_t *A,
                                  size_t lda, size_t *rank, uint32_t *det) {
   return echelon_entry(h, m, n, p, A, lda, rank, det, true, false);

@@ -154,7 +154,8 @@ enum BufSlot : int {
   BUF_FL_CSR_V = 25,  // Faugere-Lachartre CSR output: column indices and values
   BUF_PLUQ = 26,      // PLUQ: kept multipliers, assembled output, column order
   BUF_ELEM = 27,      // uint32 copies of Modular<uint8/uint16/float/double> operands
-  BUF_COUNT = 28,
+  BUF_TRANSFORM = 28, // reduced form's transform: kept multipliers, triangles, pivot columns
+  BUF_COUNT = 29,
 };
 
 // Grow-only allocation helpers; return ST_OK or ST_NOMEM.

@@ -1275,4 +1275,119 @@ int zp_pluq_dev(Ctx *c, int m, int n, uint32_t p, uint32_t *D, size_t ld,
   return e == cudaSuccess ? ST_OK : ctx_cuda(c, e, "pluq: assembly");
 }
 
+// ---------------------------------------------------------------------------
+// The standard method's reduced form with its transform:
+// Elimination::echelonize_reduced (A, L, P, rank, det, true) (lela/
+// algorithms/elimination.tcc:143-265).  There L starts as the identity and
+// takes every row operation of A, with each transposition applied to its
+// rows and columns, so that at the end R = L B with B = P A_in (the
+// transpositions in the order they were applied).
+//
+// The pivots, the transpositions and the pivot values of that loop are those
+// of the non-reduced form (the rows at and below the current one are the
+// same in both loops), so the panel pipeline above gives them, together
+// with the non-reduced rows U (r x n) and the multipliers Lk (m x r, unit
+// lower trapezoidal) with B = Lk U.  Write Lk = [L1; L2] (r and m - r rows)
+// and U_P for U at the pivot columns (upper triangular, the pivots on its
+// diagonal).  Pivot rows only ever receive multiples of pivot rows, and the
+// other rows keep their own unit entry, so L = [[X, 0], [Y, I]]; R's pivot
+// rows have the identity at the pivot columns, and its other rows are zero.
+// Hence X = U_P^-1 L1^-1, Y = -L2 L1^-1, and R's first r rows are
+// U_P^-1 U:
+//   1. Lout <- I (m x m), T <- L1 (unit lower), W <- U_P;
+//   2. Lout[0:r, 0:r] <- T^-1             (trsm, unit lower: no inversions);
+//   3. Lout[r:m, 0:r] <- -L2 Lout[0:r, 0:r]           (gemm, alpha = p - 1);
+//   4. Lout[0:r, 0:r] <- W^-1 Lout[0:r, 0:r]      (trsm, upper: the pivots);
+//   5. D[0:r, :] <- W^-1 D[0:r, :]; D's rows from r on are zero already.
+// The only inversions are of the pivots, as in the reference, so a pivot it
+// cannot invert fails here too (in the panel pipeline, before any solve).
+// ---------------------------------------------------------------------------
+
+// Step 1.  T (r x r) <- the unit lower triangle of Lk's first r rows; W
+// (r x r) <- D's first r rows at the pivot columns piv (row i of D is zero
+// left of piv[i], so W is upper triangular); Lout (m x m) <- the identity.
+__global__ void transform_setup_kernel(const uint32_t *__restrict__ Lk, size_t ldk,
+                                       const uint32_t *__restrict__ D, size_t ldd,
+                                       const int *__restrict__ piv, int m, int r,
+                                       uint32_t *__restrict__ T, uint32_t *__restrict__ W,
+                                       uint32_t *__restrict__ Lout, size_t ldl) {
+  const size_t mm = (size_t)m * m, rr = (size_t)r * r;
+  for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < mm + 2 * rr;
+       idx += (size_t)gridDim.x * blockDim.x) {
+    if (idx < mm) {
+      const size_t i = idx / m, j = idx % m;
+      Lout[i * ldl + j] = i == j ? 1u : 0u;
+    } else if (idx < mm + rr) {
+      const size_t e = idx - mm, i = e / r, j = e % r;
+      T[e] = j < i ? Lk[i * ldk + j] : (i == j ? 1u : 0u);
+    } else {
+      const size_t e = idx - mm - rr, i = e / r, j = e % r;
+      W[e] = D[i * ldd + piv[j]];
+    }
+  }
+}
+
+int zp_echelon_transform_dev(Ctx *c, int m, int n, uint32_t p, uint32_t *D, size_t ld,
+                             uint32_t *Lout, size_t ldl, std::vector<std::pair<int, int>> *P,
+                             size_t *rank, uint32_t *det) {
+  P->clear();
+  if (p < 2) return ctx_fail(c, ST_ARG, "modulus must be at least 2");
+  if (p >= 0x80000000u)
+    return ctx_fail(c, ST_ARG,
+                    "modulus must be below 2^31 (Modular<uint32>'s inverse wraps above it)");
+  if (m < 0 || n < 0) return ctx_fail(c, ST_ARG, "negative dimension");
+  if (m > 0 && ldl < (size_t)m) return ctx_fail(c, ST_ARG, "transform leading dimension too small");
+  *rank = 0;
+  *det = 1 % p;
+  if (m == 0) return ST_OK;
+  const int rmax = std::max(1, std::min(m, n));
+  const size_t k_bytes = ((size_t)m * rmax * 4 + 255) & ~(size_t)255;
+  const size_t sq_bytes = ((size_t)rmax * rmax * 4 + 255) & ~(size_t)255;
+  void *buf = nullptr;
+  int st = ctx_buffer(c, BUF_TRANSFORM, k_bytes + 2 * sq_bytes + (size_t)rmax * sizeof(int) + 256,
+                      &buf);
+  if (st) return st;
+  uint8_t *b8 = static_cast<uint8_t *>(buf);
+  uint32_t *Lk = reinterpret_cast<uint32_t *>(b8);
+  uint32_t *T = reinterpret_cast<uint32_t *>(b8 + k_bytes);
+  uint32_t *W = reinterpret_cast<uint32_t *>(b8 + k_bytes + sq_bytes);
+  int *d_piv = reinterpret_cast<int *>(b8 + k_bytes + 2 * sq_bytes);
+  std::vector<int> piv;
+  if (n > 0) {
+    EchelonKeep keep;
+    keep.L = Lk;
+    keep.ldL = (size_t)rmax;
+    if ((st = zp_echelon_dev(c, m, n, p, D, ld, rank, det, &piv, &keep))) return st;
+    for (const auto &sw : keep.swaps)
+      if (sw.first != sw.second) P->push_back(sw);  // in the order applied
+  }
+  const int r = (int)*rank;
+  cudaError_t e = cudaSuccess;
+  if (r > 0)
+    e = cudaMemcpyAsync(d_piv, piv.data(), (size_t)r * sizeof(int), cudaMemcpyHostToDevice,
+                        c->stream);
+  if (e != cudaSuccess) return ctx_cuda(c, e, "transform: pivot columns");
+  {
+    const size_t total = (size_t)m * m + 2 * (size_t)r * r;
+    const int grid = (int)std::min<size_t>((total + 255) / 256, (size_t)c->num_sms * 16);
+    transform_setup_kernel<<<grid, 256, 0, c->stream>>>(Lk, (size_t)rmax, D, ld, d_piv, m, r, T,
+                                                        W, Lout, ldl);
+    ctx_launched(c);
+    if ((e = cudaGetLastError()) != cudaSuccess) return ctx_cuda(c, e, "transform: set-up");
+  }
+  if (r > 0) {
+    size_t bad = 0;
+    if ((st = zp_trsm_dev(c, false, true, r, r, p, 1u, T, (size_t)r, Lout, ldl, &bad))) return st;
+    if (m > r &&
+        (st = zp_gemm_dev(c, GEMM_AUTO, m - r, r, r, p, p - 1, Lk + (size_t)r * rmax, (size_t)rmax,
+                          Lout, ldl, 0u, Lout + (size_t)r * ldl, ldl, nullptr)))
+      return st;
+    if ((st = zp_trsm_dev(c, true, false, r, r, p, 1u, W, (size_t)r, Lout, ldl, &bad))) return st;
+    if ((st = zp_trsm_dev(c, true, false, r, n, p, 1u, W, (size_t)r, D, ld, &bad))) return st;
+  }
+  // the host vector piv must outlive the copy above
+  e = cudaStreamSynchronize(c->stream);
+  return e == cudaSuccess ? ST_OK : ctx_cuda(c, e, "transform");
+}
+
 }  // namespace lela

@@ -35,6 +35,15 @@ int zp_pluq_dev(Ctx *c, int m, int n, uint32_t p, uint32_t *D, size_t ld,
                 std::vector<std::pair<int, int>> *P, std::vector<std::pair<int, int>> *Q,
                 size_t *rank, uint32_t *det);
 
+// The standard method's reduced form (pivots 1) of D in place with its
+// transform, as Elimination::echelonize_reduced (A, L, P, rank, det, true)
+// leaves them: Lout (m x m, leading dimension ldl) with R = Lout P D_in, P
+// the row transpositions in the order applied.  p < 2^31 (ST_ARG above);
+// ST_PIVOT when a pivot is not invertible.
+int zp_echelon_transform_dev(Ctx *c, int m, int n, uint32_t p, uint32_t *D, size_t ld,
+                             uint32_t *Lout, size_t ldl, std::vector<std::pair<int, int>> *P,
+                             size_t *rank, uint32_t *det);
+
 // Reduced row-echelon form of D in place as LELA's GaussJordan::
 // echelonize_reduced leaves it (pivots keep their values; zero above and
 // below them), or with unit_pivots as Elimination::echelonize_reduced does
