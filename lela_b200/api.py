@@ -430,12 +430,31 @@ class CudaModule:
         pairs = lambda X, c: [(int(X[2 * t]), int(X[2 * t + 1])) for t in range(c)]
         return A, pairs(P, np_.value), pairs(Q, nq.value), r.value, d.value
 
-    def echelon_reduced_transform(self, p, A, L=None):
+    def echelon_reduced_transform(self, p, A, L=None, unit_pivots=True):
         """Elimination::echelonize_reduced (A, L, P, rank, det, compute_L =
         true): A <- its reduced form with unit pivots, in place; returns (A,
         L, P, rank, det) with A_out = L P A_in, L m x m, and P a list of
         transposition pairs in the order applied.  Host numpy uint32 matrix,
-        or torch CUDA tensor (then L is a device tensor too).  p < 2^31."""
+        or torch CUDA tensor (then L is a device tensor too).  p < 2^31.
+
+        unit_pivots=False: GaussJordan::echelonize_reduced (A, L, P, rank,
+        det) instead (lela/algorithms/gauss-jordan.tcc:434-466), whose
+        pivots keep their values.  Its transposition list is the standard
+        method's, and its pivot rows of A and L are the standard method's
+        multiplied by their pivots (GaussJordanTransform's leaf leaves the
+        pivot row as it is, :74-107).  So it is the standard form, with the
+        pivots read from the fast method's reduced form
+        (lela_cuda_echelon_reduced_zp_u32 with unit_pivots = 0) of the same
+        input.  Host arrays only."""
+        if not unit_pivots:
+            _check(not _is_torch(A), "echelon_reduced_transform: the fast method's form takes host arrays")
+            A0 = np.array(A, dtype=np.uint32, copy=True)
+            A, L, P, r, d = self.echelon_reduced_transform(p, A, L)
+            if r:
+                Rg, _, _ = self.echelonize(p, A0, reduced=True, unit_pivots=False)
+                A[:r] = Rg[:r]
+                scale_pivot_rows(p, L, Rg, r)
+            return A, L, P, r, d
         m, n = A.shape
         P = np.zeros(2 * max(min(m, n), 1), dtype=np.uint64)
         np_, r, d = _S(0), _S(0), _U(0)
@@ -628,6 +647,16 @@ class CudaModule:
 
 def _is_torch(x):
     return type(x).__module__.startswith("torch")
+
+
+def scale_pivot_rows(p, L, R, r):
+    """L[i] <- x_i L[i] mod p for i < r, in place, x_i the leading entry of
+    row i of R (a reduced echelon form whose first r rows are its pivot
+    rows)."""
+    for i in range(r):
+        nz = np.flatnonzero(R[i])
+        x = np.uint64(R[i, nz[0]])
+        L[i] = (L[i].astype(np.uint64) * x % np.uint64(p)).astype(np.uint32)
 
 
 def _check(cond, msg):

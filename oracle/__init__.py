@@ -59,6 +59,8 @@ def lib():
                                          ctypes.POINTER(_S), ctypes.POINTER(_U)]
         L.oracle_echelon_reduced_L_zp_u32.argtypes = [_U, _S, _S, _P, _S, _P, _S, _P, ctypes.POINTER(_S),
                                                       ctypes.POINTER(_S), ctypes.POINTER(_U)]
+        L.oracle_gj_echelon_reduced_L_zp_u32.argtypes = [_U, _S, _S, _P, _S, _P, _S, _P, ctypes.POINTER(_S),
+                                                         ctypes.POINTER(_S), ctypes.POINTER(_U)]
         L.oracle_inv_zp.argtypes = [_U, _U]
         L.oracle_inv_zp.restype = _U
         _lib = L
@@ -104,6 +106,9 @@ def ref():
         L.lela_ref_elim_echelon_reduced_L_zp_u32.argtypes = [_U, _S, _S, _P, _S, _P, _S, _P,
                                                              ctypes.POINTER(_S), ctypes.POINTER(_S),
                                                              ctypes.POINTER(_U)]
+        L.lela_ref_gj_echelon_reduced_L_zp_u32.argtypes = [_U, _S, _S, _P, _S, _P, _S, _P,
+                                                           ctypes.POINTER(_S), ctypes.POINTER(_S),
+                                                           ctypes.POINTER(_U)]
         _ref = L
     return _ref
 
@@ -232,6 +237,12 @@ def echelon_reduced_L_zp(p, A):
     """Elimination::echelonize_reduced with compute_L, restated:
     (R, L, P, rank, det) with R = L P A."""
     return _echelon_L(lib().oracle_echelon_reduced_L_zp_u32, p, A)
+
+
+def gj_echelon_reduced_L_zp(p, A):
+    """GaussJordan::echelonize_reduced with its transform, restated:
+    (R, L, P, rank, det) with R = L P A, pivots keeping their values."""
+    return _echelon_L(lib().oracle_gj_echelon_reduced_L_zp_u32, p, A)
 
 
 def fl_echelonize_zp(p, m, n, rowptr, colidx, vals, reduced=True, only_D=False):
@@ -413,3 +424,9 @@ def ref_echelon_reduced_L_zp(p, A):
     """Elimination::echelonize_reduced with compute_L (LELA):
     (R, L, P, rank, det)."""
     return _echelon_L(ref().lela_ref_elim_echelon_reduced_L_zp_u32, p, A)
+
+
+def ref_gj_echelon_reduced_L_zp(p, A):
+    """GaussJordan::echelonize_reduced with its transform (LELA):
+    (R, L, P, rank, det)."""
+    return _echelon_L(ref().lela_ref_gj_echelon_reduced_L_zp_u32, p, A)

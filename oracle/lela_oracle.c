@@ -335,9 +335,9 @@ int oracle_echelon_reduced_unit_zp_u32 (uint32_t p, size_t m, size_t n, uint32_t
  * A = L P A_in, P the transpositions applied in order.  P holds them as
  * pairs in the reference's order (not reversed).  Returns 0, or -1 when a
  * pivot is not invertible (the reference throws). */
-int oracle_echelon_reduced_L_zp_u32 (uint32_t p, size_t m, size_t n, uint32_t *A, size_t lda,
-				     uint32_t *L, size_t ldl, size_t *P, size_t *np,
-				     size_t *rank, uint32_t *det)
+static int echelon_reduced_L (uint32_t p, size_t m, size_t n, uint32_t *A, size_t lda,
+			      uint32_t *L, size_t ldl, size_t *P, size_t *np,
+			      size_t *rank, uint32_t *det, uint32_t *pivots)
 {
 	size_t i, c, npp = 0;
 	uint32_t d = 1 % p;
@@ -374,6 +374,8 @@ int oracle_echelon_reduced_L_zp_u32 (uint32_t p, size_t m, size_t n, uint32_t *A
 		}
 		uint32_t x = A[i * lda + pc];
 		d = mulmod (p, d, x);
+		if (pivots)
+			pivots[i] = x;
 		uint32_t xinv = oracle_inv_zp (p, x);
 		if (xinv == 0)
 			return -1;
@@ -396,6 +398,42 @@ int oracle_echelon_reduced_L_zp_u32 (uint32_t p, size_t m, size_t n, uint32_t *A
 	*rank = i;
 	*det = d;
 	return 0;
+}
+
+int oracle_echelon_reduced_L_zp_u32 (uint32_t p, size_t m, size_t n, uint32_t *A, size_t lda,
+				     uint32_t *L, size_t ldl, size_t *P, size_t *np,
+				     size_t *rank, uint32_t *det)
+{
+	return echelon_reduced_L (p, m, n, A, lda, L, ldl, P, np, rank, det, NULL);
+}
+
+/* The fast method's reduced form with its transform,
+ * GaussJordan::echelonize_reduced (A, L, P, rank, det) (lela/algorithms/
+ * gauss-jordan.tcc:434-466) through GaussJordanTransform (:27-230).  The
+ * recursion takes the same pivots and transpositions, in the same order, as
+ * the standard method above; its leaf clears the pivot column in every
+ * other row and writes the multipliers into the transform's column k, but
+ * leaves the pivot row and the transform's diagonal entry as they are
+ * (:74-107).  So the result differs from the standard method's only in the
+ * pivot rows: R_i and L_i of the fast method are x_i R_i and x_i L_i of the
+ * standard one (x_i the i-th pivot), which is how it is restated here.
+ * Returns 0, or -1 when a pivot is not invertible. */
+int oracle_gj_echelon_reduced_L_zp_u32 (uint32_t p, size_t m, size_t n, uint32_t *A, size_t lda,
+					uint32_t *L, size_t ldl, size_t *P, size_t *np,
+					size_t *rank, uint32_t *det)
+{
+	size_t k = m < n ? m : n;
+	uint32_t *x = (uint32_t *) malloc ((k ? k : 1) * sizeof (uint32_t));
+	int rc = echelon_reduced_L (p, m, n, A, lda, L, ldl, P, np, rank, det, x);
+	if (rc == 0)
+		for (size_t i = 0; i < *rank; ++i) {
+			for (size_t c = 0; c < n; ++c)
+				A[i * lda + c] = mulmod (p, A[i * lda + c], x[i]);
+			for (size_t c = 0; c < m; ++c)
+				L[i * ldl + c] = mulmod (p, L[i * ldl + c], x[i]);
+		}
+	free (x);
+	return rc;
 }
 
 /* PLUQ decomposition, Elimination::pluq (lela/algorithms/elimination.tcc:

@@ -62,6 +62,13 @@ int oracle_echelon_reduced_L_zp_u32 (uint32_t p, size_t m, size_t n, uint32_t *A
 				     uint32_t *L, size_t ldl, size_t *P, size_t *np,
 				     size_t *rank, uint32_t *det);
 
+/* The fast method's reduced form (pivots keep their values) with its
+ * transform: the same with every pivot row of A and L multiplied by its
+ * pivot; R = L P A_in as above. */
+int oracle_gj_echelon_reduced_L_zp_u32 (uint32_t p, size_t m, size_t n, uint32_t *A, size_t lda,
+					uint32_t *L, size_t ldl, size_t *P, size_t *np,
+					size_t *rank, uint32_t *det);
+
 /* PLUQ decomposition in place (L strictly below the diagonal, U on and
  * above it); P and Q as transposition pairs (at most min(m, n) each), in
  * the reference's order; rank, det = product of the pivots.  Returns 0, or

@@ -408,6 +408,44 @@ int lela_ref_elim_echelon_reduced_L_zp_u32 (uint32_t p, size_t m, size_t n, uint
 	return 0;
 }
 
+/* GaussJordan::echelonize_reduced (A, L, P, rank, det) (lela/algorithms/
+ * gauss-jordan.tcc:434-466, through GaussJordanTransform :27-230): A <- its
+ * reduced form (pivots keep their values), L (m x m, dense) <- the
+ * transform with A_out = L P A_in, P the row transpositions as pairs in the
+ * reference's order (at most min(m, n)).  det = the product of the pivots,
+ * taken from the leading entries as lela_ref_echelon_reduced_zp_u32 does.
+ * Returns 0, or -1 when a pivot is not invertible. */
+int lela_ref_gj_echelon_reduced_L_zp_u32 (uint32_t p, size_t m, size_t n, uint32_t *A, size_t lda, uint32_t *L, size_t ldl, size_t *P, size_t *np, size_t *rank, uint32_t *det)
+{
+	Zp F (p);
+	Context<Zp> ctx (F);
+	DenseMatrix<uint32> MA (m, n), ML (m, m);
+	if (m && n) load_dense (MA, A, lda);
+	GaussJordan<Zp> GJ (ctx);
+	GaussJordan<Zp>::Permutation PP;
+	size_t r = 0;
+	Zp::Element d;
+	try {
+		GJ.echelonize_reduced (MA, ML, PP, r, d);
+	} catch (...) {
+		return -1;
+	}
+	if (m && n) store_dense (MA, A, lda);
+	if (m) store_dense (ML, L, ldl);
+	for (size_t k = 0; k < PP.size (); ++k) { P[2 * k] = PP[k].first; P[2 * k + 1] = PP[k].second; }
+	*np = PP.size ();
+	*rank = r;
+	Zp::Element pd = 1;
+	for (size_t i = 0; i < r; ++i) {
+		size_t c = 0;
+		while (c < n && MA[i][c] == 0) ++c;
+		if (c < n) F.mulin (pd, MA[i][c]);
+	}
+	*det = pd;
+	(void) d;
+	return 0;
+}
+
 /* Elimination::pluq (lela/algorithms/elimination.tcc:266-370) with the
  * default pivot strategy of a dense row: A <- L and U in place (L strictly
  * below the diagonal, unit diagonal implied), P and Q the row and column

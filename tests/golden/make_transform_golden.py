@@ -1,7 +1,8 @@
-"""Generate tests/golden/transform_golden.npz from LELA's own CPU code:
-Elimination::echelonize_reduced (A, L, P, rank, det, compute_L = true)
-(lela/algorithms/elimination.tcc:143-265) through
-oracle/_ref/liblela_ref.so.
+"""Generate tests/golden/transform_golden.npz and gj_transform_golden.npz
+from LELA's own CPU code: Elimination::echelonize_reduced (A, L, P, rank,
+det, compute_L = true) (lela/algorithms/elimination.tcc:143-265), and
+GaussJordan::echelonize_reduced (A, L, P, rank, det) (lela/algorithms/
+gauss-jordan.tcc:434-466), through oracle/_ref/liblela_ref.so.
 
     python tests/golden/make_transform_golden.py
 
@@ -43,8 +44,7 @@ def case_matrix(seed, m, n, p, kind):
     return A
 
 
-def main():
-    assert oracle.have_ref(), "build oracle/_ref first (make -C oracle ref)"
+def write(fn, fname):
     out = {}
     names = []
     for pi, p in enumerate(MODULI):
@@ -56,7 +56,7 @@ def main():
                 A = case_matrix(seed, m, n, p, kind)
                 pre = "tl%d_%d_%d_" % (pi, si, kind)
                 try:
-                    R, L, P, r, d = oracle.ref_echelon_reduced_L_zp(p, A)
+                    R, L, P, r, d = fn(p, A)
                     st = 0
                 except ArithmeticError:
                     R, L, P, r, d, st = np.zeros_like(A), np.zeros((m, m), np.uint32), [], 0, 0, -1
@@ -67,8 +67,15 @@ def main():
                 out[pre + "P"] = np.array(P, dtype=np.int64).reshape(-1, 2)
                 names.append(pre)
     out["names"] = np.array(names)
-    np.savez_compressed(os.path.join(HERE, "transform_golden.npz"), **out)
-    print("%d cases, %d LELA failures" % (len(names), sum(int(out[n + "meta"][1] != 0) for n in names)))
+    np.savez_compressed(os.path.join(HERE, fname), **out)
+    print("%s: %d cases, %d LELA failures" % (fname, len(names),
+                                              sum(int(out[n + "meta"][1] != 0) for n in names)))
+
+
+def main():
+    assert oracle.have_ref(), "build oracle/_ref first (make -C oracle ref)"
+    write(oracle.ref_echelon_reduced_L_zp, "transform_golden.npz")
+    write(oracle.ref_gj_echelon_reduced_L_zp, "gj_transform_golden.npz")
 
 
 if __name__ == "__main__":

@@ -86,13 +86,15 @@ def gf2_echelon_cases():
         yield pre, m, n, r, z[pre + "A"], z[pre + "E"]
 
 
-def transform_cases():
-    """Elimination::echelonize_reduced with compute_L, as LELA computed it
+def transform_cases(gj=False):
+    """Elimination::echelonize_reduced with compute_L (gj: GaussJordan::
+    echelonize_reduced with its transform), as LELA computed it
     (tests/golden/make_transform_golden.py): (pre, p, status, rank, det, A,
     R, L, P)."""
-    if "transform" not in _cache:
-        _cache["transform"] = dict(np.load(os.path.join(HERE, "transform_golden.npz")))
-    z = _cache["transform"]
+    fname = "gj_transform_golden.npz" if gj else "transform_golden.npz"
+    if fname not in _cache:
+        _cache[fname] = dict(np.load(os.path.join(HERE, fname)))
+    z = _cache[fname]
     for pre in z["names"]:
         pre = str(pre)
         p, st, r, d = (int(x) for x in z[pre + "meta"])

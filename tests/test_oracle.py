@@ -88,6 +88,41 @@ def test_golden_transform():
     assert n >= 100
 
 
+def test_golden_gj_transform():
+    """GaussJordan::echelonize_reduced with its transform: R, L, P, rank, det
+    and LELA's failures, against LELA's own results."""
+    n = 0
+    for pre, p, st, r, d, A, R, L, P in golden_io.transform_cases(gj=True):
+        if st:
+            with pytest.raises(ArithmeticError):
+                oracle.gj_echelon_reduced_L_zp(p, A)
+            continue
+        if p >= 2 ** 31:
+            continue  # LELA's wrapped inverses; the GPU form rejects such p
+        gR, gL, gP, gr, gd = oracle.gj_echelon_reduced_L_zp(p, A)
+        assert (gr, gd) == (r, d) and gP == P, pre
+        assert np.array_equal(gR, R) and np.array_equal(gL, L), pre
+        n += 1
+    assert n >= 80
+
+
+def test_gj_scaling_of_the_standard_transform():
+    """The Python mirror's fast-method form: the standard transform with
+    each pivot row scaled by its pivot, the pivots read from the fast
+    method's reduced form, gives LELA's GaussJordan transform."""
+    from lela_b200.api import scale_pivot_rows
+    n = 0
+    for pre, p, st, r, d, A, R, L, P in golden_io.transform_cases(gj=True):
+        if st or p >= 2 ** 31:
+            continue
+        _, Le, Pe, re, de = oracle.echelon_reduced_L_zp(p, A)
+        Rg, _, _ = oracle.echelon_reduced_zp(p, A)
+        scale_pivot_rows(p, Le, Rg, re)
+        assert np.array_equal(Le, L) and Pe == P and (re, de) == (r, d), pre
+        n += 1
+    assert n >= 80
+
+
 def test_transform_identity():
     """R = L P A, with L = [[X, 0], [Y, I]] in the rank's blocks, and R the
     standard method's reduced form (p < 2^31, where Modular<uint32>'s
@@ -376,5 +411,37 @@ def test_live_transform(p):
                 got = None
             assert (want is None) == (got is None), (m, n, kind)
             if want is not None:
+                assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1]), (m, n, kind)
+                assert got[2:] == want[2:], (m, n, kind)
+
+
+@need_ref
+@pytest.mark.parametrize("p", [2, 3, 251, 65521, 65536, 2147483647, 4294967291])
+def test_live_gj_transform(p):
+    """GaussJordan::echelonize_reduced with its transform against the
+    restatement (below 2^31; above it whether LELA fails must agree)."""
+    rng = np.random.default_rng(p % 977)
+    for (m, n) in ((1, 1), (2, 7), (7, 13), (13, 7), (40, 40), (48, 80), (80, 48)):
+        for kind in range(4):
+            A = gen.dense_zp(int(rng.integers(1 << 30)), m, n, p)
+            if kind == 1:
+                A[:, ::3] = 0
+            elif kind == 2:
+                r = max(1, min(m, n) // 3)
+                F = gen.dense_zp(1, m, r, p).astype(object) @ gen.dense_zp(2, r, n, p).astype(object)
+                A = (F % p).astype(np.uint32)
+            elif kind == 3:
+                A[m // 2:] = 0
+                A[:, :n // 2] = 0
+            try:
+                want = oracle.ref_gj_echelon_reduced_L_zp(p, A)
+            except ArithmeticError:
+                want = None
+            try:
+                got = oracle.gj_echelon_reduced_L_zp(p, A)
+            except ArithmeticError:
+                got = None
+            assert (want is None) == (got is None), (m, n, kind)
+            if want is not None and p < 2 ** 31:
                 assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1]), (m, n, kind)
                 assert got[2:] == want[2:], (m, n, kind)
