@@ -12,6 +12,7 @@ NumPy arrays are host matrices (uint32 for Z/p, uint64 words for GF(2));
 torch CUDA tensors are device matrices and take the ``*_dev`` entry points.
 Status codes become LELA's exceptions.
 """
+import bisect
 import ctypes
 import os
 
@@ -407,6 +408,43 @@ class CudaModule:
         return A, r.value, d.value
 
 
+    def echelonize_with_L(self, p, A, gauss_jordan=False):
+        """Elimination::echelonize (A, P, rank, det) with its default
+        compute_L = true (lela/algorithms/elimination.h:86-92,
+        elimination.tcc:47-139), or with gauss_jordan GaussJordan::
+        echelonize (A, P, rank, det) (gauss-jordan.tcc:413-432), in place:
+        A <- the non-reduced form U with, below the diagonal, the strictly
+        lower part of the unit lower triangular T with T P A_in = U; returns
+        (A, P, rank, det), P the transpositions in the order applied.  Both
+        give the same A and P; det is the product of the pivots for
+        Elimination and GaussTransform's d for GaussJordan
+        (gauss_transform_det).
+
+        In blocks of rank rows T = [[L1^-1, 0], [-L2 L1^-1, I]] (B = P A =
+        [L1; L2] U), so its bottom block is that of the reduced form's
+        transform and its top block is U_P X, X the reduced transform's top
+        block (X = U_P^-1 L1^-1, U_P the pivot columns of U).  Computed from
+        the GPU's reduced transform, its non-reduced form and one gemm.
+        Host arrays only; p < 2^31."""
+        _check(not _is_torch(A), "echelonize_with_L takes host arrays")
+        _check(A.dtype == np.uint32, "echelonize_with_L: uint32 matrix expected")
+        m, n = A.shape
+        _, T, P, r, d = self.echelon_reduced_transform(p, np.array(A, dtype=np.uint32, copy=True))
+        if r == 0:
+            return A, P, r, (1 % p if gauss_jordan else d)
+        self.echelonize(p, A)
+        piv = [int(np.flatnonzero(A[i])[0]) for i in range(r)]
+        vals = [int(A[i, c]) for i, c in enumerate(piv)]
+        UP = np.ascontiguousarray(A[:r][:, piv])
+        X = np.ascontiguousarray(T[:r, :r])
+        T11 = self.gemm(p, 1, UP, X, 0, np.zeros((r, r), dtype=np.uint32))
+        for i in range(1, r):
+            A[i, :i] = T11[i, :i]
+        A[r:, :r] = T[r:, :r]
+        if gauss_jordan:
+            d = gauss_transform_det(p, n, piv, vals)
+        return A, P, r, d
+
     def pluq(self, p, A):
         """Elimination::pluq in place: A <- L below the diagonal and U on and
         above it (columns in Q's order); returns (A, P, Q, rank, det) with P
@@ -647,6 +685,32 @@ class CudaModule:
 
 def _is_torch(x):
     return type(x).__module__.startswith("torch")
+
+
+def gauss_transform_det(p, n, pivot_cols, pivot_vals):
+    """The determinant GaussJordan::echelonize returns (lela/algorithms/
+    gauss-jordan.tcc:232-411, GaussTransform's d), from the pivot columns
+    (increasing) and pivot values of the non-reduced form.  The recursion
+    halves the columns; a block without a pivot is zero and copies d_0 into
+    d, a one-column block multiplies d by its pivot, and a wider block runs
+    its left half with d_0 into d_1 = 1 and its right half with d_1 as d_0
+    into d.  The top call has d_0 = d = 1."""
+    cols = list(pivot_cols)
+    val = dict(zip(cols, pivot_vals))
+
+    def has(c0, c1):
+        i = bisect.bisect_left(cols, c0)
+        return i < len(cols) and cols[i] < c1
+
+    def rec(c0, c1, d0, d):
+        if not has(c0, c1):
+            return d0
+        if c1 - c0 == 1:
+            return d * val[c0] % p
+        m1 = (c1 - c0) // 2
+        return rec(c0 + m1, c1, rec(c0, c0 + m1, d0, 1 % p), d)
+
+    return rec(0, n, 1 % p, 1 % p) if n else 1 % p
 
 
 def scale_pivot_rows(p, L, R, r):

@@ -61,6 +61,8 @@ def lib():
                                                       ctypes.POINTER(_S), ctypes.POINTER(_U)]
         L.oracle_gj_echelon_reduced_L_zp_u32.argtypes = [_U, _S, _S, _P, _S, _P, _S, _P, ctypes.POINTER(_S),
                                                          ctypes.POINTER(_S), ctypes.POINTER(_U)]
+        L.oracle_echelon_packed_L_zp_u32.argtypes = [_I, _U, _S, _S, _P, _S, _P, ctypes.POINTER(_S),
+                                                     ctypes.POINTER(_S), ctypes.POINTER(_U)]
         L.oracle_inv_zp.argtypes = [_U, _U]
         L.oracle_inv_zp.restype = _U
         _lib = L
@@ -109,6 +111,8 @@ def ref():
         L.lela_ref_gj_echelon_reduced_L_zp_u32.argtypes = [_U, _S, _S, _P, _S, _P, _S, _P,
                                                            ctypes.POINTER(_S), ctypes.POINTER(_S),
                                                            ctypes.POINTER(_U)]
+        L.lela_ref_echelon_packed_L_zp_u32.argtypes = [_I, _U, _S, _S, _P, _S, _P, ctypes.POINTER(_S),
+                                                       ctypes.POINTER(_S), ctypes.POINTER(_U)]
         _ref = L
     return _ref
 
@@ -237,6 +241,22 @@ def echelon_reduced_L_zp(p, A):
     """Elimination::echelonize_reduced with compute_L, restated:
     (R, L, P, rank, det) with R = L P A."""
     return _echelon_L(lib().oracle_echelon_reduced_L_zp_u32, p, A)
+
+
+def _packed(fn, gj, p, A):
+    A = _c(A, np.uint32).copy()
+    m, n = A.shape
+    P = np.zeros(2 * max(min(m, n), 1), dtype=np.uint64)
+    np_ = _S(0); r = _S(0); d = _U(0)
+    if fn(gj, p, m, n, _ptr(A), max(n, 1), _ptr(P), ctypes.byref(np_), ctypes.byref(r), ctypes.byref(d)):
+        raise ArithmeticError("pivot not invertible")
+    return A, [(int(P[2 * t]), int(P[2 * t + 1])) for t in range(np_.value)], r.value, d.value
+
+
+def echelon_packed_L_zp(p, A, gauss_jordan=False):
+    """Elimination::echelonize (gauss_jordan: GaussJordan::echelonize) with
+    L kept below the diagonal, restated: (A, P, rank, det)."""
+    return _packed(lib().oracle_echelon_packed_L_zp_u32, int(gauss_jordan), p, A)
 
 
 def gj_echelon_reduced_L_zp(p, A):
@@ -424,6 +444,12 @@ def ref_echelon_reduced_L_zp(p, A):
     """Elimination::echelonize_reduced with compute_L (LELA):
     (R, L, P, rank, det)."""
     return _echelon_L(ref().lela_ref_elim_echelon_reduced_L_zp_u32, p, A)
+
+
+def ref_echelon_packed_L_zp(p, A, gauss_jordan=False):
+    """Elimination::echelonize / GaussJordan::echelonize with L kept below
+    the diagonal (LELA): (A, P, rank, det)."""
+    return _packed(ref().lela_ref_echelon_packed_L_zp_u32, int(gauss_jordan), p, A)
 
 
 def ref_gj_echelon_reduced_L_zp(p, A):

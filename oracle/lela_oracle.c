@@ -436,6 +436,92 @@ int oracle_gj_echelon_reduced_L_zp_u32 (uint32_t p, size_t m, size_t n, uint32_t
 	return rc;
 }
 
+/* GaussTransform's d (lela/algorithms/gauss-jordan.tcc:232-411) over the
+ * column range [c0, c1), from the pivots alone: a block with no pivot
+ * copies d_0 into d (:243-247: the block is zero), a one-column block
+ * multiplies d by its pivot (:259), and a wider block runs its left half
+ * with d_0 into d_1 = 1 and its right half with d_1 as d_0 into d
+ * (:300-343).  pcol[] (increasing) and pval[] are the r pivots. */
+static uint32_t gj_det_rec (uint32_t p, size_t c0, size_t c1, uint32_t d0, uint32_t d,
+			    const size_t *pcol, const uint32_t *pval, size_t r)
+{
+	size_t lo = 0, hi = r;
+	while (lo < hi) {  /* first pivot column >= c0 */
+		size_t mid = (lo + hi) / 2;
+		if (pcol[mid] < c0) lo = mid + 1; else hi = mid;
+	}
+	if (lo == r || pcol[lo] >= c1)
+		return d0;
+	if (c1 - c0 == 1)
+		return mulmod (p, d, pval[lo]);
+	size_t m1 = (c1 - c0) / 2;
+	uint32_t d1 = gj_det_rec (p, c0, c0 + m1, d0, 1 % p, pcol, pval, r);
+	return gj_det_rec (p, c0 + m1, c1, d1, d, pcol, pval, r);
+}
+
+/* The non-reduced forms that keep L below the diagonal of A.
+ * gj = 0: Elimination::echelonize (A, P, rank, det) with its default
+ * compute_L = true (lela/algorithms/elimination.h:86-92, elimination.tcc:
+ * 47-139), step by step: the pivot rule and transpositions as above; every
+ * row j below with a nonzero a in the pivot column gets row j <- row j +
+ * (-a/x) row i over the whole row (the L entries left of column i included,
+ * :113), then (j, i) <- -a/x (:115-116).  det = product of the pivots.
+ * gj = 1: GaussJordan::echelonize (A, P, rank, det) (gauss-jordan.tcc:
+ * 413-432): the same A and P (its transform stores the same multipliers),
+ * and GaussTransform's d (gj_det_rec).  P as pairs in the order applied.
+ * Returns 0, or -1 when a pivot is not invertible. */
+int oracle_echelon_packed_L_zp_u32 (int gj, uint32_t p, size_t m, size_t n, uint32_t *A,
+				    size_t lda, size_t *P, size_t *np, size_t *rank, uint32_t *det)
+{
+	size_t k = m < n ? m : n, i, c, npp = 0, pc = 0;
+	size_t *pcol = (size_t *) malloc ((k ? k : 1) * sizeof (size_t));
+	uint32_t *pval = (uint32_t *) malloc ((k ? k : 1) * sizeof (uint32_t));
+	uint32_t d = 1 % p;
+	int rc = 0;
+	for (i = 0; i < m && pc < n; ++i, ++pc) {
+		size_t prow = m;
+		for (; pc < n; ++pc) {
+			for (size_t r = i; r < m; ++r)
+				if (A[r * lda + pc] != 0) { prow = r; break; }
+			if (prow < m) break;
+		}
+		if (prow == m)
+			break;
+		if (prow != i) {
+			for (c = 0; c < n; ++c) {
+				uint32_t t = A[i * lda + c];
+				A[i * lda + c] = A[prow * lda + c];
+				A[prow * lda + c] = t;
+			}
+			P[2 * npp] = i; P[2 * npp + 1] = prow; ++npp;
+		}
+		uint32_t x = A[i * lda + pc];
+		pcol[i] = pc;
+		pval[i] = x;
+		d = mulmod (p, d, x);
+		uint32_t xinv = oracle_inv_zp (p, x);
+		if (xinv == 0) { rc = -1; break; }
+		uint32_t negxinv = (p - xinv) % p;
+		for (size_t j = i + 1; j < m; ++j) {
+			uint32_t a = A[j * lda + pc];
+			if (a == 0)
+				continue;
+			uint32_t f = mulmod (p, a, negxinv);
+			for (c = 0; c < n; ++c)
+				A[j * lda + c] = axpy_mod (p, A[j * lda + c], f, A[i * lda + c]);
+			A[j * lda + i] = f;
+		}
+	}
+	if (rc == 0) {
+		*np = npp;
+		*rank = i;
+		*det = gj ? gj_det_rec (p, 0, n, 1 % p, 1 % p, pcol, pval, i) : d;
+	}
+	free (pcol);
+	free (pval);
+	return rc;
+}
+
 /* PLUQ decomposition, Elimination::pluq (lela/algorithms/elimination.tcc:
  * 266-370) with DensePivotStrategy (lela/algorithms/pivot-strategy.tcc:
  * 19-42).  Step i: the first column from i on, in the current column

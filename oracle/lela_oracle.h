@@ -69,6 +69,15 @@ int oracle_gj_echelon_reduced_L_zp_u32 (uint32_t p, size_t m, size_t n, uint32_t
 					uint32_t *L, size_t ldl, size_t *P, size_t *np,
 					size_t *rank, uint32_t *det);
 
+/* Non-reduced row echelon form with L kept below the diagonal: A <- U plus
+ * the strictly lower part of the transform T (T P A_in = U); gj = 0 as
+ * Elimination::echelonize (det = product of the pivots), gj = 1 as
+ * GaussJordan::echelonize (the same A and P; det as GaussTransform computes
+ * it).  P as pairs in the order applied.  Returns 0, or -1 when a pivot is
+ * not invertible mod p. */
+int oracle_echelon_packed_L_zp_u32 (int gj, uint32_t p, size_t m, size_t n, uint32_t *A,
+				    size_t lda, size_t *P, size_t *np, size_t *rank, uint32_t *det);
+
 /* PLUQ decomposition in place (L strictly below the diagonal, U on and
  * above it); P and Q as transposition pairs (at most min(m, n) each), in
  * the reference's order; rank, det = product of the pivots.  Returns 0, or

@@ -408,6 +408,42 @@ int lela_ref_elim_echelon_reduced_L_zp_u32 (uint32_t p, size_t m, size_t n, uint
 	return 0;
 }
 
+/* The non-reduced forms with L kept in A's lower part: gj = 0 runs
+ * Elimination::echelonize (A, P, rank, det) with its default compute_L =
+ * true (lela/algorithms/elimination.h:86-92, elimination.tcc:47-139: each
+ * multiplier is written to (j, i) as the rows are eliminated); gj = 1 runs
+ * GaussJordan::echelonize (A, P, rank, det) (lela/algorithms/
+ * gauss-jordan.tcc:413-432, GaussTransform :232-411), which also leaves L
+ * below the diagonal (gauss-jordan.h:92-104).  P as pairs in the
+ * reference's order.  Returns 0, or -1 when a pivot is not invertible. */
+int lela_ref_echelon_packed_L_zp_u32 (int gj, uint32_t p, size_t m, size_t n, uint32_t *A, size_t lda, size_t *P, size_t *np, size_t *rank, uint32_t *det)
+{
+	Zp F (p);
+	Context<Zp> ctx (F);
+	DenseMatrix<uint32> MA (m, n);
+	if (m && n) load_dense (MA, A, lda);
+	Elimination<Zp>::Permutation PP;
+	size_t r = 0;
+	Zp::Element d;
+	try {
+		if (gj) {
+			GaussJordan<Zp> GJ (ctx);
+			GJ.echelonize (MA, PP, r, d);
+		} else {
+			Elimination<Zp> elim (ctx);
+			elim.echelonize (MA, PP, r, d);
+		}
+	} catch (...) {
+		return -1;
+	}
+	if (m && n) store_dense (MA, A, lda);
+	for (size_t k = 0; k < PP.size (); ++k) { P[2 * k] = PP[k].first; P[2 * k + 1] = PP[k].second; }
+	*np = PP.size ();
+	*rank = r;
+	*det = d;
+	return 0;
+}
+
 /* GaussJordan::echelonize_reduced (A, L, P, rank, det) (lela/algorithms/
  * gauss-jordan.tcc:434-466, through GaussJordanTransform :27-230): A <- its
  * reduced form (pivots keep their values), L (m x m, dense) <- the

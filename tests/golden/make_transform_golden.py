@@ -1,8 +1,11 @@
-"""Generate tests/golden/transform_golden.npz and gj_transform_golden.npz
-from LELA's own CPU code: Elimination::echelonize_reduced (A, L, P, rank,
-det, compute_L = true) (lela/algorithms/elimination.tcc:143-265), and
-GaussJordan::echelonize_reduced (A, L, P, rank, det) (lela/algorithms/
-gauss-jordan.tcc:434-466), through oracle/_ref/liblela_ref.so.
+"""Generate tests/golden/transform_golden.npz, gj_transform_golden.npz and
+packed_golden.npz from LELA's own CPU code: Elimination::echelonize_reduced
+(A, L, P, rank, det, compute_L = true) (lela/algorithms/elimination.tcc:
+143-265), GaussJordan::echelonize_reduced (A, L, P, rank, det) (lela/
+algorithms/gauss-jordan.tcc:434-466), and the non-reduced forms that keep L
+below the diagonal, Elimination::echelonize (A, P, rank, det) with its
+default compute_L and GaussJordan::echelonize (A, P, rank, det), through
+oracle/_ref/liblela_ref.so.
 
     python tests/golden/make_transform_golden.py
 
@@ -72,10 +75,42 @@ def write(fn, fname):
                                               sum(int(out[n + "meta"][1] != 0) for n in names)))
 
 
+def write_packed(fname):
+    """Both packed forms of each input: prefix pk_..., A once, then for
+    g = 0 (Elimination) and 1 (GaussJordan) meta<g> = [p, status, rank,
+    det], E<g> and P<g>."""
+    out = {}
+    names = []
+    for pi, p in enumerate(MODULI):
+        for si, (m, n) in enumerate(SHAPES):
+            for kind in range(3):
+                if (m == 0 or n == 0) and kind:
+                    continue
+                A = case_matrix(1000 * pi + 10 * si + kind, m, n, p, kind)
+                pre = "pk_%d_%d_%d_" % (pi, si, kind)
+                out[pre + "A"] = A
+                for g in (0, 1):
+                    try:
+                        E, P, r, d = oracle.ref_echelon_packed_L_zp(p, A, gauss_jordan=bool(g))
+                        st = 0
+                    except ArithmeticError:
+                        E, P, r, d, st = np.zeros_like(A), [], 0, 0, -1
+                    out[pre + "meta%d" % g] = np.array([p, st, r, d], dtype=np.int64)
+                    out[pre + "E%d" % g] = E
+                    out[pre + "P%d" % g] = np.array(P, dtype=np.int64).reshape(-1, 2)
+                names.append(pre)
+    out["names"] = np.array(names)
+    np.savez_compressed(os.path.join(HERE, fname), **out)
+    print("%s: %d inputs, %d LELA failures" % (fname, len(names),
+                                               sum(int(out[n + "meta%d" % g][1] != 0)
+                                                   for n in names for g in (0, 1))))
+
+
 def main():
     assert oracle.have_ref(), "build oracle/_ref first (make -C oracle ref)"
     write(oracle.ref_echelon_reduced_L_zp, "transform_golden.npz")
     write(oracle.ref_gj_echelon_reduced_L_zp, "gj_transform_golden.npz")
+    write_packed("packed_golden.npz")
 
 
 if __name__ == "__main__":

@@ -100,3 +100,19 @@ def transform_cases(gj=False):
         p, st, r, d = (int(x) for x in z[pre + "meta"])
         P = [tuple(int(v) for v in t) for t in z[pre + "P"]]
         yield pre, p, st, r, d, z[pre + "A"], z[pre + "R"], z[pre + "L"], P
+
+
+def packed_cases():
+    """Elimination::echelonize / GaussJordan::echelonize with L kept below
+    the diagonal, as LELA computed them (tests/golden/
+    make_transform_golden.py): (pre, gauss_jordan, p, status, rank, det, A,
+    E, P)."""
+    if "packed" not in _cache:
+        _cache["packed"] = dict(np.load(os.path.join(HERE, "packed_golden.npz")))
+    z = _cache["packed"]
+    for pre in z["names"]:
+        pre = str(pre)
+        for g in (0, 1):
+            p, st, r, d = (int(x) for x in z[pre + "meta%d" % g])
+            P = [tuple(int(v) for v in t) for t in z[pre + "P%d" % g]]
+            yield pre, bool(g), p, st, r, d, z[pre + "A"], z[pre + "E%d" % g], P

@@ -123,6 +123,40 @@ def test_gj_scaling_of_the_standard_transform():
     assert n >= 80
 
 
+def test_golden_packed_L():
+    """Elimination::echelonize (default compute_L) and GaussJordan::
+    echelonize: U with L below the diagonal, P, rank and det (GaussTransform's
+    own d for GaussJordan), against LELA's own results."""
+    n = 0
+    for pre, gj, p, st, r, d, A, E, P in golden_io.packed_cases():
+        if st:
+            with pytest.raises(ArithmeticError):
+                oracle.echelon_packed_L_zp(p, A, gj)
+            continue
+        if p >= 2 ** 31:
+            continue
+        gE, gP, gr, gd = oracle.echelon_packed_L_zp(p, A, gj)
+        assert (gr, gd) == (r, d) and gP == P, (pre, gj)
+        assert np.array_equal(gE, E), (pre, gj)
+        n += 1
+    assert n >= 160
+
+
+def test_gauss_transform_det_from_pivots():
+    """The Python mirror's determinant of GaussJordan::echelonize, computed
+    from the pivot columns and values alone, equals LELA's."""
+    from lela_b200.api import gauss_transform_det
+    n = 0
+    for pre, gj, p, st, r, d, A, E, P in golden_io.packed_cases():
+        if st or not gj or p >= 2 ** 31:
+            continue
+        U, r2, _ = oracle.echelon_zp(p, A)
+        pc = [int(np.flatnonzero(U[i])[0]) for i in range(r2)]
+        assert gauss_transform_det(p, A.shape[1], pc, [int(U[i, c]) for i, c in enumerate(pc)]) == d, pre
+        n += 1
+    assert n >= 80
+
+
 def test_transform_identity():
     """R = L P A, with L = [[X, 0], [Y, I]] in the rank's blocks, and R the
     standard method's reduced form (p < 2^31, where Modular<uint32>'s
@@ -445,3 +479,35 @@ def test_live_gj_transform(p):
             if want is not None and p < 2 ** 31:
                 assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1]), (m, n, kind)
                 assert got[2:] == want[2:], (m, n, kind)
+
+
+@need_ref
+@pytest.mark.parametrize("p", [2, 3, 251, 65521, 65536, 2147483647, 4294967291])
+def test_live_packed_L(p):
+    """Both packed non-reduced forms against the restatement (below 2^31;
+    above it whether LELA fails must agree)."""
+    rng = np.random.default_rng(p % 971)
+    for (m, n) in ((1, 1), (2, 7), (7, 13), (13, 7), (40, 40), (48, 80), (80, 48)):
+        for kind in range(4):
+            A = gen.dense_zp(int(rng.integers(1 << 30)), m, n, p)
+            if kind == 1:
+                A[:, ::3] = 0
+            elif kind == 2:
+                r = max(1, min(m, n) // 3)
+                F = gen.dense_zp(1, m, r, p).astype(object) @ gen.dense_zp(2, r, n, p).astype(object)
+                A = (F % p).astype(np.uint32)
+            elif kind == 3:
+                A[m // 2:] = 0
+                A[:, :n // 2] = 0
+            for gj in (False, True):
+                try:
+                    want = oracle.ref_echelon_packed_L_zp(p, A, gj)
+                except ArithmeticError:
+                    want = None
+                try:
+                    got = oracle.echelon_packed_L_zp(p, A, gj)
+                except ArithmeticError:
+                    got = None
+                assert (want is None) == (got is None), (m, n, kind, gj)
+                if want is not None and p < 2 ** 31:
+                    assert np.array_equal(got[0], want[0]) and got[1:] == want[1:], (m, n, kind, gj)
