@@ -157,6 +157,35 @@ def test_gauss_transform_det_from_pivots():
     assert n >= 80
 
 
+def test_packed_L_reference_property():
+    """The property the reference's own tests check (tests/test-elimination.C:
+    28-96): after Elimination::echelonize with compute_L, move_L
+    (elimination.tcc:373-391) takes A's strictly lower entries into L = I,
+    clearing them in A, and then L P A_in equals that A.  The same holds for
+    GaussJordan::echelonize (tests/test-gauss-jordan.C:28-105)."""
+    rng = np.random.default_rng(17)
+    for p in (2, 251, 65521, 2147483647):
+        for (m, n) in ((1, 1), (6, 9), (9, 6), (30, 30), (25, 60), (60, 25)):
+            for kind in range(3):
+                A = gen.dense_zp(int(rng.integers(1 << 30)), m, n, p)
+                if kind == 1:
+                    A[:, ::2] = 0
+                elif kind == 2:
+                    A[m // 3:] = (A[: m - m // 3] * 5) % p
+                for gj in (False, True):
+                    E, P, r, d = oracle.echelon_packed_L_zp(p, A, gj)
+                    L = np.eye(m, dtype=object)
+                    U = E.astype(object).copy()
+                    for i in range(m):
+                        for j in range(min(i, n)):
+                            L[i, j] = U[i, j]
+                            U[i, j] = 0
+                    B = A.astype(object)
+                    for a, b in P:
+                        B[[a, b]] = B[[b, a]]
+                    assert np.array_equal(L.dot(B) % p, U), (p, m, n, kind, gj)
+
+
 def test_transform_identity():
     """R = L P A, with L = [[X, 0], [Y, I]] in the rank's blocks, and R the
     standard method's reduced form (p < 2^31, where Modular<uint32>'s
