@@ -697,10 +697,10 @@ def run_batch(args, cm, stream, torch, dev):
     kernels = [choose.choose("echelon", s_, s_, 0, 1.0, p.bit_length(), s_) for _, p, s_, _ in dense]
     tune_s = time.perf_counter() - t0
     # the selector's regret on this batch's blocks: every candidate timed
-    judge = sel.Autotuner(cm, reps=2)
+    exhaustive = sel.Autotuner(cm, reps=2)
     for _, p, s_, seed in dense:
-        judge.tune_echelon(s_, s_, p, seed=seed)
-    res_sel = sel.evaluate(choose, sel.group_blocks(judge.records))
+        exhaustive.tune_echelon(s_, s_, p, seed=seed)
+    res_sel = sel.evaluate(choose, sel.group_blocks(exhaustive.records))
 
     from lela_b200 import CudaModule
     cm_dense = CudaModule(torch.cuda.current_device())
